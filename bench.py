@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Zone-cycles/s of KHARMA's per-step GRMHD path on B200 (one 128^3 FM-torus meshblock per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl khb|reference]
+
+One step = one full RK2 step (both stages: face fluxes in 3 directions, flux-CT, divergence,
+geometric source, RK update, 1D_W inversion, floors, fixups, boundaries, CFL reduction) of the
+plain FP64 path on a 128x128x128 funky-MKS torus (a = 0.9375, r_in = 6, r_max = 12, gamma 13/9,
+SANE field at beta_min = 100, MC reconstruction, LLF, flux-CT, drift-frame floors).  One
+zone-cycle is one interior zone advanced one RK2 step.  Synthetic data: the initial state is built
+by kharma_b200.problems.fm_torus from a seeded RNG (u jitter +-4%).
+
+For N > 1 (torchrun) every rank advances its own 128^3 block (weak scaling, replicas: no domain
+decomposition and no halo exchange in this path yet); time = max over ranks.
+
+--impl reference times the reference algorithm on the host cores: the CPU oracle (a restatement of
+KHARMA's hot path; kharma.host itself cannot be built here), on a bounded slab of the same torus.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "zone-cycles/s at 128^3 torus: FP64 plain vs FP32-flux form; % of HBM roofline"
+UNIT = "zone-cycles/s"
+B_ALG_PER_ZC = 72 * 8          # algorithmic HBM bytes per zone-cycle, 72 * nvar (nvar = 8)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="khb", choices=["khb", "reference"])
+    ap.add_argument("--size", default="128,128,128")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-kernel-times", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_state(spec):
+    from kharma_b200 import problems
+    from kharma_b200.block import build_geometry
+    geom = build_geometry(spec)
+    P0 = problems.fm_torus(spec, geom, seed=1234)
+    return geom, P0
+
+
+# ----------------------------------------------------------------------------------- CPU side
+def cpu_sample(n1, n2, n3_sample, steps, warm=1):
+    """Oracle (all host threads) on a k-slab of the torus; returns zone-cycles/s and details."""
+    from kharma_b200.spec import torus_spec
+    from oracle import orc
+    spec = torus_spec(n1, n2, n3_sample)
+    o = orc.Oracle(spec)
+    from kharma_b200 import problems
+    P, U = o.init_state(problems.fm_torus(spec, o.geometry(), seed=1234))
+    dt = spec.dt_min
+    for _ in range(warm):
+        _, _, dt, _ = o.step(P, U, dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        _, _, dt, _ = o.step(P, U, dt)
+    el = time.perf_counter() - t0
+    zones = n1 * n2 * n3_sample
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return zones * steps / el, threads, el
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    n1, n2, n3 = [int(x) for x in args.size.split(",")]
+    n3s = max(8, n3 // 16)
+    from kharma_b200.spec import torus_spec
+    from oracle import orc
+    from kharma_b200 import problems
+    spec = torus_spec(n1, n2, n3s)
+    o = orc.Oracle(spec)
+    P, U = o.init_state(problems.fm_torus(spec, o.geometry(), seed=1234))
+    dt = spec.dt_min
+    for _ in range(args.warmup):
+        _, _, dt, _ = o.step(P, U, dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, _, dt, _ = o.step(P, U, dt)
+    el = time.perf_counter() - t0
+    v = n1 * n2 * n3s * args.steps / el
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = (f"oracle port of the reference hot path, {threads} OpenMP threads, {n1}x{n2}x{n3s} slab of the "
+              f"{n1}x{n2}x{n3} torus (same per-zone work), {args.steps} RK2 steps after {args.warmup} warm-up")
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": {"workload": f"FM torus FMKS {n1}x{n2}x{n3} (slab sample)",
+                                            "recon": "linear_mc", "flux": "llf", "b_field": "flux_ct"},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------------------- GPU side
+def kernel_times(block, spec, nsteps=3):
+    """Per-kernel CUDA-event timing of the stage pieces on the launching stream."""
+    import torch
+    from kharma_b200 import _lib
+    lib = block.lib
+    st = block.stream
+    cur = torch.cuda.current_stream()
+    nv = spec.nvar
+    Ps, Us = block.Pf, block.Uf
+    P1 = torch.empty_like(block.P)
+    U1 = torch.empty_like(block.U)
+    from kharma_b200.block import Fields
+    P1f, U1f = Fields(P1), Fields(U1)
+    pf = C.c_void_p(block.pflag.data_ptr())
+    ff = C.c_void_p(block.fflag.data_ptr())
+    names = []
+    times = {}
+
+    def timed(name, fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        _lib.check(fn(), name)
+        e1.record(cur)
+        names.append((name, e0, e1))
+
+    dt = 1e-4
+    for _ in range(nsteps):
+        for stage, (Pin, Uin, Pout, Uout) in ((1, (Ps, Us, P1f, U1f)), (2, (P1f, U1f, Ps, Us))):
+            for d in range(1, spec.ndim + 1):
+                timed(f"k_flux_x{d}", lambda d=d, Pin=Pin: lib.khb_get_flux(block.ctx, d, Pin.ref, st))
+            timed("k_fix_flux", lambda: lib.khb_fix_flux(block.ctx, st))
+            timed("k_zone", lambda stage=stage, Pin=Pin, Uin=Uin, Pout=Pout, Uout=Uout:
+                  lib.khb_zone_pass(block.ctx, stage, dt, Pin.ref, Uin.ref, Us.ref, Pout.ref, Uout.ref, pf, ff, st))
+            timed("k_fixup", lambda Pout=Pout, Uout=Uout: lib.khb_fix_utop_list(block.ctx, Pout.ref, Uout.ref, pf, st))
+            timed("k_boundaries", lambda Pout=Pout, Uout=Uout: lib.khb_boundaries(block.ctx, Pout.ref, Uout.ref, st))
+    torch.cuda.synchronize()
+    for name, e0, e1 in names:
+        times.setdefault(name, []).append(e0.elapsed_time(e1))
+    return {k: (float(np.mean(v)), len(v) // nsteps) for k, v in times.items()}
+
+
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from kharma_b200.block import Block, Driver
+    from kharma_b200.spec import torus_spec
+
+    torch.cuda.set_device(local_rank)
+    n1, n2, n3 = [int(x) for x in args.size.split(",")]
+    spec = torus_spec(n1, n2, n3)
+    geom, P0 = make_state(spec)
+    zones = n1 * n2 * n3
+
+    def run(precision, steps, warmup, sampler=None):
+        sp = torus_spec(n1, n2, n3, precision=precision)
+        b = Block(sp, geometry=geom)
+        b.set_prims(P0)
+        drv = Driver(b)
+        for _ in range(warmup):
+            drv.step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = b.launch_count()
+        if sampler:
+            sampler.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            drv.step()
+        e1.record()
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        if world > 1:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        launches = b.launch_count() - l0
+        return b, drv, ms, launches, clocks
+
+    sampler = ClockSampler(torch.cuda.current_device())
+    b, drv, ms, launches, clocks = run("fp64", args.steps, args.warmup, sampler)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * zones / (ms_step / 1000.0)
+
+    # FP32-flux form on the same workload
+    fp32 = None
+    if not args.no_fp32:
+        b32, _, ms32, _, _ = run("fp32_flux", args.steps, args.warmup)
+        t32 = torch.tensor([ms32], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t32, op=dist.ReduceOp.MAX)
+        v32 = world * zones / (float(t32.item()) / args.steps / 1000.0)
+        fp32 = {"value": v32, "unit": UNIT, "ms_per_step": float(t32.item()) / args.steps,
+                "speedup_vs_fp64": v32 / value}
+        del b32
+
+    # end-to-end through the C ABI with host buffers: H2D of P and U, the step, D2H of P and U
+    e2e = None
+    if not args.no_e2e:
+        hP = torch.empty(b.P.shape, dtype=torch.float64, pin_memory=True)
+        hU = torch.empty(b.U.shape, dtype=torch.float64, pin_memory=True)
+        hP.copy_(b.P)
+        hU.copy_(b.U)
+        torch.cuda.synchronize()
+        ke = max(3, args.steps // 2)
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(ke):
+            b.P.copy_(hP, non_blocking=True)
+            b.U.copy_(hU, non_blocking=True)
+            drv.step()                       # includes the min-dt read-back
+            hP.copy_(b.P, non_blocking=True)
+            hU.copy_(b.U, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        ms_e = float(te.item()) / ke
+        nbytes = 2 * b.P.numel() * 8
+        e2e = {"value": world * zones / (ms_e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes + 8, "ms_per_step": ms_e}
+
+    # roofline of the dominant kernel, timed live with CUDA events
+    peak, peak_kind = measured_peaks()
+    roofline = None
+    ktimes = None
+    if not args.no_kernel_times:
+        ktimes = kernel_times(b, spec)
+        tot = {k: v[0] * v[1] for k, v in ktimes.items()}
+        dom = max(tot, key=tot.get)
+        ms_launch = ktimes[dom][0]
+        nv = spec.nvar
+        # algorithmic bytes per launch: the zone pass moves the stage's state arrays
+        # (stage 1: read P0,U0 write P1,U1; stage 2: read P1,U1,U0 write P2,U2 -> 4.5 nv doubles
+        # per zone per launch on average); a flux pass reads P once (nv doubles per zone).
+        per_zone = {"k_zone": 4.5 * nv * 8}.get(dom, nv * 8)
+        ach = per_zone * zones / (ms_launch / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "peak_kind": peak_kind, "traffic": None,
+                    "alg_bytes_per_zone_per_launch": per_zone,
+                    "step": {"achieved": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9,
+                             "frac": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9 / peak,
+                             "alg_bytes_per_zone_cycle": B_ALG_PER_ZC},
+                    "kernel_ms_per_launch": {k: round(v[0], 4) for k, v in ktimes.items()}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n3s = max(8, n3 // 16)
+        v_cpu, threads, el = cpu_sample(n1, n2, n3s, steps=2)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"oracle port, {threads} threads, {n1}x{n2}x{n3s} slab of the torus, 2 RK2 steps ({el:.1f} s)"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": f"FM torus FMKS {n1}x{n2}x{n3} one meshblock per GPU",
+                          "recon": "linear_mc", "flux": "llf", "b_field": "flux_ct", "inverter": "onedw",
+                          "floors": "drift", "parallelism": f"replicas x{world}",
+                          "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
+               "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
+               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    try:
+        gpu_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,218 @@
+/*
+ * khb.h -- C ABI of libkhb, the B200 (sm_100a) implementation of KHARMA's per-step GRMHD path.
+ *
+ * Each entry point replaces one Kokkos loop (or a fixed sequence of them) inside a KHARMA
+ * package callback; the reference function it stands in for is cited beside it.  Paths are
+ * relative to the KHARMA source tree (AFD-Illinois/kharma).
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a negative KHB_ERR_* code on failure; it never
+ *    aborts and never traps on the device.  khb_last_error() returns a message for the
+ *    calling thread.
+ *  - All work is asynchronous on the caller's cudaStream_t (passed as void*; NULL = legacy
+ *    default stream).  No call synchronizes except the two that return a value to the host,
+ *    khb_get_min_ndt and khb_max_divb, which say so.
+ *  - The caller owns the state: primitive and conserved fields are device arrays of doubles,
+ *    one array per variable (as Parthenon allocates them), each [n3][n2][n1] with i fastest,
+ *    covering the whole block including ghosts.  n1 = nx1 + 2 ng, and n2 (n3) = nx2 + 2 ng
+ *    (nx3 + 2 ng) when that direction is active, else 1.  Variable order is
+ *    rho, u, u1, u2, u3, B1, B2, B3 (primitives) and rho u^t, T^t_t + rho u^t, T^t_1..3,
+ *    B^1..3 sqrt(-g) (conserved), matching KHARMA's VarMap for a GRMHD+flux-CT pack.
+ *  - The context owns only scratch: face fluxes, signal speeds, the intermediate RK stage,
+ *    reduction words and the geometry tables copied in by khb_set_geometry().
+ *  - Per-zone flags keep the reference encodings: pflag is Inverter::Status
+ *    (inverter/invert_template.hpp:53), fflag holds Floors::FFlag bits (floors/floors.hpp:52-70).
+ *    They are int32 device arrays over the block.
+ *  - A context is not thread-safe; use one per host thread or serialize externally.
+ */
+#ifndef KHB_H
+#define KHB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KHB_MAX_VARS 8
+
+enum { KHB_OK = 0, KHB_ERR_ARG = -1, KHB_ERR_CUDA = -2, KHB_ERR_STATE = -3, KHB_ERR_UNSUPPORTED = -4 };
+
+/* Reconstruction schemes (flux/reconstruction.hpp:49) */
+enum { KHB_RECON_DONOR_CELL = 0, KHB_RECON_LINEAR_MC = 1, KHB_RECON_WENO5 = 2, KHB_RECON_PPM = 3 };
+/* Riemann solvers (flux/flux.hpp:110-121) */
+enum { KHB_FLUX_LLF = 0, KHB_FLUX_HLLE = 1 };
+/* Boundary types per face (boundaries/boundaries.cpp:57-368) */
+enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2 };
+/* Floor injection frames (floors/floors.hpp:96) */
+enum { KHB_FRAME_FLUID = 0, KHB_FRAME_NORMAL = 1, KHB_FRAME_DRIFT = 2 };
+/* Arithmetic of reconstruction, Riemann fluxes and EMF averaging */
+enum { KHB_PREC_FP64 = 0, KHB_PREC_FP32_FLUX = 1 };
+/* Driver step semantics (driver/simple_step.cpp, driver/kharma_step.cpp) */
+enum { KHB_DRIVER_SIMPLE = 0, KHB_DRIVER_KHARMA = 1 };
+
+/* Floors::Prescription (floors/floors.hpp:100-117) */
+typedef struct {
+    double rho_min_const, u_min_const;
+    double rho_min_geom, u_min_geom, r_char;
+    double bsq_over_rho_max, bsq_over_u_max, u_over_rho_max;
+    double ktot_max, gamma_max;
+    int32_t use_r_char, temp_adjust_u, adjust_k, radius_dependent_floors;
+    double floors_switch_r;
+} khb_floors;
+
+/* Block and package parameters, filled by the calling packages from their Params. */
+typedef struct {
+    int32_t nx1, nx2, nx3, ng;        /* interior zones per direction, ghost zones */
+    double dx1, dx2, dx3;             /* native-coordinate zone widths (Dxc) */
+    double gam;                       /* GRMHD/gamma */
+    int32_t nvar;                     /* 5 (GRHD) or 8 (GRMHD with cell-centred B and flux-CT) */
+    int32_t recon, riemann, precision;
+    int32_t bc[6];                    /* inner_x1, outer_x1, inner_x2, outer_x2, inner_x3, outer_x3 */
+    int32_t check_inflow_inner_x1, check_inflow_outer_x1;   /* boundaries/check_inflow_* */
+    int32_t zero_polar_flux;          /* boundaries/zero_polar_flux */
+    int32_t fix_polar_flux;           /* b_field/fix_polar_flux */
+    int32_t fix_corner_inner;         /* boundaries/fix_corner_inner */
+    int32_t spherical;                /* coordinates are spherical (floors use r) */
+    int32_t cart_minkowski;           /* Cartesian Minkowski: geometric source is skipped (flux.cpp:407) */
+    int32_t floors_on, floor_frame, recon_floors;
+    int32_t iter_max; double err_tol; /* inverter/iter_max, inverter/err_tol (1D_W: 8, 1e-8) */
+    int32_t fix_average_neighbors, fix_atmosphere;
+    khb_floors floors;
+} khb_config;
+
+/* Coordinate system for khb_build_geometry (coordinates/coordinate_systems.hpp) */
+enum { KHB_BASE_CART_MINKOWSKI = 0, KHB_BASE_SPH_MINKOWSKI = 1, KHB_BASE_SPH_KS = 2, KHB_BASE_SPH_BL = 3 };
+enum { KHB_TRANSFORM_NULL = 0, KHB_TRANSFORM_EKS = 1, KHB_TRANSFORM_MKS = 2, KHB_TRANSFORM_FMKS = 3 };
+typedef struct {
+    int32_t base, transform;
+    double a, hslope, mks_smooth, poly_xt, poly_alpha, startx1;
+} khb_coords;
+
+typedef struct khb_ctx khb_ctx;
+
+/* One device pointer per variable (Parthenon allocates each variable separately). */
+typedef struct { double* v[KHB_MAX_VARS]; } khb_fields;
+
+const char* khb_last_error(void);
+int khb_version(void);
+
+/* Create/destroy a context for one meshblock shape and option set.  Allocates the scratch listed
+ * above on the current device. */
+int khb_create(const khb_config* cfg, khb_ctx** out);
+int khb_destroy(khb_ctx* ctx);
+
+/* Host-side GRCoordinates cache construction (coordinates/gr_coordinates.cpp:96-248,
+ * connection_average_points = 1).  Fills caller host arrays in GRCoordinates layout:
+ *   gcov, gcon  [7][n2+1][n1+1][4][4]   gdet [7][n2+1][n1+1]
+ *   gdet_conn   [n2][n1][4][4][4]       r_center [n2][n1] (embedding r, or |x| if Cartesian)
+ * x1min..x3min are the native coordinates of the first interior face. */
+int khb_build_geometry(const khb_coords* coords, const khb_config* cfg,
+                       double x1min, double x2min, double x3min,
+                       double* gcov, double* gcon, double* gdet, double* gdet_conn, double* r_center);
+
+/* Copy a block's geometry (host arrays in the layout above, e.g. GRCoordinates::gcov_direct)
+ * to the device, in the layout the kernels read. */
+int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const double* gdet,
+                     const double* gdet_conn, const double* r_center);
+
+/* ---------------------------------------------------------------------------------------------
+ * Package-level entry points (each replaces the Kokkos loops of one reference function)
+ * ------------------------------------------------------------------------------------------- */
+
+/* Flux::GetFlux<recon, dir> (flux/get_flux.hpp:60-373): reconstruct P at the dir-faces, compute
+ * conserved states and fluxes (prim_to_flux, flux_functions.hpp:116-178), signal speeds (vchar,
+ * :368-439) and the LLF/HLLE flux into the context's flux scratch for that direction.  Faces
+ * cover [s, e+1] along dir and [s-1, e+1] across it. */
+int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream);
+
+/* B_FluxCT::FixFlux polar corrections (b_flux_ct.cpp:264-303, 372-470) and
+ * KBoundaries::FixFlux (boundaries.cpp:611-690) applied to the raw face fluxes in scratch. */
+int khb_fix_flux(khb_ctx* ctx, void* stream);
+
+/* B_FluxCT::FluxCT (b_flux_ct.cpp:307-370): rewrite the B fluxes in scratch from corner EMFs.
+ * khb_update() applies the same averaging on the fly, so calling this is only needed when the
+ * caller reads the fluxes back (khb_copy_flux). */
+int khb_flux_ct(khb_ctx* ctx, void* stream);
+
+/* Copy one direction's face fluxes (nvar arrays shaped like the block) and max(cmax, cmin)
+ * (one array) from scratch to caller device memory, as doubles. */
+int khb_copy_flux(khb_ctx* ctx, int dir, const khb_fields* F_out, double* ctop_out, void* stream);
+
+/* KHARMADriver::FluxDivergence (kharma_driver.hpp:208-231) with flux-CT B fluxes, plus
+ * Flux::AddGeoSource (flux.cpp:395-444), plus AddStateUpdate's two WeightedSumData calls
+ * (kharma_driver.cpp:339-387):  U_out = gam0 U_s + gam1 U_0 + beta_dt (-div F + S(P_s)),
+ * over the interior.  U_out may alias U_0 or U_s. */
+int khb_update(khb_ctx* ctx, const khb_fields* P_s, const khb_fields* U_s, const khb_fields* U_0,
+               double gam0, double gam1, double beta_dt, const khb_fields* U_out, void* stream);
+
+/* Inverter::BlockUtoP with the 1D_W inverter (inverter.cpp:131-182, onedw.hpp:89-233) and
+ * B_FluxCT::BlockUtoP (b_flux_ct.cpp:196-217) over the interior.  P holds the guess on entry. */
+int khb_utop(khb_ctx* ctx, const khb_fields* U, const khb_fields* P, int32_t* pflag, int32_t* fflag,
+             void* stream);
+
+/* Floors::ApplyGRMHDFloors (floors.cpp:262-270, floors_impl.hpp:45-128) over the interior,
+ * including ceilings and the P->U of floored zones. */
+int khb_apply_floors(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag,
+                     int32_t* fflag, void* stream);
+
+/* Inverter::MeshFixUtoP (fixup.cpp:47-156) over the interior, periodic neighbours wrapped. */
+int khb_fix_utop(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const int32_t* pflag,
+                 void* stream);
+
+/* Physical and periodic boundary conditions for P (fluid primitives) and the conserved field,
+ * then B_P = B_U/gdet and U = U(P) in every ghost zone (boundaries.cpp:369-589 with Parthenon's
+ * outflow/reflecting functions, and Flux::MeshPtoU on the ghosts). */
+int khb_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* stream);
+
+/* Flux::MeshPtoU (flux.cpp:276-322) over the whole block. */
+int khb_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Fused step (the driver's per-stage task list, kharma_step.cpp:77-319 / simple_step.cpp:39-168)
+ * ------------------------------------------------------------------------------------------- */
+
+/* One RK2 stage (stage = 1 or 2) with Parthenon's rk2 weights: fluxes in all active directions,
+ * flux fixes, then ONE fused zone pass doing flux-CT, divergence, geometric source, the RK
+ * combination, 1D_W inversion, floors and the lock-step P->U; then fixups of failed zones and
+ * ghost zones.  P_s/U_s are the stage input, U_0 the step-start conserved state, P_out/U_out the
+ * result.  P_out may alias P_s only if the caller does not need P_s afterwards AND stage == 2
+ * is not reading it (use distinct buffers).  On the last stage the minimum zone timestep is
+ * accumulated on the device (read with khb_get_min_ndt). */
+int khb_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+              const khb_fields* U_0, const khb_fields* P_out, const khb_fields* U_out,
+              int32_t* pflag, int32_t* fflag, void* stream);
+
+/* The fused zone pass of one stage alone: flux-CT, divergence, geometric source, RK combination,
+ * 1D_W inversion, floors and P->U over the interior (and, on stage 2, the CFL reduction), reading
+ * the face fluxes left in scratch by khb_get_flux/khb_fix_flux.  khb_stage = khb_get_flux (each
+ * direction) + khb_fix_flux + khb_zone_pass + khb_fix_utop_list + khb_boundaries. */
+int khb_zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+                  const khb_fields* U_0, const khb_fields* P_out, const khb_fields* U_out,
+                  int32_t* pflag, int32_t* fflag, void* stream);
+
+/* Inverter::MeshFixUtoP over the zones the last khb_zone_pass flagged (no scan of pflag). */
+int khb_fix_utop_list(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const int32_t* pflag,
+                      void* stream);
+
+/* Full RK2 step in place on (P, U) using the context's scratch for the intermediate stage.
+ * Equivalent to two khb_stage calls.  Launches only; no host synchronisation. */
+int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
+             int32_t* pflag, int32_t* fflag, void* stream);
+
+/* Minimum zone timestep (before cfl and clipping) of the last stage-2 zone pass, as
+ * GRMHD::EstimateTimestep computes it (grmhd.cpp:294-330).  Synchronizes the stream. */
+int khb_get_min_ndt(khb_ctx* ctx, double* min_ndt_host, void* stream);
+
+/* B_FluxCT::MaxDivB (b_flux_ct.cpp:566-607): max |corner divB| of the conserved field.
+ * Synchronizes the stream. */
+int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void* stream);
+
+/* Number of device kernel launches issued through this context so far (for accounting). */
+int64_t khb_launch_count(khb_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KHB_H */

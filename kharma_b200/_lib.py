@@ -1,0 +1,129 @@
+"""ctypes binding of libkhb (include/khb.h).
+
+The shared library is built in-tree (kharma_b200/lib/libkhb.so) by kharma_b200.build.  There is
+no fallback: if the library is missing, or a call fails, an exception is raised.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libkhb.so")
+
+MAX_VARS = 8
+
+# enums (include/khb.h)
+RECON = {"donor_cell": 0, "linear_mc": 1, "weno5": 2, "ppm": 3}
+FLUX = {"llf": 0, "hlle": 1}
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
+FRAME = {"fluid": 0, "normal": 1, "drift": 2}
+PREC = {"fp64": 0, "fp32_flux": 1}
+BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
+TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
+
+
+class KhbFloors(C.Structure):
+    _fields_ = [
+        ("rho_min_const", C.c_double), ("u_min_const", C.c_double),
+        ("rho_min_geom", C.c_double), ("u_min_geom", C.c_double), ("r_char", C.c_double),
+        ("bsq_over_rho_max", C.c_double), ("bsq_over_u_max", C.c_double), ("u_over_rho_max", C.c_double),
+        ("ktot_max", C.c_double), ("gamma_max", C.c_double),
+        ("use_r_char", C.c_int32), ("temp_adjust_u", C.c_int32), ("adjust_k", C.c_int32),
+        ("radius_dependent_floors", C.c_int32),
+        ("floors_switch_r", C.c_double),
+    ]
+
+
+class KhbConfig(C.Structure):
+    _fields_ = [
+        ("nx1", C.c_int32), ("nx2", C.c_int32), ("nx3", C.c_int32), ("ng", C.c_int32),
+        ("dx1", C.c_double), ("dx2", C.c_double), ("dx3", C.c_double),
+        ("gam", C.c_double),
+        ("nvar", C.c_int32),
+        ("recon", C.c_int32), ("riemann", C.c_int32), ("precision", C.c_int32),
+        ("bc", C.c_int32 * 6),
+        ("check_inflow_inner_x1", C.c_int32), ("check_inflow_outer_x1", C.c_int32),
+        ("zero_polar_flux", C.c_int32),
+        ("fix_polar_flux", C.c_int32),
+        ("fix_corner_inner", C.c_int32),
+        ("spherical", C.c_int32),
+        ("cart_minkowski", C.c_int32),
+        ("floors_on", C.c_int32), ("floor_frame", C.c_int32), ("recon_floors", C.c_int32),
+        ("iter_max", C.c_int32), ("err_tol", C.c_double),
+        ("fix_average_neighbors", C.c_int32), ("fix_atmosphere", C.c_int32),
+        ("floors", KhbFloors),
+    ]
+
+
+class KhbCoords(C.Structure):
+    _fields_ = [
+        ("base", C.c_int32), ("transform", C.c_int32),
+        ("a", C.c_double), ("hslope", C.c_double), ("mks_smooth", C.c_double),
+        ("poly_xt", C.c_double), ("poly_alpha", C.c_double), ("startx1", C.c_double),
+    ]
+
+
+class KhbFields(C.Structure):
+    _fields_ = [("v", C.c_void_p * MAX_VARS)]
+
+
+# Every entry point declared in include/khb.h, with its ctypes signature
+_P = C.c_void_p
+_D = C.c_double
+_I = C.c_int
+SIGNATURES = {
+    "khb_last_error": (C.c_char_p, []),
+    "khb_version": (_I, []),
+    "khb_create": (_I, [C.POINTER(KhbConfig), C.POINTER(_P)]),
+    "khb_destroy": (_I, [_P]),
+    "khb_build_geometry": (_I, [C.POINTER(KhbCoords), C.POINTER(KhbConfig), _D, _D, _D, _P, _P, _P, _P, _P]),
+    "khb_set_geometry": (_I, [_P, _P, _P, _P, _P, _P]),
+    "khb_get_flux": (_I, [_P, _I, C.POINTER(KhbFields), _P]),
+    "khb_fix_flux": (_I, [_P, _P]),
+    "khb_flux_ct": (_I, [_P, _P]),
+    "khb_copy_flux": (_I, [_P, _I, C.POINTER(KhbFields), _P, _P]),
+    "khb_update": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _D, _D, _D,
+                        C.POINTER(KhbFields), _P]),
+    "khb_utop": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_apply_floors": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_fix_utop": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P]),
+    "khb_boundaries": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
+    "khb_ptou": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
+    "khb_stage": (_I, [_P, _I, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
+                       C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_zone_pass": (_I, [_P, _I, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
+                           C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_fix_utop_list": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P]),
+    "khb_step": (_I, [_P, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_get_min_ndt": (_I, [_P, C.POINTER(_D), _P]),
+    "khb_max_divb": (_I, [_P, C.POINTER(KhbFields), C.POINTER(_D), _P]),
+    "khb_launch_count": (C.c_int64, [_P]),
+}
+
+_lib = None
+
+
+class KhbError(RuntimeError):
+    pass
+
+
+def load():
+    """Load libkhb.so (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise KhbError(f"{LIB_PATH} is missing: build it with `python -m kharma_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc, what=""):
+    """Raise KhbError with the library's message on a nonzero return code."""
+    if rc != 0:
+        msg = load().khb_last_error().decode(errors="replace")
+        raise KhbError(f"{what} failed ({rc}): {msg}")

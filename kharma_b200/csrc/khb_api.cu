@@ -1,0 +1,639 @@
+// khb_api.cu -- host side of libkhb: context, scratch, geometry upload, launches, C ABI.
+#include "khb_kernels.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+
+using namespace khb;
+
+struct khb_ctx {
+    khb_config cfg;
+    Dims d;
+    Phys ph;
+    DevGeom g;
+    int nv;
+    bool fp32;
+    void* F[3];            // raw face fluxes, [nv][N] of FT
+    void* ctop[3];         // max(cmax, cmin) per face, [N] of FT
+    void* emf;             // corner EMFs for khb_flux_ct, [3][N] of FT
+    double* stageP;        // intermediate RK stage
+    double* stageU;
+    unsigned long long* words;   // [0] min zone dt bits, [1] max divB bits
+    int* fail_count;
+    int* fail_list;
+    double* geo_d;
+    float* geo_f;
+    bool geom_set;
+    int64_t launches;
+    unsigned long long dbl_max_bits;   // host source of the reduction reset (outlives async copies)
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define KHB_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(KHB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define KHB_LAUNCHED(ctx)                                                                \
+    do {                                                                                 \
+        (ctx)->launches++;                                                               \
+        cudaError_t e_ = cudaGetLastError();                                             \
+        if (e_ != cudaSuccess) return fail(KHB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+int check_fields(const khb_ctx* ctx, const khb_fields* f, const char* name)
+{
+    if (!f) return fail(KHB_ERR_ARG, std::string(name) + " is NULL");
+    for (int p = 0; p < ctx->nv; ++p)
+        if (!f->v[p]) return fail(KHB_ERR_ARG, std::string(name) + " has a NULL variable pointer");
+    return KHB_OK;
+}
+
+// ------------------------------------------------------------------ fluxes
+template <int RECON, int NV, typename R>
+void launch_flux_t(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    int lo[3], hi[3];
+    const int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
+    for (int a = 0; a < 3; ++a) {
+        const bool active = (a + 1) <= d.ndim;
+        if (a + 1 == dir) { lo[a] = s[a]; hi[a] = e[a] + 1; }
+        else if (active) { lo[a] = s[a] - 1; hi[a] = e[a] + 1; }
+        else { lo[a] = s[a]; hi[a] = e[a]; }
+    }
+    const int ci = hi[0] - lo[0] + 1, cj = hi[1] - lo[1] + 1, ck = hi[2] - lo[2] + 1;
+    const long long total = (long long)ci*cj*ck;
+    k_flux<RECON, NV, R, R><<<blocks_for(total, 128), 128, 0, st>>>(
+        d, ctx->g, ctx->ph, P, (R*)ctx->F[dir-1], (R*)ctx->ctop[dir-1], dir, lo[0], lo[1], lo[2], ci, cj, total);
+}
+
+template <int NV, typename R>
+void launch_flux_r(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
+{
+    switch (ctx->cfg.recon) {
+    case KHB_RECON_DONOR_CELL: launch_flux_t<RECON_DONOR, NV, R>(ctx, dir, P, st); break;
+    case KHB_RECON_LINEAR_MC:  launch_flux_t<RECON_MC, NV, R>(ctx, dir, P, st); break;
+    case KHB_RECON_WENO5:      launch_flux_t<RECON_WENO5, NV, R>(ctx, dir, P, st); break;
+    default:                   launch_flux_t<RECON_PPM, NV, R>(ctx, dir, P, st); break;
+    }
+}
+
+int launch_flux(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
+{
+    if (ctx->nv == 8) {
+        if (ctx->fp32) launch_flux_r<8, float>(ctx, dir, P, st); else launch_flux_r<8, double>(ctx, dir, P, st);
+    } else {
+        if (ctx->fp32) launch_flux_r<5, float>(ctx, dir, P, st); else launch_flux_r<5, double>(ctx, dir, P, st);
+    }
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+template <int NV, typename FT>
+int launch_fix_flux_t(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    FT* F1 = (FT*)ctx->F[0]; FT* F2 = (FT*)ctx->F[1]; FT* F3 = (FT*)ctx->F[2];
+    if (d.ndim >= 2 && (ph.zero_polar_flux || (NV > 5 && ph.fix_polar_flux))) {
+        const int ni = d.ie - d.is + 3, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+        for (int face = 2; face <= 3; ++face) {
+            if (d.bc[face] == KHB_BC_PERIODIC) continue;
+            k_fix_flux_x2<NV, FT><<<blocks_for((long long)ni*nk, 128), 128, 0, st>>>(d, ph, F1, F2, F3, face == 2);
+            KHB_LAUNCHED(ctx);
+        }
+    }
+    const int nj = (d.ndim > 1) ? d.je - d.js + 3 : 1, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+    if (ph.check_inflow_in && d.bc[0] != KHB_BC_PERIODIC) {
+        k_fix_flux_x1<FT><<<blocks_for((long long)nj*nk, 128), 128, 0, st>>>(d, F1, 1);
+        KHB_LAUNCHED(ctx);
+    }
+    if (ph.check_inflow_out && d.bc[1] != KHB_BC_PERIODIC) {
+        k_fix_flux_x1<FT><<<blocks_for((long long)nj*nk, 128), 128, 0, st>>>(d, F1, 0);
+        KHB_LAUNCHED(ctx);
+    }
+    return KHB_OK;
+}
+
+int launch_fix_flux(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
+{
+    if (ctx->nv == 8) return ctx->fp32 ? launch_fix_flux_t<8, float>(ctx, ph, st) : launch_fix_flux_t<8, double>(ctx, ph, st);
+    return ctx->fp32 ? launch_fix_flux_t<5, float>(ctx, ph, st) : launch_fix_flux_t<5, double>(ctx, ph, st);
+}
+
+// ------------------------------------------------------------------ zone pass
+struct ZoneCall {
+    khb_fields Ps, Us, U0, Pout, Uout;
+    int32_t* pflag;
+    int32_t* fflag;
+    double g0, g1, bdt;
+    int mode;
+};
+
+template <int NV, typename FT>
+void launch_zone_t(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    ZoneArgs<FT> a;
+    a.Ps = zc.Ps; a.Us = zc.Us; a.U0 = zc.U0; a.Pout = zc.Pout; a.Uout = zc.Uout;
+    for (int x = 0; x < 3; ++x) { a.F[x] = (const FT*)ctx->F[x]; a.ctop[x] = (const FT*)ctx->ctop[x]; }
+    a.pflag = zc.pflag; a.fflag = zc.fflag;
+    a.g0 = zc.g0; a.g1 = zc.g1; a.bdt = zc.bdt;
+    a.ndt_word = ctx->words;
+    a.fail_count = ctx->fail_count;
+    a.fail_list = ctx->fail_list;
+    a.mode = zc.mode;
+    const long long total = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
+    k_zone<NV, FT><<<blocks_for(total, 128), 128, 0, st>>>(d, ctx->g, ctx->ph, a);
+}
+
+int launch_zone(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
+{
+    if (ctx->nv == 8) { if (ctx->fp32) launch_zone_t<8, float>(ctx, zc, st); else launch_zone_t<8, double>(ctx, zc, st); }
+    else              { if (ctx->fp32) launch_zone_t<5, float>(ctx, zc, st); else launch_zone_t<5, double>(ctx, zc, st); }
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+// ------------------------------------------------------------------ fixups, boundaries
+int launch_fixup(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, const int32_t* pflag, cudaStream_t st)
+{
+    if (!ctx->ph.fix_avg && !ctx->ph.fix_atmo) return KHB_OK;
+    const unsigned nb = 4 * 148;
+    if (ctx->nv == 8) k_fixup<8><<<nb, 128, 0, st>>>(ctx->d, ctx->g, ctx->ph, P, U, pflag, ctx->fail_count, ctx->fail_list);
+    else              k_fixup<5><<<nb, 128, 0, st>>>(ctx->d, ctx->g, ctx->ph, P, U, pflag, ctx->fail_count, ctx->fail_list);
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+template <int NV>
+int launch_boundaries_t(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    const Phys& ph = ctx->ph;
+    const int cnt_k = d.ke - d.ks + 1;
+    bool physical = false;
+    // X1 faces over the interior j range, then X2 faces over all i, then the corner fix
+    for (int face = 0; face < 2; ++face) {
+        if (d.bc[face] == KHB_BC_PERIODIC) continue;
+        physical = true;
+        const int cnt_j = d.je - d.js + 1;
+        k_bc<NV><<<blocks_for((long long)d.is*cnt_j*cnt_k, 128), 128, 0, st>>>(d, ctx->g, ph, P, U, face, d.js, cnt_j, d.ks, cnt_k);
+        KHB_LAUNCHED(ctx);
+    }
+    if (d.ndim >= 2) {
+        for (int face = 2; face < 4; ++face) {
+            if (d.bc[face] == KHB_BC_PERIODIC) continue;
+            physical = true;
+            k_bc<NV><<<blocks_for((long long)d.js*d.n1*cnt_k, 128), 128, 0, st>>>(d, ctx->g, ph, P, U, face, 0, d.n1, d.ks, cnt_k);
+            KHB_LAUNCHED(ctx);
+        }
+        if (ctx->cfg.fix_corner_inner && d.bc[0] != KHB_BC_PERIODIC && d.bc[3] != KHB_BC_PERIODIC) {
+            k_bc<NV><<<blocks_for((long long)d.is*d.n2*cnt_k, 128), 128, 0, st>>>(d, ctx->g, ph, P, U, 0, 0, d.n2, d.ks, cnt_k);
+            KHB_LAUNCHED(ctx);
+        }
+    }
+    if (physical) {
+        const long long tot = (long long)d.n1*d.n2*cnt_k;
+        k_ghost_ptou<NV><<<blocks_for(tot, 128), 128, 0, st>>>(d, ctx->g, ph, P, U);
+        KHB_LAUNCHED(ctx);
+    }
+    int pmask = 0;
+    if (d.bc[0] == KHB_BC_PERIODIC) pmask |= 1;
+    if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) pmask |= 2;
+    if (d.ndim >= 3 && d.bc[4] == KHB_BC_PERIODIC) pmask |= 4;
+    if (pmask) {
+        k_periodic<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, P, U, pmask);
+        KHB_LAUNCHED(ctx);
+    }
+    return KHB_OK;
+}
+
+int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
+{
+    return ctx->nv == 8 ? launch_boundaries_t<8>(ctx, P, U, st) : launch_boundaries_t<5>(ctx, P, U, st);
+}
+
+size_t ft_size(const khb_ctx* ctx) { return ctx->fp32 ? sizeof(float) : sizeof(double); }
+
+// Parthenon "rk2" low-storage weights: gam0 = {0, 1/2}, gam1 = {1, 1/2}, beta = {1, 1/2}
+const double kRkGam0[2] = {0.0, 0.5}, kRkGam1[2] = {1.0, 0.5}, kRkBeta[2] = {1.0, 0.5};
+
+int zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+              const khb_fields& U0, const khb_fields& Pout, const khb_fields& Uout,
+              int32_t* pflag, int32_t* fflag, cudaStream_t st)
+{
+    const int s = stage - 1;
+    if (stage == 2) {
+        // the minimum is taken over bit patterns; start from the pattern of DBL_MAX
+        KHB_CUDA(cudaMemcpyAsync(ctx->words, &ctx->dbl_max_bits, sizeof(unsigned long long),
+                                 cudaMemcpyHostToDevice, st));
+    }
+    KHB_CUDA(cudaMemsetAsync(ctx->fail_count, 0, sizeof(int), st));
+    ZoneCall zc;
+    zc.Ps = Ps; zc.Us = Us; zc.U0 = U0; zc.Pout = Pout; zc.Uout = Uout;
+    zc.pflag = pflag; zc.fflag = fflag;
+    zc.g0 = kRkGam0[s]; zc.g1 = kRkGam1[s]; zc.bdt = kRkBeta[s] * dt;
+    zc.mode = M_UPDATE | M_UTOP | M_FLOORS | M_PTOU | M_FAILLIST | (stage == 2 ? M_DT : 0);
+    return launch_zone(ctx, zc, st);
+}
+
+int do_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+             const khb_fields& U0, const khb_fields& Pout, const khb_fields& Uout,
+             int32_t* pflag, int32_t* fflag, cudaStream_t st)
+{
+    int rc;
+    for (int dir = 1; dir <= ctx->d.ndim; ++dir)
+        if ((rc = launch_flux(ctx, dir, Ps, st))) return rc;
+    if ((rc = launch_fix_flux(ctx, ctx->ph, st))) return rc;
+    if ((rc = zone_pass(ctx, stage, dt, Ps, Us, U0, Pout, Uout, pflag, fflag, st))) return rc;
+    if ((rc = launch_fixup(ctx, Pout, Uout, pflag, st))) return rc;
+    return launch_boundaries(ctx, Pout, Uout, st);
+}
+
+} // namespace
+
+// ======================================================================== C ABI
+extern "C" {
+
+const char* khb_last_error(void) { return g_err.c_str(); }
+int khb_version(void) { return 100; }
+
+int khb_create(const khb_config* cfg, khb_ctx** out)
+{
+    if (!cfg || !out) return fail(KHB_ERR_ARG, "khb_create: NULL argument");
+    *out = nullptr;
+    if (cfg->nvar != 5 && cfg->nvar != 8) return fail(KHB_ERR_UNSUPPORTED, "nvar must be 5 or 8");
+    if (cfg->recon < 0 || cfg->recon > 3) return fail(KHB_ERR_UNSUPPORTED, "unknown reconstruction");
+    if (cfg->ng < 3) return fail(KHB_ERR_ARG, "need at least 3 ghost zones");
+    if (cfg->nx1 < 1 || cfg->nx2 < 1 || cfg->nx3 < 1) return fail(KHB_ERR_ARG, "bad block size");
+    if (cfg->nx2 == 1 && cfg->nx3 > 1) return fail(KHB_ERR_UNSUPPORTED, "x3 active with x2 inactive");
+    if (cfg->precision != KHB_PREC_FP64 && cfg->precision != KHB_PREC_FP32_FLUX)
+        return fail(KHB_ERR_UNSUPPORTED, "unknown precision");
+    khb_ctx* c = new khb_ctx();
+    std::memset((void*)c, 0, sizeof(khb_ctx));
+    c->cfg = *cfg;
+    c->nv = cfg->nvar;
+    c->dbl_max_bits = 0x7FEFFFFFFFFFFFFFull;
+    c->fp32 = cfg->precision == KHB_PREC_FP32_FLUX;
+    Dims& d = c->d;
+    d.nx1 = cfg->nx1; d.nx2 = cfg->nx2; d.nx3 = cfg->nx3;
+    d.ndim = 1 + (cfg->nx2 > 1) + (cfg->nx3 > 1);
+    d.n1 = cfg->nx1 + 2*cfg->ng;
+    d.n2 = (cfg->nx2 > 1) ? cfg->nx2 + 2*cfg->ng : 1;
+    d.n3 = (cfg->nx3 > 1) ? cfg->nx3 + 2*cfg->ng : 1;
+    d.is = cfg->ng; d.ie = cfg->ng + cfg->nx1 - 1;
+    d.js = (cfg->nx2 > 1) ? cfg->ng : 0; d.je = d.js + cfg->nx2 - 1;
+    d.ks = (cfg->nx3 > 1) ? cfg->ng : 0; d.ke = d.ks + cfg->nx3 - 1;
+    d.N = (long long)d.n1*d.n2*d.n3;
+    d.sj = d.n1; d.sk = (long long)d.n1*d.n2;
+    for (int x = 0; x < 6; ++x) d.bc[x] = cfg->bc[x];
+    Phys& ph = c->ph;
+    ph.gam = cfg->gam;
+    ph.riemann = cfg->riemann;
+    ph.recon_floors = cfg->recon_floors && cfg->floors_on;
+    ph.spherical = cfg->spherical;
+    ph.cart_minkowski = cfg->cart_minkowski;
+    ph.floors_on = cfg->floors_on;
+    ph.frame = cfg->floor_frame;
+    ph.iter_max = cfg->iter_max;
+    ph.err_tol = cfg->err_tol;
+    ph.fix_avg = cfg->fix_average_neighbors;
+    ph.fix_atmo = cfg->fix_atmosphere;
+    ph.dx1 = cfg->dx1; ph.dx2 = cfg->dx2; ph.dx3 = cfg->dx3;
+    ph.zero_polar_flux = cfg->zero_polar_flux;
+    ph.fix_polar_flux = cfg->fix_polar_flux && cfg->spherical;
+    ph.check_inflow_in = cfg->check_inflow_inner_x1;
+    ph.check_inflow_out = cfg->check_inflow_outer_x1;
+    std::memcpy(&ph.fl, &cfg->floors, sizeof(khb_floors));
+
+    const size_t N = (size_t)d.N, fs = ft_size(c);
+    auto alloc = [&](void** p, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+        return e;
+    };
+    cudaError_t e = cudaSuccess;
+    for (int x = 0; x < 3 && e == cudaSuccess; ++x) {
+        e = alloc(&c->F[x], fs * c->nv * N);
+        if (e == cudaSuccess) e = alloc(&c->ctop[x], fs * N);
+    }
+    if (e == cudaSuccess) e = alloc(&c->emf, fs * 3 * N);
+    if (e == cudaSuccess) e = alloc((void**)&c->stageP, sizeof(double) * c->nv * N);
+    if (e == cudaSuccess) e = alloc((void**)&c->stageU, sizeof(double) * c->nv * N);
+    if (e == cudaSuccess) e = alloc((void**)&c->words, sizeof(unsigned long long) * 4);
+    if (e == cudaSuccess) e = alloc((void**)&c->fail_count, sizeof(int) * 4);
+    if (e == cudaSuccess) e = alloc((void**)&c->fail_list, sizeof(int) * N);
+    if (e != cudaSuccess) {
+        khb_destroy(c);
+        return fail(KHB_ERR_CUDA, std::string("khb_create: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return KHB_OK;
+}
+
+int khb_destroy(khb_ctx* c)
+{
+    if (!c) return KHB_OK;
+    for (int x = 0; x < 3; ++x) { cudaFree(c->F[x]); cudaFree(c->ctop[x]); }
+    cudaFree(c->emf); cudaFree(c->stageP); cudaFree(c->stageU);
+    cudaFree(c->words); cudaFree(c->fail_count); cudaFree(c->fail_list);
+    cudaFree(c->geo_d); cudaFree(c->geo_f);
+    delete c;
+    return KHB_OK;
+}
+
+int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const double* gdet,
+                     const double* gdet_conn, const double* r_center)
+{
+    if (!ctx || !gcov || !gcon || !gdet || !gdet_conn || !r_center) return fail(KHB_ERR_ARG, "khb_set_geometry: NULL argument");
+    const Dims& d = ctx->d;
+    const int G1 = d.n1 + 1, G2 = d.n2 + 1;
+    const size_t gs = (size_t)G1*G2;
+    // device layout: for loc 0..3: gcov [16][G2][G1], gcon [16][G2][G1], gdet [G2][G1]; then
+    // gdet_conn [64][n2][n1] and r_center [n2][n1]
+    const size_t per_loc = 33 * gs, n2n1 = (size_t)d.n2*d.n1;
+    const size_t total = 4*per_loc + 64*n2n1 + n2n1;
+    std::vector<double> h(total);
+    std::vector<float> hf(3*per_loc);
+    for (int loc = 0; loc < 4; ++loc) {
+        double* base = h.data() + loc*per_loc;
+        for (size_t x = 0; x < gs; ++x) {
+            const size_t src = (size_t)loc*gs + x;
+            for (int m = 0; m < 16; ++m) {
+                base[m*gs + x] = gcov[src*16 + m];
+                base[(16 + m)*gs + x] = gcon[src*16 + m];
+            }
+            base[32*gs + x] = gdet[src];
+        }
+        if (loc < 3) for (size_t x = 0; x < per_loc; ++x) hf[loc*per_loc + x] = (float)base[x];
+    }
+    double* gc = h.data() + 4*per_loc;
+    for (size_t x = 0; x < n2n1; ++x)
+        for (int m = 0; m < 64; ++m) gc[m*n2n1 + x] = gdet_conn[x*64 + m];
+    std::memcpy(h.data() + 4*per_loc + 64*n2n1, r_center, n2n1*sizeof(double));
+    if (!ctx->geo_d) {
+        KHB_CUDA(cudaMalloc((void**)&ctx->geo_d, total*sizeof(double)));
+        KHB_CUDA(cudaMalloc((void**)&ctx->geo_f, hf.size()*sizeof(float)));
+    }
+    KHB_CUDA(cudaMemcpy(ctx->geo_d, h.data(), total*sizeof(double), cudaMemcpyHostToDevice));
+    KHB_CUDA(cudaMemcpy(ctx->geo_f, hf.data(), hf.size()*sizeof(float), cudaMemcpyHostToDevice));
+    DevGeom& g = ctx->g;
+    g.G1 = G1; g.G2 = G2; g.n1 = d.n1; g.gs = (long long)gs;
+    for (int loc = 0; loc < 4; ++loc) {
+        g.gcov[loc] = ctx->geo_d + loc*per_loc;
+        g.gcon[loc] = ctx->geo_d + loc*per_loc + 16*gs;
+        g.gdet[loc] = ctx->geo_d + loc*per_loc + 32*gs;
+        if (loc < 3) {
+            g.gcov_f[loc] = ctx->geo_f + loc*per_loc;
+            g.gcon_f[loc] = ctx->geo_f + loc*per_loc + 16*gs;
+            g.gdet_f[loc] = ctx->geo_f + loc*per_loc + 32*gs;
+        }
+    }
+    g.gdet_conn = ctx->geo_d + 4*per_loc;
+    g.rcen = ctx->geo_d + 4*per_loc + 64*n2n1;
+    ctx->geom_set = true;
+    return KHB_OK;
+}
+
+#define KHB_NEED_GEOM(ctx) do { if (!(ctx)) return fail(KHB_ERR_ARG, "NULL context"); \
+    if (!(ctx)->geom_set) return fail(KHB_ERR_STATE, "geometry not set (call khb_set_geometry)"); } while (0)
+
+int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (dir < 1 || dir > ctx->d.ndim) return fail(KHB_ERR_ARG, "khb_get_flux: dir out of range");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P"))) return rc;
+    return launch_flux(ctx, dir, *P, S(stream));
+}
+
+int khb_fix_flux(khb_ctx* ctx, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    return launch_fix_flux(ctx, ctx->ph, S(stream));
+}
+
+int khb_flux_ct(khb_ctx* ctx, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (ctx->nv < 8 || ctx->d.ndim < 2) return KHB_OK;
+    const Dims& d = ctx->d;
+    const long long tot = (long long)(d.ie - d.is + 2)*(d.je - d.js + 2)*((d.ndim > 2) ? d.ke - d.ks + 2 : 1);
+    if (ctx->fp32) {
+        k_emf<float><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (float*)ctx->F[0], (float*)ctx->F[1], (float*)ctx->F[2], (float*)ctx->emf);
+        KHB_LAUNCHED(ctx);
+        k_ct_apply<float><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (float*)ctx->F[0], (float*)ctx->F[1], (float*)ctx->F[2], (const float*)ctx->emf);
+    } else {
+        k_emf<double><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (double*)ctx->F[0], (double*)ctx->F[1], (double*)ctx->F[2], (double*)ctx->emf);
+        KHB_LAUNCHED(ctx);
+        k_ct_apply<double><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (double*)ctx->F[0], (double*)ctx->F[1], (double*)ctx->F[2], (const double*)ctx->emf);
+    }
+    KHB_LAUNCHED(ctx);
+    // zero polar fluxes again after the rewrite (KBoundaries::FixFlux acts on the final fluxes)
+    if (ctx->ph.zero_polar_flux) {
+        Phys ph = ctx->ph;
+        ph.fix_polar_flux = 0;
+        ph.check_inflow_in = ph.check_inflow_out = 0;
+        return launch_fix_flux(ctx, ph, S(stream));
+    }
+    return KHB_OK;
+}
+
+int khb_copy_flux(khb_ctx* ctx, int dir, const khb_fields* F_out, double* ctop_out, void* stream)
+{
+    if (!ctx || dir < 1 || dir > 3 || !F_out) return fail(KHB_ERR_ARG, "khb_copy_flux: bad argument");
+    const long long N = ctx->d.N;
+    if (ctx->fp32)
+        k_copy_flux<float><<<blocks_for(N, 256), 256, 0, S(stream)>>>(N, ctx->nv, (const float*)ctx->F[dir-1], (const float*)ctx->ctop[dir-1], *F_out, ctop_out);
+    else
+        k_copy_flux<double><<<blocks_for(N, 256), 256, 0, S(stream)>>>(N, ctx->nv, (const double*)ctx->F[dir-1], (const double*)ctx->ctop[dir-1], *F_out, ctop_out);
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+int khb_update(khb_ctx* ctx, const khb_fields* P_s, const khb_fields* U_s, const khb_fields* U_0,
+               double gam0, double gam1, double beta_dt, const khb_fields* U_out, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
+        (rc = check_fields(ctx, U_0, "U_0")) || (rc = check_fields(ctx, U_out, "U_out"))) return rc;
+    ZoneCall zc;
+    std::memset(&zc, 0, sizeof(zc));
+    zc.Ps = *P_s; zc.Us = *U_s; zc.U0 = *U_0; zc.Pout = *P_s; zc.Uout = *U_out;
+    zc.g0 = gam0; zc.g1 = gam1; zc.bdt = beta_dt;
+    zc.mode = M_UPDATE;
+    return launch_zone(ctx, zc, S(stream));
+}
+
+int khb_utop(khb_ctx* ctx, const khb_fields* U, const khb_fields* P, int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_utop: NULL flags");
+    ZoneCall zc;
+    std::memset(&zc, 0, sizeof(zc));
+    zc.Ps = *P; zc.Us = *U; zc.U0 = *U; zc.Pout = *P; zc.Uout = *U;
+    zc.pflag = pflag; zc.fflag = fflag;
+    zc.mode = M_UTOP;
+    return launch_zone(ctx, zc, S(stream));
+}
+
+int khb_apply_floors(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_apply_floors: NULL flags");
+    ZoneCall zc;
+    std::memset(&zc, 0, sizeof(zc));
+    zc.Ps = *P; zc.Us = *U; zc.U0 = *U; zc.Pout = *P; zc.Uout = *U;
+    zc.pflag = pflag; zc.fflag = fflag;
+    zc.mode = M_FLOORS;
+    return launch_zone(ctx, zc, S(stream));
+}
+
+int khb_fix_utop(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const int32_t* pflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
+    if (!pflag) return fail(KHB_ERR_ARG, "khb_fix_utop: NULL pflag");
+    // build the failed-zone list from pflag with a no-op zone pass
+    KHB_CUDA(cudaMemsetAsync(ctx->fail_count, 0, sizeof(int), S(stream)));
+    ZoneCall zc;
+    std::memset(&zc, 0, sizeof(zc));
+    zc.Ps = *P; zc.Us = *U; zc.U0 = *U; zc.Pout = *P; zc.Uout = *U;
+    zc.pflag = const_cast<int32_t*>(pflag); zc.fflag = const_cast<int32_t*>(pflag);
+    zc.mode = M_FAILLIST;
+    if ((rc = launch_zone(ctx, zc, S(stream)))) return rc;
+    return launch_fixup(ctx, *P, *U, pflag, S(stream));
+}
+
+int khb_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
+    return launch_boundaries(ctx, *P, *U, S(stream));
+}
+
+int khb_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
+    const long long N = ctx->d.N;
+    if (ctx->nv == 8) k_ptou<8><<<blocks_for(N, 128), 128, 0, S(stream)>>>(ctx->d, ctx->g, ctx->ph, *P, *U);
+    else              k_ptou<5><<<blocks_for(N, 128), 128, 0, S(stream)>>>(ctx->d, ctx->g, ctx->ph, *P, *U);
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+int khb_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+              const khb_fields* U_0, const khb_fields* P_out, const khb_fields* U_out,
+              int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_stage: stage must be 1 or 2");
+    int rc;
+    if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
+        (rc = check_fields(ctx, U_0, "U_0")) || (rc = check_fields(ctx, P_out, "P_out")) ||
+        (rc = check_fields(ctx, U_out, "U_out"))) return rc;
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_stage: NULL flags");
+    return do_stage(ctx, stage, dt, *P_s, *U_s, *U_0, *P_out, *U_out, pflag, fflag, S(stream));
+}
+
+int khb_zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+                  const khb_fields* U_0, const khb_fields* P_out, const khb_fields* U_out,
+                  int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_zone_pass: stage must be 1 or 2");
+    int rc;
+    if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
+        (rc = check_fields(ctx, U_0, "U_0")) || (rc = check_fields(ctx, P_out, "P_out")) ||
+        (rc = check_fields(ctx, U_out, "U_out"))) return rc;
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_zone_pass: NULL flags");
+    return zone_pass(ctx, stage, dt, *P_s, *U_s, *U_0, *P_out, *U_out, pflag, fflag, S(stream));
+}
+
+int khb_fix_utop_list(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const int32_t* pflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
+    if (!pflag) return fail(KHB_ERR_ARG, "khb_fix_utop_list: NULL pflag");
+    return launch_fixup(ctx, *P, *U, pflag, S(stream));
+}
+
+int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
+             int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_step: NULL flags");
+    khb_fields P1, U1;
+    std::memset(&P1, 0, sizeof(P1)); std::memset(&U1, 0, sizeof(U1));
+    for (int p = 0; p < ctx->nv; ++p) {
+        P1.v[p] = ctx->stageP + (size_t)p*ctx->d.N;
+        U1.v[p] = ctx->stageU + (size_t)p*ctx->d.N;
+    }
+    if ((rc = do_stage(ctx, 1, dt, *P, *U, *U, P1, U1, pflag, fflag, S(stream)))) return rc;
+    return do_stage(ctx, 2, dt, P1, U1, *U, *P, *U, pflag, fflag, S(stream));
+}
+
+int khb_get_min_ndt(khb_ctx* ctx, double* min_ndt_host, void* stream)
+{
+    if (!ctx || !min_ndt_host) return fail(KHB_ERR_ARG, "khb_get_min_ndt: NULL argument");
+    unsigned long long bits = 0;
+    KHB_CUDA(cudaMemcpyAsync(&bits, ctx->words, sizeof(bits), cudaMemcpyDeviceToHost, S(stream)));
+    KHB_CUDA(cudaStreamSynchronize(S(stream)));
+    std::memcpy(min_ndt_host, &bits, sizeof(double));
+    return KHB_OK;
+}
+
+int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (!U || !max_divb_host) return fail(KHB_ERR_ARG, "khb_max_divb: NULL argument");
+    if (ctx->nv < 8 || ctx->d.ndim < 2) { *max_divb_host = 0.; return KHB_OK; }
+    const Dims& d = ctx->d;
+    // b_flux_ct.cpp:554-564: skip the X1 corners of physical boundaries without Bflux0 fixes
+    const int avoid_in = d.bc[0] != KHB_BC_PERIODIC, avoid_out = d.bc[1] != KHB_BC_PERIODIC;
+    const int i_lo = d.is + avoid_in, i_hi = d.ie + !avoid_out;
+    KHB_CUDA(cudaMemsetAsync(ctx->words + 1, 0, sizeof(unsigned long long), S(stream)));
+    const long long tot = (long long)(i_hi - i_lo + 1)*(d.je - d.js + 2)*((d.ndim > 2) ? d.ke - d.ks + 2 : 1);
+    k_divb<<<blocks_for(tot, 256), 256, 0, S(stream)>>>(d, ctx->ph, *U, i_lo, i_hi, ctx->words + 1);
+    KHB_LAUNCHED(ctx);
+    unsigned long long bits = 0;
+    KHB_CUDA(cudaMemcpyAsync(&bits, ctx->words + 1, sizeof(bits), cudaMemcpyDeviceToHost, S(stream)));
+    KHB_CUDA(cudaStreamSynchronize(S(stream)));
+    std::memcpy(max_divb_host, &bits, sizeof(double));
+    return KHB_OK;
+}
+
+int64_t khb_launch_count(khb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+} // extern "C"

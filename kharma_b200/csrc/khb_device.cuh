@@ -1,0 +1,536 @@
+// khb_device.cuh -- device-side GRMHD functions for the per-step kernels (sm_100a).
+//
+// These restate KHARMA's device functions for one zone or face at a time.  The flux-side
+// functions are templated on the arithmetic type R so that the same code serves the FP64
+// path and the FP32-flux form; the zone-side functions (inversion, floors, P->U) are FP64.
+// Evaluation order follows the reference expression by expression so the FP64 path agrees
+// with a reference build to rounding level.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace khb {
+
+// Kokkos::max/min semantics, as used through m::max/m::min in the reference
+template <typename R> __device__ __forceinline__ R kmax(R a, R b) { return (a < b) ? b : a; }
+template <typename R> __device__ __forceinline__ R kmin(R a, R b) { return (b < a) ? b : a; }
+template <typename R> __device__ __forceinline__ R kclip(R n, R lo, R hi) { return kmin(kmax(lo, n), hi); }
+
+__device__ __forceinline__ float  dsqrt(float x)  { return sqrtf(x); }
+__device__ __forceinline__ double dsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float  dabs(float x)   { return fabsf(x); }
+__device__ __forceinline__ double dabs(double x)  { return fabs(x); }
+
+enum { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3 };
+
+// ------------------------------------------------------------------ reconstruction
+// flux/reconstruction.hpp:52-56
+template <typename R>
+__device__ __forceinline__ R mc_lim(R dm, R dp)
+{
+    const R r = (dabs(dp) > R(0) ? dm/dp : R(2));
+    return kmax(R(0), kmin(R(2), kmin(R(2)*r, R(0.5)*(R(1)+r))));
+}
+
+// Value at the right face of a zone with stencil x1..x5 (reconstruct_right, :114-204, :351-394)
+template <int RECON, typename R>
+__device__ __forceinline__ R recon_right(R x1, R x2, R x3, R x4, R x5)
+{
+    if (RECON == RECON_DONOR) {
+        return x3;
+    } else if (RECON == RECON_MC) {
+        return x3 + R(0.5)*(mc_lim(x3 - x2, x4 - x3)*(x4 - x3));
+    } else if (RECON == RECON_WENO5) {
+        // WENO5-JS (T07 A18, S11 8-9), reconstruction.hpp:183-204.  Weights are always formed in
+        // FP64: with EPS = 1e-26 the squared denominators underflow FP32.
+        const double y1 = x1, y2 = x2, y3 = x3, y4 = x4, y5 = x5;
+        double c1, c2, b0, b1, b2;
+        c1 = y1 - 2.*y2 + y3; c2 = y1 - 4.*y2 + 3.*y3;
+        b0 = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        c1 = y2 - 2.*y3 + y4; c2 = y4 - y2;
+        b1 = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        c1 = y3 - 2.*y4 + y5; c2 = y5 - 4.*y4 + 3.*y3;
+        b2 = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        double d0 = 1.e-26 + b0, d1 = 1.e-26 + b1, d2 = 1.e-26 + b2;
+        d0 *= d0; d1 *= d1; d2 *= d2;
+        const double w0 = (1./16.)/d0, w1 = (5./8.)/d1, w2 = (5./16.)/d2;
+        const double W = w0 + w1 + w2;
+        return (R)(((3./8.)*y1 - (5./4.)*y2 + (15./8.)*y3)*(w0 / W) +
+                   ((-1./8.)*y2 + (3./4.)*y3 + (3./8.)*y4)*(w1 / W) +
+                   ((3./8.)*y3 + (3./4.)*y4 - (1./8.)*y5)*(w2 / W));
+    } else {
+        // PPM (Colella & Woodward with CS limiters), reconstruction.hpp:351-381: qrv
+        R qlv = (R(7)*(x3 + x2) - (x1 + x4))/R(12);
+        R qrv = (R(7)*(x3 + x4) - (x2 + x5))/R(12);
+        qlv = kmax(qlv, kmin(x3, x2));
+        qlv = kmin(qlv, kmax(x3, x2));
+        qrv = kmax(qrv, kmin(x3, x4));
+        qrv = kmin(qrv, kmax(x3, x4));
+        const R qc = qrv - x3, qd = qlv - x3;
+        if ((qc*qd) >= R(0)) return x3;
+        if (dabs(qc) >= R(2)*dabs(qd)) qrv = x3 - R(2)*qd;
+        return qrv;
+    }
+}
+// Value at the left face of a zone (reconstruct_left, :114-204, :351-394)
+template <int RECON, typename R>
+__device__ __forceinline__ R recon_left(R x1, R x2, R x3, R x4, R x5)
+{
+    if (RECON == RECON_DONOR) {
+        return x3;
+    } else if (RECON == RECON_MC) {
+        return x3 - R(0.5)*(mc_lim(x3 - x2, x4 - x3)*(x4 - x3));
+    } else if (RECON == RECON_WENO5) {
+        const double y1 = x1, y2 = x2, y3 = x3, y4 = x4, y5 = x5;
+        double c1, c2, b0, b1, b2;
+        c1 = y1 - 2.*y2 + y3; c2 = y1 - 4.*y2 + 3.*y3;
+        b0 = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        c1 = y2 - 2.*y3 + y4; c2 = y4 - y2;
+        b1 = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        c1 = y3 - 2.*y4 + y5; c2 = y5 - 4.*y4 + 3.*y3;
+        b2 = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        double d0 = 1.e-26 + b0, d1 = 1.e-26 + b1, d2 = 1.e-26 + b2;
+        d0 *= d0; d1 *= d1; d2 *= d2;
+        const double w0 = (1./16.)/d2, w1 = (5./8.)/d1, w2 = (5./16.)/d0;
+        const double W = w0 + w1 + w2;
+        return (R)(((3./8.)*y5 - (5./4.)*y4 + (15./8.)*y3)*(w0 / W) +
+                   ((-1./8.)*y4 + (3./4.)*y3 + (3./8.)*y2)*(w1 / W) +
+                   ((3./8.)*y3 + (3./4.)*y2 - (1./8.)*y1)*(w2 / W));
+    } else {
+        R qlv = (R(7)*(x3 + x2) - (x1 + x4))/R(12);
+        R qrv = (R(7)*(x3 + x4) - (x2 + x5))/R(12);
+        qlv = kmax(qlv, kmin(x3, x2));
+        qlv = kmin(qlv, kmax(x3, x2));
+        qrv = kmax(qrv, kmin(x3, x4));
+        qrv = kmin(qrv, kmax(x3, x4));
+        const R qc = qrv - x3, qd = qlv - x3;
+        if ((qc*qd) >= R(0)) return x3;
+        if (dabs(qd) >= R(2)*dabs(qc)) qlv = x3 - R(2)*qc;
+        return qlv;
+    }
+}
+
+// ------------------------------------------------------------------ geometry at one point
+// Full covariant metric, the inverse-metric entries the flux path uses, and sqrt(-g).
+template <typename R>
+struct FaceGeom {
+    R gcov[4][4];
+    R gcon00, gcon0[4];   // gcon[0][mu]
+    R gcon_dd;            // gcon[dir][dir]
+    R gdet;
+};
+
+// 4-vectors (types.hpp:90-95)
+template <typename R>
+struct FourVec { R ucon[4], ucov[4], bcon[4], bcov[4]; };
+
+template <typename R>
+__device__ __forceinline__ R dot4(const R* a, const R* b)
+{
+    return a[0]*b[0] + a[1]*b[1] + a[2]*b[2] + a[3]*b[3];
+}
+
+// gr_coordinates.hpp:227-232 (lower with the full gcov)
+template <typename R>
+__device__ __forceinline__ void lower4(const R g[4][4], const R* vcon, R* vcov)
+{
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        R s = R(0);
+#pragma unroll
+        for (int nu = 0; nu < 4; ++nu) s += g[mu][nu] * vcon[nu];
+        vcov[mu] = s;
+    }
+}
+
+// grmhd_functions.hpp:121-133
+template <typename R>
+__device__ __forceinline__ R lorentz(const R g[4][4], R u1, R u2, R u3)
+{
+    const R qsq = g[1][1] * u1 * u1 + g[2][2] * u2 * u2 + g[3][3] * u3 * u3 +
+                  R(2.) * (g[1][2] * u1 * u2 + g[1][3] * u1 * u3 + g[2][3] * u2 * u3);
+    return dsqrt(R(1.) + qsq);
+}
+
+// grmhd_functions.hpp:225-246.  P = {rho, u, u1, u2, u3, B1, B2, B3}
+template <typename R, bool HAS_B>
+__device__ __forceinline__ void calc_4vecs(const R g[4][4], R gcon00, const R* gcon0, const R* P, FourVec<R>& D)
+{
+    const R gamma = lorentz(g, P[2], P[3], P[4]);
+    const R alpha = R(1.) / dsqrt(-gcon00);
+    D.ucon[0] = gamma / alpha;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) D.ucon[v+1] = P[2 + v] - gamma * alpha * gcon0[v+1];
+    lower4(g, D.ucon, D.ucov);
+    if (HAS_B) {
+        R b0 = R(0);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) b0 += P[5 + v] * D.ucov[v+1];
+        D.bcon[0] = b0;
+#pragma unroll
+        for (int v = 0; v < 3; ++v) D.bcon[v+1] = (P[5 + v] + b0 * D.ucon[v+1]) / D.ucon[0];
+        lower4(g, D.bcon, D.bcov);
+    } else {
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) D.bcon[mu] = D.bcov[mu] = R(0);
+    }
+}
+
+// One row T^dir_mu of the MHD (or hydro) stress tensor, grmhd_functions.hpp:51-60, 142-155
+template <typename R, bool HAS_B>
+__device__ __forceinline__ void calc_tensor(R rho, R u, R pgas, const FourVec<R>& D, int dir, R T[4])
+{
+    if (HAS_B) {
+        const R bsq = dot4(D.bcon, D.bcov);
+        const R eta = pgas + rho + u + bsq;
+        const R ptot = pgas + R(0.5) * bsq;
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+            T[mu] = eta * D.ucon[dir] * D.ucov[mu] + ptot * R(dir == mu) - D.bcon[dir] * D.bcov[mu];
+    } else {
+        const R eta = pgas + rho + u;
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+            T[mu] = eta * D.ucon[dir] * D.ucov[mu] + pgas * R(dir == mu);
+    }
+}
+
+// flux_functions.hpp:116-178: conserved variables (dir = 0) or fluxes along dir
+template <typename R, int NV>
+__device__ __forceinline__ void prim_to_flux(const R* P, const FourVec<R>& D, R gam, R gdet, int dir, R* flux)
+{
+    constexpr bool HAS_B = NV > 5;
+    flux[0] = P[0] * D.ucon[dir] * gdet;
+    R T[4];
+    calc_tensor<R, HAS_B>(P[0], P[1], (gam - R(1)) * P[1], D, dir, T);
+    flux[1] = T[0] * gdet + flux[0];
+    flux[2] = T[1] * gdet;
+    flux[3] = T[2] * gdet;
+    flux[4] = T[3] * gdet;
+    if (HAS_B) {
+        if (dir == 0) {
+#pragma unroll
+            for (int v = 0; v < 3; ++v) flux[5 + v] = P[5 + v] * gdet;
+        } else {
+#pragma unroll
+            for (int v = 0; v < 3; ++v) flux[5 + v] = (D.bcon[v+1] * D.ucon[dir] - D.bcon[dir] * D.ucon[v+1]) * gdet;
+        }
+    }
+}
+
+// flux_functions.hpp:368-439.  The reference discards its clip() results (:378, :409), so no
+// clipping happens here either.  With A_mu = delta^dir_mu and B_mu = delta^0_mu the raised
+// vectors and their contractions reduce exactly to single metric entries.
+template <typename R, bool HAS_B>
+__device__ __forceinline__ void vchar(const R* P, const FourVec<R>& D, R gam, R gcon00, R gcon0d, R gcondd,
+                                      int dir, R& cmax, R& cmin)
+{
+    const R ef  = P[0] + gam * P[1];
+    const R cs2 = gam * (gam - R(1)) * P[1] / ef;
+    R cms2;
+    if (HAS_B) {
+        const R bsq = dot4(D.bcon, D.bcov);
+        const R va2 = bsq / (bsq + ef);
+        cms2 = cs2 + va2 - cs2 * va2;
+    } else {
+        cms2 = cs2;
+    }
+    const R Asq = gcondd, Bsq = gcon00, AB = gcon0d;
+    const R Au = D.ucon[dir], Bu = D.ucon[0];
+    const R A  = Bu*Bu - (Bsq + Bu*Bu) * cms2;
+    const R Bq = R(2.) * (Au*Bu - (AB + Au*Bu) * cms2);
+    const R Cq = Au*Au - (Asq + Au*Au) * cms2;
+    const R discr = dsqrt(kmax(Bq * Bq - R(4.) * A * Cq, R(0)));
+    const R vp = -(-Bq + discr) / (R(2.) * A);
+    const R vm = -(-Bq - discr) / (R(2.) * A);
+    cmax = kmax(vp, vm);
+    cmin = kmin(vp, vm);
+}
+
+// ------------------------------------------------------------------ 1D_W inversion (FP64)
+enum Status { ST_SUCCESS = 0, ST_NEG_INPUT, ST_MAX_ITER, ST_BAD_UT, ST_BAD_GAMMA, ST_NEG_RHO, ST_NEG_U, ST_NEG_RHOU };
+
+// onedw.hpp:49-67
+__device__ __forceinline__ double lorentz_calc_w(double Bsq, double D, double QdB, double Qtsq, double Wp)
+{
+    const double QdBsq = QdB * QdB;
+    const double W = Wp + D;
+    const double W2 = W * W;
+    const double WB = W + Bsq;
+    const double utsq = -((W + WB) * QdBsq + W2 * Qtsq) / (QdBsq * (W + WB) + W2 * (Qtsq - WB * WB));
+    if (utsq < -1.e-15 || utsq > 1.e7) return -1.;
+    return sqrt(1. + fabs(utsq));
+}
+// onedw.hpp:72-84
+__device__ __forceinline__ double err_eqn(double gam, double Bsq, double D, double Ep, double QdB, double Qtsq,
+                                          double Wp, int& eflag)
+{
+    const double W = Wp + D;
+    const double gamma = lorentz_calc_w(Bsq, D, QdB, Qtsq, Wp);
+    if (gamma < 1) eflag = ST_BAD_UT;
+    const double w = W / (gamma*gamma);
+    const double rho = D / gamma;
+    const double p = (w - rho) * (gam - 1) / gam;
+    return -Ep + Wp - p + 0.5 * Bsq + 0.5 * (Bsq * Qtsq - QdB * QdB) / ((Bsq + W)*(Bsq + W));
+}
+
+// Zone-centre geometry for the inversion, floors and P->U
+struct ZoneGeom {
+    double gcov[4][4];
+    double gcon[4][4];
+    double gdet;
+};
+
+__device__ __forceinline__ void raise4(const ZoneGeom& G, const double* vcov, double* vcon)
+{
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        double s = 0.;
+#pragma unroll
+        for (int nu = 0; nu < 4; ++nu) s += G.gcon[mu][nu] * vcov[nu];
+        vcon[mu] = s;
+    }
+}
+
+// onedw.hpp:89-233.  U: conserved zone values; P: guess on entry, updated only on success.
+// The iteration count is bounded by max_iterations.
+template <int NV>
+__device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, double* P, int max_iterations, double tol)
+{
+    if (U[0] <= 0.) return ST_NEG_INPUT;
+    const double alpha = 1./sqrt(-G.gcon[0][0]);
+    const double gdet = G.gdet;
+    const double a_over_g = alpha / gdet;
+    const double D = U[0] * a_over_g;
+    double Bcon[4] = {0., 0., 0., 0.};
+    if (NV > 5) {
+        Bcon[1] = U[5] * a_over_g;
+        Bcon[2] = U[6] * a_over_g;
+        Bcon[3] = U[7] * a_over_g;
+    }
+    const double Qcov[4] = {(U[1] - U[0]) * a_over_g, U[2] * a_over_g, U[3] * a_over_g, U[4] * a_over_g};
+    const double ncov[4] = {-alpha, 0., 0., 0.};
+    double Bcov[4], Qcon[4], ncon[4];
+    lower4(G.gcov, Bcon, Bcov);
+    raise4(G, Qcov, Qcon);
+    raise4(G, ncov, ncon);
+    const double Bsq = dot4(Bcon, Bcov);
+    const double QdB = dot4(Bcon, Qcov);
+    const double Qdotn = dot4(Qcon, ncov);
+    double Qtcon[4];
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) Qtcon[mu] = Qcon[mu] + ncon[mu] * Qdotn;
+    const double Qtsq = dot4(Qcon, Qcov) + Qdotn*Qdotn;
+    const double Ep = -Qdotn - D;
+    int eflag = ST_SUCCESS;
+    double Wp, err;
+    {
+        const double gamma = lorentz(G.gcov, P[2], P[3], P[4]);
+        if (gamma < 1) return ST_BAD_UT;
+        const double rho = P[0], u = P[1];
+        Wp = (rho + u + (gam - 1) * u) * gamma * gamma - rho * gamma;
+        err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+    }
+    double dW;
+    {
+        const double Wpm = (1. - 1.e-5) * Wp;
+        const double h = Wp - Wpm;
+        const double Wpp = Wp + h;
+        const double errm = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wpm, eflag);
+        const double errp = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wpp, eflag);
+        const double dedW = (errp - errm) / (Wpp - Wpm);
+        const double dedW2 = (errp - 2. * err + errm) / (h*h);
+        const double f = kclip(0.5 * err * dedW2 / (dedW*dedW), -0.3, 0.3);
+        dW = kclip(-err / dedW / (1. - f), -0.5*Wp, 2.0*Wp);
+    }
+    double Wp1 = Wp;
+    double err1 = err;
+    Wp += dW;
+    err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+    int iter = 0;
+    for (iter = 0; iter < max_iterations; iter++) {
+        dW = kclip((Wp1 - Wp) * err / (err - err1), -0.5*Wp, 2.0*Wp);
+        Wp1 = Wp;
+        err1 = err;
+        Wp += dW;
+        if (fabs(dW / Wp) < tol) break;
+        err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+        if (fabs(err / Wp) < tol) break;
+    }
+    if (iter == max_iterations) return ST_MAX_ITER;
+    const double gamma = lorentz_calc_w(Bsq, D, QdB, Qtsq, Wp);
+    if (gamma < 1) return ST_BAD_UT;
+    const double rho = D / gamma;
+    const double W = Wp + D;
+    const double w = W / (gamma*gamma);
+    const double p = (w - rho) * (gam - 1) / gam;
+    const double u = w - (rho + p);
+    if (rho < 0 && u < 0) return ST_NEG_RHOU;
+    else if (rho < 0) return ST_NEG_RHO;
+    else if (u < 0) return ST_NEG_U;
+    P[0] = rho;
+    P[1] = u;
+    const double pre = (gamma / (W + Bsq));
+    P[2] = pre * (Qtcon[1] + QdB * Bcon[1] / W);
+    P[3] = pre * (Qtcon[2] + QdB * Bcon[2] / W);
+    P[4] = pre * (Qtcon[3] + QdB * Bcon[3] / W);
+    return ST_SUCCESS;
+}
+
+// ------------------------------------------------------------------ floors (FP64)
+// Floors::Prescription (floors.hpp:100-117); same layout as khb_floors
+struct Prescription {
+    double rho_min_const, u_min_const;
+    double rho_min_geom, u_min_geom, r_char;
+    double bsq_over_rho_max, bsq_over_u_max, u_over_rho_max;
+    double ktot_max, gamma_max;
+    int32_t use_r_char, temp_adjust_u, adjust_k, radius_dependent_floors;
+    double floors_switch_r;
+};
+
+// FFlag bits, floors.hpp:52-70
+enum { FF_GEOM_RHO = 32, FF_GEOM_U = 64, FF_B_RHO = 128, FF_B_U = 256, FF_TEMP = 512, FF_GAMMA = 1024,
+       FF_KTOT = 2048, FF_GEOM_RHO_FLUX = 4096, FF_GEOM_U_FLUX = 8192 };
+
+// Geometric floor values, floors_functions.hpp:96-104
+__device__ __forceinline__ void geo_floor_values(const Prescription& f, bool spherical, double r, double gam,
+                                                 double& rhoflr_geom, double& uflr_geom)
+{
+    if (spherical) {
+        const double rhoscal = (f.use_r_char) ? 1. / ((r*r) * (1 + r / f.r_char)) : 1. / sqrt(r*r*r);
+        rhoflr_geom = kmax(f.rho_min_geom * rhoscal, f.rho_min_const);
+        uflr_geom   = kmax(f.u_min_geom * pow(rhoscal, gam), f.u_min_const);
+    } else {
+        rhoflr_geom = f.rho_min_const;
+        uflr_geom   = f.u_min_const;
+    }
+}
+
+// floors_functions.hpp:84-160
+template <int NV>
+__device__ int determine_floors(const ZoneGeom& G, const Prescription& f, bool spherical, double r, double gam,
+                                const double* P, double& rhoflr_max, double& uflr_max)
+{
+    double rhoflr_geom, uflr_geom;
+    geo_floor_values(f, spherical, r, gam, rhoflr_geom, uflr_geom);
+    FourVec<double> D;
+    double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
+    calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, P, D);
+    const double bsq = dot4(D.bcon, D.bcov);
+    const double rhoflr_b = bsq / f.bsq_over_rho_max;
+    const double uflr_b   = bsq / f.bsq_over_u_max;
+    uflr_max = kmax(uflr_geom, uflr_b);
+    const double rho = P[0], u = P[1];
+    int fflag = 0;
+    if (!f.temp_adjust_u) {
+        const double rhoflr_temp = kmax(u, uflr_max) / f.u_over_rho_max;
+        fflag |= (rhoflr_temp > rho) * FF_TEMP;
+        rhoflr_max = kmax(kmax(rhoflr_geom, rhoflr_b), rhoflr_temp);
+    } else {
+        rhoflr_max = kmax(rhoflr_geom, rhoflr_b);
+    }
+    if (rhoflr_max > rho || uflr_max > u) {
+        fflag |= (rhoflr_geom > rho) * FF_GEOM_RHO;
+        fflag |= (uflr_geom > u) * FF_GEOM_U;
+        fflag |= (rhoflr_b > rho) * FF_B_RHO;
+        fflag |= (uflr_b > u) * FF_B_U;
+    }
+    if (lorentz(G.gcov, P[2], P[3], P[4]) > f.gamma_max) fflag |= FF_GAMMA;
+    if ((gam - 1.) * P[1] / pow(P[0], gam) > f.ktot_max) fflag |= FF_KTOT;
+    if (f.temp_adjust_u && (P[1] / P[0] > f.u_over_rho_max)) fflag |= FF_TEMP;
+    return fflag;
+}
+
+// floors_functions.hpp:50-82
+__device__ __forceinline__ void apply_ceilings(const ZoneGeom& G, const Prescription& f, double gam, double* P)
+{
+    const double gamma = lorentz(G.gcov, P[2], P[3], P[4]);
+    const double ktot  = (gam - 1.) * P[1] / pow(P[0], gam);
+    if (gamma > f.gamma_max) {
+        const double fr = sqrt((f.gamma_max*f.gamma_max - 1.) / (gamma*gamma - 1.));
+#pragma unroll
+        for (int v = 0; v < 3; ++v) P[2 + v] *= fr;
+    }
+    if (ktot > f.ktot_max) P[1] = f.ktot_max / ktot * P[1];
+    if (f.temp_adjust_u && P[1] / P[0] > f.u_over_rho_max) P[1] = f.u_over_rho_max * P[0];
+}
+
+// floors_functions.hpp:174-179 (fluid), 181-252 (drift), 254-289 (normal observer)
+template <int NV>
+__device__ int apply_floors_frame(const ZoneGeom& G, int frame, double gam, double* P, double* U,
+                                  double rhoflr_max, double uflr_max, int iter_max_nof)
+{
+    if (frame == 0) {
+        P[0] += kmax(0., rhoflr_max - P[0]);
+        P[1] += kmax(0., uflr_max - P[1]);
+        return 0;
+    } else if (frame == 2) {
+        const double lapse2 = 1. / (-G.gcon[0][0]);
+        double beta[4] = {0., 0., 0., 0.};
+        beta[1] = lapse2 * G.gcon[0][1];
+        beta[2] = lapse2 * G.gcon[0][2];
+        beta[3] = lapse2 * G.gcon[0][3];
+        const double rho = P[0];
+        const double uu  = P[1];
+        const double pg  = (gam - 1.) * uu;
+        const double w_old = kmax(rho + uu + pg, 1e-20);
+        double Bcon[4] = {0., 0., 0., 0.}, Bcov[4] = {0., 0., 0., 0.};
+        if (NV > 5) { Bcon[1] = P[5]; Bcon[2] = P[6]; Bcon[3] = P[7]; }
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+#pragma unroll
+            for (int nu = 0; nu < 4; ++nu) Bcov[mu] += G.gcov[mu][nu] * Bcon[nu];
+        const double Bsq   = kmax(dot4(Bcon, Bcov), 1e-20);
+        const double B_mag = sqrt(Bsq);
+        FourVec<double> D;
+        double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
+        calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, P, D);
+        double Qcov[4];
+        Qcov[0] = w_old * D.ucon[0] * D.ucov[0] + pg;
+        Qcov[1] = w_old * D.ucon[0] * D.ucov[1];
+        Qcov[2] = w_old * D.ucon[0] * D.ucov[2];
+        Qcov[3] = w_old * D.ucon[0] * D.ucov[3];
+        const double QdotB = dot4(Bcon, Qcov);
+        double vpar = QdotB / (B_mag * w_old * D.ucon[0]*D.ucon[0]);
+        double ucon_dr[4] = {0., 0., 0., 0.};
+        ucon_dr[0] = 1. / sqrt(1. / (D.ucon[0]*D.ucon[0]) + vpar*vpar);
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+            ucon_dr[mu] = D.ucon[mu] * (ucon_dr[0] / D.ucon[0]) - (vpar * Bcon[mu] * ucon_dr[0] / B_mag);
+        P[0] = kmax(rho, rhoflr_max);
+        P[1] = kmax(uu, uflr_max);
+        const double pg_new = (gam - 1.) * P[1];
+        const double w_new  = P[0] + P[1] + pg_new;
+        const double x = (2. * QdotB) / (B_mag * w_new * ucon_dr[0]);
+        vpar = x / (1 + sqrt(1 + x*x)) * (1. / ucon_dr[0]);
+        double uc[4];
+        uc[0] = 1. / sqrt(1/(ucon_dr[0]*ucon_dr[0]) - vpar*vpar);
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) uc[mu] = ucon_dr[mu] * (uc[0] / ucon_dr[0]) + (vpar * Bcon[mu] * uc[0] / B_mag);
+        P[2] = uc[1] + (beta[1] * uc[0]);
+        P[3] = uc[2] + (beta[2] * uc[0]);
+        P[4] = uc[3] + (beta[3] * uc[0]);
+        return 0;
+    } else {
+        const double rho_add = kmax(0., rhoflr_max - P[0]);
+        const double u_add   = kmax(0., uflr_max - P[1]);
+        double Pa[8] = {rho_add, u_add, 0., 0., 0., 0., 0., 0.};
+        FourVec<double> D;
+        double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
+        calc_4vecs<double, true>(G.gcov, G.gcon[0][0], gcon0, Pa, D);
+        const double rho_ut = rho_add * D.ucon[0] * G.gdet;
+        double mhd[4];
+        calc_tensor<double, true>(rho_add, u_add, (gam - 1) * u_add, D, 0, mhd);
+        P[0] += rho_add;
+        P[1] += u_add;
+        U[0] += rho_ut;
+        U[1] += mhd[0] * G.gdet + rho_ut;
+        U[2] += mhd[1] * G.gdet;
+        U[3] += mhd[2] * G.gdet;
+        U[4] += mhd[3] * G.gdet;
+        return u_to_p_onedw<NV>(G, gam, U, P, iter_max_nof, 1e-8);
+    }
+}
+
+} // namespace khb

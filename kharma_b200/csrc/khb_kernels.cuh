@@ -1,0 +1,717 @@
+// khb_kernels.cu -- sm_100a kernels and the C ABI of libkhb (see include/khb.h).
+//
+// Per RK stage the work is:
+//   k_flux (x ndim)   reconstruction + prim_to_flux + vchar + LLF/HLLE at every face needed,
+//                     fluxes to scratch (FP64, or FP32 in the FP32-flux form)
+//   k_fix_flux        polar and inflow flux corrections on the raw fluxes (spherical runs)
+//   k_zone            ONE pass per zone: flux-CT EMFs from the raw B fluxes, flux divergence,
+//                     geometric source, RK combination, 1D_W inversion, floors, lock-step P->U,
+//                     CFL reduction (last stage) and the failed-zone list
+//   k_fixup           neighbour averaging of failed zones (grid sized once, reads the list)
+//   k_bc_* / k_periodic  ghost zones
+// Every loop in device code is bounded; failures are reported through pflag, never by trapping.
+#include "khb_device.cuh"
+#include "../../include/khb.h"
+
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <limits>
+
+namespace khb {
+
+struct Dims {
+    int n1, n2, n3, ndim;
+    int is, ie, js, je, ks, ke;
+    int nx1, nx2, nx3;
+    long long N;
+    long long sj, sk;
+    int bc[6];
+};
+
+struct DevGeom {
+    int G1, G2, n1;
+    long long gs;                          // component stride of the location tables, G1*G2
+    const double* gcov[4];                 // face1, face2, face3, centre: [16][G2][G1]
+    const double* gcon[4];
+    const double* gdet[4];                 // [G2][G1]
+    const float* gcov_f[3];                // FP32 copies of the face tables
+    const float* gcon_f[3];
+    const float* gdet_f[3];
+    const double* gdet_conn;               // [64][n2][n1], index (nu*4+lam)*4+mu as gdet_conn(nu,lam,mu)
+    const double* rcen;                    // [n2][n1]
+};
+
+struct Phys {
+    double gam;
+    int riemann, recon_floors, spherical, cart_minkowski;
+    int floors_on, frame, iter_max, fix_avg, fix_atmo;
+    double err_tol;
+    double dx1, dx2, dx3;
+    int zero_polar_flux, fix_polar_flux, check_inflow_in, check_inflow_out;
+    Prescription fl;
+};
+
+__device__ __forceinline__ void zone_kji(const Dims& d, long long c, int& k, int& j, int& i)
+{
+    i = (int)(c % d.n1);
+    const long long r = c / d.n1;
+    j = (int)(r % d.n2);
+    k = (int)(r / d.n2);
+}
+
+// Load the centre geometry of zone (j,i)
+__device__ __forceinline__ void load_zone_geom(const DevGeom& g, int j, int i, ZoneGeom& G)
+{
+    const long long gi = (long long)j*g.G1 + i;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        G.gcov[m/4][m%4] = __ldg(g.gcov[3] + m*g.gs + gi);
+        G.gcon[m/4][m%4] = __ldg(g.gcon[3] + m*g.gs + gi);
+    }
+    G.gdet = __ldg(g.gdet[3] + gi);
+}
+
+// Flux::p_to_u for one zone (all NV conserved variables), flux_functions.hpp:343-352
+template <int NV>
+__device__ __forceinline__ void p_to_u_zone(const ZoneGeom& G, double gam, const double* P, double* U)
+{
+    FourVec<double> D;
+    const double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
+    calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, P, D);
+    prim_to_flux<double, NV>(P, D, gam, G.gdet, 0, U);
+}
+
+// ===================================================================================== fluxes
+// One thread per face.  Face (k,j,i) along dir lies between zones c - st and c.
+template <typename R> struct FaceTables;
+template <> struct FaceTables<double> {
+    static __device__ __forceinline__ const double* gcov(const DevGeom& g, int loc) { return g.gcov[loc]; }
+    static __device__ __forceinline__ const double* gcon(const DevGeom& g, int loc) { return g.gcon[loc]; }
+    static __device__ __forceinline__ const double* gdet(const DevGeom& g, int loc) { return g.gdet[loc]; }
+};
+template <> struct FaceTables<float> {
+    static __device__ __forceinline__ const float* gcov(const DevGeom& g, int loc) { return g.gcov_f[loc]; }
+    static __device__ __forceinline__ const float* gcon(const DevGeom& g, int loc) { return g.gcon_f[loc]; }
+    static __device__ __forceinline__ const float* gdet(const DevGeom& g, int loc) { return g.gdet_f[loc]; }
+};
+
+template <int RECON, int NV, typename R, typename FT>
+__global__ void __launch_bounds__(128)
+k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop,
+       int dir, int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, long long total)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int i = lo_i + (int)(t % cnt_i);
+    const long long r = t / cnt_i;
+    const int j = lo_j + (int)(r % cnt_j);
+    const int k = lo_k + (int)(r / cnt_j);
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long st = (dir == 1) ? 1 : ((dir == 2) ? d.sj : d.sk);
+    const int loc = dir - 1;
+    const R gam = (R)ph.gam;
+
+    // geometry at the face
+    const long long gi = (long long)j*g.G1 + i;
+    const auto* tcov = FaceTables<R>::gcov(g, loc);
+    const auto* tcon = FaceTables<R>::gcon(g, loc);
+    R gcov[4][4];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) gcov[m/4][m%4] = (R)__ldg(tcov + m*g.gs + gi);
+    R gcon0[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) gcon0[m] = (R)__ldg(tcon + m*g.gs + gi);
+    const R gcondd = (R)__ldg(tcon + (dir*4 + dir)*g.gs + gi);
+    const R gdet = (R)__ldg(FaceTables<R>::gdet(g, loc) + gi);
+
+    // reconstruction: left state = right face of zone c-st, right state = left face of zone c
+    R Pl[NV], Pr[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        const double* q = P.v[p];
+        const R x0 = (R)__ldg(q + c - 3*st), x1 = (R)__ldg(q + c - 2*st), x2 = (R)__ldg(q + c - st);
+        const R x3 = (R)__ldg(q + c), x4 = (R)__ldg(q + c + st), x5 = (R)__ldg(q + c + 2*st);
+        Pl[p] = recon_right<RECON, R>(x0, x1, x2, x3, x4);
+        Pr[p] = recon_left<RECON, R>(x1, x2, x3, x4, x5);
+    }
+    if (ph.recon_floors) {
+        // floors_functions.hpp:320-354 applied to both reconstructed states (get_flux.hpp:174-181)
+        double rf, uf;
+        geo_floor_values(ph.fl, ph.spherical, __ldg(g.rcen + (long long)j*g.n1 + i), ph.gam, rf, uf);
+        Pl[0] += kmax(R(0), (R)rf - Pl[0]); Pl[1] += kmax(R(0), (R)uf - Pl[1]);
+        Pr[0] += kmax(R(0), (R)rf - Pr[0]); Pr[1] += kmax(R(0), (R)uf - Pr[1]);
+    }
+
+    constexpr bool HAS_B = NV > 5;
+    FourVec<R> D;
+    R Ul[NV], Fl[NV], Ur[NV], Fr[NV];
+    R cmaxL, cminL, cmaxR, cminR;
+    calc_4vecs<R, HAS_B>(gcov, gcon0[0], gcon0, Pl, D);
+    prim_to_flux<R, NV>(Pl, D, gam, gdet, 0, Ul);
+    prim_to_flux<R, NV>(Pl, D, gam, gdet, dir, Fl);
+    vchar<R, HAS_B>(Pl, D, gam, gcon0[0], gcon0[dir], gcondd, dir, cmaxL, cminL);
+    calc_4vecs<R, HAS_B>(gcov, gcon0[0], gcon0, Pr, D);
+    prim_to_flux<R, NV>(Pr, D, gam, gdet, 0, Ur);
+    prim_to_flux<R, NV>(Pr, D, gam, gdet, dir, Fr);
+    vchar<R, HAS_B>(Pr, D, gam, gcon0[0], gcon0[dir], gcondd, dir, cmaxR, cminR);
+    // get_flux.hpp:274-275, 330-331
+    const R cmax = kmax(kmax(R(0), cmaxL), cmaxR);
+    const R cmin = -kmin(kmin(R(0), cminL), cminR);
+    if (ph.riemann == 0) {
+        const R ctp = kmax(cmax, cmin);
+#pragma unroll
+        for (int p = 0; p < NV; ++p)
+            F[p*d.N + c] = (FT)(R(0.5) * (Fl[p] + Fr[p] - ctp * (Ur[p] - Ul[p])));
+    } else {
+#pragma unroll
+        for (int p = 0; p < NV; ++p)
+            F[p*d.N + c] = (FT)((cmax*Fl[p] + cmin*Fr[p] - cmax*cmin*(Ur[p] - Ul[p])) / (cmax + cmin));
+    }
+    ctop[c] = (FT)kmax(cmax, cmin);
+}
+
+// ===================================================================================== flux fixes
+// B_FluxCT::ZeroBoundaryFlux on X2 faces (b_flux_ct.cpp:404-430) and KBoundaries::FixFlux
+// (boundaries.cpp:611-690) for inflow checks on X1 faces and zero polar fluxes on X2 faces.
+// One thread per (k, i) of an X2 face or (k, j) of an X1 face; the halo is one zone.
+template <int NV, typename FT>
+__global__ void k_fix_flux_x2(Dims d, Phys ph, FT* F1, FT* F2, FT* F3, int inner)
+{
+    const int ni = d.ie - d.is + 3;
+    const int nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ni*nk) return;
+    const int i = d.is - 1 + t % ni;
+    const int k = (d.ndim > 2) ? d.ks - 1 + t / ni : d.ks;
+    const int j = inner ? d.js : d.je + 1;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long N = d.N;
+    if (NV > 5 && ph.fix_polar_flux) {
+        F2[5*N + c] = (FT)0; F2[7*N + c] = (FT)0;
+        if (inner) {
+            F1[6*N + c - d.sj] = -F1[6*N + c];
+            if (d.ndim > 2) F3[6*N + c - d.sj] = -F3[6*N + c];
+        } else {
+            F1[6*N + c] = -F1[6*N + c - d.sj];
+            if (d.ndim > 2) F3[6*N + c] = -F3[6*N + c - d.sj];
+        }
+    }
+    if (ph.zero_polar_flux)
+#pragma unroll
+        for (int p = 0; p < NV; ++p) F2[p*N + c] = (FT)0;
+}
+template <typename FT>
+__global__ void k_fix_flux_x1(Dims d, FT* F1, int inner)
+{
+    const int nj = (d.ndim > 1) ? d.je - d.js + 3 : 1;
+    const int nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nj*nk) return;
+    const int j = (d.ndim > 1) ? d.js - 1 + t % nj : d.js;
+    const int k = (d.ndim > 2) ? d.ks - 1 + t / nj : d.ks;
+    const int i = inner ? d.is : d.ie + 1;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    FT& f = F1[c];
+    f = inner ? kmin(f, (FT)0) : kmax(f, (FT)0);
+}
+
+// ===================================================================================== zone pass
+enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST = 32 };
+
+template <typename FT>
+struct ZoneArgs {
+    khb_fields Ps, Us, U0, Pout, Uout;
+    const FT* F[3];
+    const FT* ctop[3];
+    int32_t* pflag;
+    int32_t* fflag;
+    double g0, g1, bdt;
+    unsigned long long* ndt_word;
+    int* fail_count;
+    int* fail_list;
+    int mode;
+};
+
+// Raw flux, as double
+template <typename FT>
+__device__ __forceinline__ double ldf(const FT* F, long long x) { return (double)__ldg(F + x); }
+
+template <int NV, typename FT>
+__global__ void __launch_bounds__(128)
+k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
+{
+    const int cnt_i = d.ie - d.is + 1, cnt_j = d.je - d.js + 1, cnt_k = d.ke - d.ks + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)cnt_i*cnt_j*cnt_k;
+    const bool active = t < total;
+    double ndt_zone = 1.7976931348623157e308;
+    if (active) {
+        const int i = d.is + (int)(t % cnt_i);
+        const long long r = t / cnt_i;
+        const int j = d.js + (int)(r % cnt_j);
+        const int k = d.ks + (int)(r / cnt_j);
+        const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+        const long long N = d.N, sj = d.sj, sk = d.sk;
+        const double gam = ph.gam;
+        ZoneGeom G;
+        load_zone_geom(g, j, i, G);
+
+        double U[NV], P[NV];
+        if (a.mode & M_UPDATE) {
+            // ---- flux divergence (Parthenon FluxDivHelper) with flux-CT B fluxes
+            const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
+            const double vol = ph.dx1*ph.dx2*ph.dx3;
+            const FT* F1 = a.F[0]; const FT* F2 = a.F[1]; const FT* F3 = a.F[2];
+            double dudt[NV];
+            constexpr int NH = 5;
+#pragma unroll
+            for (int p = 0; p < NH; ++p) {
+                double du = (a1 * ldf(F1, p*N + c + 1) - a1 * ldf(F1, p*N + c));
+                if (d.ndim >= 2) du += a2 * ldf(F2, p*N + c + sj) - a2 * ldf(F2, p*N + c);
+                if (d.ndim == 3) du += a3 * ldf(F3, p*N + c + sk) - a3 * ldf(F3, p*N + c);
+                dudt[p] = -du / vol;
+            }
+            if (NV > 5) {
+                // b_flux_ct.cpp:307-370, evaluated per zone from the raw B fluxes, in FT arithmetic
+                double fb[3][3][2];   // [face dir][B component][lo/hi face]
+                if (d.ndim >= 2) {
+                    const long long B1 = 5*N, B2 = 6*N, B3 = 7*N;
+                    auto e3 = [&](long long x) -> FT {
+                        return (FT)0.25 * (__ldg(F1 + B2 + x) + __ldg(F1 + B2 + x - sj) - __ldg(F2 + B1 + x) - __ldg(F2 + B1 + x - 1));
+                    };
+                    auto e1 = [&](long long x) -> FT {
+                        return (FT)0.25 * (__ldg(F2 + B3 + x) + __ldg(F2 + B3 + x - sk) - __ldg(F3 + B2 + x) - __ldg(F3 + B2 + x - sj));
+                    };
+                    auto e2 = [&](long long x) -> FT {
+                        return (FT)0.25 * (__ldg(F3 + B1 + x) + __ldg(F3 + B1 + x - 1) - __ldg(F1 + B3 + x) - __ldg(F1 + B3 + x - sk));
+                    };
+                    const bool d3 = d.ndim > 2;
+                    // X1 faces i (lo) and i+1 (hi)
+                    fb[0][0][0] = 0.; fb[0][0][1] = 0.;
+                    fb[0][1][0] = (double)((FT)0.5 * (e3(c) + e3(c + sj)));
+                    fb[0][1][1] = (double)((FT)0.5 * (e3(c + 1) + e3(c + 1 + sj)));
+                    fb[0][2][0] = d3 ? (double)((FT)-0.5 * (e2(c) + e2(c + sk))) : ldf(F1, B3 + c);
+                    fb[0][2][1] = d3 ? (double)((FT)-0.5 * (e2(c + 1) + e2(c + 1 + sk))) : ldf(F1, B3 + c + 1);
+                    // X2 faces j, j+1
+                    fb[1][0][0] = (double)((FT)-0.5 * (e3(c) + e3(c + 1)));
+                    fb[1][0][1] = (double)((FT)-0.5 * (e3(c + sj) + e3(c + sj + 1)));
+                    fb[1][1][0] = 0.; fb[1][1][1] = 0.;
+                    fb[1][2][0] = d3 ? (double)((FT)0.5 * (e1(c) + e1(c + sk))) : ldf(F2, B3 + c);
+                    fb[1][2][1] = d3 ? (double)((FT)0.5 * (e1(c + sj) + e1(c + sj + sk))) : ldf(F2, B3 + c + sj);
+                    // KBoundaries zero_polar_flux after flux-CT (boundaries.cpp:672-684)
+                    if (ph.zero_polar_flux) {
+                        if (j == d.js && d.bc[2] != KHB_BC_PERIODIC) { fb[1][0][0] = 0.; fb[1][1][0] = 0.; fb[1][2][0] = 0.; }
+                        if (j == d.je && d.bc[3] != KHB_BC_PERIODIC) { fb[1][0][1] = 0.; fb[1][1][1] = 0.; fb[1][2][1] = 0.; }
+                    }
+                    if (d3) {
+                        fb[2][0][0] = (double)((FT)0.5 * (e2(c) + e2(c + 1)));
+                        fb[2][0][1] = (double)((FT)0.5 * (e2(c + sk) + e2(c + sk + 1)));
+                        fb[2][1][0] = (double)((FT)-0.5 * (e1(c) + e1(c + sj)));
+                        fb[2][1][1] = (double)((FT)-0.5 * (e1(c + sk) + e1(c + sk + sj)));
+                        fb[2][2][0] = 0.; fb[2][2][1] = 0.;
+                    }
+                } else {
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) {
+                        fb[0][v][0] = ldf(F1, (5 + v)*N + c);
+                        fb[0][v][1] = ldf(F1, (5 + v)*N + c + 1);
+                    }
+                }
+#pragma unroll
+                for (int v = 0; v < 3; ++v) {
+                    double du = (a1 * fb[0][v][1] - a1 * fb[0][v][0]);
+                    if (d.ndim >= 2) du += a2 * fb[1][v][1] - a2 * fb[1][v][0];
+                    if (d.ndim == 3) du += a3 * fb[2][v][1] - a3 * fb[2][v][0];
+                    dudt[5 + v] = -du / vol;
+                }
+            }
+            // ---- geometric source, flux.cpp:395-444
+            if (!ph.cart_minkowski) {
+                double Ps[NV];
+#pragma unroll
+                for (int p = 0; p < NV; ++p) Ps[p] = __ldg(a.Ps.v[p] + c);
+                FourVec<double> D;
+                const double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
+                calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, Ps, D);
+                double new_du[4] = {0., 0., 0., 0.};
+                const long long cg = (long long)j*g.n1 + i, cs = (long long)(d.n2)*g.n1;
+#pragma unroll
+                for (int mu = 0; mu < 4; ++mu) {
+                    double Tmu[4];
+                    calc_tensor<double, (NV > 5)>(Ps[0], Ps[1], (gam - 1) * Ps[1], D, mu, Tmu);
+#pragma unroll
+                    for (int nu = 0; nu < 4; ++nu)
+#pragma unroll
+                        for (int lam = 0; lam < 4; ++lam)
+                            new_du[lam] += Tmu[nu] * __ldg(g.gdet_conn + ((nu*4 + lam)*4 + mu)*cs + cg);
+                }
+                dudt[1] += new_du[0];
+                dudt[2] += new_du[1];
+                dudt[3] += new_du[2];
+                dudt[4] += new_du[3];
+            }
+            // ---- RK combination (Parthenon WeightedSumData twice, kharma_driver.cpp:339-387)
+#pragma unroll
+            for (int p = 0; p < NV; ++p) {
+                double x = a.g0 * __ldg(a.Us.v[p] + c) + a.g1 * __ldg(a.U0.v[p] + c);
+                U[p] = 1.0 * x + a.bdt * dudt[p];
+            }
+        } else {
+#pragma unroll
+            for (int p = 0; p < NV; ++p) U[p] = a.Us.v[p][c];
+        }
+
+        int pflag = 0, fflag = 0;
+#pragma unroll
+        for (int p = 0; p < NV; ++p) P[p] = a.Ps.v[p][c];
+        if (a.mode & M_UTOP) {
+            // inverter.cpp:163-181 then b_flux_ct.cpp:196-217
+            const int pf = u_to_p_onedw<NV>(G, gam, U, P, ph.iter_max, ph.err_tol);
+            pflag = pf % FF_GEOM_RHO;
+            fflag = (pf / FF_GEOM_RHO) * FF_GEOM_RHO;
+            if (NV > 5) {
+#pragma unroll
+                for (int v = 0; v < 3; ++v) P[5 + v] = U[5 + v] / G.gdet;
+            }
+        } else {
+            pflag = a.pflag[c];
+            fflag = a.fflag[c];
+        }
+        if ((a.mode & M_FLOORS) && ph.floors_on) {
+            // floors.cpp:215-229 and floors_impl.hpp:77-125
+            double rf, uf;
+            const double rr = __ldg(g.rcen + (long long)j*g.n1 + i);
+            fflag |= determine_floors<NV>(G, ph.fl, ph.spherical, rr, gam, P, rf, uf);
+            if (fflag) {
+                const int pl = apply_floors_frame<NV>(G, ph.frame, gam, P, U, rf, uf, 8);
+                if (pl) pflag = pl;
+                apply_ceilings(G, ph.fl, gam, P);
+                double Ut[NV];
+                p_to_u_zone<NV>(G, gam, P, Ut);
+#pragma unroll
+                for (int p = 0; p < 5; ++p) U[p] = Ut[p];
+            }
+        }
+        if (a.mode & M_PTOU) p_to_u_zone<NV>(G, gam, P, U);
+
+#pragma unroll
+        for (int p = 0; p < NV; ++p) a.Uout.v[p][c] = U[p];
+        if (a.mode & (M_UTOP | M_FLOORS)) {
+#pragma unroll
+            for (int p = 0; p < NV; ++p) a.Pout.v[p][c] = P[p];
+            a.pflag[c] = pflag;
+            a.fflag[c] = fflag;
+        }
+        if ((a.mode & M_FAILLIST) && pflag > 0) {
+            const int slot = atomicAdd(a.fail_count, 1);
+            a.fail_list[slot] = (int)c;
+        }
+        if (a.mode & M_DT) {
+            // grmhd.cpp:313-328
+            const double c1 = kmax((double)a.ctop[0][c], 0.0), c2 = kmax((double)a.ctop[1][c], 0.0);
+            const double c3 = kmax((double)a.ctop[2][c], 0.0);
+            const double z = 1.0 / (1 / (ph.dx1 / c1) + 1 / (ph.dx2 / c2) + 1 / (ph.dx3 * 1 / c3));
+            if (!isnan(z)) ndt_zone = z;
+        }
+    }
+    if (a.mode & M_DT) {
+        // block minimum by warp shuffles, then one atomic per block on the bit pattern (values >= 0)
+        double v = ndt_zone;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        __shared__ double wmin[4];
+        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = wmin[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin(m, wmin[w]);
+            if (m >= 0.0) atomicMin(a.ndt_word, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+}
+
+// ===================================================================================== fixups
+// fixup.cpp:47-156.  Neighbours in periodic directions wrap; in other directions they must be
+// interior.  Failed zones never read each other, so one pass over the list is race-free.
+template <int NV>
+__global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, const int32_t* pflag,
+                        const int* fail_count, const int* fail_list)
+{
+    const int n = *fail_count;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const long long c = fail_list[t];
+        int k, j, i;
+        zone_kji(d, c, k, j, i);
+        double wsum = 0., sum[5] = {0., 0., 0., 0., 0.};
+        if (ph.fix_avg) {
+            for (int nn = -1; nn <= 1; nn++) for (int m = -1; m <= 1; m++) for (int l = -1; l <= 1; l++) {
+                int ii = i + l, jj = j + m, kk = k + nn;
+                if (ii < d.is || ii > d.ie) { if (d.bc[0] != KHB_BC_PERIODIC) continue; ii += (ii < d.is) ? d.nx1 : -d.nx1; }
+                if (jj < d.js || jj > d.je) { if (d.ndim < 2 || d.bc[2] != KHB_BC_PERIODIC) continue; jj += (jj < d.js) ? d.nx2 : -d.nx2; }
+                if (kk < d.ks || kk > d.ke) { if (d.ndim < 3 || d.bc[4] != KHB_BC_PERIODIC) continue; kk += (kk < d.ks) ? d.nx3 : -d.nx3; }
+                const long long cn = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+                if (!(pflag[cn] > 0)) {
+                    const double w = 1./(abs(l) + abs(m) + abs(nn) + 1);
+                    wsum += w;
+#pragma unroll
+                    for (int p = 0; p < 5; ++p) sum[p] += w * P.v[p][cn];
+                }
+            }
+        }
+        double Pz[NV], Uz[NV];
+#pragma unroll
+        for (int p = 0; p < 5; ++p) Pz[p] = (wsum < 1.e-10) ? 0. : sum[p]/wsum;
+#pragma unroll
+        for (int p = 5; p < NV; ++p) Pz[p] = P.v[p][c];
+        double rf, uf;
+        geo_floor_values(ph.fl, ph.spherical, g.rcen[(long long)j*g.n1 + i], ph.gam, rf, uf);
+        Pz[0] += kmax(0., rf - Pz[0]);
+        Pz[1] += kmax(0., uf - Pz[1]);
+        ZoneGeom G;
+        load_zone_geom(g, j, i, G);
+        p_to_u_zone<NV>(G, ph.gam, Pz, Uz);
+#pragma unroll
+        for (int p = 0; p < 5; ++p) P.v[p][c] = Pz[p];
+#pragma unroll
+        for (int p = 0; p < NV; ++p) U.v[p][c] = Uz[p];
+    }
+}
+
+// ===================================================================================== boundaries
+// Parthenon's outflow/reflecting functions (unvendored) as KHARMA applies them: fluid primitives
+// and the conserved field; then the inflow check (boundaries.hpp:101-136).  dir = 1 or 2.
+template <int NV>
+__global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int face,
+                     int lo_a, int cnt_a, int lo_k, int cnt_k)
+{
+    const int bdir = face / 2 + 1;
+    const bool inner = (face % 2) == 0;
+    const int ng = (bdir == 1) ? d.is : d.js;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ng*cnt_a*cnt_k) return;
+    const int gidx = (int)(t % ng);
+    const long long r = t / ng;
+    const int aidx = lo_a + (int)(r % cnt_a);
+    const int k = lo_k + (int)(r / cnt_a);
+    int i, j, ref;
+    if (bdir == 1) {
+        j = aidx;
+        ref = inner ? d.is : d.ie;
+        i = inner ? gidx : d.ie + 1 + gidx;
+    } else {
+        i = aidx;
+        ref = inner ? d.js : d.je;
+        j = inner ? gidx : d.je + 1 + gidx;
+    }
+    const int type = d.bc[face];
+    const int offset = 2 * ref + (inner ? -1 : 1);
+    int ii = i, jj = j;
+    if (bdir == 1) ii = (type == KHB_BC_OUTFLOW) ? ref : offset - i;
+    else           jj = (type == KHB_BC_OUTFLOW) ? ref : offset - j;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long s = ((long long)k*d.n2 + jj)*d.n1 + ii;
+    double Pz[5];
+#pragma unroll
+    for (int p = 0; p < 5; ++p) {
+        const bool flip = (type == KHB_BC_REFLECTING) && (p == 1 + bdir);
+        Pz[p] = (flip ? -1.0 : 1.0) * P.v[p][s];
+    }
+    if (NV > 5) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const bool flip = (type == KHB_BC_REFLECTING) && (v == bdir - 1);
+            U.v[5 + v][c] = (flip ? -1.0 : 1.0) * U.v[5 + v][s];
+        }
+    }
+    const bool inflow = (face == 0 && ph.check_inflow_in) || (face == 1 && ph.check_inflow_out);
+    if (inflow) {
+        ZoneGeom G;
+        load_zone_geom(g, j, i, G);
+        double uvec[3] = {Pz[2], Pz[3], Pz[4]};
+        double gamma = lorentz(G.gcov, uvec[0], uvec[1], uvec[2]);
+        const double alpha = 1. / sqrt(-G.gcon[0][0]);
+        const double ucon1 = uvec[0] - gamma * alpha * G.gcon[0][1];
+        if (((ucon1 > 0.) && inner) || ((ucon1 < 0.) && !inner)) {
+#pragma unroll
+            for (int v = 0; v < 3; ++v) uvec[v] /= gamma;
+            const double beta1 = G.gcon[0][1] * alpha * alpha;
+            uvec[0] = beta1 / alpha;
+            const double vsq = G.gcov[1][1] * uvec[0] * uvec[0] + G.gcov[2][2] * uvec[1] * uvec[1] +
+                               G.gcov[3][3] * uvec[2] * uvec[2] +
+                               2. * (G.gcov[1][2] * uvec[0] * uvec[1] + G.gcov[1][3] * uvec[0] * uvec[2] +
+                                     G.gcov[2][3] * uvec[1] * uvec[2]);
+            gamma = 1./sqrt(1. - vsq);
+#pragma unroll
+            for (int v = 0; v < 3; ++v) Pz[2 + v] = uvec[v] * gamma;
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < 5; ++p) P.v[p][c] = Pz[p];
+}
+
+// B_P = B_U/gdet and U = U(P) on the X1/X2 ghost zones of the interior k range
+template <int NV>
+__global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U)
+{
+    const int cnt_k = d.ke - d.ks + 1;
+    const long long plane = (long long)d.n1*d.n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= plane*cnt_k) return;
+    const int i = (int)(t % d.n1);
+    const int j = (int)((t / d.n1) % d.n2);
+    const int k = d.ks + (int)(t / plane);
+    const bool ghost = (i < d.is || i > d.ie) || (d.ndim > 1 && (j < d.js || j > d.je));
+    if (!ghost) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    ZoneGeom G;
+    load_zone_geom(g, j, i, G);
+    double Pz[NV], Uz[NV];
+#pragma unroll
+    for (int p = 0; p < 5; ++p) Pz[p] = P.v[p][c];
+    if (NV > 5) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) { Pz[5 + v] = U.v[5 + v][c] / G.gdet; P.v[5 + v][c] = Pz[5 + v]; }
+    }
+    p_to_u_zone<NV>(G, ph.gam, Pz, Uz);
+#pragma unroll
+    for (int p = 0; p < NV; ++p) U.v[p][c] = Uz[p];
+}
+
+// Periodic images: every zone outside the interior in a periodic direction copies all variables
+// of P and U from its image (wrapping only the periodic directions).
+template <int NV>
+__global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    int k, j, i;
+    zone_kji(d, t, k, j, i);
+    int ii = i, jj = j, kk = k;
+    bool any = false;
+    if ((pmask & 1) && (i < d.is || i > d.ie)) { ii += (i < d.is) ? d.nx1 : -d.nx1; any = true; }
+    if ((pmask & 2) && (j < d.js || j > d.je)) { jj += (j < d.js) ? d.nx2 : -d.nx2; any = true; }
+    if ((pmask & 4) && (k < d.ks || k > d.ke)) { kk += (k < d.ks) ? d.nx3 : -d.nx3; any = true; }
+    if (!any) return;
+    const long long s = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+#pragma unroll
+    for (int p = 0; p < NV; ++p) { P.v[p][t] = P.v[p][s]; U.v[p][t] = U.v[p][s]; }
+}
+
+// Whole-block P->U (Flux::MeshPtoU)
+template <int NV>
+__global__ void k_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    int k, j, i;
+    zone_kji(d, t, k, j, i);
+    ZoneGeom G;
+    load_zone_geom(g, j, i, G);
+    double Pz[NV], Uz[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) Pz[p] = P.v[p][t];
+    p_to_u_zone<NV>(G, ph.gam, Pz, Uz);
+#pragma unroll
+    for (int p = 0; p < NV; ++p) U.v[p][t] = Uz[p];
+}
+
+// Materialize flux-CT into the B flux scratch (b_flux_ct.cpp:307-370), for khb_flux_ct.
+// Reads raw fluxes from Fr (a copy) and writes the rewritten B fluxes into F.
+template <typename FT>
+__global__ void k_emf(Dims d, const FT* F1, const FT* F2, const FT* F3, FT* E)
+{
+    // corner EMFs on [ks, ke+1(3D)] x [js, je+1] x [is, ie+1]
+    const int ci = d.ie - d.is + 2, cj = d.je - d.js + 2, ck = (d.ndim > 2) ? d.ke - d.ks + 2 : 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ci*cj*ck) return;
+    const int i = d.is + (int)(t % ci);
+    const int j = d.js + (int)((t / ci) % cj);
+    const int k = d.ks + (int)(t / ((long long)ci*cj));
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i, N = d.N, sj = d.sj, sk = d.sk;
+    if (d.ndim > 2) {
+        E[c]     = (FT)0.25 * (F2[7*N + c] + F2[7*N + c - sk] - F3[6*N + c] - F3[6*N + c - sj]);
+        E[N + c] = (FT)0.25 * (F3[5*N + c] + F3[5*N + c - 1] - F1[7*N + c] - F1[7*N + c - sk]);
+    }
+    E[2*N + c] = (FT)0.25 * (F1[6*N + c] + F1[6*N + c - sj] - F2[5*N + c] - F2[5*N + c - 1]);
+}
+template <typename FT>
+__global__ void k_ct_apply(Dims d, FT* F1, FT* F2, FT* F3, const FT* E)
+{
+    // each thread owns one (k,j,i) in [ks, ke+1] x [js, je+1] x [is, ie+1] and writes the faces there
+    const int ci = d.ie - d.is + 2, cj = d.je - d.js + 2, ck = (d.ndim > 2) ? d.ke - d.ks + 2 : 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ci*cj*ck) return;
+    const int i = d.is + (int)(t % ci);
+    const int j = d.js + (int)((t / ci) % cj);
+    const int k = d.ks + (int)(t / ((long long)ci*cj));
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i, N = d.N, sj = d.sj, sk = d.sk;
+    const FT* e1 = E; const FT* e2 = E + N; const FT* e3 = E + 2*N;
+    const bool d3 = d.ndim > 2;
+    const bool kin = k <= d.ke, jin = j <= d.je, iin = i <= d.ie;
+    if (kin && jin) {
+        F1[5*N + c] = (FT)0.0;
+        F1[6*N + c] = (FT)0.5 * (e3[c] + e3[c + sj]);
+        if (d3) F1[7*N + c] = (FT)-0.5 * (e2[c] + e2[c + sk]);
+    }
+    if (kin && iin) {
+        F2[5*N + c] = (FT)-0.5 * (e3[c] + e3[c + 1]);
+        F2[6*N + c] = (FT)0.0;
+        if (d3) F2[7*N + c] = (FT)0.5 * (e1[c] + e1[c + sk]);
+    }
+    if (d3 && jin && iin) {
+        F3[5*N + c] = (FT)0.5 * (e2[c] + e2[c + 1]);
+        F3[6*N + c] = (FT)-0.5 * (e1[c] + e1[c + sj]);
+        F3[7*N + c] = (FT)0.0;
+    }
+}
+
+// Copy scratch fluxes out as doubles
+template <typename FT>
+__global__ void k_copy_flux(long long N, int nv, const FT* F, const FT* ctop, khb_fields out, double* ctop_out)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    for (int p = 0; p < nv; ++p) if (out.v[p]) out.v[p][t] = (double)F[p*N + t];
+    if (ctop_out) ctop_out[t] = (double)ctop[t];
+}
+
+// B_FluxCT::MaxDivB: corner divergence (b_flux_ct_functions.hpp:52-75), block max + atomicMax
+__global__ void k_divb(Dims d, Phys ph, khb_fields U, int i_lo, int i_hi, unsigned long long* word)
+{
+    const int ci = i_hi - i_lo + 1, cj = d.je - d.js + 2, ck = (d.ndim > 2) ? d.ke - d.ks + 2 : 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.;
+    if (t < (long long)ci*cj*ck) {
+        const int i = i_lo + (int)(t % ci);
+        const int j = d.js + (int)((t / ci) % cj);
+        const int k = d.ks + (int)(t / ((long long)ci*cj));
+        const long long c = ((long long)k*d.n2 + j)*d.n1 + i, sj = d.sj, sk = d.sk;
+        const double* B1 = U.v[5]; const double* B2 = U.v[6]; const double* B3 = U.v[7];
+        const bool do3 = d.ndim > 2;
+        const double norm = do3 ? 0.25 : 0.5;
+        double term1 = B1[c] - B1[c-1] + B1[c-sj] - B1[c-sj-1];
+        double term2 = B2[c] - B2[c-sj] + B2[c-1] - B2[c-sj-1];
+        double term3 = 0.;
+        if (do3) {
+            term1 += B1[c-sk] + B1[c-sk-sj] - B1[c-sk-1] - B1[c-sk-sj-1];
+            term2 += B2[c-sk] + B2[c-sk-1] - B2[c-sk-sj] - B2[c-sk-sj-1];
+            term3 = B3[c] + B3[c-sj] + B3[c-1] + B3[c-sj-1] - B3[c-sk] - B3[c-sk-sj] - B3[c-sk-1] - B3[c-sk-sj-1];
+        }
+        v = fabs(norm*term1/ph.dx1 + norm*term2/ph.dx2 + norm*term3/ph.dx3);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ double wmax[8];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = wmax[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
+        atomicMax(word, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+} // namespace khb

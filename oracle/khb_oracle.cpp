@@ -1,0 +1,1558 @@
+/*
+ * khb_oracle.cpp -- CPU ORACLE for the KHARMA per-step GRMHD hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path in
+ * kharma_b200/ is compared against.  Only tests/, __graft_entry__.smoke() and
+ * the CPU-baseline leg of bench.py may load it.  The product never links it.
+ *
+ * It is a plain, scalar, line-by-line restatement of the reference's device
+ * functions and step sequencing (AFD-Illinois/kharma), compiled with
+ * g++ -O2 -ffp-contract=off so every add/mul/div/sqrt is a single IEEE
+ * operation in the reference's evaluation order.  Each function cites the
+ * reference file:line it follows.
+ *
+ * Parity pinning: the reference cannot be built here (Parthenon, Kokkos and
+ * mpark::variant are empty submodules), so the oracle is pinned by the
+ * reference's own known-answer tests: the MHD linear-mode eigenvectors of
+ * kharma/prob/mhdmodes.hpp and the second-order convergence slopes that
+ * tests/mhdmodes/check.py asserts.  The pieces that live in the un-vendored
+ * Parthenon (RK2 coefficients, FluxDivHelper, WeightedSumData, outflow and
+ * reflecting boundary functions, UniformCartesian cell positions) are restated
+ * from their published algorithms and marked "Parthenon (unvendored)".
+ *
+ * Layout: every cell field is [var][k][j][i], i fastest, over the entire block
+ * including ghosts (n1 = nx1 + 2 ng; n2, n3 likewise when the direction is
+ * active, else 1).  Fluxes use the same shape; face index i is the left face
+ * of cell i.  Geometry caches follow GRCoordinates:
+ *   gcov/gcon [7][n2+1][n1+1][4][4], gdet [7][n2+1][n1+1],
+ *   conn/gdet_conn [n2][n1][4][4][4]           (gr_coordinates.cpp:105-109)
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <limits>
+
+namespace orc {
+
+// ---------------------------------------------------------------- basics
+static const double SMALL = 1e-20;                  // decs.hpp:82
+enum Loci { face1 = 0, face2, face3, center, corner, outer_half, inner_half };  // decs.hpp:104
+static const int NLOC = 7;
+
+// Kokkos::max/min semantics ((a<b)?b:a), used by the reference as m::max/m::min
+static inline double kmax(double a, double b) { return (a < b) ? b : a; }
+static inline double kmin(double a, double b) { return (b < a) ? b : a; }
+// kharma_utils.hpp:100-110
+static inline double clip(double n, double lower, double upper) { return kmin(kmax(lower, n), upper); }
+// kharma_utils.hpp:118-122
+static inline double excise(double n, double center, double range)
+{
+    return (std::fabs(n - center) > range) ? n : ((n > center) ? center + range : center - range);
+}
+// matrix.hpp:51-54
+static inline double dot4(const double* a, const double* b)
+{
+    return a[0]*b[0] + a[1]*b[1] + a[2]*b[2] + a[3]*b[3];
+}
+
+// ---------------------------------------------------------------- config
+struct Prescription {          // floors.hpp:100-117
+    double rho_min_const, u_min_const;
+    double rho_min_geom, u_min_geom, r_char;
+    double bsq_over_rho_max, bsq_over_u_max, u_over_rho_max;
+    double ktot_max, gamma_max;
+    int32_t use_r_char, temp_adjust_u, adjust_k, radius_dependent_floors;
+    double floors_switch_r;
+};
+
+struct CoordSpec {
+    int32_t base;       // 0 cartesian minkowski, 1 spherical minkowski, 2 spherical KS, 3 spherical BL
+    int32_t transform;  // 0 null, 1 exponential (eks), 2 modified (mks), 3 funky (fmks)
+    double a, hslope, mks_smooth, poly_xt, poly_alpha, startx1;
+};
+
+enum Recon { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3 };
+enum BC { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2 };
+enum Frame { FRAME_FLUID = 0, FRAME_NORMAL = 1, FRAME_DRIFT = 2 };
+
+struct Config {
+    int32_t nx1, nx2, nx3, ng;
+    double x1min, x2min, x3min, dx1, dx2, dx3;     // interior block start and widths (native coords)
+    double gam;
+    int32_t recon, riemann;                         // riemann: 0 llf, 1 hlle
+    int32_t nvar;                                   // 5 (GRHD) or 8 (GRMHD with flux-CT B)
+    int32_t driver;                                 // 0 simple, 1 kharma
+    int32_t bc[6];                                  // inner_x1, outer_x1, inner_x2, outer_x2, inner_x3, outer_x3
+    int32_t check_inflow_inner_x1, check_inflow_outer_x1;
+    int32_t zero_polar_flux, fix_polar_flux, fix_corner_inner;
+    int32_t floors_on, floor_frame, recon_floors;
+    int32_t iter_max; double err_tol;
+    int32_t fix_average_neighbors, fix_atmosphere;
+    double cfl, dt_min, max_dt_increase;
+    Prescription floors;
+};
+
+// ---------------------------------------------------------------- coordinates
+// coordinate_systems.hpp / coordinate_embedding.hpp restated
+struct Coords {
+    CoordSpec s;
+    double poly_norm;
+    bool spherical() const { return s.base != 0; }
+    bool cart_minkowski() const { return s.base == 0 && s.transform == 0; }   // coordinate_embedding.hpp:269-272
+
+    void init()
+    {
+        // coordinate_systems.hpp:599-601 (FunkyTransform constructor)
+        poly_norm = 0.5 * M_PI * 1./(1. + 1./(s.poly_alpha + 1.) * 1./std::pow(s.poly_xt, s.poly_alpha));
+    }
+    // coord_to_embed for each transform: coordinate_systems.hpp:358-367, 414-425, 538-549, 603-618
+    void coord_to_embed(const double X[4], double Xe[4]) const
+    {
+        switch (s.transform) {
+        case 0:
+            for (int mu = 0; mu < 4; ++mu) Xe[mu] = X[mu];
+            break;
+        case 1:
+            Xe[0] = X[0];
+            Xe[1] = std::exp(X[1]);
+            Xe[2] = excise(excise(X[2], 0.0, SMALL), M_PI, SMALL);
+            Xe[3] = X[3];
+            break;
+        case 2: {
+            Xe[0] = X[0];
+            Xe[1] = std::exp(X[1]);
+            const double th = M_PI*X[2] + ((1. - s.hslope)/2.)*std::sin(2.*M_PI*X[2]);
+            Xe[2] = excise(excise(th, 0.0, SMALL), M_PI, SMALL);
+            Xe[3] = X[3];
+            break;
+        }
+        default: {
+            Xe[0] = X[0];
+            Xe[1] = std::exp(X[1]);
+            const double thG = M_PI*X[2] + ((1. - s.hslope)/2.)*std::sin(2.*M_PI*X[2]);
+            const double y = 2*X[2] - 1.;
+            const double thJ = poly_norm * y * (1. + std::pow(y/s.poly_xt, s.poly_alpha) / (s.poly_alpha + 1.)) + 0.5 * M_PI;
+            const double th = thG + std::exp(s.mks_smooth * (s.startx1 - X[1])) * (thJ - thG);
+            Xe[2] = excise(excise(th, 0.0, SMALL), M_PI, SMALL);
+            Xe[3] = X[3];
+            break;
+        }
+        }
+    }
+    // dxdX: coordinate_systems.hpp:367-375, 435-443, 561-569, 630-656
+    void dxdX(const double X[4], double J[4][4]) const
+    {
+        for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) J[mu][nu] = (mu == nu);
+        switch (s.transform) {
+        case 0: break;
+        case 1:
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) J[mu][nu] = 0.;
+            J[0][0] = 1.; J[1][1] = std::exp(X[1]); J[2][2] = 1.; J[3][3] = 1.;
+            break;
+        case 2:
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) J[mu][nu] = 0.;
+            J[0][0] = 1.;
+            J[1][1] = std::exp(X[1]);
+            J[2][2] = M_PI - (s.hslope - 1.)*M_PI*std::cos(2.*M_PI*X[2]);
+            J[3][3] = 1.;
+            break;
+        default: {
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) J[mu][nu] = 0.;
+            const double hslope = s.hslope, mks_smooth = s.mks_smooth, startx1 = s.startx1;
+            const double poly_xt = s.poly_xt, poly_alpha = s.poly_alpha;
+            J[0][0] = 1.;
+            J[1][1] = std::exp(X[1]);
+            J[2][1] = -std::exp(mks_smooth * (startx1 - X[1])) * mks_smooth
+                * (
+                M_PI / 2. -
+                M_PI * X[2]
+                    + poly_norm * (2. * X[2] - 1.)
+                        * (1
+                            + (std::pow((-1. + 2 * X[2]) / poly_xt, poly_alpha))
+                                / (1 + poly_alpha))
+                    - 1. / 2. * (1. - hslope) * std::sin(2. * M_PI * X[2]));
+            J[2][2] = M_PI + (1. - hslope) * M_PI * std::cos(2. * M_PI * X[2])
+                + std::exp(mks_smooth * (startx1 - X[1]))
+                    * (-M_PI
+                        + 2. * poly_norm
+                            * (1.
+                                + std::pow((2. * X[2] - 1.) / poly_xt, poly_alpha)
+                                    / (poly_alpha + 1.))
+                        + (2. * poly_alpha * poly_norm * (2. * X[2] - 1.)
+                            * std::pow((2. * X[2] - 1.) / poly_xt, poly_alpha - 1.))
+                            / ((1. + poly_alpha) * poly_xt)
+                        - (1. - hslope) * M_PI * std::cos(2. * M_PI * X[2]));
+            J[3][3] = 1.;
+            break;
+        }
+        }
+    }
+    // gcov_embed for each base system: coordinate_systems.hpp:80-84, 94-105, 120-150, 271-289
+    void gcov_embed(const double Xe[4], double g[4][4]) const
+    {
+        const double a = s.a;
+        switch (s.base) {
+        case 0:
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu)
+                g[mu][nu] = (mu == nu) - 2*(mu == 0 && nu == 0);
+            break;
+        case 1: {
+            const double r = kmax(Xe[1], SMALL);
+            const double th = excise(excise(Xe[2], 0.0, SMALL), M_PI, SMALL);
+            const double sth = std::sin(th);
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) g[mu][nu] = 0.;
+            g[0][0] = 1.;  // sic: coordinate_systems.hpp:101
+            g[1][1] = 1.;
+            g[2][2] = r*r;
+            g[3][3] = sth*sth*r*r;
+            break;
+        }
+        case 2: {
+            const double r = Xe[1];
+            const double th = excise(excise(Xe[2], 0.0, SMALL), M_PI, SMALL);
+            const double cth = std::cos(th);
+            const double sth = std::sin(th);
+            const double sin2 = sth*sth;
+            const double rho2 = r*r + a*a*cth*cth;
+            g[0][0] = -1. + 2.*r/rho2;
+            g[0][1] = 2.*r/rho2;
+            g[0][2] = 0.;
+            g[0][3] = -2.*a*r*sin2/rho2;
+            g[1][0] = 2.*r/rho2;
+            g[1][1] = 1. + 2.*r/rho2;
+            g[1][2] = 0.;
+            g[1][3] = -a*sin2*(1. + 2.*r/rho2);
+            g[2][0] = 0.;
+            g[2][1] = 0.;
+            g[2][2] = rho2;
+            g[2][3] = 0.;
+            g[3][0] = -2.*a*r*sin2/rho2;
+            g[3][1] = -a*sin2*(1. + 2.*r/rho2);
+            g[3][2] = 0.;
+            g[3][3] = sin2*(rho2 + a*a*sin2*(1. + 2.*r/rho2));
+            break;
+        }
+        default: {
+            const double r = Xe[1];
+            const double th = excise(excise(Xe[2], 0.0, SMALL), M_PI, SMALL);
+            const double cth = std::cos(th), sth = std::sin(th);
+            const double sin2 = sth*sth;
+            const double a2 = a*a;
+            const double r2 = r*r;
+            const double mmu = 1. + a2*cth*cth/r2;
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) g[mu][nu] = 0.;
+            g[0][0] = -(1. - 2./(r*mmu));
+            g[0][3] = -2.*a*sin2/(r*mmu);
+            g[1][1] = mmu/(1. - 2./r + a2/r2);
+            g[2][2] = r2*mmu;
+            g[3][0] = -2.*a*sin2/(r*mmu);
+            g[3][3] = sin2*(r2 + a2 + 2.*a2*sin2/(r*mmu));
+            break;
+        }
+        }
+    }
+    // coordinate_embedding.hpp:488-500 (cov_tensor_to_native) and 503-514 (gcov_native)
+    void gcov_native(const double X[4], double g[4][4]) const
+    {
+        double gem[4][4], Xe[4], J[4][4];
+        coord_to_embed(X, Xe);
+        gcov_embed(Xe, gem);
+        dxdX(X, J);
+        for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) {
+            g[mu][nu] = 0;
+            for (int lam = 0; lam < 4; lam++)
+                for (int kap = 0; kap < 4; kap++)
+                    g[mu][nu] += gem[lam][kap]*J[lam][mu]*J[kap][nu];
+        }
+    }
+    double r_of(const double X[4]) const   // coordinate_embedding.hpp:362-373
+    {
+        double Xe[4];
+        coord_to_embed(X, Xe);
+        if (spherical()) return Xe[1];
+        return std::sqrt(Xe[1]*Xe[1] + Xe[2]*Xe[2] + Xe[3]*Xe[3]);
+    }
+};
+
+// matrix.hpp:56-115
+static inline double MINOR(const double m[16], int r0, int r1, int r2, int c0, int c1, int c2)
+{
+    return m[4*r0+c0]*(m[4*r1+c1]*m[4*r2+c2] - m[4*r2+c1]*m[4*r1+c2]) -
+           m[4*r0+c1]*(m[4*r1+c0]*m[4*r2+c2] - m[4*r2+c0]*m[4*r1+c2]) +
+           m[4*r0+c2]*(m[4*r1+c0]*m[4*r2+c1] - m[4*r2+c0]*m[4*r1+c1]);
+}
+static double invert(const double* m, double* o)
+{
+    o[ 0] =  MINOR(m,1,2,3,1,2,3); o[ 1] = -MINOR(m,0,2,3,1,2,3);
+    o[ 2] =  MINOR(m,0,1,3,1,2,3); o[ 3] = -MINOR(m,0,1,2,1,2,3);
+    o[ 4] = -MINOR(m,1,2,3,0,2,3); o[ 5] =  MINOR(m,0,2,3,0,2,3);
+    o[ 6] = -MINOR(m,0,1,3,0,2,3); o[ 7] =  MINOR(m,0,1,2,0,2,3);
+    o[ 8] =  MINOR(m,1,2,3,0,1,3); o[ 9] = -MINOR(m,0,2,3,0,1,3);
+    o[10] =  MINOR(m,0,1,3,0,1,3); o[11] = -MINOR(m,0,1,2,0,1,3);
+    o[12] = -MINOR(m,1,2,3,0,1,2); o[13] =  MINOR(m,0,2,3,0,1,2);
+    o[14] = -MINOR(m,0,1,3,0,1,2); o[15] =  MINOR(m,0,1,2,0,1,2);
+    const double det = m[0]*MINOR(m,1,2,3,1,2,3) - m[1]*MINOR(m,1,2,3,0,2,3) +
+                       m[2]*MINOR(m,1,2,3,0,1,3) - m[3]*MINOR(m,1,2,3,0,1,2);
+    const double inv_det = 1. / det;
+    for (int i = 0; i < 16; ++i) o[i] *= inv_det;
+    return det;
+}
+// coordinate_embedding.hpp:297-301
+static double gcon_from_gcov(const double g[4][4], double gc[4][4])
+{
+    const double gdet = invert(&g[0][0], &gc[0][0]);
+    return std::sqrt(std::fabs(gdet));
+}
+// coordinate_embedding.hpp:526-572
+static void conn_native(const Coords& C, const double X[4], double delta, double conn[4][4][4])
+{
+    double tmp[4][4][4], gcon[4][4], gcov[4][4], Xh[4], Xl[4], gh[4][4], gl[4][4];
+    for (int nu = 0; nu < 4; nu++) {
+        for (int mu = 0; mu < 4; ++mu) Xl[mu] = X[mu] - delta*(mu == nu);
+        for (int mu = 0; mu < 4; ++mu) Xh[mu] = X[mu] + delta*(mu == nu);
+        C.gcov_native(Xh, gh);
+        C.gcov_native(Xl, gl);
+        for (int lam = 0; lam < 4; lam++)
+            for (int kap = 0; kap < 4; kap++)
+                conn[lam][kap][nu] = (gh[lam][kap] - gl[lam][kap]) / (Xh[nu] - Xl[nu]);
+    }
+    for (int lam = 0; lam < 4; lam++)
+        for (int nu = 0; nu < 4; nu++)
+            for (int mu = 0; mu < 4; mu++)
+                tmp[lam][nu][mu] = 0.5 * (conn[nu][lam][mu] + conn[mu][lam][nu] - conn[mu][nu][lam]);
+    C.gcov_native(X, gcov);
+    gcon_from_gcov(gcov, gcon);
+    for (int lam = 0; lam < 4; lam++)
+        for (int nu = 0; nu < 4; nu++)
+            for (int mu = 0; mu < 4; mu++) {
+                conn[lam][nu][mu] = 0.;
+                for (int kap = 0; kap < 4; kap++)
+                    conn[lam][nu][mu] += gcon[lam][kap] * tmp[kap][nu][mu];
+            }
+}
+
+// ---------------------------------------------------------------- block
+struct Block {
+    Config c;
+    Coords C;
+    int ndim, n1, n2, n3;
+    int is, ie, js, je, ks, ke;
+    size_t N;
+    int nv;
+    // geometry caches (GRCoordinates layout)
+    std::vector<double> gcov, gcon, gdet, conn, gdet_conn;
+    std::vector<double> rcen;   // r at cell centres (j,i): floors use G.r(k,j,i)
+
+    void init(const Config& cfg, const CoordSpec& cs)
+    {
+        c = cfg; C.s = cs; C.init();
+        ndim = 1 + (c.nx2 > 1) + (c.nx3 > 1);
+        n1 = c.nx1 + 2*c.ng;
+        n2 = (c.nx2 > 1) ? c.nx2 + 2*c.ng : 1;
+        n3 = (c.nx3 > 1) ? c.nx3 + 2*c.ng : 1;
+        is = c.ng; ie = c.ng + c.nx1 - 1;
+        js = (c.nx2 > 1) ? c.ng : 0; je = js + c.nx2 - 1;
+        ks = (c.nx3 > 1) ? c.ng : 0; ke = ks + c.nx3 - 1;
+        N = (size_t)n1*n2*n3;
+        nv = c.nvar;
+    }
+    inline size_t id(int k, int j, int i) const { return ((size_t)k*n2 + j)*n1 + i; }
+
+    // Parthenon UniformCartesian (unvendored): Xf = xmin_entire + i dx, Xc = xmin_entire + (i+1/2) dx,
+    // xmin_entire = block xmin - nghost dx in active directions.
+    double Xf(int d, int idx) const
+    {
+        if (d == 1) return (c.x1min - c.ng*c.dx1) + idx*c.dx1;
+        if (d == 2) return (c.x2min - ((c.nx2 > 1) ? c.ng : 0)*c.dx2) + idx*c.dx2;
+        return (c.x3min - ((c.nx3 > 1) ? c.ng : 0)*c.dx3) + idx*c.dx3;
+    }
+    double Xc(int d, int idx) const
+    {
+        if (d == 1) return (c.x1min - c.ng*c.dx1) + (idx + 0.5)*c.dx1;
+        if (d == 2) return (c.x2min - ((c.nx2 > 1) ? c.ng : 0)*c.dx2) + (idx + 0.5)*c.dx2;
+        return (c.x3min - ((c.nx3 > 1) ? c.ng : 0)*c.dx3) + (idx + 0.5)*c.dx3;
+    }
+    double Dx(int d) const { return d == 1 ? c.dx1 : (d == 2 ? c.dx2 : c.dx3); }
+    // gr_coordinates.hpp:184-225
+    void coord(int k, int j, int i, int loc, double X[4]) const
+    {
+        X[0] = 0;
+        switch (loc) {
+        case face1:  X[1] = Xf(1, i); X[2] = Xc(2, j); X[3] = Xc(3, k); break;
+        case face2:  X[1] = Xc(1, i); X[2] = Xf(2, j); X[3] = Xc(3, k); break;
+        case face3:  X[1] = Xc(1, i); X[2] = Xc(2, j); X[3] = Xf(3, k); break;
+        case center: X[1] = Xc(1, i); X[2] = Xc(2, j); X[3] = Xc(3, k); break;
+        case corner: X[1] = Xf(1, i); X[2] = Xf(2, j); X[3] = Xf(3, k); break;
+        case outer_half: X[1] = Xc(1, i); X[2] = (Xc(2, j) + Xf(2, j+1)) / 2; X[3] = Xc(3, k); break;
+        default:     X[1] = Xc(1, i); X[2] = (Xc(2, j) + Xf(2, j)) / 2; X[3] = Xc(3, k); break;
+        }
+    }
+
+    // gr_coordinates.cpp:96-205 with connection_average_points = 1 (the default)
+    void build_geometry()
+    {
+        const int G1 = n1 + 1, G2 = n2 + 1;
+        gcov.assign((size_t)NLOC*G2*G1*16, 0.);
+        gcon.assign((size_t)NLOC*G2*G1*16, 0.);
+        gdet.assign((size_t)NLOC*G2*G1, 0.);
+        conn.assign((size_t)n2*n1*64, 0.);
+        gdet_conn.assign((size_t)n2*n1*64, 0.);
+        rcen.assign((size_t)n2*n1, 0.);
+        for (int j = 0; j < G2; ++j) for (int i = 0; i < G1; ++i) {
+            for (int loc = 0; loc < NLOC; ++loc) {
+                if ((loc == center || loc == face3) && (i >= n1 || j >= n2)) continue;
+                double X[4];
+                coord(0, j, i, loc, X);
+                double gl[4][4], gc[4][4];
+                C.gcov_native(X, gl);
+                const double gd = gcon_from_gcov(gl, gc);
+                const size_t g = ((size_t)loc*G2 + j)*G1 + i;
+                // averaging over one point: 0 + x/1 is exact
+                gdet[g] = gd;
+                for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) {
+                    gcov[g*16 + mu*4 + nu] = gl[mu][nu];
+                    gcon[g*16 + mu*4 + nu] = gc[mu][nu];
+                }
+                if (loc == center) {
+                    double cn[4][4][4];
+                    conn_native(C, X, 1.e-8, cn);      // gr_coordinates.cpp:49,158
+                    const size_t cg = ((size_t)j*n1 + i)*64;
+                    for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) for (int lam = 0; lam < 4; ++lam) {
+                        conn[cg + mu*16 + nu*4 + lam] = cn[mu][nu][lam];
+                        gdet_conn[cg + mu*16 + nu*4 + lam] = gd*cn[mu][nu][lam] / 1;
+                    }
+                    rcen[(size_t)j*n1 + i] = C.r_of(X);
+                }
+            }
+        }
+    }
+    inline size_t gi(int loc, int j, int i) const { return ((size_t)loc*(n2+1) + j)*(n1+1) + i; }
+    inline double Gcov(int loc, int j, int i, int mu, int nu) const { return gcov[gi(loc,j,i)*16 + mu*4 + nu]; }
+    inline double Gcon(int loc, int j, int i, int mu, int nu) const { return gcon[gi(loc,j,i)*16 + mu*4 + nu]; }
+    inline double Gdet(int loc, int j, int i) const { return gdet[gi(loc,j,i)]; }
+    inline double GdetConn(int j, int i, int mu, int nu, int lam) const
+    { return gdet_conn[((size_t)j*n1 + i)*64 + mu*16 + nu*4 + lam]; }
+    // gr_coordinates.hpp:227-238
+    void lower(const double* vcon, double* vcov, int j, int i, int loc) const
+    {
+        for (int mu = 0; mu < 4; ++mu) vcov[mu] = 0;
+        for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) vcov[mu] += Gcov(loc, j, i, mu, nu) * vcon[nu];
+    }
+    void raise(const double* vcov, double* vcon, int j, int i, int loc) const
+    {
+        for (int mu = 0; mu < 4; ++mu) vcon[mu] = 0;
+        for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) vcon[mu] += Gcon(loc, j, i, mu, nu) * vcov[nu];
+    }
+};
+
+// ---------------------------------------------------------------- reconstruction
+// reconstruction.hpp:46-56 and 106-204, 351-381
+static const double WENO_EPS = 1.e-26;
+static inline double mc(double dm, double dp)
+{
+    const double r = (std::fabs(dp) > 0. ? dm/dp : 2.0);
+    return kmax(0.0, kmin(2.0, kmin(2*r, 0.5*(1+r))));
+}
+// Single-zone reconstruction: lout = value at the left face of the zone, rout = at the right face
+static void recon_zone(int recon, double x1, double x2, double x3, double x4, double x5, double& lout, double& rout)
+{
+    switch (recon) {
+    case RECON_DONOR:
+        rout = x3; lout = x3;
+        break;
+    case RECON_MC: {
+        const double dq = mc(x3 - x2, x4 - x3)*(x4 - x3);
+        rout = x3 + 0.5*dq;
+        lout = x3 - 0.5*dq;
+        break;
+    }
+    case RECON_WENO5: {
+        double beta[3], c1, c2;
+        c1 = x1 - 2.*x2 + x3; c2 = x1 - 4.*x2 + 3.*x3;
+        beta[0] = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        c1 = x2 - 2.*x3 + x4; c2 = x4 - x2;
+        beta[1] = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        c1 = x3 - 2.*x4 + x5; c2 = x5 - 4.*x4 + 3.*x3;
+        beta[2] = (13./12.)*c1*c1 + (1./4.)*c2*c2;
+        double den[3] = {WENO_EPS + beta[0], WENO_EPS + beta[1], WENO_EPS + beta[2]};
+        den[0] *= den[0]; den[1] *= den[1]; den[2] *= den[2];
+        double wtr[3] = {(1./16.)/den[0], (5./8. )/den[1], (5./16.)/den[2]};
+        double Wr = wtr[0] + wtr[1] + wtr[2];
+        double wtl[3] = {(1./16.)/den[2], (5./8. )/den[1], (5./16.)/den[0]};
+        double Wl = wtl[0] + wtl[1] + wtl[2];
+        lout = ((3./8.)*x5 - (5./4.)*x4 + (15./8.)*x3)*(wtl[0] / Wl) +
+                ((-1./8.)*x4 + (3./4.)*x3 + (3./8.)*x2)*(wtl[1] / Wl) +
+                ((3./8.)*x3 + (3./4.)*x2 - (1./8.)*x1)*(wtl[2] / Wl);
+        rout = ((3./8.)*x1 - (5./4.)*x2 + (15./8.)*x3)*(wtr[0] / Wr) +
+                ((-1./8.)*x2 + (3./4.)*x3 + (3./8.)*x4)*(wtr[1] / Wr) +
+                ((3./8.)*x3 + (3./4.)*x4 - (1./8.)*x5)*(wtr[2] / Wr);
+        break;
+    }
+    default: {  // PPM
+        const double q_im2 = x1, q_im1 = x2, q_i = x3, q_ip1 = x4, q_ip2 = x5;
+        double qlv = (7.*(q_i + q_im1) - (q_im2 + q_ip1))/12.0;
+        double qrv = (7.*(q_i + q_ip1) - (q_im1 + q_ip2))/12.0;
+        qlv = kmax(qlv, kmin(q_i, q_im1));
+        qlv = kmin(qlv, kmax(q_i, q_im1));
+        qrv = kmax(qrv, kmin(q_i, q_ip1));
+        qrv = kmin(qrv, kmax(q_i, q_ip1));
+        double qc = qrv - q_i;
+        double qd = qlv - q_i;
+        if ((qc*qd) >= 0.0) {
+            qlv = q_i;
+            qrv = q_i;
+        } else {
+            if (std::fabs(qc) >= 2.0*std::fabs(qd)) qrv = q_i - 2.0*qd;
+            if (std::fabs(qd) >= 2.0*std::fabs(qc)) qlv = q_i - 2.0*qc;
+        }
+        lout = qlv; rout = qrv;
+        break;
+    }
+    }
+}
+
+// ---------------------------------------------------------------- GRMHD device functions
+struct FourVectors { double ucon[4], ucov[4], bcon[4], bcov[4]; };   // types.hpp:90-95
+
+// grmhd_functions.hpp:121-133 (local primitives)
+static double lorentz_calc(const Block& B, const double* P, int j, int i, int loc)
+{
+    const double qsq = B.Gcov(loc, j, i, 1, 1) * P[2] * P[2] +
+                       B.Gcov(loc, j, i, 2, 2) * P[3] * P[3] +
+                       B.Gcov(loc, j, i, 3, 3) * P[4] * P[4] +
+                       2. * (B.Gcov(loc, j, i, 1, 2) * P[2] * P[3] +
+                             B.Gcov(loc, j, i, 1, 3) * P[2] * P[4] +
+                             B.Gcov(loc, j, i, 2, 3) * P[3] * P[4]);
+    return std::sqrt(1. + qsq);
+}
+// grmhd_functions.hpp:225-246
+static void calc_4vecs(const Block& B, const double* P, bool has_b, int j, int i, int loc, FourVectors& D)
+{
+    const double gamma = lorentz_calc(B, P, j, i, loc);
+    const double alpha = 1. / std::sqrt(-B.Gcon(loc, j, i, 0, 0));
+    D.ucon[0] = gamma / alpha;
+    for (int v = 0; v < 3; ++v) D.ucon[v+1] = P[2 + v] - gamma * alpha * B.Gcon(loc, j, i, 0, v+1);
+    B.lower(D.ucon, D.ucov, j, i, loc);
+    if (has_b) {
+        D.bcon[0] = 0;
+        for (int v = 0; v < 3; ++v) D.bcon[0] += P[5 + v] * D.ucov[v+1];
+        for (int v = 0; v < 3; ++v) D.bcon[v+1] = (P[5 + v] + D.bcon[0] * D.ucon[v+1]) / D.ucon[0];
+        B.lower(D.bcon, D.bcov, j, i, loc);
+    } else {
+        for (int mu = 0; mu < 4; ++mu) D.bcon[mu] = D.bcov[mu] = 0.;
+    }
+}
+// grmhd_functions.hpp:51-60 (GRHD) and 142-155 (GRMHD)
+static void calc_tensor(double rho, double u, double pgas, const FourVectors& D, int dir, bool has_b, double T[4])
+{
+    if (has_b) {
+        const double bsq = dot4(D.bcon, D.bcov);
+        const double eta = pgas + rho + u + bsq;
+        const double ptot = pgas + 0.5 * bsq;
+        for (int mu = 0; mu < 4; ++mu)
+            T[mu] = eta * D.ucon[dir] * D.ucov[mu] + ptot * (dir == mu) - D.bcon[dir] * D.bcov[mu];
+    } else {
+        const double eta = pgas + rho + u;
+        for (int mu = 0; mu < 4; ++mu)
+            T[mu] = eta * D.ucon[dir] * D.ucov[mu] + pgas * (dir == mu);
+    }
+}
+// flux_functions.hpp:116-178 (local form, GRMHD variables)
+static void prim_to_flux(const Block& B, const double* P, const FourVectors& D, int j, int i, int dir,
+                         double* flux, int loc)
+{
+    const double gam = B.c.gam;
+    const bool has_b = B.nv > 5;
+    const double gdet = B.Gdet(loc, j, i);
+    flux[0] = P[0] * D.ucon[dir] * gdet;
+    double T[4];
+    calc_tensor(P[0], P[1], (gam - 1) * P[1], D, dir, has_b, T);
+    flux[1] = T[0] * gdet + flux[0];
+    flux[2] = T[1] * gdet;
+    flux[3] = T[2] * gdet;
+    flux[4] = T[3] * gdet;
+    if (has_b) {
+        if (dir == 0) {
+            for (int v = 0; v < 3; ++v) flux[5 + v] = P[5 + v] * gdet;
+        } else {
+            for (int v = 0; v < 3; ++v) flux[5 + v] = (D.bcon[v+1] * D.ucon[dir] - D.bcon[dir] * D.ucon[v+1]) * gdet;
+        }
+    }
+}
+// flux_functions.hpp:368-439.  Note clip() results are discarded in the reference (:378, :409).
+static void vchar(const Block& B, const double* P, const FourVectors& D, int j, int i, int loc, int dir,
+                  double& cmax, double& cmin)
+{
+    const double gam = B.c.gam;
+    const double ef  = P[0] + gam * P[1];
+    const double cs2 = gam * (gam - 1) * P[1] / ef;
+    double cms2;
+    if (B.nv > 5) {
+        const double bsq = dot4(D.bcon, D.bcov);
+        const double va2 = bsq / (bsq + ef);
+        cms2 = cs2 + va2 - cs2 * va2;
+    } else {
+        cms2 = cs2;
+    }
+    double Bcov[4] = {1., 0., 0., 0.};
+    double Acov[4] = {0., 0., 0., 0.}; Acov[dir] = 1.;
+    double Acon[4], Bcon[4];
+    B.raise(Acov, Acon, j, i, loc);
+    B.raise(Bcov, Bcon, j, i, loc);
+    const double Asq = dot4(Acon, Acov);
+    const double Bsq = dot4(Bcon, Bcov);
+    const double Au  = dot4(Acov, D.ucon);
+    const double Bu  = dot4(Bcov, D.ucon);
+    const double AB  = dot4(Acon, Bcov);
+    const double A  = Bu*Bu - (Bsq + Bu*Bu) * cms2;
+    const double Bq = 2. * (Au*Bu - (AB + Au*Bu) * cms2);
+    const double Cq = Au*Au - (Asq + Au*Au) * cms2;
+    const double discr = std::sqrt(kmax(Bq * Bq - 4. * A * Cq, 0.));
+    const double vp = -(-Bq + discr) / (2. * A);
+    const double vm = -(-Bq - discr) / (2. * A);
+    cmax = kmax(vp, vm);
+    cmin = kmin(vp, vm);
+}
+// flux.hpp:110-121
+static inline double llf(double fL, double fR, double cmax, double cmin, double Ul, double Ur)
+{
+    const double ctop = kmax(cmax, cmin);
+    return 0.5 * (fL + fR - ctop * (Ur - Ul));
+}
+static inline double hlle(double fL, double fR, double cmax, double cmin, double Ul, double Ur)
+{
+    return (cmax*fL + cmin*fR - cmax*cmin*(Ur - Ul)) / (cmax + cmin);
+}
+
+// floors_functions.hpp:320-354 (local form; loc ignored for r as in the reference, which uses G.r(0,j,i))
+static int apply_geo_floors_local(const Block& B, double* P, int j, int i)
+{
+    const Prescription& f = B.c.floors;
+    double rhoflr_geom, uflr_geom;
+    if (B.C.spherical()) {
+        const double r = B.rcen[(size_t)j*B.n1 + i];
+        const double rhoscal = (f.use_r_char) ? 1. / ((r*r) * (1 + r / f.r_char)) : 1. / std::sqrt(r*r*r);
+        rhoflr_geom = kmax(f.rho_min_geom * rhoscal, f.rho_min_const);
+        uflr_geom   = kmax(f.u_min_geom * std::pow(rhoscal, B.c.gam), f.u_min_const);
+    } else {
+        rhoflr_geom = f.rho_min_const;
+        uflr_geom   = f.u_min_const;
+    }
+    int fflag = 0;
+    fflag |= (rhoflr_geom > P[0]) * 4096;
+    fflag |= (uflr_geom > P[1]) * 8192;
+    P[0] += kmax(0., rhoflr_geom - P[0]);
+    P[1] += kmax(0., uflr_geom - P[1]);
+    return fflag;
+}
+
+// ---------------------------------------------------------------- GetFlux
+// get_flux.hpp:60-373.  Faces are computed on the range every consumer needs:
+// face direction [s, e+1], transverse directions [s-1, e+1] (the reference's range is a superset).
+static void get_flux(const Block& B, int dir, const double* P, double* F, double* cmaxo, double* cmino)
+{
+    const int nv = B.nv, loc = dir - 1;   // loc_of(dir): face1/2/3 = 0/1/2
+    const int d1 = (dir == 1), d2 = (dir == 2), d3 = (dir == 3);
+    const int i0 = B.is - (B.ndim >= 1 && !d1 ? 1 : 0), i1 = B.ie + 1;
+    const int j0 = (B.ndim >= 2) ? B.js - (d2 ? 0 : 1) : B.js, j1 = (B.ndim >= 2) ? B.je + 1 : B.je;
+    const int k0 = (B.ndim >= 3) ? B.ks - (d3 ? 0 : 1) : B.ks, k1 = (B.ndim >= 3) ? B.ke + 1 : B.ke;
+    const int si = d1, sj = d2 ? B.n1 : 0, sk = d3 ? B.n1*B.n2 : 0;
+    const ptrdiff_t st = si + sj + (ptrdiff_t)sk;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = k0; k <= k1; ++k) for (int j = j0; j <= j1; ++j) for (int i = i0; i <= i1; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pl[8], Pr[8];
+        for (int p = 0; p < nv; ++p) {
+            const double* q = P + (size_t)p*B.N;
+            double l, r;
+            // Left state: right face of zone c-1 (ReconstructX1 ql(i+1) / ReconstructX{2,3}l reconstruct_right)
+            recon_zone(B.c.recon, q[c - 3*st], q[c - 2*st], q[c - st], q[c], q[c + st], l, r);
+            Pl[p] = r;
+            // Right state: left face of zone c (qr(i) / reconstruct_left)
+            recon_zone(B.c.recon, q[c - 2*st], q[c - st], q[c], q[c + st], q[c + 2*st], l, r);
+            Pr[p] = l;
+        }
+        if (B.c.recon_floors) {    // get_flux.hpp:174-181
+            apply_geo_floors_local(B, Pl, j, i);
+            apply_geo_floors_local(B, Pr, j, i);
+        }
+        FourVectors Dl, Dr;
+        double Ul[8], Fl[8], Ur[8], Fr[8], cmaxL, cminL, cmaxR, cminR;
+        calc_4vecs(B, Pl, nv > 5, j, i, loc, Dl);
+        prim_to_flux(B, Pl, Dl, j, i, 0, Ul, loc);
+        prim_to_flux(B, Pl, Dl, j, i, dir, Fl, loc);
+        vchar(B, Pl, Dl, j, i, loc, dir, cmaxL, cminL);
+        double cmax = kmax(0., cmaxL);
+        double cmin = kmin(0., cminL);
+        calc_4vecs(B, Pr, nv > 5, j, i, loc, Dr);
+        prim_to_flux(B, Pr, Dr, j, i, 0, Ur, loc);
+        prim_to_flux(B, Pr, Dr, j, i, dir, Fr, loc);
+        vchar(B, Pr, Dr, j, i, loc, dir, cmaxR, cminR);
+        cmax = kmax(cmax, cmaxR);
+        cmin = -kmin(cmin, cminR);
+        cmaxo[c] = cmax; cmino[c] = cmin;
+        for (int p = 0; p < nv; ++p)
+            F[(size_t)p*B.N + c] = B.c.riemann ? hlle(Fl[p], Fr[p], cmax, cmin, Ul[p], Ur[p])
+                                               : llf(Fl[p], Fr[p], cmax, cmin, Ul[p], Ur[p]);
+    }
+}
+
+// ---------------------------------------------------------------- FixFlux
+// b_flux_ct.cpp:372-418 (ZeroBoundaryFlux, X2 faces only: fix_polar_flux)
+static void zero_boundary_flux_x2(const Block& B, double* F1, double* F2, double* F3, bool inner)
+{
+    if (B.ndim < 2) return;
+    const size_t N = B.N;
+    const int ibs_s = B.is - 1, ibs_e = B.ie + 1;
+    const int kbs_s = B.ks - (B.ndim > 2), kbs_e = B.ke + (B.ndim > 2);
+    const int j = inner ? B.js : B.je + 1;
+    for (int k = kbs_s; k <= kbs_e; ++k) for (int i = ibs_s; i <= ibs_e; ++i) {
+        F2[5*N + B.id(k, j, i)] = 0.;
+        F2[7*N + B.id(k, j, i)] = 0.;
+        if (inner) {
+            F1[6*N + B.id(k, j-1, i)] = -F1[6*N + B.id(k, j, i)];
+            if (B.ndim > 2) F3[6*N + B.id(k, j-1, i)] = -F3[6*N + B.id(k, j, i)];
+        } else {
+            F1[6*N + B.id(k, j, i)] = -F1[6*N + B.id(k, j-1, i)];
+            if (B.ndim > 2) F3[6*N + B.id(k, j, i)] = -F3[6*N + B.id(k, j-1, i)];
+        }
+    }
+}
+// b_flux_ct.cpp:307-370
+static void flux_ct(const Block& B, double* F1, double* F2, double* F3)
+{
+    if (B.ndim < 2) return;
+    const size_t N = B.N;
+    const int ndim = B.ndim;
+    const int il_s = B.is, il_e = B.ie + 1, jl_s = B.js, jl_e = B.je + 1;
+    const int kl_s = B.ks, kl_e = (ndim > 2) ? B.ke + 1 : B.ke;
+    std::vector<double> emf(3*N, 0.);
+    double* e1 = emf.data(); double* e2 = e1 + N; double* e3 = e2 + N;
+    const size_t sj = B.n1, sk = (size_t)B.n1*B.n2;
+    for (int k = kl_s; k <= kl_e; ++k) for (int j = jl_s; j <= jl_e; ++j) for (int i = il_s; i <= il_e; ++i) {
+        const size_t c = B.id(k, j, i);
+        if (ndim > 2) {
+            e1[c] = 0.25 * (F2[7*N + c] + F2[7*N + c - sk] - F3[6*N + c] - F3[6*N + c - sj]);
+            e2[c] = 0.25 * (F3[5*N + c] + F3[5*N + c - 1] - F1[7*N + c] - F1[7*N + c - sk]);
+        }
+        e3[c] = 0.25 * (F1[6*N + c] + F1[6*N + c - sj] - F2[5*N + c] - F2[5*N + c - 1]);
+    }
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = il_s; i <= il_e; ++i) {
+        const size_t c = B.id(k, j, i);
+        F1[5*N + c] = 0.0;
+        F1[6*N + c] = 0.5 * (e3[c] + e3[c + sj]);
+        if (ndim > 2) F1[7*N + c] = -0.5 * (e2[c] + e2[c + sk]);
+    }
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = jl_s; j <= jl_e; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        F2[5*N + c] = -0.5 * (e3[c] + e3[c + 1]);
+        F2[6*N + c] = 0.0;
+        if (ndim > 2) F2[7*N + c] = 0.5 * (e1[c] + e1[c + sk]);
+    }
+    if (ndim > 2) {
+        for (int k = kl_s; k <= kl_e; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+            const size_t c = B.id(k, j, i);
+            F3[5*N + c] = 0.5 * (e2[c] + e2[c + 1]);
+            F3[6*N + c] = -0.5 * (e1[c] + e1[c + sj]);
+            F3[7*N + c] = 0.0;
+        }
+    }
+}
+// boundaries.cpp:611-690 (check_inflow flux limiting on X1, zero_flux on X2 poles)
+static void boundaries_fix_flux(const Block& B, double* F[3])
+{
+    const size_t N = B.N;
+    for (int face = 0; face < 4; ++face) {
+        const int bdir = face / 2 + 1;
+        const bool binner = (face % 2) == 0;
+        if (bdir > B.ndim) continue;
+        if (B.c.bc[face] == BC_PERIODIC) continue;   // only global "user" boundaries
+        // one-zone halo range, collapsed to the boundary face
+        int is_ = B.is - 1, ie_ = B.ie + 1, js_ = B.js - (B.ndim > 1), je_ = B.je + (B.ndim > 1);
+        int ks_ = B.ks - (B.ndim > 2), ke_ = B.ke + (B.ndim > 2);
+        if (bdir == 1) is_ = ie_ = binner ? B.is : B.ie + 1;
+        else if (bdir == 2) js_ = je_ = binner ? B.js : B.je + 1;
+        const bool check_inflow = (face == 0 && B.c.check_inflow_inner_x1) || (face == 1 && B.c.check_inflow_outer_x1);
+        const bool zero_flux = B.c.zero_polar_flux && bdir == 2;
+        for (int k = ks_; k <= ke_; ++k) for (int j = js_; j <= je_; ++j) for (int i = is_; i <= ie_; ++i) {
+            const size_t c = B.id(k, j, i);
+            if (check_inflow) {
+                double& f = F[bdir-1][c];
+                f = binner ? kmin(f, 0.) : kmax(f, 0.);
+            }
+            if (zero_flux)
+                for (int p = 0; p < B.nv; ++p) F[bdir-1][(size_t)p*N + c] = 0.;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- divergence and sources
+// Parthenon FluxDivHelper (unvendored), called from kharma_driver.hpp:208-231
+static void flux_divergence(const Block& B, double* F[3], double* dudt)
+{
+    const size_t N = B.N;
+    const double a1 = B.c.dx2*B.c.dx3, a2 = B.c.dx1*B.c.dx3, a3 = B.c.dx1*B.c.dx2;
+    const double vol = B.c.dx1*B.c.dx2*B.c.dx3;
+    const size_t sj = B.n1, sk = (size_t)B.n1*B.n2;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int p = 0; p < B.nv; ++p)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i), pc = (size_t)p*N + c;
+        double du = (a1 * F[0][pc + 1] - a1 * F[0][pc]);
+        if (B.ndim >= 2) du += a2 * F[1][pc + sj] - a2 * F[1][pc];
+        if (B.ndim == 3) du += a3 * F[2][pc + sk] - a3 * F[2][pc];
+        dudt[pc] = -du / vol;
+    }
+}
+// flux.cpp:395-444
+static void add_geo_source(const Block& B, const double* P, double* dudt)
+{
+    if (B.C.cart_minkowski()) return;
+    const size_t N = B.N;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pc[8];
+        for (int p = 0; p < B.nv; ++p) Pc[p] = P[(size_t)p*N + c];
+        FourVectors D;
+        calc_4vecs(B, Pc, B.nv > 5, j, i, center, D);
+        double Tmu[4] = {0}, new_du[4] = {0};
+        for (int mu = 0; mu < 4; ++mu) {
+            calc_tensor(Pc[0], Pc[1], (B.c.gam - 1) * Pc[1], D, mu, B.nv > 5, Tmu);
+            for (int nu = 0; nu < 4; ++nu)
+                for (int lam = 0; lam < 4; ++lam)
+                    new_du[lam] += Tmu[nu] * B.GdetConn(j, i, nu, lam, mu);
+        }
+        dudt[1*N + c] += new_du[0];
+        for (int v = 0; v < 3; ++v) dudt[(size_t)(2 + v)*N + c] += new_du[1 + v];
+    }
+}
+
+// ---------------------------------------------------------------- P <-> U
+// flux_functions.hpp:343-352 (Flux::p_to_u, global): 4-vectors at the centre, gdet at loc=center
+static void p_to_u_cell(const Block& B, const double* P, double* U, size_t c, int j, int i)
+{
+    double Pc[8], Uc[8];
+    for (int p = 0; p < B.nv; ++p) Pc[p] = P[(size_t)p*B.N + c];
+    FourVectors D;
+    calc_4vecs(B, Pc, B.nv > 5, j, i, center, D);
+    prim_to_flux(B, Pc, D, j, i, 0, Uc, center);
+    for (int p = 0; p < B.nv; ++p) U[(size_t)p*B.N + c] = Uc[p];
+}
+// flux_functions.hpp:354-363 / 312-328 (p_to_u_mhd: only rho, u, uvec conserved)
+static void p_to_u_mhd_cell(const Block& B, const double* P, double* U, size_t c, int j, int i)
+{
+    double Pc[8], Uc[8];
+    for (int p = 0; p < B.nv; ++p) Pc[p] = P[(size_t)p*B.N + c];
+    FourVectors D;
+    calc_4vecs(B, Pc, B.nv > 5, j, i, center, D);
+    prim_to_flux(B, Pc, D, j, i, 0, Uc, center);
+    for (int p = 0; p < 5; ++p) U[(size_t)p*B.N + c] = Uc[p];
+}
+
+// ---------------------------------------------------------------- 1D_W inversion
+enum Status { success = 0, neg_input, max_iter, bad_ut, bad_gamma, neg_rho, neg_u, neg_rhou };  // invert_template.hpp:53
+// onedw.hpp:49-67
+static inline double lorentz_calc_w(double Bsq, double D, double QdB, double Qtsq, double Wp)
+{
+    const double QdBsq = QdB * QdB;
+    const double W = Wp + D;
+    const double W2 = W * W;
+    const double WB = W + Bsq;
+    const double utsq = -((W + WB) * QdBsq + W2 * Qtsq) / (QdBsq * (W + WB) + W2 * (Qtsq - WB * WB));
+    if (utsq < -1.e-15 || utsq > 1.e7) return -1.;
+    return std::sqrt(1. + std::fabs(utsq));
+}
+// onedw.hpp:72-84
+static inline double err_eqn(double gam, double Bsq, double D, double Ep, double QdB, double Qtsq, double Wp, int& eflag)
+{
+    const double W = Wp + D;
+    const double gamma = lorentz_calc_w(Bsq, D, QdB, Qtsq, Wp);
+    if (gamma < 1) eflag = bad_ut;
+    const double w = W / (gamma*gamma);
+    const double rho = D / gamma;
+    const double p = (w - rho) * (gam - 1) / gam;
+    return -Ep + Wp - p + 0.5 * Bsq + 0.5 * (Bsq * Qtsq - QdB * QdB) / ((Bsq + W)*(Bsq + W));
+}
+// onedw.hpp:89-233.  U and P are the cell's conserved/primitive values; P is updated only on success.
+static int u_to_p_onedw(const Block& B, const double* U, double* P, int j, int i, int loc, int max_iterations, double tol)
+{
+    const double gam = B.c.gam;
+    if (U[0] <= 0.) return neg_input;
+    const double alpha = 1./std::sqrt(-B.Gcon(loc, j, i, 0, 0));
+    const double gdet = B.Gdet(loc, j, i);
+    const double a_over_g = alpha / gdet;
+    const double D = U[0] * a_over_g;
+    double Bcon[4] = {0};
+    if (B.nv > 5) {
+        Bcon[1] = U[5] * a_over_g;
+        Bcon[2] = U[6] * a_over_g;
+        Bcon[3] = U[7] * a_over_g;
+    }
+    const double Qcov[4] = {(U[1] - U[0]) * a_over_g, U[2] * a_over_g, U[3] * a_over_g, U[4] * a_over_g};
+    const double ncov[4] = {-alpha, 0., 0., 0.};
+    double Bcov[4], Qcon[4], ncon[4];
+    B.lower(Bcon, Bcov, j, i, loc);
+    B.raise(Qcov, Qcon, j, i, loc);
+    B.raise(ncov, ncon, j, i, loc);
+    const double Bsq = dot4(Bcon, Bcov);
+    const double QdB = dot4(Bcon, Qcov);
+    const double Qdotn = dot4(Qcon, ncov);
+    double Qtcon[4];
+    for (int mu = 0; mu < 4; ++mu) Qtcon[mu] = Qcon[mu] + ncon[mu] * Qdotn;
+    const double Qtsq = dot4(Qcon, Qcov) + Qdotn*Qdotn;
+    const double Ep = -Qdotn - D;
+    int eflag = success;
+    double Wp, err;
+    {
+        const double gamma = lorentz_calc(B, P, j, i, loc);
+        if (gamma < 1) return bad_ut;
+        const double rho = P[0], u = P[1];
+        Wp = (rho + u + (gam - 1) * u) * gamma * gamma - rho * gamma;
+        err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+    }
+    double dW;
+    {
+        const double Wpm = (1. - 1.e-5) * Wp;
+        const double h = Wp - Wpm;
+        const double Wpp = Wp + h;
+        const double errm = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wpm, eflag);
+        const double errp = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wpp, eflag);
+        const double dedW = (errp - errm) / (Wpp - Wpm);
+        const double dedW2 = (errp - 2. * err + errm) / (h*h);
+        const double f = clip(0.5 * err * dedW2 / (dedW*dedW), -0.3, 0.3);
+        dW = clip(-err / dedW / (1. - f), -0.5*Wp, 2.0*Wp);
+    }
+    double Wp1 = Wp;
+    double err1 = err;
+    Wp += dW;
+    err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+    int iter = 0;
+    for (iter = 0; iter < max_iterations; iter++) {
+        dW = clip((Wp1 - Wp) * err / (err - err1), -0.5*Wp, 2.0*Wp);
+        Wp1 = Wp;
+        err1 = err;
+        Wp += dW;
+        if (std::fabs(dW / Wp) < tol) break;
+        err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+        if (std::fabs(err / Wp) < tol) break;
+    }
+    if (iter == max_iterations) return max_iter;
+    const double gamma = lorentz_calc_w(Bsq, D, QdB, Qtsq, Wp);
+    if (gamma < 1) return bad_ut;
+    const double rho = D / gamma;
+    const double W = Wp + D;
+    const double w = W / (gamma*gamma);
+    const double p = (w - rho) * (gam - 1) / gam;
+    const double u = w - (rho + p);
+    if (rho < 0 && u < 0) return neg_rhou;
+    else if (rho < 0) return neg_rho;
+    else if (u < 0) return neg_u;
+    P[0] = rho;
+    P[1] = u;
+    const double pre = (gamma / (W + Bsq));
+    P[2] = pre * (Qtcon[1] + QdB * Bcon[1] / W);
+    P[3] = pre * (Qtcon[2] + QdB * Bcon[2] / W);
+    P[4] = pre * (Qtcon[3] + QdB * Bcon[3] / W);
+    return success;
+}
+
+// ---------------------------------------------------------------- floors
+// floors_functions.hpp:84-160
+static int determine_floors(const Block& B, const double* P, int j, int i, double& rhoflr_max, double& uflr_max)
+{
+    const Prescription& f = B.c.floors;
+    const double gam = B.c.gam;
+    double rhoflr_geom, uflr_geom;
+    if (B.C.spherical()) {
+        const double r = B.rcen[(size_t)j*B.n1 + i];
+        const double rhoscal = (f.use_r_char) ? 1. / ((r*r) * (1 + r / f.r_char)) : 1. / std::sqrt(r*r*r);
+        rhoflr_geom = kmax(f.rho_min_geom * rhoscal, f.rho_min_const);
+        uflr_geom   = kmax(f.u_min_geom * std::pow(rhoscal, gam), f.u_min_const);
+    } else {
+        rhoflr_geom = f.rho_min_const;
+        uflr_geom   = f.u_min_const;
+    }
+    FourVectors D;
+    calc_4vecs(B, P, B.nv > 5, j, i, center, D);
+    const double bsq = dot4(D.bcon, D.bcov);
+    const double rhoflr_b = bsq / f.bsq_over_rho_max;
+    const double uflr_b   = bsq / f.bsq_over_u_max;
+    uflr_max = kmax(uflr_geom, uflr_b);
+    const double rho = P[0], u = P[1];
+    int fflag = 0;
+    if (!f.temp_adjust_u) {
+        const double rhoflr_temp = kmax(u, uflr_max) / f.u_over_rho_max;
+        fflag |= (rhoflr_temp > rho) * 512;
+        rhoflr_max = kmax(kmax(rhoflr_geom, rhoflr_b), rhoflr_temp);
+    } else {
+        rhoflr_max = kmax(rhoflr_geom, rhoflr_b);
+    }
+    if (rhoflr_max > rho || uflr_max > u) {
+        fflag |= (rhoflr_geom > rho) * 32;
+        fflag |= (uflr_geom > u) * 64;
+        fflag |= (rhoflr_b > rho) * 128;
+        fflag |= (uflr_b > u) * 256;
+    }
+    if (lorentz_calc(B, P, j, i, center) > f.gamma_max) fflag |= 1024;
+    if ((gam - 1.) * P[1] / std::pow(P[0], gam) > f.ktot_max) fflag |= 2048;
+    if (f.temp_adjust_u && (P[1] / P[0] > f.u_over_rho_max)) fflag |= 512;
+    return fflag;
+}
+// floors_functions.hpp:50-82
+static void apply_ceilings(const Block& B, double* P, int j, int i)
+{
+    const Prescription& f = B.c.floors;
+    const double gam = B.c.gam;
+    const double gamma = lorentz_calc(B, P, j, i, center);
+    const double ktot = (gam - 1.) * P[1] / std::pow(P[0], gam);
+    if (gamma > f.gamma_max) {
+        const double fr = std::sqrt((f.gamma_max*f.gamma_max - 1.) / (gamma*gamma - 1.));
+        for (int v = 0; v < 3; ++v) P[2 + v] *= fr;
+    }
+    if (ktot > f.ktot_max) P[1] = f.ktot_max / ktot * P[1];
+    if (f.temp_adjust_u && P[1] / P[0] > f.u_over_rho_max) P[1] = f.u_over_rho_max * P[0];
+}
+// floors_functions.hpp:174-179 (fluid) and 181-252 (drift)
+static int apply_floors_frame(const Block& B, double* P, double* U, int j, int i, double rhoflr_max, double uflr_max)
+{
+    const double gam = B.c.gam;
+    if (B.c.floor_frame == FRAME_FLUID) {
+        P[0] += kmax(0., rhoflr_max - P[0]);
+        P[1] += kmax(0., uflr_max - P[1]);
+        return 0;
+    } else if (B.c.floor_frame == FRAME_DRIFT) {
+        const double lapse2 = 1. / (-B.Gcon(center, j, i, 0, 0));
+        double beta[4] = {0};
+        beta[1] = lapse2 * B.Gcon(center, j, i, 0, 1);
+        beta[2] = lapse2 * B.Gcon(center, j, i, 0, 2);
+        beta[3] = lapse2 * B.Gcon(center, j, i, 0, 3);
+        const double rho = P[0];
+        const double uu = P[1];
+        const double pg = (gam - 1.) * uu;
+        const double w_old = kmax(rho + uu + pg, SMALL);
+        double Bcon[4] = {0}, Bcov[4] = {0};
+        if (B.nv > 5) { Bcon[0] = 0; Bcon[1] = P[5]; Bcon[2] = P[6]; Bcon[3] = P[7]; }
+        for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) Bcov[mu] += B.Gcov(center, j, i, mu, nu) * Bcon[nu];
+        const double Bsq = kmax(dot4(Bcon, Bcov), SMALL);
+        const double B_mag = std::sqrt(Bsq);
+        FourVectors D;
+        calc_4vecs(B, P, B.nv > 5, j, i, center, D);
+        double Qcov[4] = {0};
+        Qcov[0] = w_old * D.ucon[0] * D.ucov[0] + pg;
+        Qcov[1] = w_old * D.ucon[0] * D.ucov[1];
+        Qcov[2] = w_old * D.ucon[0] * D.ucov[2];
+        Qcov[3] = w_old * D.ucon[0] * D.ucov[3];
+        const double QdotB = dot4(Bcon, Qcov);
+        double vpar = QdotB / (B_mag * w_old * D.ucon[0]*D.ucon[0]);
+        double ucon_dr[4] = {0};
+        ucon_dr[0] = 1. / std::sqrt(1. / (D.ucon[0]*D.ucon[0]) + vpar*vpar);
+        for (int mu = 0; mu < 4; ++mu) ucon_dr[mu] = D.ucon[mu] * (ucon_dr[0] / D.ucon[0]) - (vpar * Bcon[mu] * ucon_dr[0] / B_mag);
+        P[0] = kmax(rho, rhoflr_max);
+        P[1] = kmax(uu, uflr_max);
+        const double pg_new = (gam - 1.) * P[1];
+        const double w_new  = P[0] + P[1] + pg_new;
+        const double x = (2. * QdotB) / (B_mag * w_new * ucon_dr[0]);
+        vpar = x / (1 + std::sqrt(1 + x*x)) * (1. / ucon_dr[0]);
+        D.ucon[0] = 1. / std::sqrt(1/(ucon_dr[0]*ucon_dr[0]) - vpar*vpar);
+        for (int mu = 0; mu < 4; ++mu) D.ucon[mu] = ucon_dr[mu] * (D.ucon[0] / ucon_dr[0]) + (vpar * Bcon[mu] * D.ucon[0] / B_mag);
+        B.lower(D.ucon, D.ucov, j, i, center);
+        P[2] = D.ucon[1] + (beta[1] * D.ucon[0]);
+        P[3] = D.ucon[2] + (beta[2] * D.ucon[0]);
+        P[4] = D.ucon[3] + (beta[3] * D.ucon[0]);
+        return 0;
+    } else {
+        // normal observer frame: floors_functions.hpp:254-289
+        const double rho_add = kmax(0., rhoflr_max - P[0]);
+        const double u_add   = kmax(0., uflr_max - P[1]);
+        double Pa[8] = {rho_add, u_add, 0., 0., 0., 0., 0., 0.};
+        FourVectors D;
+        calc_4vecs(B, Pa, true, j, i, center, D);
+        const double gdet = B.Gdet(center, j, i);
+        const double rho_ut = rho_add * D.ucon[0] * gdet;
+        double mhd[4];
+        calc_tensor(rho_add, u_add, (gam - 1) * u_add, D, 0, true, mhd);
+        double T[4];
+        T[0] = mhd[0] * gdet + rho_ut;
+        for (int v = 0; v < 3; ++v) T[1 + v] = mhd[1 + v] * gdet;
+        P[0] += rho_add;
+        P[1] += u_add;
+        U[0] += rho_ut;
+        U[1] += T[0];
+        U[2] += T[1];
+        U[3] += T[2];
+        U[4] += T[3];
+        return u_to_p_onedw(B, U, P, j, i, center, 8, 1e-8);
+    }
+}
+
+// ---------------------------------------------------------------- state helpers
+struct Fields {
+    std::vector<double> F[3], cmax[3], cmin[3];
+    void alloc(const Block& B)
+    {
+        for (int d = 0; d < 3; ++d) {
+            F[d].assign((size_t)B.nv*B.N, 0.);
+            cmax[d].assign(B.N, 0.);
+            cmin[d].assign(B.N, 0.);
+        }
+    }
+};
+
+static inline void load_cell(const Block& B, const double* A, size_t c, double* out)
+{
+    for (int p = 0; p < B.nv; ++p) out[p] = A[(size_t)p*B.N + c];
+}
+static inline void store_cell(const Block& B, double* A, size_t c, const double* in, int nvars)
+{
+    for (int p = 0; p < nvars; ++p) A[(size_t)p*B.N + c] = in[p];
+}
+
+// Inverter::BlockUtoP + B_FluxCT::BlockUtoP over a range (inverter.cpp:131-182, b_flux_ct.cpp:196-217)
+static void block_utop(const Block& B, const double* U, double* P, double* pflag, double* fflag,
+                       int ks, int ke, int js, int je, int is, int ie)
+{
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = ks; k <= ke; ++k) for (int j = js; j <= je; ++j) for (int i = is; i <= ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Uc[8], Pc[8];
+        load_cell(B, U, c, Uc);
+        load_cell(B, P, c, Pc);
+        const int pf = u_to_p_onedw(B, Uc, Pc, j, i, center, B.c.iter_max, B.c.err_tol);
+        store_cell(B, P, c, Pc, 5);
+        pflag[c] = pf % 32;
+        fflag[c] = (pf / 32) * 32;
+    }
+    if (B.nv > 5) {
+        for (int v = 0; v < 3; ++v)
+        for (int k = ks; k <= ke; ++k) for (int j = js; j <= je; ++j) for (int i = is; i <= ie; ++i) {
+            const size_t c = B.id(k, j, i);
+            P[(size_t)(5 + v)*B.N + c] = U[(size_t)(5 + v)*B.N + c] / B.Gdet(center, j, i);
+        }
+    }
+}
+
+// floors.cpp:215-229 and floors_impl.hpp:45-128
+static void apply_grmhd_floors(const Block& B, double* P, double* U, double* pflag, double* fflag,
+                               int ks, int ke, int js, int je, int is, int ie)
+{
+    const size_t N = B.N;
+    std::vector<double> rhofl(N, 0.), ufl(N, 0.);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = ks; k <= ke; ++k) for (int j = js; j <= je; ++j) for (int i = is; i <= ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pc[8];
+        load_cell(B, P, c, Pc);
+        double rf, uf;
+        const int ff = determine_floors(B, Pc, j, i, rf, uf);
+        fflag[c] = (int)fflag[c] | ff;
+        rhofl[c] = rf; ufl[c] = uf;
+    }
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = ks; k <= ke; ++k) for (int j = js; j <= je; ++j) for (int i = is; i <= ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        if ((int)fflag[c]) {
+            double Pc[8], Uc[8];
+            load_cell(B, P, c, Pc);
+            load_cell(B, U, c, Uc);
+            const int pf = apply_floors_frame(B, Pc, Uc, j, i, rhofl[c], ufl[c]);
+            if (pf) pflag[c] = pf;
+            apply_ceilings(B, Pc, j, i);
+            store_cell(B, P, c, Pc, 5);
+            store_cell(B, U, c, Uc, 5);
+            p_to_u_mhd_cell(B, P, U, c, j, i);
+        }
+    }
+}
+
+// fixup.cpp:47-156.  Neighbours are read inside [ks..ke] x [js..je] x [is..ie] (the physical range).
+static void fix_utop(const Block& B, double* P, double* U, const double* pflag,
+                     int ks, int ke, int js, int je, int is, int ie)
+{
+    if (!B.c.fix_average_neighbors && !B.c.fix_atmosphere) return;
+    const size_t N = B.N;
+    for (int k = ks; k <= ke; ++k) for (int j = js; j <= je; ++j) for (int i = is; i <= ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        if ((int)pflag[c] > 0) {
+            double wsum = 0., sum[5] = {0.};
+            if (B.c.fix_average_neighbors) {
+                for (int n = -1; n <= 1; n++) for (int m = -1; m <= 1; m++) for (int l = -1; l <= 1; l++) {
+                    const int ii = i + l, jj = j + m, kk = k + n;
+                    if (ii < is || ii > ie || jj < js || jj > je || kk < ks || kk > ke) continue;
+                    const size_t cn = B.id(kk, jj, ii);
+                    if (!((int)pflag[cn] > 0)) {
+                        const double w = 1./(std::abs(l) + std::abs(m) + std::abs(n) + 1);
+                        wsum += w;
+                        for (int p = 0; p < 5; ++p) sum[p] += w * P[(size_t)p*N + cn];
+                    }
+                }
+            }
+            for (int p = 0; p < 5; ++p) P[(size_t)p*N + c] = (wsum < 1.e-10) ? 0. : sum[p]/wsum;
+        }
+    }
+    for (int k = ks; k <= ke; ++k) for (int j = js; j <= je; ++j) for (int i = is; i <= ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        if ((int)pflag[c] > 0) {
+            double Pc[8];
+            load_cell(B, P, c, Pc);
+            // floors_functions.hpp:356-367 (global form) -- identical arithmetic to the local form
+            apply_geo_floors_local(B, Pc, j, i);
+            store_cell(B, P, c, Pc, 5);
+            // grmhd_functions.hpp:325-353 (GRMHD::p_to_u): rho, u, uvec only
+            p_to_u_mhd_cell(B, P, U, c, j, i);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- boundaries
+// Periodic: Parthenon internal sync.  Outflow/reflecting: Parthenon BoundaryFunction (unvendored):
+// outflow copies the last interior zone; reflecting mirrors about the face and flips the sign of
+// the vector component normal to it.  KHARMA applies these to the fluid primitives (rho, u, uvec)
+// and the conserved field B_U, then sets B_P = B_U/gdet (boundaries.cpp:369-589).
+static void periodic_fill(const Block& B, double* A, int nvars, int dir)
+{
+    for (int p = 0; p < nvars; ++p) {
+        double* q = A + (size_t)p*B.N;
+        for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+            int ii = i, jj = j, kk = k;
+            if (dir == 1) { if (i >= B.is && i <= B.ie) continue; ii = (i < B.is) ? i + B.c.nx1 : i - B.c.nx1; }
+            if (dir == 2) { if (j >= B.js && j <= B.je) continue; jj = (j < B.js) ? j + B.c.nx2 : j - B.c.nx2; }
+            if (dir == 3) { if (k >= B.ks && k <= B.ke) continue; kk = (k < B.ks) ? k + B.c.nx3 : k - B.c.nx3; }
+            q[B.id(k, j, i)] = q[B.id(kk, jj, ii)];
+        }
+    }
+}
+// boundaries.hpp:101-136
+static void check_inflow(const Block& B, double* P, size_t c, int j, int i, bool inner)
+{
+    double uvec[3], ucon[4];
+    for (int v = 0; v < 3; ++v) uvec[v] = P[(size_t)(2 + v)*B.N + c];
+    {
+        double Ptmp[8] = {0, 0, uvec[0], uvec[1], uvec[2], 0, 0, 0};
+        const double gamma = lorentz_calc(B, Ptmp, j, i, center);
+        const double alpha = 1. / std::sqrt(-B.Gcon(center, j, i, 0, 0));
+        ucon[0] = gamma / alpha;
+        for (int v = 0; v < 3; ++v) ucon[v+1] = uvec[v] - gamma * alpha * B.Gcon(center, j, i, 0, v+1);
+    }
+    if (((ucon[1] > 0.) && inner) || ((ucon[1] < 0.) && !inner)) {
+        double Ptmp[8] = {0, 0, uvec[0], uvec[1], uvec[2], 0, 0, 0};
+        double gamma = lorentz_calc(B, Ptmp, j, i, center);
+        for (int v = 0; v < 3; ++v) uvec[v] /= gamma;
+        const double alpha = 1. / std::sqrt(-B.Gcon(center, j, i, 0, 0));
+        const double beta1 = B.Gcon(center, j, i, 0, 1) * alpha * alpha;
+        uvec[0] = beta1 / alpha;
+        const double vsq = B.Gcov(center, j, i, 1, 1) * uvec[0] * uvec[0] +
+                           B.Gcov(center, j, i, 2, 2) * uvec[1] * uvec[1] +
+                           B.Gcov(center, j, i, 3, 3) * uvec[2] * uvec[2] +
+                           2. * (B.Gcov(center, j, i, 1, 2) * uvec[0] * uvec[1] +
+                                 B.Gcov(center, j, i, 1, 3) * uvec[0] * uvec[2] +
+                                 B.Gcov(center, j, i, 2, 3) * uvec[1] * uvec[2]);
+        // clip() result discarded in the reference (boundaries.hpp:129)
+        gamma = 1./std::sqrt(1. - vsq);
+        for (int v = 0; v < 3; ++v) uvec[v] *= gamma;
+        for (int v = 0; v < 3; ++v) P[(size_t)(2 + v)*B.N + c] = uvec[v];
+    }
+}
+// One physical face: P (fluid primitives, vars 0-4) and U_B (vars 5-7 of U)
+static void physical_face(const Block& B, double* P, double* U, int face)
+{
+    const int bdir = face / 2 + 1;
+    const bool binner = (face % 2) == 0;
+    const int type = B.c.bc[face];
+    const size_t N = B.N;
+    // boundary domain: ghost zones in bdir, all zones in the other directions
+    int i0 = 0, i1 = B.n1 - 1, j0 = 0, j1 = B.n2 - 1, k0 = 0, k1 = B.n3 - 1;
+    int ref, offset;
+    if (bdir == 1) { if (binner) { i0 = 0; i1 = B.is - 1; ref = B.is; } else { i0 = B.ie + 1; i1 = B.n1 - 1; ref = B.ie; } }
+    else if (bdir == 2) { if (binner) { j0 = 0; j1 = B.js - 1; ref = B.js; } else { j0 = B.je + 1; j1 = B.n2 - 1; ref = B.je; } }
+    else { if (binner) { k0 = 0; k1 = B.ks - 1; ref = B.ks; } else { k0 = B.ke + 1; k1 = B.n3 - 1; ref = B.ke; } }
+    offset = 2 * ref + (binner ? -1 : 1);
+    for (int k = k0; k <= k1; ++k) for (int j = j0; j <= j1; ++j) for (int i = i0; i <= i1; ++i) {
+        const size_t c = B.id(k, j, i);
+        int kk = k, jj = j, ii = i;
+        if (type == BC_OUTFLOW) {
+            if (bdir == 1) ii = ref; else if (bdir == 2) jj = ref; else kk = ref;
+        } else {
+            if (bdir == 1) ii = offset - i; else if (bdir == 2) jj = offset - j; else kk = offset - k;
+        }
+        const size_t s = B.id(kk, jj, ii);
+        for (int p = 0; p < 5; ++p) {
+            const bool flip = (type == BC_REFLECT) && (p == 1 + bdir);
+            P[(size_t)p*N + c] = (flip ? -1.0 : 1.0) * P[(size_t)p*N + s];
+        }
+        if (B.nv > 5)
+            for (int v = 0; v < 3; ++v) {
+                const bool flip = (type == BC_REFLECT) && (v == bdir - 1);
+                U[(size_t)(5 + v)*N + c] = (flip ? -1.0 : 1.0) * U[(size_t)(5 + v)*N + s];
+            }
+    }
+    const bool inflow = (face == 0 && B.c.check_inflow_inner_x1) || (face == 1 && B.c.check_inflow_outer_x1);
+    if (inflow)
+        for (int k = k0; k <= k1; ++k) for (int j = j0; j <= j1; ++j) for (int i = i0; i <= i1; ++i)
+            check_inflow(B, P, B.id(k, j, i), j, i, binner);
+}
+// Fill all ghost zones: physical faces in the order Parthenon applies them (x1, x2, then the
+// fix_corner re-application of inner x1: boundaries.cpp:538-559), then periodic directions.
+static void apply_boundaries(const Block& B, double* P, double* U)
+{
+    // periodic directions first, so physical faces see filled corners exactly as after a sync
+    for (int d = 1; d <= B.ndim; ++d)
+        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, B.nv, d); periodic_fill(B, U, B.nv, d); }
+    for (int face = 0; face < 2*B.ndim; ++face) {
+        if (B.c.bc[face] == BC_PERIODIC) continue;
+        physical_face(B, P, U, face);
+        if (face == 3 && B.c.fix_corner_inner && B.c.bc[0] != BC_PERIODIC) physical_face(B, P, U, 0);
+    }
+    for (int d = 1; d <= B.ndim; ++d)
+        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, B.nv, d); periodic_fill(B, U, B.nv, d); }
+    // B_P = B_U/gdet in the ghost zones (BoundaryUtoP of B_FluxCT)
+    if (B.nv > 5)
+        for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+            if (i >= B.is && i <= B.ie && j >= B.js && j <= B.je && k >= B.ks && k <= B.ke) continue;
+            const size_t c = B.id(k, j, i);
+            for (int v = 0; v < 3; ++v) P[(size_t)(5 + v)*B.N + c] = U[(size_t)(5 + v)*B.N + c] / B.Gdet(center, j, i);
+        }
+}
+
+// ---------------------------------------------------------------- timestep and diagnostics
+// grmhd.cpp:294-339 (minimum of the zone timestep over the interior, before cfl and clipping)
+static double min_ndt(const Block& B, const Fields& f)
+{
+    double m = std::numeric_limits<double>::max();
+#pragma omp parallel for collapse(2) reduction(min:m)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        const double ndt_zone = 1.0 / (1 / (B.c.dx1 / kmax(f.cmax[0][c], f.cmin[0][c])) +
+                                       1 / (B.c.dx2 / kmax(f.cmax[1][c], f.cmin[1][c])) +
+                                       1 / (B.c.dx3 * 1 / kmax(f.cmax[2][c], f.cmin[2][c])));
+        if (!std::isnan(ndt_zone) && (ndt_zone < m)) m = ndt_zone;
+    }
+    return m;
+}
+// b_flux_ct.cpp:566-607 and b_flux_ct_functions.hpp:52-75
+static double max_divb(const Block& B, const double* U, int avoid_inner, int avoid_outer)
+{
+    if (B.ndim < 2) return 0.;
+    const size_t N = B.N;
+    const double* B1 = U + 5*N; const double* B2 = U + 6*N; const double* B3 = U + 7*N;
+    const size_t sj = B.n1, sk = (size_t)B.n1*B.n2;
+    const bool do3 = B.ndim > 2;
+    double mx = 0.;
+    for (int k = B.ks; k <= B.ke + (B.ndim > 2); ++k)
+    for (int j = B.js; j <= B.je + 1; ++j)
+    for (int i = B.is + avoid_inner; i <= B.ie + !avoid_outer; ++i) {
+        const size_t c = B.id(k, j, i);
+        const double norm = do3 ? 0.25 : 0.5;
+        double term1 = B1[c] - B1[c-1] + B1[c-sj] - B1[c-sj-1];
+        double term2 = B2[c] - B2[c-sj] + B2[c-1] - B2[c-sj-1];
+        double term3 = 0.;
+        if (do3) {
+            term1 += B1[c-sk] + B1[c-sk-sj] - B1[c-sk-1] - B1[c-sk-sj-1];
+            term2 += B2[c-sk] + B2[c-sk-1] - B2[c-sk-sj] - B2[c-sk-sj-1];
+            term3 = B3[c] + B3[c-sj] + B3[c-1] + B3[c-sj-1] - B3[c-sk] - B3[c-sk-sj] - B3[c-sk-1] - B3[c-sk-sj-1];
+        }
+        const double d = std::fabs(norm*term1/B.c.dx1 + norm*term2/B.c.dx2 + norm*term3/B.c.dx3);
+        if (d > mx) mx = d;
+    }
+    return mx;
+}
+
+// ---------------------------------------------------------------- one RK2 stage
+// Parthenon "rk2" low-storage integrator (unvendored): gam0 = {0, 1/2}, gam1 = {1, 1/2}, beta = {1, 1/2}.
+static const double RK_GAM0[2] = {0.0, 0.5}, RK_GAM1[2] = {1.0, 0.5}, RK_BETA[2] = {1.0, 0.5};
+
+// Full-domain ghost refresh + lock-step P->U, shared by both drivers after the UtoP/floors/fixup region
+static void finish_stage(const Block& B, double* P, double* U)
+{
+    apply_boundaries(B, P, U);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i)
+        p_to_u_cell(B, P, U, B.id(k, j, i), j, i);      // Flux::MeshPtoU(entire), flux.cpp:317-322
+}
+
+// One stage.  P_s/U_s: stage-start state; U_0: step-start conserved state; outputs P_n/U_n.
+static void stage(const Block& B, Fields& f, int s, double dt,
+                  const double* P_s, const double* U_s, const double* U_0,
+                  double* P_n, double* U_n, double* pflag, double* fflag)
+{
+    const size_t N = B.N, NV = (size_t)B.nv*N;
+    // 1. fluxes (kharma_driver.cpp:203-290)
+    for (int d = 1; d <= B.ndim; ++d)
+        get_flux(B, d, P_s, f.F[d-1].data(), f.cmax[d-1].data(), f.cmin[d-1].data());
+    // 2. FixFlux: B_FluxCT then Boundaries (kharma_package.cpp:43-56; the order does not change results)
+    double* F[3] = {f.F[0].data(), f.F[1].data(), f.F[2].data()};
+    if (B.nv > 5) {
+        if (B.c.fix_polar_flux && B.C.spherical()) {
+            if (B.c.bc[2] != BC_PERIODIC) zero_boundary_flux_x2(B, F[0], F[1], F[2], true);
+            if (B.c.bc[3] != BC_PERIODIC) zero_boundary_flux_x2(B, F[0], F[1], F[2], false);
+        }
+        flux_ct(B, F[0], F[1], F[2]);
+    }
+    boundaries_fix_flux(B, F);
+    // 3-4. dU/dt = -div F + geometric source (kharma_driver.hpp:208-231, flux.cpp:395-444)
+    std::vector<double> dudt(NV, 0.);
+    flux_divergence(B, F, dudt.data());
+    add_geo_source(B, P_s, dudt.data());
+    // 5. U_n = gam0 U_s + gam1 U_0 ; U_n = 1.0 U_n + (beta dt) dU/dt (Parthenon WeightedSumData, all zones)
+    const double g0 = RK_GAM0[s], g1 = RK_GAM1[s], bdt = RK_BETA[s] * dt;
+#pragma omp parallel for schedule(static)
+    for (size_t x = 0; x < NV; ++x) U_n[x] = g0 * U_s[x] + g1 * U_0[x];
+#pragma omp parallel for schedule(static)
+    for (size_t x = 0; x < NV; ++x) U_n[x] = 1.0 * U_n[x] + bdt * dudt[x];
+    // copy P_s -> P_n as the inversion guess (kharma_driver.cpp:380-384; fluid prims only)
+    std::memcpy(P_n, P_s, 5*N*sizeof(double));
+    // 7-8. UtoP and floors on the interior (periodic ghosts are exact images and are refreshed below)
+    for (size_t x = 0; x < N; ++x) { pflag[x] = 0; fflag[x] = 0; }
+    block_utop(B, U_n, P_n, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
+    if (B.c.floors_on) apply_grmhd_floors(B, P_n, U_n, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
+    // 9. FixUtoP over the physical range: periodic ghosts of P and pflag are needed as neighbours
+    {
+        int ks = B.ks, ke = B.ke, js = B.js, je = B.je, is = B.is, ie = B.ie;
+        for (int d = 1; d <= B.ndim; ++d)
+            if (B.c.bc[2*(d-1)] == BC_PERIODIC) {
+                periodic_fill(B, P_n, 5, d);
+                periodic_fill(B, pflag, 1, d);
+                if (d == 1) { is = 0; ie = B.n1 - 1; }
+                if (d == 2) { js = 0; je = B.n2 - 1; }
+                if (d == 3) { ks = 0; ke = B.n3 - 1; }
+            }
+        fix_utop(B, P_n, U_n, pflag, ks, ke, js, je, is, ie);
+    }
+    // 10-11. boundaries, then U = U(P) over the entire block
+    finish_stage(B, P_n, U_n);
+}
+
+struct Handle {
+    Block B;
+    Fields f;
+    std::vector<double> P1, U1, U0;
+};
+
+} // namespace orc
+
+// ======================================================================== C ABI (for the tests)
+using namespace orc;
+extern "C" {
+
+void* orc_create(const Config* cfg, const CoordSpec* cs)
+{
+    Handle* h = new Handle();
+    h->B.init(*cfg, *cs);
+    h->B.build_geometry();
+    h->f.alloc(h->B);
+    return h;
+}
+void orc_destroy(void* hp) { delete (Handle*)hp; }
+
+void orc_get_dims(void* hp, int32_t* dims)
+{
+    const Block& B = ((Handle*)hp)->B;
+    dims[0] = B.n1; dims[1] = B.n2; dims[2] = B.n3; dims[3] = B.ndim;
+    dims[4] = B.is; dims[5] = B.ie; dims[6] = B.js; dims[7] = B.je; dims[8] = B.ks; dims[9] = B.ke;
+}
+
+// Copy the geometry caches out (GRCoordinates layout) or replace them with caller tables.
+void orc_get_geometry(void* hp, double* gcov, double* gcon, double* gdet, double* gdet_conn, double* rcen)
+{
+    const Block& B = ((Handle*)hp)->B;
+    if (gcov) std::memcpy(gcov, B.gcov.data(), B.gcov.size()*sizeof(double));
+    if (gcon) std::memcpy(gcon, B.gcon.data(), B.gcon.size()*sizeof(double));
+    if (gdet) std::memcpy(gdet, B.gdet.data(), B.gdet.size()*sizeof(double));
+    if (gdet_conn) std::memcpy(gdet_conn, B.gdet_conn.data(), B.gdet_conn.size()*sizeof(double));
+    if (rcen) std::memcpy(rcen, B.rcen.data(), B.rcen.size()*sizeof(double));
+}
+void orc_set_geometry(void* hp, const double* gcov, const double* gcon, const double* gdet,
+                      const double* gdet_conn, const double* rcen)
+{
+    Block& B = ((Handle*)hp)->B;
+    if (gcov) std::memcpy(B.gcov.data(), gcov, B.gcov.size()*sizeof(double));
+    if (gcon) std::memcpy(B.gcon.data(), gcon, B.gcon.size()*sizeof(double));
+    if (gdet) std::memcpy(B.gdet.data(), gdet, B.gdet.size()*sizeof(double));
+    if (gdet_conn) std::memcpy(B.gdet_conn.data(), gdet_conn, B.gdet_conn.size()*sizeof(double));
+    if (rcen) std::memcpy(B.rcen.data(), rcen, B.rcen.size()*sizeof(double));
+}
+
+// Flux::GetFlux<recon, dir> on the consumer range; F is [nvar][cells]
+void orc_get_flux(void* hp, int dir, const double* P, double* F, double* cmax, double* cmin)
+{
+    Handle* h = (Handle*)hp;
+    get_flux(h->B, dir, P, F, cmax, cmin);
+}
+
+// B_FluxCT::FixFlux + KBoundaries::FixFlux on raw fluxes (in place)
+void orc_fix_flux(void* hp, double* F1, double* F2, double* F3)
+{
+    Handle* h = (Handle*)hp;
+    const Block& B = h->B;
+    double* F[3] = {F1, F2, F3};
+    if (B.nv > 5) {
+        if (B.c.fix_polar_flux && B.C.spherical()) {
+            if (B.c.bc[2] != BC_PERIODIC) zero_boundary_flux_x2(B, F1, F2, F3, true);
+            if (B.c.bc[3] != BC_PERIODIC) zero_boundary_flux_x2(B, F1, F2, F3, false);
+        }
+        flux_ct(B, F1, F2, F3);
+    }
+    boundaries_fix_flux(B, F);
+}
+
+// Inverter::BlockUtoP (+ B) over the interior
+void orc_utop(void* hp, const double* U, double* P, double* pflag, double* fflag)
+{
+    const Block& B = ((Handle*)hp)->B;
+    block_utop(B, U, P, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
+}
+// Floors::ApplyGRMHDFloors over the interior
+void orc_floors(void* hp, double* P, double* U, double* pflag, double* fflag)
+{
+    const Block& B = ((Handle*)hp)->B;
+    apply_grmhd_floors(B, P, U, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
+}
+// Flux::MeshPtoU over the entire block
+void orc_ptou(void* hp, const double* P, double* U)
+{
+    const Block& B = ((Handle*)hp)->B;
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i)
+        p_to_u_cell(B, P, U, B.id(k, j, i), j, i);
+}
+void orc_boundaries(void* hp, double* P, double* U)
+{
+    apply_boundaries(((Handle*)hp)->B, P, U);
+}
+
+// One full RK2 step (both stages).  Returns the next dt per SetGlobalTimeStep + EstimateTimestep
+// (kharma_driver.cpp:439-460, grmhd.cpp:294-339), and the raw minimum zone timestep.
+void orc_step(void* hp, double* P, double* U, double* pflag, double* fflag, double dt,
+              double* dt_next, double* min_ndt_out)
+{
+    Handle* h = (Handle*)hp;
+    const Block& B = h->B;
+    const size_t NV = (size_t)B.nv*B.N;
+    h->P1.assign(NV, 0.); h->U1.assign(NV, 0.); h->U0.assign(U, U + NV);
+    // the B primitives of the new state are always rebuilt from B_U; seed the fluid prims copy
+    std::memcpy(h->P1.data(), P, NV*sizeof(double));
+    stage(B, h->f, 0, dt, P, h->U0.data(), h->U0.data(), h->P1.data(), h->U1.data(), pflag, fflag);
+    stage(B, h->f, 1, dt, h->P1.data(), h->U1.data(), h->U0.data(), P, U, pflag, fflag);
+    const double mn = min_ndt(B, h->f);
+    if (min_ndt_out) *min_ndt_out = mn;
+    if (dt_next) {
+        // EstimateTimestep: clip(cfl*min, dt_min, max_dt_increase*dt_last); SetGlobalTimeStep: min(2 dt, that)
+        const double ndt = clip(mn * B.c.cfl, B.c.dt_min, B.c.max_dt_increase * dt);
+        *dt_next = std::min(2.0 * dt, ndt);
+    }
+}
+
+double orc_max_divb(void* hp, const double* U, int avoid_inner, int avoid_outer)
+{
+    return max_divb(((Handle*)hp)->B, U, avoid_inner, avoid_outer);
+}
+
+// Single-cell inversion, for golden/unit tests: U and P are nvar-long arrays at (j,i) of the centre
+int orc_utop_cell(void* hp, int j, int i, const double* U, double* P)
+{
+    const Block& B = ((Handle*)hp)->B;
+    return u_to_p_onedw(B, U, P, j, i, center, B.c.iter_max, B.c.err_tol);
+}
+
+} // extern "C"

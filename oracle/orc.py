@@ -1,0 +1,219 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liborc.so).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the CPU-baseline leg of
+bench.py as the checker.  Builds the library with `make -C oracle` on first use.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liborc.so")
+
+
+class Prescription(C.Structure):
+    _fields_ = [
+        ("rho_min_const", C.c_double), ("u_min_const", C.c_double),
+        ("rho_min_geom", C.c_double), ("u_min_geom", C.c_double), ("r_char", C.c_double),
+        ("bsq_over_rho_max", C.c_double), ("bsq_over_u_max", C.c_double), ("u_over_rho_max", C.c_double),
+        ("ktot_max", C.c_double), ("gamma_max", C.c_double),
+        ("use_r_char", C.c_int32), ("temp_adjust_u", C.c_int32), ("adjust_k", C.c_int32),
+        ("radius_dependent_floors", C.c_int32),
+        ("floors_switch_r", C.c_double),
+    ]
+
+
+class CoordSpec(C.Structure):
+    _fields_ = [("base", C.c_int32), ("transform", C.c_int32),
+                ("a", C.c_double), ("hslope", C.c_double), ("mks_smooth", C.c_double),
+                ("poly_xt", C.c_double), ("poly_alpha", C.c_double), ("startx1", C.c_double)]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("nx1", C.c_int32), ("nx2", C.c_int32), ("nx3", C.c_int32), ("ng", C.c_int32),
+        ("x1min", C.c_double), ("x2min", C.c_double), ("x3min", C.c_double),
+        ("dx1", C.c_double), ("dx2", C.c_double), ("dx3", C.c_double),
+        ("gam", C.c_double),
+        ("recon", C.c_int32), ("riemann", C.c_int32),
+        ("nvar", C.c_int32),
+        ("driver", C.c_int32),
+        ("bc", C.c_int32 * 6),
+        ("check_inflow_inner_x1", C.c_int32), ("check_inflow_outer_x1", C.c_int32),
+        ("zero_polar_flux", C.c_int32), ("fix_polar_flux", C.c_int32), ("fix_corner_inner", C.c_int32),
+        ("floors_on", C.c_int32), ("floor_frame", C.c_int32), ("recon_floors", C.c_int32),
+        ("iter_max", C.c_int32), ("err_tol", C.c_double),
+        ("fix_average_neighbors", C.c_int32), ("fix_atmosphere", C.c_int32),
+        ("cfl", C.c_double), ("dt_min", C.c_double), ("max_dt_increase", C.c_double),
+        ("floors", Prescription),
+    ]
+
+
+RECON = {"donor_cell": 0, "linear_mc": 1, "weno5": 2, "ppm": 3}
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
+FRAME = {"fluid": 0, "normal": 1, "drift": 2}
+BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
+TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    src = os.path.join(HERE, "khb_oracle.cpp")
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    lib = C.CDLL(LIB)
+    P = C.c_void_p
+    lib.orc_create.restype = P
+    lib.orc_create.argtypes = [C.POINTER(Config), C.POINTER(CoordSpec)]
+    lib.orc_destroy.argtypes = [P]
+    lib.orc_get_dims.argtypes = [P, P]
+    lib.orc_get_geometry.argtypes = [P, P, P, P, P, P]
+    lib.orc_set_geometry.argtypes = [P, P, P, P, P, P]
+    lib.orc_get_flux.argtypes = [P, C.c_int, P, P, P, P]
+    lib.orc_fix_flux.argtypes = [P, P, P, P]
+    lib.orc_utop.argtypes = [P, P, P, P, P]
+    lib.orc_floors.argtypes = [P, P, P, P, P]
+    lib.orc_ptou.argtypes = [P, P, P]
+    lib.orc_boundaries.argtypes = [P, P, P]
+    lib.orc_step.argtypes = [P, P, P, P, P, C.c_double, P, P]
+    lib.orc_max_divb.restype = C.c_double
+    lib.orc_max_divb.argtypes = [P, P, C.c_int, C.c_int]
+    lib.orc_utop_cell.restype = C.c_int
+    lib.orc_utop_cell.argtypes = [P, C.c_int, C.c_int, P, P]
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    assert a.flags["C_CONTIGUOUS"] and a.dtype == np.float64
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def config_from_spec(spec):
+    c = Config()
+    c.nx1, c.nx2, c.nx3, c.ng = spec.nx1, spec.nx2, spec.nx3, spec.ng
+    c.x1min, c.x2min, c.x3min = spec.x1min, spec.x2min, spec.x3min
+    c.dx1, c.dx2, c.dx3 = spec.dx
+    c.gam = spec.gam
+    c.recon = RECON[spec.recon]
+    c.riemann = 1 if spec.riemann == "hlle" else 0
+    c.nvar = spec.nvar
+    c.driver = 0 if spec.driver == "simple" else 1
+    for x in range(6):
+        c.bc[x] = BC[spec.bc[x]]
+    c.check_inflow_inner_x1 = int(spec.check_inflow_inner_x1)
+    c.check_inflow_outer_x1 = int(spec.check_inflow_outer_x1)
+    c.zero_polar_flux = int(spec.zero_polar_flux)
+    c.fix_polar_flux = int(spec.fix_polar_flux)
+    c.fix_corner_inner = int(spec.fix_corner_inner)
+    c.floors_on = int(spec.floors_on)
+    c.floor_frame = FRAME[spec.floor_frame]
+    c.recon_floors = int(spec.recon_floors and spec.floors_on)
+    c.iter_max, c.err_tol = spec.iter_max, spec.err_tol
+    c.fix_average_neighbors = int(spec.fix_average_neighbors)
+    c.fix_atmosphere = int(spec.fix_atmosphere)
+    c.cfl, c.dt_min, c.max_dt_increase = spec.cfl, spec.dt_min, spec.max_dt_increase
+    for name, _ in Prescription._fields_:
+        setattr(c.floors, name, type(getattr(c.floors, name))(getattr(spec.floors, name)))
+    return c
+
+
+def coords_from_spec(spec):
+    s = CoordSpec()
+    s.base, s.transform = BASE[spec.base], TRANSFORM[spec.transform]
+    s.a, s.hslope, s.mks_smooth = spec.a, spec.hslope, spec.mks_smooth
+    s.poly_xt, s.poly_alpha, s.startx1 = spec.poly_xt, spec.poly_alpha, spec.startx1
+    return s
+
+
+class Oracle:
+    """One block in the CPU restatement.  Arrays are numpy float64 (nvar, n3, n2, n1)."""
+
+    def __init__(self, spec):
+        self.lib = load()
+        self.spec = spec
+        self._cfg = config_from_spec(spec)
+        self._cs = coords_from_spec(spec)
+        self.h = self.lib.orc_create(C.byref(self._cfg), C.byref(self._cs))
+        self.shape = spec.shape
+        n3, n2, n1 = self.shape
+        self.N = n1 * n2 * n3
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.orc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def geometry(self):
+        n3, n2, n1 = self.shape
+        G1, G2 = n1 + 1, n2 + 1
+        g = {"gcov": np.zeros((7, G2, G1, 4, 4)), "gcon": np.zeros((7, G2, G1, 4, 4)),
+             "gdet": np.zeros((7, G2, G1)), "gdet_conn": np.zeros((n2, n1, 4, 4, 4)),
+             "r_center": np.zeros((n2, n1))}
+        self.lib.orc_get_geometry(self.h, _ptr(g["gcov"]), _ptr(g["gcon"]), _ptr(g["gdet"]),
+                                  _ptr(g["gdet_conn"]), _ptr(g["r_center"]))
+        return g
+
+    def set_geometry(self, g):
+        arrs = [np.ascontiguousarray(g[k], dtype=np.float64) for k in ("gcov", "gcon", "gdet", "gdet_conn", "r_center")]
+        self.lib.orc_set_geometry(self.h, *[_ptr(a) for a in arrs])
+        self._keep = arrs
+
+    def zeros(self):
+        return np.zeros((self.spec.nvar,) + self.shape)
+
+    def ptou(self, P):
+        U = self.zeros()
+        self.lib.orc_ptou(self.h, _ptr(P), _ptr(U))
+        return U
+
+    def boundaries(self, P, U):
+        self.lib.orc_boundaries(self.h, _ptr(P), _ptr(U))
+
+    def init_state(self, P):
+        """Same initialisation sequence as kharma_b200.block.Block.set_prims."""
+        P = np.ascontiguousarray(P, dtype=np.float64).copy()
+        U = self.ptou(P)
+        self.boundaries(P, U)
+        self.lib.orc_ptou(self.h, _ptr(P), _ptr(U))
+        return P, U
+
+    def get_flux(self, dir, P):
+        F = self.zeros()
+        cmax = np.zeros(self.shape)
+        cmin = np.zeros(self.shape)
+        self.lib.orc_get_flux(self.h, dir, _ptr(P), _ptr(F), _ptr(cmax), _ptr(cmin))
+        return F, cmax, cmin
+
+    def fix_flux(self, F1, F2, F3):
+        self.lib.orc_fix_flux(self.h, _ptr(F1), _ptr(F2), _ptr(F3))
+
+    def utop(self, U, P):
+        pflag = np.zeros(self.shape)
+        fflag = np.zeros(self.shape)
+        self.lib.orc_utop(self.h, _ptr(U), _ptr(P), _ptr(pflag), _ptr(fflag))
+        return pflag, fflag
+
+    def floors(self, P, U, pflag, fflag):
+        self.lib.orc_floors(self.h, _ptr(P), _ptr(U), _ptr(pflag), _ptr(fflag))
+
+    def step(self, P, U, dt):
+        """One RK2 step in place; returns (pflag, fflag, dt_next, min_ndt)."""
+        pflag = np.zeros(self.shape)
+        fflag = np.zeros(self.shape)
+        dtn = C.c_double()
+        mn = C.c_double()
+        self.lib.orc_step(self.h, _ptr(P), _ptr(U), _ptr(pflag), _ptr(fflag), dt, C.byref(dtn), C.byref(mn))
+        return pflag, fflag, dtn.value, mn.value
+
+    def max_divb(self, U, avoid_inner=False, avoid_outer=False):
+        return self.lib.orc_max_divb(self.h, _ptr(U), int(avoid_inner), int(avoid_outer))
