@@ -1,8 +1,13 @@
 """Build libkhb.so in-tree for sm_100a with nvcc.
 
-    python -m kharma_b200.build [--fmad=false]
+    python -m kharma_b200.build
 
-The library is a plain shared object (no torch extension); the Python layer binds it with ctypes.
+Translation units and their arithmetic flags:
+  khb_fp64.cu      FP64 path (fluxes, zone pass, ghost zones)      -fmad=false
+  khb_fp32.cu      FP32-flux form (fluxes, EMFs in FP32)           FMA contraction on
+  khb_api.cu       host side and C ABI
+  khb_geometry.cpp host construction of the geometry tables
+The library is a plain shared object; the Python layer binds it with ctypes.
 """
 import os
 import subprocess
@@ -11,34 +16,57 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libkhb.so")
-SOURCES = ["khb_api.cu", "khb_geometry.cpp"]
-HEADERS = ["khb_device.cuh", "khb_kernels.cuh", os.path.join("..", "..", "include", "khb.h")]
+OBJ = os.path.join(HERE, "lib", "obj")
+UNITS = {
+    "khb_fp64.cu": ["-fmad=false"],
+    "khb_fp32.cu": [],
+    "khb_api.cu": [],
+    "khb_geometry.cpp": [],
+}
+HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", os.path.join("..", "..", "include", "khb.h")]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 
-def nvcc_command(out=OUT, extra=()):
-    return ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-            "-Xcompiler", "-fPIC", "-shared", *extra, "-o", out] + [os.path.join(CSRC, s) for s in SOURCES]
+def _deps_mtime():
+    paths = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.abspath(__file__)]
+    return max(os.path.getmtime(p) for p in paths)
 
 
-def up_to_date(out=OUT):
-    if not os.path.exists(out):
-        return False
-    t = os.path.getmtime(out)
-    deps = SOURCES + HEADERS + ["build.py"]
-    return all(os.path.getmtime(os.path.join(CSRC if d != "build.py" else HERE, d)) <= t for d in deps)
-
-
-def build(force=False, extra=(), out=OUT, verbose=False):
-    os.makedirs(os.path.dirname(out), exist_ok=True)
-    if not force and not extra and up_to_date(out):
-        return out
-    cmd = nvcc_command(out, extra)
-    if verbose:
-        print(" ".join(cmd))
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libkhb")
+def build(force=False, extra=(), out=OUT, verbose=False, jobs=4):
+    os.makedirs(OBJ, exist_ok=True)
+    hdr_t = _deps_mtime()
+    procs = []
+    objs = []
+    for src, flags in UNITS.items():
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        stale = force or extra or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t)
+        if not stale:
+            continue
+        cmd = ["nvcc", *ARCH, *COMMON, *flags, *extra, "-c", s, "-o", o]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    failed = []
+    for src, p in procs:
+        log, _ = p.communicate()
+        if p.returncode != 0:
+            failed.append(src)
+            sys.stderr.write(log)
+        elif verbose and log.strip():
+            print(log)
+    if failed:
+        raise RuntimeError(f"nvcc failed on {failed}")
+    if procs or not os.path.exists(out):
+        cmd = ["nvcc", *ARCH, "-shared", "-o", out, *objs]
+        if verbose:
+            print(" ".join(cmd))
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("nvcc link failed")
     return out
 
 

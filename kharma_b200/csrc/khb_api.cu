@@ -1,5 +1,5 @@
 // khb_api.cu -- host side of libkhb: context, scratch, geometry upload, launches, C ABI.
-#include "khb_kernels.cuh"
+#include "khb_types.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -55,8 +55,6 @@ int fail(int code, const std::string& msg)
         if (e_ != cudaSuccess) return fail(KHB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
     } while (0)
 
-inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
-
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
 int check_fields(const khb_ctx* ctx, const khb_fields* f, const char* name)
@@ -68,66 +66,47 @@ int check_fields(const khb_ctx* ctx, const khb_fields* f, const char* name)
 }
 
 // ------------------------------------------------------------------ fluxes
-template <int RECON, int NV, typename R>
-void launch_flux_t(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
+int launch_flux(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
 {
     const Dims& d = ctx->d;
-    int lo[3], hi[3];
+    int lo[3], cnt[3];
     const int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
     for (int a = 0; a < 3; ++a) {
         const bool active = (a + 1) <= d.ndim;
-        if (a + 1 == dir) { lo[a] = s[a]; hi[a] = e[a] + 1; }
-        else if (active) { lo[a] = s[a] - 1; hi[a] = e[a] + 1; }
-        else { lo[a] = s[a]; hi[a] = e[a]; }
+        int hi;
+        if (a + 1 == dir) { lo[a] = s[a]; hi = e[a] + 1; }
+        else if (active) { lo[a] = s[a] - 1; hi = e[a] + 1; }
+        else { lo[a] = s[a]; hi = e[a]; }
+        cnt[a] = hi - lo[a] + 1;
     }
-    const int ci = hi[0] - lo[0] + 1, cj = hi[1] - lo[1] + 1, ck = hi[2] - lo[2] + 1;
-    const long long total = (long long)ci*cj*ck;
-    k_flux<RECON, NV, R, R><<<blocks_for(total, 128), 128, 0, st>>>(
-        d, ctx->g, ctx->ph, P, (R*)ctx->F[dir-1], (R*)ctx->ctop[dir-1], dir, lo[0], lo[1], lo[2], ci, cj, total);
-}
-
-template <int NV, typename R>
-void launch_flux_r(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
-{
-    switch (ctx->cfg.recon) {
-    case KHB_RECON_DONOR_CELL: launch_flux_t<RECON_DONOR, NV, R>(ctx, dir, P, st); break;
-    case KHB_RECON_LINEAR_MC:  launch_flux_t<RECON_MC, NV, R>(ctx, dir, P, st); break;
-    case KHB_RECON_WENO5:      launch_flux_t<RECON_WENO5, NV, R>(ctx, dir, P, st); break;
-    default:                   launch_flux_t<RECON_PPM, NV, R>(ctx, dir, P, st); break;
-    }
-}
-
-int launch_flux(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
-{
-    if (ctx->nv == 8) {
-        if (ctx->fp32) launch_flux_r<8, float>(ctx, dir, P, st); else launch_flux_r<8, double>(ctx, dir, P, st);
-    } else {
-        if (ctx->fp32) launch_flux_r<5, float>(ctx, dir, P, st); else launch_flux_r<5, double>(ctx, dir, P, st);
-    }
+    if (ctx->fp32)
+        Launch<float>::flux(ctx->cfg.recon, ctx->nv, dir, d, ctx->g, ctx->ph, P, (float*)ctx->F[dir-1],
+                            (float*)ctx->ctop[dir-1], lo, cnt, st);
+    else
+        Launch<double>::flux(ctx->cfg.recon, ctx->nv, dir, d, ctx->g, ctx->ph, P, (double*)ctx->F[dir-1],
+                             (double*)ctx->ctop[dir-1], lo, cnt, st);
     KHB_LAUNCHED(ctx);
     return KHB_OK;
 }
 
-template <int NV, typename FT>
+template <typename FT>
 int launch_fix_flux_t(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
 {
     const Dims& d = ctx->d;
     FT* F1 = (FT*)ctx->F[0]; FT* F2 = (FT*)ctx->F[1]; FT* F3 = (FT*)ctx->F[2];
-    if (d.ndim >= 2 && (ph.zero_polar_flux || (NV > 5 && ph.fix_polar_flux))) {
-        const int ni = d.ie - d.is + 3, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+    if (d.ndim >= 2 && (ph.zero_polar_flux || (ctx->nv > 5 && ph.fix_polar_flux))) {
         for (int face = 2; face <= 3; ++face) {
             if (d.bc[face] == KHB_BC_PERIODIC) continue;
-            k_fix_flux_x2<NV, FT><<<blocks_for((long long)ni*nk, 128), 128, 0, st>>>(d, ph, F1, F2, F3, face == 2);
+            Launch<FT>::fix_flux_x2(ctx->nv, d, ph, F1, F2, F3, face == 2, st);
             KHB_LAUNCHED(ctx);
         }
     }
-    const int nj = (d.ndim > 1) ? d.je - d.js + 3 : 1, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
     if (ph.check_inflow_in && d.bc[0] != KHB_BC_PERIODIC) {
-        k_fix_flux_x1<FT><<<blocks_for((long long)nj*nk, 128), 128, 0, st>>>(d, F1, 1);
+        Launch<FT>::fix_flux_x1(d, F1, 1, st);
         KHB_LAUNCHED(ctx);
     }
     if (ph.check_inflow_out && d.bc[1] != KHB_BC_PERIODIC) {
-        k_fix_flux_x1<FT><<<blocks_for((long long)nj*nk, 128), 128, 0, st>>>(d, F1, 0);
+        Launch<FT>::fix_flux_x1(d, F1, 0, st);
         KHB_LAUNCHED(ctx);
     }
     return KHB_OK;
@@ -135,8 +114,7 @@ int launch_fix_flux_t(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
 
 int launch_fix_flux(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
 {
-    if (ctx->nv == 8) return ctx->fp32 ? launch_fix_flux_t<8, float>(ctx, ph, st) : launch_fix_flux_t<8, double>(ctx, ph, st);
-    return ctx->fp32 ? launch_fix_flux_t<5, float>(ctx, ph, st) : launch_fix_flux_t<5, double>(ctx, ph, st);
+    return ctx->fp32 ? launch_fix_flux_t<float>(ctx, ph, st) : launch_fix_flux_t<double>(ctx, ph, st);
 }
 
 // ------------------------------------------------------------------ zone pass
@@ -148,10 +126,9 @@ struct ZoneCall {
     int mode;
 };
 
-template <int NV, typename FT>
+template <typename FT>
 void launch_zone_t(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
 {
-    const Dims& d = ctx->d;
     ZoneArgs<FT> a;
     a.Ps = zc.Ps; a.Us = zc.Us; a.U0 = zc.U0; a.Pout = zc.Pout; a.Uout = zc.Uout;
     for (int x = 0; x < 3; ++x) { a.F[x] = (const FT*)ctx->F[x]; a.ctop[x] = (const FT*)ctx->ctop[x]; }
@@ -161,14 +138,12 @@ void launch_zone_t(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
     a.fail_count = ctx->fail_count;
     a.fail_list = ctx->fail_list;
     a.mode = zc.mode;
-    const long long total = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
-    k_zone<NV, FT><<<blocks_for(total, 128), 128, 0, st>>>(d, ctx->g, ctx->ph, a);
+    Launch<FT>::zone(ctx->nv, ctx->d, ctx->g, ctx->ph, a, st);
 }
 
 int launch_zone(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
 {
-    if (ctx->nv == 8) { if (ctx->fp32) launch_zone_t<8, float>(ctx, zc, st); else launch_zone_t<8, double>(ctx, zc, st); }
-    else              { if (ctx->fp32) launch_zone_t<5, float>(ctx, zc, st); else launch_zone_t<5, double>(ctx, zc, st); }
+    if (ctx->fp32) launch_zone_t<float>(ctx, zc, st); else launch_zone_t<double>(ctx, zc, st);
     KHB_LAUNCHED(ctx);
     return KHB_OK;
 }
@@ -177,43 +152,38 @@ int launch_zone(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
 int launch_fixup(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, const int32_t* pflag, cudaStream_t st)
 {
     if (!ctx->ph.fix_avg && !ctx->ph.fix_atmo) return KHB_OK;
-    const unsigned nb = 4 * 148;
-    if (ctx->nv == 8) k_fixup<8><<<nb, 128, 0, st>>>(ctx->d, ctx->g, ctx->ph, P, U, pflag, ctx->fail_count, ctx->fail_list);
-    else              k_fixup<5><<<nb, 128, 0, st>>>(ctx->d, ctx->g, ctx->ph, P, U, pflag, ctx->fail_count, ctx->fail_list);
+    LaunchCommon::fixup(ctx->nv, ctx->d, ctx->g, ctx->ph, P, U, pflag, ctx->fail_count, ctx->fail_list, st);
     KHB_LAUNCHED(ctx);
     return KHB_OK;
 }
 
-template <int NV>
-int launch_boundaries_t(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
+int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
 {
     const Dims& d = ctx->d;
-    const Phys& ph = ctx->ph;
+    const int nv = ctx->nv;
     const int cnt_k = d.ke - d.ks + 1;
     bool physical = false;
     // X1 faces over the interior j range, then X2 faces over all i, then the corner fix
     for (int face = 0; face < 2; ++face) {
         if (d.bc[face] == KHB_BC_PERIODIC) continue;
         physical = true;
-        const int cnt_j = d.je - d.js + 1;
-        k_bc<NV><<<blocks_for((long long)d.is*cnt_j*cnt_k, 128), 128, 0, st>>>(d, ctx->g, ph, P, U, face, d.js, cnt_j, d.ks, cnt_k);
+        LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, d.js, d.je - d.js + 1, d.ks, cnt_k, st);
         KHB_LAUNCHED(ctx);
     }
     if (d.ndim >= 2) {
         for (int face = 2; face < 4; ++face) {
             if (d.bc[face] == KHB_BC_PERIODIC) continue;
             physical = true;
-            k_bc<NV><<<blocks_for((long long)d.js*d.n1*cnt_k, 128), 128, 0, st>>>(d, ctx->g, ph, P, U, face, 0, d.n1, d.ks, cnt_k);
+            LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, 0, d.n1, d.ks, cnt_k, st);
             KHB_LAUNCHED(ctx);
         }
         if (ctx->cfg.fix_corner_inner && d.bc[0] != KHB_BC_PERIODIC && d.bc[3] != KHB_BC_PERIODIC) {
-            k_bc<NV><<<blocks_for((long long)d.is*d.n2*cnt_k, 128), 128, 0, st>>>(d, ctx->g, ph, P, U, 0, 0, d.n2, d.ks, cnt_k);
+            LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, 0, 0, d.n2, d.ks, cnt_k, st);
             KHB_LAUNCHED(ctx);
         }
     }
     if (physical) {
-        const long long tot = (long long)d.n1*d.n2*cnt_k;
-        k_ghost_ptou<NV><<<blocks_for(tot, 128), 128, 0, st>>>(d, ctx->g, ph, P, U);
+        LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st);
         KHB_LAUNCHED(ctx);
     }
     int pmask = 0;
@@ -221,15 +191,10 @@ int launch_boundaries_t(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, 
     if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) pmask |= 2;
     if (d.ndim >= 3 && d.bc[4] == KHB_BC_PERIODIC) pmask |= 4;
     if (pmask) {
-        k_periodic<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, P, U, pmask);
+        LaunchCommon::periodic(nv, d, P, U, pmask, st);
         KHB_LAUNCHED(ctx);
     }
     return KHB_OK;
-}
-
-int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
-{
-    return ctx->nv == 8 ? launch_boundaries_t<8>(ctx, P, U, st) : launch_boundaries_t<5>(ctx, P, U, st);
 }
 
 size_t ft_size(const khb_ctx* ctx) { return ctx->fp32 ? sizeof(float) : sizeof(double); }
@@ -436,17 +401,11 @@ int khb_flux_ct(khb_ctx* ctx, void* stream)
 {
     KHB_NEED_GEOM(ctx);
     if (ctx->nv < 8 || ctx->d.ndim < 2) return KHB_OK;
-    const Dims& d = ctx->d;
-    const long long tot = (long long)(d.ie - d.is + 2)*(d.je - d.js + 2)*((d.ndim > 2) ? d.ke - d.ks + 2 : 1);
-    if (ctx->fp32) {
-        k_emf<float><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (float*)ctx->F[0], (float*)ctx->F[1], (float*)ctx->F[2], (float*)ctx->emf);
-        KHB_LAUNCHED(ctx);
-        k_ct_apply<float><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (float*)ctx->F[0], (float*)ctx->F[1], (float*)ctx->F[2], (const float*)ctx->emf);
-    } else {
-        k_emf<double><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (double*)ctx->F[0], (double*)ctx->F[1], (double*)ctx->F[2], (double*)ctx->emf);
-        KHB_LAUNCHED(ctx);
-        k_ct_apply<double><<<blocks_for(tot, 128), 128, 0, S(stream)>>>(d, (double*)ctx->F[0], (double*)ctx->F[1], (double*)ctx->F[2], (const double*)ctx->emf);
-    }
+    if (ctx->fp32)
+        Launch<float>::flux_ct(ctx->d, (float*)ctx->F[0], (float*)ctx->F[1], (float*)ctx->F[2], (float*)ctx->emf, S(stream));
+    else
+        Launch<double>::flux_ct(ctx->d, (double*)ctx->F[0], (double*)ctx->F[1], (double*)ctx->F[2], (double*)ctx->emf, S(stream));
+    ctx->launches++;
     KHB_LAUNCHED(ctx);
     // zero polar fluxes again after the rewrite (KBoundaries::FixFlux acts on the final fluxes)
     if (ctx->ph.zero_polar_flux) {
@@ -463,9 +422,9 @@ int khb_copy_flux(khb_ctx* ctx, int dir, const khb_fields* F_out, double* ctop_o
     if (!ctx || dir < 1 || dir > 3 || !F_out) return fail(KHB_ERR_ARG, "khb_copy_flux: bad argument");
     const long long N = ctx->d.N;
     if (ctx->fp32)
-        k_copy_flux<float><<<blocks_for(N, 256), 256, 0, S(stream)>>>(N, ctx->nv, (const float*)ctx->F[dir-1], (const float*)ctx->ctop[dir-1], *F_out, ctop_out);
+        Launch<float>::copy_flux(N, ctx->nv, (const float*)ctx->F[dir-1], (const float*)ctx->ctop[dir-1], *F_out, ctop_out, S(stream));
     else
-        k_copy_flux<double><<<blocks_for(N, 256), 256, 0, S(stream)>>>(N, ctx->nv, (const double*)ctx->F[dir-1], (const double*)ctx->ctop[dir-1], *F_out, ctop_out);
+        Launch<double>::copy_flux(N, ctx->nv, (const double*)ctx->F[dir-1], (const double*)ctx->ctop[dir-1], *F_out, ctop_out, S(stream));
     KHB_LAUNCHED(ctx);
     return KHB_OK;
 }
@@ -543,9 +502,7 @@ int khb_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* strea
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
-    const long long N = ctx->d.N;
-    if (ctx->nv == 8) k_ptou<8><<<blocks_for(N, 128), 128, 0, S(stream)>>>(ctx->d, ctx->g, ctx->ph, *P, *U);
-    else              k_ptou<5><<<blocks_for(N, 128), 128, 0, S(stream)>>>(ctx->d, ctx->g, ctx->ph, *P, *U);
+    LaunchCommon::ptou(ctx->nv, ctx->d, ctx->g, ctx->ph, *P, *U, S(stream));
     KHB_LAUNCHED(ctx);
     return KHB_OK;
 }
@@ -624,8 +581,7 @@ int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void*
     const int avoid_in = d.bc[0] != KHB_BC_PERIODIC, avoid_out = d.bc[1] != KHB_BC_PERIODIC;
     const int i_lo = d.is + avoid_in, i_hi = d.ie + !avoid_out;
     KHB_CUDA(cudaMemsetAsync(ctx->words + 1, 0, sizeof(unsigned long long), S(stream)));
-    const long long tot = (long long)(i_hi - i_lo + 1)*(d.je - d.js + 2)*((d.ndim > 2) ? d.ke - d.ks + 2 : 1);
-    k_divb<<<blocks_for(tot, 256), 256, 0, S(stream)>>>(d, ctx->ph, *U, i_lo, i_hi, ctx->words + 1);
+    LaunchCommon::divb(d, ctx->ph, *U, i_lo, i_hi, ctx->words + 1, S(stream));
     KHB_LAUNCHED(ctx);
     unsigned long long bits = 0;
     KHB_CUDA(cudaMemcpyAsync(&bits, ctx->words + 1, sizeof(bits), cudaMemcpyDeviceToHost, S(stream)));

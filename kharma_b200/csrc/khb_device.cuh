@@ -10,6 +10,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "khb_types.cuh"
+
 namespace khb {
 
 // Kokkos::max/min semantics, as used through m::max/m::min in the reference
@@ -379,16 +381,6 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
 }
 
 // ------------------------------------------------------------------ floors (FP64)
-// Floors::Prescription (floors.hpp:100-117); same layout as khb_floors
-struct Prescription {
-    double rho_min_const, u_min_const;
-    double rho_min_geom, u_min_geom, r_char;
-    double bsq_over_rho_max, bsq_over_u_max, u_over_rho_max;
-    double ktot_max, gamma_max;
-    int32_t use_r_char, temp_adjust_u, adjust_k, radius_dependent_floors;
-    double floors_switch_r;
-};
-
 // FFlag bits, floors.hpp:52-70
 enum { FF_GEOM_RHO = 32, FF_GEOM_U = 64, FF_B_RHO = 128, FF_B_U = 256, FF_TEMP = 512, FF_GAMMA = 1024,
        FF_KTOT = 2048, FF_GEOM_RHO_FLUX = 4096, FF_GEOM_U_FLUX = 8192 };

@@ -1,4 +1,4 @@
-// khb_kernels.cu -- sm_100a kernels and the C ABI of libkhb (see include/khb.h).
+// khb_kernels.cuh -- sm_100a kernels of libkhb (host side in khb_api.cu, C ABI in include/khb.h).
 //
 // Per RK stage the work is:
 //   k_flux (x ndim)   reconstruction + prim_to_flux + vchar + LLF/HLLE at every face needed,
@@ -11,7 +11,7 @@
 //   k_bc_* / k_periodic  ghost zones
 // Every loop in device code is bounded; failures are reported through pflag, never by trapping.
 #include "khb_device.cuh"
-#include "../../include/khb.h"
+#include "khb_types.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -21,38 +21,6 @@
 #include <limits>
 
 namespace khb {
-
-struct Dims {
-    int n1, n2, n3, ndim;
-    int is, ie, js, je, ks, ke;
-    int nx1, nx2, nx3;
-    long long N;
-    long long sj, sk;
-    int bc[6];
-};
-
-struct DevGeom {
-    int G1, G2, n1;
-    long long gs;                          // component stride of the location tables, G1*G2
-    const double* gcov[4];                 // face1, face2, face3, centre: [16][G2][G1]
-    const double* gcon[4];
-    const double* gdet[4];                 // [G2][G1]
-    const float* gcov_f[3];                // FP32 copies of the face tables
-    const float* gcon_f[3];
-    const float* gdet_f[3];
-    const double* gdet_conn;               // [64][n2][n1], index (nu*4+lam)*4+mu as gdet_conn(nu,lam,mu)
-    const double* rcen;                    // [n2][n1]
-};
-
-struct Phys {
-    double gam;
-    int riemann, recon_floors, spherical, cart_minkowski;
-    int floors_on, frame, iter_max, fix_avg, fix_atmo;
-    double err_tol;
-    double dx1, dx2, dx3;
-    int zero_polar_flux, fix_polar_flux, check_inflow_in, check_inflow_out;
-    Prescription fl;
-};
 
 __device__ __forceinline__ void zone_kji(const Dims& d, long long c, int& k, int& j, int& i)
 {
@@ -98,11 +66,12 @@ template <> struct FaceTables<float> {
     static __device__ __forceinline__ const float* gdet(const DevGeom& g, int loc) { return g.gdet_f[loc]; }
 };
 
-template <int RECON, int NV, typename R, typename FT>
+template <int DIR, int RECON, int NV, typename R, typename FT>
 __global__ void __launch_bounds__(128)
 k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop,
-       int dir, int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, long long total)
+       int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, long long total)
 {
+    constexpr int dir = DIR;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     const int i = lo_i + (int)(t % cnt_i);
@@ -219,22 +188,6 @@ __global__ void k_fix_flux_x1(Dims d, FT* F1, int inner)
 }
 
 // ===================================================================================== zone pass
-enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST = 32 };
-
-template <typename FT>
-struct ZoneArgs {
-    khb_fields Ps, Us, U0, Pout, Uout;
-    const FT* F[3];
-    const FT* ctop[3];
-    int32_t* pflag;
-    int32_t* fflag;
-    double g0, g1, bdt;
-    unsigned long long* ndt_word;
-    int* fail_count;
-    int* fail_list;
-    int mode;
-};
-
 // Raw flux, as double
 template <typename FT>
 __device__ __forceinline__ double ldf(const FT* F, long long x) { return (double)__ldg(F + x); }
@@ -678,6 +631,7 @@ __global__ void k_copy_flux(long long N, int nv, const FT* F, const FT* ctop, kh
     if (ctop_out) ctop_out[t] = (double)ctop[t];
 }
 
+#ifdef KHB_COMMON_KERNELS
 // B_FluxCT::MaxDivB: corner divergence (b_flux_ct_functions.hpp:52-75), block max + atomicMax
 __global__ void k_divb(Dims d, Phys ph, khb_fields U, int i_lo, int i_hi, unsigned long long* word)
 {
@@ -713,5 +667,128 @@ __global__ void k_divb(Dims d, Phys ph, khb_fields U, int i_lo, int i_hi, unsign
         atomicMax(word, (unsigned long long)__double_as_longlong(m));
     }
 }
+
+
+#endif
+
+// ===================================================================================== launchers
+template <int DIR, int NV, typename FT>
+static void flux_dir_recon(int recon, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                           FT* F, FT* ctop, const int lo[3], const int cnt[3], cudaStream_t st)
+{
+    const long long total = (long long)cnt[0]*cnt[1]*cnt[2];
+    const unsigned nb = blocks_for(total, 128);
+    switch (recon) {
+    case RECON_DONOR: k_flux<DIR, RECON_DONOR, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
+    case RECON_MC:    k_flux<DIR, RECON_MC, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
+    case RECON_WENO5: k_flux<DIR, RECON_WENO5, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
+    default:          k_flux<DIR, RECON_PPM, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
+    }
+}
+
+template <int NV, typename FT>
+static void flux_nv(int recon, int dir, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                    FT* F, FT* ctop, const int lo[3], const int cnt[3], cudaStream_t st)
+{
+    if (dir == 1) flux_dir_recon<1, NV, FT>(recon, d, g, ph, P, F, ctop, lo, cnt, st);
+    else if (dir == 2) flux_dir_recon<2, NV, FT>(recon, d, g, ph, P, F, ctop, lo, cnt, st);
+    else flux_dir_recon<3, NV, FT>(recon, d, g, ph, P, F, ctop, lo, cnt, st);
+}
+
+template <typename FT>
+void Launch<FT>::flux(int recon, int nv, int dir, const Dims& d, const DevGeom& g, const Phys& ph,
+                      const khb_fields& P, FT* F, FT* ctop, const int lo[3], const int cnt[3], cudaStream_t st)
+{
+    if (nv == 8) flux_nv<8, FT>(recon, dir, d, g, ph, P, F, ctop, lo, cnt, st);
+    else flux_nv<5, FT>(recon, dir, d, g, ph, P, F, ctop, lo, cnt, st);
+}
+
+template <typename FT>
+void Launch<FT>::fix_flux_x2(int nv, const Dims& d, const Phys& ph, FT* F1, FT* F2, FT* F3, int inner, cudaStream_t st)
+{
+    const int ni = d.ie - d.is + 3, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+    const unsigned nb = blocks_for((long long)ni*nk, 128);
+    if (nv == 8) k_fix_flux_x2<8, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
+    else k_fix_flux_x2<5, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
+}
+
+template <typename FT>
+void Launch<FT>::fix_flux_x1(const Dims& d, FT* F1, int inner, cudaStream_t st)
+{
+    const int nj = (d.ndim > 1) ? d.je - d.js + 3 : 1, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+    k_fix_flux_x1<FT><<<blocks_for((long long)nj*nk, 128), 128, 0, st>>>(d, F1, inner);
+}
+
+template <typename FT>
+void Launch<FT>::zone(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a, cudaStream_t st)
+{
+    const long long total = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
+    const unsigned nb = blocks_for(total, 128);
+    if (nv == 8) k_zone<8, FT><<<nb, 128, 0, st>>>(d, g, ph, a);
+    else k_zone<5, FT><<<nb, 128, 0, st>>>(d, g, ph, a);
+}
+
+template <typename FT>
+void Launch<FT>::flux_ct(const Dims& d, FT* F1, FT* F2, FT* F3, FT* emf, cudaStream_t st)
+{
+    const long long tot = (long long)(d.ie - d.is + 2)*(d.je - d.js + 2)*((d.ndim > 2) ? d.ke - d.ks + 2 : 1);
+    k_emf<FT><<<blocks_for(tot, 128), 128, 0, st>>>(d, F1, F2, F3, emf);
+    k_ct_apply<FT><<<blocks_for(tot, 128), 128, 0, st>>>(d, F1, F2, F3, emf);
+}
+
+template <typename FT>
+void Launch<FT>::copy_flux(long long N, int nv, const FT* F, const FT* ctop, const khb_fields& out, double* ctop_out,
+                           cudaStream_t st)
+{
+    k_copy_flux<FT><<<blocks_for(N, 256), 256, 0, st>>>(N, nv, F, ctop, out, ctop_out);
+}
+
+#ifdef KHB_COMMON_KERNELS
+void LaunchCommon::fixup(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                         const khb_fields& U, const int32_t* pflag, const int* fail_count, const int* fail_list,
+                         cudaStream_t st)
+{
+    const unsigned nb = 4 * 148;
+    if (nv == 8) k_fixup<8><<<nb, 128, 0, st>>>(d, g, ph, P, U, pflag, fail_count, fail_list);
+    else k_fixup<5><<<nb, 128, 0, st>>>(d, g, ph, P, U, pflag, fail_count, fail_list);
+}
+
+void LaunchCommon::bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
+                      int face, int lo_a, int cnt_a, int lo_k, int cnt_k, cudaStream_t st)
+{
+    const int ng = (face < 2) ? d.is : d.js;
+    const unsigned nb = blocks_for((long long)ng*cnt_a*cnt_k, 128);
+    if (nv == 8) k_bc<8><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
+    else k_bc<5><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
+}
+
+void LaunchCommon::ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                              const khb_fields& U, cudaStream_t st)
+{
+    const long long tot = (long long)d.n1*d.n2*(d.ke - d.ks + 1);
+    if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U);
+    else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U);
+}
+
+void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st)
+{
+    if (nv == 8) k_periodic<8><<<blocks_for(d.N, 256), 256, 0, st>>>(d, P, U, pmask);
+    else k_periodic<5><<<blocks_for(d.N, 256), 256, 0, st>>>(d, P, U, pmask);
+}
+
+void LaunchCommon::ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                        const khb_fields& U, cudaStream_t st)
+{
+    if (nv == 8) k_ptou<8><<<blocks_for(d.N, 128), 128, 0, st>>>(d, g, ph, P, U);
+    else k_ptou<5><<<blocks_for(d.N, 128), 128, 0, st>>>(d, g, ph, P, U);
+}
+
+void LaunchCommon::divb(const Dims& d, const Phys& ph, const khb_fields& U, int i_lo, int i_hi,
+                        unsigned long long* word, cudaStream_t st)
+{
+    const long long tot = (long long)(i_hi - i_lo + 1)*(d.je - d.js + 2)*((d.ndim > 2) ? d.ke - d.ks + 2 : 1);
+    k_divb<<<blocks_for(tot, 256), 256, 0, st>>>(d, ph, U, i_lo, i_hi, word);
+}
+#endif
 
 } // namespace khb

@@ -1,0 +1,102 @@
+// khb_types.cuh -- plain structs shared by the host side (khb_api.cu) and the kernels, and the
+// launcher interface the precision-specific translation units implement.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/khb.h"
+
+namespace khb {
+
+// Floors::Prescription (floors.hpp:100-117); same layout as khb_floors
+struct Prescription {
+    double rho_min_const, u_min_const;
+    double rho_min_geom, u_min_geom, r_char;
+    double bsq_over_rho_max, bsq_over_u_max, u_over_rho_max;
+    double ktot_max, gamma_max;
+    int32_t use_r_char, temp_adjust_u, adjust_k, radius_dependent_floors;
+    double floors_switch_r;
+};
+
+struct Dims {
+    int n1, n2, n3, ndim;
+    int is, ie, js, je, ks, ke;
+    int nx1, nx2, nx3;
+    long long N;
+    long long sj, sk;
+    int bc[6];
+};
+
+struct DevGeom {
+    int G1, G2, n1;
+    long long gs;                          // component stride of the location tables, G1*G2
+    const double* gcov[4];                 // face1, face2, face3, centre: [16][G2][G1]
+    const double* gcon[4];
+    const double* gdet[4];                 // [G2][G1]
+    const float* gcov_f[3];                // FP32 copies of the face tables
+    const float* gcon_f[3];
+    const float* gdet_f[3];
+    const double* gdet_conn;               // [64][n2][n1], index (nu*4+lam)*4+mu as gdet_conn(nu,lam,mu)
+    const double* rcen;                    // [n2][n1]
+};
+
+struct Phys {
+    double gam;
+    int riemann, recon_floors, spherical, cart_minkowski;
+    int floors_on, frame, iter_max, fix_avg, fix_atmo;
+    double err_tol;
+    double dx1, dx2, dx3;
+    int zero_polar_flux, fix_polar_flux, check_inflow_in, check_inflow_out;
+    Prescription fl;
+};
+
+enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST = 32 };
+
+template <typename FT>
+struct ZoneArgs {
+    khb_fields Ps, Us, U0, Pout, Uout;
+    const FT* F[3];
+    const FT* ctop[3];
+    int32_t* pflag;
+    int32_t* fflag;
+    double g0, g1, bdt;
+    unsigned long long* ndt_word;
+    int* fail_count;
+    int* fail_list;
+    int mode;
+};
+
+
+// Launchers.  Launch<double> is compiled without FMA contraction (the FP64 path keeps the
+// reference's rounding); Launch<float> (the FP32-flux form) is compiled with contraction.
+template <typename FT>
+struct Launch {
+    static void flux(int recon, int nv, int dir, const Dims& d, const DevGeom& g, const Phys& ph,
+                     const khb_fields& P, FT* F, FT* ctop, const int lo[3], const int cnt[3], cudaStream_t st);
+    static void fix_flux_x2(int nv, const Dims& d, const Phys& ph, FT* F1, FT* F2, FT* F3, int inner, cudaStream_t st);
+    static void fix_flux_x1(const Dims& d, FT* F1, int inner, cudaStream_t st);
+    static void zone(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a, cudaStream_t st);
+    static void flux_ct(const Dims& d, FT* F1, FT* F2, FT* F3, FT* emf, cudaStream_t st);
+    static void copy_flux(long long N, int nv, const FT* F, const FT* ctop, const khb_fields& out, double* ctop_out,
+                          cudaStream_t st);
+};
+
+// Zone-local FP64 work shared by both forms (compiled with the FP64 unit)
+struct LaunchCommon {
+    static void fixup(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
+                      const int32_t* pflag, const int* fail_count, const int* fail_list, cudaStream_t st);
+    static void bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
+                   int face, int lo_a, int cnt_a, int lo_k, int cnt_k, cudaStream_t st);
+    static void ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                           const khb_fields& U, cudaStream_t st);
+    static void periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st);
+    static void ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
+                     cudaStream_t st);
+    static void divb(const Dims& d, const Phys& ph, const khb_fields& U, int i_lo, int i_hi,
+                     unsigned long long* word, cudaStream_t st);
+};
+
+inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+} // namespace khb
