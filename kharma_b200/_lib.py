@@ -97,6 +97,8 @@ SIGNATURES = {
     "khb_get_min_ndt": (_I, [_P, C.POINTER(_D), _P]),
     "khb_max_divb": (_I, [_P, C.POINTER(KhbFields), C.POINTER(_D), _P]),
     "khb_launch_count": (C.c_int64, [_P]),
+    "khb_max_divb_noalloc": (_I, [C.POINTER(KhbConfig), C.POINTER(KhbFields), _P, _P]),
+    "khb_noalloc_last_error": (C.c_char_p, []),
 }
 
 _lib = None

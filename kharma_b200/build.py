@@ -6,6 +6,7 @@ Translation units and their arithmetic flags:
   khb_fp64.cu      FP64 path (fluxes, zone pass, ghost zones)      -fmad=false
   khb_fp32.cu      FP32-flux form (fluxes, EMFs in FP32)           FMA contraction on
   khb_api.cu       host side and C ABI
+  khb_noalloc.cu   khb_max_divb_noalloc (static device scratch)   -fmad=false
   khb_geometry.cpp host construction of the geometry tables
 The library is a plain shared object; the Python layer binds it with ctypes.
 """
@@ -21,6 +22,7 @@ UNITS = {
     "khb_fp64.cu": ["-fmad=false"],
     "khb_fp32.cu": [],
     "khb_api.cu": [],
+    "khb_noalloc.cu": ["-fmad=false"],
     "khb_geometry.cpp": [],
 }
 HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", os.path.join("..", "..", "include", "khb.h")]

@@ -236,30 +236,19 @@ int do_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb
 
 } // namespace
 
-// ======================================================================== C ABI
-extern "C" {
-
-const char* khb_last_error(void) { return g_err.c_str(); }
-int khb_version(void) { return 100; }
-
-int khb_create(const khb_config* cfg, khb_ctx** out)
+int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why)
 {
-    if (!cfg || !out) return fail(KHB_ERR_ARG, "khb_create: NULL argument");
-    *out = nullptr;
-    if (cfg->nvar != 5 && cfg->nvar != 8) return fail(KHB_ERR_UNSUPPORTED, "nvar must be 5 or 8");
-    if (cfg->recon < 0 || cfg->recon > 3) return fail(KHB_ERR_UNSUPPORTED, "unknown reconstruction");
-    if (cfg->ng < 3) return fail(KHB_ERR_ARG, "need at least 3 ghost zones");
-    if (cfg->nx1 < 1 || cfg->nx2 < 1 || cfg->nx3 < 1) return fail(KHB_ERR_ARG, "bad block size");
-    if (cfg->nx2 == 1 && cfg->nx3 > 1) return fail(KHB_ERR_UNSUPPORTED, "x3 active with x2 inactive");
-    if (cfg->precision != KHB_PREC_FP64 && cfg->precision != KHB_PREC_FP32_FLUX)
-        return fail(KHB_ERR_UNSUPPORTED, "unknown precision");
-    khb_ctx* c = new khb_ctx();
-    std::memset((void*)c, 0, sizeof(khb_ctx));
-    c->cfg = *cfg;
-    c->nv = cfg->nvar;
-    c->dbl_max_bits = 0x7FEFFFFFFFFFFFFFull;
-    c->fp32 = cfg->precision == KHB_PREC_FP32_FLUX;
-    Dims& d = c->d;
+    if (cfg->nvar != 5 && cfg->nvar != 8) { *why = "nvar must be 5 or 8"; return KHB_ERR_UNSUPPORTED; }
+    if (cfg->recon < 0 || cfg->recon > 3) { *why = "unknown reconstruction"; return KHB_ERR_UNSUPPORTED; }
+    if (cfg->ng < 3) { *why = "need at least 3 ghost zones"; return KHB_ERR_ARG; }
+    if (cfg->nx1 < 1 || cfg->nx2 < 1 || cfg->nx3 < 1) { *why = "bad block size"; return KHB_ERR_ARG; }
+    if (cfg->nx2 == 1 && cfg->nx3 > 1) { *why = "x3 active with x2 inactive"; return KHB_ERR_UNSUPPORTED; }
+    if (cfg->precision != KHB_PREC_FP64 && cfg->precision != KHB_PREC_FP32_FLUX) {
+        *why = "unknown precision";
+        return KHB_ERR_UNSUPPORTED;
+    }
+    std::memset(&d, 0, sizeof(d));
+    std::memset(&ph, 0, sizeof(ph));
     d.nx1 = cfg->nx1; d.nx2 = cfg->nx2; d.nx3 = cfg->nx3;
     d.ndim = 1 + (cfg->nx2 > 1) + (cfg->nx3 > 1);
     d.n1 = cfg->nx1 + 2*cfg->ng;
@@ -271,7 +260,6 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     d.N = (long long)d.n1*d.n2*d.n3;
     d.sj = d.n1; d.sk = (long long)d.n1*d.n2;
     for (int x = 0; x < 6; ++x) d.bc[x] = cfg->bc[x];
-    Phys& ph = c->ph;
     ph.gam = cfg->gam;
     ph.riemann = cfg->riemann;
     ph.recon_floors = cfg->recon_floors && cfg->floors_on;
@@ -289,7 +277,33 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     ph.check_inflow_in = cfg->check_inflow_inner_x1;
     ph.check_inflow_out = cfg->check_inflow_outer_x1;
     std::memcpy(&ph.fl, &cfg->floors, sizeof(khb_floors));
+    return KHB_OK;
+}
 
+// ======================================================================== C ABI
+extern "C" {
+
+const char* khb_last_error(void) { return g_err.c_str(); }
+int khb_version(void) { return 100; }
+
+int khb_create(const khb_config* cfg, khb_ctx** out)
+{
+    if (!cfg || !out) return fail(KHB_ERR_ARG, "khb_create: NULL argument");
+    *out = nullptr;
+    Dims dd;
+    Phys pp;
+    const char* why = nullptr;
+    const int drc = khb::derive_block(cfg, dd, pp, &why);
+    if (drc) return fail(drc, why);
+    khb_ctx* c = new khb_ctx();
+    std::memset((void*)c, 0, sizeof(khb_ctx));
+    c->cfg = *cfg;
+    c->nv = cfg->nvar;
+    c->dbl_max_bits = 0x7FEFFFFFFFFFFFFFull;
+    c->fp32 = cfg->precision == KHB_PREC_FP32_FLUX;
+    c->d = dd;
+    c->ph = pp;
+    const Dims& d = c->d;
     const size_t N = (size_t)d.N, fs = ft_size(c);
     auto alloc = [&](void** p, size_t bytes) -> cudaError_t {
         cudaError_t e = cudaMalloc(p, bytes);

@@ -631,44 +631,58 @@ __global__ void k_copy_flux(long long N, int nv, const FT* F, const FT* ctop, kh
     if (ctop_out) ctop_out[t] = (double)ctop[t];
 }
 
-#ifdef KHB_COMMON_KERNELS
-// B_FluxCT::MaxDivB: corner divergence (b_flux_ct_functions.hpp:52-75), block max + atomicMax
-__global__ void k_divb(Dims d, Phys ph, khb_fields U, int i_lo, int i_hi, unsigned long long* word)
+// |corner divB| at corner (k,j,i) of the conserved field (b_flux_ct_functions.hpp:52-75)
+__device__ __forceinline__ double corner_divb(const Dims& d, const Phys& ph, const khb_fields& U,
+                                              int k, int j, int i)
 {
-    const int ci = i_hi - i_lo + 1, cj = d.je - d.js + 2, ck = (d.ndim > 2) ? d.ke - d.ks + 2 : 1;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double v = 0.;
-    if (t < (long long)ci*cj*ck) {
-        const int i = i_lo + (int)(t % ci);
-        const int j = d.js + (int)((t / ci) % cj);
-        const int k = d.ks + (int)(t / ((long long)ci*cj));
-        const long long c = ((long long)k*d.n2 + j)*d.n1 + i, sj = d.sj, sk = d.sk;
-        const double* B1 = U.v[5]; const double* B2 = U.v[6]; const double* B3 = U.v[7];
-        const bool do3 = d.ndim > 2;
-        const double norm = do3 ? 0.25 : 0.5;
-        double term1 = B1[c] - B1[c-1] + B1[c-sj] - B1[c-sj-1];
-        double term2 = B2[c] - B2[c-sj] + B2[c-1] - B2[c-sj-1];
-        double term3 = 0.;
-        if (do3) {
-            term1 += B1[c-sk] + B1[c-sk-sj] - B1[c-sk-1] - B1[c-sk-sj-1];
-            term2 += B2[c-sk] + B2[c-sk-1] - B2[c-sk-sj] - B2[c-sk-sj-1];
-            term3 = B3[c] + B3[c-sj] + B3[c-1] + B3[c-sj-1] - B3[c-sk] - B3[c-sk-sj] - B3[c-sk-1] - B3[c-sk-sj-1];
-        }
-        v = fabs(norm*term1/ph.dx1 + norm*term2/ph.dx2 + norm*term3/ph.dx3);
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i, sj = d.sj, sk = d.sk;
+    const double* B1 = U.v[5]; const double* B2 = U.v[6]; const double* B3 = U.v[7];
+    const bool do3 = d.ndim > 2;
+    const double norm = do3 ? 0.25 : 0.5;
+    double term1 = B1[c] - B1[c-1] + B1[c-sj] - B1[c-sj-1];
+    double term2 = B2[c] - B2[c-sj] + B2[c-1] - B2[c-sj-1];
+    double term3 = 0.;
+    if (do3) {
+        term1 += B1[c-sk] + B1[c-sk-sj] - B1[c-sk-1] - B1[c-sk-sj-1];
+        term2 += B2[c-sk] + B2[c-sk-1] - B2[c-sk-sj] - B2[c-sk-sj-1];
+        term3 = B3[c] + B3[c-sj] + B3[c-1] + B3[c-sj-1] - B3[c-sk] - B3[c-sk-sj] - B3[c-sk-1] - B3[c-sk-sj-1];
     }
+    return fabs(norm*term1/ph.dx1 + norm*term2/ph.dx2 + norm*term3/ph.dx3);
+}
+
+// Maximum over the 256 threads of a block (blockDim.x == 256)
+__device__ __forceinline__ double block_max256(double v)
+{
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     __shared__ double wmax[8];
     if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = v;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = wmax[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
-        atomicMax(word, (unsigned long long)__double_as_longlong(m));
-    }
+    double m = wmax[0];
+    for (int w = 1; w < 8; ++w) m = fmax(m, wmax[w]);
+    return m;
 }
 
+// One corner per thread over [ks, ke+1(3D)] x [js, je+1] x [i_lo, i_hi]
+__device__ __forceinline__ double divb_of_thread(const Dims& d, const Phys& ph, const khb_fields& U,
+                                                 int i_lo, int i_hi)
+{
+    const int ci = i_hi - i_lo + 1, cj = d.je - d.js + 2, ck = (d.ndim > 2) ? d.ke - d.ks + 2 : 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ci*cj*ck) return 0.;
+    const int i = i_lo + (int)(t % ci);
+    const int j = d.js + (int)((t / ci) % cj);
+    const int k = d.ks + (int)(t / ((long long)ci*cj));
+    return corner_divb(d, ph, U, k, j, i);
+}
 
+#ifdef KHB_COMMON_KERNELS
+// B_FluxCT::MaxDivB (b_flux_ct.cpp:566-607): block max, then one atomicMax on the bit pattern
+__global__ void __launch_bounds__(256) k_divb(Dims d, Phys ph, khb_fields U, int i_lo, int i_hi, unsigned long long* word)
+{
+    const double m = block_max256(divb_of_thread(d, ph, U, i_lo, i_hi));
+    if (threadIdx.x == 0) atomicMax(word, (unsigned long long)__double_as_longlong(m));
+}
 #endif
 
 // ===================================================================================== launchers

@@ -99,4 +99,8 @@ struct LaunchCommon {
 
 inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// Validate a khb_config and derive the block index ranges and physics parameters (no allocation).
+// Returns KHB_OK or a KHB_ERR_* code with a message in *why.
+int derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why);
+
 } // namespace khb
