@@ -275,6 +275,20 @@ def gpu_arm(args, rank, world, local_rank):
         fp32 = {"value": v32, "unit": UNIT, "ms_per_step": float(t32.item()) / args.steps,
                 "speedup_vs_fp64": v32 / value}
         del b32
+        # accuracy: 100 steps of each form from the same state with the FP64 run's dt sequence
+        ref = Block(torus_spec(n1, n2, n3), geometry=geom)
+        ref.set_prims(P0)
+        dref = Driver(ref)
+        dts = [dref.step()[0] for _ in range(100)]
+        f32 = Block(torus_spec(n1, n2, n3, precision="fp32_flux"), geometry=geom)
+        f32.set_prims(P0)
+        for dt in dts:
+            f32.step(dt)
+        torch.cuda.synchronize()
+        sl = spec.interior
+        r64, r32 = ref.P[0][sl], f32.P[0][sl]
+        fp32["rel_l1_rho_after_100_steps"] = float((r32 - r64).abs().sum() / r64.abs().sum())
+        del ref, f32
 
     # end-to-end through the C ABI with host buffers: H2D of P and U, the step, D2H of P and U
     e2e = None

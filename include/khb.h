@@ -221,6 +221,10 @@ int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void*
 int khb_max_divb_noalloc(const khb_config* cfg, const khb_fields* U, double* max_divb_out, void* stream);
 const char* khb_noalloc_last_error(void);
 
+/* Launch-shape choices that do not change results (bitwise): "zone_split" = 0 runs the zone pass
+ * as one kernel, 1 (the default) as two (update; inversion + floors + P->U). */
+int khb_set_tuning(khb_ctx* ctx, const char* key, int value);
+
 /* Number of device kernel launches issued through this context so far (for accounting). */
 int64_t khb_launch_count(khb_ctx* ctx);
 

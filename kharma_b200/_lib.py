@@ -7,7 +7,8 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libkhb.so")
+# KHB_LIB_PATH selects another build of the same library (e.g. a variant under test)
+LIB_PATH = os.environ.get("KHB_LIB_PATH", os.path.join(_HERE, "lib", "libkhb.so"))
 
 MAX_VARS = 8
 
@@ -97,6 +98,7 @@ SIGNATURES = {
     "khb_get_min_ndt": (_I, [_P, C.POINTER(_D), _P]),
     "khb_max_divb": (_I, [_P, C.POINTER(KhbFields), C.POINTER(_D), _P]),
     "khb_launch_count": (C.c_int64, [_P]),
+    "khb_set_tuning": (_I, [_P, C.c_char_p, _I]),
     "khb_max_divb_noalloc": (_I, [C.POINTER(KhbConfig), C.POINTER(KhbFields), _P, _P]),
     "khb_noalloc_last_error": (C.c_char_p, []),
 }

@@ -119,6 +119,9 @@ class Block:
         _lib.check(self.lib.khb_max_divb(self.ctx, self.Uf.ref, C.byref(out), self.stream), "khb_max_divb")
         return out.value
 
+    def set_tuning(self, key, value):
+        _lib.check(self.lib.khb_set_tuning(self.ctx, key.encode(), int(value)), "khb_set_tuning")
+
     def launch_count(self):
         return int(self.lib.khb_launch_count(self.ctx))
 

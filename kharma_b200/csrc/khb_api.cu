@@ -29,6 +29,7 @@ struct khb_ctx {
     bool geom_set;
     int64_t launches;
     unsigned long long dbl_max_bits;   // host source of the reduction reset (outlives async copies)
+    int zone_split;        // 1: run the zone pass as two kernels (update; inversion+floors+P->U)
 };
 
 namespace {
@@ -217,7 +218,16 @@ int zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const kh
     zc.Ps = Ps; zc.Us = Us; zc.U0 = U0; zc.Pout = Pout; zc.Uout = Uout;
     zc.pflag = pflag; zc.fflag = fflag;
     zc.g0 = kRkGam0[s]; zc.g1 = kRkGam1[s]; zc.bdt = kRkBeta[s] * dt;
-    zc.mode = M_UPDATE | M_UTOP | M_FLOORS | M_PTOU | M_FAILLIST | (stage == 2 ? M_DT : 0);
+    const int dtm = (stage == 2) ? M_DT : 0;
+    if (!ctx->zone_split) {
+        zc.mode = M_ZONE_FUSED | dtm;
+        return launch_zone(ctx, zc, st);
+    }
+    int rc;
+    zc.mode = M_UPDATE;
+    if ((rc = launch_zone(ctx, zc, st))) return rc;
+    zc.Us = Uout;          // the updated conserved state is the inversion's input
+    zc.mode = M_ZONE_CELL | dtm;
     return launch_zone(ctx, zc, st);
 }
 
@@ -303,6 +313,7 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     c->fp32 = cfg->precision == KHB_PREC_FP32_FLUX;
     c->d = dd;
     c->ph = pp;
+    c->zone_split = 1;
     const Dims& d = c->d;
     const size_t N = (size_t)d.N, fs = ft_size(c);
     auto alloc = [&](void** p, size_t bytes) -> cudaError_t {
@@ -350,7 +361,7 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
     // device layout: for loc 0..3: gcov [16][G2][G1], gcon [16][G2][G1], gdet [G2][G1]; then
     // gdet_conn [64][n2][n1] and r_center [n2][n1]
     const size_t per_loc = 33 * gs, n2n1 = (size_t)d.n2*d.n1;
-    const size_t total = 4*per_loc + 64*n2n1 + n2n1;
+    const size_t total = 4*per_loc + 64*n2n1 + 3*n2n1;
     std::vector<double> h(total);
     std::vector<float> hf(3*per_loc);
     for (int loc = 0; loc < 4; ++loc) {
@@ -369,6 +380,22 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
     for (size_t x = 0; x < n2n1; ++x)
         for (int m = 0; m < 64; ++m) gc[m*n2n1 + x] = gdet_conn[x*64 + m];
     std::memcpy(h.data() + 4*per_loc + 64*n2n1, r_center, n2n1*sizeof(double));
+    // geometric floors per zone centre (floors_functions.hpp:96-104), x3-independent
+    double* frho = h.data() + 4*per_loc + 65*n2n1;
+    double* fu = frho + n2n1;
+    const khb_floors& f = ctx->cfg.floors;
+    for (size_t x = 0; x < n2n1; ++x) {
+        if (ctx->cfg.spherical) {
+            const double r = r_center[x];
+            const double rhoscal = (f.use_r_char) ? 1. / ((r*r) * (1 + r / f.r_char)) : 1. / std::sqrt(r*r*r);
+            const double a = f.rho_min_geom * rhoscal, b = f.u_min_geom * std::pow(rhoscal, ctx->cfg.gam);
+            frho[x] = (a < f.rho_min_const) ? f.rho_min_const : a;
+            fu[x] = (b < f.u_min_const) ? f.u_min_const : b;
+        } else {
+            frho[x] = f.rho_min_const;
+            fu[x] = f.u_min_const;
+        }
+    }
     if (!ctx->geo_d) {
         KHB_CUDA(cudaMalloc((void**)&ctx->geo_d, total*sizeof(double)));
         KHB_CUDA(cudaMalloc((void**)&ctx->geo_f, hf.size()*sizeof(float)));
@@ -389,6 +416,8 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
     }
     g.gdet_conn = ctx->geo_d + 4*per_loc;
     g.rcen = ctx->geo_d + 4*per_loc + 64*n2n1;
+    g.floor_rho = g.rcen + n2n1;
+    g.floor_u = g.rcen + 2*n2n1;
     ctx->geom_set = true;
     return KHB_OK;
 }
@@ -602,6 +631,13 @@ int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void*
     KHB_CUDA(cudaStreamSynchronize(S(stream)));
     std::memcpy(max_divb_host, &bits, sizeof(double));
     return KHB_OK;
+}
+
+int khb_set_tuning(khb_ctx* ctx, const char* key, int value)
+{
+    if (!ctx || !key) return fail(KHB_ERR_ARG, "khb_set_tuning: NULL argument");
+    if (std::strcmp(key, "zone_split") == 0) { ctx->zone_split = value ? 1 : 0; return KHB_OK; }
+    return fail(KHB_ERR_ARG, std::string("khb_set_tuning: unknown key ") + key);
 }
 
 int64_t khb_launch_count(khb_ctx* ctx) { return ctx ? ctx->launches : 0; }

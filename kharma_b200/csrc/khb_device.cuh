@@ -385,28 +385,13 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
 enum { FF_GEOM_RHO = 32, FF_GEOM_U = 64, FF_B_RHO = 128, FF_B_U = 256, FF_TEMP = 512, FF_GAMMA = 1024,
        FF_KTOT = 2048, FF_GEOM_RHO_FLUX = 4096, FF_GEOM_U_FLUX = 8192 };
 
-// Geometric floor values, floors_functions.hpp:96-104
-__device__ __forceinline__ void geo_floor_values(const Prescription& f, bool spherical, double r, double gam,
-                                                 double& rhoflr_geom, double& uflr_geom)
-{
-    if (spherical) {
-        const double rhoscal = (f.use_r_char) ? 1. / ((r*r) * (1 + r / f.r_char)) : 1. / sqrt(r*r*r);
-        rhoflr_geom = kmax(f.rho_min_geom * rhoscal, f.rho_min_const);
-        uflr_geom   = kmax(f.u_min_geom * pow(rhoscal, gam), f.u_min_const);
-    } else {
-        rhoflr_geom = f.rho_min_const;
-        uflr_geom   = f.u_min_const;
-    }
-}
-
 // floors_functions.hpp:84-160
+// rhoflr_geom, uflr_geom: the geometric floor values of this zone (x3-independent, tabulated per
+// (j,i) at set-up with the same formula, floors_functions.hpp:96-104).  D returns the 4-vectors of P.
 template <int NV>
-__device__ int determine_floors(const ZoneGeom& G, const Prescription& f, bool spherical, double r, double gam,
-                                const double* P, double& rhoflr_max, double& uflr_max)
+__device__ int determine_floors(const ZoneGeom& G, const Prescription& f, double rhoflr_geom, double uflr_geom,
+                                double gam, const double* P, double& rhoflr_max, double& uflr_max, FourVec<double>& D)
 {
-    double rhoflr_geom, uflr_geom;
-    geo_floor_values(f, spherical, r, gam, rhoflr_geom, uflr_geom);
-    FourVec<double> D;
     double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
     calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, P, D);
     const double bsq = dot4(D.bcon, D.bcov);

@@ -66,8 +66,13 @@ template <> struct FaceTables<float> {
     static __device__ __forceinline__ const float* gdet(const DevGeom& g, int loc) { return g.gdet_f[loc]; }
 };
 
+// FP64 faces: cap registers at 128 so four 128-thread blocks fit per SM (measured faster despite a
+// few bytes of spill); the FP32 form needs fewer registers and is left unconstrained.
+template <typename R> struct FluxMinBlocks { static constexpr int value = 1; };
+template <> struct FluxMinBlocks<double> { static constexpr int value = 4; };
+
 template <int DIR, int RECON, int NV, typename R, typename FT>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, FluxMinBlocks<R>::value)
 k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop,
        int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, long long total)
 {
@@ -108,8 +113,7 @@ k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restr
     }
     if (ph.recon_floors) {
         // floors_functions.hpp:320-354 applied to both reconstructed states (get_flux.hpp:174-181)
-        double rf, uf;
-        geo_floor_values(ph.fl, ph.spherical, __ldg(g.rcen + (long long)j*g.n1 + i), ph.gam, rf, uf);
+        const double rf = __ldg(g.floor_rho + (long long)j*g.n1 + i), uf = __ldg(g.floor_u + (long long)j*g.n1 + i);
         Pl[0] += kmax(R(0), (R)rf - Pl[0]); Pl[1] += kmax(R(0), (R)uf - Pl[1]);
         Pr[0] += kmax(R(0), (R)rf - Pr[0]); Pr[1] += kmax(R(0), (R)uf - Pr[1]);
     }
@@ -192,10 +196,13 @@ __global__ void k_fix_flux_x1(Dims d, FT* F1, int inner)
 template <typename FT>
 __device__ __forceinline__ double ldf(const FT* F, long long x) { return (double)__ldg(F + x); }
 
-template <int NV, typename FT>
+// MODE: compile-time mask of M_* steps (0: take the mask from the arguments at run time).  The
+// CFL reduction (M_DT) is always a run-time choice.
+template <int NV, typename FT, int MODE>
 __global__ void __launch_bounds__(128)
 k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
 {
+    const int mode = MODE ? (MODE | (a.mode & M_DT)) : a.mode;
     const int cnt_i = d.ie - d.is + 1, cnt_j = d.je - d.js + 1, cnt_k = d.ke - d.ks + 1;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long total = (long long)cnt_i*cnt_j*cnt_k;
@@ -213,7 +220,7 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
         load_zone_geom(g, j, i, G);
 
         double U[NV], P[NV];
-        if (a.mode & M_UPDATE) {
+        if (mode & M_UPDATE) {
             // ---- flux divergence (Parthenon FluxDivHelper) with flux-CT B fluxes
             const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
             const double vol = ph.dx1*ph.dx2*ph.dx3;
@@ -318,9 +325,11 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
         }
 
         int pflag = 0, fflag = 0;
+        FourVec<double> D;
+        bool have_D = false;
 #pragma unroll
         for (int p = 0; p < NV; ++p) P[p] = a.Ps.v[p][c];
-        if (a.mode & M_UTOP) {
+        if (mode & M_UTOP) {
             // inverter.cpp:163-181 then b_flux_ct.cpp:196-217
             const int pf = u_to_p_onedw<NV>(G, gam, U, P, ph.iter_max, ph.err_tol);
             pflag = pf % FF_GEOM_RHO;
@@ -333,11 +342,11 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
             pflag = a.pflag[c];
             fflag = a.fflag[c];
         }
-        if ((a.mode & M_FLOORS) && ph.floors_on) {
+        if ((mode & M_FLOORS) && ph.floors_on) {
             // floors.cpp:215-229 and floors_impl.hpp:77-125
             double rf, uf;
-            const double rr = __ldg(g.rcen + (long long)j*g.n1 + i);
-            fflag |= determine_floors<NV>(G, ph.fl, ph.spherical, rr, gam, P, rf, uf);
+            const long long cg = (long long)j*g.n1 + i;
+            fflag |= determine_floors<NV>(G, ph.fl, __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), gam, P, rf, uf, D);
             if (fflag) {
                 const int pl = apply_floors_frame<NV>(G, ph.frame, gam, P, U, rf, uf, 8);
                 if (pl) pflag = pl;
@@ -346,23 +355,28 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
                 p_to_u_zone<NV>(G, gam, P, Ut);
 #pragma unroll
                 for (int p = 0; p < 5; ++p) U[p] = Ut[p];
+            } else {
+                have_D = true;   // P is unchanged: its 4-vectors serve the P->U below
             }
         }
-        if (a.mode & M_PTOU) p_to_u_zone<NV>(G, gam, P, U);
+        if (mode & M_PTOU) {
+            if (have_D) prim_to_flux<double, NV>(P, D, gam, G.gdet, 0, U);
+            else p_to_u_zone<NV>(G, gam, P, U);
+        }
 
 #pragma unroll
         for (int p = 0; p < NV; ++p) a.Uout.v[p][c] = U[p];
-        if (a.mode & (M_UTOP | M_FLOORS)) {
+        if (mode & (M_UTOP | M_FLOORS)) {
 #pragma unroll
             for (int p = 0; p < NV; ++p) a.Pout.v[p][c] = P[p];
             a.pflag[c] = pflag;
             a.fflag[c] = fflag;
         }
-        if ((a.mode & M_FAILLIST) && pflag > 0) {
+        if ((mode & M_FAILLIST) && pflag > 0) {
             const int slot = atomicAdd(a.fail_count, 1);
             a.fail_list[slot] = (int)c;
         }
-        if (a.mode & M_DT) {
+        if (mode & M_DT) {
             // grmhd.cpp:313-328
             const double c1 = kmax((double)a.ctop[0][c], 0.0), c2 = kmax((double)a.ctop[1][c], 0.0);
             const double c3 = kmax((double)a.ctop[2][c], 0.0);
@@ -370,7 +384,7 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
             if (!isnan(z)) ndt_zone = z;
         }
     }
-    if (a.mode & M_DT) {
+    if (mode & M_DT) {
         // block minimum by warp shuffles, then one atomic per block on the bit pattern (values >= 0)
         double v = ndt_zone;
 #pragma unroll
@@ -419,8 +433,7 @@ __global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, 
         for (int p = 0; p < 5; ++p) Pz[p] = (wsum < 1.e-10) ? 0. : sum[p]/wsum;
 #pragma unroll
         for (int p = 5; p < NV; ++p) Pz[p] = P.v[p][c];
-        double rf, uf;
-        geo_floor_values(ph.fl, ph.spherical, g.rcen[(long long)j*g.n1 + i], ph.gam, rf, uf);
+        const double rf = g.floor_rho[(long long)j*g.n1 + i], uf = g.floor_u[(long long)j*g.n1 + i];
         Pz[0] += kmax(0., rf - Pz[0]);
         Pz[1] += kmax(0., uf - Pz[1]);
         ZoneGeom G;
@@ -733,13 +746,23 @@ void Launch<FT>::fix_flux_x1(const Dims& d, FT* F1, int inner, cudaStream_t st)
     k_fix_flux_x1<FT><<<blocks_for((long long)nj*nk, 128), 128, 0, st>>>(d, F1, inner);
 }
 
-template <typename FT>
-void Launch<FT>::zone(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a, cudaStream_t st)
+template <int NV, typename FT>
+static void zone_nv(const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a, cudaStream_t st)
 {
     const long long total = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
     const unsigned nb = blocks_for(total, 128);
-    if (nv == 8) k_zone<8, FT><<<nb, 128, 0, st>>>(d, g, ph, a);
-    else k_zone<5, FT><<<nb, 128, 0, st>>>(d, g, ph, a);
+    const int m = a.mode & ~M_DT;
+    if (m == M_ZONE_FUSED) k_zone<NV, FT, M_ZONE_FUSED><<<nb, 128, 0, st>>>(d, g, ph, a);
+    else if (m == M_UPDATE) k_zone<NV, FT, M_UPDATE><<<nb, 128, 0, st>>>(d, g, ph, a);
+    else if (m == M_ZONE_CELL) k_zone<NV, FT, M_ZONE_CELL><<<nb, 128, 0, st>>>(d, g, ph, a);
+    else k_zone<NV, FT, 0><<<nb, 128, 0, st>>>(d, g, ph, a);
+}
+
+template <typename FT>
+void Launch<FT>::zone(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a, cudaStream_t st)
+{
+    if (nv == 8) zone_nv<8, FT>(d, g, ph, a, st);
+    else zone_nv<5, FT>(d, g, ph, a, st);
 }
 
 template <typename FT>

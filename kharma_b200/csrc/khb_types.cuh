@@ -39,6 +39,8 @@ struct DevGeom {
     const float* gdet_f[3];
     const double* gdet_conn;               // [64][n2][n1], index (nu*4+lam)*4+mu as gdet_conn(nu,lam,mu)
     const double* rcen;                    // [n2][n1]
+    const double* floor_rho;               // geometric density floor per zone centre, [n2][n1]
+    const double* floor_u;                 // geometric internal-energy floor, [n2][n1]
 };
 
 struct Phys {
@@ -52,6 +54,8 @@ struct Phys {
 };
 
 enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST = 32 };
+// The whole zone pass in one kernel, or its two halves (update; inversion + floors + P->U)
+enum { M_ZONE_CELL = M_UTOP | M_FLOORS | M_PTOU | M_FAILLIST, M_ZONE_FUSED = M_UPDATE | M_ZONE_CELL };
 
 template <typename FT>
 struct ZoneArgs {
