@@ -144,7 +144,7 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     n1, n2, n3 = [int(x) for x in args.size.split(",")]
-    n3s = max(8, n3 // 16)
+    n3s = max(8, n3 // 4)
     from kharma_b200.spec import torus_spec
     from oracle import orc
     from kharma_b200 import problems
@@ -345,10 +345,11 @@ def gpu_arm(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        n3s = max(8, n3 // 16)
-        v_cpu, threads, el = cpu_sample(n1, n2, n3s, steps=2)
+        n3s = max(8, n3 // 2)
+        v_cpu, threads, el = cpu_sample(n1, n2, n3s, steps=8)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"oracle port, {threads} threads, {n1}x{n2}x{n3s} slab of the torus, 2 RK2 steps ({el:.1f} s)"}
+               "sample": f"oracle port, {threads} OpenMP threads, {n1}x{n2}x{n3s} slab of the torus "
+                         f"(same per-zone work), 8 RK2 steps after 1 warm-up ({el:.1f} s)"}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
