@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-kernel-times", action="store_true")
+    ap.add_argument("--no-emhd", action="store_true")
+    ap.add_argument("--emhd-only", action="store_true",
+                    help="run only the implicit EMHD Newton measurement and print its JSON object")
     return ap.parse_args()
 
 
@@ -215,6 +218,66 @@ def kernel_times(block, spec, nsteps=3):
     return {k: (float(np.mean(v)), len(v) // nsteps) for k, v in times.items()}
 
 
+def emhd_newton(n=128, reps=3):
+    """Per-zone implicit EMHD Newton solve (Implicit::Step) on the conducting atmosphere at n^3:
+    forward-difference Jacobian (the reference's) vs the exact tangent Jacobian.  Each form solves
+    the same system to a maximum residual of 1e-10 relative to max|U|/dt; reported are the Newton
+    iterations the device-side stopping test took and the CUDA-event time of the whole solve."""
+    import torch
+    from kharma_b200 import problems
+    from kharma_b200.block import Block, build_geometry
+    from kharma_b200.emhd import ImplicitSolver
+    from kharma_b200.spec import EmhdSpec, ImplicitSpec, atmosphere_spec
+    spec = atmosphere_spec(n, n, n)
+    emhd = EmhdSpec(closure_type="kappa_eta", higher_order_terms=True, tau=1.0, kappa=0.1, eta=0.1)
+    prof = np.load(os.path.join(ROOT, "tests", "golden", "atmosphere_profiles.npz"))
+    prof = {k: prof["%s_%d" % (k, n)] for k in ("rCoords", "rho", "u", "phi")}
+    geom = build_geometry(spec)
+    P = problems.conducting_atmosphere(spec, geom, emhd, prof, jitter=1e-3, seed=1234)
+    b = Block(spec, geometry=geom)
+    sol = ImplicitSolver(b, emhd)
+    dt = 0.1
+    Pd = torch.tensor(P, dtype=torch.float64, device="cuda")
+    Ud = sol.ptou(Pd)
+    Sd = torch.zeros_like(Pd)
+    sol.add_source(Pd, Sd)
+    # stand-in for the flux divergence of the perturbed atmosphere: seeded noise of 1e-3 |U|/dt
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    Sd += (2 * torch.rand(Pd.shape, generator=g, device="cuda", dtype=torch.float64) - 1) * 1e-3 * Ud.abs() / dt
+    k, j, i = spec.interior
+    tol = 1e-10 * float(Ud[:, k, j, i].abs().max()) / dt
+    out = {"workload": f"conducting atmosphere (KS a=0, MKS hslope 1, r 200-300) {n}^3, 10 primitives, "
+                       f"kappa_eta closure tau=1 kappa=eta=0.1, higher-order terms; dt={dt}",
+           "tolerance_abs": tol, "tolerance_rel": 1e-10, "zones": n ** 3}
+    Psol = torch.empty_like(Pd)
+    norm = sol.scalar_field()
+    fail = sol.scalar_field()
+    for jac in ("fd", "exact"):
+        sol.set_implicit(ImplicitSpec(min_nonlinear_iter=1, max_nonlinear_iter=16, rootfind_tol=tol, jacobian=jac))
+        times = []
+        for r in range(reps + 1):
+            Psol.copy_(Pd)
+            norm.zero_()
+            fail.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sol.step(Pd, Ud, Pd, Sd, Psol, norm, fail, dt)
+            e1.record()
+            torch.cuda.synchronize()
+            if r:
+                times.append(e0.elapsed_time(e1))
+        it, mx = sol.stats()
+        ms = float(np.median(times))
+        out[jac] = {"iterations": it, "ms_per_solve": ms, "ms_per_iteration": ms / max(it, 1),
+                    "zone_iterations_per_s": n ** 3 * it / (ms / 1000.0),
+                    "max_norm_per_iteration": [float(x) for x in mx],
+                    "failed_zones": int((fail[k, j, i] == 1).sum())}
+    out["exact_vs_fd_wall_time"] = out["fd"]["ms_per_solve"] / out["exact"]["ms_per_solve"]
+    return out
+
+
 def gpu_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -346,6 +409,10 @@ def gpu_arm(args, rank, world, local_rank):
                              "alg_bytes_per_zone_cycle": B_ALG_PER_ZC},
                     "kernel_ms_per_launch": {k: round(v[0], 4) for k, v in ktimes.items()}}
 
+    emhd = None
+    if rank == 0 and world == 1 and not args.no_emhd:
+        emhd = emhd_newton()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n3s = max(8, n3 // 2)
@@ -363,7 +430,7 @@ def gpu_arm(args, rank, world, local_rank):
                           "floors": "drift", "parallelism": f"replicas x{world}",
                           "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
-               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu}
+               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd}
         print(json.dumps(out), flush=True)
 
 
@@ -376,6 +443,10 @@ def main():
         reference_arm(args, rank, world)
         return
     import torch
+    if args.emhd_only:
+        if rank == 0:
+            print(json.dumps({"emhd_newton": emhd_newton()}), flush=True)
+        return
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta

@@ -17,7 +17,9 @@
  *    covering the whole block including ghosts.  n1 = nx1 + 2 ng, and n2 (n3) = nx2 + 2 ng
  *    (nx3 + 2 ng) when that direction is active, else 1.  Variable order is
  *    rho, u, u1, u2, u3, B1, B2, B3 (primitives) and rho u^t, T^t_t + rho u^t, T^t_1..3,
- *    B^1..3 sqrt(-g) (conserved), matching KHARMA's VarMap for a GRMHD+flux-CT pack.
+ *    B^1..3 sqrt(-g) (conserved), matching KHARMA's VarMap for a GRMHD+flux-CT pack.  The EMHD
+ *    entry points also read q~, dP~ (primitives) and q~ u^t sqrt(-g), dP~ u^t sqrt(-g) (conserved)
+ *    from slots 8 and 9.
  *  - The context owns only scratch: face fluxes, signal speeds, the intermediate RK stage,
  *    reduction words and the geometry tables copied in by khb_set_geometry().
  *  - Per-zone flags keep the reference encodings: pflag is Inverter::Status
@@ -34,7 +36,11 @@
 extern "C" {
 #endif
 
-#define KHB_MAX_VARS 8
+#define KHB_MAX_VARS 10
+
+/* Slots of khb_fields: rho, u, u1-u3, B1-B3 in 0-7; the EMHD variables q~ and dP~ (the "tilde"
+ * primitives of emhd/emhd.hpp:313-332 and their conserved forms) in 8 and 9 when EMHD is on. */
+enum { KHB_RHO = 0, KHB_UU = 1, KHB_U1 = 2, KHB_B1 = 5, KHB_Q = 8, KHB_DP = 9 };
 
 enum { KHB_OK = 0, KHB_ERR_ARG = -1, KHB_ERR_CUDA = -2, KHB_ERR_STATE = -3, KHB_ERR_UNSUPPORTED = -4 };
 
@@ -90,6 +96,27 @@ typedef struct {
 } khb_coords;
 
 typedef struct khb_ctx khb_ctx;
+
+/* EMHD closures (emhd/emhd.hpp:58, selected by emhd/closure_type, emhd.cpp:62-102) */
+enum { KHB_CLOSURE_CONSTANT = 0, KHB_CLOSURE_SOUNDSPEED = 1, KHB_CLOSURE_KAPPA_ETA = 2, KHB_CLOSURE_TORUS = 3 };
+/* Jacobian of the implicit residual: the reference's forward differences (implicit.hpp:208-255)
+ * or the exact Jacobian by a hand-written tangent (no counterpart in the reference) */
+enum { KHB_JACOBIAN_FD = 0, KHB_JACOBIAN_EXACT = 1 };
+/* Per-zone solver status (implicit/implicit.hpp:63-69), stored as doubles like solve_fail */
+enum { KHB_SOLVE_CONVERGED = 0, KHB_SOLVE_FAIL = 1, KHB_SOLVE_BEYOND_TOL = 2, KHB_SOLVE_BACKTRACK = 3 };
+
+/* EMHD::EMHD_parameters (emhd/emhd.hpp:60-84) with the package switches emhd/conduction and
+ * emhd/viscosity (emhd.cpp:60-72); q~ is evolved iff conduction, dP~ iff viscosity. */
+typedef struct {
+    int32_t closure, higher_order_terms, feedback, conduction, viscosity, pad;
+    double tau, conduction_alpha, viscosity_alpha, kappa, eta;
+} khb_emhd_params;
+
+/* Implicit package parameters (implicit/implicit.cpp:99-119); max_nonlinear_iter <= 64 */
+typedef struct {
+    int32_t min_nonlinear_iter, max_nonlinear_iter, use_qr, linesearch, max_linesearch_iter, jacobian;
+    double jacobian_delta, rootfind_tol, linesearch_eps, linesearch_lambda;
+} khb_implicit_params;
 
 /* One device pointer per variable (Parthenon allocates each variable separately). */
 typedef struct { double* v[KHB_MAX_VARS]; } khb_fields;
@@ -220,6 +247,64 @@ int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void*
  * share the array and race; serialize them.  Errors: khb_noalloc_last_error(). */
 int khb_max_divb_noalloc(const khb_config* cfg, const khb_fields* U, double* max_divb_out, void* stream);
 const char* khb_noalloc_last_error(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Extended MHD and the implicit solve (emhd/, implicit/)
+ * ------------------------------------------------------------------------------------------- */
+
+/* Host construction of the connection coefficients Gamma^a_bc at zone centres
+ * (gr_coordinates.cpp:156-161, conn_direct): conn [n2][n1][4][4][4], same arguments as
+ * khb_build_geometry. */
+int khb_build_connection(const khb_coords* coords, const khb_config* cfg, double x1min, double x2min,
+                         double x3min, double* conn);
+
+/* Copy the connection (host, layout above) to the device and allocate the EMHD scratch of this
+ * context (5 + 7 doubles per zone).  Required before khb_emhd_add_source and khb_fix_solve. */
+int khb_set_connection(khb_ctx* ctx, const double* conn);
+
+/* Flux::MeshPtoU with the EMHD stress tensor (flux_functions.hpp:80-107, 180-232) and
+ * EMHD::BlockPtoU (emhd.cpp:251-281) over the whole block: all 8 + (q, dP) conserved variables. */
+int khb_emhd_ptou(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* U,
+                  void* stream);
+
+/* EMHD::AddSource (emhd.cpp:288-397): adds the explicit conduction and viscosity sources
+ * (gradients of u_mu and Theta by MC slopes, emhd_utils.hpp:55-79) to slots 8/9 of dUdt over the
+ * interior.  P needs one valid ghost layer in each active direction. */
+int khb_emhd_add_source(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* dUdt,
+                        void* stream);
+
+/* Implicit::Step (implicit.cpp:159-571) over the interior: up to max_nonlinear_iter Newton
+ * iterations of the per-zone implicit residual (implicit.hpp:139-200) with a forward-difference
+ * (reference) or exact Jacobian, QR with column pivoting (or the LU path), backtracking and line
+ * search.  P_full/U_full: state at the start of the step; P_sub: at the start of this sub-step;
+ * src: flux divergence plus explicit sources (dU/dt); P_solver: initial guess on entry, result on
+ * return (implicit variables only; its B is used as given).  solve_norm and solve_fail are the
+ * reference's per-zone fields (doubles over the block), read and written; a zone that enters with
+ * solve_fail == KHB_SOLVE_FAIL is skipped.  The iteration stops, as in the reference, after
+ * min_nonlinear_iter iterations once the maximum solve_norm is below rootfind_tol; that test runs on
+ * the device, so nothing is synchronized. */
+int khb_implicit_step(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp,
+                      const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub,
+                      const khb_fields* src, const khb_fields* P_solver, double* solve_norm, double* solve_fail,
+                      double dt, void* stream);
+
+/* Iterations taken by the last khb_implicit_step and the maximum solve_norm of each (max_norms
+ * has room for max_nonlinear_iter values).  Synchronizes the stream. */
+int khb_implicit_stats(khb_ctx* ctx, int32_t* iterations, double* max_norms, void* stream);
+
+/* Residual and Jacobian at P_solver without updating it (the split implicit_jacobian kernel,
+ * implicit.cpp:286-320, which stores Implicit.jacobian and Implicit.residual): jacobian is
+ * [nf*nf][n3][n2][n1] row-major per zone, residual [nf][n3][n2][n1], nf = 5 + conduction + viscosity. */
+int khb_implicit_jacobian(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp,
+                          const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub,
+                          const khb_fields* src, const khb_fields* P_solver, double dt, double* jacobian,
+                          double* residual, void* stream);
+
+/* Implicit::FixSolve (fix_solve.cpp:44-130) over the whole block: zones with solve_fail ==
+ * KHB_SOLVE_FAIL get the distance-weighted average of their non-failed neighbours' implicit
+ * primitives (all neighbours if none is good), read from the state before this call, and U = U(P). */
+int khb_fix_solve(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* U,
+                  const double* solve_fail, void* stream);
 
 /* Launch-shape choices that do not change results (bitwise): "zone_split" = 0 runs the zone pass
  * as one kernel, 1 (the default) as two (update; inversion + floors + P->U). */

@@ -10,7 +10,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 # KHB_LIB_PATH selects another build of the same library (e.g. a variant under test)
 LIB_PATH = os.environ.get("KHB_LIB_PATH", os.path.join(_HERE, "lib", "libkhb.so"))
 
-MAX_VARS = 8
+MAX_VARS = 10
+Q, DP = 8, 9           # khb_fields slots of the EMHD variables
 
 # enums (include/khb.h)
 RECON = {"donor_cell": 0, "linear_mc": 1, "weno5": 2, "ppm": 3}
@@ -20,6 +21,9 @@ FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 PREC = {"fp64": 0, "fp32_flux": 1}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
 TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
+CLOSURE = {"constant": 0, "soundspeed": 1, "sound_speed": 1, "kappa_eta": 2, "torus": 3}
+JACOBIAN = {"fd": 0, "exact": 1}
+SOLVE = {"converged": 0, "fail": 1, "beyond_tol": 2, "backtrack": 3}
 
 
 class KhbFloors(C.Structure):
@@ -67,6 +71,20 @@ class KhbFields(C.Structure):
     _fields_ = [("v", C.c_void_p * MAX_VARS)]
 
 
+class KhbEmhdParams(C.Structure):
+    _fields_ = [("closure", C.c_int32), ("higher_order_terms", C.c_int32), ("feedback", C.c_int32),
+                ("conduction", C.c_int32), ("viscosity", C.c_int32), ("pad", C.c_int32),
+                ("tau", C.c_double), ("conduction_alpha", C.c_double), ("viscosity_alpha", C.c_double),
+                ("kappa", C.c_double), ("eta", C.c_double)]
+
+
+class KhbImplicitParams(C.Structure):
+    _fields_ = [("min_nonlinear_iter", C.c_int32), ("max_nonlinear_iter", C.c_int32), ("use_qr", C.c_int32),
+                ("linesearch", C.c_int32), ("max_linesearch_iter", C.c_int32), ("jacobian", C.c_int32),
+                ("jacobian_delta", C.c_double), ("rootfind_tol", C.c_double),
+                ("linesearch_eps", C.c_double), ("linesearch_lambda", C.c_double)]
+
+
 # Every entry point declared in include/khb.h, with its ctypes signature
 _P = C.c_void_p
 _D = C.c_double
@@ -101,6 +119,18 @@ SIGNATURES = {
     "khb_set_tuning": (_I, [_P, C.c_char_p, _I]),
     "khb_max_divb_noalloc": (_I, [C.POINTER(KhbConfig), C.POINTER(KhbFields), _P, _P]),
     "khb_noalloc_last_error": (C.c_char_p, []),
+    "khb_build_connection": (_I, [C.POINTER(KhbCoords), C.POINTER(KhbConfig), _D, _D, _D, _P]),
+    "khb_set_connection": (_I, [_P, _P]),
+    "khb_emhd_ptou": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
+    "khb_emhd_add_source": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
+    "khb_implicit_step": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbImplicitParams), C.POINTER(KhbFields),
+                               C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
+                               C.POINTER(KhbFields), _P, _P, _D, _P]),
+    "khb_implicit_stats": (_I, [_P, C.POINTER(C.c_int32), _P, _P]),
+    "khb_implicit_jacobian": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbImplicitParams),
+                                   C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
+                                   C.POINTER(KhbFields), C.POINTER(KhbFields), _D, _P, _P, _P]),
+    "khb_fix_solve": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P]),
 }
 
 _lib = None

@@ -7,6 +7,7 @@ Translation units and their arithmetic flags:
   khb_fp32.cu      FP32-flux form (fluxes, EMFs in FP32)           FMA contraction on
   khb_api.cu       host side and C ABI
   khb_noalloc.cu   khb_max_divb_noalloc (static device scratch)   -fmad=false
+  khb_emhd.cu      EMHD sources and the implicit Newton solve      -fmad=false
   khb_geometry.cpp host construction of the geometry tables
 The library is a plain shared object; the Python layer binds it with ctypes.
 """
@@ -23,6 +24,7 @@ UNITS = {
     "khb_fp32.cu": [],
     "khb_api.cu": [],
     "khb_noalloc.cu": ["-fmad=false"],
+    "khb_emhd.cu": ["-fmad=false"],
     "khb_geometry.cpp": [],
 }
 HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", os.path.join("..", "..", "include", "khb.h")]

@@ -30,6 +30,11 @@ struct khb_ctx {
     int64_t launches;
     unsigned long long dbl_max_bits;   // host source of the reduction reset (outlives async copies)
     int zone_split;        // 1: run the zone pass as two kernels (update; inversion+floors+P->U)
+    // EMHD / implicit solve
+    double* conn_d;        // connection Gamma^lam_{mu nu}, [64][n2][n1] with index lam*16 + mu*4 + nu
+    double* emhd_tmp;      // EMHD::AddSource temporaries u_mu, Theta: [5][N]
+    double* fix_buf;       // FixSolve replacement values: [7][N]
+    unsigned long long* imp_words;   // implicit-solve reductions, IMP_WORDS entries
 };
 
 namespace {
@@ -332,6 +337,7 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     if (e == cudaSuccess) e = alloc((void**)&c->words, sizeof(unsigned long long) * 4);
     if (e == cudaSuccess) e = alloc((void**)&c->fail_count, sizeof(int) * 4);
     if (e == cudaSuccess) e = alloc((void**)&c->fail_list, sizeof(int) * N);
+    if (e == cudaSuccess) e = alloc((void**)&c->imp_words, sizeof(unsigned long long) * IMP_WORDS);
     if (e != cudaSuccess) {
         khb_destroy(c);
         return fail(KHB_ERR_CUDA, std::string("khb_create: ") + cudaGetErrorString(e));
@@ -347,6 +353,7 @@ int khb_destroy(khb_ctx* c)
     cudaFree(c->emf); cudaFree(c->stageP); cudaFree(c->stageU);
     cudaFree(c->words); cudaFree(c->fail_count); cudaFree(c->fail_list);
     cudaFree(c->geo_d); cudaFree(c->geo_f);
+    cudaFree(c->conn_d); cudaFree(c->emhd_tmp); cudaFree(c->fix_buf); cudaFree(c->imp_words);
     delete c;
     return KHB_OK;
 }
@@ -641,5 +648,157 @@ int khb_set_tuning(khb_ctx* ctx, const char* key, int value)
 }
 
 int64_t khb_launch_count(khb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+// ---------------------------------------------------------------------------- EMHD and implicit solve
+static int check_emhd(const khb_emhd_params* e)
+{
+    if (!e) return fail(KHB_ERR_ARG, "EMHD parameters are NULL");
+    if (e->closure < KHB_CLOSURE_CONSTANT || e->closure > KHB_CLOSURE_TORUS) return fail(KHB_ERR_ARG, "unknown EMHD closure");
+    return KHB_OK;
+}
+
+static int check_fields10(const khb_emhd_params* e, const khb_fields* f, const char* name)
+{
+    if (!f) return fail(KHB_ERR_ARG, std::string(name) + " is NULL");
+    for (int p = 0; p < 8; ++p)
+        if (!f->v[p]) return fail(KHB_ERR_ARG, std::string(name) + " has a NULL variable pointer");
+    if (e->conduction && !f->v[KHB_Q]) return fail(KHB_ERR_ARG, std::string(name) + ": q slot is NULL with conduction on");
+    if (e->viscosity && !f->v[KHB_DP]) return fail(KHB_ERR_ARG, std::string(name) + ": dP slot is NULL with viscosity on");
+    return KHB_OK;
+}
+
+int khb_set_connection(khb_ctx* ctx, const double* conn)
+{
+    KHB_NEED_GEOM(ctx);
+    if (!conn) return fail(KHB_ERR_ARG, "khb_set_connection: NULL argument");
+    const Dims& d = ctx->d;
+    const size_t n2n1 = (size_t)d.n2 * d.n1, N = (size_t)d.N;
+    std::vector<double> h(64 * n2n1);
+    for (size_t x = 0; x < n2n1; ++x)
+        for (int m = 0; m < 64; ++m) h[m*n2n1 + x] = conn[x*64 + m];
+    if (!ctx->conn_d) {
+        KHB_CUDA(cudaMalloc((void**)&ctx->conn_d, h.size() * sizeof(double)));
+        KHB_CUDA(cudaMalloc((void**)&ctx->emhd_tmp, 5 * N * sizeof(double)));
+        KHB_CUDA(cudaMalloc((void**)&ctx->fix_buf, 7 * N * sizeof(double)));
+        KHB_CUDA(cudaMemset(ctx->emhd_tmp, 0, 5 * N * sizeof(double)));
+        KHB_CUDA(cudaMemset(ctx->fix_buf, 0, 7 * N * sizeof(double)));
+    }
+    KHB_CUDA(cudaMemcpy(ctx->conn_d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return KHB_OK;
+}
+
+int khb_emhd_ptou(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* U, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_emhd(emhd)) || (rc = check_fields10(emhd, P, "P")) || (rc = check_fields10(emhd, U, "U"))) return rc;
+    if (ctx->nv != 8) return fail(KHB_ERR_UNSUPPORTED, "khb_emhd_ptou: the block must carry B (nvar = 8)");
+    LaunchEmhd::ptou(ctx->d, ctx->g, ctx->ph.gam, *emhd, *P, *U, S(stream));
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+int khb_emhd_add_source(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* dUdt,
+                        void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_emhd(emhd)) || (rc = check_fields10(emhd, P, "P")) || (rc = check_fields10(emhd, dUdt, "dUdt")))
+        return rc;
+    if (!ctx->conn_d) return fail(KHB_ERR_STATE, "khb_emhd_add_source: connection not set (call khb_set_connection)");
+    if (ctx->nv != 8) return fail(KHB_ERR_UNSUPPORTED, "khb_emhd_add_source: the block must carry B (nvar = 8)");
+    if (!(emhd->conduction || emhd->viscosity)) return KHB_OK;
+    LaunchEmhd::add_source(ctx->d, ctx->g, ctx->conn_d, ctx->ph.gam, *emhd, ctx->ph, *P, ctx->emhd_tmp, *dUdt,
+                           S(stream));
+    ctx->launches += 1;
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+static int implicit_args(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp,
+                         const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub,
+                         const khb_fields* src, const khb_fields* P_solver, ImpFields& f)
+{
+    int rc;
+    if ((rc = check_emhd(emhd))) return rc;
+    if (!imp) return fail(KHB_ERR_ARG, "implicit parameters are NULL");
+    if (imp->max_nonlinear_iter < 1 || imp->max_nonlinear_iter > IMP_MAX_ITER)
+        return fail(KHB_ERR_ARG, "max_nonlinear_iter must be in [1, 64]");
+    if (imp->max_linesearch_iter < 0 || imp->max_linesearch_iter > 1000)
+        return fail(KHB_ERR_ARG, "max_linesearch_iter must be in [0, 1000]");
+    if (imp->jacobian != KHB_JACOBIAN_FD && imp->jacobian != KHB_JACOBIAN_EXACT)
+        return fail(KHB_ERR_ARG, "unknown Jacobian kind");
+    if (ctx->nv != 8) return fail(KHB_ERR_UNSUPPORTED, "implicit solve: the block must carry B (nvar = 8)");
+    if ((rc = check_fields10(emhd, P_full, "P_full")) || (rc = check_fields10(emhd, U_full, "U_full")) ||
+        (rc = check_fields10(emhd, P_sub, "P_sub")) || (rc = check_fields10(emhd, src, "src")) ||
+        (rc = check_fields10(emhd, P_solver, "P_solver")))
+        return rc;
+    f.Pf = *P_full; f.Uf = *U_full; f.Ps = *P_sub; f.S = *src; f.Psol = *P_solver;
+    return KHB_OK;
+}
+
+int khb_implicit_step(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp,
+                      const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub,
+                      const khb_fields* src, const khb_fields* P_solver, double* solve_norm, double* solve_fail,
+                      double dt, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    ImpFields f;
+    int rc;
+    if ((rc = implicit_args(ctx, emhd, imp, P_full, U_full, P_sub, src, P_solver, f))) return rc;
+    if (!solve_norm || !solve_fail) return fail(KHB_ERR_ARG, "khb_implicit_step: NULL solve_norm/solve_fail");
+    f.solve_norm = solve_norm;
+    f.solve_fail = solve_fail;
+    KHB_CUDA(cudaMemsetAsync(ctx->imp_words, 0, sizeof(unsigned long long) * IMP_WORDS, S(stream)));
+    for (int iter = 1; iter <= imp->max_nonlinear_iter; ++iter) {
+        LaunchEmhd::implicit_iter(ctx->d, ctx->g, ctx->ph.gam, *emhd, *imp, f, dt, ctx->imp_words, iter, S(stream));
+        KHB_LAUNCHED(ctx);
+    }
+    return KHB_OK;
+}
+
+int khb_implicit_stats(khb_ctx* ctx, int32_t* iterations, double* max_norms, void* stream)
+{
+    if (!ctx || !iterations) return fail(KHB_ERR_ARG, "khb_implicit_stats: NULL argument");
+    unsigned long long w[IMP_WORDS];
+    KHB_CUDA(cudaMemcpyAsync(w, ctx->imp_words, sizeof(w), cudaMemcpyDeviceToHost, S(stream)));
+    KHB_CUDA(cudaStreamSynchronize(S(stream)));
+    *iterations = (int32_t)w[IMP_ITER_WORD];
+    if (max_norms)
+        for (int it = 0; it < *iterations; ++it) std::memcpy(max_norms + it, w + it, sizeof(double));
+    return KHB_OK;
+}
+
+int khb_implicit_jacobian(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp,
+                          const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub,
+                          const khb_fields* src, const khb_fields* P_solver, double dt, double* jacobian,
+                          double* residual, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    ImpFields f;
+    int rc;
+    if ((rc = implicit_args(ctx, emhd, imp, P_full, U_full, P_sub, src, P_solver, f))) return rc;
+    if (!jacobian || !residual) return fail(KHB_ERR_ARG, "khb_implicit_jacobian: NULL output");
+    f.solve_norm = nullptr;
+    f.solve_fail = nullptr;
+    LaunchEmhd::implicit_jacobian(ctx->d, ctx->g, ctx->ph.gam, *emhd, *imp, f, dt, jacobian, residual, S(stream));
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+int khb_fix_solve(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* U,
+                  const double* solve_fail, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_emhd(emhd)) || (rc = check_fields10(emhd, P, "P")) || (rc = check_fields10(emhd, U, "U"))) return rc;
+    if (!solve_fail) return fail(KHB_ERR_ARG, "khb_fix_solve: NULL solve_fail");
+    if (!ctx->fix_buf) return fail(KHB_ERR_STATE, "khb_fix_solve: EMHD scratch not allocated (call khb_set_connection)");
+    if (ctx->nv != 8) return fail(KHB_ERR_UNSUPPORTED, "khb_fix_solve: the block must carry B (nvar = 8)");
+    LaunchEmhd::fix_solve(ctx->d, ctx->g, ctx->ph.gam, *emhd, *P, *U, solve_fail, ctx->fix_buf, S(stream));
+    ctx->launches += 1;
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
 
 } // extern "C"

@@ -243,3 +243,26 @@ extern "C" int khb_build_geometry(const khb_coords* coords, const khb_config* cf
     }
     return KHB_OK;
 }
+
+// The connection itself at zone centres (conn_direct, gr_coordinates.cpp:156-161): 0 + conn/1 with
+// connection_average_points = 1, i.e. the centred-difference value unchanged.
+extern "C" int khb_build_connection(const khb_coords* coords, const khb_config* cfg,
+                                    double x1min, double x2min, double x3min, double* conn)
+{
+    if (!coords || !cfg || !conn) return KHB_ERR_ARG;
+    const System S(*coords);
+    const int ng = cfg->ng;
+    const int n1 = cfg->nx1 + 2*ng;
+    const int n2 = (cfg->nx2 > 1) ? cfg->nx2 + 2*ng : 1;
+    const int g2 = (cfg->nx2 > 1) ? ng : 0, g3 = (cfg->nx3 > 1) ? ng : 0;
+    const double o1 = x1min - ng*cfg->dx1, o2 = x2min - g2*cfg->dx2, o3 = x3min - g3*cfg->dx3;
+    for (int j = 0; j < n2; ++j) for (int i = 0; i < n1; ++i) {
+        double X[4] = {0., o1 + (i + 0.5)*cfg->dx1, o2 + (j + 0.5)*cfg->dx2, o3 + (0 + 0.5)*cfg->dx3};
+        double cn[4][4][4];
+        connection(S, X, 1.e-8, cn);
+        const long long q = ((long long)j*n1 + i)*64;
+        for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) for (int c = 0; c < 4; ++c)
+            conn[q + a*16 + b*4 + c] = cn[a][b][c];
+    }
+    return KHB_OK;
+}

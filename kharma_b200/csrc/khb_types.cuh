@@ -101,6 +101,35 @@ struct LaunchCommon {
                      unsigned long long* word, cudaStream_t st);
 };
 
+// EMHD and implicit-solve parameters are passed to the kernels as the C-ABI structs themselves
+typedef khb_emhd_params EmhdArgs;
+typedef khb_implicit_params ImplicitArgs;
+
+// Device fields of one implicit solve (all [10 slots][N] like khb_fields)
+struct ImpFields {
+    khb_fields Pf, Uf, Ps, S, Psol;
+    double* solve_norm;
+    double* solve_fail;
+};
+
+// Reduction words of the implicit solve: [it-1] maximum solve_norm of iteration it (bit pattern),
+// [IMP_ITER_WORD] iterations taken
+enum { IMP_MAX_ITER = 64, IMP_ITER_WORD = 64, IMP_WORDS = 65 };
+
+struct LaunchEmhd {
+    static void ptou(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,
+                     const khb_fields& U, cudaStream_t st);
+    static void add_source(const Dims& d, const DevGeom& g, const double* conn, double gam, const EmhdArgs& E,
+                           const Phys& ph, const khb_fields& P, double* tmp, const khb_fields& dUdt, cudaStream_t st);
+    static void implicit_iter(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const ImplicitArgs& ip,
+                              const ImpFields& f, double dt, unsigned long long* words, int iter, cudaStream_t st);
+    static void implicit_jacobian(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E,
+                                  const ImplicitArgs& ip, const ImpFields& f, double dt, double* jac, double* res,
+                                  cudaStream_t st);
+    static void fix_solve(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,
+                          const khb_fields& U, const double* solve_fail, double* scratch, cudaStream_t st);
+};
+
 inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 // Validate a khb_config and derive the block index ranges and physics parameters (no allocation).

@@ -250,3 +250,56 @@ def _bsq(P, gcov, gcon):
     bcon = np.stack([b0] + [(P[5 + v] + b0 * ucon[1 + v]) / ucon[0] for v in range(3)])
     bcov = np.einsum("...mn,n...->m...", g, bcon)
     return np.sum(bcon * bcov, axis=0)
+
+
+def conducting_atmosphere(spec, geom, emhd, profile, jitter=1e-3, seed=1234, B10=1.0):
+    """Hydrostatic conducting atmosphere in Schwarzschild/MKS (prob/emhd/conducting_atmosphere.cpp:52-240).
+
+    profile: dict with the radial ODE solution arrays 'rCoords', 'rho', 'u', 'phi', one entry per
+    radial zone including ghosts (the reference reads them from atmosphere_soln_*.txt).  The fluid
+    is at rest with respect to the normal observer (u^mu = (1/sqrt(-g_00), 0, 0, 0)), q = phi
+    converted to q~ by the higher-order-terms scaling, dP~ = 0, and a monopole field
+    B^1 = B10 / r^3 (prob/seed_B.hpp:155-158).  rho, u and q~ are then multiplied by
+    (1 + jitter * U(-1, 1)) from a seeded PCG64 stream.  Returns P with 10 slots
+    (rho, u, u1-u3, B1-B3, q~, dP~) over the entire block.
+    """
+    n3, n2, n1 = spec.shape
+    gam = spec.gam
+    rc = np.asarray(geom["r_center"])[:, :n1]                    # (n2, n1)
+    if len(profile["rCoords"]) != n1 or np.max(np.abs(rc - profile["rCoords"][None, :])) > 1e-10:
+        raise ValueError("atmosphere profile does not match the grid radii")
+    gcov = np.asarray(geom["gcov"])[3, :n2, :n1]
+    gcon = np.asarray(geom["gcon"])[3, :n2, :n1]
+    rho = np.broadcast_to(profile["rho"][None, :], (n2, n1))
+    u = np.broadcast_to(profile["u"][None, :], (n2, n1))
+    q = np.broadcast_to(profile["phi"][None, :], (n2, n1)).copy()
+    ucon0 = 1.0 / np.sqrt(-gcov[..., 0, 0])
+    alpha2 = -1.0 / gcon[..., 0, 0]
+    uprim = [ucon0 * alpha2 * gcon[..., 0, 1 + v] for v in range(3)]
+    if emhd.higher_order_terms:
+        Theta = (gam - 1.) * u / rho
+        # EMHD::set_parameters with q = dP = bsq = 0 (emhd.hpp:179-261)
+        cs2 = gam * (gam - 1.) * u / (rho + gam * u)
+        if emhd.closure_type == "kappa_eta":
+            tau, chi = emhd.tau, emhd.kappa / np.maximum(rho, 1e-20)
+        elif emhd.closure_type == "constant":
+            tau, chi = emhd.tau, np.full_like(rho, emhd.conduction_alpha)
+        elif emhd.closure_type in ("soundspeed", "sound_speed"):
+            tau = emhd.tau
+            chi = emhd.conduction_alpha * cs2 * tau
+        else:
+            tau = np.sqrt(rc ** 3)
+            cs2 = np.maximum(cs2, 1e-20)
+            max_alpha = (1 - cs2) / (2 * cs2 + 1.e-12)
+            chi = np.minimum(max_alpha, emhd.conduction_alpha) * cs2 * tau
+        q = q * np.where(chi != 0, np.sqrt(tau / (chi * rho * Theta * Theta)), 0.0)
+    P = np.zeros((10, n3, n2, n1))
+    P[0], P[1], P[8] = rho[None], u[None], q[None]
+    for v in range(3):
+        P[2 + v] = uprim[v][None]
+    P[5] = (B10 / rc ** 3)[None]
+    if jitter:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        for plane in (0, 1, 8):
+            P[plane] *= 1.0 + jitter * rng.uniform(-1.0, 1.0, size=P[plane].shape)
+    return P

@@ -192,3 +192,68 @@ def torus_spec(n1, n2, n3, r_out=1000.0, a=0.9375, recon="linear_mc", precision=
                      floors=FloorSpec(rho_min_geom=1e-6, u_min_geom=1e-8, bsq_over_rho_max=100.0,
                                       u_over_rho_max=2.0),
                      driver=driver)
+
+
+@dataclass
+class EmhdSpec:
+    """EMHD package options (emhd/emhd.cpp:60-130).  Defaults are the reference's GetOrAdd defaults."""
+    closure_type: str = "torus"
+    higher_order_terms: bool = False
+    feedback: bool = True
+    conduction: bool = True
+    viscosity: bool = True
+    tau: float = 1.0
+    conduction_alpha: float = 1.0
+    viscosity_alpha: float = 1.0
+    kappa: float = 1.0
+    eta: float = 1.0
+
+    @property
+    def nfvar(self):
+        """Implicitly evolved variables: rho, u, u1-u3, then q and dP when present."""
+        return 5 + int(self.conduction) + int(self.viscosity)
+
+    def to_struct(self):
+        s = _lib.KhbEmhdParams()
+        s.closure = _lib.CLOSURE[self.closure_type]
+        s.higher_order_terms, s.feedback = int(self.higher_order_terms), int(self.feedback)
+        s.conduction, s.viscosity = int(self.conduction), int(self.viscosity)
+        s.tau, s.conduction_alpha, s.viscosity_alpha = self.tau, self.conduction_alpha, self.viscosity_alpha
+        s.kappa, s.eta = self.kappa, self.eta
+        return s
+
+
+@dataclass
+class ImplicitSpec:
+    """Implicit package options (implicit/implicit.cpp:99-119); jacobian selects the reference's
+    forward-difference Jacobian ("fd") or the exact tangent Jacobian ("exact")."""
+    min_nonlinear_iter: int = 1
+    max_nonlinear_iter: int = 3
+    jacobian_delta: float = 4e-8
+    rootfind_tol: float = 1e-12
+    use_qr: bool = True
+    linesearch: bool = True
+    max_linesearch_iter: int = 3
+    linesearch_eps: float = 1e-4
+    linesearch_lambda: float = 1.0
+    jacobian: str = "fd"
+
+    def to_struct(self):
+        s = _lib.KhbImplicitParams()
+        s.min_nonlinear_iter, s.max_nonlinear_iter = self.min_nonlinear_iter, self.max_nonlinear_iter
+        s.use_qr, s.linesearch, s.max_linesearch_iter = int(self.use_qr), int(self.linesearch), self.max_linesearch_iter
+        s.jacobian = _lib.JACOBIAN[self.jacobian]
+        s.jacobian_delta, s.rootfind_tol = self.jacobian_delta, self.rootfind_tol
+        s.linesearch_eps, s.linesearch_lambda = self.linesearch_eps, self.linesearch_lambda
+        return s
+
+
+def atmosphere_spec(n1, n2, n3, r_in=200.0, r_out=300.0):
+    """Conducting-atmosphere geometry (tests/conducting_atmosphere/conducting_atmosphere.par):
+    Schwarzschild (KS, a = 0) in MKS with hslope = 1, r in [r_in, r_out], gamma 4/3, WENO5/LLF.
+    Boundaries are not part of the implicit operator; outflow/reflecting/periodic are set."""
+    return BlockSpec(nx1=n1, nx2=n2, nx3=n3, x1min=math.log(r_in), x1max=math.log(r_out),
+                     x2min=0.0, x2max=1.0, x3min=0.0, x3max=2 * math.pi, gam=4.0 / 3.0, nvar=8,
+                     recon="weno5", riemann="llf", base="spherical_ks", transform="mks", a=0.0, hslope=1.0,
+                     bc=("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"),
+                     floors_on=False, driver="kharma")

@@ -1424,6 +1424,716 @@ static void stage(const Block& B, Fields& f, int s, double dt,
     finish_stage(B, P_n, U_n);
 }
 
+// ======================================================================== EMHD and the implicit solve
+// Extended GRMHD (emhd/) and the per-zone Newton solve (implicit/).  Zone state for these
+// functions is a 10-slot array: rho, u, u1..u3, B1..B3 (slots 0-7 as above), q~ (8), dP~ (9).
+// Field arrays are [10][N] in the same slot order.
+static const int IQ = 8, IDP = 9, NVE = 10;
+
+enum Closure { CL_CONSTANT = 0, CL_SOUNDSPEED = 1, CL_KAPPA_ETA = 2, CL_TORUS = 3 };   // emhd.hpp:58
+struct EmhdParams {            // emhd.hpp:60-84 plus the package switches of emhd.cpp:60-72
+    int32_t type, higher_order_terms, feedback, conduction, viscosity, pad;
+    double tau, conduction_alpha, viscosity_alpha, kappa, eta;
+};
+struct ImplicitParams {        // implicit.cpp:99-119 (jacobian: 0 finite difference, 1 exact)
+    int32_t min_nonlinear_iter, max_nonlinear_iter, use_qr, linesearch, max_linesearch_iter, jacobian;
+    double jacobian_delta, rootfind_tol, linesearch_eps, linesearch_lambda;
+};
+enum { SOLVE_CONVERGED = 0, SOLVE_FAIL = 1, SOLVE_BEYOND_TOL = 2, SOLVE_BACKTRACK = 3 };   // implicit.hpp:63-69
+
+// The implicitly evolved variables in the reference's pack order (Implicit::GetOrderedNames,
+// implicit.cpp:64-83: implicit-flagged first): rho, u, uvec, then q and dP when present.
+static int implicit_map(const EmhdParams& ep, int map[7])
+{
+    int n = 0;
+    for (int p = 0; p < 5; ++p) map[n++] = p;
+    if (ep.conduction) map[n++] = IQ;
+    if (ep.viscosity) map[n++] = IDP;
+    return n;
+}
+
+// Forward-mode dual number with NDIR tangent directions.  The oracle's exact Jacobian is the
+// residual below evaluated on Dual inputs seeded with unit vectors; the value part performs
+// the same IEEE operations as the plain double evaluation.
+static const int NDIR = 7;
+struct Dual {
+    double v, d[NDIR];
+    Dual() : v(0.) { for (int k = 0; k < NDIR; ++k) d[k] = 0.; }
+    Dual(double x) : v(x) { for (int k = 0; k < NDIR; ++k) d[k] = 0.; }
+};
+static inline Dual operator+(const Dual& a, const Dual& b) { Dual r(a.v + b.v); for (int k = 0; k < NDIR; ++k) r.d[k] = a.d[k] + b.d[k]; return r; }
+static inline Dual operator-(const Dual& a, const Dual& b) { Dual r(a.v - b.v); for (int k = 0; k < NDIR; ++k) r.d[k] = a.d[k] - b.d[k]; return r; }
+static inline Dual operator-(const Dual& a) { Dual r(-a.v); for (int k = 0; k < NDIR; ++k) r.d[k] = -a.d[k]; return r; }
+static inline Dual operator*(const Dual& a, const Dual& b)
+{ Dual r(a.v * b.v); for (int k = 0; k < NDIR; ++k) r.d[k] = a.d[k]*b.v + a.v*b.d[k]; return r; }
+static inline Dual operator/(const Dual& a, const Dual& b)
+{ Dual r(a.v / b.v); for (int k = 0; k < NDIR; ++k) r.d[k] = (a.d[k]*b.v - a.v*b.d[k]) / (b.v*b.v); return r; }
+static inline Dual operator+(const Dual& a, double b) { Dual r(a); r.v = a.v + b; return r; }
+static inline Dual operator+(double a, const Dual& b) { Dual r(b); r.v = a + b.v; return r; }
+static inline Dual operator-(const Dual& a, double b) { Dual r(a); r.v = a.v - b; return r; }
+static inline Dual operator-(double a, const Dual& b) { Dual r(a - b.v); for (int k = 0; k < NDIR; ++k) r.d[k] = -b.d[k]; return r; }
+static inline Dual operator*(const Dual& a, double b) { Dual r(a.v * b); for (int k = 0; k < NDIR; ++k) r.d[k] = a.d[k]*b; return r; }
+static inline Dual operator*(double a, const Dual& b) { Dual r(a * b.v); for (int k = 0; k < NDIR; ++k) r.d[k] = a*b.d[k]; return r; }
+static inline Dual operator/(const Dual& a, double b) { Dual r(a.v / b); for (int k = 0; k < NDIR; ++k) r.d[k] = a.d[k]/b; return r; }
+static inline Dual operator/(double a, const Dual& b)
+{ Dual r(a / b.v); for (int k = 0; k < NDIR; ++k) r.d[k] = -a*b.d[k]/(b.v*b.v); return r; }
+static inline Dual& operator+=(Dual& a, const Dual& b) { a = a + b; return a; }
+static inline Dual& operator-=(Dual& a, const Dual& b) { a = a - b; return a; }
+static inline Dual& operator*=(Dual& a, const Dual& b) { a = a * b; return a; }
+static inline Dual& operator+=(Dual& a, double b) { a = a + b; return a; }
+static inline Dual& operator-=(Dual& a, double b) { a = a - b; return a; }
+static inline Dual& operator*=(Dual& a, double b) { a = a * b; return a; }
+static inline double tval(double x) { return x; }
+static inline double tval(const Dual& x) { return x.v; }
+static inline double tsqrt(double x) { return std::sqrt(x); }
+static inline Dual tsqrt(const Dual& a)
+{ Dual r(std::sqrt(a.v)); for (int k = 0; k < NDIR; ++k) r.d[k] = a.d[k] / (2. * r.v); return r; }
+// m::max(x, c) with a constant c: derivative of the selected branch
+template <class T> static inline T tmax(const T& x, double c) { return (tval(x) < c) ? T(c) : x; }
+
+template <class T> struct FV { T ucon[4], ucov[4], bcon[4], bcov[4]; };
+template <class T> static inline T tdot(const T* a, const T* b) { return a[0]*b[0] + a[1]*b[1] + a[2]*b[2] + a[3]*b[3]; }
+
+// GRMHD::calc_ucon at the zone centre (grmhd_functions.hpp:121-133, 282-291)
+template <class T>
+static void calc_ucon_t(const Block& B, const T* P, int j, int i, T ucon[4])
+{
+    const int loc = center;
+    const T qsq = B.Gcov(loc, j, i, 1, 1) * P[2] * P[2] +
+                  B.Gcov(loc, j, i, 2, 2) * P[3] * P[3] +
+                  B.Gcov(loc, j, i, 3, 3) * P[4] * P[4] +
+                  2. * (B.Gcov(loc, j, i, 1, 2) * P[2] * P[3] +
+                        B.Gcov(loc, j, i, 1, 3) * P[2] * P[4] +
+                        B.Gcov(loc, j, i, 2, 3) * P[3] * P[4]);
+    const T gamma = tsqrt(1. + qsq);
+    const double alpha = 1. / std::sqrt(-B.Gcon(loc, j, i, 0, 0));
+    ucon[0] = gamma / alpha;
+    for (int v = 0; v < 3; ++v) ucon[v+1] = P[2 + v] - gamma * alpha * B.Gcon(loc, j, i, 0, v+1);
+}
+// GRCoordinates::lower at the centre (gr_coordinates.hpp:227-232)
+template <class T>
+static void lower_t(const Block& B, const T* vcon, T* vcov, int j, int i)
+{
+    for (int mu = 0; mu < 4; ++mu) vcov[mu] = T(0.);
+    for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) vcov[mu] += B.Gcov(center, j, i, mu, nu) * vcon[nu];
+}
+// GRMHD::calc_4vecs at the centre with B (grmhd_functions.hpp:225-246)
+template <class T>
+static void calc_4vecs_t(const Block& B, const T* P, int j, int i, FV<T>& D)
+{
+    calc_ucon_t(B, P, j, i, D.ucon);
+    lower_t(B, D.ucon, D.ucov, j, i);
+    D.bcon[0] = T(0.);
+    for (int v = 0; v < 3; ++v) D.bcon[0] += P[5 + v] * D.ucov[v+1];
+    for (int v = 0; v < 3; ++v) D.bcon[v+1] = (P[5 + v] + D.bcon[0] * D.ucon[v+1]) / D.ucon[0];
+    lower_t(B, D.bcon, D.bcov, j, i);
+}
+
+// EMHD::set_parameters, scalar form (emhd.hpp:179-261)
+static void emhd_set_parameters(const Block& B, const EmhdParams& ep, double gam, double rho, double u,
+                                double qtilde, double dPtilde, double bsq, int j, int i,
+                                double& tau, double& chi_e, double& nu_e)
+{
+    if (ep.type == CL_CONSTANT) {
+        tau = ep.tau;
+        chi_e = ep.conduction_alpha;
+        nu_e = ep.viscosity_alpha;
+    } else if (ep.type == CL_SOUNDSPEED) {
+        const double cs2 = (gam * (gam - 1.) * u) / (rho + (gam * u));
+        tau = ep.tau;
+        chi_e = ep.conduction_alpha * cs2 * tau;
+        nu_e = ep.viscosity_alpha * cs2 * tau;
+    } else if (ep.type == CL_KAPPA_ETA) {
+        tau = ep.tau;
+        chi_e = ep.kappa / kmax(rho, SMALL);
+        nu_e = ep.eta / kmax(rho, SMALL);
+    } else {
+        const double r = B.rcen[(size_t)j*B.n1 + i];
+        const double tau_dyn = std::sqrt(r*r*r);
+        tau = tau_dyn;
+        const double pg = (gam - 1.) * u;
+        const double Theta = pg / rho;
+        const double cs2 = clip(gam * pg / (rho + (gam * u)), SMALL, 0./0.);
+        const double lambda = 0.01;
+        {
+            const double q = (ep.higher_order_terms)
+                ? qtilde * std::sqrt(rho * ep.conduction_alpha * cs2 * Theta * Theta) : qtilde;
+            const double q_max = ep.conduction_alpha * rho * cs2 * std::sqrt(cs2);
+            const double q_ratio = std::fabs(q) / q_max;
+            const double inv_exp_g = std::exp(-(q_ratio - 1.) / lambda);
+            const double f_fmin = inv_exp_g / (inv_exp_g + 1.) + 1.e-5;
+            tau = kmin(tau, f_fmin * tau_dyn);
+        }
+        {
+            const double dP = (ep.higher_order_terms)
+                ? dPtilde * std::sqrt(rho * ep.viscosity_alpha * cs2 * Theta) : dPtilde;
+            const double dP_comp_ratio = kmax(pg - 2./3. * dP, SMALL) / kmax(pg + 1./3. * dP, SMALL);
+            const double dP_max = (dP > 0.) ? kmin(0.5 * bsq * dP_comp_ratio, 1.49 * pg / 1.07)
+                                            : kmax(-bsq, -2.99 * pg / 1.07);
+            const double dP_ratio = std::fabs(dP) / (std::fabs(dP_max) + SMALL);
+            const double inv_exp_g = std::exp((1. - dP_ratio) / lambda);
+            const double f_fmin = inv_exp_g / (inv_exp_g + 1.) + 1.e-5;
+            tau = kmin(tau, f_fmin * tau_dyn);
+        }
+        const double max_alpha = (1 - cs2) / (2 * cs2 + 1.e-12);
+        chi_e = kmin(max_alpha, ep.conduction_alpha) * cs2 * tau;
+        nu_e = kmin(max_alpha, ep.viscosity_alpha) * cs2 * tau;
+    }
+}
+// EMHD::set_parameters on a zone's primitives (emhd.hpp:262-287)
+static void emhd_set_parameters_P(const Block& B, const EmhdParams& ep, double gam, const double* P, int j, int i,
+                                  double& tau, double& chi_e, double& nu_e)
+{
+    FV<double> D;
+    calc_4vecs_t(B, P, j, i, D);
+    const double bsq = kmax(tdot(D.bcon, D.bcov), SMALL);
+    const double qtilde = ep.conduction ? P[IQ] : 0.;
+    const double dPtilde = ep.viscosity ? P[IDP] : 0.;
+    emhd_set_parameters(B, ep, gam, P[0], P[1], qtilde, dPtilde, bsq, j, i, tau, chi_e, nu_e);
+}
+// EMHD::convert_prims_to_q_dP (emhd.hpp:313-332)
+template <class T>
+static void convert_prims_to_q_dP_t(const T& q_tilde, const T& dP_tilde, const T& rho, const T& Theta,
+                                    const T& cs2, const EmhdParams& ep, T& q, T& dP)
+{
+    q = q_tilde;
+    if (ep.higher_order_terms) {
+        if (ep.type == CL_KAPPA_ETA) q *= tsqrt(ep.kappa * Theta * Theta / ep.tau);
+        else                         q *= tsqrt(rho * ep.conduction_alpha * cs2 * Theta * Theta);
+    }
+    dP = dP_tilde;
+    if (ep.higher_order_terms) {
+        if (ep.type == CL_KAPPA_ETA) dP *= tsqrt(ep.eta * Theta / ep.tau);
+        else                         dP *= tsqrt(rho * ep.viscosity_alpha * cs2 * Theta);
+    }
+}
+// Flux::calc_tensor with the EMHD / GRMHD branches (flux_functions.hpp:80-107, emhd.hpp:296-309,
+// grmhd_functions.hpp:142-155)
+template <class T>
+static void calc_tensor_t(const EmhdParams& ep, double gam, const T* P, const FV<T>& D, int dir, T Tm[4])
+{
+    if ((ep.conduction || ep.viscosity) && ep.feedback) {
+        const T qtilde = ep.conduction ? P[IQ] : T(0.);
+        const T dPtilde = ep.viscosity ? P[IDP] : T(0.);
+        const T Theta = (gam - 1) * P[1] / P[0];
+        const T cs2 = gam * (gam - 1) * P[1] / (P[0] + gam * P[1]);
+        T q, dP;
+        convert_prims_to_q_dP_t(qtilde, dPtilde, P[0], Theta, cs2, ep, q, dP);
+        const T pgas = (gam - 1) * P[1];
+        const T bsq = tmax(tdot(D.bcon, D.bcov), SMALL);
+        const T b_mag = tsqrt(bsq);
+        const T eta = pgas + P[0] + P[1] + bsq;
+        const T ptot = pgas + 0.5 * bsq;
+        for (int mu = 0; mu < 4; ++mu)
+            Tm[mu] = eta * D.ucon[dir] * D.ucov[mu] + ptot * (double)(dir == mu) - D.bcon[dir] * D.bcov[mu]
+                   + (q / b_mag) * ((D.ucon[dir] * D.bcov[mu]) + (D.bcon[dir] * D.ucov[mu]))
+                   - dP * ((D.bcon[dir] * D.bcov[mu] / bsq) - (1./3.) * ((double)(dir == mu) + D.ucon[dir] * D.ucov[mu]));
+    } else {
+        const T pgas = (gam - 1) * P[1];
+        const T bsq = tdot(D.bcon, D.bcov);
+        const T eta = pgas + P[0] + P[1] + bsq;
+        const T ptot = pgas + 0.5 * bsq;
+        for (int mu = 0; mu < 4; ++mu)
+            Tm[mu] = eta * D.ucon[dir] * D.ucov[mu] + ptot * (double)(dir == mu) - D.bcon[dir] * D.bcov[mu];
+    }
+}
+// Flux::prim_to_flux for the 10-slot state at the centre (flux_functions.hpp:180-232)
+template <class T>
+static void prim_to_flux_t(const Block& B, const EmhdParams& ep, double gam, const T* P, const FV<T>& D,
+                           int j, int i, int dir, T* flux)
+{
+    const double gdet = B.Gdet(center, j, i);
+    flux[0] = P[0] * D.ucon[dir] * gdet;
+    T Tm[4];
+    calc_tensor_t(ep, gam, P, D, dir, Tm);
+    flux[1] = Tm[0] * gdet + flux[0];
+    flux[2] = Tm[1] * gdet;
+    flux[3] = Tm[2] * gdet;
+    flux[4] = Tm[3] * gdet;
+    if (dir == 0) {
+        for (int v = 0; v < 3; ++v) flux[5 + v] = P[5 + v] * gdet;
+    } else {
+        for (int v = 0; v < 3; ++v) flux[5 + v] = (D.bcon[v+1] * D.ucon[dir] - D.bcon[dir] * D.ucon[v+1]) * gdet;
+    }
+    if (ep.conduction) flux[IQ] = P[IQ] * D.ucon[dir] * gdet;
+    if (ep.viscosity) flux[IDP] = P[IDP] * D.ucon[dir] * gdet;
+}
+// EMHD::implicit_sources (emhd_sources.hpp:52-63)
+template <class T>
+static void implicit_sources_t(const Block& B, const EmhdParams& ep, const T* P, double tau, int j, int i,
+                               T& dUq, T& dUdP)
+{
+    if (ep.conduction) dUq = -B.Gdet(center, j, i) * (P[IQ] / tau);
+    if (ep.viscosity) dUdP = -B.Gdet(center, j, i) * (P[IDP] / tau);
+}
+// EMHD::time_derivative_sources (emhd_sources.hpp:69-128); P_new is the trial state
+template <class T>
+static void time_derivative_sources_t(const Block& B, const EmhdParams& ep, const T* P_new, const double* P_old,
+                                      const double* P, double tau, double chi_e, double nu_e,
+                                      const FV<double>& D, double gam, double dt, int j, int i, T& dUq, T& dUdP)
+{
+    const bool ho = ep.higher_order_terms;
+    const double bsq = kmax(tdot(D.bcon, D.bcov), SMALL);
+    const double mag_b = std::sqrt(bsq);
+    double ucon_o[4], ucov_old[4];
+    T ucon_n[4], ucov_new[4];
+    calc_ucon_t(B, P_old, j, i, ucon_o);
+    lower_t(B, ucon_o, ucov_old, j, i);
+    calc_ucon_t(B, P_new, j, i, ucon_n);
+    lower_t(B, ucon_n, ucov_new, j, i);
+    T dt_ucov[4];
+    for (int mu = 0; mu < 4; ++mu) dt_ucov[mu] = (ucov_new[mu] - ucov_old[mu]) / dt;
+    T div_ucon = T(0.);
+    for (int mu = 0; mu < 4; ++mu) div_ucon += B.Gcon(center, j, i, 0, mu) * dt_ucov[mu];
+    const T Theta_new = tmax((gam-1) * P_new[1] / P_new[0], SMALL);
+    const double Theta_old = kmax((gam-1) * P_old[1] / P_old[0], SMALL);
+    const T dt_Theta = (Theta_new - Theta_old) / dt;
+    const double rho = P[0];
+    const double Theta = (gam-1) * P[1] / P[0];
+    if (ep.conduction) {
+        const double qtilde = P[IQ];
+        T q0 = -rho * chi_e * (D.bcon[0] / mag_b) * dt_Theta;
+        for (int mu = 0; mu < 4; ++mu) q0 -= rho * chi_e * (D.bcon[mu] / mag_b) * Theta * D.ucon[0] * dt_ucov[mu];
+        T q0_tilde = q0;
+        if (ho) q0_tilde *= (chi_e != 0) ? std::sqrt(tau / (chi_e * rho * Theta * Theta)) : 0.0;
+        dUq = B.Gdet(center, j, i) * (q0_tilde / tau);
+        if (ho) dUq += B.Gdet(center, j, i) * (qtilde / 2.) * div_ucon;
+    }
+    if (ep.viscosity) {
+        const double dPtilde = P[IDP];
+        T dP0 = -rho * nu_e * div_ucon;
+        for (int mu = 0; mu < 4; ++mu) dP0 += 3. * rho * nu_e * (D.bcon[0] * D.bcon[mu] / bsq) * dt_ucov[mu];
+        T dP0_tilde = dP0;
+        if (ho) dP0_tilde *= (nu_e != 0) ? std::sqrt(tau / (nu_e * rho * Theta)) : 0.0;
+        dUdP = B.Gdet(center, j, i) * (dP0_tilde / tau);
+        if (ho) dUdP += B.Gdet(center, j, i) * (dPtilde / 2.) * div_ucon;
+    }
+}
+// Implicit::calc_residual (implicit.hpp:139-200).  Pi/Ui: full-step initial state; Ps: sub-step
+// initial state; src: flux divergence plus explicit sources; dUi: implicit sources of Pi.
+template <class T>
+static void calc_residual_t(const Block& B, const EmhdParams& ep, double gam, const T* Pt, const double* Pi,
+                            const double* Ui, const double* Ps, const double* src, const double* dUi,
+                            int nf, const int* map, int j, int i, double dt, T* res)
+{
+    T Utmp[NVE];
+    FV<T> Dt;
+    calc_4vecs_t(B, Pt, j, i, Dt);
+    prim_to_flux_t(B, ep, gam, Pt, Dt, j, i, 0, Utmp);
+    for (int ip = 0; ip < nf; ++ip) res[ip] = (Utmp[map[ip]] - Ui[map[ip]]) / dt - src[map[ip]];
+    if (ep.conduction || ep.viscosity) {
+        T throwaway;
+        T& rq = ep.conduction ? res[5] : throwaway;
+        T& rdP = ep.viscosity ? res[ep.conduction ? 6 : 5] : throwaway;
+        double tau, chi_e, nu_e;
+        emhd_set_parameters_P(B, ep, gam, Ps, j, i, tau, chi_e, nu_e);
+        FV<double> D;
+        calc_4vecs_t(B, Ps, j, i, D);
+        T dUq = T(0.), dUdP = T(0.);
+        implicit_sources_t(B, ep, Pt, tau, j, i, dUq, dUdP);
+        if (ep.conduction) rq -= 0.5*(dUq + dUi[IQ]);
+        if (ep.viscosity) rdP -= 0.5*(dUdP + dUi[IDP]);
+        emhd_set_parameters_P(B, ep, gam, Ps, j, i, tau, chi_e, nu_e);
+        time_derivative_sources_t(B, ep, Pt, Pi, Ps, tau, chi_e, nu_e, D, gam, dt, j, i, dUq, dUdP);
+        rq -= dUq;
+        rdP -= dUdP;
+        rq *= tau;
+        rdP *= tau;
+        if (ep.higher_order_terms) {
+            const double rho = Ps[0], uu = Ps[1];
+            const double Theta = (gam - 1.) * uu / rho;
+            rq *= (chi_e != 0) ? std::sqrt(rho * chi_e * tau * Theta * Theta) / tau : 1.;
+            rdP *= (nu_e != 0) ? std::sqrt(rho * nu_e * tau * Theta) / tau : 1.;
+        }
+    }
+}
+// Implicit sources of the full-step initial state, with tau from the sub-step state
+// (implicit.cpp:294-305)
+static void implicit_dU(const Block& B, const EmhdParams& ep, double gam, const double* Pfull, const double* Psub,
+                        int j, int i, double* dUi)
+{
+    dUi[IQ] = 0.; dUi[IDP] = 0.;
+    if (ep.conduction || ep.viscosity) {
+        double tau, chi_e, nu_e;
+        emhd_set_parameters_P(B, ep, gam, Psub, j, i, tau, chi_e, nu_e);
+        implicit_sources_t(B, ep, Pfull, tau, j, i, dUi[IQ], dUi[IDP]);
+    }
+}
+// Implicit::calc_jacobian, forward differences (implicit.hpp:208-255).  Ps_ is modified and restored.
+static void calc_jacobian_fd(const Block& B, const EmhdParams& ep, double gam, double delta, double* Psol,
+                             const double* Pi, const double* Ui, const double* Ps, const double* src,
+                             const double* dUi, int nf, const int* map, int j, int i, double dt,
+                             double* J, double* res)
+{
+    calc_residual_t<double>(B, ep, gam, Psol, Pi, Ui, Ps, src, dUi, nf, map, j, i, dt, res);
+    double rsave[7], Psave[NVE];
+    for (int ip = 0; ip < nf; ++ip) rsave[ip] = res[ip];
+    for (int p = 0; p < NVE; ++p) Psave[p] = Psol[p];
+    for (int col = 0; col < nf; ++col) {
+        const int pc = map[col];
+        if (std::fabs(Psave[pc]) < (0.5 * delta)) Psol[pc] = Psave[pc] + delta;
+        else Psol[pc] = (1 + delta) * Psave[pc];
+        calc_residual_t<double>(B, ep, gam, Psol, Pi, Ui, Ps, src, dUi, nf, map, j, i, dt, res);
+        for (int row = 0; row < nf; ++row)
+            J[row*nf + col] = (res[row] - rsave[row]) / (Psol[pc] - Psave[pc] + SMALL);
+        Psol[pc] = Psave[pc];
+    }
+    for (int ip = 0; ip < nf; ++ip) res[ip] = rsave[ip];
+}
+// Exact Jacobian of the same residual (not in the reference, whose Jacobian is only by finite
+// differences): forward mode over the nf implicit primitives.
+static void calc_jacobian_exact(const Block& B, const EmhdParams& ep, double gam, const double* Psol,
+                                const double* Pi, const double* Ui, const double* Ps, const double* src,
+                                const double* dUi, int nf, const int* map, int j, int i, double dt,
+                                double* J, double* res)
+{
+    Dual Pt[NVE], r[7];
+    for (int p = 0; p < NVE; ++p) Pt[p] = Dual(Psol[p]);
+    for (int col = 0; col < nf; ++col) Pt[map[col]].d[col] = 1.;
+    calc_residual_t<Dual>(B, ep, gam, Pt, Pi, Ui, Ps, src, dUi, nf, map, j, i, dt, r);
+    for (int row = 0; row < nf; ++row) {
+        res[row] = r[row].v;
+        for (int col = 0; col < nf; ++col) J[row*nf + col] = r[row].d[col];
+    }
+}
+// Linear solve J x = b by Householder QR with column pivoting, then Q^T b, back substitution
+// and the inverse permutation: KokkosBatched SerialQR (unblocked, with pivots), SerialApplyQ
+// (left, transpose), SerialTrsv (upper, non-unit) and SerialApplyPivot (left, backward) as
+// called at implicit.cpp:374-383 (external/kokkos-kernels, KokkosBatched_QR_Serial_Internal.hpp,
+// _Householder_Serial_Internal.hpp, _ApplyHouseholder_Serial_Internal.hpp,
+// _ApplyQ_Serial_Internal.hpp, _Trsv_Serial_Internal.hpp, _ApplyPivot_Internal.hpp,
+// _FindAmax_Internal.hpp).  A is row-major n x n and is overwritten by the factorisation.
+static void qr_solve(int n, double* A, double* b)
+{
+    double tau[7], norm[7], w[7];
+    int piv[7];
+    for (int c = 0; c < n; ++c) {
+        norm[c] = 0.;
+        for (int r = 0; r < n; ++r) norm[c] += A[r*n + c] * A[r*n + c];
+    }
+    for (int k = 0; k < n; ++k) {
+        int p = 0;
+        double mx = norm[k];
+        for (int c = 1; c < n - k; ++c) if (norm[k + c] > mx) { mx = norm[k + c]; p = c; }
+        piv[k] = p;
+        if (p != 0) {
+            std::swap(norm[k], norm[k + p]);
+            for (int r = 0; r < n; ++r) std::swap(A[r*n + k], A[r*n + k + p]);
+        }
+        const int m2 = n - k - 1;
+        double& chi1 = A[k*n + k];
+        double nx2 = 0.;
+        for (int r = 0; r < m2; ++r) { const double x = A[(k+1+r)*n + k]; nx2 += x * x; }
+        if (nx2 == 0.) {
+            chi1 = -chi1;
+            tau[k] = 0.5;
+        } else {
+            const double nchi1 = std::fabs(chi1);
+            const double nx = std::sqrt(nx2 + nchi1 * nchi1);
+            const double alpha = (chi1 < 0 ? 1. : -1.) * nx;
+            const double cma = chi1 - alpha;
+            const double inv = 1. / cma;
+            for (int r = 0; r < m2; ++r) A[(k+1+r)*n + k] *= inv;
+            const double cma2 = cma * cma;
+            tau[k] = 0.5 + 0.5 * (nx2 / cma2);
+            chi1 = alpha;
+        }
+        const double inv_tau = 1. / tau[k];
+        for (int c = 0; c < m2; ++c) {
+            double t = A[k*n + k+1+c];
+            for (int r = 0; r < m2; ++r) t += A[(k+1+r)*n + k] * A[(k+1+r)*n + k+1+c];
+            w[c] = t * inv_tau;
+        }
+        for (int c = 0; c < m2; ++c) A[k*n + k+1+c] -= w[c];
+        for (int c = 0; c < m2; ++c) for (int r = 0; r < m2; ++r) A[(k+1+r)*n + k+1+c] -= A[(k+1+r)*n + k] * w[c];
+        for (int c = 0; c < m2; ++c) norm[k+1+c] -= A[k*n + k+1+c] * A[k*n + k+1+c];
+    }
+    for (int k = 0; k < n; ++k) {
+        const int m2 = n - k - 1;
+        const double inv_tau = 1. / tau[k];
+        double t = b[k];
+        for (int r = 0; r < m2; ++r) t += A[(k+1+r)*n + k] * b[k+1+r];
+        const double wk = t * inv_tau;
+        b[k] -= wk;
+        for (int r = 0; r < m2; ++r) b[k+1+r] -= A[(k+1+r)*n + k] * wk;
+    }
+    for (int p = n - 1; p >= 0; --p) {
+        b[p] = b[p] / A[p*n + p];
+        for (int r = 0; r < p; ++r) b[r] -= A[r*n + p] * b[p];
+    }
+    for (int k = n - 1; k >= 0; --k) if (piv[k] != 0) std::swap(b[k], b[k + piv[k]]);
+}
+// The use_qr = false path: KokkosBatched SerialLU (no pivoting, diagonal nudged by tiny = SMALL)
+// followed by the upper-triangular solve only, exactly as implicit.cpp:387-401 calls them.
+static void lu_solve(int n, double* A, double* b)
+{
+    for (int p = 0; p < n; ++p) {
+        const double a_real = A[p*n + p];
+        A[p*n + p] += -SMALL * (double)(a_real < 0);
+        A[p*n + p] += SMALL * (double)(a_real >= 0);
+        const double a11 = A[p*n + p];
+        for (int r = 0; r < n - p - 1; ++r) {
+            A[(p+1+r)*n + p] /= a11;
+            for (int c = 0; c < n - p - 1; ++c) A[(p+1+r)*n + p+1+c] -= A[(p+1+r)*n + p] * A[p*n + p+1+c];
+        }
+    }
+    for (int p = n - 1; p >= 0; --p) {
+        b[p] = b[p] / A[p*n + p];
+        for (int r = 0; r < p; ++r) b[r] -= A[r*n + p] * b[p];
+    }
+}
+static inline void load10(const double* A, size_t N, size_t c, double* out)
+{
+    for (int p = 0; p < NVE; ++p) out[p] = A[(size_t)p*N + c];
+}
+// One Newton iteration of Implicit::Step for one zone (implicit.cpp:286-522: the jacobian,
+// solve and set-step kernels in sequence).  Psol is the zone's solver state, read and written.
+static void implicit_zone_iteration(const Block& B, const EmhdParams& ep, const ImplicitParams& ip, double gam,
+                                    const double* Pf, const double* Uf, const double* Ps, const double* S,
+                                    double* Psol, double& solve_norm, double& solve_fail, double dt, int j, int i)
+{
+    int map[7];
+    const int nf = implicit_map(ep, map);
+    if (solve_fail == SOLVE_FAIL) return;
+    solve_fail = SOLVE_CONVERGED;
+    double dUi[NVE] = {0};
+    implicit_dU(B, ep, gam, Pf, Ps, j, i, dUi);
+    double J[49], res[7], delta[7];
+    if (ip.jacobian == 1) calc_jacobian_exact(B, ep, gam, Psol, Pf, Uf, Ps, S, dUi, nf, map, j, i, dt, J, res);
+    else calc_jacobian_fd(B, ep, gam, ip.jacobian_delta, Psol, Pf, Uf, Ps, S, dUi, nf, map, j, i, dt, J, res);
+    for (int q = 0; q < nf; ++q) delta[q] = -res[q];
+    if (ip.use_qr) qr_solve(nf, J, delta);
+    else lu_solve(nf, J, delta);
+    // implicit_set_step (implicit.cpp:426-521)
+    double Pls[NVE];
+    for (int p = 0; p < NVE; ++p) Pls[p] = Psol[p];
+    double lambda = ip.linesearch_lambda;
+    if ((Psol[0] + lambda*delta[0] < 0.) || (Psol[1] + lambda*delta[1] < 0.)) {
+        solve_fail = SOLVE_BACKTRACK;
+        lambda = 0.1;
+    }
+    if ((Psol[0] + lambda*delta[0] < 0.) || (Psol[1] + lambda*delta[1] < 0.)) {
+        solve_fail = SOLVE_FAIL;
+        for (int q = 0; q < nf; ++q) Psol[map[q]] = Ps[map[q]];
+        return;
+    }
+    if (ip.linesearch) {
+        solve_norm = 0.;
+        for (int q = 0; q < nf; ++q) solve_norm += res[q]*res[q];
+        solve_norm = std::sqrt(solve_norm);
+        const double f0 = 0.5 * solve_norm;
+        const double fprime0 = -2. * f0;
+        for (int it = 0; it < ip.max_linesearch_iter; it++) {
+            for (int q = 0; q < nf; ++q) Pls[map[q]] = Psol[map[q]] + (lambda * delta[q]);
+            calc_residual_t<double>(B, ep, gam, Pls, Pf, Uf, Ps, S, dUi, nf, map, j, i, dt, res);
+            solve_norm = 0.;
+            for (int q = 0; q < nf; ++q) solve_norm += res[q]*res[q];
+            solve_norm = std::sqrt(solve_norm);
+            const double f1 = 0.5 * solve_norm;
+            const int condition = f1 > (f0 * (1. - ip.linesearch_eps * lambda) + SMALL);
+            const double denom = (f1 - f0 - (fprime0 * lambda)) * condition + (1 - condition);
+            const double lambda_new = -fprime0 * lambda * lambda / denom * 0.5;
+            lambda = lambda * (1 - condition) + (condition * lambda_new);
+            if (condition == 0) break;
+        }
+    }
+    for (int q = 0; q < nf; ++q) Psol[map[q]] += lambda * delta[q];
+    calc_residual_t<double>(B, ep, gam, Psol, Pf, Uf, Ps, S, dUi, nf, map, j, i, dt, res);
+    solve_norm = 0;
+    for (int q = 0; q < nf; ++q) solve_norm += res[q]*res[q];
+    solve_norm = std::sqrt(solve_norm);
+    if (std::isnan(solve_norm)) {
+        solve_fail = SOLVE_FAIL;
+        for (int q = 0; q < nf; ++q) Psol[map[q]] = Ps[map[q]];
+    } else if (solve_norm > ip.rootfind_tol) {
+        solve_fail = SOLVE_BEYOND_TOL;
+    }
+}
+// Implicit::Step over the block interior (implicit.cpp:159-571).  Arrays are [10][N].  Returns
+// the number of Newton iterations taken; maxnorm[iter-1] receives each iteration's maximum
+// solve_norm (the reduction of implicit.cpp:527-534; NaN norms are skipped as Kokkos::Max does).
+static int implicit_step(const Block& B, const EmhdParams& ep, const ImplicitParams& ip, double gam,
+                         const double* Pf, const double* Uf, const double* Ps, const double* S, double* Psol,
+                         double* solve_norm, double* solve_fail, double dt, double* maxnorm)
+{
+    const size_t N = B.N;
+    int iters = 0;
+    for (int iter = 1; iter <= ip.max_nonlinear_iter; ++iter) {
+        iters = iter;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+            const size_t c = B.id(k, j, i);
+            double pf[NVE], uf[NVE], ps[NVE], s[NVE], psol[NVE];
+            load10(Pf, N, c, pf); load10(Uf, N, c, uf); load10(Ps, N, c, ps); load10(S, N, c, s);
+            load10(Psol, N, c, psol);
+            implicit_zone_iteration(B, ep, ip, gam, pf, uf, ps, s, psol, solve_norm[c], solve_fail[c], dt, j, i);
+            for (int p = 0; p < NVE; ++p) Psol[(size_t)p*N + c] = psol[p];
+        }
+        double m = -std::numeric_limits<double>::max();
+        for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+            const double v = solve_norm[B.id(k, j, i)];
+            if (v > m) m = v;
+        }
+        if (maxnorm) maxnorm[iter - 1] = m;
+        if (iter >= ip.min_nonlinear_iter && m < ip.rootfind_tol) break;
+    }
+    return iters;
+}
+// Implicit::FixSolve (fix_solve.cpp:44-130) over the entire block.  Neighbours are read from the
+// state before this pass (the reference reads them while other failed zones are being replaced).
+static void fix_solve(const Block& B, const EmhdParams& ep, double gam, double* P, double* U, const double* solve_fail)
+{
+    int map[7];
+    const int nf = implicit_map(ep, map);
+    const size_t N = B.N;
+    std::vector<double> P0(P, P + (size_t)NVE*N);
+    auto failed = [](double s) { return (int)s == SOLVE_FAIL; };
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+        const size_t c = B.id(k, j, i);
+        if (!failed(solve_fail[c])) continue;
+        double wsum = 0., wsum_x = 0., sum[7] = {0.}, sum_x[7] = {0.};
+        for (int n = -1; n <= 1; n++) for (int m = -1; m <= 1; m++) for (int l = -1; l <= 1; l++) {
+            const int ii = i + l, jj = j + m, kk = k + n;
+            if (ii < 0 || ii >= B.n1 || jj < 0 || jj >= B.n2 || kk < 0 || kk >= B.n3) continue;
+            const double w = 1./(std::abs(l) + std::abs(m) + std::abs(n) + 1);
+            const size_t cn = B.id(kk, jj, ii);
+            if (!failed(solve_fail[cn])) {
+                wsum += w;
+                for (int q = 0; q < nf; ++q) sum[q] += w * P0[(size_t)map[q]*N + cn];
+            }
+            wsum_x += w;
+            for (int q = 0; q < nf; ++q) sum_x[q] += w * P0[(size_t)map[q]*N + cn];
+        }
+        if (wsum < 1.e-10) { for (int q = 0; q < nf; ++q) P[(size_t)map[q]*N + c] = sum_x[q]/wsum_x; }
+        else               { for (int q = 0; q < nf; ++q) P[(size_t)map[q]*N + c] = sum[q]/wsum; }
+    }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+        const size_t c = B.id(k, j, i);
+        if (!failed(solve_fail[c])) continue;
+        double Pc[NVE], Uc[NVE];
+        load10(P, N, c, Pc);
+        FV<double> D;
+        calc_4vecs_t(B, Pc, j, i, D);
+        prim_to_flux_t(B, ep, gam, Pc, D, j, i, 0, Uc);
+        for (int p = 0; p < NVE; ++p)
+            if (p < 8 || (p == IQ && ep.conduction) || (p == IDP && ep.viscosity)) U[(size_t)p*N + c] = Uc[p];
+    }
+}
+// Flux::p_to_u for the 10-slot state over the entire block (flux_functions.hpp:343-352)
+static void emhd_ptou(const Block& B, const EmhdParams& ep, double gam, const double* P, double* U)
+{
+    const size_t N = B.N;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pc[NVE], Uc[NVE];
+        load10(P, N, c, Pc);
+        FV<double> D;
+        calc_4vecs_t(B, Pc, j, i, D);
+        prim_to_flux_t(B, ep, gam, Pc, D, j, i, 0, Uc);
+        for (int p = 0; p < NVE; ++p)
+            if (p < 8 || (p == IQ && ep.conduction) || (p == IDP && ep.viscosity)) U[(size_t)p*N + c] = Uc[p];
+    }
+}
+// KReconstruction::slope_limit<linear_mc> (reconstruction.hpp:781-798)
+static inline double slope_mc(double x1, double x2, double x3, double dx)
+{
+    const double Dqm = 2 * (x2 - x1) / dx;
+    const double Dqp = 2 * (x3 - x2) / dx;
+    const double Dqc = 0.5 * (x3 - x1) / dx;
+    if (Dqm * Dqp <= 0) return 0;
+    if ((std::fabs(Dqm) < std::fabs(Dqp)) && (std::fabs(Dqm) < std::fabs(Dqc))) return Dqm;
+    else if (std::fabs(Dqp) < std::fabs(Dqc)) return Dqp;
+    return Dqc;
+}
+// EMHD::AddSource: explicit conduction and viscosity sources added to dUdt over the interior
+// (emhd.cpp:288-397, gradients by EMHD::gradient_calc<linear_mc>, emhd_utils.hpp:55-79)
+static void emhd_add_source(const Block& B, const EmhdParams& ep, double gam, const double* P, double* dUdt)
+{
+    if (!(ep.conduction || ep.viscosity)) return;
+    const size_t N = B.N;
+    // temporaries ucov and Theta over the interior plus a one-zone halo in active directions
+    std::vector<double> Tmp((size_t)5*N, 0.);
+    const int il = B.is - 1, ih = B.ie + 1;
+    const int jl = (B.ndim > 1) ? B.js - 1 : B.js, jh = (B.ndim > 1) ? B.je + 1 : B.je;
+    const int kl = (B.ndim > 2) ? B.ks - 1 : B.ks, kh = (B.ndim > 2) ? B.ke + 1 : B.ke;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = kl; k <= kh; ++k) for (int j = jl; j <= jh; ++j) for (int i = il; i <= ih; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pc[NVE], ucon[4], ucov[4];
+        load10(P, N, c, Pc);
+        calc_ucon_t(B, Pc, j, i, ucon);
+        lower_t(B, ucon, ucov, j, i);
+        for (int mu = 0; mu < 4; ++mu) Tmp[(size_t)mu*N + c] = ucov[mu];
+        Tmp[4*N + c] = kmax((gam - 1) * Pc[1] / Pc[0], SMALL);
+    }
+    const size_t sj = B.n1, sk = (size_t)B.n1*B.n2;
+    const bool do_2d = B.ndim > 1, do_3d = B.ndim > 2;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pc[NVE];
+        load10(P, N, c, Pc);
+        double tau, chi_e, nu_e;
+        emhd_set_parameters_P(B, ep, gam, Pc, j, i, tau, chi_e, nu_e);
+        FV<double> D;
+        calc_4vecs_t(B, Pc, j, i, D);
+        const double bsq = kmax(tdot(D.bcon, D.bcov), SMALL);
+        auto slope = [&](int var, int dir) {
+            const double* T = &Tmp[(size_t)var*N];
+            if (dir == 1) return slope_mc(T[c - 1], T[c], T[c + 1], B.c.dx1);
+            if (dir == 2) return slope_mc(T[c - sj], T[c], T[c + sj], B.c.dx2);
+            return slope_mc(T[c - sk], T[c], T[c + sk], B.c.dx3);
+        };
+        double grad_ucov[4][4], grad_Theta[4];
+        for (int mu = 0; mu < 4; ++mu) {
+            grad_ucov[0][mu] = 0;
+            grad_ucov[1][mu] = slope(mu, 1);
+            grad_ucov[2][mu] = do_2d ? slope(mu, 2) : 0.;
+            grad_ucov[3][mu] = do_3d ? slope(mu, 3) : 0.;
+        }
+        const size_t cg = ((size_t)j*B.n1 + i)*64;
+        for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) for (int lam = 0; lam < 4; ++lam)
+            grad_ucov[mu][nu] -= B.conn[cg + lam*16 + mu*4 + nu] * Tmp[(size_t)lam*N + c];
+        grad_Theta[0] = 0;
+        grad_Theta[1] = slope(4, 1);
+        grad_Theta[2] = do_2d ? slope(4, 2) : 0.;
+        grad_Theta[3] = do_3d ? slope(4, 3) : 0.;
+        double div_ucon = 0;
+        for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu)
+            div_ucon += B.Gcon(center, j, i, mu, nu) * grad_ucov[mu][nu];
+        const double rho = Pc[0];
+        const double Theta = Tmp[4*N + c];
+        const double gdet = B.Gdet(center, j, i);
+        if (ep.conduction) {
+            const double qtilde = Pc[IQ];
+            const double inv_mag_b = 1. / std::sqrt(bsq);
+            double q0 = 0;
+            for (int mu = 0; mu < 4; ++mu) q0 -= rho * chi_e * (D.bcon[mu] * inv_mag_b) * grad_Theta[mu];
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu)
+                q0 -= rho * chi_e * (D.bcon[mu] * inv_mag_b) * Theta * D.ucon[nu] * grad_ucov[nu][mu];
+            double q0_tilde = q0;
+            if (ep.higher_order_terms)
+                q0_tilde *= (chi_e != 0) ? std::sqrt(tau / (chi_e * rho * Theta * Theta)) : 0.0;
+            dUdt[(size_t)IQ*N + c] += gdet * q0_tilde / tau;
+            if (ep.higher_order_terms) dUdt[(size_t)IQ*N + c] += gdet * (qtilde / 2.) * div_ucon;
+        }
+        if (ep.viscosity) {
+            const double dPtilde = Pc[IDP];
+            double dP0 = -rho * nu_e * div_ucon;
+            for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu)
+                dP0 += 3. * rho * nu_e * (D.bcon[mu] * D.bcon[nu] / bsq) * grad_ucov[mu][nu];
+            double dP0_tilde = dP0;
+            if (ep.higher_order_terms)
+                dP0_tilde *= (nu_e != 0) ? std::sqrt(tau / (nu_e * rho * Theta)) : 0.0;
+            dUdt[(size_t)IDP*N + c] += gdet * dP0_tilde / tau;
+            if (ep.higher_order_terms) dUdt[(size_t)IDP*N + c] += gdet * (dPtilde / 2.) * div_ucon;
+        }
+    }
+}
+
 struct Handle {
     Block B;
     Fields f;
@@ -1553,6 +2263,81 @@ int orc_utop_cell(void* hp, int j, int i, const double* U, double* P)
 {
     const Block& B = ((Handle*)hp)->B;
     return u_to_p_onedw(B, U, P, j, i, center, B.c.iter_max, B.c.err_tol);
+}
+
+// ---- EMHD and the implicit solve.  All field arrays are [10][N] (slots rho..B3, q, dP).
+void orc_get_connection(void* hp, double* conn)
+{
+    const Block& B = ((Handle*)hp)->B;
+    std::memcpy(conn, B.conn.data(), B.conn.size()*sizeof(double));
+}
+void orc_emhd_ptou(void* hp, const EmhdParams* ep, const double* P, double* U)
+{
+    const Block& B = ((Handle*)hp)->B;
+    emhd_ptou(B, *ep, B.c.gam, P, U);
+}
+void orc_emhd_add_source(void* hp, const EmhdParams* ep, const double* P, double* dUdt)
+{
+    const Block& B = ((Handle*)hp)->B;
+    emhd_add_source(B, *ep, B.c.gam, P, dUdt);
+}
+// Residual and Jacobian at the solver state over the interior, as the split "implicit_jacobian"
+// kernel stores them (implicit.cpp:286-320): res [nf][N], J [nf*nf][N] (row-major per zone).
+void orc_implicit_jacobian(void* hp, const EmhdParams* ep, const ImplicitParams* ip, const double* Pf,
+                           const double* Uf, const double* Ps, const double* S, const double* Psol, double dt,
+                           double* J, double* res)
+{
+    const Block& B = ((Handle*)hp)->B;
+    const size_t N = B.N;
+    int map[7];
+    const int nf = implicit_map(*ep, map);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double pf[NVE], uf[NVE], ps[NVE], s[NVE], psol[NVE], dUi[NVE] = {0}, Jz[49], rz[7];
+        load10(Pf, N, c, pf); load10(Uf, N, c, uf); load10(Ps, N, c, ps); load10(S, N, c, s); load10(Psol, N, c, psol);
+        implicit_dU(B, *ep, B.c.gam, pf, ps, j, i, dUi);
+        if (ip->jacobian == 1) calc_jacobian_exact(B, *ep, B.c.gam, psol, pf, uf, ps, s, dUi, nf, map, j, i, dt, Jz, rz);
+        else calc_jacobian_fd(B, *ep, B.c.gam, ip->jacobian_delta, psol, pf, uf, ps, s, dUi, nf, map, j, i, dt, Jz, rz);
+        for (int q = 0; q < nf; ++q) res[(size_t)q*N + c] = rz[q];
+        for (int q = 0; q < nf*nf; ++q) J[(size_t)q*N + c] = Jz[q];
+    }
+}
+// Residual only at a trial state (the linesearch call of implicit.cpp:469-473)
+void orc_implicit_residual(void* hp, const EmhdParams* ep, const double* Pf, const double* Uf, const double* Ps,
+                           const double* S, const double* Ptest, double dt, double* res)
+{
+    const Block& B = ((Handle*)hp)->B;
+    const size_t N = B.N;
+    int map[7];
+    const int nf = implicit_map(*ep, map);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double pf[NVE], uf[NVE], ps[NVE], s[NVE], pt[NVE], dUi[NVE] = {0}, rz[7];
+        load10(Pf, N, c, pf); load10(Uf, N, c, uf); load10(Ps, N, c, ps); load10(S, N, c, s); load10(Ptest, N, c, pt);
+        implicit_dU(B, *ep, B.c.gam, pf, ps, j, i, dUi);
+        calc_residual_t<double>(B, *ep, B.c.gam, pt, pf, uf, ps, s, dUi, nf, map, j, i, dt, rz);
+        for (int q = 0; q < nf; ++q) res[(size_t)q*N + c] = rz[q];
+    }
+}
+// Dense solve of one system with the reference's QR (use_qr = 1) or LU path; A row-major n x n.
+void orc_dense_solve(int n, int use_qr, double* A, double* b)
+{
+    if (use_qr) qr_solve(n, A, b);
+    else lu_solve(n, A, b);
+}
+int orc_implicit_step(void* hp, const EmhdParams* ep, const ImplicitParams* ip, const double* Pf, const double* Uf,
+                      const double* Ps, const double* S, double* Psol, double* solve_norm, double* solve_fail,
+                      double dt, double* maxnorm)
+{
+    const Block& B = ((Handle*)hp)->B;
+    return implicit_step(B, *ep, *ip, B.c.gam, Pf, Uf, Ps, S, Psol, solve_norm, solve_fail, dt, maxnorm);
+}
+void orc_fix_solve(void* hp, const EmhdParams* ep, double* P, double* U, const double* solve_fail)
+{
+    const Block& B = ((Handle*)hp)->B;
+    fix_solve(B, *ep, B.c.gam, P, U, solve_fail);
 }
 
 } // extern "C"

@@ -86,6 +86,15 @@ def load():
     lib.orc_max_divb.argtypes = [P, P, C.c_int, C.c_int]
     lib.orc_utop_cell.restype = C.c_int
     lib.orc_utop_cell.argtypes = [P, C.c_int, C.c_int, P, P]
+    lib.orc_get_connection.argtypes = [P, P]
+    lib.orc_emhd_ptou.argtypes = [P, P, P, P]
+    lib.orc_emhd_add_source.argtypes = [P, P, P, P]
+    lib.orc_implicit_jacobian.argtypes = [P, P, P, P, P, P, P, P, C.c_double, P, P]
+    lib.orc_implicit_residual.argtypes = [P, P, P, P, P, P, P, C.c_double, P]
+    lib.orc_dense_solve.argtypes = [C.c_int, C.c_int, P, P]
+    lib.orc_implicit_step.restype = C.c_int
+    lib.orc_implicit_step.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_double, P]
+    lib.orc_fix_solve.argtypes = [P, P, P, P, P]
     _lib = lib
     return lib
 
@@ -217,3 +226,93 @@ class Oracle:
 
     def max_divb(self, U, avoid_inner=False, avoid_outer=False):
         return self.lib.orc_max_divb(self.h, _ptr(U), int(avoid_inner), int(avoid_outer))
+
+    # ---------------------------------------------------------------- EMHD and the implicit solve
+    # Field arrays here are (10, n3, n2, n1): rho, u, u1..u3, B1..B3, q~, dP~.
+    def connection(self):
+        n3, n2, n1 = self.shape
+        conn = np.zeros((n2, n1, 4, 4, 4))
+        self.lib.orc_get_connection(self.h, _ptr(conn))
+        return conn
+
+    def zeros10(self):
+        return np.zeros((10,) + self.shape)
+
+    def emhd_ptou(self, emhd, P):
+        U = self.zeros10()
+        self.lib.orc_emhd_ptou(self.h, C.byref(emhd_params(emhd)), _ptr(P), _ptr(U))
+        return U
+
+    def emhd_add_source(self, emhd, P, dUdt):
+        self.lib.orc_emhd_add_source(self.h, C.byref(emhd_params(emhd)), _ptr(P), _ptr(dUdt))
+
+    def implicit_jacobian(self, emhd, imp, Pf, Uf, Ps, S, Psol, dt):
+        nf = 5 + int(emhd.conduction) + int(emhd.viscosity)
+        J = np.zeros((nf * nf,) + self.shape)
+        res = np.zeros((nf,) + self.shape)
+        self.lib.orc_implicit_jacobian(self.h, C.byref(emhd_params(emhd)), C.byref(implicit_params(imp)),
+                                       _ptr(Pf), _ptr(Uf), _ptr(Ps), _ptr(S), _ptr(Psol), dt, _ptr(J), _ptr(res))
+        return J, res
+
+    def implicit_residual(self, emhd, Pf, Uf, Ps, S, Ptest, dt):
+        nf = 5 + int(emhd.conduction) + int(emhd.viscosity)
+        res = np.zeros((nf,) + self.shape)
+        self.lib.orc_implicit_residual(self.h, C.byref(emhd_params(emhd)), _ptr(Pf), _ptr(Uf), _ptr(Ps), _ptr(S),
+                                       _ptr(Ptest), dt, _ptr(res))
+        return res
+
+    def implicit_step(self, emhd, imp, Pf, Uf, Ps, S, Psol, solve_norm, solve_fail, dt):
+        """Implicit::Step in place on Psol, solve_norm, solve_fail; returns (iterations, max norms)."""
+        mx = np.zeros(imp.max_nonlinear_iter)
+        it = self.lib.orc_implicit_step(self.h, C.byref(emhd_params(emhd)), C.byref(implicit_params(imp)),
+                                        _ptr(Pf), _ptr(Uf), _ptr(Ps), _ptr(S), _ptr(Psol), _ptr(solve_norm),
+                                        _ptr(solve_fail), dt, _ptr(mx))
+        return it, mx[:it]
+
+    def fix_solve(self, emhd, P, U, solve_fail):
+        self.lib.orc_fix_solve(self.h, C.byref(emhd_params(emhd)), _ptr(P), _ptr(U), _ptr(solve_fail))
+
+
+class EmhdParams(C.Structure):
+    _fields_ = [("type", C.c_int32), ("higher_order_terms", C.c_int32), ("feedback", C.c_int32),
+                ("conduction", C.c_int32), ("viscosity", C.c_int32), ("pad", C.c_int32),
+                ("tau", C.c_double), ("conduction_alpha", C.c_double), ("viscosity_alpha", C.c_double),
+                ("kappa", C.c_double), ("eta", C.c_double)]
+
+
+class ImplicitParams(C.Structure):
+    _fields_ = [("min_nonlinear_iter", C.c_int32), ("max_nonlinear_iter", C.c_int32), ("use_qr", C.c_int32),
+                ("linesearch", C.c_int32), ("max_linesearch_iter", C.c_int32), ("jacobian", C.c_int32),
+                ("jacobian_delta", C.c_double), ("rootfind_tol", C.c_double),
+                ("linesearch_eps", C.c_double), ("linesearch_lambda", C.c_double)]
+
+
+CLOSURE = {"constant": 0, "soundspeed": 1, "sound_speed": 1, "kappa_eta": 2, "torus": 3}
+
+
+def emhd_params(e):
+    s = EmhdParams()
+    s.type = CLOSURE[e.closure_type]
+    s.higher_order_terms, s.feedback = int(e.higher_order_terms), int(e.feedback)
+    s.conduction, s.viscosity = int(e.conduction), int(e.viscosity)
+    s.tau, s.conduction_alpha, s.viscosity_alpha = e.tau, e.conduction_alpha, e.viscosity_alpha
+    s.kappa, s.eta = e.kappa, e.eta
+    return s
+
+
+def implicit_params(p):
+    s = ImplicitParams()
+    s.min_nonlinear_iter, s.max_nonlinear_iter = p.min_nonlinear_iter, p.max_nonlinear_iter
+    s.use_qr, s.linesearch, s.max_linesearch_iter = int(p.use_qr), int(p.linesearch), p.max_linesearch_iter
+    s.jacobian = 1 if p.jacobian == "exact" else 0
+    s.jacobian_delta, s.rootfind_tol = p.jacobian_delta, p.rootfind_tol
+    s.linesearch_eps, s.linesearch_lambda = p.linesearch_eps, p.linesearch_lambda
+    return s
+
+
+def dense_solve(A, b, use_qr=True):
+    """The reference's per-zone dense solve (QR with column pivoting, or its LU path) on one system."""
+    A = np.ascontiguousarray(A, dtype=np.float64).copy()
+    b = np.ascontiguousarray(b, dtype=np.float64).copy()
+    load().orc_dense_solve(A.shape[0], int(use_qr), _ptr(A), _ptr(b))
+    return b

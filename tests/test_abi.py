@@ -8,7 +8,7 @@ import pytest
 
 from kharma_b200 import _lib
 from kharma_b200.block import build_geometry
-from kharma_b200.spec import mhdmodes_spec, torus_spec
+from kharma_b200.spec import atmosphere_spec, mhdmodes_spec, torus_spec
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -55,3 +55,21 @@ def test_geometry_matches_oracle(oracle_mod, spec):
     gp = build_geometry(spec)
     for key in go:
         assert np.array_equal(go[key], gp[key]), f"{key} differs from the oracle"
+
+
+def test_emhd_struct_layout():
+    # include/khb.h khb_emhd_params / khb_implicit_params
+    assert C_sizeof(_lib.KhbEmhdParams) == 64 and _lib.KhbEmhdParams.tau.offset == 24
+    assert C_sizeof(_lib.KhbImplicitParams) == 56 and _lib.KhbImplicitParams.jacobian_delta.offset == 24
+    assert C_sizeof(_lib.KhbFields) == 8 * _lib.MAX_VARS == 80
+
+
+def C_sizeof(t):
+    import ctypes
+    return ctypes.sizeof(t)
+
+
+@pytest.mark.parametrize("spec", [atmosphere_spec(64, 8, 1), torus_spec(24, 16, 4)], ids=["mks_ks", "fmks"])
+def test_connection_matches_oracle(oracle_mod, spec):
+    from kharma_b200.emhd import build_connection
+    assert np.array_equal(oracle_mod.Oracle(spec).connection(), build_connection(spec))

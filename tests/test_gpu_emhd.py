@@ -1,0 +1,171 @@
+"""EMHD sources and the implicit Newton solve on the GPU against the oracle.
+
+With the reference's forward-difference Jacobian every output (primitives, solve_norm, solve_fail,
+iteration count and per-iteration maximum norms) must agree bit for bit: the kernels are compiled
+without FMA contraction in the reference's evaluation order.  The exact-Jacobian form is compared
+with the oracle's dual-number Jacobian to 1e-12 relative (Jacobian) and 1e-11 (converged iterates).  The torus closure calls exp, whose CUDA
+and glibc results differ in the last bits, so it is compared to 1e-12 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+from emhd_cases import EMHD_VARIANTS, atmosphere_case, implicit, source
+from kharma_b200.block import Block
+from kharma_b200.emhd import ImplicitSolver
+
+pytestmark = pytest.mark.gpu
+
+SLOTS = {True: [8], False: []}
+
+
+def setup(oracle_mod, variant, shape=(64, 6, 1)):
+    spec, emhd, P, dt, xi = atmosphere_case(*shape, emhd=EMHD_VARIANTS[variant])
+    o = oracle_mod.Oracle(spec)
+    b = Block(spec, geometry=o.geometry())
+    sol = ImplicitSolver(b, emhd, conn=o.connection())
+    U = o.emhd_ptou(emhd, P)
+    S_e = o.zeros10()
+    o.emhd_add_source(emhd, P, S_e)
+    S = source(U, S_e, xi, dt)
+    return spec, emhd, o, b, sol, P, U, S_e, S, dt
+
+
+def dev(a):
+    return torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+def slots(emhd):
+    return [0, 1, 2, 3, 4, 5, 6, 7] + ([8] if emhd.conduction else []) + ([9] if emhd.viscosity else [])
+
+
+def rel_err(a, b):
+    scale = np.abs(b).max() + 1e-300
+    return np.abs(a - b).max() / scale
+
+
+SHAPES = {"2d": (64, 6, 1), "3d": (64, 4, 4)}
+
+
+@pytest.mark.parametrize("shape", ["2d", "3d"])
+@pytest.mark.parametrize("variant", ["kappa_eta_ho", "constant", "soundspeed_q_only", "dp_only", "grmhd_only"])
+def test_emhd_ptou_and_explicit_sources_bitwise(oracle_mod, variant, shape):
+    spec, emhd, o, b, sol, P, U, S_e, S, dt = setup(oracle_mod, variant, SHAPES[shape])
+    Pd = dev(P)
+    Ud = sol.ptou(Pd)
+    Sd = torch.zeros_like(Pd)
+    sol.add_source(Pd, Sd)
+    torch.cuda.synchronize()
+    for s in slots(emhd):
+        assert np.array_equal(Ud[s].cpu().numpy(), U[s]), f"U slot {s}"
+    assert np.array_equal(Sd.cpu().numpy(), S_e), "explicit EMHD sources differ"
+
+
+@pytest.mark.parametrize("variant", ["kappa_eta_ho", "constant", "soundspeed_q_only", "dp_only", "grmhd_only"])
+def test_jacobian_fd_bitwise_and_exact_close(oracle_mod, variant):
+    spec, emhd, o, b, sol, P, U, S_e, S, dt = setup(oracle_mod, variant)
+    Psol = P.copy()
+    Psol[[0, 1]] *= 1.002
+    sl = (slice(None),) + spec.interior
+    for jac in ("fd", "exact"):
+        sol.set_implicit(implicit(jac))
+        Jd, rd = sol.jacobian(dev(P), dev(U), dev(P), dev(S), dev(Psol), dt)
+        Jo, ro = o.implicit_jacobian(emhd, implicit(jac), P, U, P, S, Psol, dt)
+        torch.cuda.synchronize()
+        Jd, rd = Jd.cpu().numpy(), rd.cpu().numpy()
+        assert np.array_equal(rd[sl], ro[sl]), f"{jac}: residual differs"
+        if jac == "fd":
+            assert np.array_equal(Jd[sl], Jo[sl]), "forward-difference Jacobian differs"
+        else:
+            nf = emhd.nfvar
+            for row in range(nf):
+                a = Jd[row * nf:(row + 1) * nf][sl]
+                c = Jo[row * nf:(row + 1) * nf][sl]
+                assert rel_err(a, c) < 1e-12, (row, rel_err(a, c))
+
+
+def run_step(sol, o, emhd, imp, spec, P, U, S, dt, P_guess=None, fail0=None):
+    Psol = (P if P_guess is None else P_guess).copy()
+    norm = np.zeros(spec.shape)
+    fail = np.zeros(spec.shape) if fail0 is None else fail0.copy()
+    Psd, nd, fd = dev(Psol), dev(norm), dev(fail)
+    sol.set_implicit(imp)
+    sol.step(dev(P), dev(U), dev(P), dev(S), Psd, nd, fd, dt)
+    it_d, mx_d = sol.stats()
+    it_o, mx_o = o.implicit_step(emhd, imp, P, U, P, S, Psol, norm, fail, dt)
+    return (Psd.cpu().numpy(), nd.cpu().numpy(), fd.cpu().numpy(), it_d, mx_d), (Psol, norm, fail, it_o, mx_o)
+
+
+@pytest.mark.parametrize("solver", ["qr", "lu"])
+@pytest.mark.parametrize("variant", ["kappa_eta_ho", "constant", "soundspeed_q_only", "dp_only", "grmhd_only"])
+def test_implicit_step_fd_bitwise(oracle_mod, variant, solver):
+    spec, emhd, o, b, sol, P, U, S_e, S, dt = setup(oracle_mod, variant)
+    tol = 1e-12 * np.abs(U[(slice(None),) + spec.interior]).max() / dt
+    imp = implicit("fd", rootfind_tol=tol, use_qr=(solver == "qr"))
+    (Pd, nd, fd, itd, mxd), (Po, no, fo, ito, mxo) = run_step(sol, o, emhd, imp, spec, P, U, S, dt)
+    sl = spec.interior
+    print(variant, solver, "iterations", ito, "max norms", mxo)
+    assert itd == ito
+    assert np.array_equal(mxd, mxo)
+    assert np.array_equal(fd[sl], fo[sl])
+    assert np.array_equal(nd[sl], no[sl])
+    for s in slots(emhd):
+        assert np.array_equal(Pd[s][sl], Po[s][sl]), f"slot {s}"
+
+
+@pytest.mark.parametrize("variant", ["kappa_eta_ho", "constant", "grmhd_only"])
+def test_implicit_step_exact_close(oracle_mod, variant):
+    spec, emhd, o, b, sol, P, U, S_e, S, dt = setup(oracle_mod, variant, SHAPES["3d"])
+    imp = implicit("exact", rootfind_tol=0.0, max_nonlinear_iter=4)      # a fixed number of iterations
+    (Pd, nd, fd, itd, mxd), (Po, no, fo, ito, mxo) = run_step(sol, o, emhd, imp, spec, P, U, S, dt)
+    sl = spec.interior
+    assert itd == ito == 4
+    assert np.array_equal(fd[sl], fo[sl])
+    # the two exact Jacobians differ by rounding (~1e-15); after the iterates reach the residual's
+    # round-off floor they differ by up to ~1e-12 of the smallest variable's scale (dP~ ~ 1e-5)
+    for s in slots(emhd):
+        assert rel_err(Pd[s][sl], Po[s][sl]) < 1e-11, s
+    assert np.abs(mxd[-1] - mxo[-1]) <= 1e-12 * np.abs(U[(slice(None),) + sl]).max() / dt
+
+
+def test_failures_backtracking_and_fix_solve_bitwise(oracle_mod):
+    spec, emhd, o, b, sol, P, U, S_e, S, dt = setup(oracle_mod, "kappa_eta_ho")
+    sl = spec.interior
+    k, j = sl[0].start, sl[1].start + 2
+    bad = [(k, j, sl[2].start + 5), (k, j + 1, sl[2].start + 17), (k, j + 1, sl[2].start + 18)]
+    for z in bad:
+        S[(0,) + z] = -50.0 * U[(0,) + z] / dt
+    z2 = (k, j + 3, sl[2].start + 30)
+    S[(0,) + z2] = -3.0 * U[(0,) + z2] / dt        # recovers by backtracking (lambda = 0.1)
+    fail0 = np.zeros(spec.shape)
+    fail0[k, j + 2, sl[2].start + 40] = 1.0         # failed in an earlier stage: skipped
+    imp = implicit("fd", max_nonlinear_iter=3)
+    (Pd, nd, fd, itd, mxd), (Po, no, fo, ito, mxo) = run_step(sol, o, emhd, imp, spec, P, U, S, dt, fail0=fail0)
+    assert np.count_nonzero(fo[sl] == 1) == len(bad) + 1
+    assert np.array_equal(fd[sl], fo[sl]) and np.array_equal(nd[sl], no[sl])
+    for s in slots(emhd):
+        assert np.array_equal(Pd[s][sl], Po[s][sl])
+    # FixSolve over the whole block
+    Uo = o.emhd_ptou(emhd, Po)
+    Pdd, Udd = dev(Po), dev(Uo)
+    sol.fix_solve(Pdd, Udd, dev(fo))
+    o.fix_solve(emhd, Po, Uo, fo)
+    torch.cuda.synchronize()
+    assert np.array_equal(Pdd.cpu().numpy(), Po)
+    for s in slots(emhd):
+        assert np.array_equal(Udd[s].cpu().numpy(), Uo[s])
+
+
+def test_torus_closure_close(oracle_mod):
+    spec, emhd, o, b, sol, P, U, S_e, S, dt = setup(oracle_mod, "torus")
+    Pd = dev(P)
+    Sd = torch.zeros_like(Pd)
+    sol.add_source(Pd, Sd)
+    torch.cuda.synchronize()
+    sl = (slice(None),) + spec.interior
+    for s in slots(emhd)[8:]:
+        assert rel_err(Sd[s].cpu().numpy()[spec.interior], S_e[s][spec.interior]) < 1e-12
+    imp = implicit("fd", rootfind_tol=0.0, max_nonlinear_iter=3)
+    (Pd_, nd, fd, itd, mxd), (Po, no, fo, ito, mxo) = run_step(sol, o, emhd, imp, spec, P, U, S, dt)
+    for s in slots(emhd):
+        assert rel_err(Pd_[s][spec.interior], Po[s][spec.interior]) < 1e-10, s
