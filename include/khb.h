@@ -48,8 +48,11 @@ enum { KHB_OK = 0, KHB_ERR_ARG = -1, KHB_ERR_CUDA = -2, KHB_ERR_STATE = -3, KHB_
 enum { KHB_RECON_DONOR_CELL = 0, KHB_RECON_LINEAR_MC = 1, KHB_RECON_WENO5 = 2, KHB_RECON_PPM = 3 };
 /* Riemann solvers (flux/flux.hpp:110-121) */
 enum { KHB_FLUX_LLF = 0, KHB_FLUX_HLLE = 1 };
-/* Boundary types per face (boundaries/boundaries.cpp:57-368) */
-enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2 };
+/* Boundary types per face (boundaries/boundaries.cpp:57-368).  KHB_BC_EXCHANGE (x3 faces only)
+ * marks a face whose ghost planes the caller fills from the neighbouring block (Parthenon's
+ * boundary communication): khb_boundaries leaves them alone, and khb_fix_utop reads the
+ * neighbour values there instead of wrapping. */
+enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2, KHB_BC_EXCHANGE = 3 };
 /* Floor injection frames (floors/floors.hpp:96) */
 enum { KHB_FRAME_FLUID = 0, KHB_FRAME_NORMAL = 1, KHB_FRAME_DRIFT = 2 };
 /* Arithmetic of reconstruction, Riemann fluxes and EMF averaging */

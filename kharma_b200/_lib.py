@@ -16,7 +16,7 @@ Q, DP = 8, 9           # khb_fields slots of the EMHD variables
 # enums (include/khb.h)
 RECON = {"donor_cell": 0, "linear_mc": 1, "weno5": 2, "ppm": 3}
 FLUX = {"llf": 0, "hlle": 1}
-BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 PREC = {"fp64": 0, "fp32_flux": 1}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}

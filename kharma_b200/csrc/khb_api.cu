@@ -262,6 +262,14 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
         *why = "unknown precision";
         return KHB_ERR_UNSUPPORTED;
     }
+    for (int x = 0; x < 6; ++x) {
+        if (cfg->bc[x] < KHB_BC_PERIODIC || cfg->bc[x] > KHB_BC_EXCHANGE) { *why = "unknown boundary type"; return KHB_ERR_ARG; }
+        if (cfg->bc[x] == KHB_BC_EXCHANGE && (x < 4 || cfg->nx3 == 1)) {
+            *why = "exchange boundaries are supported on active x3 faces only";
+            return KHB_ERR_UNSUPPORTED;
+        }
+    }
+    if ((cfg->bc[4] == KHB_BC_PERIODIC) != (cfg->bc[5] == KHB_BC_PERIODIC)) { *why = "x3 periodic on one face only"; return KHB_ERR_ARG; }
     std::memset(&d, 0, sizeof(d));
     std::memset(&ph, 0, sizeof(ph));
     d.nx1 = cfg->nx1; d.nx2 = cfg->nx2; d.nx3 = cfg->nx3;

@@ -401,8 +401,8 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
 }
 
 // ===================================================================================== fixups
-// fixup.cpp:47-156.  Neighbours in periodic directions wrap; in other directions they must be
-// interior.  Failed zones never read each other, so one pass over the list is race-free.
+// fixup.cpp:47-156.  Neighbours in periodic directions wrap; across exchanged x3 faces they are
+// read from the ghost planes; in other directions they must be interior.  Failed zones never read each other, so one pass over the list is race-free.
 template <int NV>
 __global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, const int32_t* pflag,
                         const int* fail_count, const int* fail_list)
@@ -418,7 +418,14 @@ __global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, 
                 int ii = i + l, jj = j + m, kk = k + nn;
                 if (ii < d.is || ii > d.ie) { if (d.bc[0] != KHB_BC_PERIODIC) continue; ii += (ii < d.is) ? d.nx1 : -d.nx1; }
                 if (jj < d.js || jj > d.je) { if (d.ndim < 2 || d.bc[2] != KHB_BC_PERIODIC) continue; jj += (jj < d.js) ? d.nx2 : -d.nx2; }
-                if (kk < d.ks || kk > d.ke) { if (d.ndim < 3 || d.bc[4] != KHB_BC_PERIODIC) continue; kk += (kk < d.ks) ? d.nx3 : -d.nx3; }
+                if (kk < d.ks || kk > d.ke) {
+                    // exchanged faces hold the neighbouring block's values in the ghost planes
+                    const bool exch = (kk < d.ks) ? d.bc[4] == KHB_BC_EXCHANGE : d.bc[5] == KHB_BC_EXCHANGE;
+                    if (!exch) {
+                        if (d.ndim < 3 || d.bc[4] != KHB_BC_PERIODIC) continue;
+                        kk += (kk < d.ks) ? d.nx3 : -d.nx3;
+                    }
+                }
                 const long long cn = ((long long)kk*d.n2 + jj)*d.n1 + ii;
                 if (!(pflag[cn] > 0)) {
                     const double w = 1./(abs(l) + abs(m) + abs(nn) + 1);
