@@ -168,10 +168,18 @@ struct ResidZone {
     double norm_q, norm_d;          // final residual normalisation (implicit.hpp:190-198)
 };
 
-// Intermediates of the trial state kept for the exact Jacobian
-struct ResidState {
+// The velocity-dependent part of the residual at a trial state: 4-vectors, Lorentz factor and
+// (EMHD) the time derivative of u_mu and div u.  Columns of the forward-difference Jacobian that
+// perturb rho, u, q~ or dP~ reuse the base state's: same inputs, same bits.
+struct VelState {
     FourVec<double> D;
     double gamma;
+    double dt_ucov[4];
+    double div_ucon;
+};
+
+// Intermediates of the trial state kept for the exact Jacobian
+struct ResidState {
     double Theta, cs2, fq, fd, q, dP;
     double bsq, bmag, eta;
     bool bsq_clamped, theta_clamped;
@@ -243,30 +251,48 @@ __device__ __forceinline__ void setup_zone(const EmhdArgs& E, double gam, double
     }
 }
 
-// Implicit::calc_residual (implicit.hpp:139-200) at the trial implicit variables x (rho, u, u1-u3[, q~][, dP~])
+// GRMHD::calc_4vecs of the trial state (grmhd_functions.hpp:225-246) and, for EMHD, the
+// time-derivative pieces of EMHD::time_derivative_sources (emhd_sources.hpp:84-93)
 template <bool HQ, bool HD>
-__device__ __forceinline__ void residual(const EmhdArgs& E, double gam, double dt, const ResidZone<Imp<HQ, HD>::NF>& Z,
-                                         const double* x, double* res, ResidState& S)
+__device__ __forceinline__ void velocity_part(double dt, const ResidZone<Imp<HQ, HD>::NF>& Z, const double* x,
+                                              VelState& V)
 {
     using I = Imp<HQ, HD>;
     const CenterGeom& G = Z.G;
-    const double P8[8] = {x[0], x[1], x[2], x[3], x[4], Z.B[0], Z.B[1], Z.B[2]};
-    FourVec<double>& D = S.D;
-    S.gamma = lorentz(G.gcov, x[2], x[3], x[4]);
-    {
-        const double alpha = 1. / sqrt(-G.gcon0[0]);
-        D.ucon[0] = S.gamma / alpha;
+    FourVec<double>& D = V.D;
+    V.gamma = lorentz(G.gcov, x[2], x[3], x[4]);
+    const double alpha = 1. / sqrt(-G.gcon0[0]);
+    D.ucon[0] = V.gamma / alpha;
 #pragma unroll
-        for (int v = 0; v < 3; ++v) D.ucon[v+1] = P8[2 + v] - S.gamma * alpha * G.gcon0[v+1];
-        lower4(G.gcov, D.ucon, D.ucov);
-        double b0 = 0.;
+    for (int v = 0; v < 3; ++v) D.ucon[v+1] = x[2 + v] - V.gamma * alpha * G.gcon0[v+1];
+    lower4(G.gcov, D.ucon, D.ucov);
+    double b0 = 0.;
 #pragma unroll
-        for (int v = 0; v < 3; ++v) b0 += P8[5 + v] * D.ucov[v+1];
-        D.bcon[0] = b0;
+    for (int v = 0; v < 3; ++v) b0 += Z.B[v] * D.ucov[v+1];
+    D.bcon[0] = b0;
 #pragma unroll
-        for (int v = 0; v < 3; ++v) D.bcon[v+1] = (P8[5 + v] + b0 * D.ucon[v+1]) / D.ucon[0];
-        lower4(G.gcov, D.bcon, D.bcov);
+    for (int v = 0; v < 3; ++v) D.bcon[v+1] = (Z.B[v] + b0 * D.ucon[v+1]) / D.ucon[0];
+    lower4(G.gcov, D.bcon, D.bcov);
+    if (I::EM) {
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) V.dt_ucov[mu] = (D.ucov[mu] - Z.ucov_old[mu]) / dt;
+        double div_ucon = 0.;
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) div_ucon += G.gcon0[mu] * V.dt_ucov[mu];
+        V.div_ucon = div_ucon;
     }
+}
+
+// Implicit::calc_residual (implicit.hpp:139-200) at the trial implicit variables x (rho, u, u1-u3[, q~][, dP~])
+// given their velocity part V
+template <bool HQ, bool HD>
+__device__ __forceinline__ void residual_with(const EmhdArgs& E, double gam, double dt,
+                                              const ResidZone<Imp<HQ, HD>::NF>& Z, const double* x,
+                                              const VelState& V, double* res, ResidState& S)
+{
+    using I = Imp<HQ, HD>;
+    const CenterGeom& G = Z.G;
+    const FourVec<double>& D = V.D;
     const double gdet = G.gdet;
     double U[I::NF];
     U[0] = x[0] * D.ucon[0] * gdet;
@@ -304,12 +330,6 @@ __device__ __forceinline__ void residual(const EmhdArgs& E, double gam, double d
     for (int p = 0; p < I::NF; ++p) res[p] = (U[p] - Z.Ui[p]) / dt - Z.S[p];
     if (I::EM) {
         const double tau = Z.tau;
-        double dt_ucov[4];
-#pragma unroll
-        for (int mu = 0; mu < 4; ++mu) dt_ucov[mu] = (D.ucov[mu] - Z.ucov_old[mu]) / dt;
-        double div_ucon = 0.;
-#pragma unroll
-        for (int mu = 0; mu < 4; ++mu) div_ucon += G.gcon0[mu] * dt_ucov[mu];
         const double th = (gam-1) * x[1] / x[0];
         S.theta_clamped = th < SMALL;
         const double Theta_new = kmax(th, SMALL);
@@ -320,11 +340,11 @@ __device__ __forceinline__ void residual(const EmhdArgs& E, double gam, double d
             rq -= 0.5*(dUq + Z.dUi_q);
             double q0 = Z.cq0 * dt_Theta;
 #pragma unroll
-            for (int mu = 0; mu < 4; ++mu) q0 -= Z.cq[mu] * dt_ucov[mu];
+            for (int mu = 0; mu < 4; ++mu) q0 -= Z.cq[mu] * V.dt_ucov[mu];
             double q0t = q0;
             if (E.higher_order_terms) q0t *= Z.fac_q;
             double dUqt = gdet * (q0t / tau);
-            if (E.higher_order_terms) dUqt += Z.gq * div_ucon;
+            if (E.higher_order_terms) dUqt += Z.gq * V.div_ucon;
             rq -= dUqt;
             rq *= tau;
             if (E.higher_order_terms) rq *= Z.norm_q;
@@ -334,19 +354,29 @@ __device__ __forceinline__ void residual(const EmhdArgs& E, double gam, double d
             double rd = res[I::ID];
             const double dUd = -gdet * (x[I::ID] / tau);
             rd -= 0.5*(dUd + Z.dUi_d);
-            double dP0 = Z.cd0 * div_ucon;
+            double dP0 = Z.cd0 * V.div_ucon;
 #pragma unroll
-            for (int mu = 0; mu < 4; ++mu) dP0 += Z.cd[mu] * dt_ucov[mu];
+            for (int mu = 0; mu < 4; ++mu) dP0 += Z.cd[mu] * V.dt_ucov[mu];
             double dP0t = dP0;
             if (E.higher_order_terms) dP0t *= Z.fac_d;
             double dUdt_ = gdet * (dP0t / tau);
-            if (E.higher_order_terms) dUdt_ += Z.gd * div_ucon;
+            if (E.higher_order_terms) dUdt_ += Z.gd * V.div_ucon;
             rd -= dUdt_;
             rd *= tau;
             if (E.higher_order_terms) rd *= Z.norm_d;
             res[I::ID] = rd;
         }
     }
+}
+
+template <bool HQ, bool HD>
+__device__ __forceinline__ void residual(const EmhdArgs& E, double gam, double dt, const ResidZone<Imp<HQ, HD>::NF>& Z,
+                                         const double* x, double* res)
+{
+    VelState V;
+    ResidState S;
+    velocity_part<HQ, HD>(dt, Z, x, V);
+    residual_with<HQ, HD>(E, gam, dt, Z, x, V, res, S);
 }
 
 // Forward-difference Jacobian (Implicit::calc_jacobian, implicit.hpp:208-255).  res: residual at x.
@@ -356,8 +386,10 @@ __device__ __forceinline__ void jacobian_fd(const EmhdArgs& E, double gam, doubl
                                             double* res, double (&J)[Imp<HQ, HD>::NF][Imp<HQ, HD>::NF])
 {
     constexpr int NF = Imp<HQ, HD>::NF;
+    VelState V0;
     ResidState S;
-    residual<HQ, HD>(E, gam, dt, Z, x, res, S);
+    velocity_part<HQ, HD>(dt, Z, x, V0);
+    residual_with<HQ, HD>(E, gam, dt, Z, x, V0, res, S);
 #pragma unroll
     for (int col = 0; col < NF; ++col) {
         double xp[NF];
@@ -366,7 +398,13 @@ __device__ __forceinline__ void jacobian_fd(const EmhdArgs& E, double gam, doubl
         if (fabs(x[col]) < (0.5 * delta)) xp[col] = x[col] + delta;
         else xp[col] = (1 + delta) * x[col];
         double rp[NF];
-        residual<HQ, HD>(E, gam, dt, Z, xp, rp, S);
+        if (col >= 2 && col <= 4) {
+            VelState V;
+            velocity_part<HQ, HD>(dt, Z, xp, V);
+            residual_with<HQ, HD>(E, gam, dt, Z, xp, V, rp, S);
+        } else {
+            residual_with<HQ, HD>(E, gam, dt, Z, xp, V0, rp, S);
+        }
         const double h = xp[col] - x[col] + SMALL;
 #pragma unroll
         for (int row = 0; row < NF; ++row) J[row][col] = (rp[row] - res[row]) / h;
@@ -378,7 +416,9 @@ __device__ __forceinline__ void jacobian_fd(const EmhdArgs& E, double gam, doubl
 //   rho, u      enter through eta, p_gas and (EMHD) q, dP via Theta and cs2
 //   u~1..u~3    enter through u^mu, u_mu, b^mu, b_mu and b^2 (Lorentz factor, lowering, b^0)
 //   q~, dP~     enter linearly through q, dP and their conserved forms
-// then the product rule through T^t_mu, the conserved variables and the EMHD source terms.
+// then the product rule through T^t_mu, the conserved variables and the EMHD source terms.  The
+// tangent is not bound to the reference's operation order, so divisions are replaced by products
+// with reciprocals computed once.
 template <bool HQ, bool HD>
 __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, double dt,
                                                const ResidZone<Imp<HQ, HD>::NF>& Z, const double* x,
@@ -386,34 +426,42 @@ __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, do
 {
     using I = Imp<HQ, HD>;
     constexpr int NF = I::NF;
+    VelState V;
     ResidState S;
-    residual<HQ, HD>(E, gam, dt, Z, x, res, S);
+    velocity_part<HQ, HD>(dt, Z, x, V);
+    residual_with<HQ, HD>(E, gam, dt, Z, x, V, res, S);
     const CenterGeom& G = Z.G;
-    const FourVec<double>& D = S.D;
+    const FourVec<double>& D = V.D;
     const double u0 = D.ucon[0], b0 = D.bcon[0];
-    const double gdet = G.gdet, tau = Z.tau, rho = x[0], uu = x[1];
+    const double gdet = G.gdet, rho = x[0], uu = x[1];
+    const double inv_dt = 1. / dt, inv_u0 = 1. / u0, inv_rho = 1. / rho;
+    const double inv_tau = I::EM ? 1. / Z.tau : 0.;
+    const double gdt = gdet * inv_dt;
     const bool emt = I::EM && E.feedback;
     // EMHD tensor pieces: T^t_mu = ... + (q/|b|) X_mu - dP Y_mu
-    double X[4], Y[4], qb = 0., fq = 1., fd = 1.;
+    double X[4], Y[4], qb = 0., fq = 1., fd = 1., inv_bsq = 0., inv_bmag = 0.;
     double dq[2] = {0., 0.}, ddP[2] = {0., 0.};
     if (emt) {
-        qb = S.q / S.bmag;
+        inv_bsq = 1. / S.bsq;
+        inv_bmag = 1. / S.bmag;
+        qb = S.q * inv_bmag;
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu) {
             X[mu] = u0 * D.bcov[mu] + b0 * D.ucov[mu];
-            Y[mu] = b0 * D.bcov[mu] / S.bsq - ((double)(mu == 0) + u0 * D.ucov[mu]) / 3.;
+            Y[mu] = b0 * D.bcov[mu] * inv_bsq - ((double)(mu == 0) + u0 * D.ucov[mu]) * (1. / 3.);
         }
         if (E.higher_order_terms) {
-            const double Th = S.Theta, cs2 = S.cs2, den = rho + gam * uu;
-            const double dTh[2] = {-Th / rho, (gam - 1) / rho};
-            const double dcs2[2] = {-cs2 / den, (gam * (gam - 1) - gam * cs2) / den};
+            const double Th = S.Theta, cs2 = S.cs2, inv_den = 1. / (rho + gam * uu);
+            const double dTh[2] = {-Th * inv_rho, (gam - 1) * inv_rho};
+            const double dcs2[2] = {-cs2 * inv_den, (gam * (gam - 1) - gam * cs2) * inv_den};
             const double qt = HQ ? x[I::IQ] : 0., dPt = HD ? x[I::ID] : 0.;
             double sq, sd, dsq[2], dsd[2];
             if (E.closure == CL_KAPPA_ETA) {
-                sq = E.kappa * Th * Th / E.tau;
-                sd = E.eta * Th / E.tau;
+                const double kt = E.kappa / E.tau, et = E.eta / E.tau;
+                sq = kt * Th * Th;
+                sd = et * Th;
 #pragma unroll
-                for (int a = 0; a < 2; ++a) { dsq[a] = 2. * E.kappa * Th * dTh[a] / E.tau; dsd[a] = E.eta * dTh[a] / E.tau; }
+                for (int a = 0; a < 2; ++a) { dsq[a] = 2. * kt * Th * dTh[a]; dsd[a] = et * dTh[a]; }
             } else {
                 const double ac = E.conduction_alpha, av = E.viscosity_alpha;
                 sq = rho * ac * cs2 * Th * Th;
@@ -421,17 +469,15 @@ __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, do
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
                     const double dr = (a == 0) ? 1. : 0.;
-                    dsq[a] = ac * (dr * cs2 * Th * Th + rho * dcs2[a] * Th * Th + 2. * rho * cs2 * Th * dTh[a]);
+                    dsq[a] = ac * Th * (dr * cs2 * Th + rho * dcs2[a] * Th + 2. * rho * cs2 * dTh[a]);
                     dsd[a] = av * (dr * cs2 * Th + rho * dcs2[a] * Th + rho * cs2 * dTh[a]);
                 }
             }
             fq = sqrt(sq);
             fd = sqrt(sd);
+            const double hq = (fq > 0.) ? 0.5 * qt / fq : 0., hd = (fd > 0.) ? 0.5 * dPt / fd : 0.;
 #pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                dq[a] = (fq > 0.) ? qt * dsq[a] / (2. * fq) : 0.;
-                ddP[a] = (fd > 0.) ? dPt * dsd[a] / (2. * fd) : 0.;
-            }
+            for (int a = 0; a < 2; ++a) { dq[a] = hq * dsq[a]; ddP[a] = hd * dsd[a]; }
         }
     }
     // Fills column k from the tangent of T^t_mu (dT), of u^t (du0), of dt_Theta and of div u and
@@ -439,15 +485,15 @@ __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, do
     auto column = [&](int k, const double* dT, double drho, double du0, double dqt, double ddPt,
                       double ddt_Theta, double ddiv, const double* dtu) {
         double dU[NF];
-        dU[0] = (drho * u0 + rho * du0) * gdet;
-        dU[1] = dT[0] * gdet + dU[0];
-        dU[2] = dT[1] * gdet;
-        dU[3] = dT[2] * gdet;
-        dU[4] = dT[3] * gdet;
-        if (HQ) dU[I::IQ] = (dqt * u0 + x[I::IQ] * du0) * gdet;
-        if (HD) dU[I::ID] = (ddPt * u0 + x[I::ID] * du0) * gdet;
+        dU[0] = (drho * u0 + rho * du0) * gdt;
+        dU[1] = dT[0] * gdt + dU[0];
+        dU[2] = dT[1] * gdt;
+        dU[3] = dT[2] * gdt;
+        dU[4] = dT[3] * gdt;
+        if (HQ) dU[I::IQ] = (dqt * u0 + x[I::IQ] * du0) * gdt;
+        if (HD) dU[I::ID] = (ddPt * u0 + x[I::ID] * du0) * gdt;
 #pragma unroll
-        for (int row = 0; row < NF; ++row) J[row][k] = dU[row] / dt;
+        for (int row = 0; row < NF; ++row) J[row][k] = dU[row];
         if (HQ) {
             double dq0 = Z.cq0 * ddt_Theta;
             if (dtu) {
@@ -455,10 +501,9 @@ __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, do
                 for (int mu = 0; mu < 4; ++mu) dq0 -= Z.cq[mu] * dtu[mu];
             }
             if (E.higher_order_terms) dq0 *= Z.fac_q;
-            double dsrc = gdet * (dq0 / tau);
+            double dsrc = gdet * dq0 * inv_tau;
             if (E.higher_order_terms) dsrc += Z.gq * ddiv;
-            double dr = J[I::IQ][k] + 0.5 * gdet * (dqt / tau) - dsrc;
-            dr *= tau;
+            double dr = (dU[I::IQ] + 0.5 * gdet * dqt * inv_tau - dsrc) * Z.tau;
             if (E.higher_order_terms) dr *= Z.norm_q;
             J[I::IQ][k] = dr;
         }
@@ -469,45 +514,46 @@ __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, do
                 for (int mu = 0; mu < 4; ++mu) dd0 += Z.cd[mu] * dtu[mu];
             }
             if (E.higher_order_terms) dd0 *= Z.fac_d;
-            double dsrc = gdet * (dd0 / tau);
+            double dsrc = gdet * dd0 * inv_tau;
             if (E.higher_order_terms) dsrc += Z.gd * ddiv;
-            double dr = J[I::ID][k] + 0.5 * gdet * (ddPt / tau) - dsrc;
-            dr *= tau;
+            double dr = (dU[I::ID] + 0.5 * gdet * ddPt * inv_tau - dsrc) * Z.tau;
             if (E.higher_order_terms) dr *= Z.norm_d;
             J[I::ID][k] = dr;
         }
     };
-    const double dThn = (gam - 1) / dt;
+    const double dThn = (gam - 1) * inv_dt * inv_rho;
     // rho: d eta = 1
     {
         double dT[4];
+        const double a = dq[0] * inv_bmag, c = ddP[0];
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu) {
             dT[mu] = u0 * D.ucov[mu];
-            if (emt) dT[mu] += (dq[0] / S.bmag) * X[mu] - ddP[0] * Y[mu];
+            if (emt) dT[mu] += a * X[mu] - c * Y[mu];
         }
-        column(0, dT, 1., 0., 0., 0., S.theta_clamped ? 0. : -dThn * uu / (rho * rho), 0., nullptr);
+        column(0, dT, 1., 0., 0., 0., S.theta_clamped ? 0. : -dThn * uu * inv_rho, 0., nullptr);
     }
     // u: d eta = gam, d p_tot = gam - 1
     {
         double dT[4];
+        const double a = dq[1] * inv_bmag, c = ddP[1];
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu) {
             dT[mu] = gam * u0 * D.ucov[mu] + (gam - 1) * (double)(mu == 0);
-            if (emt) dT[mu] += (dq[1] / S.bmag) * X[mu] - ddP[1] * Y[mu];
+            if (emt) dT[mu] += a * X[mu] - c * Y[mu];
         }
-        column(1, dT, 0., 0., 0., 0., S.theta_clamped ? 0. : dThn / rho, 0., nullptr);
+        column(1, dT, 0., 0., 0., 0., S.theta_clamped ? 0. : dThn, 0., nullptr);
     }
     // velocities
-    const double alpha = 1. / sqrt(-G.gcon0[0]);
+    const double inv_alpha = sqrt(-G.gcon0[0]), alpha = 1. / inv_alpha, inv_gamma = 1. / V.gamma;
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
         double gk = 0.;
 #pragma unroll
         for (int w = 0; w < 3; ++w) gk += G.gcov[v+1][w+1] * x[2 + w];
-        const double dgam = gk / S.gamma;
+        const double dgam = gk * inv_gamma;
         double du[4], dul[4], db[4], dbl[4];
-        du[0] = dgam / alpha;
+        du[0] = dgam * inv_alpha;
 #pragma unroll
         for (int m = 1; m < 4; ++m) du[m] = (double)(m - 1 == v) - alpha * G.gcon0[m] * dgam;
         lower4(G.gcov, du, dul);
@@ -516,7 +562,7 @@ __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, do
         for (int w = 0; w < 3; ++w) d0 += Z.B[w] * dul[w+1];
         db[0] = d0;
 #pragma unroll
-        for (int m = 1; m < 4; ++m) db[m] = (d0 * D.ucon[m] + b0 * du[m] - D.bcon[m] * du[0]) / u0;
+        for (int m = 1; m < 4; ++m) db[m] = (d0 * D.ucon[m] + b0 * du[m] - D.bcon[m] * du[0]) * inv_u0;
         lower4(G.gcov, db, dbl);
         const double dbs = S.bsq_clamped ? 0. : 2. * dot4(D.bcov, db);
         double dT[4];
@@ -525,25 +571,27 @@ __device__ __forceinline__ void jacobian_exact(const EmhdArgs& E, double gam, do
             dT[mu] = dbs * u0 * D.ucov[mu] + S.eta * (du[0] * D.ucov[mu] + u0 * dul[mu])
                    + 0.5 * dbs * (double)(mu == 0) - (db[0] * D.bcov[mu] + b0 * dbl[mu]);
         if (emt) {
-            const double dqb = -S.q * (dbs / (2. * S.bmag)) / (S.bmag * S.bmag);
+            const double dqb = -S.q * 0.5 * dbs * inv_bmag * inv_bsq;
+            const double yb = b0 * dbs * inv_bsq * inv_bsq;
 #pragma unroll
             for (int mu = 0; mu < 4; ++mu) {
                 const double dX = du[0] * D.bcov[mu] + u0 * dbl[mu] + db[0] * D.ucov[mu] + b0 * dul[mu];
-                const double dY = (db[0] * D.bcov[mu] + b0 * dbl[mu]) / S.bsq - b0 * D.bcov[mu] * dbs / (S.bsq * S.bsq)
-                                - (du[0] * D.ucov[mu] + u0 * dul[mu]) / 3.;
+                const double dY = (db[0] * D.bcov[mu] + b0 * dbl[mu]) * inv_bsq - yb * D.bcov[mu]
+                                - (du[0] * D.ucov[mu] + u0 * dul[mu]) * (1. / 3.);
                 dT[mu] += dqb * X[mu] + qb * dX - S.dP * dY;
             }
         }
         double dtu[4], ddiv = 0.;
 #pragma unroll
-        for (int mu = 0; mu < 4; ++mu) { dtu[mu] = dul[mu] / dt; ddiv += G.gcon0[mu] * dtu[mu]; }
+        for (int mu = 0; mu < 4; ++mu) { dtu[mu] = dul[mu] * inv_dt; ddiv += G.gcon0[mu] * dtu[mu]; }
         column(2 + v, dT, 0., du[0], 0., 0., 0., ddiv, dtu);
     }
     // q~ and dP~
     if (HQ) {
         double dT[4];
+        const double a = fq * inv_bmag;
 #pragma unroll
-        for (int mu = 0; mu < 4; ++mu) dT[mu] = emt ? (fq / S.bmag) * X[mu] : 0.;
+        for (int mu = 0; mu < 4; ++mu) dT[mu] = emt ? a * X[mu] : 0.;
         column(I::IQ, dT, 0., 0., 1., 0., 0., 0., nullptr);
     }
     if (HD) {
@@ -912,7 +960,6 @@ __global__ void __launch_bounds__(128) k_implicit_iter(Dims d, DevGeom g, double
                 failed_now = true;
             }
             if (!failed_now) {
-                ResidState S;
                 if (ip.linesearch) {
                     double nrm = 0.;
 #pragma unroll
@@ -924,7 +971,7 @@ __global__ void __launch_bounds__(128) k_implicit_iter(Dims d, DevGeom g, double
                         double xl[NF];
 #pragma unroll
                         for (int p = 0; p < NF; ++p) xl[p] = x[p] + (lambda * delta[p]);
-                        residual<HQ, HD>(E, gam, dt, Z, xl, res, S);
+                        residual<HQ, HD>(E, gam, dt, Z, xl, res);
                         nrm = 0.;
 #pragma unroll
                         for (int p = 0; p < NF; ++p) nrm += res[p]*res[p];
@@ -939,7 +986,7 @@ __global__ void __launch_bounds__(128) k_implicit_iter(Dims d, DevGeom g, double
                 }
 #pragma unroll
                 for (int p = 0; p < NF; ++p) x[p] += lambda * delta[p];
-                residual<HQ, HD>(E, gam, dt, Z, x, res, S);
+                residual<HQ, HD>(E, gam, dt, Z, x, res);
                 double nrm = 0;
 #pragma unroll
                 for (int p = 0; p < NF; ++p) nrm += res[p]*res[p];
