@@ -10,8 +10,11 @@ SANE field at beta_min = 100, MC reconstruction, LLF, flux-CT, drift-frame floor
 zone-cycle is one interior zone advanced one RK2 step.  Synthetic data: the initial state is built
 by kharma_b200.problems.fm_torus from a seeded RNG (u jitter +-4%).
 
-For N > 1 (torchrun) every rank advances its own 128^3 block (weak scaling, replicas: no domain
-decomposition and no halo exchange in this path yet); time = max over ranks.
+For N > 1 (torchrun) the torus is n1 x n2 x (128 N) zones split into x3 slabs, one 128^3 slab per
+rank (weak scaling): per stage the ranks exchange one plane of fluid primitives and pflag before
+the inversion fixups and 4 planes of every primitive and conserved variable after the physical
+boundaries (NCCL point-to-point), and reduce the timestep (allreduce MIN) every step; time = max
+over ranks.
 
 --impl reference times the reference algorithm on the host cores: the CPU oracle (a restatement of
 KHARMA's hot path; kharma.host itself cannot be built here), on a bounded slab of the same torus.
@@ -49,6 +52,8 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-kernel-times", action="store_true")
     ap.add_argument("--no-emhd", action="store_true")
+    ap.add_argument("--slab-path", action="store_true",
+                    help="at N = 1, step the block through the x3-slab path (one slab, local exchange)")
     ap.add_argument("--emhd-only", action="store_true",
                     help="run only the implicit EMHD Newton measurement and print its JSON object")
     return ap.parse_args()
@@ -289,6 +294,7 @@ def emhd_newton(n=128, reps=3):
 def gpu_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
+    from kharma_b200 import problems
     from kharma_b200.block import Block, Driver
     from kharma_b200.spec import torus_spec
 
@@ -298,11 +304,24 @@ def gpu_arm(args, rank, world, local_rank):
     geom, P0 = make_state(spec)
     zones = n1 * n2 * n3
 
+    def make(precision):
+        """N = 1: the whole block, khb_step per step.  N > 1: this rank's 128^3 slab of a
+        n1 x n2 x (n3 N) torus (x3 decomposition, NCCL halo exchange, global dt reduction)."""
+        if world == 1 and not args.slab_path:
+            b = Block(torus_spec(n1, n2, n3, precision=precision), geometry=geom)
+            b.set_prims(P0)
+            return b, Driver(b)
+        from kharma_b200 import slabs as sl
+        local = world == 1
+        gspec = torus_spec(n1, n2, n3 * world, precision=precision)
+        ex = sl.LocalExchange() if local else sl.DistExchange()
+        sb = sl.SlabBlock(gspec, world, rank, ex, geometry=geom)
+        Ploc = P0 if local else problems.fm_torus(sb.spec, geom, seed=1234 + rank)
+        sl.set_prims([sb], ex, [Ploc], local=local)
+        return sb.block, sl.SlabDriver([sb], ex, local=local)
+
     def run(precision, steps, warmup, sampler=None):
-        sp = torus_spec(n1, n2, n3, precision=precision)
-        b = Block(sp, geometry=geom)
-        b.set_prims(P0)
-        drv = Driver(b)
+        b, drv = make(precision)
         for _ in range(warmup):
             drv.step()
         torch.cuda.synchronize()
@@ -337,7 +356,7 @@ def gpu_arm(args, rank, world, local_rank):
 
     # FP32-flux form on the same workload
     fp32 = None
-    if not args.no_fp32:
+    if not args.no_fp32 and world == 1:
         b32, _, ms32, _, _ = run("fp32_flux", args.steps, args.warmup)
         t32 = torch.tensor([ms32], dtype=torch.float64, device="cuda")
         if world > 1:
@@ -395,7 +414,7 @@ def gpu_arm(args, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     roofline = None
     ktimes = None
-    if not args.no_kernel_times:
+    if not args.no_kernel_times and world == 1:
         ktimes = kernel_times(b, spec)
         tot = {k: v[0] * v[1] for k, v in ktimes.items()}
         dom = max(tot, key=tot.get)
@@ -433,9 +452,11 @@ def gpu_arm(args, rank, world, local_rank):
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": f"FM torus FMKS {n1}x{n2}x{n3} one meshblock per GPU",
+               "config": {"workload": (f"FM torus FMKS {n1}x{n2}x{n3} one meshblock per GPU" if world == 1 else
+                                       f"FM torus FMKS {n1}x{n2}x{n3 * world}, one {n1}x{n2}x{n3} x3 slab per GPU"),
                           "recon": "linear_mc", "flux": "llf", "b_field": "flux_ct", "inverter": "onedw",
-                          "floors": "drift", "parallelism": f"replicas x{world}",
+                          "floors": "drift",
+                          "parallelism": "single block" if world == 1 else f"x3 slabs x{world} (NCCL halo exchange)",
                           "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
                "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd}

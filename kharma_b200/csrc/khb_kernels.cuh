@@ -66,13 +66,35 @@ template <> struct FaceTables<float> {
     static __device__ __forceinline__ const float* gdet(const DevGeom& g, int loc) { return g.gdet_f[loc]; }
 };
 
-// FP64 faces: cap registers at 128 so four 128-thread blocks fit per SM (measured faster despite a
-// few bytes of spill); the FP32 form needs fewer registers and is left unconstrained.
-template <typename R> struct FluxMinBlocks { static constexpr int value = 1; };
-template <> struct FluxMinBlocks<double> { static constexpr int value = 4; };
+// Resident 128-thread blocks per SM requested from the compiler for each kernel (register caps
+// of 65536 / (128 x blocks)), chosen by measurement on B200: FP64 faces 5 blocks along x1/x2 and 4
+// along x3, FP32 faces 8, the update half of the zone pass 8 and its inversion half 5.  Each can
+// be overridden at build time.
+#ifndef KHB_FLUX64_MINB
+#define KHB_FLUX64_MINB 5
+#endif
+#ifndef KHB_FLUX64_X3_MINB
+#define KHB_FLUX64_X3_MINB 4
+#endif
+#ifndef KHB_FLUX32_MINB
+#define KHB_FLUX32_MINB 8
+#endif
+#ifndef KHB_ZONE_UPDATE_MINB
+#define KHB_ZONE_UPDATE_MINB 8
+#endif
+#ifndef KHB_ZONE_CELL_MINB
+#define KHB_ZONE_CELL_MINB 5
+#endif
+template <typename R, int DIR> struct FluxMinBlocks { static constexpr int value = KHB_FLUX32_MINB; };
+template <int DIR> struct FluxMinBlocks<double, DIR> {
+    static constexpr int value = (DIR == 3) ? KHB_FLUX64_X3_MINB : KHB_FLUX64_MINB;
+};
+template <int MODE> struct ZoneMinBlocks {
+    static constexpr int value = (MODE == M_UPDATE) ? KHB_ZONE_UPDATE_MINB : ((MODE & M_UTOP) ? KHB_ZONE_CELL_MINB : 1);
+};
 
 template <int DIR, int RECON, int NV, typename R, typename FT>
-__global__ void __launch_bounds__(128, FluxMinBlocks<R>::value)
+__global__ void __launch_bounds__(128, FluxMinBlocks<R, DIR>::value)
 k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop,
        int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, long long total)
 {
@@ -199,7 +221,7 @@ __device__ __forceinline__ double ldf(const FT* F, long long x) { return (double
 // MODE: compile-time mask of M_* steps (0: take the mask from the arguments at run time).  The
 // CFL reduction (M_DT) is always a run-time choice.
 template <int NV, typename FT, int MODE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE>::value)
 k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
 {
     const int mode = MODE ? (MODE | (a.mode & M_DT)) : a.mode;

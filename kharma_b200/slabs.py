@@ -186,3 +186,26 @@ def min_ndt(slabs, local=True):
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
         m = float(t.item())
     return m
+
+
+class SlabDriver:
+    """The reference's timestep schedule (Driver) over decomposed slabs: the per-rank minimum zone
+    timestep is reduced over all slabs (and ranks) before the next dt is chosen."""
+
+    def __init__(self, slabs, exchanger, local=True, dt_start=None):
+        self.slabs = slabs
+        self.ex = exchanger
+        self.local = local
+        spec = slabs[0].spec
+        self.dt = spec.dt_min if dt_start is None else dt_start
+        self.nstep = 0
+
+    def step(self, dt=None):
+        dt = self.dt if dt is None else dt
+        step(self.slabs, self.ex, dt, self.local)
+        mn = min_ndt(self.slabs, self.local)
+        s = self.slabs[0].spec
+        ndt = min(max(mn * s.cfl, s.dt_min), s.max_dt_increase * dt)
+        self.dt = min(2.0 * dt, ndt)
+        self.nstep += 1
+        return dt, mn
