@@ -43,7 +43,7 @@ B_ALG_PER_ZC = 72 * 8          # algorithmic HBM bytes per zone-cycle, 72 * nvar
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="khb", choices=["khb", "reference"])
     ap.add_argument("--size", default="128,128,128")
@@ -364,6 +364,9 @@ def gpu_arm(args, rank, world, local_rank):
         v32 = world * zones / (float(t32.item()) / args.steps / 1000.0)
         fp32 = {"value": v32, "unit": UNIT, "ms_per_step": float(t32.item()) / args.steps,
                 "speedup_vs_fp64": v32 / value}
+        if not args.no_kernel_times:
+            kt32 = kernel_times(b32, b32.spec)
+            fp32["kernel_ms_per_launch"] = {k: round(v[0], 4) for k, v in kt32.items()}
         del b32
         # accuracy: 100 steps of each form from the same state with the FP64 run's dt sequence
         ref = Block(torus_spec(n1, n2, n3), geometry=geom)

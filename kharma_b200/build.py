@@ -4,7 +4,8 @@
 
 Translation units and their arithmetic flags:
   khb_fp64.cu      FP64 path (fluxes, zone pass, ghost zones)      -fmad=false
-  khb_fp32.cu      FP32-flux form (fluxes, EMFs in FP32)           FMA contraction on
+  khb_fp32.cu      FP32-flux form (fluxes, EMFs in FP32)           FMA contraction, fast FP32
+                                                                   divide and square root, FTZ
   khb_api.cu       host side and C ABI
   khb_noalloc.cu   khb_max_divb_noalloc (static device scratch)   -fmad=false
   khb_emhd.cu      EMHD sources and the implicit Newton solve      -fmad=false
@@ -21,7 +22,7 @@ OUT = os.path.join(HERE, "lib", "libkhb.so")
 OBJ = os.path.join(HERE, "lib", "obj")
 UNITS = {
     "khb_fp64.cu": ["-fmad=false"],
-    "khb_fp32.cu": [],
+    "khb_fp32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "khb_api.cu": [],
     "khb_noalloc.cu": ["-fmad=false"],
     "khb_emhd.cu": ["-fmad=false"],

@@ -385,6 +385,35 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
 enum { FF_GEOM_RHO = 32, FF_GEOM_U = 64, FF_B_RHO = 128, FF_B_U = 256, FF_TEMP = 512, FF_GAMMA = 1024,
        FF_KTOT = 2048, FF_GEOM_RHO_FLUX = 4096, FF_GEOM_U_FLUX = 8192 };
 
+// (gam - 1) u / pow(rho, gam) > ktot_max, decided exactly as that expression evaluates, with pow
+// evaluated only when a cheap bound cannot settle the comparison.  The bound takes log2 of each
+// factor from its binary exponent plus a single-precision log2 of its mantissa: the estimate of
+// log2(ktot / ktot_max) is within 2e-6 of the true value for gam <= 4, and the exact quotient is
+// within a few ulp of the true one, so an estimate beyond +-1/64 puts both on the same side.
+// Zero, negative, subnormal, huge or non-finite operands and results near the exponent range take
+// the exact path.
+__device__ __forceinline__ double log2_est(double x)   // x positive and normal
+{
+    int e;
+    const double m = frexp(x, &e);                     // x = m 2^e, m in [0.5, 1)
+    return (double)e + (double)__log2f((float)m);
+}
+__device__ __forceinline__ bool ktot_above(double gam, double rho, double u, double ktot_max)
+{
+    const double a = (gam - 1.) * u;
+    const double dmin = 2.2250738585072014e-308;
+    if (rho >= dmin && a >= dmin && ktot_max >= dmin && rho <= 1e300 && a <= 1e300 && ktot_max <= 1e300 &&
+        gam > 0. && gam <= 4.) {
+        const double lr = gam * log2_est(rho);
+        if (lr > -1000. && lr < 1000.) {
+            const double est = log2_est(a) - lr - log2_est(ktot_max);
+            if (est < -0.015625) return false;
+            if (est > 0.015625) return true;
+        }
+    }
+    return a / pow(rho, gam) > ktot_max;
+}
+
 // floors_functions.hpp:84-160
 // rhoflr_geom, uflr_geom: the geometric floor values of this zone (x3-independent, tabulated per
 // (j,i) at set-up with the same formula, floors_functions.hpp:96-104).  D returns the 4-vectors of P.
@@ -414,7 +443,7 @@ __device__ int determine_floors(const ZoneGeom& G, const Prescription& f, double
         fflag |= (uflr_b > u) * FF_B_U;
     }
     if (lorentz(G.gcov, P[2], P[3], P[4]) > f.gamma_max) fflag |= FF_GAMMA;
-    if ((gam - 1.) * P[1] / pow(P[0], gam) > f.ktot_max) fflag |= FF_KTOT;
+    if (ktot_above(gam, P[0], P[1], f.ktot_max)) fflag |= FF_KTOT;
     if (f.temp_adjust_u && (P[1] / P[0] > f.u_over_rho_max)) fflag |= FF_TEMP;
     return fflag;
 }
@@ -423,13 +452,17 @@ __device__ int determine_floors(const ZoneGeom& G, const Prescription& f, double
 __device__ __forceinline__ void apply_ceilings(const ZoneGeom& G, const Prescription& f, double gam, double* P)
 {
     const double gamma = lorentz(G.gcov, P[2], P[3], P[4]);
-    const double ktot  = (gam - 1.) * P[1] / pow(P[0], gam);
     if (gamma > f.gamma_max) {
         const double fr = sqrt((f.gamma_max*f.gamma_max - 1.) / (gamma*gamma - 1.));
 #pragma unroll
         for (int v = 0; v < 3; ++v) P[2 + v] *= fr;
     }
-    if (ktot > f.ktot_max) P[1] = f.ktot_max / ktot * P[1];
+    // ktot is formed from rho and u before either ceiling changes them (the velocity ceiling above
+    // leaves both alone)
+    if (ktot_above(gam, P[0], P[1], f.ktot_max)) {
+        const double ktot = (gam - 1.) * P[1] / pow(P[0], gam);
+        P[1] = f.ktot_max / ktot * P[1];
+    }
     if (f.temp_adjust_u && P[1] / P[0] > f.u_over_rho_max) P[1] = f.u_over_rho_max * P[0];
 }
 

@@ -30,6 +30,41 @@ __device__ __forceinline__ void zone_kji(const Dims& d, long long c, int& k, int
     k = (int)(r / d.n2);
 }
 
+// Thread -> (k, j, i) of a box [lo, lo + cnt) in 32-bit arithmetic (no 64-bit division).  A block
+// of 128 threads covers 32 consecutive (j, i) plane positions, i fastest, in each of 4 consecutive
+// k planes when the box is at least 4 planes thick (else 128 consecutive positions of one plane), so
+// the four warps of a block read the same x3-independent geometry and three of them find it in L1.
+struct Box {
+    int lo_i, lo_j, lo_k, cnt_i, cnt_j, cnt_k;
+    unsigned np;      // cnt_i * cnt_j
+    unsigned nbp;     // blocks across the plane
+    int kz;           // k planes per block (4 or 1)
+};
+inline Box make_box(int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, int cnt_k)
+{
+    Box b;
+    b.lo_i = lo_i; b.lo_j = lo_j; b.lo_k = lo_k; b.cnt_i = cnt_i; b.cnt_j = cnt_j; b.cnt_k = cnt_k;
+    b.np = (unsigned)cnt_i * (unsigned)cnt_j;
+    b.kz = (cnt_k >= 4) ? 4 : 1;
+    const unsigned per = (b.kz == 4) ? 32u : 128u;
+    b.nbp = (b.np + per - 1) / per;
+    return b;
+}
+inline unsigned box_blocks(const Box& b) { return b.nbp * (unsigned)((b.cnt_k + b.kz - 1) / b.kz); }
+__device__ __forceinline__ bool box_cell(const Box& b, int& i, int& j, int& k)
+{
+    const unsigned per = (b.kz == 4) ? 32u : 128u;
+    const unsigned w = threadIdx.x / per, q = threadIdx.x - w * per;
+    const unsigned bk = blockIdx.x / b.nbp, bp = blockIdx.x - bk * b.nbp;
+    const unsigned p = bp * per + q, kk = bk * (unsigned)b.kz + w;
+    if (p >= b.np || kk >= (unsigned)b.cnt_k) return false;
+    const unsigned jj = p / (unsigned)b.cnt_i;
+    i = b.lo_i + (int)(p - jj * (unsigned)b.cnt_i);
+    j = b.lo_j + (int)jj;
+    k = b.lo_k + (int)kk;
+    return true;
+}
+
 // Load the centre geometry of zone (j,i)
 __device__ __forceinline__ void load_zone_geom(const DevGeom& g, int j, int i, ZoneGeom& G)
 {
@@ -95,16 +130,11 @@ template <int MODE> struct ZoneMinBlocks {
 
 template <int DIR, int RECON, int NV, typename R, typename FT>
 __global__ void __launch_bounds__(128, FluxMinBlocks<R, DIR>::value)
-k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop,
-       int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, long long total)
+k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop, Box bx)
 {
     constexpr int dir = DIR;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const int i = lo_i + (int)(t % cnt_i);
-    const long long r = t / cnt_i;
-    const int j = lo_j + (int)(r % cnt_j);
-    const int k = lo_k + (int)(r / cnt_j);
+    int i, j, k;
+    if (!box_cell(bx, i, j, k)) return;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     const long long st = (dir == 1) ? 1 : ((dir == 2) ? d.sj : d.sk);
     const int loc = dir - 1;
@@ -222,19 +252,13 @@ __device__ __forceinline__ double ldf(const FT* F, long long x) { return (double
 // CFL reduction (M_DT) is always a run-time choice.
 template <int NV, typename FT, int MODE>
 __global__ void __launch_bounds__(128, ZoneMinBlocks<MODE>::value)
-k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a)
+k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
 {
     const int mode = MODE ? (MODE | (a.mode & M_DT)) : a.mode;
-    const int cnt_i = d.ie - d.is + 1, cnt_j = d.je - d.js + 1, cnt_k = d.ke - d.ks + 1;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long total = (long long)cnt_i*cnt_j*cnt_k;
-    const bool active = t < total;
+    int i, j, k;
+    const bool active = box_cell(bx, i, j, k);
     double ndt_zone = 1.7976931348623157e308;
     if (active) {
-        const int i = d.is + (int)(t % cnt_i);
-        const long long r = t / cnt_i;
-        const int j = d.js + (int)(r % cnt_j);
-        const int k = d.ks + (int)(r / cnt_j);
         const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
         const long long N = d.N, sj = d.sj, sk = d.sk;
         const double gam = ph.gam;
@@ -732,13 +756,13 @@ template <int DIR, int NV, typename FT>
 static void flux_dir_recon(int recon, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
                            FT* F, FT* ctop, const int lo[3], const int cnt[3], cudaStream_t st)
 {
-    const long long total = (long long)cnt[0]*cnt[1]*cnt[2];
-    const unsigned nb = blocks_for(total, 128);
+    const Box bx = make_box(lo[0], lo[1], lo[2], cnt[0], cnt[1], cnt[2]);
+    const unsigned nb = box_blocks(bx);
     switch (recon) {
-    case RECON_DONOR: k_flux<DIR, RECON_DONOR, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
-    case RECON_MC:    k_flux<DIR, RECON_MC, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
-    case RECON_WENO5: k_flux<DIR, RECON_WENO5, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
-    default:          k_flux<DIR, RECON_PPM, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, lo[0], lo[1], lo[2], cnt[0], cnt[1], total); break;
+    case RECON_DONOR: k_flux<DIR, RECON_DONOR, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
+    case RECON_MC:    k_flux<DIR, RECON_MC, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
+    case RECON_WENO5: k_flux<DIR, RECON_WENO5, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
+    default:          k_flux<DIR, RECON_PPM, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
     }
 }
 
@@ -778,13 +802,13 @@ void Launch<FT>::fix_flux_x1(const Dims& d, FT* F1, int inner, cudaStream_t st)
 template <int NV, typename FT>
 static void zone_nv(const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a, cudaStream_t st)
 {
-    const long long total = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
-    const unsigned nb = blocks_for(total, 128);
+    const Box bx = make_box(d.is, d.js, d.ks, d.ie - d.is + 1, d.je - d.js + 1, d.ke - d.ks + 1);
+    const unsigned nb = box_blocks(bx);
     const int m = a.mode & ~M_DT;
-    if (m == M_ZONE_FUSED) k_zone<NV, FT, M_ZONE_FUSED><<<nb, 128, 0, st>>>(d, g, ph, a);
-    else if (m == M_UPDATE) k_zone<NV, FT, M_UPDATE><<<nb, 128, 0, st>>>(d, g, ph, a);
-    else if (m == M_ZONE_CELL) k_zone<NV, FT, M_ZONE_CELL><<<nb, 128, 0, st>>>(d, g, ph, a);
-    else k_zone<NV, FT, 0><<<nb, 128, 0, st>>>(d, g, ph, a);
+    if (m == M_ZONE_FUSED) k_zone<NV, FT, M_ZONE_FUSED><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
+    else if (m == M_UPDATE) k_zone<NV, FT, M_UPDATE><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
+    else if (m == M_ZONE_CELL) k_zone<NV, FT, M_ZONE_CELL><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
+    else k_zone<NV, FT, 0><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
 }
 
 template <typename FT>
