@@ -310,7 +310,8 @@ int khb_fix_solve(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P
                   const double* solve_fail, void* stream);
 
 /* Launch-shape choices that do not change results (bitwise): "zone_split" = 0 runs the zone pass
- * as one kernel, 1 (the default) as two (update; inversion + floors + P->U). */
+ * as one kernel, 1 (the default) as two (update; inversion + floors + P->U), 2 as three (update;
+ * inversion; floors + P->U). */
 int khb_set_tuning(khb_ctx* ctx, const char* key, int value);
 
 /* Number of device kernel launches issued through this context so far (for accounting). */

@@ -29,7 +29,8 @@ struct khb_ctx {
     bool geom_set;
     int64_t launches;
     unsigned long long dbl_max_bits;   // host source of the reduction reset (outlives async copies)
-    int zone_split;        // 1: run the zone pass as two kernels (update; inversion+floors+P->U)
+    int zone_split;        // zone pass as 1 kernel (0), 2 (1: update; inversion+floors+P->U) or
+                           // 3 (2: update; inversion; floors+P->U)
     // EMHD / implicit solve
     double* conn_d;        // connection Gamma^lam_{mu nu}, [64][n2][n1] with index lam*16 + mu*4 + nu
     double* emhd_tmp;      // EMHD::AddSource temporaries u_mu, Theta: [5][N]
@@ -232,7 +233,14 @@ int zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const kh
     zc.mode = M_UPDATE;
     if ((rc = launch_zone(ctx, zc, st))) return rc;
     zc.Us = Uout;          // the updated conserved state is the inversion's input
-    zc.mode = M_ZONE_CELL | dtm;
+    if (ctx->zone_split == 1) {
+        zc.mode = M_ZONE_CELL | dtm;
+        return launch_zone(ctx, zc, st);
+    }
+    zc.mode = M_UTOP;
+    if ((rc = launch_zone(ctx, zc, st))) return rc;
+    zc.Ps = Pout;          // floors start from the inverted primitives and their flags
+    zc.mode = M_ZONE_FLOORS | dtm;
     return launch_zone(ctx, zc, st);
 }
 
@@ -651,7 +659,11 @@ int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void*
 int khb_set_tuning(khb_ctx* ctx, const char* key, int value)
 {
     if (!ctx || !key) return fail(KHB_ERR_ARG, "khb_set_tuning: NULL argument");
-    if (std::strcmp(key, "zone_split") == 0) { ctx->zone_split = value ? 1 : 0; return KHB_OK; }
+    if (std::strcmp(key, "zone_split") == 0) {
+        if (value < 0 || value > 2) return fail(KHB_ERR_ARG, "khb_set_tuning: zone_split must be 0, 1 or 2");
+        ctx->zone_split = value;
+        return KHB_OK;
+    }
     return fail(KHB_ERR_ARG, std::string("khb_set_tuning: unknown key ") + key);
 }
 

@@ -120,12 +120,21 @@ template <> struct FaceTables<float> {
 #ifndef KHB_ZONE_CELL_MINB
 #define KHB_ZONE_CELL_MINB 5
 #endif
+#ifndef KHB_ZONE_INV_MINB
+#define KHB_ZONE_INV_MINB 6
+#endif
+#ifndef KHB_ZONE_FLOOR_MINB
+#define KHB_ZONE_FLOOR_MINB 6
+#endif
 template <typename R, int DIR> struct FluxMinBlocks { static constexpr int value = KHB_FLUX32_MINB; };
 template <int DIR> struct FluxMinBlocks<double, DIR> {
     static constexpr int value = (DIR == 3) ? KHB_FLUX64_X3_MINB : KHB_FLUX64_MINB;
 };
 template <int MODE> struct ZoneMinBlocks {
-    static constexpr int value = (MODE == M_UPDATE) ? KHB_ZONE_UPDATE_MINB : ((MODE & M_UTOP) ? KHB_ZONE_CELL_MINB : 1);
+    static constexpr int value = (MODE == M_UPDATE) ? KHB_ZONE_UPDATE_MINB :
+                                 (MODE == M_UTOP) ? KHB_ZONE_INV_MINB :
+                                 (MODE == M_ZONE_FLOORS) ? KHB_ZONE_FLOOR_MINB :
+                                 ((MODE & M_UTOP) ? KHB_ZONE_CELL_MINB : 1);
 };
 
 template <int DIR, int RECON, int NV, typename R, typename FT>
@@ -410,8 +419,10 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
             else p_to_u_zone<NV>(G, gam, P, U);
         }
 
+        if (mode & (M_UPDATE | M_FLOORS | M_PTOU)) {
 #pragma unroll
-        for (int p = 0; p < NV; ++p) a.Uout.v[p][c] = U[p];
+            for (int p = 0; p < NV; ++p) a.Uout.v[p][c] = U[p];
+        }
         if (mode & (M_UTOP | M_FLOORS)) {
 #pragma unroll
             for (int p = 0; p < NV; ++p) a.Pout.v[p][c] = P[p];
@@ -571,19 +582,41 @@ __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int
     for (int p = 0; p < 5; ++p) P.v[p][c] = Pz[p];
 }
 
+// Ghost zones of one (j, i) plane, enumerated without the interior: the rows below js, the zones
+// left and right of the interior in rows js..je, the rows above je.  Returns false past the end.
+__device__ __forceinline__ bool plane_ghost(const Dims& d, unsigned t, int& j, int& i)
+{
+    const unsigned n1 = d.n1, side = n1 - (unsigned)(d.ie - d.is + 1);
+    const unsigned below = (unsigned)d.js * n1, rows = (unsigned)(d.je - d.js + 1);
+    const unsigned mid = rows * side, above = (unsigned)(d.n2 - 1 - d.je) * n1;
+    if (t < below) { j = (int)(t / n1); i = (int)(t - (unsigned)j * n1); return true; }
+    t -= below;
+    if (t < mid) {
+        const unsigned r = t / side, q = t - r * side;
+        j = d.js + (int)r;
+        i = (q < (unsigned)d.is) ? (int)q : (int)q + (d.ie - d.is + 1);
+        return true;
+    }
+    t -= mid;
+    if (t < above) { const unsigned r = t / n1; j = d.je + 1 + (int)r; i = (int)(t - r * n1); return true; }
+    return false;
+}
+__host__ __device__ inline unsigned plane_ghost_count(const Dims& d)
+{
+    return (unsigned)(d.n1 * d.n2) - (unsigned)((d.ie - d.is + 1) * (d.je - d.js + 1));
+}
+
 // B_P = B_U/gdet and U = U(P) on the X1/X2 ghost zones of the interior k range
 template <int NV>
 __global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U)
 {
-    const int cnt_k = d.ke - d.ks + 1;
-    const long long plane = (long long)d.n1*d.n2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= plane*cnt_k) return;
-    const int i = (int)(t % d.n1);
-    const int j = (int)((t / d.n1) % d.n2);
-    const int k = d.ks + (int)(t / plane);
-    const bool ghost = (i < d.is || i > d.ie) || (d.ndim > 1 && (j < d.js || j > d.je));
-    if (!ghost) return;
+    const unsigned per = plane_ghost_count(d);
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned kk = t / per;
+    if (kk >= (unsigned)(d.ke - d.ks + 1)) return;
+    int j, i;
+    if (!plane_ghost(d, t - kk * per, j, i)) return;
+    const int k = d.ks + (int)kk;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     ZoneGeom G;
     load_zone_geom(g, j, i, G);
@@ -601,13 +634,30 @@ __global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_field
 
 // Periodic images: every zone outside the interior in a periodic direction copies all variables
 // of P and U from its image (wrapping only the periodic directions).
+// Launched over the zones outside the interior only: the k ghost planes whole, then the X1/X2
+// ghost zones of each interior plane.
 template <int NV>
 __global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= d.N) return;
+    const unsigned plane = (unsigned)(d.n1 * d.n2);
+    const unsigned kg = (unsigned)(d.n3 - (d.ke - d.ks + 1));     // k ghost planes
+    unsigned u = blockIdx.x * blockDim.x + threadIdx.x;
     int k, j, i;
-    zone_kji(d, t, k, j, i);
+    if (u < kg * plane) {
+        const unsigned kp = u / plane, r = u - kp * plane;
+        k = (kp < (unsigned)d.ks) ? (int)kp : d.ke + 1 + (int)(kp - (unsigned)d.ks);
+        j = (int)(r / (unsigned)d.n1);
+        i = (int)(r - (unsigned)j * (unsigned)d.n1);
+    } else {
+        u -= kg * plane;
+        const unsigned per = plane_ghost_count(d);
+        if (per == 0) return;
+        const unsigned kk = u / per;
+        if (kk >= (unsigned)(d.ke - d.ks + 1)) return;
+        if (!plane_ghost(d, u - kk * per, j, i)) return;
+        k = d.ks + (int)kk;
+    }
+    const long long t = ((long long)k*d.n2 + j)*d.n1 + i;
     int ii = i, jj = j, kk = k;
     bool any = false;
     if ((pmask & 1) && (i < d.is || i > d.ie)) { ii += (i < d.is) ? d.nx1 : -d.nx1; any = true; }
@@ -808,6 +858,8 @@ static void zone_nv(const Dims& d, const DevGeom& g, const Phys& ph, const ZoneA
     if (m == M_ZONE_FUSED) k_zone<NV, FT, M_ZONE_FUSED><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
     else if (m == M_UPDATE) k_zone<NV, FT, M_UPDATE><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
     else if (m == M_ZONE_CELL) k_zone<NV, FT, M_ZONE_CELL><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
+    else if (m == M_UTOP) k_zone<NV, FT, M_UTOP><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
+    else if (m == M_ZONE_FLOORS) k_zone<NV, FT, M_ZONE_FLOORS><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
     else k_zone<NV, FT, 0><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
 }
 
@@ -855,15 +907,19 @@ void LaunchCommon::bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, c
 void LaunchCommon::ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
                               const khb_fields& U, cudaStream_t st)
 {
-    const long long tot = (long long)d.n1*d.n2*(d.ke - d.ks + 1);
+    const long long tot = (long long)plane_ghost_count(d)*(d.ke - d.ks + 1);
+    if (tot == 0) return;
     if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U);
     else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U);
 }
 
 void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st)
 {
-    if (nv == 8) k_periodic<8><<<blocks_for(d.N, 256), 256, 0, st>>>(d, P, U, pmask);
-    else k_periodic<5><<<blocks_for(d.N, 256), 256, 0, st>>>(d, P, U, pmask);
+    const long long nint = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
+    const long long tot = d.N - nint;
+    if (tot == 0) return;
+    if (nv == 8) k_periodic<8><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
+    else k_periodic<5><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
 }
 
 void LaunchCommon::ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,

@@ -56,6 +56,8 @@ struct Phys {
 enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST = 32 };
 // The whole zone pass in one kernel, or its two halves (update; inversion + floors + P->U)
 enum { M_ZONE_CELL = M_UTOP | M_FLOORS | M_PTOU | M_FAILLIST, M_ZONE_FUSED = M_UPDATE | M_ZONE_CELL };
+// ... or in three (update; inversion; floors + P->U)
+enum { M_ZONE_FLOORS = M_FLOORS | M_PTOU | M_FAILLIST };
 
 template <typename FT>
 struct ZoneArgs {
