@@ -48,10 +48,10 @@ enum { KHB_OK = 0, KHB_ERR_ARG = -1, KHB_ERR_CUDA = -2, KHB_ERR_STATE = -3, KHB_
 enum { KHB_RECON_DONOR_CELL = 0, KHB_RECON_LINEAR_MC = 1, KHB_RECON_WENO5 = 2, KHB_RECON_PPM = 3 };
 /* Riemann solvers (flux/flux.hpp:110-121) */
 enum { KHB_FLUX_LLF = 0, KHB_FLUX_HLLE = 1 };
-/* Boundary types per face (boundaries/boundaries.cpp:57-368).  KHB_BC_EXCHANGE (x3 faces only)
- * marks a face whose ghost planes the caller fills from the neighbouring block (Parthenon's
- * boundary communication): khb_boundaries leaves them alone, and khb_fix_utop reads the
- * neighbour values there instead of wrapping. */
+/* Boundary types per face (boundaries/boundaries.cpp:57-368).  KHB_BC_EXCHANGE (any face of an
+ * active direction) marks a face whose ghost zones the caller fills from the neighbouring block
+ * (Parthenon's boundary communication): khb_boundaries and the flux fixes leave it alone, and
+ * khb_fix_utop reads the neighbour values there. */
 enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2, KHB_BC_EXCHANGE = 3 };
 /* Floor injection frames (floors/floors.hpp:96) */
 enum { KHB_FRAME_FLUID = 0, KHB_FRAME_NORMAL = 1, KHB_FRAME_DRIFT = 2 };
@@ -205,7 +205,9 @@ int khb_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* strea
 /* One RK2 stage (stage = 1 or 2) with Parthenon's rk2 weights: fluxes in all active directions,
  * flux fixes, then ONE fused zone pass doing flux-CT, divergence, geometric source, the RK
  * combination, 1D_W inversion, floors and the lock-step P->U; then fixups of failed zones and
- * ghost zones.  P_s/U_s are the stage input, U_0 the step-start conserved state, P_out/U_out the
+ * ghost zones.  A block with exchange faces first carries the ghost shell of P_s/U_s over to
+ * P_out/U_out (the reference's P_s -> P_{s+1} guess copy, kharma_driver.cpp:380-384), as it stands
+ * until the caller's exchange replaces it.  P_s/U_s are the stage input, U_0 the step-start conserved state, P_out/U_out the
  * result.  P_out may alias P_s only if the caller does not need P_s afterwards AND stage == 2
  * is not reading it (use distinct buffers).  On the last stage the minimum zone timestep is
  * accumulated on the device (read with khb_get_min_ndt). */
@@ -250,6 +252,53 @@ int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void*
  * share the array and race; serialize them.  Errors: khb_noalloc_last_error(). */
 int khb_max_divb_noalloc(const khb_config* cfg, const khb_fields* U, double* max_divb_out, void* stream);
 const char* khb_noalloc_last_error(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Batches of meshblocks (no single counterpart in the reference: Parthenon's MeshData packs run the
+ * same task list over all blocks of a partition, kharma_step.cpp:77-319, with uniform block
+ * sizes).  Every block of a mesh, of uneven sizes, goes through one launch per kernel per RK stage;
+ * the step can be replayed from a CUDA graph; the tile shape per block size is chosen by timing.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct khb_batch khb_batch;
+
+/* Group nblocks contexts (each created and given its geometry as for a single block; sizes may
+ * differ, while nvar, dimension, reconstruction, Riemann solver and precision must agree) with the
+ * state each block is stepped on: P[b], U[b] (its fields), pflag[b], fflag[b] (its flags).  The
+ * contexts and arrays must outlive the batch.  Ghost zones of exchange faces are the caller's;
+ * physical and periodic faces are filled per block as khb_boundaries does. */
+int khb_batch_create(khb_ctx* const* blocks, int nblocks, const khb_fields* P, const khb_fields* U,
+                     int32_t* const* pflag, int32_t* const* fflag, khb_batch** out);
+int khb_batch_destroy(khb_batch* batch);
+
+/* One RK2 step of every block in place: the arithmetic of khb_step on each block (bitwise), with
+ * each kernel launched once per stage for all blocks.  No host synchronisation. */
+int khb_batch_step(khb_batch* batch, double dt, void* stream);
+
+/* The same step replayed from a CUDA graph captured on the first call on a non-default stream
+ * (captured again after khb_batch_set_tuning or khb_batch_autotune).  dt is read from device memory
+ * by the kernels, so one graph serves every timestep. */
+int khb_batch_step_graph(khb_batch* batch, double dt, void* stream);
+
+/* Minimum zone timestep over all blocks from the last step, as khb_get_min_ndt.  Synchronizes. */
+int khb_batch_get_min_ndt(khb_batch* batch, double* min_ndt_host, void* stream);
+
+/* Block-size classes (distinct nx1, nx2, nx3) in order of first appearance: sizes[3 c + a] and
+ * the planes per CTA kz[c] of each (0 = the default shape); up to max classes are written. */
+int khb_batch_classes(khb_batch* batch, int32_t* nclasses, int32_t* sizes, int32_t* kz, int max);
+
+/* Tile shape of one class (kz = 1, 2 or 4 k planes per 128-thread CTA, 0 = default; size_class < 0
+ * leaves the classes alone) and the launch mode: persistent = 1 sizes each grid to the SMs times
+ * the CTAs each can hold, and the CTAs loop over the tiles; 0 launches one CTA per tile. */
+int khb_batch_set_tuning(khb_batch* batch, int size_class, int kz, int persistent);
+
+/* Autotuner: for each class in turn, time reps runs of a stage-1 pass with each tile shape and
+ * keep the fastest; then the same for the launch mode.  Stage 1 writes only the contexts' stage
+ * scratch, the flags and the failed-zone lists, so the state is unchanged.  Writes the chosen kz
+ * per class and the launch mode.  Synchronizes. */
+int khb_batch_autotune(khb_batch* batch, int reps, int32_t* kz_out, int32_t* persistent_out, void* stream);
+
+/* Device kernel launches issued for this batch so far (a graph replay counts its nodes). */
+int64_t khb_batch_launch_count(khb_batch* batch);
 
 /* ---------------------------------------------------------------------------------------------
  * Extended MHD and the implicit solve (emhd/, implicit/)

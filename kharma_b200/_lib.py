@@ -131,6 +131,16 @@ SIGNATURES = {
                                    C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
                                    C.POINTER(KhbFields), C.POINTER(KhbFields), _D, _P, _P, _P]),
     "khb_fix_solve": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P]),
+    "khb_batch_create": (_I, [C.POINTER(_P), _I, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(_P),
+                              C.POINTER(_P), C.POINTER(_P)]),
+    "khb_batch_destroy": (_I, [_P]),
+    "khb_batch_step": (_I, [_P, _D, _P]),
+    "khb_batch_step_graph": (_I, [_P, _D, _P]),
+    "khb_batch_get_min_ndt": (_I, [_P, C.POINTER(_D), _P]),
+    "khb_batch_classes": (_I, [_P, C.POINTER(C.c_int32), _P, _P, _I]),
+    "khb_batch_set_tuning": (_I, [_P, _I, _I, _I]),
+    "khb_batch_autotune": (_I, [_P, _I, _P, C.POINTER(C.c_int32), _P]),
+    "khb_batch_launch_count": (C.c_int64, [_P]),
 }
 
 _lib = None

@@ -7,6 +7,7 @@ Translation units and their arithmetic flags:
   khb_fp32.cu      FP32-flux form (fluxes, EMFs in FP32)           FMA contraction, fast FP32
                                                                    divide and square root, FTZ
   khb_api.cu       host side and C ABI
+  khb_batch.cu     batches of meshblocks: tile tables, CUDA graph, autotuner
   khb_noalloc.cu   khb_max_divb_noalloc (static device scratch)   -fmad=false
   khb_emhd.cu      EMHD sources and the implicit Newton solve      -fmad=false
   khb_geometry.cpp host construction of the geometry tables
@@ -24,11 +25,12 @@ UNITS = {
     "khb_fp64.cu": ["-fmad=false"],
     "khb_fp32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "khb_api.cu": [],
+    "khb_batch.cu": [],
     "khb_noalloc.cu": ["-fmad=false"],
     "khb_emhd.cu": ["-fmad=false"],
     "khb_geometry.cpp": [],
 }
-HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", os.path.join("..", "..", "include", "khb.h")]
+HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", "khb_internal.hpp", os.path.join("..", "..", "include", "khb.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 

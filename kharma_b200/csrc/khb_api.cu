@@ -9,34 +9,7 @@
 
 using namespace khb;
 
-struct khb_ctx {
-    khb_config cfg;
-    Dims d;
-    Phys ph;
-    DevGeom g;
-    int nv;
-    bool fp32;
-    void* F[3];            // raw face fluxes, [nv][N] of FT
-    void* ctop[3];         // max(cmax, cmin) per face, [N] of FT
-    void* emf;             // corner EMFs for khb_flux_ct, [3][N] of FT
-    double* stageP;        // intermediate RK stage
-    double* stageU;
-    unsigned long long* words;   // [0] min zone dt bits, [1] max divB bits
-    int* fail_count;
-    int* fail_list;
-    double* geo_d;
-    float* geo_f;
-    bool geom_set;
-    int64_t launches;
-    unsigned long long dbl_max_bits;   // host source of the reduction reset (outlives async copies)
-    int zone_split;        // zone pass as 1 kernel (0), 2 (1: update; inversion+floors+P->U) or
-                           // 3 (2: update; inversion; floors+P->U)
-    // EMHD / implicit solve
-    double* conn_d;        // connection Gamma^lam_{mu nu}, [64][n2][n1] with index lam*16 + mu*4 + nu
-    double* emhd_tmp;      // EMHD::AddSource temporaries u_mu, Theta: [5][N]
-    double* fix_buf;       // FixSolve replacement values: [7][N]
-    unsigned long long* imp_words;   // implicit-solve reductions, IMP_WORDS entries
-};
+#include "khb_internal.hpp"
 
 namespace {
 
@@ -103,16 +76,16 @@ int launch_fix_flux_t(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
     FT* F1 = (FT*)ctx->F[0]; FT* F2 = (FT*)ctx->F[1]; FT* F3 = (FT*)ctx->F[2];
     if (d.ndim >= 2 && (ph.zero_polar_flux || (ctx->nv > 5 && ph.fix_polar_flux))) {
         for (int face = 2; face <= 3; ++face) {
-            if (d.bc[face] == KHB_BC_PERIODIC) continue;
+            if (!phys_face(d.bc[face])) continue;
             Launch<FT>::fix_flux_x2(ctx->nv, d, ph, F1, F2, F3, face == 2, st);
             KHB_LAUNCHED(ctx);
         }
     }
-    if (ph.check_inflow_in && d.bc[0] != KHB_BC_PERIODIC) {
+    if (ph.check_inflow_in && phys_face(d.bc[0])) {
         Launch<FT>::fix_flux_x1(d, F1, 1, st);
         KHB_LAUNCHED(ctx);
     }
-    if (ph.check_inflow_out && d.bc[1] != KHB_BC_PERIODIC) {
+    if (ph.check_inflow_out && phys_face(d.bc[1])) {
         Launch<FT>::fix_flux_x1(d, F1, 0, st);
         KHB_LAUNCHED(ctx);
     }
@@ -172,19 +145,19 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
     bool physical = false;
     // X1 faces over the interior j range, then X2 faces over all i, then the corner fix
     for (int face = 0; face < 2; ++face) {
-        if (d.bc[face] == KHB_BC_PERIODIC) continue;
+        if (!phys_face(d.bc[face])) continue;
         physical = true;
         LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, d.js, d.je - d.js + 1, d.ks, cnt_k, st);
         KHB_LAUNCHED(ctx);
     }
     if (d.ndim >= 2) {
         for (int face = 2; face < 4; ++face) {
-            if (d.bc[face] == KHB_BC_PERIODIC) continue;
+            if (!phys_face(d.bc[face])) continue;
             physical = true;
             LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, 0, d.n1, d.ks, cnt_k, st);
             KHB_LAUNCHED(ctx);
         }
-        if (ctx->cfg.fix_corner_inner && d.bc[0] != KHB_BC_PERIODIC && d.bc[3] != KHB_BC_PERIODIC) {
+        if (ctx->cfg.fix_corner_inner && phys_face(d.bc[0]) && phys_face(d.bc[3])) {
             LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, 0, 0, d.n2, d.ks, cnt_k, st);
             KHB_LAUNCHED(ctx);
         }
@@ -206,8 +179,24 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
 
 size_t ft_size(const khb_ctx* ctx) { return ctx->fp32 ? sizeof(float) : sizeof(double); }
 
-// Parthenon "rk2" low-storage weights: gam0 = {0, 1/2}, gam1 = {1, 1/2}, beta = {1, 1/2}
-const double kRkGam0[2] = {0.0, 0.5}, kRkGam1[2] = {1.0, 0.5}, kRkBeta[2] = {1.0, 0.5};
+bool has_exchange_face(const Dims& d)
+{
+    for (int f = 0; f < 2 * d.ndim; ++f)
+        if (d.bc[f] == KHB_BC_EXCHANGE) return true;
+    return false;
+}
+
+// Ghost shell of the stage input carried to the output (blocks with exchange faces only), before
+// the zone pass so that the fixups see the neighbour values across exchange faces
+int launch_ghost_copy(khb_ctx* ctx, const khb_fields& Ps, const khb_fields& Us, const khb_fields& Pout,
+                      const khb_fields& Uout, cudaStream_t st)
+{
+    if (!has_exchange_face(ctx->d) || (Ps.v[0] == Pout.v[0] && Us.v[0] == Uout.v[0])) return KHB_OK;
+    LaunchCommon::ghost_copy(ctx->nv, ctx->d, Ps, Us, Pout, Uout, st);
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
 
 int zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
               const khb_fields& U0, const khb_fields& Pout, const khb_fields& Uout,
@@ -252,12 +241,20 @@ int do_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb
     for (int dir = 1; dir <= ctx->d.ndim; ++dir)
         if ((rc = launch_flux(ctx, dir, Ps, st))) return rc;
     if ((rc = launch_fix_flux(ctx, ctx->ph, st))) return rc;
+    if ((rc = launch_ghost_copy(ctx, Ps, Us, Pout, Uout, st))) return rc;
     if ((rc = zone_pass(ctx, stage, dt, Ps, Us, U0, Pout, Uout, pflag, fflag, st))) return rc;
     if ((rc = launch_fixup(ctx, Pout, Uout, pflag, st))) return rc;
     return launch_boundaries(ctx, Pout, Uout, st);
 }
 
 } // namespace
+
+int khb::set_error(int code, const std::string& msg) { return fail(code, msg); }
+int khb::ctx_fix_flux(khb_ctx* ctx, cudaStream_t st) { return launch_fix_flux(ctx, ctx->ph, st); }
+int khb::ctx_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
+{
+    return launch_boundaries(ctx, P, U, st);
+}
 
 int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why)
 {
@@ -272,12 +269,17 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
     }
     for (int x = 0; x < 6; ++x) {
         if (cfg->bc[x] < KHB_BC_PERIODIC || cfg->bc[x] > KHB_BC_EXCHANGE) { *why = "unknown boundary type"; return KHB_ERR_ARG; }
-        if (cfg->bc[x] == KHB_BC_EXCHANGE && (x < 4 || cfg->nx3 == 1)) {
-            *why = "exchange boundaries are supported on active x3 faces only";
+        const bool active = x < 2 || (x < 4 ? cfg->nx2 > 1 : cfg->nx3 > 1);
+        if (cfg->bc[x] == KHB_BC_EXCHANGE && !active) {
+            *why = "exchange boundaries are supported on faces of active directions only";
             return KHB_ERR_UNSUPPORTED;
         }
     }
-    if ((cfg->bc[4] == KHB_BC_PERIODIC) != (cfg->bc[5] == KHB_BC_PERIODIC)) { *why = "x3 periodic on one face only"; return KHB_ERR_ARG; }
+    for (int x = 0; x < 6; x += 2)
+        if ((cfg->bc[x] == KHB_BC_PERIODIC) != (cfg->bc[x + 1] == KHB_BC_PERIODIC)) {
+            *why = "periodic on one face of a direction only";
+            return KHB_ERR_ARG;
+        }
     std::memset(&d, 0, sizeof(d));
     std::memset(&ph, 0, sizeof(ph));
     d.nx1 = cfg->nx1; d.nx2 = cfg->nx2; d.nx3 = cfg->nx3;
@@ -354,6 +356,9 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     if (e == cudaSuccess) e = alloc((void**)&c->fail_count, sizeof(int) * 4);
     if (e == cudaSuccess) e = alloc((void**)&c->fail_list, sizeof(int) * N);
     if (e == cudaSuccess) e = alloc((void**)&c->imp_words, sizeof(unsigned long long) * IMP_WORDS);
+    // the memsets above run on the legacy default stream, which the caller's (non-blocking) streams
+    // do not wait for: finish them before the context is handed out
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         khb_destroy(c);
         return fail(KHB_ERR_CUDA, std::string("khb_create: ") + cudaGetErrorString(e));
@@ -425,6 +430,9 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
     }
     KHB_CUDA(cudaMemcpy(ctx->geo_d, h.data(), total*sizeof(double), cudaMemcpyHostToDevice));
     KHB_CUDA(cudaMemcpy(ctx->geo_f, hf.data(), hf.size()*sizeof(float), cudaMemcpyHostToDevice));
+    // a copy from pageable memory may return before it lands, and kernels on non-blocking streams
+    // do not wait for the legacy stream: complete the upload before any kernel can read it
+    KHB_CUDA(cudaDeviceSynchronize());
     DevGeom& g = ctx->g;
     g.G1 = G1; g.G2 = G2; g.n1 = d.n1; g.gs = (long long)gs;
     for (int loc = 0; loc < 4; ++loc) {
@@ -644,7 +652,7 @@ int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void*
     if (ctx->nv < 8 || ctx->d.ndim < 2) { *max_divb_host = 0.; return KHB_OK; }
     const Dims& d = ctx->d;
     // b_flux_ct.cpp:554-564: skip the X1 corners of physical boundaries without Bflux0 fixes
-    const int avoid_in = d.bc[0] != KHB_BC_PERIODIC, avoid_out = d.bc[1] != KHB_BC_PERIODIC;
+    const int avoid_in = phys_face(d.bc[0]), avoid_out = phys_face(d.bc[1]);
     const int i_lo = d.is + avoid_in, i_hi = d.ie + !avoid_out;
     KHB_CUDA(cudaMemsetAsync(ctx->words + 1, 0, sizeof(unsigned long long), S(stream)));
     LaunchCommon::divb(d, ctx->ph, *U, i_lo, i_hi, ctx->words + 1, S(stream));
@@ -704,6 +712,7 @@ int khb_set_connection(khb_ctx* ctx, const double* conn)
         KHB_CUDA(cudaMemset(ctx->fix_buf, 0, 7 * N * sizeof(double)));
     }
     KHB_CUDA(cudaMemcpy(ctx->conn_d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    KHB_CUDA(cudaDeviceSynchronize());          // complete the upload (see khb_set_geometry)
     return KHB_OK;
 }
 

@@ -1,0 +1,50 @@
+// khb_internal.hpp -- the context object and host helpers shared by the host units of libkhb
+// (khb_api.cu, khb_batch.cu).  Not part of the C ABI.
+#pragma once
+
+#include "khb_types.cuh"
+
+#include <string>
+
+struct khb_ctx {
+    khb_config cfg;
+    khb::Dims d;
+    khb::Phys ph;
+    khb::DevGeom g;
+    int nv;
+    bool fp32;
+    void* F[3];            // raw face fluxes, [nv][N] of FT
+    void* ctop[3];         // max(cmax, cmin) per face, [N] of FT
+    void* emf;             // corner EMFs for khb_flux_ct, [3][N] of FT
+    double* stageP;        // intermediate RK stage
+    double* stageU;
+    unsigned long long* words;   // [0] min zone dt bits, [1] max divB bits
+    int* fail_count;
+    int* fail_list;
+    double* geo_d;
+    float* geo_f;
+    bool geom_set;
+    int64_t launches;
+    unsigned long long dbl_max_bits;   // host source of the reduction reset (outlives async copies)
+    int zone_split;        // zone pass as 1 kernel (0), 2 (1: update; inversion+floors+P->U) or
+                           // 3 (2: update; inversion; floors+P->U)
+    // EMHD / implicit solve
+    double* conn_d;        // connection Gamma^lam_{mu nu}, [64][n2][n1] with index lam*16 + mu*4 + nu
+    double* emhd_tmp;      // EMHD::AddSource temporaries u_mu, Theta: [5][N]
+    double* fix_buf;       // FixSolve replacement values: [7][N]
+    unsigned long long* imp_words;   // implicit-solve reductions, IMP_WORDS entries
+};
+
+
+namespace khb {
+
+// Parthenon "rk2" low-storage weights: gam0 = {0, 1/2}, gam1 = {1, 1/2}, beta = {1, 1/2}
+constexpr double kRkGam0[2] = {0.0, 0.5}, kRkGam1[2] = {1.0, 0.5}, kRkBeta[2] = {1.0, 0.5};
+
+// Record an error message for khb_last_error and return code
+int set_error(int code, const std::string& msg);
+// Flux fixes and ghost zones of one block, as khb_stage issues them
+int ctx_fix_flux(khb_ctx* ctx, cudaStream_t st);
+int ctx_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st);
+
+} // namespace khb

@@ -31,32 +31,16 @@ __device__ __forceinline__ void zone_kji(const Dims& d, long long c, int& k, int
 }
 
 // Thread -> (k, j, i) of a box [lo, lo + cnt) in 32-bit arithmetic (no 64-bit division).  A block
-// of 128 threads covers 32 consecutive (j, i) plane positions, i fastest, in each of 4 consecutive
-// k planes when the box is at least 4 planes thick (else 128 consecutive positions of one plane), so
-// the four warps of a block read the same x3-independent geometry and three of them find it in L1.
-struct Box {
-    int lo_i, lo_j, lo_k, cnt_i, cnt_j, cnt_k;
-    unsigned np;      // cnt_i * cnt_j
-    unsigned nbp;     // blocks across the plane
-    int kz;           // k planes per block (4 or 1)
-};
-inline Box make_box(int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, int cnt_k)
+// of 128 threads covers 128/kz consecutive (j, i) plane positions, i fastest, in each of kz
+// consecutive k planes (kz = 1, 2 or 4; by default 4 when the box is at least 4 planes thick, else
+// 1), so the warps of a block read the same x3-independent geometry and all but the first find it
+// in L1.
+// blk: the block's index within the box (blockIdx.x for a single-box launch)
+__device__ __forceinline__ bool box_cell(const Box& b, unsigned blk, int& i, int& j, int& k)
 {
-    Box b;
-    b.lo_i = lo_i; b.lo_j = lo_j; b.lo_k = lo_k; b.cnt_i = cnt_i; b.cnt_j = cnt_j; b.cnt_k = cnt_k;
-    b.np = (unsigned)cnt_i * (unsigned)cnt_j;
-    b.kz = (cnt_k >= 4) ? 4 : 1;
-    const unsigned per = (b.kz == 4) ? 32u : 128u;
-    b.nbp = (b.np + per - 1) / per;
-    return b;
-}
-inline unsigned box_blocks(const Box& b) { return b.nbp * (unsigned)((b.cnt_k + b.kz - 1) / b.kz); }
-__device__ __forceinline__ bool box_cell(const Box& b, int& i, int& j, int& k)
-{
-    const unsigned per = (b.kz == 4) ? 32u : 128u;
-    const unsigned w = threadIdx.x / per, q = threadIdx.x - w * per;
-    const unsigned bk = blockIdx.x / b.nbp, bp = blockIdx.x - bk * b.nbp;
-    const unsigned p = bp * per + q, kk = bk * (unsigned)b.kz + w;
+    const unsigned w = threadIdx.x >> b.pshift, q = threadIdx.x & ((1u << b.pshift) - 1u);
+    const unsigned bk = blk / b.nbp, bp = blk - bk * b.nbp;
+    const unsigned p = (bp << b.pshift) + q, kk = bk * (unsigned)b.kz + w;
     if (p >= b.np || kk >= (unsigned)b.cnt_k) return false;
     const unsigned jj = p / (unsigned)b.cnt_i;
     i = b.lo_i + (int)(p - jj * (unsigned)b.cnt_i);
@@ -138,12 +122,10 @@ template <int MODE> struct ZoneMinBlocks {
 };
 
 template <int DIR, int RECON, int NV, typename R, typename FT>
-__global__ void __launch_bounds__(128, FluxMinBlocks<R, DIR>::value)
-k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop, Box bx)
+__device__ __forceinline__ void flux_face(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                                          FT* __restrict__ F, FT* __restrict__ ctop, int i, int j, int k)
 {
     constexpr int dir = DIR;
-    int i, j, k;
-    if (!box_cell(bx, i, j, k)) return;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     const long long st = (dir == 1) ? 1 : ((dir == 2) ? d.sj : d.sk);
     const int loc = dir - 1;
@@ -207,6 +189,15 @@ k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restr
     ctop[c] = (FT)kmax(cmax, cmin);
 }
 
+template <int DIR, int RECON, int NV, typename R, typename FT>
+__global__ void __launch_bounds__(128, FluxMinBlocks<R, DIR>::value)
+k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restrict__ ctop, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    flux_face<DIR, RECON, NV, R, FT>(d, g, ph, P, F, ctop, i, j, k);
+}
+
 // ===================================================================================== flux fixes
 // B_FluxCT::ZeroBoundaryFlux on X2 faces (b_flux_ct.cpp:404-430) and KBoundaries::FixFlux
 // (boundaries.cpp:611-690) for inflow checks on X1 faces and zero polar fluxes on X2 faces.
@@ -259,15 +250,14 @@ __device__ __forceinline__ double ldf(const FT* F, long long x) { return (double
 
 // MODE: compile-time mask of M_* steps (0: take the mask from the arguments at run time).  The
 // CFL reduction (M_DT) is always a run-time choice.
+// One zone of the zone pass; returns the zone's timestep for the CFL minimum (DBL_MAX if none)
 template <int NV, typename FT, int MODE>
-__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE>::value)
-k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
+__device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a,
+                                            int i, int j, int k)
 {
     const int mode = MODE ? (MODE | (a.mode & M_DT)) : a.mode;
-    int i, j, k;
-    const bool active = box_cell(bx, i, j, k);
     double ndt_zone = 1.7976931348623157e308;
-    if (active) {
+    {
         const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
         const long long N = d.N, sj = d.sj, sk = d.sk;
         const double gam = ph.gam;
@@ -318,8 +308,8 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
                     fb[1][2][1] = d3 ? (double)((FT)0.5 * (e1(c + sj) + e1(c + sj + sk))) : ldf(F2, B3 + c + sj);
                     // KBoundaries zero_polar_flux after flux-CT (boundaries.cpp:672-684)
                     if (ph.zero_polar_flux) {
-                        if (j == d.js && d.bc[2] != KHB_BC_PERIODIC) { fb[1][0][0] = 0.; fb[1][1][0] = 0.; fb[1][2][0] = 0.; }
-                        if (j == d.je && d.bc[3] != KHB_BC_PERIODIC) { fb[1][0][1] = 0.; fb[1][1][1] = 0.; fb[1][2][1] = 0.; }
+                        if (j == d.js && phys_face(d.bc[2])) { fb[1][0][0] = 0.; fb[1][1][0] = 0.; fb[1][2][0] = 0.; }
+                        if (j == d.je && phys_face(d.bc[3])) { fb[1][0][1] = 0.; fb[1][1][1] = 0.; fb[1][2][1] = 0.; }
                     }
                     if (d3) {
                         fb[2][0][0] = (double)((FT)0.5 * (e2(c) + e2(c + 1)));
@@ -441,47 +431,70 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
             if (!isnan(z)) ndt_zone = z;
         }
     }
-    if (mode & M_DT) {
-        // block minimum by warp shuffles, then one atomic per block on the bit pattern (values >= 0)
-        double v = ndt_zone;
+    return ndt_zone;
+}
+
+// Block minimum of the zone timesteps by warp shuffles, then one atomic per block on the bit
+// pattern (values >= 0).  Every thread of the 128-thread block must call it.
+__device__ __forceinline__ void block_min_ndt(double v, unsigned long long* word)
+{
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-        __shared__ double wmin[4];
-        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = v;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double m = wmin[0];
-            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin(m, wmin[w]);
-            if (m >= 0.0) atomicMin(a.ndt_word, (unsigned long long)__double_as_longlong(m));
-        }
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ double wmin[4];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = wmin[0];
+        for (int w = 1; w < 4; ++w) m = fmin(m, wmin[w]);
+        if (m >= 0.0) atomicMin(word, (unsigned long long)__double_as_longlong(m));
     }
+}
+
+template <int NV, typename FT, int MODE>
+__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE>::value)
+k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
+{
+    int i, j, k;
+    double ndt_zone = 1.7976931348623157e308;
+    if (box_cell(bx, blockIdx.x, i, j, k)) ndt_zone = zone_body<NV, FT, MODE>(d, g, ph, a, i, j, k);
+    if (a.mode & M_DT) block_min_ndt(ndt_zone, a.ndt_word);
 }
 
 // ===================================================================================== fixups
 // fixup.cpp:47-156.  Neighbours in periodic directions wrap; across exchanged x3 faces they are
 // read from the ghost planes; in other directions they must be interior.  Failed zones never read each other, so one pass over the list is race-free.
 template <int NV>
-__global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, const int32_t* pflag,
-                        const int* fail_count, const int* fail_list)
+__device__ __forceinline__ void fixup_zone(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                                           const khb_fields& U, const int32_t* pflag, long long c)
 {
-    const int n = *fail_count;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const long long c = fail_list[t];
+    {
         int k, j, i;
         zone_kji(d, c, k, j, i);
+        // the list holds interior zones only; anything else is skipped, since its neighbours across an
+        // exchange face would lie outside the block
+        if (c < 0 || c >= d.N || i < d.is || i > d.ie || j < d.js || j > d.je || k < d.ks || k > d.ke) return;
         double wsum = 0., sum[5] = {0., 0., 0., 0., 0.};
         if (ph.fix_avg) {
             for (int nn = -1; nn <= 1; nn++) for (int m = -1; m <= 1; m++) for (int l = -1; l <= 1; l++) {
                 int ii = i + l, jj = j + m, kk = k + nn;
-                if (ii < d.is || ii > d.ie) { if (d.bc[0] != KHB_BC_PERIODIC) continue; ii += (ii < d.is) ? d.nx1 : -d.nx1; }
-                if (jj < d.js || jj > d.je) { if (d.ndim < 2 || d.bc[2] != KHB_BC_PERIODIC) continue; jj += (jj < d.js) ? d.nx2 : -d.nx2; }
+                // exchanged faces hold the neighbouring block's values in the ghost zones;
+                // periodic directions wrap; other faces end the neighbourhood
+                if (ii < d.is || ii > d.ie) {
+                    const int bc = d.bc[(ii < d.is) ? 0 : 1];
+                    if (bc == KHB_BC_PERIODIC) ii += (ii < d.is) ? d.nx1 : -d.nx1;
+                    else if (bc != KHB_BC_EXCHANGE) continue;
+                }
+                if (jj < d.js || jj > d.je) {
+                    const int bc = d.bc[(jj < d.js) ? 2 : 3];
+                    if (d.ndim < 2) continue;
+                    if (bc == KHB_BC_PERIODIC) jj += (jj < d.js) ? d.nx2 : -d.nx2;
+                    else if (bc != KHB_BC_EXCHANGE) continue;
+                }
                 if (kk < d.ks || kk > d.ke) {
-                    // exchanged faces hold the neighbouring block's values in the ghost planes
-                    const bool exch = (kk < d.ks) ? d.bc[4] == KHB_BC_EXCHANGE : d.bc[5] == KHB_BC_EXCHANGE;
-                    if (!exch) {
-                        if (d.ndim < 3 || d.bc[4] != KHB_BC_PERIODIC) continue;
-                        kk += (kk < d.ks) ? d.nx3 : -d.nx3;
-                    }
+                    const int bc = d.bc[(kk < d.ks) ? 4 : 5];
+                    if (d.ndim < 3) continue;
+                    if (bc == KHB_BC_PERIODIC) kk += (kk < d.ks) ? d.nx3 : -d.nx3;
+                    else if (bc != KHB_BC_EXCHANGE) continue;
                 }
                 const long long cn = ((long long)kk*d.n2 + jj)*d.n1 + ii;
                 if (!(pflag[cn] > 0)) {
@@ -508,6 +521,15 @@ __global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, 
 #pragma unroll
         for (int p = 0; p < NV; ++p) U.v[p][c] = Uz[p];
     }
+}
+
+template <int NV>
+__global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, const int32_t* pflag,
+                        const int* fail_count, const int* fail_list)
+{
+    const int n = *fail_count;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        fixup_zone<NV>(d, g, ph, P, U, pflag, fail_list[t]);
 }
 
 // ===================================================================================== boundaries
@@ -669,6 +691,59 @@ __global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
     for (int p = 0; p < NV; ++p) { P.v[p][t] = P.v[p][s]; U.v[p][t] = U.v[p][s]; }
 }
 
+// The ghost shell (every zone outside the interior) of a stage's input copied to its output: the
+// stage's copy of P_s into P_{s+1} as the inversion guess (kharma_driver.cpp:380-384) and U = U(P)
+// there, as they stand before the caller's boundary exchange replaces them.  Needed only for blocks
+// with exchange faces; physical and periodic faces are filled afterwards by the boundary kernels.
+__device__ __forceinline__ bool shell_zone(const Dims& d, unsigned u, long long& c)
+{
+    const unsigned plane = (unsigned)(d.n1 * d.n2);
+    const unsigned kg = (unsigned)(d.n3 - (d.ke - d.ks + 1));
+    int k, j, i;
+    if (u < kg * plane) {
+        const unsigned kp = u / plane, r = u - kp * plane;
+        k = (kp < (unsigned)d.ks) ? (int)kp : d.ke + 1 + (int)(kp - (unsigned)d.ks);
+        j = (int)(r / (unsigned)d.n1);
+        i = (int)(r - (unsigned)j * (unsigned)d.n1);
+    } else {
+        u -= kg * plane;
+        const unsigned per = plane_ghost_count(d);
+        if (per == 0) return false;
+        const unsigned kk = u / per;
+        if (kk >= (unsigned)(d.ke - d.ks + 1)) return false;
+        if (!plane_ghost(d, u - kk * per, j, i)) return false;
+        k = d.ks + (int)kk;
+    }
+    c = ((long long)k*d.n2 + j)*d.n1 + i;
+    return true;
+}
+template <int NV>
+__device__ __forceinline__ void copy_zone(const khb_fields& Pin, const khb_fields& Uin, const khb_fields& Pout,
+                                          const khb_fields& Uout, long long c)
+{
+#pragma unroll
+    for (int p = 0; p < NV; ++p) { Pout.v[p][c] = Pin.v[p][c]; Uout.v[p][c] = Uin.v[p][c]; }
+}
+template <int NV>
+__global__ void k_ghost_copy(Dims d, khb_fields Pin, khb_fields Uin, khb_fields Pout, khb_fields Uout)
+{
+    long long c;
+    if (shell_zone(d, blockIdx.x * blockDim.x + threadIdx.x, c)) copy_zone<NV>(Pin, Uin, Pout, Uout, c);
+}
+// One row of CTAs per block (blockIdx.y), grid-striding over that block's shell
+template <int NV>
+__global__ void k_batch_ghost_copy(const FixupBlock* __restrict__ blocks, int stage)
+{
+    const FixupBlock& B = blocks[blockIdx.y];
+    if (!B.exch) return;
+    const int s = stage - 1;
+    const unsigned n = (unsigned)(B.d.N - (long long)(B.d.ie - B.d.is + 1)*(B.d.je - B.d.js + 1)*(B.d.ke - B.d.ks + 1));
+    for (unsigned u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        long long c;
+        if (shell_zone(B.d, u, c)) copy_zone<NV>(B.Pin[s], B.Uin[s], B.P[s], B.U[s], c);
+    }
+}
+
 // Whole-block P->U (Flux::MeshPtoU)
 template <int NV>
 __global__ void k_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U)
@@ -801,6 +876,93 @@ __global__ void __launch_bounds__(256) k_divb(Dims d, Phys ph, khb_fields U, int
 }
 #endif
 
+// ===================================================================================== batches
+// Every meshblock of a batch in one launch per kernel: a CTA takes tiles (128-thread boxes of one
+// block) from the tile table, stages that block's descriptor in shared memory and runs the same
+// per-face / per-zone code as the single-block kernels on it.  With a persistent grid each CTA
+// walks the table with a stride of gridDim.x.
+template <typename T>
+__device__ __forceinline__ void stage_desc(T& dst, const T* __restrict__ src)
+{
+    static_assert(sizeof(T) % 8 == 0, "descriptor size must be a multiple of 8 bytes");
+    const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* o = reinterpret_cast<unsigned long long*>(&dst);
+    for (unsigned x = threadIdx.x; x < sizeof(T) / 8; x += blockDim.x) o[x] = __ldg(s + x);
+}
+
+template <int DIR, int RECON, int NV, typename R, typename FT>
+__global__ void __launch_bounds__(128, FluxMinBlocks<R, DIR>::value)
+k_batch_flux(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ tiles, unsigned ntiles, int stage)
+{
+    __shared__ __align__(16) BatchBlock<FT> sb;
+    int cur = -1;
+    for (unsigned t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int b = __ldg(tiles + t);
+        if (b != cur) {
+            __syncthreads();
+            stage_desc(sb, blocks + b);
+            __syncthreads();
+            cur = b;
+        }
+        int i, j, k;
+        if (box_cell(sb.fbox[DIR - 1], t - sb.tile0[DIR - 1], i, j, k))
+            flux_face<DIR, RECON, NV, R, FT>(sb.d, sb.g, sb.ph, sb.Pin[stage - 1], sb.F[DIR - 1], sb.ctop[DIR - 1],
+                                            i, j, k);
+    }
+}
+
+template <int NV, typename FT, int MODE>
+__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE>::value)
+k_batch_zone(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ tiles, unsigned ntiles, int stage,
+             int dtm, double beta, const double* __restrict__ dt)
+{
+    __shared__ __align__(16) BatchBlock<FT> sb;
+    const int s = stage - 1;
+    int cur = -1;
+    for (unsigned t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int b = __ldg(tiles + t);
+        if (b != cur) {
+            __syncthreads();
+            stage_desc(sb, blocks + b);
+            __syncthreads();                          // the whole descriptor is in place before the patch
+            if (threadIdx.x == 0) {
+                sb.za[s].bdt = beta * __ldg(dt);      // as the single-block path forms beta * dt
+                sb.za[s].mode = dtm;
+                if (MODE & M_UTOP) sb.za[s].Us = sb.za[s].Uout;   // the inversion reads the updated state
+            }
+            __syncthreads();
+            cur = b;
+        }
+        int i, j, k;
+        double ndt_zone = 1.7976931348623157e308;
+        if (box_cell(sb.zbox, t - sb.tile0[3], i, j, k)) ndt_zone = zone_body<NV, FT, MODE>(sb.d, sb.g, sb.ph, sb.za[s], i, j, k);
+        if (dtm & M_DT) {
+            block_min_ndt(ndt_zone, sb.za[s].ndt_word);
+            __syncthreads();          // wmin is reused by the next tile of this CTA
+        }
+    }
+}
+
+#ifdef KHB_COMMON_KERNELS
+// One row of CTAs per block (blockIdx.y), each walking that block's failed-zone list
+template <int NV>
+__global__ void k_batch_fixup(const FixupBlock* __restrict__ blocks, int stage)
+{
+    const FixupBlock& B = blocks[blockIdx.y];
+    if (!B.ph.fix_avg && !B.ph.fix_atmo) return;
+    const int s = stage - 1;
+    const int n = *B.fail_count;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        fixup_zone<NV>(B.d, B.g, B.ph, B.P[s], B.U[s], B.pflag, B.fail_list[t]);
+}
+__global__ void k_batch_reset(int* const* counts, int nblocks, unsigned long long* word)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nblocks) *counts[t] = 0;
+    if (t == 0 && word) *word = 0x7FEFFFFFFFFFFFFFull;     // bit pattern of DBL_MAX
+}
+#endif
+
 // ===================================================================================== launchers
 template <int DIR, int NV, typename FT>
 static void flux_dir_recon(int recon, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
@@ -885,7 +1047,85 @@ void Launch<FT>::copy_flux(long long N, int nv, const FT* F, const FT* ctop, con
     k_copy_flux<FT><<<blocks_for(N, 256), 256, 0, st>>>(N, nv, F, ctop, out, ctop_out);
 }
 
+// Batched flux launch; ntiles == 0 returns the resident CTAs per SM of the kernel
+template <int DIR, int NV, typename FT>
+static int batch_flux_dir(int recon, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles, unsigned grid,
+                          int stage, cudaStream_t st)
+{
+    const void* fn;
+    switch (recon) {
+    case RECON_DONOR: fn = (const void*)k_batch_flux<DIR, RECON_DONOR, NV, FT, FT>; break;
+    case RECON_MC:    fn = (const void*)k_batch_flux<DIR, RECON_MC, NV, FT, FT>; break;
+    case RECON_WENO5: fn = (const void*)k_batch_flux<DIR, RECON_WENO5, NV, FT, FT>; break;
+    default:          fn = (const void*)k_batch_flux<DIR, RECON_PPM, NV, FT, FT>; break;
+    }
+    if (ntiles == 0) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, 0);
+        return occ;
+    }
+    const unsigned nb = grid ? grid : ntiles;
+    switch (recon) {
+    case RECON_DONOR: k_batch_flux<DIR, RECON_DONOR, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage); break;
+    case RECON_MC:    k_batch_flux<DIR, RECON_MC, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage); break;
+    case RECON_WENO5: k_batch_flux<DIR, RECON_WENO5, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage); break;
+    default:          k_batch_flux<DIR, RECON_PPM, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage); break;
+    }
+    return 0;
+}
+template <int NV, typename FT>
+static int batch_flux_nv(int recon, int dir, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
+                         unsigned grid, int stage, cudaStream_t st)
+{
+    if (dir == 1) return batch_flux_dir<1, NV, FT>(recon, blocks, tiles, ntiles, grid, stage, st);
+    if (dir == 2) return batch_flux_dir<2, NV, FT>(recon, blocks, tiles, ntiles, grid, stage, st);
+    return batch_flux_dir<3, NV, FT>(recon, blocks, tiles, ntiles, grid, stage, st);
+}
+template <typename FT>
+int Launch<FT>::batch_flux(int recon, int nv, int dir, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
+                           unsigned grid, int stage, cudaStream_t st)
+{
+    return (nv == 8) ? batch_flux_nv<8, FT>(recon, dir, blocks, tiles, ntiles, grid, stage, st)
+                     : batch_flux_nv<5, FT>(recon, dir, blocks, tiles, ntiles, grid, stage, st);
+}
+
+template <int NV, typename FT, int MODE>
+static int batch_zone_mode(const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles, unsigned grid, int stage,
+                           int dtm, double beta, const double* dt, cudaStream_t st)
+{
+    if (ntiles == 0) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_batch_zone<NV, FT, MODE>, 128, 0);
+        return occ;
+    }
+    k_batch_zone<NV, FT, MODE><<<grid ? grid : ntiles, 128, 0, st>>>(blocks, tiles, ntiles, stage, dtm, beta, dt);
+    return 0;
+}
+template <typename FT>
+int Launch<FT>::batch_zone(int nv, int mode, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
+                           unsigned grid, int stage, int dtm, double beta, const double* dt, cudaStream_t st)
+{
+    if (nv == 8) {
+        if (mode == M_UPDATE) return batch_zone_mode<8, FT, M_UPDATE>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+        return batch_zone_mode<8, FT, M_ZONE_CELL>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+    }
+    if (mode == M_UPDATE) return batch_zone_mode<5, FT, M_UPDATE>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+    return batch_zone_mode<5, FT, M_ZONE_CELL>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+}
+
 #ifdef KHB_COMMON_KERNELS
+void LaunchCommon::batch_fixup(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st)
+{
+    const dim3 grid(4, nblocks);
+    if (nv == 8) k_batch_fixup<8><<<grid, 128, 0, st>>>(blocks, stage);
+    else k_batch_fixup<5><<<grid, 128, 0, st>>>(blocks, stage);
+}
+
+void LaunchCommon::batch_reset(int* const* counts, int nblocks, unsigned long long* word, cudaStream_t st)
+{
+    k_batch_reset<<<blocks_for(nblocks, 128), 128, 0, st>>>(counts, nblocks, word);
+}
+
 void LaunchCommon::fixup(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
                          const khb_fields& U, const int32_t* pflag, const int* fail_count, const int* fail_list,
                          cudaStream_t st)
@@ -920,6 +1160,23 @@ void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const kh
     if (tot == 0) return;
     if (nv == 8) k_periodic<8><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
     else k_periodic<5><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
+}
+
+void LaunchCommon::ghost_copy(int nv, const Dims& d, const khb_fields& Pin, const khb_fields& Uin,
+                              const khb_fields& Pout, const khb_fields& Uout, cudaStream_t st)
+{
+    const long long nint = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
+    const long long tot = d.N - nint;
+    if (tot == 0) return;
+    if (nv == 8) k_ghost_copy<8><<<blocks_for(tot, 256), 256, 0, st>>>(d, Pin, Uin, Pout, Uout);
+    else k_ghost_copy<5><<<blocks_for(tot, 256), 256, 0, st>>>(d, Pin, Uin, Pout, Uout);
+}
+
+void LaunchCommon::batch_ghost_copy(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st)
+{
+    const dim3 grid(16, nblocks);
+    if (nv == 8) k_batch_ghost_copy<8><<<grid, 256, 0, st>>>(blocks, stage);
+    else k_batch_ghost_copy<5><<<grid, 256, 0, st>>>(blocks, stage);
 }
 
 void LaunchCommon::ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,

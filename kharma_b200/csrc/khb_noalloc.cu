@@ -77,7 +77,7 @@ extern "C" int khb_max_divb_noalloc(const khb_config* cfg, const khb_fields* U, 
         return e == cudaSuccess ? KHB_OK : noalloc_fail(KHB_ERR_CUDA, cudaGetErrorString(e));
     }
     // same corner range as khb_max_divb (b_flux_ct.cpp:554-564)
-    const int avoid_in = d.bc[0] != KHB_BC_PERIODIC, avoid_out = d.bc[1] != KHB_BC_PERIODIC;
+    const int avoid_in = khb::phys_face(d.bc[0]), avoid_out = khb::phys_face(d.bc[1]);
     const int i_lo = d.is + avoid_in, i_hi = d.ie + !avoid_out;
     const long long corners = (long long)(i_hi - i_lo + 1)*(d.je - d.js + 2)*((d.ndim > 2) ? d.ke - d.ks + 2 : 1);
     const long long nblocks = (corners + 255) / 256;

@@ -59,6 +59,26 @@ enum { M_ZONE_CELL = M_UTOP | M_FLOORS | M_PTOU | M_FAILLIST, M_ZONE_FUSED = M_U
 // ... or in three (update; inversion; floors + P->U)
 enum { M_ZONE_FLOORS = M_FLOORS | M_PTOU | M_FAILLIST };
 
+struct Box {
+    int lo_i, lo_j, lo_k, cnt_i, cnt_j, cnt_k;
+    unsigned np;      // cnt_i * cnt_j
+    unsigned nbp;     // blocks across the plane
+    int kz;           // k planes per block (1, 2 or 4)
+    int pshift;       // log2(128 / kz): plane positions per block = 1 << pshift
+};
+inline Box make_box(int lo_i, int lo_j, int lo_k, int cnt_i, int cnt_j, int cnt_k, int kz = 0)
+{
+    Box b;
+    b.lo_i = lo_i; b.lo_j = lo_j; b.lo_k = lo_k; b.cnt_i = cnt_i; b.cnt_j = cnt_j; b.cnt_k = cnt_k;
+    b.np = (unsigned)cnt_i * (unsigned)cnt_j;
+    if (kz <= 0) kz = (cnt_k >= 4) ? 4 : 1;
+    b.kz = kz;
+    b.pshift = (kz == 4) ? 5 : ((kz == 2) ? 6 : 7);
+    const unsigned per = 1u << b.pshift;
+    b.nbp = (b.np + per - 1) / per;
+    return b;
+}
+inline unsigned box_blocks(const Box& b) { return b.nbp * (unsigned)((b.cnt_k + b.kz - 1) / b.kz); }
 template <typename FT>
 struct ZoneArgs {
     khb_fields Ps, Us, U0, Pout, Uout;
@@ -74,6 +94,38 @@ struct ZoneArgs {
 };
 
 
+// One meshblock of a batch as the batched kernels see it: built once by khb_batch_create in device
+// memory and staged in shared memory by each CTA.  za[s] are the zone-pass arguments of stage s + 1
+// (bdt and the timestep flag are set in the kernel from the device timestep); Pin[s] is the flux
+// input of that stage.  tile0[x]: the first tile of this block in the flux x1..x3 (x = 0..2) and
+// zone (x = 3) launches.
+template <typename FT>
+struct BatchBlock {
+    Dims d;
+    DevGeom g;
+    Phys ph;
+    ZoneArgs<FT> za[2];
+    khb_fields Pin[2];
+    FT* F[3];
+    FT* ctop[3];
+    Box fbox[3];
+    Box zbox;
+    unsigned tile0[4];
+};
+
+// What the batched fixup reads of each block (independent of the flux precision)
+struct FixupBlock {
+    Dims d;
+    DevGeom g;
+    Phys ph;
+    khb_fields Pin[2], Uin[2]; // stage inputs of stage 1 and 2
+    khb_fields P[2], U[2];     // stage outputs of stage 1 and 2
+    int exch;                  // the block has an exchange face: its ghost shell carries over
+    int32_t* pflag;
+    int* fail_count;
+    int* fail_list;
+};
+
 // Launchers.  Launch<double> is compiled without FMA contraction (the FP64 path keeps the
 // reference's rounding); Launch<float> (the FP32-flux form) is compiled with contraction.
 template <typename FT>
@@ -86,6 +138,13 @@ struct Launch {
     static void flux_ct(const Dims& d, FT* F1, FT* F2, FT* F3, FT* emf, cudaStream_t st);
     static void copy_flux(long long N, int nv, const FT* F, const FT* ctop, const khb_fields& out, double* ctop_out,
                           cudaStream_t st);
+    // Batched launches over every block of a batch: tiles[t] is the block of tile t; grid = 0 runs
+    // one CTA per tile, otherwise grid CTAs loop over the tiles.  Return the CTAs per SM the kernel
+    // can keep resident (for sizing a persistent grid) when called with ntiles = 0.
+    static int batch_flux(int recon, int nv, int dir, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
+                          unsigned grid, int stage, cudaStream_t st);
+    static int batch_zone(int nv, int mode, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
+                          unsigned grid, int stage, int dtm, double beta, const double* dt, cudaStream_t st);
 };
 
 // Zone-local FP64 work shared by both forms (compiled with the FP64 unit)
@@ -97,10 +156,17 @@ struct LaunchCommon {
     static void ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
                            const khb_fields& U, cudaStream_t st);
     static void periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st);
+    static void ghost_copy(int nv, const Dims& d, const khb_fields& Pin, const khb_fields& Uin, const khb_fields& Pout,
+                           const khb_fields& Uout, cudaStream_t st);
+    static void batch_ghost_copy(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st);
     static void ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
                      cudaStream_t st);
     static void divb(const Dims& d, const Phys& ph, const khb_fields& U, int i_lo, int i_hi,
                      unsigned long long* word, cudaStream_t st);
+    // Batched fixups (one CTA row per block) and the per-stage reset of the failed-zone counters
+    // (and, when word != NULL, of the timestep minimum)
+    static void batch_fixup(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st);
+    static void batch_reset(int* const* counts, int nblocks, unsigned long long* word, cudaStream_t st);
 };
 
 // EMHD and implicit-solve parameters are passed to the kernels as the C-ABI structs themselves
@@ -133,6 +199,10 @@ struct LaunchEmhd {
 };
 
 inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// A face of the global domain with a physical boundary condition (outflow or reflecting), as
+// opposed to a periodic face or an exchange face filled by the caller from a neighbouring block
+__host__ __device__ inline bool phys_face(int bc) { return bc == KHB_BC_OUTFLOW || bc == KHB_BC_REFLECTING; }
 
 // Validate a khb_config and derive the block index ranges and physics parameters (no allocation).
 // Returns KHB_OK or a KHB_ERR_* code with a message in *why.

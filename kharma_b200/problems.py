@@ -303,3 +303,86 @@ def conducting_atmosphere(spec, geom, emhd, profile, jitter=1e-3, seed=1234, B10
         for plane in (0, 1, 8):
             P[plane] *= 1.0 + jitter * rng.uniform(-1.0, 1.0, size=P[plane].shape)
     return P
+
+
+# ------------------------------------------------------------------------ Bondi accretion
+def _bondi_T(r, C1, C2, n, rs):
+    """bondi.hpp get_T: bisection for the temperature on the inflowing branch, vectorised with a
+    per-zone stopping mask (rtol 1e-12, ftol 1e-14 as in the reference)."""
+    rtol, ftol = 1.e-12, 1.e-14
+
+    def tfunc(T):
+        A = 1. + (1. + n) * T
+        B = C1 / (r * r * np.power(T, n))
+        return A * A * (1. - 2. / r + B * B) - C2
+
+    Tinf = (math.sqrt(C2) - 1.) / (n + 1)
+    Tnear = np.power(C1 * np.sqrt(2. / (r * r * r)), 1. / n)
+    Tmin = np.where(r < rs, Tinf, np.maximum(Tnear, Tinf))
+    Tmax = np.where(r < rs, Tnear, 1.0)
+    T0, T1 = Tmin.copy(), Tmax.copy()
+    f0, f1 = tfunc(T0), tfunc(T1)
+    bad = f0 * f1 > 0
+    Th = (T0 + T1) / 2.
+    fh = tfunc(Th)
+    epsT = rtol * (Tmin + Tmax)
+    for _ in range(200):
+        go = (np.abs(Th - T0) > epsT) & (np.abs(Th - T1) > epsT) & (np.abs(fh) > ftol)
+        if not go.any():
+            break
+        up = go & (fh * f0 > 0.)
+        dn = go & ~(fh * f0 > 0.)
+        T0 = np.where(up, Th, T0)
+        f0 = np.where(up, fh, f0)
+        T1 = np.where(dn, Th, T1)
+        f1 = np.where(dn, fh, f1)
+        Th = np.where(go, (T0 + T1) / 2., Th)
+        fh = np.where(go, tfunc(Th), fh)
+    return np.where(bad, -1., Th)
+
+
+def bondi_solution(r, rs=8.0, mdot=1.0, gam=5.0 / 3.0):
+    """bondi.hpp get_bondi_soln: rho, u and the Boyer-Lindquist u^r of the steady Bondi inflow."""
+    n = 1. / (gam - 1.)
+    uc = math.sqrt(1. / (2. * rs))
+    Vc = math.sqrt(uc * uc / (1. - 3. * uc * uc))
+    Tc = -n * Vc * Vc / ((n + 1.) * (n * Vc * Vc - 1.))
+    C1 = uc * rs * rs * Tc ** n
+    A = 1. + (1. + n) * Tc
+    C2 = A * A * (1. - 2. / rs + uc * uc)
+    K = (4 * math.pi * C1 / mdot) ** (1 / n)
+    Kn = K ** n
+    T = _bondi_T(r, C1, C2, n, rs)
+    Tn = np.power(T, n)
+    rho = Tn / Kn
+    u = rho * T * n
+    ur = -C1 / (Tn * r * r)
+    return rho, u, ur
+
+
+def bondi(spec, geom, rs=8.0, mdot=1.0):
+    """Bondi inflow on a spherical-KS (a = 0) MKS block, every zone including the ghosts set to the
+    analytic solution (prob/bondi.hpp get_prim_bondi with ur_frac = 1, uphi = 0, no diffinit):
+    u^r in Boyer-Lindquist, u^t from the BL metric (set_ut, coordinate_utils.hpp:170-187), BL -> KS
+    (coordinate_systems.hpp:154-164), KS -> native through dX/dx of MKS, then the primitive
+    velocity (fourvel_to_prim, coordinate_utils.hpp:195-202)."""
+    assert spec.base == "spherical_ks" and spec.transform == "mks" and spec.a == 0.0
+    n3, n2, n1 = spec.shape
+    x1, x2, _ = cell_centers(spec)
+    X1, _ = np.meshgrid(x1, x2, indexing="xy")              # (n2, n1)
+    r = np.exp(X1)
+    rho, u, ur = bondi_solution(r, rs, mdot, spec.gam)
+    # BL metric at a = 0: g_tt = -(1 - 2/r), g_rr = 1/(1 - 2/r); u^t from the normalisation
+    AA = -(1. - 2. / r)
+    CC = 1. + (1. / (1. - 2. / r)) * ur * ur
+    ut_bl = (-0. - np.sqrt(0. - 4. * AA * CC)) / (2. * AA)
+    ut_ks = ut_bl + (2. * r / (r * r - 2. * r)) * ur
+    # MKS: r = exp(X1), dr/dX1 = r; theta depends on X2 only, u^theta = 0
+    ucon = [ut_ks, ur / r, np.zeros_like(r), np.zeros_like(r)]
+    gcon = np.asarray(geom["gcon"])[3, :n2, :n1]
+    alpha2 = -1.0 / gcon[..., 0, 0]
+    uprim = [ucon[1 + v] + ucon[0] * alpha2 * gcon[..., 0, 1 + v] for v in range(3)]
+    P = np.zeros((spec.nvar, n3, n2, n1))
+    for p, val in enumerate((rho, u, uprim[0], uprim[1], uprim[2])):
+        P[p] = val[None, :, :]
+    return P

@@ -194,6 +194,19 @@ def torus_spec(n1, n2, n3, r_out=1000.0, a=0.9375, recon="linear_mc", precision=
                      driver=driver)
 
 
+def bondi_spec(nx1, nx2, nx3, x1min, x1max, x2min=0.0, x2max=1.0, x3min=0.0, x3max=2 * math.pi,
+               precision="fp64", recon="weno5", bc=("exchange",) * 6):
+    """One meshblock of the Bondi problem (pars/bondi/bondi.par): spherical KS at a = 0 in MKS
+    coordinates (hslope 0.3), gamma 5/3, WENO5, LLF, hydro only (b_field none: 5 variables),
+    floors off.  The block covers the given native-coordinate ranges; by default every face is an
+    exchange face whose ghost zones the caller fills (here: with the analytic solution)."""
+    return BlockSpec(nx1=nx1, nx2=nx2, nx3=nx3, x1min=x1min, x1max=x1max, x2min=x2min, x2max=x2max,
+                     x3min=x3min, x3max=x3max, gam=5.0 / 3.0, nvar=5, cfl=0.9, dt_min=1e-5,
+                     recon=recon, riemann="llf", precision=precision,
+                     base="spherical_ks", transform="mks", a=0.0, hslope=0.3,
+                     bc=tuple(bc), floors_on=False, driver="kharma")
+
+
 @dataclass
 class EmhdSpec:
     """EMHD package options (emhd/emhd.cpp:60-130).  Defaults are the reference's GetOrAdd defaults."""

@@ -74,7 +74,10 @@ struct CoordSpec {
 };
 
 enum Recon { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3 };
-enum BC { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2 };
+enum BC { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2, BC_EXCHANGE = 3 };
+// Exchange faces are internal block boundaries whose ghost zones the caller fills (Parthenon's
+// boundary communication); only outflow and reflecting faces are global "user" boundaries.
+static inline bool phys_face(int bc) { return bc == BC_OUTFLOW || bc == BC_REFLECT; }
 enum Frame { FRAME_FLUID = 0, FRAME_NORMAL = 1, FRAME_DRIFT = 2 };
 
 struct Config {
@@ -768,7 +771,7 @@ static void boundaries_fix_flux(const Block& B, double* F[3])
         const int bdir = face / 2 + 1;
         const bool binner = (face % 2) == 0;
         if (bdir > B.ndim) continue;
-        if (B.c.bc[face] == BC_PERIODIC) continue;   // only global "user" boundaries
+        if (!phys_face(B.c.bc[face])) continue;       // only global "user" boundaries
         // one-zone halo range, collapsed to the boundary face
         int is_ = B.is - 1, ie_ = B.ie + 1, js_ = B.js - (B.ndim > 1), je_ = B.je + (B.ndim > 1);
         int ks_ = B.ks - (B.ndim > 2), ke_ = B.ke + (B.ndim > 2);
@@ -1301,9 +1304,9 @@ static void apply_boundaries(const Block& B, double* P, double* U)
     for (int d = 1; d <= B.ndim; ++d)
         if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, B.nv, d); periodic_fill(B, U, B.nv, d); }
     for (int face = 0; face < 2*B.ndim; ++face) {
-        if (B.c.bc[face] == BC_PERIODIC) continue;
+        if (!phys_face(B.c.bc[face])) continue;
         physical_face(B, P, U, face);
-        if (face == 3 && B.c.fix_corner_inner && B.c.bc[0] != BC_PERIODIC) physical_face(B, P, U, 0);
+        if (face == 3 && B.c.fix_corner_inner && phys_face(B.c.bc[0])) physical_face(B, P, U, 0);
     }
     for (int d = 1; d <= B.ndim; ++d)
         if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, B.nv, d); periodic_fill(B, U, B.nv, d); }
@@ -1385,8 +1388,8 @@ static void stage(const Block& B, Fields& f, int s, double dt,
     double* F[3] = {f.F[0].data(), f.F[1].data(), f.F[2].data()};
     if (B.nv > 5) {
         if (B.c.fix_polar_flux && B.C.spherical()) {
-            if (B.c.bc[2] != BC_PERIODIC) zero_boundary_flux_x2(B, F[0], F[1], F[2], true);
-            if (B.c.bc[3] != BC_PERIODIC) zero_boundary_flux_x2(B, F[0], F[1], F[2], false);
+            if (phys_face(B.c.bc[2])) zero_boundary_flux_x2(B, F[0], F[1], F[2], true);
+            if (phys_face(B.c.bc[3])) zero_boundary_flux_x2(B, F[0], F[1], F[2], false);
         }
         flux_ct(B, F[0], F[1], F[2]);
     }
@@ -1418,6 +1421,14 @@ static void stage(const Block& B, Fields& f, int s, double dt,
                 if (d == 2) { js = 0; je = B.n2 - 1; }
                 if (d == 3) { ks = 0; ke = B.n3 - 1; }
             }
+        // exchange faces: the neighbour's values in the ghost zones are valid neighbours (their
+        // flags are the caller's; zero unless it exchanges them)
+        if (B.c.bc[0] == BC_EXCHANGE) is = 0;
+        if (B.c.bc[1] == BC_EXCHANGE) ie = B.n1 - 1;
+        if (B.ndim > 1 && B.c.bc[2] == BC_EXCHANGE) js = 0;
+        if (B.ndim > 1 && B.c.bc[3] == BC_EXCHANGE) je = B.n2 - 1;
+        if (B.ndim > 2 && B.c.bc[4] == BC_EXCHANGE) ks = 0;
+        if (B.ndim > 2 && B.c.bc[5] == BC_EXCHANGE) ke = B.n3 - 1;
         fix_utop(B, P_n, U_n, pflag, ks, ke, js, je, is, ie);
     }
     // 10-11. boundaries, then U = U(P) over the entire block
@@ -2199,8 +2210,8 @@ void orc_fix_flux(void* hp, double* F1, double* F2, double* F3)
     double* F[3] = {F1, F2, F3};
     if (B.nv > 5) {
         if (B.c.fix_polar_flux && B.C.spherical()) {
-            if (B.c.bc[2] != BC_PERIODIC) zero_boundary_flux_x2(B, F1, F2, F3, true);
-            if (B.c.bc[3] != BC_PERIODIC) zero_boundary_flux_x2(B, F1, F2, F3, false);
+            if (phys_face(B.c.bc[2])) zero_boundary_flux_x2(B, F1, F2, F3, true);
+            if (phys_face(B.c.bc[3])) zero_boundary_flux_x2(B, F1, F2, F3, false);
         }
         flux_ct(B, F1, F2, F3);
     }

@@ -52,7 +52,7 @@ class Config(C.Structure):
 
 
 RECON = {"donor_cell": 0, "linear_mc": 1, "weno5": 2, "ppm": 3}
-BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
 TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
