@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-kernel-times", action="store_true")
     ap.add_argument("--no-emhd", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--slab-path", action="store_true",
                     help="at N = 1, step the block through the x3-slab path (one slab, local exchange)")
     ap.add_argument("--emhd-only", action="store_true",
@@ -291,6 +292,53 @@ def emhd_newton(n=128, reps=3):
     return out
 
 
+def batching(steps=20, warm=3):
+    """The batching form: the 184-block three-level Bondi mesh (8 x 64^3, 48 x 32^3, 128 x 16^3 zones,
+    KS a = 0, MKS, WENO5, LLF, hydro) stepped through the plain per-block launch path (khb_step per
+    block), the batched path (one launch per kernel per stage), and its CUDA-graph replay after the
+    autotuner has chosen the tile shapes; FP64 and FP32-flux.  CUDA events on the batch's stream."""
+    import torch
+    from kharma_b200.batch import Batch, bondi_smr_layout
+
+    def timed(fn, n):
+        s = torch.cuda.current_stream()
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(n):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {"workload": "Bondi (r_s = 8, mdot = 1, gamma 5/3) on a 3-level static-refined mesh of 184 blocks: "
+                       "8 x 64^3, 48 x 32^3, 128 x 16^3 zones, KS a=0 MKS, WENO5, LLF, hydro; ghost zones "
+                       "hold the analytic solution (blocks advance independently)"}
+    dt = 1e-3
+    for prec in ("fp64", "fp32_flux"):
+        b = Batch(bondi_smr_layout(precision=prec))
+        zones = b.zones
+        r = {"zones": zones}
+        with torch.cuda.stream(b.torch_stream):
+            r["per_block_ms_per_step"] = timed(lambda: b.step_per_block(dt), max(3, steps // 4))
+            r["batched_ms_per_step"] = timed(lambda: b.step(dt), steps)
+            tune, pers = b.autotune(3)
+            r["autotune"] = {"planes_per_cta": tune, "persistent": pers}
+            l0 = b.launch_count()
+            r["graph_ms_per_step"] = timed(lambda: b.step_graph(dt), steps)
+            r["launches_per_step"] = (b.launch_count() - l0) / (steps + warm)
+        for k in ("per_block", "batched", "graph"):
+            r[k + "_zone_cycles_per_s"] = zones / (r[k + "_ms_per_step"] / 1000.0)
+        r["speedup_graph_vs_per_block"] = r["per_block_ms_per_step"] / r["graph_ms_per_step"]
+        out[prec] = r
+        del b
+        torch.cuda.empty_cache()
+    return out
+
+
 def gpu_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -443,6 +491,12 @@ def gpu_arm(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_emhd:
         emhd = emhd_newton()
 
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        del b, drv
+        torch.cuda.empty_cache()
+        batch = batching()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n3s = max(8, n3 // 2)
@@ -462,7 +516,7 @@ def gpu_arm(args, rank, world, local_rank):
                           "parallelism": "single block" if world == 1 else f"x3 slabs x{world} (NCCL halo exchange)",
                           "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
-               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd}
+               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch}
         print(json.dumps(out), flush=True)
 
 

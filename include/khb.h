@@ -57,6 +57,9 @@ enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2, KHB_BC_EX
 enum { KHB_FRAME_FLUID = 0, KHB_FRAME_NORMAL = 1, KHB_FRAME_DRIFT = 2 };
 /* Arithmetic of reconstruction, Riemann fluxes and EMF averaging */
 enum { KHB_PREC_FP64 = 0, KHB_PREC_FP32_FLUX = 1 };
+/* Primitive recovery (inverter/type, inverter.cpp:54-64): 1D_W of Noble et al. (2006) or the
+ * robust Kastaun et al. (2021) scheme with the inverter floors inside its residual */
+enum { KHB_INVERTER_ONEDW = 0, KHB_INVERTER_KASTAUN = 1 };
 /* Driver step semantics (driver/simple_step.cpp, driver/kharma_step.cpp) */
 enum { KHB_DRIVER_SIMPLE = 0, KHB_DRIVER_KHARMA = 1 };
 
@@ -85,9 +88,11 @@ typedef struct {
     int32_t spherical;                /* coordinates are spherical (floors use r) */
     int32_t cart_minkowski;           /* Cartesian Minkowski: geometric source is skipped (flux.cpp:407) */
     int32_t floors_on, floor_frame, recon_floors;
-    int32_t iter_max; double err_tol; /* inverter/iter_max, inverter/err_tol (1D_W: 8, 1e-8) */
+    int32_t iter_max; double err_tol; /* inverter/iter_max, inverter/err_tol (1D_W: 8, 1e-8;
+                                         Kastaun: 25, 1e-12) */
     int32_t fix_average_neighbors, fix_atmosphere;
-    khb_floors floors;
+    khb_floors floors;                /* floors; also the inverter floors of the Kastaun scheme */
+    int32_t inverter;                 /* KHB_INVERTER_* */
 } khb_config;
 
 /* Coordinate system for khb_build_geometry (coordinates/coordinate_systems.hpp) */

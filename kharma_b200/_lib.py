@@ -19,6 +19,7 @@ FLUX = {"llf": 0, "hlle": 1}
 BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 PREC = {"fp64": 0, "fp32_flux": 1}
+INVERTER = {"onedw": 0, "kastaun": 1}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
 TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
 CLOSURE = {"constant": 0, "soundspeed": 1, "sound_speed": 1, "kappa_eta": 2, "torus": 3}
@@ -56,6 +57,7 @@ class KhbConfig(C.Structure):
         ("iter_max", C.c_int32), ("err_tol", C.c_double),
         ("fix_average_neighbors", C.c_int32), ("fix_atmosphere", C.c_int32),
         ("floors", KhbFloors),
+        ("inverter", C.c_int32),
     ]
 
 

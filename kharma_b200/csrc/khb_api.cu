@@ -121,8 +121,10 @@ void launch_zone_t(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
     Launch<FT>::zone(ctx->nv, ctx->d, ctx->g, ctx->ph, a, st);
 }
 
-int launch_zone(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
+int launch_zone(khb_ctx* ctx, const ZoneCall& zc_in, cudaStream_t st)
 {
+    ZoneCall zc = zc_in;
+    if ((zc.mode & M_UTOP) && ctx->ph.inverter == KHB_INVERTER_KASTAUN) zc.mode |= M_KASTAUN;
     if (ctx->fp32) launch_zone_t<float>(ctx, zc, st); else launch_zone_t<double>(ctx, zc, st);
     KHB_LAUNCHED(ctx);
     return KHB_OK;
@@ -309,6 +311,11 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
     ph.fix_polar_flux = cfg->fix_polar_flux && cfg->spherical;
     ph.check_inflow_in = cfg->check_inflow_inner_x1;
     ph.check_inflow_out = cfg->check_inflow_outer_x1;
+    if (cfg->inverter != KHB_INVERTER_ONEDW && cfg->inverter != KHB_INVERTER_KASTAUN) {
+        *why = "unknown inverter";
+        return KHB_ERR_UNSUPPORTED;
+    }
+    ph.inverter = cfg->inverter;
     std::memcpy(&ph.fl, &cfg->floors, sizeof(khb_floors));
     return KHB_OK;
 }

@@ -208,7 +208,8 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
     Launch<FT>::batch_zone(b->nv, M_UPDATE, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage, 0, kRkBeta[s],
                            b->dt_dev, st);
     KHB_BLAUNCHED(b, 1);
-    Launch<FT>::batch_zone(b->nv, M_ZONE_CELL, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage,
+    const int cell = M_ZONE_CELL | ((b->ctx[0]->ph.inverter == KHB_INVERTER_KASTAUN) ? M_KASTAUN : 0);
+    Launch<FT>::batch_zone(b->nv, cell, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage,
                            s == 1 ? M_DT : 0, kRkBeta[s], b->dt_dev, st);
     KHB_BLAUNCHED(b, 1);
     LaunchCommon::batch_fixup(b->nv, b->fix, b->nb, stage, st);
@@ -305,10 +306,10 @@ int khb_batch_create(khb_ctx* const* blocks, int nblocks, const khb_fields* P, c
         if (x == 0) {
             b->nv = c->nv; b->recon = c->cfg.recon; b->fp32 = c->fp32; b->ndim = c->d.ndim;
         } else if (c->nv != b->nv || c->cfg.recon != b->recon || c->fp32 != b->fp32 || c->d.ndim != b->ndim ||
-                   c->cfg.riemann != blocks[0]->cfg.riemann) {
+                   c->cfg.riemann != blocks[0]->cfg.riemann || c->ph.inverter != blocks[0]->ph.inverter) {
             delete b;
             return set_error(KHB_ERR_ARG, "khb_batch_create: blocks differ in nvar, dimension, reconstruction, "
-                                          "Riemann solver or precision");
+                                          "Riemann solver, inverter or precision");
         }
         for (int p = 0; p < c->nv; ++p)
             if (!P[x].v[p] || !U[x].v[p]) { delete b; return set_error(KHB_ERR_ARG, "khb_batch_create: NULL field"); }

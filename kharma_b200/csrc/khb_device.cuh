@@ -380,6 +380,155 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
     return ST_SUCCESS;
 }
 
+// ------------------------------------------------------------------ Kastaun inversion (FP64)
+// inverter/kastaun.hpp:83-406: master function of mu = 1/(h W), Illinois false position for a
+// bracket (eq. 49) and then the root (eq. 44), inverter floors inside the residual.  Returns the
+// FFlag bits of the floors hit (FF_INVERTER_*), or ST_MAX_ITER with P untouched.
+enum { FF_INVERTER_RHO = 16384, FF_INVERTER_U = 32768, FF_INVERTER_GAMMA = 65536, FF_INVERTER_U_MAX = 131072 };
+
+struct KastaunResidual {
+    double D, q, bsq, bsq_rpsq, rsq, rbsq, v0sq, gam, rho_floor, e_floor, e_max;
+    bool used_density_floor, used_energy_floor, used_energy_max, used_gamma_max;
+    __device__ __forceinline__ double x_mu(double mu) const { return 1.0 / (1.0 + mu * bsq); }
+    __device__ __forceinline__ double rbarsq_mu(double mu, double x) const { return x * (x * rsq + mu * (1.0 + x) * rbsq); }
+    __device__ __forceinline__ double qbar_mu(double mu, double x) const
+    {
+        const double mux = mu * x;
+        return q - 0.5 * (bsq + mux * mux * bsq_rpsq);
+    }
+    __device__ __forceinline__ double vhatsq_mu(double mu, double rbarsq)
+    {
+        const double vsq_trial = mu * mu * rbarsq;
+        used_gamma_max = vsq_trial > v0sq;
+        return used_gamma_max ? v0sq : vsq_trial;
+    }
+    __device__ __forceinline__ double rhohat_mu(double iWhat)
+    {
+        const double rho_trial = D * iWhat;
+        used_density_floor = rho_trial <= rho_floor;
+        return used_density_floor ? rho_floor : rho_trial;
+    }
+    __device__ __forceinline__ double ehat_mu(double mu, double qbar, double rbarsq, double vhatsq, double What)
+    {
+        const double ehat_trial = What * (qbar - mu * rbarsq) + vhatsq * What * What / (1.0 + What);
+        used_energy_floor = false;
+        used_energy_max = false;
+        if (ehat_trial <= e_floor) { used_energy_floor = true; return e_floor; }
+        if (ehat_trial > e_max) { used_energy_max = true; return e_max; }
+        return ehat_trial;
+    }
+    __device__ __forceinline__ double master(double mu)      // eq. 44
+    {
+        const double x = x_mu(mu);
+        const double rbarsq = rbarsq_mu(mu, x);
+        const double qbar = qbar_mu(mu, x);
+        const double vhatsq = vhatsq_mu(mu, rbarsq);
+        const double iWhat = sqrt(1.0 - vhatsq);
+        const double What = 1.0 / iWhat;
+        const double rhohat = rhohat_mu(iWhat);
+        const double ehat = ehat_mu(mu, qbar, rbarsq, vhatsq, What);
+        const double Phat = ehat * rhohat * (gam - 1.0);
+        const double hhat = rhohat * (1.0 + ehat) + Phat;
+        const double ahat = Phat / (hhat - Phat);
+        const double nua = (1.0 + ahat) * (1.0 + ehat) * iWhat;
+        const double nub = (1.0 + ahat) * (1.0 + qbar - mu * rbarsq);
+        const double nuhat = kmax(nua, nub);
+        const double muhat = 1.0 / (nuhat + mu * rbarsq);
+        return mu - muhat;
+    }
+    __device__ __forceinline__ double aux(double mu) const    // eq. 49
+    {
+        const double x = 1.0 / (1.0 + mu * bsq);
+        const double rbarsq = x * (rsq * x + mu * (1.0 + x) * rbsq);
+        return mu * sqrt(1.0 + rbarsq) - 1.0;
+    }
+    // Illinois false position on [zm, zp] (kastaun.hpp:305-331, 343-368); iter at exit
+    template <bool MASTER>
+    __device__ __forceinline__ double solve(double zm, double zp, int max_iterations, double tol, int& iter)
+    {
+        double fm = MASTER ? master(zm) : aux(zm);
+        double fp = MASTER ? master(zp) : aux(zp);
+        int iterations = max_iterations;
+        if ((fabs(zm - zp) < tol) || ((fabs(fm) + fabs(fp)) < 2.0 * tol)) iterations = -1;
+        double z = 0.5 * (zm + zp);
+        for (iter = 0; iter < iterations; ++iter) {
+            z = (zm * fp - zp * fm) / (fp - fm);
+            const double fz = MASTER ? master(z) : aux(z);
+            if ((fabs(zm - zp) < tol) || (fabs(fz) < tol)) break;
+            if (fz * fp < 0.0) { zm = zp; fm = fp; zp = z; fp = fz; }
+            else { fm = 0.5 * fm; zp = z; fp = fz; }
+        }
+        return z;
+    }
+};
+
+template <int NV>
+__device__ int u_to_p_kastaun(const ZoneGeom& G, double gam, const Prescription& fl, const double* U, double* P,
+                              int max_iterations, double tol)
+{
+    const double alpha = 1. / sqrt(-G.gcon[0][0]);
+    const double a_over_g = alpha / G.gdet;
+    const double D = U[0] * a_over_g;
+    const double D_fl = kmax(D, fl.rho_min_const);
+    const double Qcov[4] = {(U[1] - U[0]) * a_over_g, U[2] * a_over_g, U[3] * a_over_g, U[4] * a_over_g};
+    const double ncov[4] = {-alpha, 0., 0., 0.};
+    double ncon[4];
+    raise4(G, ncov, ncon);
+    const double q = (-dot4(Qcov, ncon) - D) / D;
+    const double rcov[3] = {U[2] / U[0], U[3] / U[0], U[4] / U[0]};
+    double rcon[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)   // gamma^ij = g^ij - g^0i g^0j / g^00 (kastaun.hpp:250-262)
+        rcon[a] = ((G.gcon[a+1][1] - G.gcon[0][a+1]*G.gcon[0][1]/G.gcon[0][0])*rcov[0] +
+                   (G.gcon[a+1][2] - G.gcon[0][a+1]*G.gcon[0][2]/G.gcon[0][0])*rcov[1] +
+                   (G.gcon[a+1][3] - G.gcon[0][a+1]*G.gcon[0][3]/G.gcon[0][0])*rcov[2]);
+    double rsq = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) rsq += rcon[a] * rcov[a];
+    double bsq = 0.0, bsq_rpsq = 0.0, rbsq = 0.0, bdotr = 0.0, bu[3] = {0.0, 0.0, 0.0};
+    if (NV > 5) {
+        const double sD = 1.0 / sqrt(D_fl);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            bu[a] = (U[5 + a] * a_over_g) * sD;
+            bdotr += bu[a] * rcov[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) bsq += G.gcov[a + 1][b + 1] * bu[a] * bu[b];
+        bsq = kmax(0.0, bsq);
+        rbsq = bdotr * bdotr;
+        bsq_rpsq = bsq * rsq - rbsq;
+    }
+    const double zsq = rsq;
+    KastaunResidual res;
+    res.D = D; res.q = q; res.bsq = bsq; res.bsq_rpsq = bsq_rpsq; res.rsq = rsq; res.rbsq = rbsq;
+    res.v0sq = kmin(zsq / (1.0 + zsq), 1.0 - 1.0 / (fl.gamma_max * fl.gamma_max));
+    res.gam = gam; res.rho_floor = fl.rho_min_const; res.e_floor = fl.u_min_const / D_fl; res.e_max = fl.u_over_rho_max;
+    res.used_density_floor = res.used_energy_floor = res.used_energy_max = res.used_gamma_max = false;
+    int iter = 0;
+    const double zb = res.solve<false>(0., 1., max_iterations, tol, iter);
+    const double mu = res.solve<true>(0., zb, max_iterations, tol, iter);
+    if (iter == max_iterations) return ST_MAX_ITER;
+    const double x = res.x_mu(mu);
+    const double rbarsq = res.rbarsq_mu(mu, x);
+    const double vsq = res.vhatsq_mu(mu, rbarsq);
+    const double iW = sqrt(1.0 - vsq);
+    const double W = 1. / iW;
+    P[0] = res.rhohat_mu(iW);
+    const double qbar = res.qbar_mu(mu, x);
+    P[1] = res.ehat_mu(mu, qbar, rbarsq, vsq, W) * P[0];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) P[2 + a] = W * mu * x * (rcon[a] + mu * bdotr * bu[a]);
+    int fflag = 0;
+    if (res.used_density_floor) fflag |= FF_INVERTER_RHO;
+    if (res.used_energy_floor) fflag |= FF_INVERTER_U;
+    if (res.used_gamma_max) fflag |= FF_INVERTER_GAMMA;
+    if (res.used_energy_max) fflag |= FF_INVERTER_U_MAX;
+    return fflag;
+}
+
 // ------------------------------------------------------------------ floors (FP64)
 // FFlag bits, floors.hpp:52-70
 enum { FF_GEOM_RHO = 32, FF_GEOM_U = 64, FF_B_RHO = 128, FF_B_U = 256, FF_TEMP = 512, FF_GAMMA = 1024,
@@ -467,9 +616,12 @@ __device__ __forceinline__ void apply_ceilings(const ZoneGeom& G, const Prescrip
 }
 
 // floors_functions.hpp:174-179 (fluid), 181-252 (drift), 254-289 (normal observer)
+// D_pre: the 4-vectors of P on entry when the caller has them (determine_floors computed them from the
+// same P and geometry, so they are the ones the drift frame would compute), else NULL
 template <int NV>
 __device__ int apply_floors_frame(const ZoneGeom& G, int frame, double gam, double* P, double* U,
-                                  double rhoflr_max, double uflr_max, int iter_max_nof)
+                                  double rhoflr_max, double uflr_max, int iter_max_nof,
+                                  const FourVec<double>* D_pre = nullptr)
 {
     if (frame == 0) {
         P[0] += kmax(0., rhoflr_max - P[0]);
@@ -494,8 +646,12 @@ __device__ int apply_floors_frame(const ZoneGeom& G, int frame, double gam, doub
         const double Bsq   = kmax(dot4(Bcon, Bcov), 1e-20);
         const double B_mag = sqrt(Bsq);
         FourVec<double> D;
-        double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
-        calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, P, D);
+        if (D_pre) {
+            D = *D_pre;
+        } else {
+            double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
+            calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, P, D);
+        }
         double Qcov[4];
         Qcov[0] = w_old * D.ucon[0] * D.ucov[0] + pg;
         Qcov[1] = w_old * D.ucon[0] * D.ucov[1];

@@ -87,8 +87,8 @@ template <> struct FaceTables<float> {
 
 // Resident 128-thread blocks per SM requested from the compiler for each kernel (register caps
 // of 65536 / (128 x blocks)), chosen by measurement on B200: FP64 faces 5 blocks along x1/x2 and 4
-// along x3, FP32 faces 8, the update half of the zone pass 8 and its inversion half 5.  Each can
-// be overridden at build time.
+// along x3, FP32 faces 8, the update half of the zone pass 4 (FP64 fluxes; no spills) or 5 (FP32
+// fluxes) and its inversion half 5.  Each can be overridden at build time.
 #ifndef KHB_FLUX64_MINB
 #define KHB_FLUX64_MINB 5
 #endif
@@ -99,7 +99,10 @@ template <> struct FaceTables<float> {
 #define KHB_FLUX32_MINB 8
 #endif
 #ifndef KHB_ZONE_UPDATE_MINB
-#define KHB_ZONE_UPDATE_MINB 8
+#define KHB_ZONE_UPDATE_MINB 4
+#endif
+#ifndef KHB_ZONE_UPDATE32_MINB
+#define KHB_ZONE_UPDATE32_MINB 5
 #endif
 #ifndef KHB_ZONE_CELL_MINB
 #define KHB_ZONE_CELL_MINB 5
@@ -114,8 +117,9 @@ template <typename R, int DIR> struct FluxMinBlocks { static constexpr int value
 template <int DIR> struct FluxMinBlocks<double, DIR> {
     static constexpr int value = (DIR == 3) ? KHB_FLUX64_X3_MINB : KHB_FLUX64_MINB;
 };
-template <int MODE> struct ZoneMinBlocks {
-    static constexpr int value = (MODE == M_UPDATE) ? KHB_ZONE_UPDATE_MINB :
+template <int MODE_, typename FT> struct ZoneMinBlocks {
+    static constexpr int MODE = MODE_ & ~M_KASTAUN;
+    static constexpr int value = (MODE == M_UPDATE) ? (sizeof(FT) == 8 ? KHB_ZONE_UPDATE_MINB : KHB_ZONE_UPDATE32_MINB) :
                                  (MODE == M_UTOP) ? KHB_ZONE_INV_MINB :
                                  (MODE == M_ZONE_FLOORS) ? KHB_ZONE_FLOOR_MINB :
                                  ((MODE & M_UTOP) ? KHB_ZONE_CELL_MINB : 1);
@@ -376,7 +380,8 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
         for (int p = 0; p < NV; ++p) P[p] = a.Ps.v[p][c];
         if (mode & M_UTOP) {
             // inverter.cpp:163-181 then b_flux_ct.cpp:196-217
-            const int pf = u_to_p_onedw<NV>(G, gam, U, P, ph.iter_max, ph.err_tol);
+            const int pf = (mode & M_KASTAUN) ? u_to_p_kastaun<NV>(G, gam, ph.fl, U, P, ph.iter_max, ph.err_tol)
+                                              : u_to_p_onedw<NV>(G, gam, U, P, ph.iter_max, ph.err_tol);
             pflag = pf % FF_GEOM_RHO;
             fflag = (pf / FF_GEOM_RHO) * FF_GEOM_RHO;
             if (NV > 5) {
@@ -393,13 +398,17 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
             const long long cg = (long long)j*g.n1 + i;
             fflag |= determine_floors<NV>(G, ph.fl, __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), gam, P, rf, uf, D);
             if (fflag) {
-                const int pl = apply_floors_frame<NV>(G, ph.frame, gam, P, U, rf, uf, 8);
+                const int pl = apply_floors_frame<NV>(G, ph.frame, gam, P, U, rf, uf, 8, &D);
                 if (pl) pflag = pl;
                 apply_ceilings(G, ph.fl, gam, P);
-                double Ut[NV];
-                p_to_u_zone<NV>(G, gam, P, Ut);
+                // the fluid part of U(P) after the floors; the lock-step P->U below computes the same
+                // values from the same P, so it is formed here only when that step is not part of the pass
+                if (!(mode & M_PTOU)) {
+                    double Ut[NV];
+                    p_to_u_zone<NV>(G, gam, P, Ut);
 #pragma unroll
-                for (int p = 0; p < 5; ++p) U[p] = Ut[p];
+                    for (int p = 0; p < 5; ++p) U[p] = Ut[p];
+                }
             } else {
                 have_D = true;   // P is unchanged: its 4-vectors serve the P->U below
             }
@@ -451,7 +460,7 @@ __device__ __forceinline__ void block_min_ndt(double v, unsigned long long* word
 }
 
 template <int NV, typename FT, int MODE>
-__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE>::value)
+__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE, FT>::value)
 k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
 {
     int i, j, k;
@@ -912,7 +921,7 @@ k_batch_flux(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ 
 }
 
 template <int NV, typename FT, int MODE>
-__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE>::value)
+__global__ void __launch_bounds__(128, ZoneMinBlocks<MODE, FT>::value)
 k_batch_zone(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ tiles, unsigned ntiles, int stage,
              int dtm, double beta, const double* __restrict__ dt)
 {
@@ -1017,12 +1026,17 @@ static void zone_nv(const Dims& d, const DevGeom& g, const Phys& ph, const ZoneA
     const Box bx = make_box(d.is, d.js, d.ks, d.ie - d.is + 1, d.je - d.js + 1, d.ke - d.ks + 1);
     const unsigned nb = box_blocks(bx);
     const int m = a.mode & ~M_DT;
-    if (m == M_ZONE_FUSED) k_zone<NV, FT, M_ZONE_FUSED><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
-    else if (m == M_UPDATE) k_zone<NV, FT, M_UPDATE><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
-    else if (m == M_ZONE_CELL) k_zone<NV, FT, M_ZONE_CELL><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
-    else if (m == M_UTOP) k_zone<NV, FT, M_UTOP><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
-    else if (m == M_ZONE_FLOORS) k_zone<NV, FT, M_ZONE_FLOORS><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
-    else k_zone<NV, FT, 0><<<nb, 128, 0, st>>>(d, g, ph, a, bx);
+    switch (m) {
+    case M_ZONE_FUSED: k_zone<NV, FT, M_ZONE_FUSED><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    case M_ZONE_FUSED | M_KASTAUN: k_zone<NV, FT, M_ZONE_FUSED | M_KASTAUN><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    case M_UPDATE: k_zone<NV, FT, M_UPDATE><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    case M_ZONE_CELL: k_zone<NV, FT, M_ZONE_CELL><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    case M_ZONE_CELL | M_KASTAUN: k_zone<NV, FT, M_ZONE_CELL | M_KASTAUN><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    case M_UTOP: k_zone<NV, FT, M_UTOP><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    case M_UTOP | M_KASTAUN: k_zone<NV, FT, M_UTOP | M_KASTAUN><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    case M_ZONE_FLOORS: k_zone<NV, FT, M_ZONE_FLOORS><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    default: k_zone<NV, FT, 0><<<nb, 128, 0, st>>>(d, g, ph, a, bx); break;
+    }
 }
 
 template <typename FT>
@@ -1107,9 +1121,13 @@ int Launch<FT>::batch_zone(int nv, int mode, const BatchBlock<FT>* blocks, const
 {
     if (nv == 8) {
         if (mode == M_UPDATE) return batch_zone_mode<8, FT, M_UPDATE>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+        if (mode & M_KASTAUN)
+            return batch_zone_mode<8, FT, M_ZONE_CELL | M_KASTAUN>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
         return batch_zone_mode<8, FT, M_ZONE_CELL>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
     }
     if (mode == M_UPDATE) return batch_zone_mode<5, FT, M_UPDATE>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+    if (mode & M_KASTAUN)
+        return batch_zone_mode<5, FT, M_ZONE_CELL | M_KASTAUN>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
     return batch_zone_mode<5, FT, M_ZONE_CELL>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
 }
 

@@ -50,6 +50,7 @@ struct Phys {
     double err_tol;
     double dx1, dx2, dx3;
     int zero_polar_flux, fix_polar_flux, check_inflow_in, check_inflow_out;
+    int inverter;                          // KHB_INVERTER_*
     Prescription fl;
 };
 
@@ -58,6 +59,8 @@ enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST
 enum { M_ZONE_CELL = M_UTOP | M_FLOORS | M_PTOU | M_FAILLIST, M_ZONE_FUSED = M_UPDATE | M_ZONE_CELL };
 // ... or in three (update; inversion; floors + P->U)
 enum { M_ZONE_FLOORS = M_FLOORS | M_PTOU | M_FAILLIST };
+// Inversion by the Kastaun scheme instead of 1D_W (a compile-time variant of the kernels with M_UTOP)
+enum { M_KASTAUN = 64 };
 
 struct Box {
     int lo_i, lo_j, lo_k, cnt_i, cnt_j, cnt_k;

@@ -80,7 +80,8 @@ class BlockSpec:
     floors_on: bool = False
     floor_frame: str = "drift"
     floors: FloorSpec = field(default_factory=FloorSpec)
-    # inverter (inverter.cpp:46-115): 1D_W
+    # inverter (inverter.cpp:46-115): 1D_W (8 iterations, 1e-8) or Kastaun (25, 1e-12)
+    inverter: str = "onedw"
     iter_max: int = 8
     err_tol: float = 1e-8
     fix_average_neighbors: bool = True
@@ -147,6 +148,7 @@ class BlockSpec:
         c.fix_average_neighbors = int(self.fix_average_neighbors)
         c.fix_atmosphere = int(self.fix_atmosphere)
         c.floors = self.floors.to_struct()
+        c.inverter = _lib.INVERTER[self.inverter]
         return c
 
     def khb_coords(self):
@@ -168,7 +170,7 @@ def mhdmodes_spec(n1, n2, n3, recon="weno5", riemann="llf", precision="fp64", dr
 
 
 def torus_spec(n1, n2, n3, r_out=1000.0, a=0.9375, recon="linear_mc", precision="fp64", gam=13.0 / 9.0,
-               driver="kharma"):
+               driver="kharma", inverter="onedw"):
     """FM torus in funky-MKS coordinates (kharma.cpp:144-316 domain logic; pars/benchmark decks).
 
     x1 spans [x1min, log(r_out)] with x1min chosen to put 5.5 zones inside the horizon, x2 in [0,1],
@@ -191,7 +193,12 @@ def torus_spec(n1, n2, n3, r_out=1000.0, a=0.9375, recon="linear_mc", precision=
                      floors_on=True, floor_frame="drift",
                      floors=FloorSpec(rho_min_geom=1e-6, u_min_geom=1e-8, bsq_over_rho_max=100.0,
                                       u_over_rho_max=2.0),
-                     driver=driver)
+                     driver=driver, inverter=inverter,
+                     # inverter.cpp:66-92: Kastaun defaults to 25 iterations to 1e-12 and to the
+                     # atmosphere fixup without neighbour averaging
+                     iter_max=25 if inverter == "kastaun" else 8,
+                     err_tol=1e-12 if inverter == "kastaun" else 1e-8,
+                     fix_average_neighbors=inverter != "kastaun")
 
 
 def bondi_spec(nx1, nx2, nx3, x1min, x1max, x2min=0.0, x2max=1.0, x3min=0.0, x3max=2 * math.pi,

@@ -95,6 +95,7 @@ struct Config {
     int32_t fix_average_neighbors, fix_atmosphere;
     double cfl, dt_min, max_dt_increase;
     Prescription floors;
+    int32_t inverter;                               // 0 onedw, 1 kastaun (inverter/type)
 };
 
 // ---------------------------------------------------------------- coordinates
@@ -1091,6 +1092,161 @@ static int apply_floors_frame(const Block& B, double* P, double* U, int j, int i
     }
 }
 
+// ---------------------------------------------------------------- Kastaun inversion
+// inverter/kastaun.hpp:83-406 (Kastaun et al. 2021, as adapted from Phoebus and AthenaK): a master
+// function of mu = 1/(h W) solved by the Illinois false-position method, first for a bracket (the
+// auxiliary function, eq. 49) and then for the root (eq. 44), with the inverter floors applied
+// inside the residual.  Returns the Inverter FFlag bits of the floors hit, or max_iter.
+enum { FF_INVERTER_RHO = 16384, FF_INVERTER_U = 32768, FF_INVERTER_GAMMA = 65536, FF_INVERTER_U_MAX = 131072 };
+
+struct KastaunResidual {            // kastaun.hpp:83-218
+    double D, q, bsq, bsq_rpsq, rsq, rbsq, v0sq, gam, rho_floor, e_floor, gamma_max, e_max;
+    bool used_density_floor = false, used_energy_floor = false, used_energy_max = false, used_gamma_max = false;
+    double x_mu(double mu) const { return 1.0 / (1.0 + mu * bsq); }
+    double rbarsq_mu(double mu, double x) const { return x * (x * rsq + mu * (1.0 + x) * rbsq); }
+    double qbar_mu(double mu, double x) const
+    {
+        const double mux = mu * x;
+        return q - 0.5 * (bsq + mux * mux * bsq_rpsq);
+    }
+    double vhatsq_mu(double mu, double rbarsq)
+    {
+        const double vsq_trial = mu * mu * rbarsq;
+        if (vsq_trial > v0sq) { used_gamma_max = true; return v0sq; }
+        used_gamma_max = false;
+        return vsq_trial;
+    }
+    double iWhat_mu(double vhatsq) const { return std::sqrt(1.0 - vhatsq); }
+    double rhohat_mu(double iWhat)
+    {
+        const double rho_trial = D * iWhat;
+        if (rho_trial <= rho_floor) { used_density_floor = true; return rho_floor; }
+        used_density_floor = false;
+        return rho_trial;
+    }
+    double ehat_mu(double mu, double qbar, double rbarsq, double vhatsq, double What)
+    {
+        const double ehat_trial = What * (qbar - mu * rbarsq) + vhatsq * What * What / (1.0 + What);
+        used_energy_floor = false;
+        used_energy_max = false;
+        if (ehat_trial <= e_floor) { used_energy_floor = true; return e_floor; }
+        else if (ehat_trial > e_max) { used_energy_max = true; return e_max; }
+        return ehat_trial;
+    }
+    double operator()(double mu)    // eq. 44
+    {
+        const double x = x_mu(mu);
+        const double rbarsq = rbarsq_mu(mu, x);
+        const double qbar = qbar_mu(mu, x);
+        const double vhatsq = vhatsq_mu(mu, rbarsq);
+        const double iWhat = iWhat_mu(vhatsq);
+        const double What = 1.0 / iWhat;
+        const double rhohat = rhohat_mu(iWhat);
+        const double ehat = ehat_mu(mu, qbar, rbarsq, vhatsq, What);
+        const double Phat = ehat * rhohat * (gam - 1.0);
+        const double hhat = rhohat * (1.0 + ehat) + Phat;
+        const double ahat = Phat / (hhat - Phat);
+        const double nua = (1.0 + ahat) * (1.0 + ehat) * iWhat;
+        const double nub = (1.0 + ahat) * (1.0 + qbar - mu * rbarsq);
+        const double nuhat = kmax(nua, nub);
+        const double muhat = 1.0 / (nuhat + mu * rbarsq);
+        return mu - muhat;
+    }
+    double aux_func(double mu) const    // eq. 49
+    {
+        const double x = 1.0 / (1.0 + mu * bsq);
+        const double rbarsq = x * (rsq * x + mu * (1.0 + x) * rbsq);
+        return mu * std::sqrt(1.0 + rbarsq) - 1.0;
+    }
+};
+
+// Illinois false position on [zm, zp] (kastaun.hpp:305-331 and 343-368); returns the last iterate
+// and the iteration count at exit (max_iterations when it did not converge)
+template <typename F>
+static double illinois(F&& f, double zm, double zp, int max_iterations, double tol, int& iter)
+{
+    double fm = f(zm), fp = f(zp);
+    int iterations = max_iterations;
+    if ((std::fabs(zm - zp) < tol) || ((std::fabs(fm) + std::fabs(fp)) < 2.0 * tol)) iterations = -1;
+    double z = 0.5 * (zm + zp);
+    for (iter = 0; iter < iterations; ++iter) {
+        z = (zm * fp - zp * fm) / (fp - fm);
+        const double fz = f(z);
+        if ((std::fabs(zm - zp) < tol) || (std::fabs(fz) < tol)) break;
+        if (fz * fp < 0.0) { zm = zp; fm = fp; zp = z; fp = fz; }
+        else { fm = 0.5 * fm; zp = z; fp = fz; }
+    }
+    return z;
+}
+
+static int u_to_p_kastaun(const Block& B, const double* U, double* P, int j, int i, int loc, int max_iterations,
+                          double tol)
+{
+    const Prescription& fl = B.c.floors;
+    const double gam = B.c.gam;
+    const double alpha = 1. / std::sqrt(-B.Gcon(loc, j, i, 0, 0));
+    const double a_over_g = alpha / B.Gdet(loc, j, i);
+    const double D = U[0] * a_over_g;
+    const double D_fl = kmax(D, fl.rho_min_const);
+    const double Qcov[4] = {(U[1] - U[0]) * a_over_g, U[2] * a_over_g, U[3] * a_over_g, U[4] * a_over_g};
+    const double ncov[4] = {-alpha, 0., 0., 0.};
+    double ncon[4];
+    B.raise(ncov, ncon, j, i, loc);
+    const double q = (-dot4(Qcov, ncon) - D) / D;
+    const double rcov[3] = {U[2] / U[0], U[3] / U[0], U[4] / U[0]};
+    double g[4][4];
+    for (int mu = 0; mu < 4; ++mu) for (int nu = 0; nu < 4; ++nu) g[mu][nu] = B.Gcon(loc, j, i, mu, nu);
+    double rcon[3];
+    for (int a = 0; a < 3; ++a)        // gamma^ij = g^ij - g^0i g^0j / g^00 (kastaun.hpp:250-262)
+        rcon[a] = ((g[a+1][1] - g[0][a+1]*g[0][1]/g[0][0])*rcov[0] +
+                   (g[a+1][2] - g[0][a+1]*g[0][2]/g[0][0])*rcov[1] +
+                   (g[a+1][3] - g[0][a+1]*g[0][3]/g[0][0])*rcov[2]);
+    double rsq = 0.0;
+    for (int a = 0; a < 3; ++a) rsq += rcon[a] * rcov[a];
+    double bsq = 0.0, bsq_rpsq = 0.0, rbsq = 0.0, bdotr = 0.0, bu[3] = {0.0, 0.0, 0.0};
+    if (B.nv > 5) {
+        const double sD = 1.0 / std::sqrt(D_fl);
+        for (int a = 0; a < 3; ++a) {
+            bu[a] = (U[5 + a] * a_over_g) * sD;
+            bdotr += bu[a] * rcov[a];
+        }
+        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) bsq += B.Gcov(loc, j, i, a + 1, b + 1) * bu[a] * bu[b];
+        bsq = kmax(0.0, bsq);
+        rbsq = bdotr * bdotr;
+        bsq_rpsq = bsq * rsq - rbsq;
+    }
+    const double zsq = rsq;
+    const double v0sq = kmin(zsq / (1.0 + zsq), 1.0 - 1.0 / (fl.gamma_max * fl.gamma_max));
+    KastaunResidual res{D, q, bsq, bsq_rpsq, rsq, rbsq, v0sq, gam, fl.rho_min_const, fl.u_min_const / D_fl,
+                        fl.gamma_max, fl.u_over_rho_max};
+    int iter = 0;
+    const double zb = illinois([&](double z) { return res.aux_func(z); }, 0., 1., max_iterations, tol, iter);
+    const double mu = illinois([&](double z) { return res(z); }, 0., zb, max_iterations, tol, iter);
+    if (iter == max_iterations) return max_iter;
+    const double x = res.x_mu(mu);
+    const double rbarsq = res.rbarsq_mu(mu, x);
+    const double vsq = res.vhatsq_mu(mu, rbarsq);
+    const double iW = res.iWhat_mu(vsq);
+    const double W = 1. / iW;
+    P[0] = res.rhohat_mu(iW);
+    const double qbar = res.qbar_mu(mu, x);
+    P[1] = res.ehat_mu(mu, qbar, rbarsq, vsq, W) * P[0];
+    for (int a = 0; a < 3; ++a) P[2 + a] = W * mu * x * (rcon[a] + mu * bdotr * bu[a]);
+    int fflag = 0;
+    if (res.used_density_floor) fflag |= FF_INVERTER_RHO;
+    if (res.used_energy_floor) fflag |= FF_INVERTER_U;
+    if (res.used_gamma_max) fflag |= FF_INVERTER_GAMMA;
+    if (res.used_energy_max) fflag |= FF_INVERTER_U_MAX;
+    return fflag;
+}
+
+// Inverter::u_to_p dispatch on inverter/type (inverter.cpp:54-64)
+static int u_to_p(const Block& B, const double* U, double* P, int j, int i, int loc, int max_iterations, double tol)
+{
+    if (B.c.inverter == 1) return u_to_p_kastaun(B, U, P, j, i, loc, max_iterations, tol);
+    return u_to_p_onedw(B, U, P, j, i, loc, max_iterations, tol);
+}
+
 // ---------------------------------------------------------------- state helpers
 struct Fields {
     std::vector<double> F[3], cmax[3], cmin[3];
@@ -1123,7 +1279,7 @@ static void block_utop(const Block& B, const double* U, double* P, double* pflag
         double Uc[8], Pc[8];
         load_cell(B, U, c, Uc);
         load_cell(B, P, c, Pc);
-        const int pf = u_to_p_onedw(B, Uc, Pc, j, i, center, B.c.iter_max, B.c.err_tol);
+        const int pf = u_to_p(B, Uc, Pc, j, i, center, B.c.iter_max, B.c.err_tol);
         store_cell(B, P, c, Pc, 5);
         pflag[c] = pf % 32;
         fflag[c] = (pf / 32) * 32;
@@ -2273,7 +2429,7 @@ double orc_max_divb(void* hp, const double* U, int avoid_inner, int avoid_outer)
 int orc_utop_cell(void* hp, int j, int i, const double* U, double* P)
 {
     const Block& B = ((Handle*)hp)->B;
-    return u_to_p_onedw(B, U, P, j, i, center, B.c.iter_max, B.c.err_tol);
+    return u_to_p(B, U, P, j, i, center, B.c.iter_max, B.c.err_tol);
 }
 
 // ---- EMHD and the implicit solve.  All field arrays are [10][N] (slots rho..B3, q, dP).

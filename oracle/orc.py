@@ -48,6 +48,7 @@ class Config(C.Structure):
         ("fix_average_neighbors", C.c_int32), ("fix_atmosphere", C.c_int32),
         ("cfl", C.c_double), ("dt_min", C.c_double), ("max_dt_increase", C.c_double),
         ("floors", Prescription),
+        ("inverter", C.c_int32),
     ]
 
 
@@ -128,6 +129,7 @@ def config_from_spec(spec):
     c.fix_average_neighbors = int(spec.fix_average_neighbors)
     c.fix_atmosphere = int(spec.fix_atmosphere)
     c.cfl, c.dt_min, c.max_dt_increase = spec.cfl, spec.dt_min, spec.max_dt_increase
+    c.inverter = 1 if spec.inverter == "kastaun" else 0
     for name, _ in Prescription._fields_:
         setattr(c.floors, name, type(getattr(c.floors, name))(getattr(spec.floors, name)))
     return c
