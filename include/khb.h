@@ -345,6 +345,29 @@ int khb_implicit_step(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_impli
                       const khb_fields* src, const khb_fields* P_solver, double* solve_norm, double* solve_fail,
                       double dt, void* stream);
 
+/* Flux::GetFlux with the EMHD variables (get_flux.hpp:60-373; prim_to_flux with the EMHD stress
+ * tensor, flux_functions.hpp:80-107 and 180-232; vchar with the EMHD-augmented sound speed,
+ * flux_functions.hpp:380-403): face fluxes of all 10 slots along dir into the context's EMHD flux
+ * scratch (allocated by khb_set_connection).  FP64 contexts with B only. */
+int khb_get_flux_emhd(khb_ctx* ctx, const khb_emhd_params* emhd, int dir, const khb_fields* P, void* stream);
+
+/* Copy one direction's EMHD face fluxes (10 slots, as doubles) and max(cmax, cmin) out of scratch. */
+int khb_copy_flux_emhd(khb_ctx* ctx, int dir, const khb_fields* F_out, double* ctop_out, void* stream);
+
+/* One ImEx stage (driver/imex_step.cpp:58-356) of the vl2 integrator the implicit package forces
+ * (implicit.cpp:96; stage 1: beta 1/2, stage 2: beta 1, both from the step-start state):
+ * EMHD fluxes, flux-CT, divergence, the geometric source with the EMHD tensor and EMHD::AddSource
+ * into dU/dt; the explicit update of B and B_P = B_U/gdet; the implicit guess copied from the
+ * sub-step state; Implicit::Step with beta dt (fluid and EMHD variables); FixSolve; periodic ghost
+ * zones; P -> U with the EMHD tensor over the whole block.  P_out/U_out must not alias P_sub/U_sub;
+ * exchange faces carry the sub-step ghost zones over.  Floors and physical (outflow/reflecting)
+ * faces on the EMHD state are rejected (KHB_ERR_UNSUPPORTED).  The last stage accumulates the zone
+ * timestep minimum (khb_get_min_ndt). */
+int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp, int stage, double dt,
+                   const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub, const khb_fields* U_sub,
+                   const khb_fields* P_out, const khb_fields* U_out, double* solve_norm, double* solve_fail,
+                   void* stream);
+
 /* Iterations taken by the last khb_implicit_step and the maximum solve_norm of each (max_norms
  * has room for max_nonlinear_iter values).  Synchronizes the stream. */
 int khb_implicit_stats(khb_ctx* ctx, int32_t* iterations, double* max_norms, void* stream);

@@ -133,6 +133,11 @@ SIGNATURES = {
                                    C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
                                    C.POINTER(KhbFields), C.POINTER(KhbFields), _D, _P, _P, _P]),
     "khb_fix_solve": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P]),
+    "khb_get_flux_emhd": (_I, [_P, C.POINTER(KhbEmhdParams), _I, C.POINTER(KhbFields), _P]),
+    "khb_copy_flux_emhd": (_I, [_P, _I, C.POINTER(KhbFields), _P, _P]),
+    "khb_imex_stage": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbImplicitParams), _I, _D,
+                            C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
+                            C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
     "khb_batch_create": (_I, [C.POINTER(_P), _I, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(_P),
                               C.POINTER(_P), C.POINTER(_P)]),
     "khb_batch_destroy": (_I, [_P]),

@@ -382,6 +382,8 @@ int khb_destroy(khb_ctx* c)
     cudaFree(c->words); cudaFree(c->fail_count); cudaFree(c->fail_list);
     cudaFree(c->geo_d); cudaFree(c->geo_f);
     cudaFree(c->conn_d); cudaFree(c->emhd_tmp); cudaFree(c->fix_buf); cudaFree(c->imp_words);
+    for (int x = 0; x < 3; ++x) cudaFree(c->F10[x]);
+    cudaFree(c->dudt10);
     delete c;
     return KHB_OK;
 }
@@ -717,6 +719,12 @@ int khb_set_connection(khb_ctx* ctx, const double* conn)
         KHB_CUDA(cudaMalloc((void**)&ctx->fix_buf, 7 * N * sizeof(double)));
         KHB_CUDA(cudaMemset(ctx->emhd_tmp, 0, 5 * N * sizeof(double)));
         KHB_CUDA(cudaMemset(ctx->fix_buf, 0, 7 * N * sizeof(double)));
+        for (int x = 0; x < 3; ++x) {
+            KHB_CUDA(cudaMalloc((void**)&ctx->F10[x], 10 * N * sizeof(double)));
+            KHB_CUDA(cudaMemset(ctx->F10[x], 0, 10 * N * sizeof(double)));
+        }
+        KHB_CUDA(cudaMalloc((void**)&ctx->dudt10, 10 * N * sizeof(double)));
+        KHB_CUDA(cudaMemset(ctx->dudt10, 0, 10 * N * sizeof(double)));
     }
     KHB_CUDA(cudaMemcpy(ctx->conn_d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     KHB_CUDA(cudaDeviceSynchronize());          // complete the upload (see khb_set_geometry)
@@ -791,6 +799,119 @@ int khb_implicit_step(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_impli
         KHB_LAUNCHED(ctx);
     }
     return KHB_OK;
+}
+
+// ---------------------------------------------------------------------------- explicit EMHD step and ImEx stage
+namespace {
+int emhd_flux_ready(khb_ctx* ctx, const khb_emhd_params* emhd, const char* who)
+{
+    if (check_emhd(emhd)) return KHB_ERR_ARG;
+    if (!ctx->F10[0]) return fail(KHB_ERR_STATE, std::string(who) + ": EMHD scratch not allocated (call khb_set_connection)");
+    if (ctx->nv != 8) return fail(KHB_ERR_UNSUPPORTED, std::string(who) + ": the block must carry B (nvar = 8)");
+    if (ctx->fp32) return fail(KHB_ERR_UNSUPPORTED, std::string(who) + ": the EMHD path is FP64 only");
+    return KHB_OK;
+}
+void emhd_face_range(const Dims& d, int dir, int lo[3], int cnt[3])
+{
+    const int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
+    for (int a = 0; a < 3; ++a) {
+        const bool active = (a + 1) <= d.ndim;
+        int hi;
+        if (a + 1 == dir) { lo[a] = s[a]; hi = e[a] + 1; }
+        else if (active) { lo[a] = s[a] - 1; hi = e[a] + 1; }
+        else { lo[a] = s[a]; hi = e[a]; }
+        cnt[a] = hi - lo[a] + 1;
+    }
+}
+khb_fields fields_of(double* base, long long N)
+{
+    khb_fields f;
+    for (int p = 0; p < KHB_MAX_VARS; ++p) f.v[p] = base + (size_t)p * N;
+    return f;
+}
+} // namespace
+
+int khb_get_flux_emhd(khb_ctx* ctx, const khb_emhd_params* emhd, int dir, const khb_fields* P, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = emhd_flux_ready(ctx, emhd, "khb_get_flux_emhd")) || (rc = check_fields10(emhd, P, "P"))) return rc;
+    if (dir < 1 || dir > ctx->d.ndim) return fail(KHB_ERR_ARG, "khb_get_flux_emhd: bad direction");
+    int lo[3], cnt[3];
+    emhd_face_range(ctx->d, dir, lo, cnt);
+    LaunchEmhd::flux(ctx->cfg.recon, dir, ctx->d, ctx->g, ctx->ph, *emhd, *P, ctx->F10[dir - 1],
+                     (double*)ctx->ctop[dir - 1], lo, cnt, S(stream));
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+int khb_copy_flux_emhd(khb_ctx* ctx, int dir, const khb_fields* F_out, double* ctop_out, void* stream)
+{
+    if (!ctx || dir < 1 || dir > 3 || !F_out) return fail(KHB_ERR_ARG, "khb_copy_flux_emhd: bad argument");
+    if (!ctx->F10[0]) return fail(KHB_ERR_STATE, "khb_copy_flux_emhd: EMHD scratch not allocated");
+    const size_t N = (size_t)ctx->d.N;
+    for (int p = 0; p < 10; ++p)
+        if (F_out->v[p])
+            KHB_CUDA(cudaMemcpyAsync(F_out->v[p], ctx->F10[dir - 1] + p * N, N * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, S(stream)));
+    if (ctop_out)
+        KHB_CUDA(cudaMemcpyAsync(ctop_out, ctx->ctop[dir - 1], N * sizeof(double), cudaMemcpyDeviceToDevice, S(stream)));
+    return KHB_OK;
+}
+
+int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp, int stage, double dt,
+                   const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub, const khb_fields* U_sub,
+                   const khb_fields* P_out, const khb_fields* U_out, double* solve_norm, double* solve_fail,
+                   void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = emhd_flux_ready(ctx, emhd, "khb_imex_stage"))) return rc;
+    if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_imex_stage: stage must be 1 or 2");
+    if ((rc = check_fields10(emhd, P_full, "P_full")) || (rc = check_fields10(emhd, U_full, "U_full")) ||
+        (rc = check_fields10(emhd, P_sub, "P_sub")) || (rc = check_fields10(emhd, U_sub, "U_sub")) ||
+        (rc = check_fields10(emhd, P_out, "P_out")) || (rc = check_fields10(emhd, U_out, "U_out"))) return rc;
+    if (P_out->v[0] == P_sub->v[0] || U_out->v[0] == U_sub->v[0])
+        return fail(KHB_ERR_ARG, "khb_imex_stage: the output state must not alias the sub-step state");
+    if (!solve_norm || !solve_fail) return fail(KHB_ERR_ARG, "khb_imex_stage: NULL solve_norm/solve_fail");
+    if (ctx->ph.floors_on) return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: floors on the EMHD state are not supported");
+    const Dims& d = ctx->d;
+    for (int f = 0; f < 2 * d.ndim; ++f)
+        if (phys_face(d.bc[f]))
+            return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: physical boundaries of the EMHD state are not supported "
+                                             "(use periodic or exchange faces)");
+    cudaStream_t st = S(stream);
+    const int s = stage - 1;
+    // vl2, which the implicit package forces (implicit.cpp:96): gam0 = {0, 0}, gam1 = {1, 1}, beta = {1/2, 1}
+    const double g0 = 0.0, g1 = 1.0, beta = (stage == 1) ? 0.5 : 1.0, bdt = beta * dt;
+    for (int dir = 1; dir <= d.ndim; ++dir)
+        if ((rc = khb_get_flux_emhd(ctx, emhd, dir, P_sub, stream))) return rc;
+    if (stage == 2)
+        KHB_CUDA(cudaMemcpyAsync(ctx->words, &ctx->dbl_max_bits, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+    khb_fields du = fields_of(ctx->dudt10, d.N);
+    for (int p = 8; p < 10; ++p)
+        if (!((p == 8 && emhd->conduction) || (p == 9 && emhd->viscosity))) du.v[p] = nullptr;
+    double* ct[3] = {(double*)ctx->ctop[0], (double*)ctx->ctop[1], (double*)ctx->ctop[2]};
+    LaunchEmhd::dudt(d, ctx->g, ctx->ph, *emhd, ctx->F10, ct, *P_sub, du, stage == 2, ctx->words, st);
+    KHB_LAUNCHED(ctx);
+    LaunchEmhd::add_source(d, ctx->g, ctx->conn_d, ctx->ph.gam, *emhd, ctx->ph, *P_sub, ctx->emhd_tmp, du, st);
+    ctx->launches += 1;
+    KHB_LAUNCHED(ctx);
+    LaunchEmhd::imex_explicit(d, ctx->g, *P_sub, *U_sub, *U_full, du, *P_out, *U_out, g0, g1, bdt, st);
+    KHB_LAUNCHED(ctx);
+    (void)s;
+    if ((rc = khb_implicit_step(ctx, emhd, imp, P_full, U_full, P_sub, &du, P_out, solve_norm, solve_fail, bdt,
+                                stream))) return rc;
+    if ((rc = khb_fix_solve(ctx, emhd, P_out, U_out, solve_fail, stream))) return rc;
+    int pmask = 0;
+    if (d.bc[0] == KHB_BC_PERIODIC) pmask |= 1;
+    if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) pmask |= 2;
+    if (d.ndim >= 3 && d.bc[4] == KHB_BC_PERIODIC) pmask |= 4;
+    if (pmask) {
+        LaunchCommon::periodic(10, d, *P_out, *U_out, pmask, st);
+        KHB_LAUNCHED(ctx);
+    }
+    return khb_emhd_ptou(ctx, emhd, P_out, U_out, stream);
 }
 
 int khb_implicit_stats(khb_ctx* ctx, int32_t* iterations, double* max_norms, void* stream)

@@ -221,6 +221,23 @@ __device__ __forceinline__ void prim_to_flux(const R* P, const FourVec<R>& D, R 
     }
 }
 
+// The fast-magnetosonic signal speeds along dir for a given cms2 (flux_functions.hpp:411-438)
+template <typename R>
+__device__ __forceinline__ void vchar_speeds(R cms2, const FourVec<R>& D, R gcon00, R gcon0d, R gcondd, int dir,
+                                             R& cmax, R& cmin)
+{
+    const R Asq = gcondd, Bsq = gcon00, AB = gcon0d;
+    const R Au = D.ucon[dir], Bu = D.ucon[0];
+    const R A  = Bu*Bu - (Bsq + Bu*Bu) * cms2;
+    const R Bq = R(2.) * (Au*Bu - (AB + Au*Bu) * cms2);
+    const R Cq = Au*Au - (Asq + Au*Au) * cms2;
+    const R discr = dsqrt(kmax(Bq * Bq - R(4.) * A * Cq, R(0)));
+    const R vp = -(-Bq + discr) / (R(2.) * A);
+    const R vm = -(-Bq - discr) / (R(2.) * A);
+    cmax = kmax(vp, vm);
+    cmin = kmin(vp, vm);
+}
+
 // flux_functions.hpp:368-439.  The reference discards its clip() results (:378, :409), so no
 // clipping happens here either.  With A_mu = delta^dir_mu and B_mu = delta^0_mu the raised
 // vectors and their contractions reduce exactly to single metric entries.
@@ -238,16 +255,7 @@ __device__ __forceinline__ void vchar(const R* P, const FourVec<R>& D, R gam, R 
     } else {
         cms2 = cs2;
     }
-    const R Asq = gcondd, Bsq = gcon00, AB = gcon0d;
-    const R Au = D.ucon[dir], Bu = D.ucon[0];
-    const R A  = Bu*Bu - (Bsq + Bu*Bu) * cms2;
-    const R Bq = R(2.) * (Au*Bu - (AB + Au*Bu) * cms2);
-    const R Cq = Au*Au - (Asq + Au*Au) * cms2;
-    const R discr = dsqrt(kmax(Bq * Bq - R(4.) * A * Cq, R(0)));
-    const R vp = -(-Bq + discr) / (R(2.) * A);
-    const R vm = -(-Bq - discr) / (R(2.) * A);
-    cmax = kmax(vp, vm);
-    cmin = kmin(vp, vm);
+    vchar_speeds<R>(cms2, D, gcon00, gcon0d, gcondd, dir, cmax, cmin);
 }
 
 // ------------------------------------------------------------------ 1D_W inversion (FP64)

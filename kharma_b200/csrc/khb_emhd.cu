@@ -153,6 +153,56 @@ __device__ __forceinline__ void emhd_p_to_u(const EmhdArgs& E, double gam, const
     if (E.viscosity) U[9] = P[9] * D.ucon[0] * gdet;
 }
 
+// Flux::prim_to_flux for the 10-slot state at any location (dir = 0: conserved variables), with the
+// EMHD stress tensor when q or dP feed back (flux_functions.hpp:80-107, 180-232).  Inactive EMHD
+// slots get 0.
+__device__ __forceinline__ void emhd_prim_to_flux(const EmhdArgs& E, double gam, double gdet, const double* P,
+                                                  const FourVec<double>& D, int dir, double* flux)
+{
+    flux[0] = P[0] * D.ucon[dir] * gdet;
+    double T[4];
+    if ((E.conduction || E.viscosity) && E.feedback) {
+        const double qt = E.conduction ? P[8] : 0., dPt = E.viscosity ? P[9] : 0.;
+        const double Theta = (gam - 1) * P[1] / P[0];
+        const double cs2 = gam * (gam - 1) * P[1] / (P[0] + gam * P[1]);
+        double q, dP;
+        convert_q_dP(E, qt, dPt, P[0], Theta, cs2, q, dP);
+        emhd_tensor(P[0], P[1], (gam - 1) * P[1], q, dP, D, dir, T);
+    } else {
+        calc_tensor<double, true>(P[0], P[1], (gam - 1) * P[1], D, dir, T);
+    }
+    flux[1] = T[0] * gdet + flux[0];
+    flux[2] = T[1] * gdet;
+    flux[3] = T[2] * gdet;
+    flux[4] = T[3] * gdet;
+    if (dir == 0) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) flux[5 + v] = P[5 + v] * gdet;
+    } else {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) flux[5 + v] = (D.bcon[v+1] * D.ucon[dir] - D.bcon[dir] * D.ucon[v+1]) * gdet;
+    }
+    flux[8] = E.conduction ? P[8] * D.ucon[dir] * gdet : 0.;
+    flux[9] = E.viscosity ? P[9] * D.ucon[dir] * gdet : 0.;
+}
+
+// vchar with the EMHD-augmented sound speed (flux_functions.hpp:380-403); the closure parameters the
+// reference computes there are unused, so they are not formed
+__device__ __forceinline__ void emhd_vchar(const EmhdArgs& E, double gam, const double* P, const FourVec<double>& D,
+                                           double gcon00, double gcon0d, double gcondd, int dir,
+                                           double& cmax, double& cmin)
+{
+    const double ef  = P[0] + gam * P[1];
+    const double cs2 = gam * (gam - 1) * P[1] / ef;
+    const double bsq = dot4(D.bcon, D.bcov);
+    const double va2 = bsq / (bsq + ef);
+    const double ccond2 = E.conduction ? (gam - 1.) * E.conduction_alpha * cs2 : 0.0;
+    const double cvis2 = E.viscosity ? (4./3.) / (P[0] + (gam * P[1])) * P[0] * E.viscosity_alpha * cs2 : 0.0;
+    const double cs2_emhd = 0.5*(cs2 + ccond2 + sqrt(cs2*cs2 + ccond2*ccond2)) + cvis2;
+    const double cms2 = cs2_emhd + va2 - cs2_emhd*va2;
+    vchar_speeds<double>(cms2, D, gcon00, gcon0d, gcondd, dir, cmax, cmin);
+}
+
 // ------------------------------------------------------------------------------ residual
 // Constants of one zone's residual (everything that does not depend on the trial state)
 template <int NF>
@@ -759,6 +809,170 @@ __global__ void __launch_bounds__(128) k_emhd_ptou(Dims d, DevGeom g, double gam
     if (E.viscosity) U.v[9][c] = Uz[9];
 }
 
+// ------------------------------------------------------------------------------ explicit EMHD step
+// Flux::GetFlux with the EMHD variables (get_flux.hpp:60-373): one thread per face, every active
+// slot reconstructed, U and F with the EMHD tensor, EMHD signal speeds, LLF/HLLE.  F is [10][N].
+template <int DIR, int RECON, bool HQ, bool HD>
+__global__ void __launch_bounds__(128) k_flux_emhd(Dims d, DevGeom g, Phys ph, EmhdArgs E, khb_fields P,
+                                                   double* __restrict__ F, double* __restrict__ ctop, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long st = (DIR == 1) ? 1 : ((DIR == 2) ? d.sj : d.sk);
+    const int loc = DIR - 1;
+    const double gam = ph.gam;
+    const long long gi = (long long)j*g.G1 + i;
+    double gcov[4][4], gcon0[4];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) gcov[m/4][m%4] = __ldg(g.gcov[loc] + m*g.gs + gi);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) gcon0[m] = __ldg(g.gcon[loc] + m*g.gs + gi);
+    const double gcondd = __ldg(g.gcon[loc] + (DIR*4 + DIR)*g.gs + gi);
+    const double gdet = __ldg(g.gdet[loc] + gi);
+    double Pl[10], Pr[10];
+#pragma unroll
+    for (int p = 0; p < 10; ++p) {
+        const bool on = p < 8 || (p == 8 && HQ) || (p == 9 && HD);
+        if (!on) { Pl[p] = Pr[p] = 0.; continue; }
+        const double* q = P.v[p];
+        const double x0 = __ldg(q + c - 3*st), x1 = __ldg(q + c - 2*st), x2 = __ldg(q + c - st);
+        const double x3 = __ldg(q + c), x4 = __ldg(q + c + st), x5 = __ldg(q + c + 2*st);
+        Pl[p] = recon_right<RECON, double>(x0, x1, x2, x3, x4);
+        Pr[p] = recon_left<RECON, double>(x1, x2, x3, x4, x5);
+    }
+    FourVec<double> D;
+    double Ul[10], Fl[10], Ur[10], Fr[10], cmaxL, cminL, cmaxR, cminR;
+    calc_4vecs<double, true>(gcov, gcon0[0], gcon0, Pl, D);
+    emhd_prim_to_flux(E, gam, gdet, Pl, D, 0, Ul);
+    emhd_prim_to_flux(E, gam, gdet, Pl, D, DIR, Fl);
+    emhd_vchar(E, gam, Pl, D, gcon0[0], gcon0[DIR], gcondd, DIR, cmaxL, cminL);
+    calc_4vecs<double, true>(gcov, gcon0[0], gcon0, Pr, D);
+    emhd_prim_to_flux(E, gam, gdet, Pr, D, 0, Ur);
+    emhd_prim_to_flux(E, gam, gdet, Pr, D, DIR, Fr);
+    emhd_vchar(E, gam, Pr, D, gcon0[0], gcon0[DIR], gcondd, DIR, cmaxR, cminR);
+    const double cmax = kmax(kmax(0., cmaxL), cmaxR);
+    const double cmin = -kmin(kmin(0., cminL), cminR);
+#pragma unroll
+    for (int p = 0; p < 10; ++p) {
+        const bool on = p < 8 || (p == 8 && HQ) || (p == 9 && HD);
+        double f = 0.;
+        if (on) {
+            if (ph.riemann == 0) f = 0.5 * (Fl[p] + Fr[p] - kmax(cmax, cmin) * (Ur[p] - Ul[p]));
+            else f = (cmax*Fl[p] + cmin*Fr[p] - cmax*cmin*(Ur[p] - Ul[p])) / (cmax + cmin);
+        }
+        F[p*d.N + c] = f;
+    }
+    ctop[c] = kmax(cmax, cmin);
+}
+
+// dU/dt over the interior: -div F of every active slot (flux-CT for B), plus Flux::AddGeoSource with
+// the EMHD stress tensor (flux.cpp:395-444); the EMHD explicit sources are added by k_emhd_sources.
+// With dtm the stage's zone timestep minimum is accumulated as in k_zone.
+template <bool HQ, bool HD>
+__global__ void __launch_bounds__(128) k_emhd_dudt(Dims d, DevGeom g, Phys ph, EmhdArgs E, const double* F1,
+                                                   const double* F2, const double* F3, const double* c1,
+                                                   const double* c2, const double* c3, khb_fields Ps,
+                                                   khb_fields dUdt, int dtm, unsigned long long* word, Box bx)
+{
+    int i, j, k;
+    double ndt_zone = 1.7976931348623157e308;
+    if (box_cell(bx, blockIdx.x, i, j, k)) {
+        const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+        const long long N = d.N, sj = d.sj, sk = d.sk;
+        const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
+        const double vol = ph.dx1*ph.dx2*ph.dx3;
+        double du_[10];
+#pragma unroll
+        for (int p = 0; p < 10; ++p) {
+            const bool on = p < 5 || (p == 8 && HQ) || (p == 9 && HD);
+            if (!on) { du_[p] = 0.; continue; }
+            double du = (a1 * __ldg(F1 + p*N + c + 1) - a1 * __ldg(F1 + p*N + c));
+            if (d.ndim >= 2) du += a2 * __ldg(F2 + p*N + c + sj) - a2 * __ldg(F2 + p*N + c);
+            if (d.ndim == 3) du += a3 * __ldg(F3 + p*N + c + sk) - a3 * __ldg(F3 + p*N + c);
+            du_[p] = -du / vol;
+        }
+        double db[3];
+        ct_divergence<double>(d, ph, F1, F2, F3, c, j, db);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) du_[5 + v] = db[v];
+        if (!ph.cart_minkowski) {
+            CenterGeom G;
+            load_center(g, j, i, G);
+            double Pz[10];
+            load10(Ps, c, Pz);
+            FourVec<double> D;
+            calc_4vecs<double, true>(G.gcov, G.gcon0[0], G.gcon0, Pz, D);
+            double new_du[4] = {0., 0., 0., 0.};
+            const long long cg = (long long)j*g.n1 + i, cs = (long long)(d.n2)*g.n1;
+            const double gam = ph.gam;
+#pragma unroll
+            for (int mu = 0; mu < 4; ++mu) {
+                double Tmu[4];
+                if ((E.conduction || E.viscosity) && E.feedback) {
+                    const double qt = E.conduction ? Pz[8] : 0., dPt = E.viscosity ? Pz[9] : 0.;
+                    const double Theta = (gam - 1) * Pz[1] / Pz[0];
+                    const double cs2 = gam * (gam - 1) * Pz[1] / (Pz[0] + gam * Pz[1]);
+                    double q, dP;
+                    convert_q_dP(E, qt, dPt, Pz[0], Theta, cs2, q, dP);
+                    emhd_tensor(Pz[0], Pz[1], (gam - 1) * Pz[1], q, dP, D, mu, Tmu);
+                } else {
+                    calc_tensor<double, true>(Pz[0], Pz[1], (gam - 1) * Pz[1], D, mu, Tmu);
+                }
+#pragma unroll
+                for (int nu = 0; nu < 4; ++nu)
+#pragma unroll
+                    for (int lam = 0; lam < 4; ++lam)
+                        new_du[lam] += Tmu[nu] * __ldg(g.gdet_conn + ((nu*4 + lam)*4 + mu)*cs + cg);
+            }
+            du_[1] += new_du[0];
+            du_[2] += new_du[1];
+            du_[3] += new_du[2];
+            du_[4] += new_du[3];
+        }
+#pragma unroll
+        for (int p = 0; p < 10; ++p) if (dUdt.v[p]) dUdt.v[p][c] = du_[p];
+        if (dtm) {
+            const double z = 1.0 / (1 / (ph.dx1 / kmax(c1[c], 0.0)) + 1 / (ph.dx2 / kmax(c2[c], 0.0)) +
+                                    1 / (ph.dx3 * 1 / kmax(c3[c], 0.0)));
+            if (!isnan(z)) ndt_zone = z;
+        }
+    }
+    if (dtm) block_min_ndt(ndt_zone, word);
+}
+
+// The explicit half of AddStateUpdate for an ImEx stage (imex_step.cpp:200-215 with the Explicit
+// flag on B only) and the solver's starting state: P_out/U_out = the sub-step state over the whole
+// block (the implicit guess copy, imex_step.cpp:228-238), B_U updated over the interior with the
+// stage weights, then B_P = B_U/gdet everywhere (B_FluxCT::BlockUtoP).
+__global__ void __launch_bounds__(128) k_imex_explicit(Dims d, DevGeom g, khb_fields Psub, khb_fields Usub,
+                                                       khb_fields Ufull, khb_fields dUdt, khb_fields Pout,
+                                                       khb_fields Uout, double g0, double g1, double bdt)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N) return;
+    int k, j, i;
+    zone_kji(d, c, k, j, i);
+    const bool interior = i >= d.is && i <= d.ie && j >= d.js && j <= d.je && k >= d.ks && k <= d.ke;
+    const double gdet = __ldg(g.gdet[3] + (long long)j*g.G1 + i);
+#pragma unroll
+    for (int p = 0; p < 10; ++p) {
+        if (!Pout.v[p]) continue;
+        if (p >= 5 && p < 8) {
+            double u = Usub.v[p][c];
+            if (interior) {
+                u = g0 * u + g1 * Ufull.v[p][c];
+                u = 1.0 * u + bdt * dUdt.v[p][c];
+            }
+            Uout.v[p][c] = u;
+            Pout.v[p][c] = u / gdet;
+        } else {
+            Pout.v[p][c] = Psub.v[p][c];
+            Uout.v[p][c] = Usub.v[p][c];
+        }
+    }
+}
+
 // EMHD::AddSource temporaries (emhd.cpp:329-343): u_mu (4) and Theta over the interior plus one halo zone
 __global__ void __launch_bounds__(128) k_emhd_temps(Dims d, DevGeom g, double gam, khb_fields P, double* tmp,
                                                     int il, int jl, int kl, int ci, int cj, int ck)
@@ -1143,6 +1357,57 @@ static void fix_hd(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& 
         else if ((E).viscosity) FN<false, true>(__VA_ARGS__);        \
         else FN<false, false>(__VA_ARGS__);                          \
     } while (0)
+
+template <int DIR, bool HQ, bool HD>
+static void flux_emhd_dir(int recon, const Dims& d, const DevGeom& g, const Phys& ph, const EmhdArgs& E,
+                          const khb_fields& P, double* F, double* ctop, const Box& bx, cudaStream_t st)
+{
+    const unsigned nb = box_blocks(bx);
+    switch (recon) {
+    case RECON_DONOR: k_flux_emhd<DIR, RECON_DONOR, HQ, HD><<<nb, 128, 0, st>>>(d, g, ph, E, P, F, ctop, bx); break;
+    case RECON_MC:    k_flux_emhd<DIR, RECON_MC, HQ, HD><<<nb, 128, 0, st>>>(d, g, ph, E, P, F, ctop, bx); break;
+    case RECON_WENO5: k_flux_emhd<DIR, RECON_WENO5, HQ, HD><<<nb, 128, 0, st>>>(d, g, ph, E, P, F, ctop, bx); break;
+    default:          k_flux_emhd<DIR, RECON_PPM, HQ, HD><<<nb, 128, 0, st>>>(d, g, ph, E, P, F, ctop, bx); break;
+    }
+}
+template <bool HQ, bool HD>
+static void flux_emhd_hd(int recon, int dir, const Dims& d, const DevGeom& g, const Phys& ph, const EmhdArgs& E,
+                         const khb_fields& P, double* F, double* ctop, const Box& bx, cudaStream_t st)
+{
+    if (dir == 1) flux_emhd_dir<1, HQ, HD>(recon, d, g, ph, E, P, F, ctop, bx, st);
+    else if (dir == 2) flux_emhd_dir<2, HQ, HD>(recon, d, g, ph, E, P, F, ctop, bx, st);
+    else flux_emhd_dir<3, HQ, HD>(recon, d, g, ph, E, P, F, ctop, bx, st);
+}
+void LaunchEmhd::flux(int recon, int dir, const Dims& d, const DevGeom& g, const Phys& ph, const EmhdArgs& E,
+                      const khb_fields& P, double* F, double* ctop, const int lo[3], const int cnt[3], cudaStream_t st)
+{
+    const Box bx = make_box(lo[0], lo[1], lo[2], cnt[0], cnt[1], cnt[2]);
+    if (E.conduction && E.viscosity) flux_emhd_hd<true, true>(recon, dir, d, g, ph, E, P, F, ctop, bx, st);
+    else if (E.conduction) flux_emhd_hd<true, false>(recon, dir, d, g, ph, E, P, F, ctop, bx, st);
+    else if (E.viscosity) flux_emhd_hd<false, true>(recon, dir, d, g, ph, E, P, F, ctop, bx, st);
+    else flux_emhd_hd<false, false>(recon, dir, d, g, ph, E, P, F, ctop, bx, st);
+}
+void LaunchEmhd::dudt(const Dims& d, const DevGeom& g, const Phys& ph, const EmhdArgs& E, double* const F[3],
+                      double* const ctop[3], const khb_fields& Ps, const khb_fields& dUdt, int dtm,
+                      unsigned long long* word, cudaStream_t st)
+{
+    const Box bx = make_box(d.is, d.js, d.ks, d.ie - d.is + 1, d.je - d.js + 1, d.ke - d.ks + 1);
+    const unsigned nb = box_blocks(bx);
+    if (E.conduction && E.viscosity)
+        k_emhd_dudt<true, true><<<nb, 128, 0, st>>>(d, g, ph, E, F[0], F[1], F[2], ctop[0], ctop[1], ctop[2], Ps, dUdt, dtm, word, bx);
+    else if (E.conduction)
+        k_emhd_dudt<true, false><<<nb, 128, 0, st>>>(d, g, ph, E, F[0], F[1], F[2], ctop[0], ctop[1], ctop[2], Ps, dUdt, dtm, word, bx);
+    else if (E.viscosity)
+        k_emhd_dudt<false, true><<<nb, 128, 0, st>>>(d, g, ph, E, F[0], F[1], F[2], ctop[0], ctop[1], ctop[2], Ps, dUdt, dtm, word, bx);
+    else
+        k_emhd_dudt<false, false><<<nb, 128, 0, st>>>(d, g, ph, E, F[0], F[1], F[2], ctop[0], ctop[1], ctop[2], Ps, dUdt, dtm, word, bx);
+}
+void LaunchEmhd::imex_explicit(const Dims& d, const DevGeom& g, const khb_fields& Psub, const khb_fields& Usub,
+                               const khb_fields& Ufull, const khb_fields& dUdt, const khb_fields& Pout,
+                               const khb_fields& Uout, double g0, double g1, double bdt, cudaStream_t st)
+{
+    k_imex_explicit<<<blocks_for(d.N, 128), 128, 0, st>>>(d, g, Psub, Usub, Ufull, dUdt, Pout, Uout, g0, g1, bdt);
+}
 
 void LaunchEmhd::ptou(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,
                       const khb_fields& U, cudaStream_t st)

@@ -33,6 +33,8 @@ struct khb_ctx {
     double* emhd_tmp;      // EMHD::AddSource temporaries u_mu, Theta: [5][N]
     double* fix_buf;       // FixSolve replacement values: [7][N]
     unsigned long long* imp_words;   // implicit-solve reductions, IMP_WORDS entries
+    double* F10[3];        // EMHD face fluxes, [10][N] per direction
+    double* dudt10;        // EMHD dU/dt of an ImEx stage, [10][N]
 };
 
 

@@ -252,6 +252,69 @@ __global__ void k_fix_flux_x1(Dims d, FT* F1, int inner)
 template <typename FT>
 __device__ __forceinline__ double ldf(const FT* F, long long x) { return (double)__ldg(F + x); }
 
+// Divergence of the B fluxes with flux-CT applied on the fly (b_flux_ct.cpp:307-370): corner EMFs
+// from the raw B fluxes in FT arithmetic, the face B fluxes from the EMFs, then -div over the zone.
+// F1..F3 hold nvar-major fluxes with the B components in slots 5-7 (stride d.N).
+template <typename FT>
+__device__ __forceinline__ void ct_divergence(const Dims& d, const Phys& ph, const FT* F1, const FT* F2, const FT* F3,
+                                              long long c, int j, double dudt_b[3])
+{
+    const long long N = d.N, sj = d.sj, sk = d.sk;
+    const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
+    const double vol = ph.dx1*ph.dx2*ph.dx3;
+    double fb[3][3][2];   // [face dir][B component][lo/hi face]
+    if (d.ndim >= 2) {
+        const long long B1 = 5*N, B2 = 6*N, B3 = 7*N;
+        auto e3 = [&](long long x) -> FT {
+            return (FT)0.25 * (__ldg(F1 + B2 + x) + __ldg(F1 + B2 + x - sj) - __ldg(F2 + B1 + x) - __ldg(F2 + B1 + x - 1));
+        };
+        auto e1 = [&](long long x) -> FT {
+            return (FT)0.25 * (__ldg(F2 + B3 + x) + __ldg(F2 + B3 + x - sk) - __ldg(F3 + B2 + x) - __ldg(F3 + B2 + x - sj));
+        };
+        auto e2 = [&](long long x) -> FT {
+            return (FT)0.25 * (__ldg(F3 + B1 + x) + __ldg(F3 + B1 + x - 1) - __ldg(F1 + B3 + x) - __ldg(F1 + B3 + x - sk));
+        };
+        const bool d3 = d.ndim > 2;
+        // X1 faces i (lo) and i+1 (hi)
+        fb[0][0][0] = 0.; fb[0][0][1] = 0.;
+        fb[0][1][0] = (double)((FT)0.5 * (e3(c) + e3(c + sj)));
+        fb[0][1][1] = (double)((FT)0.5 * (e3(c + 1) + e3(c + 1 + sj)));
+        fb[0][2][0] = d3 ? (double)((FT)-0.5 * (e2(c) + e2(c + sk))) : ldf(F1, B3 + c);
+        fb[0][2][1] = d3 ? (double)((FT)-0.5 * (e2(c + 1) + e2(c + 1 + sk))) : ldf(F1, B3 + c + 1);
+        // X2 faces j, j+1
+        fb[1][0][0] = (double)((FT)-0.5 * (e3(c) + e3(c + 1)));
+        fb[1][0][1] = (double)((FT)-0.5 * (e3(c + sj) + e3(c + sj + 1)));
+        fb[1][1][0] = 0.; fb[1][1][1] = 0.;
+        fb[1][2][0] = d3 ? (double)((FT)0.5 * (e1(c) + e1(c + sk))) : ldf(F2, B3 + c);
+        fb[1][2][1] = d3 ? (double)((FT)0.5 * (e1(c + sj) + e1(c + sj + sk))) : ldf(F2, B3 + c + sj);
+        // KBoundaries zero_polar_flux after flux-CT (boundaries.cpp:672-684)
+        if (ph.zero_polar_flux) {
+            if (j == d.js && phys_face(d.bc[2])) { fb[1][0][0] = 0.; fb[1][1][0] = 0.; fb[1][2][0] = 0.; }
+            if (j == d.je && phys_face(d.bc[3])) { fb[1][0][1] = 0.; fb[1][1][1] = 0.; fb[1][2][1] = 0.; }
+        }
+        if (d3) {
+            fb[2][0][0] = (double)((FT)0.5 * (e2(c) + e2(c + 1)));
+            fb[2][0][1] = (double)((FT)0.5 * (e2(c + sk) + e2(c + sk + 1)));
+            fb[2][1][0] = (double)((FT)-0.5 * (e1(c) + e1(c + sj)));
+            fb[2][1][1] = (double)((FT)-0.5 * (e1(c + sk) + e1(c + sk + sj)));
+            fb[2][2][0] = 0.; fb[2][2][1] = 0.;
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            fb[0][v][0] = ldf(F1, (5 + v)*N + c);
+            fb[0][v][1] = ldf(F1, (5 + v)*N + c + 1);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        double du = (a1 * fb[0][v][1] - a1 * fb[0][v][0]);
+        if (d.ndim >= 2) du += a2 * fb[1][v][1] - a2 * fb[1][v][0];
+        if (d.ndim == 3) du += a3 * fb[2][v][1] - a3 * fb[2][v][0];
+        dudt_b[v] = -du / vol;
+    }
+}
+
 // MODE: compile-time mask of M_* steps (0: take the mask from the arguments at run time).  The
 // CFL reduction (M_DT) is always a run-time choice.
 // One zone of the zone pass; returns the zone's timestep for the CFL minimum (DBL_MAX if none)
@@ -284,58 +347,10 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
                 dudt[p] = -du / vol;
             }
             if (NV > 5) {
-                // b_flux_ct.cpp:307-370, evaluated per zone from the raw B fluxes, in FT arithmetic
-                double fb[3][3][2];   // [face dir][B component][lo/hi face]
-                if (d.ndim >= 2) {
-                    const long long B1 = 5*N, B2 = 6*N, B3 = 7*N;
-                    auto e3 = [&](long long x) -> FT {
-                        return (FT)0.25 * (__ldg(F1 + B2 + x) + __ldg(F1 + B2 + x - sj) - __ldg(F2 + B1 + x) - __ldg(F2 + B1 + x - 1));
-                    };
-                    auto e1 = [&](long long x) -> FT {
-                        return (FT)0.25 * (__ldg(F2 + B3 + x) + __ldg(F2 + B3 + x - sk) - __ldg(F3 + B2 + x) - __ldg(F3 + B2 + x - sj));
-                    };
-                    auto e2 = [&](long long x) -> FT {
-                        return (FT)0.25 * (__ldg(F3 + B1 + x) + __ldg(F3 + B1 + x - 1) - __ldg(F1 + B3 + x) - __ldg(F1 + B3 + x - sk));
-                    };
-                    const bool d3 = d.ndim > 2;
-                    // X1 faces i (lo) and i+1 (hi)
-                    fb[0][0][0] = 0.; fb[0][0][1] = 0.;
-                    fb[0][1][0] = (double)((FT)0.5 * (e3(c) + e3(c + sj)));
-                    fb[0][1][1] = (double)((FT)0.5 * (e3(c + 1) + e3(c + 1 + sj)));
-                    fb[0][2][0] = d3 ? (double)((FT)-0.5 * (e2(c) + e2(c + sk))) : ldf(F1, B3 + c);
-                    fb[0][2][1] = d3 ? (double)((FT)-0.5 * (e2(c + 1) + e2(c + 1 + sk))) : ldf(F1, B3 + c + 1);
-                    // X2 faces j, j+1
-                    fb[1][0][0] = (double)((FT)-0.5 * (e3(c) + e3(c + 1)));
-                    fb[1][0][1] = (double)((FT)-0.5 * (e3(c + sj) + e3(c + sj + 1)));
-                    fb[1][1][0] = 0.; fb[1][1][1] = 0.;
-                    fb[1][2][0] = d3 ? (double)((FT)0.5 * (e1(c) + e1(c + sk))) : ldf(F2, B3 + c);
-                    fb[1][2][1] = d3 ? (double)((FT)0.5 * (e1(c + sj) + e1(c + sj + sk))) : ldf(F2, B3 + c + sj);
-                    // KBoundaries zero_polar_flux after flux-CT (boundaries.cpp:672-684)
-                    if (ph.zero_polar_flux) {
-                        if (j == d.js && phys_face(d.bc[2])) { fb[1][0][0] = 0.; fb[1][1][0] = 0.; fb[1][2][0] = 0.; }
-                        if (j == d.je && phys_face(d.bc[3])) { fb[1][0][1] = 0.; fb[1][1][1] = 0.; fb[1][2][1] = 0.; }
-                    }
-                    if (d3) {
-                        fb[2][0][0] = (double)((FT)0.5 * (e2(c) + e2(c + 1)));
-                        fb[2][0][1] = (double)((FT)0.5 * (e2(c + sk) + e2(c + sk + 1)));
-                        fb[2][1][0] = (double)((FT)-0.5 * (e1(c) + e1(c + sj)));
-                        fb[2][1][1] = (double)((FT)-0.5 * (e1(c + sk) + e1(c + sk + sj)));
-                        fb[2][2][0] = 0.; fb[2][2][1] = 0.;
-                    }
-                } else {
+                double dudt_b[3];
+                ct_divergence<FT>(d, ph, F1, F2, F3, c, j, dudt_b);
 #pragma unroll
-                    for (int v = 0; v < 3; ++v) {
-                        fb[0][v][0] = ldf(F1, (5 + v)*N + c);
-                        fb[0][v][1] = ldf(F1, (5 + v)*N + c + 1);
-                    }
-                }
-#pragma unroll
-                for (int v = 0; v < 3; ++v) {
-                    double du = (a1 * fb[0][v][1] - a1 * fb[0][v][0]);
-                    if (d.ndim >= 2) du += a2 * fb[1][v][1] - a2 * fb[1][v][0];
-                    if (d.ndim == 3) du += a3 * fb[2][v][1] - a3 * fb[2][v][0];
-                    dudt[5 + v] = -du / vol;
-                }
+                for (int v = 0; v < 3; ++v) dudt[5 + v] = dudt_b[v];
             }
             // ---- geometric source, flux.cpp:395-444
             if (!ph.cart_minkowski) {
@@ -697,7 +712,10 @@ __global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
     if (!any) return;
     const long long s = ((long long)kk*d.n2 + jj)*d.n1 + ii;
 #pragma unroll
-    for (int p = 0; p < NV; ++p) { P.v[p][t] = P.v[p][s]; U.v[p][t] = U.v[p][s]; }
+    for (int p = 0; p < NV; ++p) {
+        if (NV > 8 && !P.v[p]) continue;       // EMHD slots that are not evolved
+        P.v[p][t] = P.v[p][s]; U.v[p][t] = U.v[p][s];
+    }
 }
 
 // The ghost shell (every zone outside the interior) of a stage's input copied to its output: the
@@ -1176,7 +1194,8 @@ void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const kh
     const long long nint = (long long)(d.ie - d.is + 1)*(d.je - d.js + 1)*(d.ke - d.ks + 1);
     const long long tot = d.N - nint;
     if (tot == 0) return;
-    if (nv == 8) k_periodic<8><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
+    if (nv == 10) k_periodic<10><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
+    else if (nv == 8) k_periodic<8><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
     else k_periodic<5><<<blocks_for(tot, 256), 256, 0, st>>>(d, P, U, pmask);
 }
 

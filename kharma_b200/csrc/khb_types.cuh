@@ -188,6 +188,16 @@ struct ImpFields {
 enum { IMP_MAX_ITER = 64, IMP_ITER_WORD = 64, IMP_WORDS = 65 };
 
 struct LaunchEmhd {
+    // explicit EMHD step: face fluxes of the 10-slot state ([10][N] per direction), dU/dt with the
+    // EMHD geometric source (and the zone timestep minimum when dtm), the ImEx explicit update
+    static void flux(int recon, int dir, const Dims& d, const DevGeom& g, const Phys& ph, const EmhdArgs& E,
+                     const khb_fields& P, double* F, double* ctop, const int lo[3], const int cnt[3], cudaStream_t st);
+    static void dudt(const Dims& d, const DevGeom& g, const Phys& ph, const EmhdArgs& E, double* const F[3],
+                     double* const ctop[3], const khb_fields& Ps, const khb_fields& dUdt, int dtm,
+                     unsigned long long* word, cudaStream_t st);
+    static void imex_explicit(const Dims& d, const DevGeom& g, const khb_fields& Psub, const khb_fields& Usub,
+                              const khb_fields& Ufull, const khb_fields& dUdt, const khb_fields& Pout,
+                              const khb_fields& Uout, double g0, double g1, double bdt, cudaStream_t st);
     static void ptou(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,
                      const khb_fields& U, cudaStream_t st);
     static void add_source(const Dims& d, const DevGeom& g, const double* conn, double gam, const EmhdArgs& E,

@@ -5,6 +5,8 @@ Mirrors the calls the reference's EMHD and Implicit packages make per stage:
   * Implicit::Step (implicit/implicit.cpp:159-571)     -> ImplicitSolver.step
   * Implicit::FixSolve (implicit/fix_solve.cpp:44-130)  -> ImplicitSolver.fix_solve
   * Flux::MeshPtoU with EMHD + EMHD::BlockPtoU         -> ImplicitSolver.ptou
+  * Flux::GetFlux with the EMHD variables               -> ImplicitSolver.get_flux
+  * one ImEx stage / vl2 step (driver/imex_step.cpp)    -> ImplicitSolver.imex_stage / imex_step
 
 State tensors are (10, n3, n2, n1) float64 CUDA tensors with slots rho, u, u1-u3, B1-B3, q~, dP~
 (conserved: rho u^t, T^t_t + rho u^t, T^t_i, B^i gdet, q~ u^t gdet, dP~ u^t gdet); solve_norm and
@@ -98,6 +100,33 @@ class ImplicitSolver:
                                                   C.c_void_p(J.data_ptr()), C.c_void_p(r.data_ptr()),
                                                   self.block.stream), "khb_implicit_jacobian")
         return J, r
+
+    def get_flux(self, dir, P):
+        """EMHD face fluxes along dir: (F (10, ...), ctop) as new device tensors."""
+        _lib.check(self.lib.khb_get_flux_emhd(self.block.ctx, C.byref(self._e), dir, Fields(P).ref,
+                                              self.block.stream), "khb_get_flux_emhd")
+        F = self.zeros()
+        ctop = self.scalar_field()
+        _lib.check(self.lib.khb_copy_flux_emhd(self.block.ctx, dir, Fields(F).ref, C.c_void_p(ctop.data_ptr()),
+                                               self.block.stream), "khb_copy_flux_emhd")
+        return F, ctop
+
+    def imex_stage(self, stage, dt, P_full, U_full, P_sub, U_sub, P_out, U_out, solve_norm, solve_fail):
+        """One ImEx stage (vl2): fluxes, sources, explicit B update, Newton solve, FixSolve, P -> U."""
+        _lib.check(self.lib.khb_imex_stage(self.block.ctx, C.byref(self._e), C.byref(self._i), stage, float(dt),
+                                           Fields(P_full).ref, Fields(U_full).ref, Fields(P_sub).ref,
+                                           Fields(U_sub).ref, Fields(P_out).ref, Fields(U_out).ref,
+                                           C.c_void_p(solve_norm.data_ptr()), C.c_void_p(solve_fail.data_ptr()),
+                                           self.block.stream), "khb_imex_stage")
+
+    def imex_step(self, P, U, dt, solve_norm, solve_fail):
+        """One vl2 ImEx step in place on (P, U) through an intermediate state."""
+        P1, U1 = self.zeros(), self.zeros()
+        P2, U2 = self.zeros(), self.zeros()
+        self.imex_stage(1, dt, P, U, P, U, P1, U1, solve_norm, solve_fail)
+        self.imex_stage(2, dt, P, U, P1, U1, P2, U2, solve_norm, solve_fail)
+        P.copy_(P2)
+        U.copy_(U2)
 
     def fix_solve(self, P, U, solve_fail):
         _lib.check(self.lib.khb_fix_solve(self.block.ctx, C.byref(self._e), Fields(P).ref, Fields(U).ref,

@@ -2301,6 +2301,221 @@ static void emhd_add_source(const Block& B, const EmhdParams& ep, double gam, co
     }
 }
 
+// ---------------------------------------------------------------- EMHD explicit path and ImEx stage
+// The explicit part of the EMHD step: Flux::GetFlux with the EMHD variables present (get_flux.hpp
+// with prim_to_flux at the faces, flux_functions.hpp:180-232, and vchar's EMHD signal speeds,
+// :368-439), flux-CT, the divergence of every variable, Flux::AddGeoSource with the EMHD stress
+// tensor (flux.cpp:395-444 through Flux::calc_tensor, :80-107) and EMHD::AddSource; then the ImEx
+// stage of imex_step.cpp:58-356 with the vl2 integrator the implicit package forces
+// (implicit.cpp:96): explicit update of B only, B_P = B_U/gdet, the implicit guess copied from the
+// sub-step state, Implicit::Step with beta dt, FixSolve, ghost zones, P -> U.
+static const double VL2_GAM0[2] = {0.0, 0.0}, VL2_GAM1[2] = {1.0, 1.0}, VL2_BETA[2] = {0.5, 1.0};
+
+static inline FV<double> to_fv(const FourVectors& D)
+{
+    FV<double> F;
+    for (int mu = 0; mu < 4; ++mu) { F.ucon[mu] = D.ucon[mu]; F.ucov[mu] = D.ucov[mu]; F.bcon[mu] = D.bcon[mu]; F.bcov[mu] = D.bcov[mu]; }
+    return F;
+}
+static inline bool emhd_active(const EmhdParams& ep, int p) { return p < 8 || (p == IQ && ep.conduction) || (p == IDP && ep.viscosity); }
+
+// Flux::prim_to_flux at a face location for the 10-slot state
+static void emhd_prim_to_flux_loc(const Block& B, const EmhdParams& ep, const double* P, const FourVectors& Dv,
+                                  int j, int i, int loc, int dir, double* flux)
+{
+    const double gam = B.c.gam, gdet = B.Gdet(loc, j, i);
+    const FV<double> D = to_fv(Dv);
+    flux[0] = P[0] * D.ucon[dir] * gdet;
+    double Tm[4];
+    calc_tensor_t(ep, gam, P, D, dir, Tm);
+    flux[1] = Tm[0] * gdet + flux[0];
+    flux[2] = Tm[1] * gdet;
+    flux[3] = Tm[2] * gdet;
+    flux[4] = Tm[3] * gdet;
+    if (dir == 0) {
+        for (int v = 0; v < 3; ++v) flux[5 + v] = P[5 + v] * gdet;
+    } else {
+        for (int v = 0; v < 3; ++v) flux[5 + v] = (D.bcon[v+1] * D.ucon[dir] - D.bcon[dir] * D.ucon[v+1]) * gdet;
+    }
+    flux[IQ] = ep.conduction ? P[IQ] * D.ucon[dir] * gdet : 0.;
+    flux[IDP] = ep.viscosity ? P[IDP] * D.ucon[dir] * gdet : 0.;
+}
+// vchar with the EMHD-augmented sound speed (flux_functions.hpp:380-403)
+static void emhd_vchar(const Block& B, const EmhdParams& ep, const double* P, const FourVectors& D, int j, int i,
+                       int loc, int dir, double& cmax, double& cmin)
+{
+    const double gam = B.c.gam;
+    const double ef  = P[0] + gam * P[1];
+    const double cs2 = gam * (gam - 1) * P[1] / ef;
+    const double bsq = dot4(D.bcon, D.bcov);
+    const double va2 = bsq / (bsq + ef);
+    const double ccond2 = ep.conduction ? (gam - 1.) * ep.conduction_alpha * cs2 : 0.0;
+    const double cvis2 = ep.viscosity ? (4./3.) / (P[0] + (gam * P[1])) * P[0] * ep.viscosity_alpha * cs2 : 0.0;
+    const double cs2_emhd = 0.5*(cs2 + ccond2 + std::sqrt(cs2*cs2 + ccond2*ccond2)) + cvis2;
+    const double cms2 = cs2_emhd + va2 - cs2_emhd*va2;
+    double Bcov[4] = {1., 0., 0., 0.};
+    double Acov[4] = {0., 0., 0., 0.}; Acov[dir] = 1.;
+    double Acon[4], Bcon[4];
+    B.raise(Acov, Acon, j, i, loc);
+    B.raise(Bcov, Bcon, j, i, loc);
+    const double Asq = dot4(Acon, Acov);
+    const double Bsq = dot4(Bcon, Bcov);
+    const double Au  = dot4(Acov, D.ucon);
+    const double Bu  = dot4(Bcov, D.ucon);
+    const double AB  = dot4(Acon, Bcov);
+    const double A  = Bu*Bu - (Bsq + Bu*Bu) * cms2;
+    const double Bq = 2. * (Au*Bu - (AB + Au*Bu) * cms2);
+    const double Cq = Au*Au - (Asq + Au*Au) * cms2;
+    const double discr = std::sqrt(kmax(Bq * Bq - 4. * A * Cq, 0.));
+    const double vp = -(-Bq + discr) / (2. * A);
+    const double vm = -(-Bq - discr) / (2. * A);
+    cmax = kmax(vp, vm);
+    cmin = kmin(vp, vm);
+}
+// Face fluxes of the 10-slot state along dir (same face ranges and cmin sign as get_flux)
+static void get_flux_emhd(const Block& B, const EmhdParams& ep, int dir, const double* P, double* F,
+                          double* cmaxo, double* cmino)
+{
+    const int loc = dir - 1;
+    const int d1 = (dir == 1), d2 = (dir == 2), d3 = (dir == 3);
+    const int i0 = B.is - (!d1 ? 1 : 0), i1 = B.ie + 1;
+    const int j0 = (B.ndim >= 2) ? B.js - (d2 ? 0 : 1) : B.js, j1 = (B.ndim >= 2) ? B.je + 1 : B.je;
+    const int k0 = (B.ndim >= 3) ? B.ks - (d3 ? 0 : 1) : B.ks, k1 = (B.ndim >= 3) ? B.ke + 1 : B.ke;
+    const ptrdiff_t st = d1 + (d2 ? B.n1 : 0) + (d3 ? (ptrdiff_t)B.n1*B.n2 : 0);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = k0; k <= k1; ++k) for (int j = j0; j <= j1; ++j) for (int i = i0; i <= i1; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pl[NVE] = {0.}, Pr[NVE] = {0.};
+        for (int p = 0; p < NVE; ++p) {
+            if (!emhd_active(ep, p)) continue;
+            const double* q = P + (size_t)p*B.N;
+            double l, r;
+            recon_zone(B.c.recon, q[c - 3*st], q[c - 2*st], q[c - st], q[c], q[c + st], l, r);
+            Pl[p] = r;
+            recon_zone(B.c.recon, q[c - 2*st], q[c - st], q[c], q[c + st], q[c + 2*st], l, r);
+            Pr[p] = l;
+        }
+        FourVectors Dl, Dr;
+        double Ul[NVE], Fl[NVE], Ur[NVE], Fr[NVE], cmaxL, cminL, cmaxR, cminR;
+        calc_4vecs(B, Pl, true, j, i, loc, Dl);
+        emhd_prim_to_flux_loc(B, ep, Pl, Dl, j, i, loc, 0, Ul);
+        emhd_prim_to_flux_loc(B, ep, Pl, Dl, j, i, loc, dir, Fl);
+        emhd_vchar(B, ep, Pl, Dl, j, i, loc, dir, cmaxL, cminL);
+        calc_4vecs(B, Pr, true, j, i, loc, Dr);
+        emhd_prim_to_flux_loc(B, ep, Pr, Dr, j, i, loc, 0, Ur);
+        emhd_prim_to_flux_loc(B, ep, Pr, Dr, j, i, loc, dir, Fr);
+        emhd_vchar(B, ep, Pr, Dr, j, i, loc, dir, cmaxR, cminR);
+        const double cmax = kmax(kmax(0., cmaxL), cmaxR);
+        const double cmin = -kmin(kmin(0., cminL), cminR);
+        cmaxo[c] = cmax; cmino[c] = cmin;
+        for (int p = 0; p < NVE; ++p)
+            F[(size_t)p*B.N + c] = !emhd_active(ep, p) ? 0.
+                                 : (B.c.riemann ? hlle(Fl[p], Fr[p], cmax, cmin, Ul[p], Ur[p])
+                                                : llf(Fl[p], Fr[p], cmax, cmin, Ul[p], Ur[p]));
+    }
+}
+// FluxDivergence of every active variable, then AddGeoSource with the EMHD tensor and EMHD::AddSource
+static void emhd_dudt(const Block& B, const EmhdParams& ep, double* F[3], const double* P, double* dudt)
+{
+    const size_t N = B.N;
+    const double a1 = B.c.dx2*B.c.dx3, a2 = B.c.dx1*B.c.dx3, a3 = B.c.dx1*B.c.dx2;
+    const double vol = B.c.dx1*B.c.dx2*B.c.dx3;
+    const size_t sj = B.n1, sk = (size_t)B.n1*B.n2;
+    const double gam = B.c.gam;
+    std::fill(dudt, dudt + (size_t)NVE*N, 0.);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        for (int p = 0; p < NVE; ++p) {
+            if (!emhd_active(ep, p)) continue;
+            const size_t pc = (size_t)p*N + c;
+            double du = (a1 * F[0][pc + 1] - a1 * F[0][pc]);
+            if (B.ndim >= 2) du += a2 * F[1][pc + sj] - a2 * F[1][pc];
+            if (B.ndim == 3) du += a3 * F[2][pc + sk] - a3 * F[2][pc];
+            dudt[pc] = -du / vol;
+        }
+        if (!B.C.cart_minkowski()) {
+            double Pc[NVE];
+            load10(P, N, c, Pc);
+            FourVectors Dv;
+            calc_4vecs(B, Pc, true, j, i, center, Dv);
+            const FV<double> D = to_fv(Dv);
+            double Tmu[4] = {0}, new_du[4] = {0};
+            for (int mu = 0; mu < 4; ++mu) {
+                calc_tensor_t(ep, gam, Pc, D, mu, Tmu);
+                for (int nu = 0; nu < 4; ++nu)
+                    for (int lam = 0; lam < 4; ++lam)
+                        new_du[lam] += Tmu[nu] * B.GdetConn(j, i, nu, lam, mu);
+            }
+            dudt[1*N + c] += new_du[0];
+            for (int v = 0; v < 3; ++v) dudt[(size_t)(2 + v)*N + c] += new_du[1 + v];
+        }
+    }
+    emhd_add_source(B, ep, gam, P, dudt);
+}
+// Minimum zone timestep from the signal speeds (grmhd.cpp:294-339)
+static double min_ndt_from(const Block& B, const std::vector<double> cmax[3], const std::vector<double> cmin[3])
+{
+    double m = std::numeric_limits<double>::max();
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        const double ndt_zone = 1.0 / (1 / (B.c.dx1 / kmax(cmax[0][c], cmin[0][c])) +
+                                       1 / (B.c.dx2 / kmax(cmax[1][c], cmin[1][c])) +
+                                       1 / (B.c.dx3 * 1 / kmax(cmax[2][c], cmin[2][c])));
+        if (!std::isnan(ndt_zone) && (ndt_zone < m)) m = ndt_zone;
+    }
+    return m;
+}
+// One ImEx stage (s = 0, 1).  All arrays [10][N]; ghost zones of Pout/Uout start as copies of the
+// sub-step state (the guess copy) and periodic faces are refreshed; other faces must be exchange
+// faces (the caller's).  Returns the Newton iterations; *min_ndt from this stage's fluxes.
+static int imex_stage(const Block& B, const EmhdParams& ep, const ImplicitParams& ip, int s, double dt,
+                      const double* Pfull, const double* Ufull, const double* Psub, const double* Usub,
+                      double* Pout, double* Uout, double* solve_norm, double* solve_fail, double* min_ndt_out)
+{
+    const size_t N = B.N, NA = (size_t)NVE*N;
+    const double gam = B.c.gam;
+    std::vector<double> Fv[3], cmx[3], cmn[3];
+    double* F[3];
+    for (int d = 0; d < 3; ++d) {
+        Fv[d].assign(NA, 0.); cmx[d].assign(N, 0.); cmn[d].assign(N, 0.);
+        F[d] = Fv[d].data();
+    }
+    for (int d = 1; d <= B.ndim; ++d) get_flux_emhd(B, ep, d, Psub, F[d-1], cmx[d-1].data(), cmn[d-1].data());
+    if (B.c.fix_polar_flux && B.C.spherical()) {
+        if (phys_face(B.c.bc[2])) zero_boundary_flux_x2(B, F[0], F[1], F[2], true);
+        if (phys_face(B.c.bc[3])) zero_boundary_flux_x2(B, F[0], F[1], F[2], false);
+    }
+    flux_ct(B, F[0], F[1], F[2]);
+    std::vector<double> dudt(NA, 0.);
+    emhd_dudt(B, ep, F, Psub, dudt.data());
+    // solver state: the sub-step state everywhere; explicit update of B over the interior
+    std::vector<double> Psol(Psub, Psub + NA), Usol(Usub, Usub + NA);
+    const double g0 = VL2_GAM0[s], g1 = VL2_GAM1[s], bdt = VL2_BETA[s] * dt;
+    for (int v = 5; v < 8; ++v)
+        for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+            const size_t x = (size_t)v*N + B.id(k, j, i);
+            Usol[x] = g0 * Usub[x] + g1 * Ufull[x];
+            Usol[x] = 1.0 * Usol[x] + bdt * dudt[x];
+        }
+    // B_FluxCT::BlockUtoP over the entire block (b_flux_ct.cpp:172-217)
+    for (int v = 5; v < 8; ++v)
+        for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+            const size_t c = B.id(k, j, i);
+            Psol[(size_t)v*N + c] = Usol[(size_t)v*N + c] / B.Gdet(center, j, i);
+        }
+    const int iters = implicit_step(B, ep, ip, gam, Pfull, Ufull, Psub, dudt.data(), Psol.data(), solve_norm,
+                                    solve_fail, bdt, nullptr);
+    std::memcpy(Pout, Psol.data(), NA*sizeof(double));
+    std::memcpy(Uout, Usol.data(), NA*sizeof(double));
+    fix_solve(B, ep, gam, Pout, Uout, solve_fail);
+    for (int d = 1; d <= B.ndim; ++d)
+        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, Pout, NVE, d); periodic_fill(B, Uout, NVE, d); }
+    emhd_ptou(B, ep, gam, Pout, Uout);
+    if (min_ndt_out) *min_ndt_out = min_ndt_from(B, cmx, cmn);
+    return iters;
+}
+
 struct Handle {
     Block B;
     Fields f;
@@ -2430,6 +2645,19 @@ int orc_utop_cell(void* hp, int j, int i, const double* U, double* P)
 {
     const Block& B = ((Handle*)hp)->B;
     return u_to_p(B, U, P, j, i, center, B.c.iter_max, B.c.err_tol);
+}
+
+// ---- EMHD explicit fluxes and the ImEx stage
+void orc_get_flux_emhd(void* hp, const EmhdParams* ep, int dir, const double* P, double* F, double* cmax, double* cmin)
+{
+    get_flux_emhd(((Handle*)hp)->B, *ep, dir, P, F, cmax, cmin);
+}
+int orc_imex_stage(void* hp, const EmhdParams* ep, const ImplicitParams* ip, int stage, double dt,
+                   const double* Pfull, const double* Ufull, const double* Psub, const double* Usub,
+                   double* Pout, double* Uout, double* solve_norm, double* solve_fail, double* min_ndt)
+{
+    return imex_stage(((Handle*)hp)->B, *ep, *ip, stage - 1, dt, Pfull, Ufull, Psub, Usub, Pout, Uout,
+                      solve_norm, solve_fail, min_ndt);
 }
 
 // ---- EMHD and the implicit solve.  All field arrays are [10][N] (slots rho..B3, q, dP).

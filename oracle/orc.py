@@ -96,6 +96,9 @@ def load():
     lib.orc_implicit_step.restype = C.c_int
     lib.orc_implicit_step.argtypes = [P, P, P, P, P, P, P, P, P, P, C.c_double, P]
     lib.orc_fix_solve.argtypes = [P, P, P, P, P]
+    lib.orc_get_flux_emhd.argtypes = [P, P, C.c_int, P, P, P, P]
+    lib.orc_imex_stage.restype = C.c_int
+    lib.orc_imex_stage.argtypes = [P, P, P, C.c_int, C.c_double, P, P, P, P, P, P, P, P, P]
     _lib = lib
     return lib
 
@@ -273,6 +276,23 @@ class Oracle:
 
     def fix_solve(self, emhd, P, U, solve_fail):
         self.lib.orc_fix_solve(self.h, C.byref(emhd_params(emhd)), _ptr(P), _ptr(U), _ptr(solve_fail))
+
+    def get_flux_emhd(self, emhd, dir, P):
+        """EMHD face fluxes of the 10-slot state along dir: (F [10, ...], cmax, cmin)."""
+        F = self.zeros10()
+        cmax = np.zeros(self.shape)
+        cmin = np.zeros(self.shape)
+        self.lib.orc_get_flux_emhd(self.h, C.byref(emhd_params(emhd)), dir, _ptr(P), _ptr(F), _ptr(cmax), _ptr(cmin))
+        return F, cmax, cmin
+
+    def imex_stage(self, emhd, imp, stage, dt, Pfull, Ufull, Psub, Usub, solve_norm, solve_fail):
+        """One ImEx stage (vl2 weights); returns (Pout, Uout, newton iterations, min zone dt)."""
+        Pout, Uout = self.zeros10(), self.zeros10()
+        mn = C.c_double()
+        it = self.lib.orc_imex_stage(self.h, C.byref(emhd_params(emhd)), C.byref(implicit_params(imp)), stage, dt,
+                                     _ptr(Pfull), _ptr(Ufull), _ptr(Psub), _ptr(Usub), _ptr(Pout), _ptr(Uout),
+                                     _ptr(solve_norm), _ptr(solve_fail), C.byref(mn))
+        return Pout, Uout, it, mn.value
 
 
 class EmhdParams(C.Structure):

@@ -157,3 +157,31 @@ def test_backtracking_failure_and_fix_solve(oracle_mod):
     Uref = o.emhd_ptou(emhd, Pfix)
     for z in bad:
         assert np.array_equal(Ufix[(slice(None),) + z], Uref[(slice(None),) + z])
+
+
+def test_imex_keeps_conducting_atmosphere_in_equilibrium(oracle_mod):
+    """The reference's conducting atmosphere (tests/conducting_atmosphere) is a steady state of the
+    EMHD equations: its ODE profile (heat flux phi included) balances the explicit fluxes, the
+    geometric source with the EMHD stress tensor, and the implicit q relaxation.  Ten vl2 ImEx steps
+    of the oracle (imex_step.cpp:58-356) must leave rho, u and q~ within 1e-4 of the profile."""
+    import dataclasses
+    from emhd_cases import EMHD_VARIANTS, implicit, profile
+    from kharma_b200 import problems
+    from kharma_b200.block import build_geometry
+    from kharma_b200.spec import atmosphere_spec
+    n1 = 64
+    spec = dataclasses.replace(atmosphere_spec(n1, 8, 1), bc=("exchange",) * 4 + ("periodic",) * 2)
+    emhd = EMHD_VARIANTS["kappa_eta_ho"]
+    P = problems.conducting_atmosphere(spec, build_geometry(spec), emhd, profile(n1), jitter=0.0)
+    o = oracle_mod.Oracle(spec)
+    U = o.emhd_ptou(emhd, P)
+    imp = implicit("fd", max_nonlinear_iter=3, rootfind_tol=1e-12)
+    sn, sf = np.zeros(spec.shape), np.zeros(spec.shape)
+    P0 = P.copy()
+    for _ in range(10):
+        P1, U1, _, _ = o.imex_stage(emhd, imp, 1, 0.5, P, U, P, U, sn, sf)
+        P, U, _, _ = o.imex_stage(emhd, imp, 2, 0.5, P, U, P1, U1, sn, sf)
+    sl = spec.interior
+    assert not (sf[sl] == 1).any()
+    for v in (0, 1, 8):
+        assert np.max(np.abs(P[v][sl] - P0[v][sl])) / np.max(np.abs(P0[v][sl])) < 1e-4, v
