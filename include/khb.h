@@ -93,6 +93,10 @@ typedef struct {
     int32_t fix_average_neighbors, fix_atmosphere;
     khb_floors floors;                /* floors; also the inverter floors of the Kastaun scheme */
     int32_t inverter;                 /* KHB_INVERTER_* */
+    /* first-order flux correction (fofc/on, fofc/polar_cells, fofc/eh_buffer; flux.cpp:175-221) and
+     * the event-horizon radius of the coordinates (0 without one, coordinate_embedding.hpp:247-258) */
+    int32_t fofc, fofc_polar_cells;
+    double fofc_eh_buffer, r_horizon;
 } khb_config;
 
 /* Coordinate system for khb_build_geometry (coordinates/coordinate_systems.hpp) */
@@ -160,6 +164,16 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
  * :368-439) and the LLF/HLLE flux into the context's flux scratch for that direction.  Faces
  * cover [s, e+1] along dir and [s-1, e+1] across it. */
 int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream);
+
+/* First-order flux correction of one stage (KHARMADriver::AddFOFC, kharma_driver.cpp:292-337;
+ * Flux::MarkFOFC and Flux::FOFC, fofc.cpp:45-226), between khb_get_flux and khb_fix_flux: a guess of
+ * the stage's conserved state from the raw face fluxes (interior plus the zones whose flags the
+ * corrected faces read), its inversion (started from P_s) and floor test; zones that would hit
+ * floors, lie within fofc_eh_buffer of the horizon or in the polar rows are flagged (periodic ghost
+ * zones take their images' flags); every face bordering a flagged zone gets the donor-cell LLF flux
+ * of all variables and its signal speed.  khb_stage and khb_step call it when cfg.fofc is set. */
+int khb_fofc(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+             const khb_fields* U_0, void* stream);
 
 /* B_FluxCT::FixFlux polar corrections (b_flux_ct.cpp:264-303, 372-470) and
  * KBoundaries::FixFlux (boundaries.cpp:611-690) applied to the raw face fluxes in scratch. */

@@ -58,6 +58,8 @@ class KhbConfig(C.Structure):
         ("fix_average_neighbors", C.c_int32), ("fix_atmosphere", C.c_int32),
         ("floors", KhbFloors),
         ("inverter", C.c_int32),
+        ("fofc", C.c_int32), ("fofc_polar_cells", C.c_int32),
+        ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
     ]
 
 
@@ -100,6 +102,7 @@ SIGNATURES = {
     "khb_set_geometry": (_I, [_P, _P, _P, _P, _P, _P]),
     "khb_get_flux": (_I, [_P, _I, C.POINTER(KhbFields), _P]),
     "khb_fix_flux": (_I, [_P, _P]),
+    "khb_fofc": (_I, [_P, _I, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
     "khb_flux_ct": (_I, [_P, _P]),
     "khb_copy_flux": (_I, [_P, _I, C.POINTER(KhbFields), _P, _P]),
     "khb_update": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _D, _D, _D,

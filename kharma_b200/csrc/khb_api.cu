@@ -92,6 +92,27 @@ int launch_fix_flux_t(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
     return KHB_OK;
 }
 
+// First-order flux correction of a stage (stage weights from the rk2 tables)
+template <typename FT>
+void launch_fofc_t(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+                   const khb_fields& U0, cudaStream_t st)
+{
+    const int s = stage - 1;
+    FT* F[3] = {(FT*)ctx->F[0], (FT*)ctx->F[1], (FT*)ctx->F[2]};
+    FT* ct[3] = {(FT*)ctx->ctop[0], (FT*)ctx->ctop[1], (FT*)ctx->ctop[2]};
+    Launch<FT>::fofc(ctx->nv, ctx->d, ctx->g, ctx->ph, Ps, Us, U0, F, ct, kRkGam0[s], kRkGam1[s], kRkBeta[s] * dt,
+                     ctx->fofc_flag, st);
+}
+int launch_fofc(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+                const khb_fields& U0, cudaStream_t st)
+{
+    if (!ctx->ph.fofc) return KHB_OK;
+    if (ctx->fp32) launch_fofc_t<float>(ctx, stage, dt, Ps, Us, U0, st);
+    else launch_fofc_t<double>(ctx, stage, dt, Ps, Us, U0, st);
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
 int launch_fix_flux(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
 {
     return ctx->fp32 ? launch_fix_flux_t<float>(ctx, ph, st) : launch_fix_flux_t<double>(ctx, ph, st);
@@ -242,6 +263,7 @@ int do_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb
     int rc;
     for (int dir = 1; dir <= ctx->d.ndim; ++dir)
         if ((rc = launch_flux(ctx, dir, Ps, st))) return rc;
+    if ((rc = launch_fofc(ctx, stage, dt, Ps, Us, U0, st))) return rc;
     if ((rc = launch_fix_flux(ctx, ctx->ph, st))) return rc;
     if ((rc = launch_ghost_copy(ctx, Ps, Us, Pout, Uout, st))) return rc;
     if ((rc = zone_pass(ctx, stage, dt, Ps, Us, U0, Pout, Uout, pflag, fflag, st))) return rc;
@@ -316,6 +338,10 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
         return KHB_ERR_UNSUPPORTED;
     }
     ph.inverter = cfg->inverter;
+    ph.fofc = cfg->fofc;
+    ph.fofc_polar_cells = cfg->fofc_polar_cells;
+    ph.fofc_r_mark = cfg->r_horizon + cfg->fofc_eh_buffer;
+    if (cfg->fofc && cfg->fofc_polar_cells < 0) { *why = "fofc_polar_cells must be >= 0"; return KHB_ERR_ARG; }
     std::memcpy(&ph.fl, &cfg->floors, sizeof(khb_floors));
     return KHB_OK;
 }
@@ -363,6 +389,7 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     if (e == cudaSuccess) e = alloc((void**)&c->fail_count, sizeof(int) * 4);
     if (e == cudaSuccess) e = alloc((void**)&c->fail_list, sizeof(int) * N);
     if (e == cudaSuccess) e = alloc((void**)&c->imp_words, sizeof(unsigned long long) * IMP_WORDS);
+    if (e == cudaSuccess && cfg->fofc) e = alloc((void**)&c->fofc_flag, sizeof(int32_t) * N);
     // the memsets above run on the legacy default stream, which the caller's (non-blocking) streams
     // do not wait for: finish them before the context is handed out
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -384,6 +411,7 @@ int khb_destroy(khb_ctx* c)
     cudaFree(c->conn_d); cudaFree(c->emhd_tmp); cudaFree(c->fix_buf); cudaFree(c->imp_words);
     for (int x = 0; x < 3; ++x) cudaFree(c->F10[x]);
     cudaFree(c->dudt10);
+    cudaFree(c->fofc_flag);
     delete c;
     return KHB_OK;
 }
@@ -472,6 +500,18 @@ int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream)
     int rc;
     if ((rc = check_fields(ctx, P, "P"))) return rc;
     return launch_flux(ctx, dir, *P, S(stream));
+}
+
+int khb_fofc(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+             const khb_fields* U_0, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_fofc: stage must be 1 or 2");
+    if (!ctx->ph.fofc) return fail(KHB_ERR_STATE, "khb_fofc: the context was created with fofc off");
+    int rc;
+    if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
+        (rc = check_fields(ctx, U_0, "U_0"))) return rc;
+    return launch_fofc(ctx, stage, dt, *P_s, *U_s, *U_0, S(stream));
 }
 
 int khb_fix_flux(khb_ctx* ctx, void* stream)

@@ -35,6 +35,7 @@ struct khb_ctx {
     unsigned long long* imp_words;   // implicit-solve reductions, IMP_WORDS entries
     double* F10[3];        // EMHD face fluxes, [10][N] per direction
     double* dudt10;        // EMHD dU/dt of an ImEx stage, [10][N]
+    int32_t* fofc_flag;    // first-order flux correction flags, [N] (when fofc is on)
 };
 
 

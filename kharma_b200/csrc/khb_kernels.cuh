@@ -484,6 +484,122 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
     if (a.mode & M_DT) block_min_ndt(ndt_zone, a.ndt_word);
 }
 
+// ===================================================================================== FOFC
+// First-order flux correction (flux/fofc.cpp:45-226, driver/kharma_driver.cpp:292-337), between the
+// flux calculation and the flux fixes.  The guess update of each zone uses the raw face fluxes as
+// they stand (faces outside the flux calculation's range hold zeros or earlier corrections, as in the
+// reference), starts its inversion from P_s, and flags zones that would hit floors or lie within
+// fofc_r_mark of the centre (event horizon plus buffer).
+template <int NV, typename FT, bool KAST>
+__global__ void __launch_bounds__(128) k_fofc_guess(Dims d, DevGeom g, Phys ph, khb_fields Ps, khb_fields Us,
+                                                    khb_fields U0, const FT* F1, const FT* F2, const FT* F3,
+                                                    double g0, double g1, double bdt, int32_t* flag, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long N = d.N, sj = d.sj, sk = d.sk;
+    const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
+    const double vol = ph.dx1*ph.dx2*ph.dx3;
+    ZoneGeom G;
+    load_zone_geom(g, j, i, G);
+    double Ug[NV], Pg[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        double du = (a1 * ldf(F1, p*N + c + 1) - a1 * ldf(F1, p*N + c));
+        if (d.ndim >= 2) du += a2 * ldf(F2, p*N + c + sj) - a2 * ldf(F2, p*N + c);
+        if (d.ndim == 3) du += a3 * ldf(F3, p*N + c + sk) - a3 * ldf(F3, p*N + c);
+        const double dudt = -du / vol;
+        const double x = g0 * Us.v[p][c] + g1 * U0.v[p][c];
+        Ug[p] = 1.0 * x + bdt * dudt;
+        Pg[p] = Ps.v[p][c];
+    }
+    if (NV > 5) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) Pg[5 + v] = Ug[5 + v] / G.gdet;
+    }
+    const int pf = KAST ? u_to_p_kastaun<NV>(G, ph.gam, ph.fl, Ug, Pg, ph.iter_max, ph.err_tol)
+                        : u_to_p_onedw<NV>(G, ph.gam, Ug, Pg, ph.iter_max, ph.err_tol);
+    int ff = (pf / FF_GEOM_RHO) * FF_GEOM_RHO;
+    if (ph.floors_on) {
+        const long long cg = (long long)j*g.n1 + i;
+        double rf, uf;
+        FourVec<double> D;
+        ff |= determine_floors<NV>(G, ph.fl, __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), ph.gam, Pg, rf, uf, D);
+    }
+    const bool eh = ph.spherical && __ldg(g.rcen + (long long)j*g.n1 + i) < ph.fofc_r_mark;
+    flag[c] = (ff != 0 || eh) ? 1 : 0;
+}
+// Rows [j0, j1] of every (k, i) flagged (fofc/polar_cells next to a physical X2 face)
+static __global__ void k_fofc_rows(Dims d, int j0, int j1, int32_t* flag)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long rows = (long long)(j1 - j0 + 1) * d.n1;
+    if (t >= rows * d.n3) return;
+    const int k = (int)(t / rows);
+    const long long r = t - (long long)k * rows;
+    const int j = j0 + (int)(r / d.n1), i = (int)(r % d.n1);
+    flag[((long long)k*d.n2 + j)*d.n1 + i] = 1;
+}
+// Flags of zones outside the interior in periodic directions from their images (the flag's sync)
+static __global__ void k_fofc_periodic(Dims d, int pmask, int32_t* flag)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    int k, j, i;
+    zone_kji(d, t, k, j, i);
+    int ii = i, jj = j, kk = k;
+    bool any = false;
+    if ((pmask & 1) && (i < d.is || i > d.ie)) { ii += (i < d.is) ? d.nx1 : -d.nx1; any = true; }
+    if ((pmask & 2) && (j < d.js || j > d.je)) { jj += (j < d.js) ? d.nx2 : -d.nx2; any = true; }
+    if ((pmask & 4) && (k < d.ks || k > d.ke)) { kk += (k < d.ks) ? d.nx3 : -d.nx3; any = true; }
+    if (!any) return;
+    flag[t] = flag[((long long)kk*d.n2 + jj)*d.n1 + ii];
+}
+// Donor-cell LLF flux (all variables) on each face of the box bordering a flagged zone (fofc.cpp:159-219)
+template <int DIR, int NV, typename R, typename FT>
+__global__ void __launch_bounds__(128) k_fofc_replace(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F,
+                                                      FT* __restrict__ ctop, const int32_t* __restrict__ flag, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long st = (DIR == 1) ? 1 : ((DIR == 2) ? d.sj : d.sk);
+    if (!(flag[c] || flag[c - st])) return;
+    const int loc = DIR - 1;
+    const R gam = (R)ph.gam;
+    const long long gi = (long long)j*g.G1 + i;
+    const auto* tcov = FaceTables<R>::gcov(g, loc);
+    const auto* tcon = FaceTables<R>::gcon(g, loc);
+    R gcov[4][4], gcon0[4];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) gcov[m/4][m%4] = (R)__ldg(tcov + m*g.gs + gi);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) gcon0[m] = (R)__ldg(tcon + m*g.gs + gi);
+    const R gcondd = (R)__ldg(tcon + (DIR*4 + DIR)*g.gs + gi);
+    const R gdet = (R)__ldg(FaceTables<R>::gdet(g, loc) + gi);
+    R Pl[NV], Pr[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) { Pl[p] = (R)P.v[p][c - st]; Pr[p] = (R)P.v[p][c]; }
+    constexpr bool HAS_B = NV > 5;
+    FourVec<R> D;
+    R Ul[NV], Fl[NV], Ur[NV], Fr[NV], cmaxL, cminL, cmaxR, cminR;
+    calc_4vecs<R, HAS_B>(gcov, gcon0[0], gcon0, Pl, D);
+    prim_to_flux<R, NV>(Pl, D, gam, gdet, 0, Ul);
+    prim_to_flux<R, NV>(Pl, D, gam, gdet, DIR, Fl);
+    vchar<R, HAS_B>(Pl, D, gam, gcon0[0], gcon0[DIR], gcondd, DIR, cmaxL, cminL);
+    calc_4vecs<R, HAS_B>(gcov, gcon0[0], gcon0, Pr, D);
+    prim_to_flux<R, NV>(Pr, D, gam, gdet, 0, Ur);
+    prim_to_flux<R, NV>(Pr, D, gam, gdet, DIR, Fr);
+    vchar<R, HAS_B>(Pr, D, gam, gcon0[0], gcon0[DIR], gcondd, DIR, cmaxR, cminR);
+    const R cmax = kmax(kmax(R(0), cmaxL), cmaxR);
+    const R cmin = -kmin(kmin(R(0), cminL), cminR);
+    const R ctp = kmax(cmax, cmin);
+#pragma unroll
+    for (int p = 0; p < NV; ++p) F[p*d.N + c] = (FT)(R(0.5) * (Fl[p] + Fr[p] - ctp * (Ur[p] - Ul[p])));
+    ctop[c] = (FT)ctp;
+}
+
 // ===================================================================================== fixups
 // fixup.cpp:47-156.  Neighbours in periodic directions wrap; across exchanged x3 faces they are
 // read from the ghost planes; in other directions they must be interior.  Failed zones never read each other, so one pass over the list is race-free.
@@ -1077,6 +1193,55 @@ void Launch<FT>::copy_flux(long long N, int nv, const FT* F, const FT* ctop, con
                            cudaStream_t st)
 {
     k_copy_flux<FT><<<blocks_for(N, 256), 256, 0, st>>>(N, nv, F, ctop, out, ctop_out);
+}
+
+template <int NV, typename FT>
+static void fofc_nv(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& Ps, const khb_fields& Us,
+                    const khb_fields& U0, FT* const F[3], FT* const ctop[3], double g0, double g1, double bdt,
+                    int32_t* flag, cudaStream_t st)
+{
+    // flags are read over the interior +-2 (+-0 along periodic directions, filled from the images)
+    const int p1 = d.bc[0] == KHB_BC_PERIODIC, p2 = d.bc[2] == KHB_BC_PERIODIC, p3 = d.bc[4] == KHB_BC_PERIODIC;
+    const int h2 = d.ndim > 1, h3 = d.ndim > 2;
+    const int i0 = d.is - (p1 ? 0 : 2), i1 = d.ie + (p1 ? 0 : 2);
+    const int j0 = d.js - (p2 ? 0 : 2*h2), j1 = d.je + (p2 ? 0 : 2*h2);
+    const int k0 = d.ks - (p3 ? 0 : 2*h3), k1 = d.ke + (p3 ? 0 : 2*h3);
+    cudaMemsetAsync(flag, 0, sizeof(int32_t) * d.N, st);
+    const Box gb = make_box(i0, j0, k0, i1 - i0 + 1, j1 - j0 + 1, k1 - k0 + 1);
+    if (ph.inverter == KHB_INVERTER_KASTAUN)
+        k_fofc_guess<NV, FT, true><<<box_blocks(gb), 128, 0, st>>>(d, g, ph, Ps, Us, U0, F[0], F[1], F[2], g0, g1, bdt, flag, gb);
+    else
+        k_fofc_guess<NV, FT, false><<<box_blocks(gb), 128, 0, st>>>(d, g, ph, Ps, Us, U0, F[0], F[1], F[2], g0, g1, bdt, flag, gb);
+    if (ph.spherical && ph.fofc_polar_cells > 0 && d.ndim > 1) {
+        for (int face = 2; face <= 3; ++face) {
+            if (!phys_face(d.bc[face])) continue;
+            const int ja = (face == 2) ? d.js : d.je - ph.fofc_polar_cells + 1;
+            const int jb = (face == 2) ? d.js + ph.fofc_polar_cells - 1 : d.je;
+            const long long n = (long long)(jb - ja + 1) * d.n1 * d.n3;
+            k_fofc_rows<<<blocks_for(n, 128), 128, 0, st>>>(d, ja, jb, flag);
+        }
+    }
+    const int pmask = (p1 ? 1 : 0) | ((h2 && p2) ? 2 : 0) | ((h3 && p3) ? 4 : 0);
+    if (pmask) k_fofc_periodic<<<blocks_for(d.N, 256), 256, 0, st>>>(d, pmask, flag);
+    // faces over the interior +-1 (one more along the face direction), with a left neighbour in range
+    for (int dir = 1; dir <= d.ndim; ++dir) {
+        const int lo_i = max(d.is - 1, dir == 1 ? 1 : 0), hi_i = min(d.ie + 1 + (dir == 1), d.n1 - 1);
+        const int lo_j = h2 ? max(d.js - 1, dir == 2 ? 1 : 0) : d.js, hi_j = h2 ? min(d.je + 1 + (dir == 2), d.n2 - 1) : d.je;
+        const int lo_k = h3 ? max(d.ks - 1, dir == 3 ? 1 : 0) : d.ks, hi_k = h3 ? min(d.ke + 1 + (dir == 3), d.n3 - 1) : d.ke;
+        const Box fb = make_box(lo_i, lo_j, lo_k, hi_i - lo_i + 1, hi_j - lo_j + 1, hi_k - lo_k + 1);
+        const unsigned nb = box_blocks(fb);
+        if (dir == 1) k_fofc_replace<1, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, Ps, F[0], ctop[0], flag, fb);
+        else if (dir == 2) k_fofc_replace<2, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, Ps, F[1], ctop[1], flag, fb);
+        else k_fofc_replace<3, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, Ps, F[2], ctop[2], flag, fb);
+    }
+}
+template <typename FT>
+void Launch<FT>::fofc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& Ps,
+                      const khb_fields& Us, const khb_fields& U0, FT* const F[3], FT* const ctop[3], double g0,
+                      double g1, double bdt, int32_t* flag, cudaStream_t st)
+{
+    if (nv == 8) fofc_nv<8, FT>(d, g, ph, Ps, Us, U0, F, ctop, g0, g1, bdt, flag, st);
+    else fofc_nv<5, FT>(d, g, ph, Ps, Us, U0, F, ctop, g0, g1, bdt, flag, st);
 }
 
 // Batched flux launch; ntiles == 0 returns the resident CTAs per SM of the kernel

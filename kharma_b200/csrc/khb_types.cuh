@@ -51,6 +51,8 @@ struct Phys {
     double dx1, dx2, dx3;
     int zero_polar_flux, fix_polar_flux, check_inflow_in, check_inflow_out;
     int inverter;                          // KHB_INVERTER_*
+    int fofc, fofc_polar_cells;            // first-order flux correction
+    double fofc_r_mark;                    // r_horizon + fofc/eh_buffer (spherical coordinates)
     Prescription fl;
 };
 
@@ -141,6 +143,11 @@ struct Launch {
     static void flux_ct(const Dims& d, FT* F1, FT* F2, FT* F3, FT* emf, cudaStream_t st);
     static void copy_flux(long long N, int nv, const FT* F, const FT* ctop, const khb_fields& out, double* ctop_out,
                           cudaStream_t st);
+    // First-order flux correction of one stage: guess update from the raw fluxes, inversion and floor
+    // test, flags (polar rows, periodic images), donor-cell LLF on the faces bordering a flagged zone
+    static void fofc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& Ps,
+                     const khb_fields& Us, const khb_fields& U0, FT* const F[3], FT* const ctop[3], double g0,
+                     double g1, double bdt, int32_t* flag, cudaStream_t st);
     // Batched launches over every block of a batch: tiles[t] is the block of tile t; grid = 0 runs
     // one CTA per tile, otherwise grid CTAs loop over the tiles.  Return the CTAs per SM the kernel
     // can keep resident (for sizing a persistent grid) when called with ntiles = 0.

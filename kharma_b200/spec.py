@@ -86,6 +86,10 @@ class BlockSpec:
     err_tol: float = 1e-8
     fix_average_neighbors: bool = True
     fix_atmosphere: bool = True
+    # first-order flux correction (flux.cpp:175-221)
+    fofc: bool = False
+    fofc_polar_cells: int = 0
+    fofc_eh_buffer: float = 0.1
     # driver
     driver: str = "simple"
 
@@ -149,7 +153,16 @@ class BlockSpec:
         c.fix_atmosphere = int(self.fix_atmosphere)
         c.floors = self.floors.to_struct()
         c.inverter = _lib.INVERTER[self.inverter]
+        c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(self.fofc), self.fofc_polar_cells, self.fofc_eh_buffer
+        c.r_horizon = self.r_horizon
         return c
+
+    @property
+    def r_horizon(self):
+        """Event-horizon radius of the coordinates (coordinate_embedding.hpp:247-258)."""
+        if self.base in ("spherical_ks", "spherical_bl"):
+            return 1.0 + math.sqrt(1.0 - self.a * self.a)
+        return 0.0
 
     def khb_coords(self):
         s = _lib.KhbCoords()
@@ -170,7 +183,7 @@ def mhdmodes_spec(n1, n2, n3, recon="weno5", riemann="llf", precision="fp64", dr
 
 
 def torus_spec(n1, n2, n3, r_out=1000.0, a=0.9375, recon="linear_mc", precision="fp64", gam=13.0 / 9.0,
-               driver="kharma", inverter="onedw"):
+               driver="kharma", inverter="onedw", fofc=False):
     """FM torus in funky-MKS coordinates (kharma.cpp:144-316 domain logic; pars/benchmark decks).
 
     x1 spans [x1min, log(r_out)] with x1min chosen to put 5.5 zones inside the horizon, x2 in [0,1],
@@ -198,7 +211,8 @@ def torus_spec(n1, n2, n3, r_out=1000.0, a=0.9375, recon="linear_mc", precision=
                      # atmosphere fixup without neighbour averaging
                      iter_max=25 if inverter == "kastaun" else 8,
                      err_tol=1e-12 if inverter == "kastaun" else 1e-8,
-                     fix_average_neighbors=inverter != "kastaun")
+                     fix_average_neighbors=inverter != "kastaun",
+                     fofc=fofc)
 
 
 def bondi_spec(nx1, nx2, nx3, x1min, x1max, x2min=0.0, x2max=1.0, x3min=0.0, x3max=2 * math.pi,

@@ -96,6 +96,8 @@ struct Config {
     double cfl, dt_min, max_dt_increase;
     Prescription floors;
     int32_t inverter;                               // 0 onedw, 1 kastaun (inverter/type)
+    int32_t fofc, fofc_polar_cells;                 // fofc/on, fofc/polar_cells
+    double fofc_eh_buffer, r_horizon;               // fofc/eh_buffer, coords.get_horizon()
 };
 
 // ---------------------------------------------------------------- coordinates
@@ -1531,6 +1533,105 @@ static void finish_stage(const Block& B, double* P, double* U)
         p_to_u_cell(B, P, U, B.id(k, j, i), j, i);      // Flux::MeshPtoU(entire), flux.cpp:317-322
 }
 
+// ---------------------------------------------------------------- first-order flux correction
+// KHARMADriver::AddFOFC (kharma_driver.cpp:292-337), Flux::MarkFOFC and Flux::FOFC (fofc.cpp:45-226),
+// run between the flux calculation and FixFlux.  A guess of the stage result from the high-order
+// fluxes marks the zones where it would hit floors (or lie within eh_buffer of the horizon, or in
+// the polar rows); every face bordering a marked zone then gets the donor-cell LLF flux.
+//  * the guess divergence covers the interior plus 3 zones (kharma_driver.cpp:306-307) and uses the
+//    flux arrays as they stand: faces the flux calculation does not cover hold zeros or the values a
+//    previous correction left there, as in the reference;
+//  * the guess inversion starts from the stage's primitives (the reference's guess container holds
+//    whatever its previous inversion left, a history this restatement does not keep);
+//  * periodic directions take the flags of their images (the flag's boundary sync).
+static void fofc_correct(const Block& B, Fields& f, int s, double dt, const double* P_s, const double* U_s,
+                         const double* U_0)
+{
+    const size_t N = B.N, nv = B.nv;
+    const double g0 = RK_GAM0[s], g1 = RK_GAM1[s], bdt = RK_BETA[s] * dt;
+    const double a1 = B.c.dx2*B.c.dx3, a2 = B.c.dx1*B.c.dx3, a3 = B.c.dx1*B.c.dx2;
+    const double vol = B.c.dx1*B.c.dx2*B.c.dx3;
+    const size_t sj = B.n1, sk = (size_t)B.n1*B.n2;
+    const int h2 = B.ndim > 1, h3 = B.ndim > 2;
+    // zones whose flags a corrected face reads: interior +-2 (+-0 along periodic directions, whose
+    // ghost flags come from their images)
+    const int per1 = B.c.bc[0] == BC_PERIODIC, per2 = B.c.bc[2] == BC_PERIODIC, per3 = B.c.bc[4] == BC_PERIODIC;
+    const int i0 = B.is - (per1 ? 0 : 2), i1 = B.ie + (per1 ? 0 : 2);
+    const int j0 = B.js - (per2 ? 0 : 2*h2), j1 = B.je + (per2 ? 0 : 2*h2);
+    const int k0 = B.ks - (per3 ? 0 : 2*h3), k1 = B.ke + (per3 ? 0 : 2*h3);
+    std::vector<int> flag(N, 0);
+    const double r_mark = B.c.r_horizon + B.c.fofc_eh_buffer;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = k0; k <= k1; ++k) for (int j = j0; j <= j1; ++j) for (int i = i0; i <= i1; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Ug[8], Pg[8];
+        for (size_t p = 0; p < nv; ++p) {
+            const size_t pc = p*N + c;
+            double du = (a1 * f.F[0][pc + 1] - a1 * f.F[0][pc]);
+            if (B.ndim >= 2) du += a2 * f.F[1][pc + sj] - a2 * f.F[1][pc];
+            if (B.ndim == 3) du += a3 * f.F[2][pc + sk] - a3 * f.F[2][pc];
+            const double dudt = -du / vol;
+            double x = g0 * U_s[pc] + g1 * U_0[pc];
+            Ug[p] = 1.0 * x + bdt * dudt;
+            Pg[p] = P_s[pc];
+        }
+        if (nv > 5) for (int v = 0; v < 3; ++v) Pg[5 + v] = Ug[5 + v] / B.Gdet(center, j, i);
+        const int pf = u_to_p(B, Ug, Pg, j, i, center, B.c.iter_max, B.c.err_tol);
+        int ff = (pf / 32) * 32;
+        if (B.c.floors_on) {
+            double rf, uf;
+            ff |= determine_floors(B, Pg, j, i, rf, uf);
+        }
+        const bool eh = B.C.spherical() && B.rcen[(size_t)j*B.n1 + i] < r_mark;
+        flag[c] = (ff != 0 || eh) ? 1 : 0;
+    }
+    if (B.C.spherical() && B.c.fofc_polar_cells > 0 && B.ndim > 1) {
+        for (int face = 2; face <= 3; ++face) {
+            if (!phys_face(B.c.bc[face])) continue;
+            const int js_ = (face == 2) ? B.js : B.je - B.c.fofc_polar_cells + 1;
+            const int je_ = (face == 2) ? B.js + B.c.fofc_polar_cells - 1 : B.je;
+            for (int k = 0; k < B.n3; ++k) for (int j = js_; j <= je_; ++j) for (int i = 0; i < B.n1; ++i)
+                flag[B.id(k, j, i)] = 1;
+        }
+    }
+    for (int d = 1; d <= B.ndim; ++d) {
+        if (B.c.bc[2*(d-1)] != BC_PERIODIC) continue;
+        std::vector<double> tmp(flag.begin(), flag.end());
+        periodic_fill(B, tmp.data(), 1, d);
+        for (size_t x = 0; x < N; ++x) flag[x] = (int)tmp[x];
+    }
+    // donor-cell LLF fluxes on faces bordering a marked zone, faces over the interior +-1 (fofc.cpp:144-221)
+    for (int dir = 1; dir <= B.ndim; ++dir) {
+        const int loc = dir - 1;
+        const ptrdiff_t st = (dir == 1) ? 1 : ((dir == 2) ? (ptrdiff_t)sj : (ptrdiff_t)sk);
+        const int fi1 = kmin(B.ie + 1 + (dir == 1), B.n1 - 1), fi0 = kmax(B.is - 1, dir == 1 ? 1 : 0);
+        const int fj0 = h2 ? kmax(B.js - 1, dir == 2 ? 1 : 0) : B.js, fj1 = h2 ? kmin(B.je + 1 + (dir == 2), B.n2 - 1) : B.je;
+        const int fk0 = h3 ? kmax(B.ks - 1, dir == 3 ? 1 : 0) : B.ks, fk1 = h3 ? kmin(B.ke + 1 + (dir == 3), B.n3 - 1) : B.ke;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = fk0; k <= fk1; ++k) for (int j = fj0; j <= fj1; ++j) for (int i = fi0; i <= fi1; ++i) {
+            const size_t c = B.id(k, j, i);
+            if (!(flag[c] || flag[c - st])) continue;
+            double Pl[8], Pr[8];
+            for (size_t p = 0; p < nv; ++p) { Pl[p] = P_s[p*N + c - st]; Pr[p] = P_s[p*N + c]; }
+            FourVectors Dl, Dr;
+            double Ul[8], Fl[8], Ur[8], Fr[8], cmaxL, cminL, cmaxR, cminR;
+            calc_4vecs(B, Pl, nv > 5, j, i, loc, Dl);
+            prim_to_flux(B, Pl, Dl, j, i, 0, Ul, loc);
+            prim_to_flux(B, Pl, Dl, j, i, dir, Fl, loc);
+            vchar(B, Pl, Dl, j, i, loc, dir, cmaxL, cminL);
+            calc_4vecs(B, Pr, nv > 5, j, i, loc, Dr);
+            prim_to_flux(B, Pr, Dr, j, i, 0, Ur, loc);
+            prim_to_flux(B, Pr, Dr, j, i, dir, Fr, loc);
+            vchar(B, Pr, Dr, j, i, loc, dir, cmaxR, cminR);
+            const double cmax = kmax(kmax(0., cmaxL), cmaxR);
+            const double cmin = -kmin(kmin(0., cminL), cminR);
+            f.cmax[dir-1][c] = cmax;
+            f.cmin[dir-1][c] = cmin;
+            for (size_t p = 0; p < nv; ++p) f.F[dir-1][p*N + c] = llf(Fl[p], Fr[p], cmax, cmin, Ul[p], Ur[p]);
+        }
+    }
+}
+
 // One stage.  P_s/U_s: stage-start state; U_0: step-start conserved state; outputs P_n/U_n.
 static void stage(const Block& B, Fields& f, int s, double dt,
                   const double* P_s, const double* U_s, const double* U_0,
@@ -1540,6 +1641,8 @@ static void stage(const Block& B, Fields& f, int s, double dt,
     // 1. fluxes (kharma_driver.cpp:203-290)
     for (int d = 1; d <= B.ndim; ++d)
         get_flux(B, d, P_s, f.F[d-1].data(), f.cmax[d-1].data(), f.cmin[d-1].data());
+    // 1b. first-order flux correction (kharma_step.cpp:168-173), before FixFlux
+    if (B.c.fofc) fofc_correct(B, f, s, dt, P_s, U_s, U_0);
     // 2. FixFlux: B_FluxCT then Boundaries (kharma_package.cpp:43-56; the order does not change results)
     double* F[3] = {f.F[0].data(), f.F[1].data(), f.F[2].data()};
     if (B.nv > 5) {

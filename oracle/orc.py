@@ -49,6 +49,8 @@ class Config(C.Structure):
         ("cfl", C.c_double), ("dt_min", C.c_double), ("max_dt_increase", C.c_double),
         ("floors", Prescription),
         ("inverter", C.c_int32),
+        ("fofc", C.c_int32), ("fofc_polar_cells", C.c_int32),
+        ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
     ]
 
 
@@ -133,6 +135,8 @@ def config_from_spec(spec):
     c.fix_atmosphere = int(spec.fix_atmosphere)
     c.cfl, c.dt_min, c.max_dt_increase = spec.cfl, spec.dt_min, spec.max_dt_increase
     c.inverter = 1 if spec.inverter == "kastaun" else 0
+    c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(spec.fofc), spec.fofc_polar_cells, spec.fofc_eh_buffer
+    c.r_horizon = spec.r_horizon
     for name, _ in Prescription._fields_:
         setattr(c.floors, name, type(getattr(c.floors, name))(getattr(spec.floors, name)))
     return c

@@ -120,13 +120,17 @@ FULL = {
     "torus2d_mc_128": lambda: torus_spec(128, 128, 1),
     # the reference's default inverter (inverter/type = kastaun, inverter.cpp:54)
     "torus3d_mc_kastaun": lambda: torus_spec(32, 24, 8, inverter="kastaun"),
+    # first-order flux correction on (the production SANE deck's setting, pars/tori_3d/sane.par:80-81)
+    "torus3d_mc_fofc": lambda: torus_spec(32, 24, 8, fofc=True),
+    "torus3d_mc_128_fofc": lambda: torus_spec(128, 128, 128, fofc=True),
 }
 CASES.update(FULL)
 
 
 @pytest.mark.parametrize("name,nsteps", [("mhdmodes3d_weno5", 10), ("mhdmodes2d_ppm_hlle", 10), ("torus3d_mc", 5),
                                          ("mhdmodes3d_weno5_64", 10), ("torus3d_mc_128", 3),
-                                         ("torus2d_mc_128", 10), ("torus3d_mc_kastaun", 10)])
+                                         ("torus2d_mc_128", 10), ("torus3d_mc_kastaun", 10),
+                                         ("torus3d_mc_fofc", 10), ("torus3d_mc_128_fofc", 3)])
 def test_step_parity(oracle_mod, name, nsteps):
     spec = CASES[name]()
     o, b, Po, Uo = make_pair(oracle_mod, spec, initial(oracle_mod, name, spec))
