@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-kernel-times", action="store_true")
     ap.add_argument("--no-emhd", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32_flux"],
+                    help="arithmetic of the timed step (the FP32-flux form is also measured beside FP64 by default)")
     ap.add_argument("--slab-path", action="store_true",
                     help="at N = 1, step the block through the x3-slab path (one slab, local exchange)")
     ap.add_argument("--emhd-only", action="store_true",
@@ -368,8 +370,15 @@ def gpu_arm(args, rank, world, local_rank):
         sl.set_prims([sb], ex, [Ploc], local=local)
         return sb.block, sl.SlabDriver([sb], ex, local=local)
 
-    def run(precision, steps, warmup, sampler=None):
+    def run(precision, steps, warmup, sampler=None, graph=None):
+        """Time `steps` RK2 steps.  graph (N = 1): the step replayed from a CUDA graph with the
+        timestep kept on the device (khb_step_graph), else the host-driven step (khb_step plus the
+        timestep read-back each step)."""
+        graph = (world == 1 and not args.slab_path) if graph is None else graph
         b, drv = make(precision)
+        if graph:
+            from kharma_b200.block import DeviceDriver
+            drv = DeviceDriver(b, graph=True)
         for _ in range(warmup):
             drv.step()
         torch.cuda.synchronize()
@@ -394,7 +403,14 @@ def gpu_arm(args, rank, world, local_rank):
         return b, drv, ms, launches, clocks
 
     sampler = ClockSampler(torch.cuda.current_device())
-    b, drv, ms, launches, clocks = run("fp64", args.steps, args.warmup, sampler)
+    bench_stream = torch.cuda.Stream()
+    torch.cuda.set_stream(bench_stream)          # graph capture needs a non-default stream
+    b, drv, ms, launches, clocks = run(args.form, args.steps, args.warmup, sampler)
+    host_driven = None
+    if world == 1 and not args.slab_path:
+        _, _, ms_h, _, _ = run(args.form, max(3, args.steps // 4), args.warmup, graph=False)
+        host_driven = {"ms_per_step": ms_h / max(3, args.steps // 4),
+                       "value": zones / (ms_h / max(3, args.steps // 4) / 1000.0)}
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -448,7 +464,7 @@ def gpu_arm(args, rank, world, local_rank):
         for _ in range(ke):
             b.P.copy_(hP, non_blocking=True)
             b.U.copy_(hU, non_blocking=True)
-            drv.step()                       # includes the min-dt read-back
+            drv.step()                       # the graph-replayed step; its timestep stays on the device
             hP.copy_(b.P, non_blocking=True)
             hU.copy_(b.U, non_blocking=True)
         e1.record()
@@ -459,7 +475,7 @@ def gpu_arm(args, rank, world, local_rank):
         ms_e = float(te.item()) / ke
         nbytes = 2 * b.P.numel() * 8
         e2e = {"value": world * zones / (ms_e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": nbytes + 8, "ms_per_step": ms_e}
+               "d2h_bytes_per_step": nbytes if world == 1 else nbytes + 8, "ms_per_step": ms_e}
 
     # roofline of the dominant kernel, timed live with CUDA events
     peak, peak_kind = measured_peaks()
@@ -516,7 +532,8 @@ def gpu_arm(args, rank, world, local_rank):
                           "parallelism": "single block" if world == 1 else f"x3 slabs x{world} (NCCL halo exchange)",
                           "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
-               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch}
+               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch,
+               "host_driven_step": host_driven}
         print(json.dumps(out), flush=True)
 
 

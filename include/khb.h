@@ -255,6 +255,23 @@ int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
  * GRMHD::EstimateTimestep computes it (grmhd.cpp:294-330).  Synchronizes the stream. */
 int khb_get_min_ndt(khb_ctx* ctx, double* min_ndt_host, void* stream);
 
+/* Device-resident timestep control: GRMHD::EstimateTimestep and KHARMADriver::SetGlobalTimeStep
+ * (grmhd.cpp:252-343, kharma_driver.cpp:439-460) evaluated on the device after each step, so a
+ * step needs no host synchronisation.  khb_set_timestep gives the first dt and the schedule
+ * (GRMHD/cfl, parthenon/time/dt_min, max_dt_increase); khb_get_timestep reads back the next dt, the
+ * accumulated time and the dt of the last step (synchronizes). */
+int khb_set_timestep(khb_ctx* ctx, double dt, double cfl, double dt_min, double max_dt_increase);
+int khb_get_timestep(khb_ctx* ctx, double* dt_next, double* t, double* dt_last, void* stream);
+
+/* khb_step with the device timestep, followed by the next timestep on the device.  Launches only. */
+int khb_step_device_dt(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag,
+                       void* stream);
+
+/* The same step replayed from a CUDA graph, captured on the first call with a given state (P, U,
+ * flags) on a non-default stream and replayed while the state pointers stay the same. */
+int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag,
+                   void* stream);
+
 /* B_FluxCT::MaxDivB (b_flux_ct.cpp:566-607): max |corner divB| of the conserved field.
  * Synchronizes the stream. */
 int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void* stream);

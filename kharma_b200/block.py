@@ -180,3 +180,33 @@ class Driver:
         self.nstep += 1
         self.dt = self.next_dt(mn, dt)
         return dt, mn
+
+
+class DeviceDriver:
+    """The reference's timestep schedule (as Driver) kept on the device: each step reads its dt from
+    device memory and sets the next one there (khb_set_timestep / khb_step_device_dt), so a step
+    needs no host synchronisation and can be replayed from a CUDA graph (khb_step_graph, on the
+    block's current stream, which must not be the default stream)."""
+
+    def __init__(self, block: Block, dt_start=None, graph=True):
+        self.block = block
+        s = block.spec
+        dt0 = s.dt_min if dt_start is None else dt_start
+        _lib.check(block.lib.khb_set_timestep(block.ctx, float(dt0), s.cfl, s.dt_min, s.max_dt_increase),
+                   "khb_set_timestep")
+        self.graph = graph
+        self.nstep = 0
+
+    def step(self):
+        b = self.block
+        fn = b.lib.khb_step_graph if self.graph else b.lib.khb_step_device_dt
+        _lib.check(fn(b.ctx, b.Pf.ref, b.Uf.ref, C.c_void_p(b.pflag.data_ptr()), C.c_void_p(b.fflag.data_ptr()),
+                      b.stream), "khb_step_graph" if self.graph else "khb_step_device_dt")
+        self.nstep += 1
+
+    def timestep(self):
+        """(next dt, time, dt of the last step); synchronizes."""
+        dt, t, last = C.c_double(), C.c_double(), C.c_double()
+        _lib.check(self.block.lib.khb_get_timestep(self.block.ctx, C.byref(dt), C.byref(t), C.byref(last),
+                                                   self.block.stream), "khb_get_timestep")
+        return dt.value, t.value, last.value

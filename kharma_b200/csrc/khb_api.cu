@@ -101,7 +101,7 @@ void launch_fofc_t(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, con
     FT* F[3] = {(FT*)ctx->F[0], (FT*)ctx->F[1], (FT*)ctx->F[2]};
     FT* ct[3] = {(FT*)ctx->ctop[0], (FT*)ctx->ctop[1], (FT*)ctx->ctop[2]};
     Launch<FT>::fofc(ctx->nv, ctx->d, ctx->g, ctx->ph, Ps, Us, U0, F, ct, kRkGam0[s], kRkGam1[s], kRkBeta[s] * dt,
-                     ctx->fofc_flag, st);
+                     ctx->dt_active, kRkBeta[s], ctx->fofc_flag, st);
 }
 int launch_fofc(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
                 const khb_fields& U0, cudaStream_t st)
@@ -124,6 +124,8 @@ struct ZoneCall {
     int32_t* pflag;
     int32_t* fflag;
     double g0, g1, bdt;
+    const double* dt_dev;       // device timestep (then bdt = beta * dt_dev[0])
+    double beta;
     int mode;
 };
 
@@ -135,6 +137,7 @@ void launch_zone_t(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
     for (int x = 0; x < 3; ++x) { a.F[x] = (const FT*)ctx->F[x]; a.ctop[x] = (const FT*)ctx->ctop[x]; }
     a.pflag = zc.pflag; a.fflag = zc.fflag;
     a.g0 = zc.g0; a.g1 = zc.g1; a.bdt = zc.bdt;
+    a.dt_dev = zc.dt_dev; a.beta = zc.beta;
     a.ndt_word = ctx->words;
     a.fail_count = ctx->fail_count;
     a.fail_list = ctx->fail_list;
@@ -226,16 +229,15 @@ int zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const kh
               int32_t* pflag, int32_t* fflag, cudaStream_t st)
 {
     const int s = stage - 1;
-    if (stage == 2) {
-        // the minimum is taken over bit patterns; start from the pattern of DBL_MAX
-        KHB_CUDA(cudaMemcpyAsync(ctx->words, &ctx->dbl_max_bits, sizeof(unsigned long long),
-                                 cudaMemcpyHostToDevice, st));
-    }
-    KHB_CUDA(cudaMemsetAsync(ctx->fail_count, 0, sizeof(int), st));
+    // failed-zone counter, and on the last stage the timestep minimum (taken over bit patterns,
+    // from the pattern of DBL_MAX), reset on the device so that the stage can be graph-captured
+    LaunchCommon::stage_reset(ctx->fail_count, stage == 2 ? ctx->words : nullptr, st);
+    KHB_LAUNCHED(ctx);
     ZoneCall zc;
     zc.Ps = Ps; zc.Us = Us; zc.U0 = U0; zc.Pout = Pout; zc.Uout = Uout;
     zc.pflag = pflag; zc.fflag = fflag;
     zc.g0 = kRkGam0[s]; zc.g1 = kRkGam1[s]; zc.bdt = kRkBeta[s] * dt;
+    zc.dt_dev = ctx->dt_active; zc.beta = kRkBeta[s];
     const int dtm = (stage == 2) ? M_DT : 0;
     if (!ctx->zone_split) {
         zc.mode = M_ZONE_FUSED | dtm;
@@ -412,6 +414,9 @@ int khb_destroy(khb_ctx* c)
     for (int x = 0; x < 3; ++x) cudaFree(c->F10[x]);
     cudaFree(c->dudt10);
     cudaFree(c->fofc_flag);
+    cudaFree(c->dt_state);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
     delete c;
     return KHB_OK;
 }
@@ -682,6 +687,85 @@ int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
     }
     if ((rc = do_stage(ctx, 1, dt, *P, *U, *U, P1, U1, pflag, fflag, S(stream)))) return rc;
     return do_stage(ctx, 2, dt, P1, U1, *U, *P, *U, pflag, fflag, S(stream));
+}
+
+int khb_set_timestep(khb_ctx* ctx, double dt, double cfl, double dt_min, double max_dt_increase)
+{
+    if (!ctx) return fail(KHB_ERR_ARG, "khb_set_timestep: NULL context");
+    if (!(dt > 0.) || !(cfl > 0.) || !(max_dt_increase > 0.)) return fail(KHB_ERR_ARG, "khb_set_timestep: bad value");
+    if (!ctx->dt_state) KHB_CUDA(cudaMalloc((void**)&ctx->dt_state, 3 * sizeof(double)));
+    const double h[3] = {dt, 0., 0.};
+    KHB_CUDA(cudaMemcpy(ctx->dt_state, h, sizeof(h), cudaMemcpyHostToDevice));
+    KHB_CUDA(cudaDeviceSynchronize());       // the upload is complete before any stream reads it
+    ctx->dt_cfl = cfl; ctx->dt_min = dt_min; ctx->dt_max_increase = max_dt_increase;
+    return KHB_OK;
+}
+
+int khb_get_timestep(khb_ctx* ctx, double* dt_next, double* t, double* dt_last, void* stream)
+{
+    if (!ctx || !ctx->dt_state) return fail(KHB_ERR_STATE, "khb_get_timestep: no device timestep (khb_set_timestep)");
+    double h[3];
+    KHB_CUDA(cudaMemcpyAsync(h, ctx->dt_state, sizeof(h), cudaMemcpyDeviceToHost, S(stream)));
+    KHB_CUDA(cudaStreamSynchronize(S(stream)));
+    if (dt_next) *dt_next = h[0];
+    if (t) *t = h[1];
+    if (dt_last) *dt_last = h[2];
+    return KHB_OK;
+}
+
+int khb_step_device_dt(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag,
+                       void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (!ctx->dt_state) return fail(KHB_ERR_STATE, "khb_step_device_dt: no device timestep (khb_set_timestep)");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_step_device_dt: NULL flags");
+    khb_fields P1, U1;
+    std::memset(&P1, 0, sizeof(P1)); std::memset(&U1, 0, sizeof(U1));
+    for (int p = 0; p < ctx->nv; ++p) {
+        P1.v[p] = ctx->stageP + (size_t)p*ctx->d.N;
+        U1.v[p] = ctx->stageU + (size_t)p*ctx->d.N;
+    }
+    ctx->dt_active = ctx->dt_state;
+    rc = do_stage(ctx, 1, 0., *P, *U, *U, P1, U1, pflag, fflag, S(stream));
+    if (!rc) rc = do_stage(ctx, 2, 0., P1, U1, *U, *P, *U, pflag, fflag, S(stream));
+    ctx->dt_active = nullptr;
+    if (rc) return rc;
+    LaunchCommon::next_dt(ctx->words, ctx->dt_state, ctx->dt_cfl, ctx->dt_min, ctx->dt_max_increase, S(stream));
+    KHB_LAUNCHED(ctx);
+    return KHB_OK;
+}
+
+int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag,
+                   void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    cudaStream_t st = S(stream);
+    if (!st) return fail(KHB_ERR_ARG, "khb_step_graph: needs a non-default stream to capture");
+    if (!P || !U || !pflag || !fflag) return fail(KHB_ERR_ARG, "khb_step_graph: NULL argument");
+    const bool same = ctx->gexec && !std::memcmp(&ctx->graph_P, P, sizeof(khb_fields)) &&
+                      !std::memcmp(&ctx->graph_U, U, sizeof(khb_fields)) && ctx->graph_pflag == pflag &&
+                      ctx->graph_fflag == fflag;
+    if (!same) {
+        if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+        if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+        const int64_t l0 = ctx->launches;
+        KHB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int rc = khb_step_device_dt(ctx, P, U, pflag, fflag, stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        ctx->graph_launches = ctx->launches - l0;
+        ctx->launches = l0;
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return fail(KHB_ERR_CUDA, std::string("khb_step_graph: capture: ") + cudaGetErrorString(e));
+        ctx->graph = g;
+        KHB_CUDA(cudaGraphInstantiate(&ctx->gexec, g, 0));
+        ctx->graph_P = *P; ctx->graph_U = *U; ctx->graph_pflag = pflag; ctx->graph_fflag = fflag;
+    }
+    KHB_CUDA(cudaGraphLaunch(ctx->gexec, st));
+    ctx->launches += ctx->graph_launches;
+    return KHB_OK;
 }
 
 int khb_get_min_ndt(khb_ctx* ctx, double* min_ndt_host, void* stream)

@@ -36,6 +36,17 @@ struct khb_ctx {
     double* F10[3];        // EMHD face fluxes, [10][N] per direction
     double* dudt10;        // EMHD dU/dt of an ImEx stage, [10][N]
     int32_t* fofc_flag;    // first-order flux correction flags, [N] (when fofc is on)
+    // device-resident timestep: state [dt, t, dt_last] and the schedule parameters
+    double* dt_state;
+    const double* dt_active;          // set while a step reads its dt from dt_state
+    double dt_cfl, dt_min, dt_max_increase;
+    // CUDA graph of one step with the device timestep, for the state it was captured with
+    cudaGraph_t graph;
+    cudaGraphExec_t gexec;
+    khb_fields graph_P, graph_U;
+    int32_t* graph_pflag;
+    int32_t* graph_fflag;
+    int64_t graph_launches;
 };
 
 

@@ -378,10 +378,11 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
                 dudt[4] += new_du[3];
             }
             // ---- RK combination (Parthenon WeightedSumData twice, kharma_driver.cpp:339-387)
+            const double bdt = a.dt_dev ? a.beta * __ldg(a.dt_dev) : a.bdt;
 #pragma unroll
             for (int p = 0; p < NV; ++p) {
                 double x = a.g0 * __ldg(a.Us.v[p] + c) + a.g1 * __ldg(a.U0.v[p] + c);
-                U[p] = 1.0 * x + a.bdt * dudt[p];
+                U[p] = 1.0 * x + bdt * dudt[p];
             }
         } else {
 #pragma unroll
@@ -493,10 +494,12 @@ k_zone(Dims d, DevGeom g, Phys ph, ZoneArgs<FT> a, Box bx)
 template <int NV, typename FT, bool KAST>
 __global__ void __launch_bounds__(128) k_fofc_guess(Dims d, DevGeom g, Phys ph, khb_fields Ps, khb_fields Us,
                                                     khb_fields U0, const FT* F1, const FT* F2, const FT* F3,
-                                                    double g0, double g1, double bdt, int32_t* flag, Box bx)
+                                                    double g0, double g1, double bdt_host, const double* dt_dev,
+                                                    double beta, int32_t* flag, Box bx)
 {
     int i, j, k;
     if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const double bdt = dt_dev ? beta * __ldg(dt_dev) : bdt_host;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     const long long N = d.N, sj = d.sj, sk = d.sk;
     const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
@@ -1098,6 +1101,23 @@ __global__ void k_batch_fixup(const FixupBlock* __restrict__ blocks, int stage)
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
         fixup_zone<NV>(B.d, B.g, B.ph, B.P[s], B.U[s], B.pflag, B.fail_list[t]);
 }
+__global__ void k_stage_reset(int* count, unsigned long long* word)
+{
+    *count = 0;
+    if (word) *word = 0x7FEFFFFFFFFFFFFFull;     // bit pattern of DBL_MAX
+}
+// GRMHD::EstimateTimestep: clip(cfl * min_ndt, dt_min, max_dt_increase * dt_last); then
+// KHARMADriver::SetGlobalTimeStep: min(2 dt_last, that) (grmhd.cpp:320-339, kharma_driver.cpp:439-460)
+__global__ void k_next_dt(const unsigned long long* ndt_word, double* state, double cfl, double dt_min,
+                          double max_dt_increase)
+{
+    const double mn = __longlong_as_double((long long)*ndt_word);
+    const double dt = state[0];
+    const double ndt = kmin(kmax(mn * cfl, dt_min), max_dt_increase * dt);
+    state[1] += dt;
+    state[2] = dt;
+    state[0] = kmin(2.0 * dt, ndt);
+}
 __global__ void k_batch_reset(int* const* counts, int nblocks, unsigned long long* word)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1198,7 +1218,7 @@ void Launch<FT>::copy_flux(long long N, int nv, const FT* F, const FT* ctop, con
 template <int NV, typename FT>
 static void fofc_nv(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& Ps, const khb_fields& Us,
                     const khb_fields& U0, FT* const F[3], FT* const ctop[3], double g0, double g1, double bdt,
-                    int32_t* flag, cudaStream_t st)
+                    const double* dt_dev, double beta, int32_t* flag, cudaStream_t st)
 {
     // flags are read over the interior +-2 (+-0 along periodic directions, filled from the images)
     const int p1 = d.bc[0] == KHB_BC_PERIODIC, p2 = d.bc[2] == KHB_BC_PERIODIC, p3 = d.bc[4] == KHB_BC_PERIODIC;
@@ -1209,9 +1229,9 @@ static void fofc_nv(const Dims& d, const DevGeom& g, const Phys& ph, const khb_f
     cudaMemsetAsync(flag, 0, sizeof(int32_t) * d.N, st);
     const Box gb = make_box(i0, j0, k0, i1 - i0 + 1, j1 - j0 + 1, k1 - k0 + 1);
     if (ph.inverter == KHB_INVERTER_KASTAUN)
-        k_fofc_guess<NV, FT, true><<<box_blocks(gb), 128, 0, st>>>(d, g, ph, Ps, Us, U0, F[0], F[1], F[2], g0, g1, bdt, flag, gb);
+        k_fofc_guess<NV, FT, true><<<box_blocks(gb), 128, 0, st>>>(d, g, ph, Ps, Us, U0, F[0], F[1], F[2], g0, g1, bdt, dt_dev, beta, flag, gb);
     else
-        k_fofc_guess<NV, FT, false><<<box_blocks(gb), 128, 0, st>>>(d, g, ph, Ps, Us, U0, F[0], F[1], F[2], g0, g1, bdt, flag, gb);
+        k_fofc_guess<NV, FT, false><<<box_blocks(gb), 128, 0, st>>>(d, g, ph, Ps, Us, U0, F[0], F[1], F[2], g0, g1, bdt, dt_dev, beta, flag, gb);
     if (ph.spherical && ph.fofc_polar_cells > 0 && d.ndim > 1) {
         for (int face = 2; face <= 3; ++face) {
             if (!phys_face(d.bc[face])) continue;
@@ -1238,10 +1258,10 @@ static void fofc_nv(const Dims& d, const DevGeom& g, const Phys& ph, const khb_f
 template <typename FT>
 void Launch<FT>::fofc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& Ps,
                       const khb_fields& Us, const khb_fields& U0, FT* const F[3], FT* const ctop[3], double g0,
-                      double g1, double bdt, int32_t* flag, cudaStream_t st)
+                      double g1, double bdt, const double* dt_dev, double beta, int32_t* flag, cudaStream_t st)
 {
-    if (nv == 8) fofc_nv<8, FT>(d, g, ph, Ps, Us, U0, F, ctop, g0, g1, bdt, flag, st);
-    else fofc_nv<5, FT>(d, g, ph, Ps, Us, U0, F, ctop, g0, g1, bdt, flag, st);
+    if (nv == 8) fofc_nv<8, FT>(d, g, ph, Ps, Us, U0, F, ctop, g0, g1, bdt, dt_dev, beta, flag, st);
+    else fofc_nv<5, FT>(d, g, ph, Ps, Us, U0, F, ctop, g0, g1, bdt, dt_dev, beta, flag, st);
 }
 
 // Batched flux launch; ntiles == 0 returns the resident CTAs per SM of the kernel
@@ -1325,6 +1345,17 @@ void LaunchCommon::batch_fixup(int nv, const FixupBlock* blocks, int nblocks, in
 void LaunchCommon::batch_reset(int* const* counts, int nblocks, unsigned long long* word, cudaStream_t st)
 {
     k_batch_reset<<<blocks_for(nblocks, 128), 128, 0, st>>>(counts, nblocks, word);
+}
+
+void LaunchCommon::stage_reset(int* count, unsigned long long* word, cudaStream_t st)
+{
+    k_stage_reset<<<1, 1, 0, st>>>(count, word);
+}
+
+void LaunchCommon::next_dt(const unsigned long long* ndt_word, double* state, double cfl, double dt_min,
+                           double max_dt_increase, cudaStream_t st)
+{
+    k_next_dt<<<1, 1, 0, st>>>(ndt_word, state, cfl, dt_min, max_dt_increase);
 }
 
 void LaunchCommon::fixup(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,

@@ -92,6 +92,8 @@ struct ZoneArgs {
     int32_t* pflag;
     int32_t* fflag;
     double g0, g1, bdt;
+    const double* dt_dev;      // when set, bdt = beta * dt_dev[0] (device-resident timestep)
+    double beta;
     unsigned long long* ndt_word;
     int* fail_count;
     int* fail_list;
@@ -147,7 +149,7 @@ struct Launch {
     // test, flags (polar rows, periodic images), donor-cell LLF on the faces bordering a flagged zone
     static void fofc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& Ps,
                      const khb_fields& Us, const khb_fields& U0, FT* const F[3], FT* const ctop[3], double g0,
-                     double g1, double bdt, int32_t* flag, cudaStream_t st);
+                     double g1, double bdt, const double* dt_dev, double beta, int32_t* flag, cudaStream_t st);
     // Batched launches over every block of a batch: tiles[t] is the block of tile t; grid = 0 runs
     // one CTA per tile, otherwise grid CTAs loop over the tiles.  Return the CTAs per SM the kernel
     // can keep resident (for sizing a persistent grid) when called with ntiles = 0.
@@ -177,6 +179,12 @@ struct LaunchCommon {
     // (and, when word != NULL, of the timestep minimum)
     static void batch_fixup(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st);
     static void batch_reset(int* const* counts, int nblocks, unsigned long long* word, cudaStream_t st);
+    // Per-stage reset of one block's failed-zone counter (and of the timestep minimum when word)
+    static void stage_reset(int* count, unsigned long long* word, cudaStream_t st);
+    // Device-resident timestep (grmhd.cpp:252-343, kharma_driver.cpp:439-460): state[0] = dt,
+    // state[1] = time, state[2] = the dt of the last step; advanced from the minimum zone timestep
+    static void next_dt(const unsigned long long* ndt_word, double* state, double cfl, double dt_min,
+                        double max_dt_increase, cudaStream_t st);
 };
 
 // EMHD and implicit-solve parameters are passed to the kernels as the C-ABI structs themselves
