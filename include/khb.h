@@ -272,6 +272,33 @@ int khb_step_device_dt(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, i
 int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag,
                    void* stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Discrete adjoint of the step (no reference counterpart: KHARMA has no adjoint; the step it
+ * differentiates is khb_step, i.e. kharma_step.cpp:77-319 with the flux, flux-CT, update and
+ * inversion kernels above)
+ * ------------------------------------------------------------------------------------------- */
+
+/* Adjoint of one khb_step (P_n, U_n) -> (P_np1, U_np1) at the given dt.  On entry (Pbar, Ubar)
+ * hold the adjoint of the step's output; on return, the adjoint of its input (P_n, U_n), so that
+ * calls for steps N-1, ..., 0 in turn carry an adjoint back through a run.  rho_flux1_weight (NULL:
+ * none) adds the objective sum over stages of weight_scale * sum_faces weight[f] * F1[rho][f] of
+ * the raw x1 face fluxes ([N] doubles, indexed like the zone arrays; with weight_scale = dt/2 and
+ * weights of dx2 dx3 on one x1 face layer, the RK2-consistent mass through that layer in the step).
+ * The intermediate stage is recomputed from (P_n, U_n) into the context's stage scratch; the
+ * inversion is differentiated by the implicit-function theorem at the converged state; periodic
+ * ghost-zone adjoints are folded into their images, exchange ghost zones are constants.  Supported:
+ * LLF fluxes with linear MC or donor-cell reconstruction, periodic or exchange faces, floors,
+ * recon floors and FOFC off (KHB_ERR_UNSUPPORTED otherwise).  Ghost zones of Pbar/Ubar are zero on
+ * return.  Scratch (6 nv N doubles, 2 N flags) is allocated on the first call. */
+int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_fields* U_n,
+                     const khb_fields* P_np1, const khb_fields* Pbar, const khb_fields* Ubar,
+                     const double* rho_flux1_weight, double weight_scale, void* stream);
+
+/* Pbar += (dU/dP)^T Ubar at every zone of P (the adjoint of Flux::p_to_u, flux_functions.hpp:343-352,
+ * e.g. of the conserved initial state formed from primitive initial data). */
+int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, const khb_fields* Pbar,
+                     void* stream);
+
 /* B_FluxCT::MaxDivB (b_flux_ct.cpp:566-607): max |corner divB| of the conserved field.
  * Synchronizes the stream. */
 int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void* stream);

@@ -28,9 +28,10 @@ UNITS = {
     "khb_batch.cu": [],
     "khb_noalloc.cu": ["-fmad=false"],
     "khb_emhd.cu": ["-fmad=false"],
+    "khb_adjoint.cu": ["-fmad=false"],
     "khb_geometry.cpp": [],
 }
-HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", "khb_internal.hpp", os.path.join("..", "..", "include", "khb.h")]
+HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", "khb_internal.hpp", "khb_dual.cuh", os.path.join("..", "..", "include", "khb.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 

@@ -1,0 +1,614 @@
+// khb_adjoint.cu -- discrete adjoint of the explicit RK2 stage (the differentiation form).
+//
+// For one stage (P_s, U_s, U_0) -> (P_out, U_out) of khb_stage, and given the adjoint of its output
+// (Pbar_out, Ubar_out), accumulate the adjoints of its inputs.  The stage is the composition
+//   face fluxes F_d(P_s)  (MC or donor-cell reconstruction, prim_to_flux, vchar, LLF)
+//   U_upd = g0 U_s + g1 U_0 + beta dt (-div F(flux-CT for B) + S(P_s))   (geometric source S)
+//   P_out = inverse of U(P) at U_upd (1D_W / Kastaun), U_out = U(P_out) (the lock-step P -> U)
+// whose adjoint, in reverse order, is
+//   Ubar_upd = Ubar_out + J(P_out)^-T Pbar_out           (implicit-function adjoint of the inversion;
+//                                                           J = dU/dP, so U_out = U_upd to the inverter's
+//                                                           tolerance and contributes Ubar_out)
+//   Ubar_s += g0 Ubar_upd, Ubar_0 += g1 Ubar_upd,
+//   Fbar += transpose of the divergence (and of flux-CT), Pbar_s += beta dt (dS/dP)^T Ubar_upd,
+//   Pbar_s += (dF/dP_stencil)^T Fbar                      (per face, scattered with atomics).
+// Local Jacobians come from the same templated device functions the forward kernels use, evaluated
+// on Dual numbers with one unit tangent per input.  Out of scope (rejected): floors, failed-zone
+// fixups, physical boundaries (outflow/reflecting faces), WENO5/PPM, HLLE.  Periodic ghost zones are
+// copies of their images, so their adjoints are folded into the images; exchange ghost zones are
+// the caller's constants and their adjoints are dropped.  The timestep is taken as given (the
+// forward run's sequence).
+#include "khb_internal.hpp"
+#include "khb_dual.cuh"
+#include "khb_kernels.cuh"
+
+#include <cstring>
+#include <string>
+
+namespace khb {
+
+// MC face values of a zone from its left, centre and right values (reconstruction.hpp:107-123)
+template <typename R>
+__device__ __forceinline__ R mc_right(R xm, R x0, R xp) { return x0 + R(0.5) * (mc_lim<R>(x0 - xm, xp - x0) * (xp - x0)); }
+template <typename R>
+__device__ __forceinline__ R mc_left(R xm, R x0, R xp) { return x0 - R(0.5) * (mc_lim<R>(x0 - xm, xp - x0) * (xp - x0)); }
+
+// One side of a face in arithmetic R: conserved state, flux and signal speeds (get_flux.hpp:219-331)
+template <typename R, int NV, int DIR>
+__device__ __forceinline__ void face_side(const R gcov[4][4], const R* gcon0, R gcondd, R gdet, R gam, const R* P,
+                                          R* U, R* F, R& cmax, R& cmin)
+{
+    FourVec<R> D;
+    calc_4vecs<R, (NV > 5)>(gcov, gcon0[0], gcon0, P, D);
+    prim_to_flux<R, NV>(P, D, gam, gdet, 0, U);
+    prim_to_flux<R, NV>(P, D, gam, gdet, DIR, F);
+    vchar<R, (NV > 5)>(P, D, gam, gcon0[0], gcon0[DIR], gcondd, DIR, cmax, cmin);
+}
+
+// ---------------------------------------------------------------------------- face fluxes
+// Pbar += (dF/dP)^T Fbar for every face of the box (faces [s, e+1] along DIR, [s-1, e+1] across).
+// R: the arithmetic of the forward face kernel (double, or float in the FP32-flux form).
+template <int DIR, int NV, int RECON, typename R>
+__global__ void __launch_bounds__(128) k_adj_flux(Dims d, DevGeom g, Phys ph, khb_fields P, const double* Fbar,
+                                                  khb_fields Pbar, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long st = (DIR == 1) ? 1 : ((DIR == 2) ? d.sj : d.sk);
+    double fb[NV];
+    bool any = false;
+#pragma unroll
+    for (int p = 0; p < NV; ++p) { fb[p] = Fbar[p*d.N + c]; any |= fb[p] != 0.; }
+    if (!any) return;
+    typedef Dual<R> DR;
+    const int loc = DIR - 1;
+    const long long gi = (long long)j*g.G1 + i;
+    // the face tables of the forward kernel's arithmetic (FP32 copies in the FP32-flux form)
+    const auto* tcov = FaceTables<R>::gcov(g, loc);
+    const auto* tcon = FaceTables<R>::gcon(g, loc);
+    R gcov[4][4], gcon0[4];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) gcov[m/4][m%4] = (R)__ldg(tcov + m*g.gs + gi);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) gcon0[m] = (R)__ldg(tcon + m*g.gs + gi);
+    const R gcondd = (R)__ldg(tcon + (DIR*4 + DIR)*g.gs + gi);
+    const R gdet = (R)__ldg(FaceTables<R>::gdet(g, loc) + gi);
+    const R gam = (R)ph.gam;
+    // stencil c-2 .. c+1 (MC uses zones c-2..c for the left state and c-1..c+1 for the right)
+    R x[4][NV];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int p = 0; p < NV; ++p) x[s][p] = (R)P.v[p][c + (s - 2)*st];
+    R Pl[NV], Pr[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        if (RECON == RECON_DONOR) { Pl[p] = x[1][p]; Pr[p] = x[2][p]; }
+        else { Pl[p] = mc_right<R>(x[0][p], x[1][p], x[2][p]); Pr[p] = mc_left<R>(x[1][p], x[2][p], x[3][p]); }
+    }
+    // values of both sides
+    R Uv[2][NV], Fv[2][NV], cmx[2], cmn[2];
+    face_side<R, NV, DIR>(gcov, gcon0, gcondd, gdet, gam, Pl, Uv[0], Fv[0], cmx[0], cmn[0]);
+    face_side<R, NV, DIR>(gcov, gcon0, gcondd, gdet, gam, Pr, Uv[1], Fv[1], cmx[1], cmn[1]);
+    // dual geometry
+    DR Dgcov[4][4], Dgcon0[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        Dgcon0[a] = DR(gcon0[a]);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) Dgcov[a][b] = DR(gcov[a][b]);
+    }
+    const DR Dgcondd(gcondd), Dgdet(gdet), Dgam(gam);
+    double Pbar_side[2][NV];
+    for (int side = 0; side < 2; ++side) {
+        const R* Ps = side ? Pr : Pl;
+        for (int q = 0; q < NV; ++q) {
+            DR Pd[NV];
+#pragma unroll
+            for (int p = 0; p < NV; ++p) Pd[p] = DR(Ps[p], (p == q) ? R(1) : R(0));
+            DR Ud[NV], Fd[NV], cmaxd, cmind;
+            face_side<DR, NV, DIR>(Dgcov, Dgcon0, Dgcondd, Dgdet, Dgam, Pd, Ud, Fd, cmaxd, cmind);
+            // LLF of the two sides with this side in duals (flux.hpp:110-121, get_flux.hpp:274-331)
+            const DR o_cmax(cmx[1 - side]), o_cmin(cmn[1 - side]);
+            const DR cmaxL = side ? o_cmax : cmaxd, cminL = side ? o_cmin : cmind;
+            const DR cmaxR = side ? cmaxd : o_cmax, cminR = side ? cmind : o_cmin;
+            const DR cmax = kmax(kmax(DR(R(0)), cmaxL), cmaxR);
+            const DR cmin = -kmin(kmin(DR(R(0)), cminL), cminR);
+            const DR ctp = kmax(cmax, cmin);
+            double acc = 0.;
+#pragma unroll
+            for (int p = 0; p < NV; ++p) {
+                const DR FL = side ? DR(Fv[0][p]) : Fd[p], FR = side ? Fd[p] : DR(Fv[1][p]);
+                const DR UL = side ? DR(Uv[0][p]) : Ud[p], UR = side ? Ud[p] : DR(Uv[1][p]);
+                const DR f = DR(R(0.5)) * (FL + FR - ctp * (UR - UL));
+                acc += fb[p] * (double)f.d;
+            }
+            Pbar_side[side][q] = acc;
+        }
+    }
+    // through the reconstruction to the stencil zones
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        if (RECON == RECON_DONOR) {
+            atomicAdd(Pbar.v[p] + c - st, Pbar_side[0][p]);
+            atomicAdd(Pbar.v[p] + c, Pbar_side[1][p]);
+            continue;
+        }
+        double gl[3], gr[3];
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            DR a[3];
+#pragma unroll
+            for (int t = 0; t < 3; ++t) a[t] = DR(x[t][p], (t == s) ? R(1) : R(0));
+            gl[s] = (double)mc_right<DR>(a[0], a[1], a[2]).d;
+            DR b[3];
+#pragma unroll
+            for (int t = 0; t < 3; ++t) b[t] = DR(x[t + 1][p], (t == s) ? R(1) : R(0));
+            gr[s] = (double)mc_left<DR>(b[0], b[1], b[2]).d;
+        }
+        // left state from zones c-2, c-1, c; right state from c-1, c, c+1
+        atomicAdd(Pbar.v[p] + c - 2*st, Pbar_side[0][p] * gl[0]);
+        atomicAdd(Pbar.v[p] + c - st, Pbar_side[0][p] * gl[1] + Pbar_side[1][p] * gr[0]);
+        atomicAdd(Pbar.v[p] + c, Pbar_side[0][p] * gl[2] + Pbar_side[1][p] * gr[1]);
+        atomicAdd(Pbar.v[p] + c + st, Pbar_side[1][p] * gr[2]);
+    }
+}
+
+// ---------------------------------------------------------------------------- update
+// Adjoint of U_upd = g0 U_s + g1 U_0 + bdt (-div F + S(P_s)) over the interior: Fbar (atomics),
+// Pbar_s (own zone), Ubar_s and Ubar_0 (own zone; they may be the same array).
+template <int NV>
+__global__ void __launch_bounds__(128) k_adj_update(Dims d, DevGeom g, Phys ph, const double* Ubar_upd, khb_fields Ps,
+                                                    double g0, double g1, double bdt, double* F1b, double* F2b,
+                                                    double* F3b, khb_fields Pbar_s, khb_fields Ubar_s,
+                                                    khb_fields Ubar_0, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long N = d.N, sj = d.sj, sk = d.sk;
+    double ub[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) ub[p] = Ubar_upd[p*N + c];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        Ubar_s.v[p][c] += g0 * ub[p];
+        Ubar_0.v[p][c] += g1 * ub[p];
+    }
+    const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
+    const double w = bdt / (ph.dx1*ph.dx2*ph.dx3);
+    // hydro divergence: U += bdt * -(a1 (F1(c+1) - F1(c)) + ...)/vol
+#pragma unroll
+    for (int p = 0; p < 5; ++p) {
+        const double u = w * ub[p];
+        atomicAdd(F1b + p*N + c + 1, -a1 * u); atomicAdd(F1b + p*N + c, a1 * u);
+        if (d.ndim >= 2) { atomicAdd(F2b + p*N + c + sj, -a2 * u); atomicAdd(F2b + p*N + c, a2 * u); }
+        if (d.ndim == 3) { atomicAdd(F3b + p*N + c + sk, -a3 * u); atomicAdd(F3b + p*N + c, a3 * u); }
+    }
+    if (NV > 5) {
+        // flux-CT (b_flux_ct.cpp:307-370) as ct_divergence forms it: face B fluxes from corner EMFs,
+        // EMFs from the raw B fluxes; transposed term by term
+        const long long B1 = 5*N, B2 = 6*N, B3 = 7*N;
+        const bool d3 = d.ndim > 2;
+        auto e3 = [&](long long x, double v) {      // e3 = 0.25 (F1[B2](x) + F1[B2](x-sj) - F2[B1](x) - F2[B1](x-1))
+            atomicAdd(F1b + B2 + x, 0.25 * v); atomicAdd(F1b + B2 + x - sj, 0.25 * v);
+            atomicAdd(F2b + B1 + x, -0.25 * v); atomicAdd(F2b + B1 + x - 1, -0.25 * v);
+        };
+        auto e1 = [&](long long x, double v) {      // e1 = 0.25 (F2[B3](x) + F2[B3](x-sk) - F3[B2](x) - F3[B2](x-sj))
+            atomicAdd(F2b + B3 + x, 0.25 * v); atomicAdd(F2b + B3 + x - sk, 0.25 * v);
+            atomicAdd(F3b + B2 + x, -0.25 * v); atomicAdd(F3b + B2 + x - sj, -0.25 * v);
+        };
+        auto e2 = [&](long long x, double v) {      // e2 = 0.25 (F3[B1](x) + F3[B1](x-1) - F1[B3](x) - F1[B3](x-sk))
+            atomicAdd(F3b + B1 + x, 0.25 * v); atomicAdd(F3b + B1 + x - 1, 0.25 * v);
+            atomicAdd(F1b + B3 + x, -0.25 * v); atomicAdd(F1b + B3 + x - sk, -0.25 * v);
+        };
+        // adjoints of the face B fluxes: U_B[v] += -bdt (a_d (fb[d][v][hi] - fb[d][v][lo]))/vol
+        double fbb[3][3][2];
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const double u = w * ub[5 + v];
+            fbb[0][v][1] = -a1 * u; fbb[0][v][0] = a1 * u;
+            fbb[1][v][1] = (d.ndim >= 2) ? -a2 * u : 0.; fbb[1][v][0] = (d.ndim >= 2) ? a2 * u : 0.;
+            fbb[2][v][1] = (d.ndim == 3) ? -a3 * u : 0.; fbb[2][v][0] = (d.ndim == 3) ? a3 * u : 0.;
+        }
+        if (d.ndim >= 2) {
+            if (ph.zero_polar_flux) {
+                if (j == d.js && phys_face(d.bc[2])) { fbb[1][0][0] = 0.; fbb[1][1][0] = 0.; fbb[1][2][0] = 0.; }
+                if (j == d.je && phys_face(d.bc[3])) { fbb[1][0][1] = 0.; fbb[1][1][1] = 0.; fbb[1][2][1] = 0.; }
+            }
+            // X1 faces: fb[0][1] = 0.5 (e3 + e3), fb[0][2] = -0.5 (e2 + e2) or raw F1[B3]
+            e3(c, 0.5 * fbb[0][1][0]); e3(c + sj, 0.5 * fbb[0][1][0]);
+            e3(c + 1, 0.5 * fbb[0][1][1]); e3(c + 1 + sj, 0.5 * fbb[0][1][1]);
+            if (d3) {
+                e2(c, -0.5 * fbb[0][2][0]); e2(c + sk, -0.5 * fbb[0][2][0]);
+                e2(c + 1, -0.5 * fbb[0][2][1]); e2(c + 1 + sk, -0.5 * fbb[0][2][1]);
+            } else {
+                atomicAdd(F1b + B3 + c, fbb[0][2][0]); atomicAdd(F1b + B3 + c + 1, fbb[0][2][1]);
+            }
+            // X2 faces: fb[1][0] = -0.5 (e3 + e3), fb[1][2] = 0.5 (e1 + e1) or raw F2[B3]
+            e3(c, -0.5 * fbb[1][0][0]); e3(c + 1, -0.5 * fbb[1][0][0]);
+            e3(c + sj, -0.5 * fbb[1][0][1]); e3(c + sj + 1, -0.5 * fbb[1][0][1]);
+            if (d3) {
+                e1(c, 0.5 * fbb[1][2][0]); e1(c + sk, 0.5 * fbb[1][2][0]);
+                e1(c + sj, 0.5 * fbb[1][2][1]); e1(c + sj + sk, 0.5 * fbb[1][2][1]);
+                // X3 faces: fb[2][0] = 0.5 (e2 + e2), fb[2][1] = -0.5 (e1 + e1)
+                e2(c, 0.5 * fbb[2][0][0]); e2(c + 1, 0.5 * fbb[2][0][0]);
+                e2(c + sk, 0.5 * fbb[2][0][1]); e2(c + sk + 1, 0.5 * fbb[2][0][1]);
+                e1(c, -0.5 * fbb[2][1][0]); e1(c + sj, -0.5 * fbb[2][1][0]);
+                e1(c + sk, -0.5 * fbb[2][1][1]); e1(c + sk + sj, -0.5 * fbb[2][1][1]);
+            } else {
+                atomicAdd(F2b + B3 + c, fbb[1][2][0]); atomicAdd(F2b + B3 + c + sj, fbb[1][2][1]);
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                atomicAdd(F1b + (5 + v)*N + c, fbb[0][v][0]);
+                atomicAdd(F1b + (5 + v)*N + c + 1, fbb[0][v][1]);
+            }
+        }
+    }
+    // geometric source (flux.cpp:395-444): Pbar_s += bdt (dS/dP)^T Ubar[1..4]
+    if (!ph.cart_minkowski) {
+        typedef Dual<double> DD;
+        ZoneGeom G;
+        load_zone_geom(g, j, i, G);
+        DD gcov[4][4], gcon0[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            gcon0[a] = DD(G.gcon[0][a]);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) gcov[a][b] = DD(G.gcov[a][b]);
+        }
+        const long long cg = (long long)j*g.n1 + i, cs = (long long)(d.n2)*g.n1;
+        double P0[NV];
+#pragma unroll
+        for (int p = 0; p < NV; ++p) P0[p] = Ps.v[p][c];
+        for (int q = 0; q < NV; ++q) {
+            DD P[NV];
+#pragma unroll
+            for (int p = 0; p < NV; ++p) P[p] = DD(P0[p], (p == q) ? 1. : 0.);
+            FourVec<DD> D;
+            calc_4vecs<DD, (NV > 5)>(gcov, gcon0[0], gcon0, P, D);
+            DD new_du[4] = {DD(0.), DD(0.), DD(0.), DD(0.)};
+            for (int mu = 0; mu < 4; ++mu) {
+                DD Tmu[4];
+                calc_tensor<DD, (NV > 5)>(P[0], P[1], DD(ph.gam - 1) * P[1], D, mu, Tmu);
+#pragma unroll
+                for (int nu = 0; nu < 4; ++nu)
+#pragma unroll
+                    for (int lam = 0; lam < 4; ++lam)
+                        new_du[lam] += Tmu[nu] * DD(__ldg(g.gdet_conn + ((nu*4 + lam)*4 + mu)*cs + cg));
+            }
+            double acc = 0.;
+#pragma unroll
+            for (int lam = 0; lam < 4; ++lam) acc += ub[1 + lam] * new_du[lam].d;
+            Pbar_s.v[q][c] += bdt * acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------- inversion + P -> U
+// J = dU/dP at P (conserved from primitives, flux_functions.hpp:343-352) by NV dual evaluations
+template <int NV>
+__device__ __forceinline__ void ptou_jacobian(const ZoneGeom& G, double gam, const double* P0, double J[NV][NV])
+{
+    typedef Dual<double> DD;
+    DD gcov[4][4], gcon0[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        gcon0[a] = DD(G.gcon[0][a]);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) gcov[a][b] = DD(G.gcov[a][b]);
+    }
+    for (int q = 0; q < NV; ++q) {
+        DD P[NV], U[NV];
+#pragma unroll
+        for (int p = 0; p < NV; ++p) P[p] = DD(P0[p], (p == q) ? 1. : 0.);
+        FourVec<DD> D;
+        calc_4vecs<DD, (NV > 5)>(gcov, gcon0[0], gcon0, P, D);
+        prim_to_flux<DD, NV>(P, D, DD(gam), DD(G.gdet), 0, U);
+#pragma unroll
+        for (int p = 0; p < NV; ++p) J[p][q] = U[p].d;
+    }
+}
+
+// Solve A^T y = b in place (b <- y) by Gaussian elimination with partial pivoting on A^T
+template <int N>
+__device__ __forceinline__ void solve_transposed(double A[N][N], double b[N])
+{
+    double M[N][N];
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int s = 0; s < N; ++s) M[r][s] = A[s][r];
+    for (int col = 0; col < N; ++col) {
+        int piv = col;
+        double best = fabs(M[col][col]);
+        for (int r = col + 1; r < N; ++r) if (fabs(M[r][col]) > best) { best = fabs(M[r][col]); piv = r; }
+        if (piv != col) {
+            for (int s = 0; s < N; ++s) { const double t = M[col][s]; M[col][s] = M[piv][s]; M[piv][s] = t; }
+            const double t = b[col]; b[col] = b[piv]; b[piv] = t;
+        }
+        const double inv = 1.0 / M[col][col];
+        for (int r = col + 1; r < N; ++r) {
+            const double f = M[r][col] * inv;
+            for (int s = col; s < N; ++s) M[r][s] -= f * M[col][s];
+            b[r] -= f * b[col];
+        }
+    }
+    for (int r = N - 1; r >= 0; --r) {
+        double s = b[r];
+        for (int t = r + 1; t < N; ++t) s -= M[r][t] * b[t];
+        b[r] = s / M[r][r];
+    }
+}
+
+// Ubar_upd = Ubar_out + J(P_out)^-T Pbar_out over the interior (zero elsewhere)
+template <int NV>
+__global__ void __launch_bounds__(128) k_adj_cell(Dims d, DevGeom g, Phys ph, khb_fields Pout, khb_fields Pbar_out,
+                                                  khb_fields Ubar_out, double* Ubar_upd, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    ZoneGeom G;
+    load_zone_geom(g, j, i, G);
+    double P[NV], J[NV][NV], y[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) { P[p] = Pout.v[p][c]; y[p] = Pbar_out.v[p][c]; }
+    ptou_jacobian<NV>(G, ph.gam, P, J);
+    solve_transposed<NV>(J, y);
+#pragma unroll
+    for (int p = 0; p < NV; ++p) Ubar_upd[p*d.N + c] = Ubar_out.v[p][c] + y[p];
+}
+
+// Pbar += J(P)^T Ubar over the whole block (the adjoint of U = U(P) of an initial state)
+template <int NV>
+__global__ void __launch_bounds__(128) k_adj_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields Ubar,
+                                                  khb_fields Pbar)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N) return;
+    int k, j, i;
+    zone_kji(d, c, k, j, i);
+    ZoneGeom G;
+    load_zone_geom(g, j, i, G);
+    double Pz[NV], J[NV][NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) Pz[p] = P.v[p][c];
+    ptou_jacobian<NV>(G, ph.gam, Pz, J);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double s = 0.;
+#pragma unroll
+        for (int p = 0; p < NV; ++p) s += J[p][q] * Ubar.v[p][c];
+        Pbar.v[q][c] += s;
+    }
+}
+
+// Ghost-zone adjoints: a zone outside the interior only in periodic directions is a copy of its
+// image, so its adjoint is added to the image; any other ghost zone is the caller's constant.  All
+// ghost adjoints are zeroed afterwards (two launches: fold, then clear).
+template <int NV>
+__global__ void k_adj_fold(Dims d, khb_fields A, int pmask)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    int k, j, i;
+    zone_kji(d, t, k, j, i);
+    const bool gi = i < d.is || i > d.ie, gj = j < d.js || j > d.je, gk = k < d.ks || k > d.ke;
+    if (!(gi || gj || gk)) return;
+    if ((gi && !(pmask & 1)) || (gj && !(pmask & 2)) || (gk && !(pmask & 4))) return;
+    const int ii = gi ? i + ((i < d.is) ? d.nx1 : -d.nx1) : i;
+    const int jj = gj ? j + ((j < d.js) ? d.nx2 : -d.nx2) : j;
+    const int kk = gk ? k + ((k < d.ks) ? d.nx3 : -d.nx3) : k;
+    const long long s = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+#pragma unroll
+    for (int p = 0; p < NV; ++p) atomicAdd(A.v[p] + s, A.v[p][t]);
+}
+template <int NV>
+__global__ void k_adj_clear_ghosts(Dims d, khb_fields A)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.N) return;
+    int k, j, i;
+    zone_kji(d, t, k, j, i);
+    const bool interior = i >= d.is && i <= d.ie && j >= d.js && j <= d.je && k >= d.ks && k <= d.ke;
+    if (interior) return;
+#pragma unroll
+    for (int p = 0; p < NV; ++p) A.v[p][t] = 0.;
+}
+
+// Seed of the objective: Fbar1[RHO] += scale * weight over all faces
+__global__ void k_adj_seed(long long N, const double* weight, double scale, double* F1b)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    const double w = weight[t];
+    if (w != 0.) F1b[t] += scale * w;
+}
+
+} // namespace khb
+
+using namespace khb;
+
+namespace {
+
+#define KHB_ACUDA(call)                                                                                        \
+    do {                                                                                                       \
+        cudaError_t e_ = (call);                                                                               \
+        if (e_ != cudaSuccess) return set_error(KHB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int adj_supported(const khb_ctx* ctx, const char* who)
+{
+    const Dims& d = ctx->d;
+    const std::string w(who);
+    if (ctx->ph.floors_on || ctx->ph.recon_floors) return set_error(KHB_ERR_UNSUPPORTED, w + ": floors are not differentiated");
+    if (ctx->ph.fofc) return set_error(KHB_ERR_UNSUPPORTED, w + ": first-order flux correction is not differentiated");
+    if (ctx->ph.riemann != 0) return set_error(KHB_ERR_UNSUPPORTED, w + ": LLF fluxes only");
+    if (ctx->cfg.recon != KHB_RECON_LINEAR_MC && ctx->cfg.recon != KHB_RECON_DONOR_CELL)
+        return set_error(KHB_ERR_UNSUPPORTED, w + ": linear MC or donor-cell reconstruction only");
+    for (int f = 0; f < 2 * d.ndim; ++f)
+        if (phys_face(d.bc[f])) return set_error(KHB_ERR_UNSUPPORTED, w + ": periodic or exchange faces only");
+    return KHB_OK;
+}
+
+int pmask_of(const Dims& d)
+{
+    int m = 0;
+    if (d.bc[0] == KHB_BC_PERIODIC) m |= 1;
+    if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) m |= 2;
+    if (d.ndim >= 3 && d.bc[4] == KHB_BC_PERIODIC) m |= 4;
+    return m;
+}
+
+khb_fields slice_fields(double* base, long long N, int nv)
+{
+    khb_fields f;
+    std::memset(&f, 0, sizeof(f));
+    for (int p = 0; p < nv; ++p) f.v[p] = base + (size_t)p * N;
+    return f;
+}
+
+template <int NV>
+void fold(const Dims& d, const khb_fields& A, cudaStream_t st)
+{
+    k_adj_fold<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, A, pmask_of(d));
+    k_adj_clear_ghosts<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, A);
+}
+
+template <int DIR, int NV, typename R>
+void adj_flux_dir(const khb_ctx* ctx, const khb_fields& P, const double* Fb, const khb_fields& Pbar, cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    int lo[3], cnt[3];
+    const int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
+    for (int a = 0; a < 3; ++a) {
+        const bool active = (a + 1) <= d.ndim;
+        int hi;
+        if (a + 1 == DIR) { lo[a] = s[a]; hi = e[a] + 1; }
+        else if (active) { lo[a] = s[a] - 1; hi = e[a] + 1; }
+        else { lo[a] = s[a]; hi = e[a]; }
+        cnt[a] = hi - lo[a] + 1;
+    }
+    const Box bx = make_box(lo[0], lo[1], lo[2], cnt[0], cnt[1], cnt[2]);
+    if (ctx->cfg.recon == KHB_RECON_DONOR_CELL)
+        k_adj_flux<DIR, NV, RECON_DONOR, R><<<box_blocks(bx), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Fb, Pbar, bx);
+    else
+        k_adj_flux<DIR, NV, RECON_MC, R><<<box_blocks(bx), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Fb, Pbar, bx);
+}
+
+// Adjoint of one stage.  Pbar_out/Ubar_out are read by the first kernel; with clear_out they are
+// zeroed right after, so that they can receive Ubar_0 (stage 2 passes the caller's arrays both ways).
+// Launches: memset, cell, [clear], [seed], update, ndim flux, 2-3 folds x 2.
+template <int NV>
+int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Pout,
+                     const khb_fields& Pbar_out, const khb_fields& Ubar_out, bool clear_out, const double* weight,
+                     double wscale, const khb_fields& Pbar_s, const khb_fields& Ubar_s, const khb_fields& Ubar_0,
+                     cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    const size_t N = (size_t)d.N;
+    double* Fb[3] = {ctx->adj_buf, ctx->adj_buf + NV * N, ctx->adj_buf + 2 * NV * N};
+    double* Uupd = ctx->adj_buf + 3 * NV * N;
+    KHB_ACUDA(cudaMemsetAsync(ctx->adj_buf, 0, sizeof(double) * 4 * NV * N, st));
+    const Box zb = make_box(d.is, d.js, d.ks, d.ie - d.is + 1, d.je - d.js + 1, d.ke - d.ks + 1);
+    k_adj_cell<NV><<<box_blocks(zb), 128, 0, st>>>(d, ctx->g, ctx->ph, Pout, Pbar_out, Ubar_out, Uupd, zb);
+    if (clear_out)
+        for (int p = 0; p < NV; ++p) {
+            KHB_ACUDA(cudaMemsetAsync(Pbar_out.v[p], 0, sizeof(double) * N, st));
+            KHB_ACUDA(cudaMemsetAsync(Ubar_out.v[p], 0, sizeof(double) * N, st));
+        }
+    if (weight) k_adj_seed<<<blocks_for(d.N, 256), 256, 0, st>>>(d.N, weight, wscale, Fb[0]);
+    const int s = stage - 1;
+    k_adj_update<NV><<<box_blocks(zb), 128, 0, st>>>(d, ctx->g, ctx->ph, Uupd, Ps, kRkGam0[s], kRkGam1[s],
+                                                     kRkBeta[s] * dt, Fb[0], Fb[1], Fb[2], Pbar_s, Ubar_s, Ubar_0, zb);
+    for (int dir = 1; dir <= d.ndim; ++dir) {
+        if (ctx->fp32) {
+            if (dir == 1) adj_flux_dir<1, NV, float>(ctx, Ps, Fb[0], Pbar_s, st);
+            else if (dir == 2) adj_flux_dir<2, NV, float>(ctx, Ps, Fb[1], Pbar_s, st);
+            else adj_flux_dir<3, NV, float>(ctx, Ps, Fb[2], Pbar_s, st);
+        } else {
+            if (dir == 1) adj_flux_dir<1, NV, double>(ctx, Ps, Fb[0], Pbar_s, st);
+            else if (dir == 2) adj_flux_dir<2, NV, double>(ctx, Ps, Fb[1], Pbar_s, st);
+            else adj_flux_dir<3, NV, double>(ctx, Ps, Fb[2], Pbar_s, st);
+        }
+    }
+    fold<NV>(d, Pbar_s, st);
+    fold<NV>(d, Ubar_s, st);
+    if (Ubar_0.v[0] != Ubar_s.v[0]) fold<NV>(d, Ubar_0, st);
+    KHB_ACUDA(cudaGetLastError());
+    ctx->launches += 4 + d.ndim + (weight ? 1 : 0) + (clear_out ? 2 * NV : 0) + 2 * (Ubar_0.v[0] != Ubar_s.v[0] ? 3 : 2);
+    return KHB_OK;
+}
+
+template <int NV>
+int adjoint_step_nv(khb_ctx* ctx, double dt, const khb_fields& Pn, const khb_fields& Pstar,
+                    const khb_fields& Pnp1, const khb_fields& Pbar, const khb_fields& Ubar, const double* weight,
+                    double wscale, cudaStream_t st)
+{
+    const size_t N = (size_t)ctx->d.N;
+    const khb_fields Pbar_star = slice_fields(ctx->adj_buf + 4 * NV * N, ctx->d.N, NV);
+    const khb_fields Ubar_star = slice_fields(ctx->adj_buf + 5 * NV * N, ctx->d.N, NV);
+    KHB_ACUDA(cudaMemsetAsync(ctx->adj_buf + 4 * NV * N, 0, sizeof(double) * 2 * NV * N, st));
+    ctx->launches += 1;
+    int rc;
+    // stage 2: (P*, U*, U^n) -> (P^{n+1}, U^{n+1}); the caller's arrays turn into the adjoint of U^n
+    if ((rc = adjoint_stage_nv<NV>(ctx, 2, dt, Pstar, Pnp1, Pbar, Ubar, true, weight, wscale, Pbar_star, Ubar_star,
+                                   Ubar, st)))
+        return rc;
+    // stage 1: (P^n, U^n, U^n) -> (P*, U*)
+    return adjoint_stage_nv<NV>(ctx, 1, dt, Pn, Pstar, Pbar_star, Ubar_star, false, weight, wscale, Pbar, Ubar, Ubar,
+                                st);
+}
+
+} // namespace
+
+extern "C" {
+
+int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_fields* U_n,
+                     const khb_fields* P_np1, const khb_fields* Pbar, const khb_fields* Ubar,
+                     const double* rho_flux1_weight, double weight_scale, void* stream)
+{
+    if (!ctx || !ctx->geom_set) return set_error(KHB_ERR_STATE, "khb_adjoint_step: context without geometry");
+    if (!P_n || !U_n || !P_np1 || !Pbar || !Ubar) return set_error(KHB_ERR_ARG, "khb_adjoint_step: NULL argument");
+    for (int p = 0; p < ctx->nv; ++p)
+        if (!P_n->v[p] || !U_n->v[p] || !P_np1->v[p] || !Pbar->v[p] || !Ubar->v[p])
+            return set_error(KHB_ERR_ARG, "khb_adjoint_step: NULL variable pointer");
+    if (!(dt > 0.)) return set_error(KHB_ERR_ARG, "khb_adjoint_step: dt must be positive");
+    int rc;
+    if ((rc = adj_supported(ctx, "khb_adjoint_step"))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const Dims& d = ctx->d;
+    if (!ctx->adj_buf) {
+        KHB_ACUDA(cudaMalloc((void**)&ctx->adj_buf, sizeof(double) * 6 * ctx->nv * (size_t)d.N));
+        KHB_ACUDA(cudaMalloc((void**)&ctx->adj_flags, sizeof(int32_t) * 2 * (size_t)d.N));
+        KHB_ACUDA(cudaMemset(ctx->adj_flags, 0, sizeof(int32_t) * 2 * (size_t)d.N));
+        KHB_ACUDA(cudaDeviceSynchronize());
+    }
+    // recompute the intermediate stage (P*, U*) into the context's stage scratch
+    const khb_fields Pstar = slice_fields(ctx->stageP, d.N, ctx->nv), Ustar = slice_fields(ctx->stageU, d.N, ctx->nv);
+    if ((rc = khb_stage(ctx, 1, dt, P_n, U_n, U_n, &Pstar, &Ustar, ctx->adj_flags, ctx->adj_flags + d.N, stream)))
+        return rc;
+    if (ctx->nv == 8) return adjoint_step_nv<8>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, st);
+    return adjoint_step_nv<5>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, st);
+}
+
+int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, const khb_fields* Pbar, void* stream)
+{
+    if (!ctx || !ctx->geom_set) return set_error(KHB_ERR_STATE, "khb_adjoint_ptou: context without geometry");
+    if (!P || !Ubar || !Pbar) return set_error(KHB_ERR_ARG, "khb_adjoint_ptou: NULL argument");
+    for (int p = 0; p < ctx->nv; ++p)
+        if (!P->v[p] || !Ubar->v[p] || !Pbar->v[p]) return set_error(KHB_ERR_ARG, "khb_adjoint_ptou: NULL variable pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Dims& d = ctx->d;
+    if (ctx->nv == 8) k_adj_ptou<8><<<blocks_for(d.N, 128), 128, 0, st>>>(d, ctx->g, ctx->ph, *P, *Ubar, *Pbar);
+    else k_adj_ptou<5><<<blocks_for(d.N, 128), 128, 0, st>>>(d, ctx->g, ctx->ph, *P, *Ubar, *Pbar);
+    KHB_ACUDA(cudaGetLastError());
+    ctx->launches += 1;
+    return KHB_OK;
+}
+
+} // extern "C"

@@ -47,6 +47,10 @@ struct khb_ctx {
     int32_t* graph_pflag;
     int32_t* graph_fflag;
     int64_t graph_launches;
+    // adjoint scratch (khb_adjoint_step): face-flux adjoints [3][nv][N], the updated-state adjoint
+    // [nv][N] and the intermediate stage's adjoints [2][nv][N]; flags of the recomputed stage [2][N]
+    double* adj_buf;
+    int32_t* adj_flags;
 };
 
 
