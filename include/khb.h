@@ -294,6 +294,12 @@ int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_f
                      const khb_fields* P_np1, const khb_fields* Pbar, const khb_fields* Ubar,
                      const double* rho_flux1_weight, double weight_scale, void* stream);
 
+/* *out += scale * sum_f weight[f] * F_dir[var][f] over the raw face fluxes left in the context's
+ * scratch by the last khb_stage / khb_get_flux (the objective whose adjoint khb_adjoint_step seeds
+ * for var = rho, dir = 1).  weight: [N] device doubles indexed like the zone arrays; out: one device
+ * double.  Summed in a fixed order (reproducible).  Launches only. */
+int khb_flux_dot(khb_ctx* ctx, int dir, int var, const double* weight, double scale, double* out, void* stream);
+
 /* Pbar += (dU/dP)^T Ubar at every zone of P (the adjoint of Flux::p_to_u, flux_functions.hpp:343-352,
  * e.g. of the conserved initial state formed from primitive initial data). */
 int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, const khb_fields* Pbar,

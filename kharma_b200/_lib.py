@@ -126,6 +126,7 @@ SIGNATURES = {
     "khb_adjoint_step": (_I, [_P, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
                               C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _D, _P]),
     "khb_adjoint_ptou": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
+    "khb_flux_dot": (_I, [_P, _I, _I, _P, _D, _P, _P]),
     "khb_max_divb": (_I, [_P, C.POINTER(KhbFields), C.POINTER(_D), _P]),
     "khb_launch_count": (C.c_int64, [_P]),
     "khb_set_tuning": (_I, [_P, C.c_char_p, _I]),

@@ -52,25 +52,24 @@ class Run:
                                       C.c_void_p(b.pflag.data_ptr()), C.c_void_p(b.fflag.data_ptr()), b.stream),
                    "khb_stage")
 
-    def _mass_flux(self):
-        """sum_f weight[f] * F1[rho][f] of the fluxes the last stage left in scratch (device scalar)."""
-        F, _ = self.b.copy_flux(1)
-        return (self.weight * F[0].reshape(-1)).sum()
+    def _mass_flux(self, J, scale):
+        """J += scale * sum_f weight[f] * F1[rho][f] of the fluxes the last stage left in scratch."""
+        if self.weight is not None and J is not None:
+            _lib.check(self.lib.khb_flux_dot(self.b.ctx, 1, 0, C.c_void_p(self.weight.data_ptr()), float(scale),
+                                             C.c_void_p(J.data_ptr()), self.b.stream), "khb_flux_dot")
 
-    def _step(self, dt, fails=None):
-        """One step in place on the block's (P, U); returns its objective contribution (device scalar).
-        fails: a device counter that receives the number of failed inversions of both stages."""
+    def _step(self, dt, fails=None, J=None):
+        """One step in place on the block's (P, U), adding its objective contribution to J (a device
+        double).  fails: a device counter that receives the number of failed inversions of both stages."""
         b = self.b
         self._stage(1, dt, b.Pf, b.Uf, b.Uf, self.Psf, self.Usf)
         if fails is not None:
             fails += (b.pflag != 0).sum()
-        j = self._mass_flux() * (0.5 * dt) if self.weight is not None else None
+        self._mass_flux(J, 0.5 * dt)
         self._stage(2, dt, self.Psf, self.Usf, b.Uf, b.Pf, b.Uf)
         if fails is not None:
             fails += (b.pflag != 0).sum()
-        if self.weight is not None:
-            j = j + self._mass_flux() * (0.5 * dt)
-        return j
+        self._mass_flux(J, 0.5 * dt)
 
     def forward(self):
         """Run all steps from the block's current state; returns J (a Python float)."""
@@ -81,9 +80,7 @@ class Run:
         for n, dt in enumerate(self.dts):
             if n % self.K == 0:
                 self.checkpoints.append((b.P.clone(), b.U.clone()))
-            j = self._step(dt, fails)
-            if j is not None:
-                J = J + j
+            self._step(dt, fails, J)
         if int(fails.item()):
             raise NotDifferentiable(f"{int(fails.item())} zone inversions failed: fixups are not differentiated")
         if self.Pw is not None:

@@ -429,6 +429,38 @@ __global__ void k_adj_seed(long long N, const double* weight, double scale, doub
     if (w != 0.) F1b[t] += scale * w;
 }
 
+// Deterministic sum_f w[f] * F[f] (times scale) added to *out: fixed-size grid of partial sums,
+// then one block adds them in order.
+constexpr int kDotBlocks = 592, kDotThreads = 256;
+template <typename FT>
+__global__ void __launch_bounds__(kDotThreads) k_flux_dot_partial(long long N, const FT* F, const double* w,
+                                                                  double* partial)
+{
+    double s = 0.;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const double ww = w[t];
+        if (ww != 0.) s += ww * (double)F[t];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double ws[kDotThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.;
+        for (int i = 0; i < kDotThreads / 32; ++i) t += ws[i];
+        partial[blockIdx.x] = t;
+    }
+}
+__global__ void k_flux_dot_final(const double* partial, int n, double scale, double* out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double t = 0.;
+        for (int i = 0; i < n; ++i) t += partial[i];
+        *out += scale * t;
+    }
+}
+
 } // namespace khb
 
 using namespace khb;
@@ -594,6 +626,29 @@ int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_f
         return rc;
     if (ctx->nv == 8) return adjoint_step_nv<8>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, st);
     return adjoint_step_nv<5>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, st);
+}
+
+int khb_flux_dot(khb_ctx* ctx, int dir, int var, const double* weight, double scale, double* out, void* stream)
+{
+    if (!ctx || !weight || !out) return set_error(KHB_ERR_ARG, "khb_flux_dot: NULL argument");
+    if (dir < 1 || dir > ctx->d.ndim) return set_error(KHB_ERR_ARG, "khb_flux_dot: inactive direction");
+    if (var < 0 || var >= ctx->nv) return set_error(KHB_ERR_ARG, "khb_flux_dot: bad variable");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long N = ctx->d.N;
+    if (!ctx->adj_red) {
+        KHB_ACUDA(cudaMalloc((void**)&ctx->adj_red, sizeof(double) * kDotBlocks));
+        KHB_ACUDA(cudaDeviceSynchronize());
+    }
+    if (ctx->fp32)
+        k_flux_dot_partial<float><<<kDotBlocks, kDotThreads, 0, st>>>(N, (const float*)ctx->F[dir - 1] + (size_t)var * N,
+                                                                      weight, ctx->adj_red);
+    else
+        k_flux_dot_partial<double><<<kDotBlocks, kDotThreads, 0, st>>>(N, (const double*)ctx->F[dir - 1] + (size_t)var * N,
+                                                                       weight, ctx->adj_red);
+    k_flux_dot_final<<<1, 32, 0, st>>>(ctx->adj_red, kDotBlocks, scale, out);
+    KHB_ACUDA(cudaGetLastError());
+    ctx->launches += 2;
+    return KHB_OK;
 }
 
 int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, const khb_fields* Pbar, void* stream)

@@ -415,7 +415,7 @@ int khb_destroy(khb_ctx* c)
     cudaFree(c->dudt10);
     cudaFree(c->fofc_flag);
     cudaFree(c->dt_state);
-    cudaFree(c->adj_buf); cudaFree(c->adj_flags);
+    cudaFree(c->adj_buf); cudaFree(c->adj_flags); cudaFree(c->adj_red);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->graph) cudaGraphDestroy(c->graph);
     delete c;

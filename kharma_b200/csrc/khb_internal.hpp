@@ -51,6 +51,7 @@ struct khb_ctx {
     // [nv][N] and the intermediate stage's adjoints [2][nv][N]; flags of the recomputed stage [2][N]
     double* adj_buf;
     int32_t* adj_flags;
+    double* adj_red;       // partial sums of khb_flux_dot
 };
 
 

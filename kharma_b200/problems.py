@@ -386,3 +386,23 @@ def bondi(spec, geom, rs=8.0, mdot=1.0):
     for p, val in enumerate((rho, u, uprim[0], uprim[1], uprim[2])):
         P[p] = val[None, :, :]
     return P
+
+
+# ------------------------------------------------------------------------ derivative-check states
+def add_ramps(spec, P, frac=0.05, seed=9):
+    """P_q + amp_q (a x1' + b x2' + c x3'), x' the native coordinates normalised to [-1/2, 1/2] over the
+    interior, seeded a, b, c in [1/2, 3/2], amp_q = frac times the variable's mean magnitude (1e-3 for
+    a variable that is zero).  A state with no flat neighbourhood in any variable or direction: at a
+    flat neighbourhood the MC-limited slope is not differentiable, so derivative checks start here."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    x1, x2, x3 = cell_centers(spec)
+    nrm = lambda x, lo, hi: (x - 0.5 * (lo + hi)) / (hi - lo)
+    X3, X2, X1 = np.meshgrid(nrm(x3, spec.x3min, spec.x3max), nrm(x2, spec.x2min, spec.x2max),
+                             nrm(x1, spec.x1min, spec.x1max), indexing="ij")
+    sc = np.abs(P).mean(axis=(1, 2, 3))
+    amp = np.where(sc > 1e-12, frac * sc, 1e-3)
+    P = P.copy()
+    for q in range(P.shape[0]):
+        a, b, c = rng.uniform(0.5, 1.5, 3)
+        P[q] += amp[q] * (a * X1 + (b * X2 if spec.nx2 > 1 else 0) + (c * X3 if spec.nx3 > 1 else 0))
+    return P

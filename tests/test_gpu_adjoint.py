@@ -89,22 +89,8 @@ def directions(spec, P0, n, seed):
     return out
 
 
-def ramps(spec, P, seed=9):
-    """P_q + amp_q (a x1' + b x2' + c x3') with x' the native coordinates normalised to [-1/2, 1/2]
-    over the interior, seeded a, b, c in [1/2, 3/2], amp_q 5% of the variable's mean magnitude (1e-3
-    for a variable that is zero)."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    x1, x2, x3 = cell_centers(spec)
-    nrm = lambda x, lo, hi: (x - 0.5 * (lo + hi)) / (hi - lo)
-    X3, X2, X1 = np.meshgrid(nrm(x3, spec.x3min, spec.x3max), nrm(x2, spec.x2min, spec.x2max),
-                             nrm(x1, spec.x1min, spec.x1max), indexing="ij")
-    sc = np.abs(P).mean(axis=(1, 2, 3))
-    amp = np.where(sc > 1e-12, 0.05 * sc, 1e-3)
-    P = P.copy()
-    for q in range(spec.nvar):
-        a, b, c = rng.uniform(0.5, 1.5, 3)
-        P[q] += amp[q] * (a * X1 + (b * X2 if spec.nx2 > 1 else 0) + (c * X3 if spec.nx3 > 1 else 0))
-    return P
+def ramps(spec, P):
+    return problems.add_ramps(spec, P)
 
 
 def check_fd(block, P0, dts, weight, Pw, ndir, seed, eps=(1e-6, 1e-7, 1e-8), tol=1e-5):
