@@ -97,7 +97,14 @@ typedef struct {
      * the event-horizon radius of the coordinates (0 without one, coordinate_embedding.hpp:247-258) */
     int32_t fofc, fofc_polar_cells;
     double fofc_eh_buffer, r_horizon;
+    /* magnetic field transport: KHB_CT_NONE is B_FluxCT (cell-centred B, flux-CT); the others are
+     * B_CT (face-centred B, edge EMFs, b_field/ct_scheme, b_ct.cpp:65-67) and need the khb_ct_* calls */
+    int32_t ct_scheme;
 } khb_config;
+
+/* B_CT EMF schemes (b_ct.cpp:65): Balsara & Spicer 1999 flux averaging, Gardiner & Stone 2005
+ * with the zone-centred EMF (E^0), and with upwinded E^c corrections (also "sg07") */
+enum { KHB_CT_NONE = 0, KHB_CT_BS99 = 1, KHB_CT_GS05_0 = 2, KHB_CT_GS05_C = 3 };
 
 /* Coordinate system for khb_build_geometry (coordinates/coordinate_systems.hpp) */
 enum { KHB_BASE_CART_MINKOWSKI = 0, KHB_BASE_SPH_MINKOWSKI = 1, KHB_BASE_SPH_KS = 2, KHB_BASE_SPH_BL = 3 };
@@ -304,6 +311,40 @@ int khb_flux_dot(khb_ctx* ctx, int dir, int var, const double* weight, double sc
  * e.g. of the conserved initial state formed from primitive initial data). */
 int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, const khb_fields* Pbar,
                      void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * B_CT: face-centred magnetic field (cfg.ct_scheme != KHB_CT_NONE; 2D and 3D blocks with periodic or
+ * exchange faces).  Face fields are passed as khb_fields with v[0..2] = the conserved sqrt(-g) B^1,
+ * B^2, B^3 on x1, x2, x3 faces, each [n3][n2][n1] like the zone arrays, face i being the left face
+ * of zone i (faces of the interior, [is, ie+1] along their own direction, are the state; the cell
+ * B slots of P and U are derived from them).
+ * ------------------------------------------------------------------------------------------- */
+
+/* One RK2 stage with B_CT (kharma_step.cpp:163-214 with use_b_ct): fluxes, FixFlux, then
+ * B_CT::CalculateEMF (b_ct.cpp:262-410: zone-centred EMF, edge EMFs by the configured scheme),
+ * B_CT::AddSource (b_ct.cpp:412-470: face changes from the EMF circulation) and the face update
+ * Bf_out = gam0 Bf_s + gam1 Bf_0 + beta dt dBf/dt (kharma_driver.cpp:339-387, WeightedSumDataFace),
+ * then the zone pass with the zone B taken from the updated faces (B_CT::BlockUtoP,
+ * b_ct.cpp:160-188) instead of the flux-CT divergence, fixups and ghost zones as khb_stage. */
+int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+                 const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
+                 const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream);
+
+/* Full RK2 step with B_CT in place on (P, U, Bf), the intermediate stage in context scratch. */
+int khb_ct_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
+                int32_t* pflag, int32_t* fflag, void* stream);
+
+/* B_CT::BlockUtoP (b_ct.cpp:160-188) over the interior: zone B^i (P slots 5-7) as the average of the
+ * two faces' B^i, zone sqrt(-g) B^i (U slots 5-7) from it.  Ghost zones: khb_boundaries. */
+int khb_ct_utop(khb_ctx* ctx, const khb_fields* Bf, const khb_fields* P, const khb_fields* U, void* stream);
+
+/* B_CT::DangerousPtoU (b_ct.cpp:190-253): interior faces from the zone B of P (average of the two
+ * zones times sqrt(-g) at the face), e.g. to start from cell-centred initial data. */
+int khb_ct_faces_from_prims(khb_ctx* ctx, const khb_fields* P, const khb_fields* Bf, void* stream);
+
+/* B_CT::BlockMaxDivB (b_ct.cpp:499-520, face_div b_ct_functions.hpp:47-56): max over the interior of
+ * |sum_d (Bf_d(+) - Bf_d(-)) / dx_d|.  Synchronizes the stream. */
+int khb_ct_max_divb(khb_ctx* ctx, const khb_fields* Bf, double* max_divb_host, void* stream);
 
 /* B_FluxCT::MaxDivB (b_flux_ct.cpp:566-607): max |corner divB| of the conserved field.
  * Synchronizes the stream. */

@@ -20,6 +20,7 @@ BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 PREC = {"fp64": 0, "fp32_flux": 1}
 INVERTER = {"onedw": 0, "kastaun": 1}
+CT_SCHEME = {"none": 0, "bs99": 1, "gs05_0": 2, "gs05_c": 3, "sg07": 3}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
 TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
 CLOSURE = {"constant": 0, "soundspeed": 1, "sound_speed": 1, "kappa_eta": 2, "torus": 3}
@@ -60,6 +61,7 @@ class KhbConfig(C.Structure):
         ("inverter", C.c_int32),
         ("fofc", C.c_int32), ("fofc_polar_cells", C.c_int32),
         ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
+        ("ct_scheme", C.c_int32),
     ]
 
 
@@ -127,6 +129,11 @@ SIGNATURES = {
                               C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _D, _P]),
     "khb_adjoint_ptou": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
     "khb_flux_dot": (_I, [_P, _I, _I, _P, _D, _P, _P]),
+    "khb_ct_stage": (_I, [_P, _I, _D] + [C.POINTER(KhbFields)] * 8 + [_P, _P, _P]),
+    "khb_ct_step": (_I, [_P, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_ct_utop": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
+    "khb_ct_faces_from_prims": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
+    "khb_ct_max_divb": (_I, [_P, C.POINTER(KhbFields), C.POINTER(_D), _P]),
     "khb_max_divb": (_I, [_P, C.POINTER(KhbFields), C.POINTER(_D), _P]),
     "khb_launch_count": (C.c_int64, [_P]),
     "khb_set_tuning": (_I, [_P, C.c_char_p, _I]),

@@ -68,6 +68,11 @@ class Block:
         self.fflag = torch.zeros(spec.shape, dtype=torch.int32, device=self.device)
         self.Pf = Fields(self.P)
         self.Uf = Fields(self.U)
+        # B_CT: the face-centred field sqrt(-g) B^d on the x_d faces, (3, n3, n2, n1)
+        self.ct = spec.b_ct != "none"
+        if self.ct:
+            self.Bf = torch.zeros((3,) + spec.shape, dtype=torch.float64, device=self.device)
+            self.Bff = Fields(self.Bf)
 
     def _set_geometry(self, g):
         arrs = [np.ascontiguousarray(g[k], dtype=np.float64) for k in ("gcov", "gcon", "gdet", "gdet_conn", "r_center")]
@@ -87,12 +92,22 @@ class Block:
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 
     # ------------------------------------------------------------- state
-    def set_prims(self, P_host):
-        """Load primitives (interior at least), fill ghost zones and set U = U(P) everywhere."""
+    def set_prims(self, P_host, faces=None):
+        """Load primitives (interior at least), fill ghost zones and set U = U(P) everywhere.  A B_CT
+        block also sets its face field: `faces` (3, n3, n2, n1) if given, else interpolated from the
+        zone B (khb_ct_faces_from_prims); the zone B is then rebuilt from the faces."""
         self.P.copy_(torch.as_tensor(P_host, dtype=torch.float64))
         # ghost B_P is rebuilt from B_U by the boundary call: seed B_U = B_P sqrt(-g) first
         self.ptou()
         self.boundaries()
+        if self.ct:
+            if faces is None:
+                _lib.check(self.lib.khb_ct_faces_from_prims(self.ctx, self.Pf.ref, self.Bff.ref, self.stream),
+                           "khb_ct_faces_from_prims")
+            else:
+                self.Bf.copy_(torch.as_tensor(faces, dtype=torch.float64))
+            _lib.check(self.lib.khb_ct_utop(self.ctx, self.Bff.ref, self.Pf.ref, self.Uf.ref, self.stream), "khb_ct_utop")
+            self.boundaries()
         self.ptou()
 
     def ptou(self):
@@ -104,6 +119,11 @@ class Block:
     # ------------------------------------------------------------- stepping
     def step(self, dt):
         """One RK2 step in place (launch only)."""
+        if self.ct:
+            _lib.check(self.lib.khb_ct_step(self.ctx, float(dt), self.Pf.ref, self.Uf.ref, self.Bff.ref,
+                                            C.c_void_p(self.pflag.data_ptr()), C.c_void_p(self.fflag.data_ptr()),
+                                            self.stream), "khb_ct_step")
+            return
         _lib.check(self.lib.khb_step(self.ctx, float(dt), self.Pf.ref, self.Uf.ref,
                                      C.c_void_p(self.pflag.data_ptr()), C.c_void_p(self.fflag.data_ptr()),
                                      self.stream), "khb_step")
@@ -116,6 +136,9 @@ class Block:
 
     def max_divb(self):
         out = C.c_double()
+        if self.ct:
+            _lib.check(self.lib.khb_ct_max_divb(self.ctx, self.Bff.ref, C.byref(out), self.stream), "khb_ct_max_divb")
+            return out.value
         _lib.check(self.lib.khb_max_divb(self.ctx, self.Uf.ref, C.byref(out), self.stream), "khb_max_divb")
         return out.value
 

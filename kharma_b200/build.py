@@ -29,6 +29,7 @@ UNITS = {
     "khb_noalloc.cu": ["-fmad=false"],
     "khb_emhd.cu": ["-fmad=false"],
     "khb_adjoint.cu": ["-fmad=false"],
+    "khb_ct.cu": ["-fmad=false"],
     "khb_geometry.cpp": [],
 }
 HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", "khb_internal.hpp", "khb_dual.cuh", os.path.join("..", "..", "include", "khb.h")]

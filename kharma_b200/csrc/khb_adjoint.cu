@@ -479,6 +479,7 @@ int adj_supported(const khb_ctx* ctx, const char* who)
     const std::string w(who);
     if (ctx->ph.floors_on || ctx->ph.recon_floors) return set_error(KHB_ERR_UNSUPPORTED, w + ": floors are not differentiated");
     if (ctx->ph.fofc) return set_error(KHB_ERR_UNSUPPORTED, w + ": first-order flux correction is not differentiated");
+    if (ctx->ph.ct_scheme) return set_error(KHB_ERR_UNSUPPORTED, w + ": B_CT is not differentiated");
     if (ctx->ph.riemann != 0) return set_error(KHB_ERR_UNSUPPORTED, w + ": LLF fluxes only");
     if (ctx->cfg.recon != KHB_RECON_LINEAR_MC && ctx->cfg.recon != KHB_RECON_DONOR_CELL)
         return set_error(KHB_ERR_UNSUPPORTED, w + ": linear MC or donor-cell reconstruction only");

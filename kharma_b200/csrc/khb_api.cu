@@ -142,6 +142,7 @@ void launch_zone_t(khb_ctx* ctx, const ZoneCall& zc, cudaStream_t st)
     a.fail_count = ctx->fail_count;
     a.fail_list = ctx->fail_list;
     a.mode = zc.mode;
+    for (int x = 0; x < 3; ++x) a.Bf[x] = ctx->ct_active ? ctx->ct_bf[x] : nullptr;
     Launch<FT>::zone(ctx->nv, ctx->d, ctx->g, ctx->ph, a, st);
 }
 
@@ -149,6 +150,7 @@ int launch_zone(khb_ctx* ctx, const ZoneCall& zc_in, cudaStream_t st)
 {
     ZoneCall zc = zc_in;
     if ((zc.mode & M_UTOP) && ctx->ph.inverter == KHB_INVERTER_KASTAUN) zc.mode |= M_KASTAUN;
+    if (ctx->ct_active && (zc.mode & (M_UPDATE | M_UTOP))) zc.mode |= M_BCT;
     if (ctx->fp32) launch_zone_t<float>(ctx, zc, st); else launch_zone_t<double>(ctx, zc, st);
     KHB_LAUNCHED(ctx);
     return KHB_OK;
@@ -273,6 +275,28 @@ int do_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb
     return launch_boundaries(ctx, Pout, Uout, st);
 }
 
+// One stage of a B_CT block: fluxes and their fixes, edge EMFs and the face update, then the zone pass
+// with the zone B from the new faces (M_BCT), fixups and ghost zones
+int do_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+                const khb_fields& U0, const khb_fields& Bs, const khb_fields& B0, const khb_fields& Pout,
+                const khb_fields& Uout, const khb_fields& Bout, int32_t* pflag, int32_t* fflag, cudaStream_t st)
+{
+    int rc;
+    for (int dir = 1; dir <= ctx->d.ndim; ++dir)
+        if ((rc = launch_flux(ctx, dir, Ps, st))) return rc;
+    if ((rc = launch_fix_flux(ctx, ctx->ph, st))) return rc;
+    if ((rc = khb::ct_emf(ctx, Ps, st))) return rc;
+    if ((rc = khb::ct_face_update(ctx, stage, dt, Bs, B0, Bout, st))) return rc;
+    if ((rc = launch_ghost_copy(ctx, Ps, Us, Pout, Uout, st))) return rc;
+    for (int x = 0; x < 3; ++x) ctx->ct_bf[x] = Bout.v[x];
+    ctx->ct_active = true;
+    rc = zone_pass(ctx, stage, dt, Ps, Us, U0, Pout, Uout, pflag, fflag, st);
+    ctx->ct_active = false;
+    if (rc) return rc;
+    if ((rc = launch_fixup(ctx, Pout, Uout, pflag, st))) return rc;
+    return launch_boundaries(ctx, Pout, Uout, st);
+}
+
 } // namespace
 
 int khb::set_error(int code, const std::string& msg) { return fail(code, msg); }
@@ -344,6 +368,15 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
     ph.fofc_polar_cells = cfg->fofc_polar_cells;
     ph.fofc_r_mark = cfg->r_horizon + cfg->fofc_eh_buffer;
     if (cfg->fofc && cfg->fofc_polar_cells < 0) { *why = "fofc_polar_cells must be >= 0"; return KHB_ERR_ARG; }
+    if (cfg->ct_scheme < KHB_CT_NONE || cfg->ct_scheme > KHB_CT_GS05_C) { *why = "unknown ct_scheme"; return KHB_ERR_ARG; }
+    if (cfg->ct_scheme != KHB_CT_NONE) {
+        if (cfg->nvar != 8) { *why = "B_CT needs the magnetic field (nvar 8)"; return KHB_ERR_UNSUPPORTED; }
+        if (d.ndim < 2) { *why = "B_CT blocks are 2D or 3D"; return KHB_ERR_UNSUPPORTED; }
+        for (int f = 0; f < 2 * d.ndim; ++f)
+            if (phys_face(cfg->bc[f])) { *why = "B_CT blocks have periodic or exchange faces only"; return KHB_ERR_UNSUPPORTED; }
+        if (cfg->fofc) { *why = "FOFC with B_CT is not supported"; return KHB_ERR_UNSUPPORTED; }
+    }
+    ph.ct_scheme = cfg->ct_scheme;
     std::memcpy(&ph.fl, &cfg->floors, sizeof(khb_floors));
     return KHB_OK;
 }
@@ -392,6 +425,8 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     if (e == cudaSuccess) e = alloc((void**)&c->fail_list, sizeof(int) * N);
     if (e == cudaSuccess) e = alloc((void**)&c->imp_words, sizeof(unsigned long long) * IMP_WORDS);
     if (e == cudaSuccess && cfg->fofc) e = alloc((void**)&c->fofc_flag, sizeof(int32_t) * N);
+    if (e == cudaSuccess && cfg->ct_scheme) e = alloc(&c->ct_emfc, fs * 3 * N);
+    if (e == cudaSuccess && cfg->ct_scheme) e = alloc((void**)&c->ct_stageBf, sizeof(double) * 3 * N);
     // the memsets above run on the legacy default stream, which the caller's (non-blocking) streams
     // do not wait for: finish them before the context is handed out
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -416,6 +451,7 @@ int khb_destroy(khb_ctx* c)
     cudaFree(c->fofc_flag);
     cudaFree(c->dt_state);
     cudaFree(c->adj_buf); cudaFree(c->adj_flags); cudaFree(c->adj_red);
+    cudaFree(c->ct_emfc); cudaFree(c->ct_stageBf);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->graph) cudaGraphDestroy(c->graph);
     delete c;
@@ -641,6 +677,7 @@ int khb_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const k
               int32_t* pflag, int32_t* fflag, void* stream)
 {
     KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_stage: a B_CT block steps with khb_ct_stage/khb_ct_step");
     if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_stage: stage must be 1 or 2");
     int rc;
     if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
@@ -655,6 +692,7 @@ int khb_zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, con
                   int32_t* pflag, int32_t* fflag, void* stream)
 {
     KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_zone_pass: a B_CT block steps with khb_ct_stage/khb_ct_step");
     if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_zone_pass: stage must be 1 or 2");
     int rc;
     if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
@@ -677,6 +715,7 @@ int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
              int32_t* pflag, int32_t* fflag, void* stream)
 {
     KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step: a B_CT block steps with khb_ct_stage/khb_ct_step");
     int rc;
     if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
     if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_step: NULL flags");
@@ -688,6 +727,43 @@ int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
     }
     if ((rc = do_stage(ctx, 1, dt, *P, *U, *U, P1, U1, pflag, fflag, S(stream)))) return rc;
     return do_stage(ctx, 2, dt, P1, U1, *U, *P, *U, pflag, fflag, S(stream));
+}
+
+int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+                 const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
+                 const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_stage: block is not B_CT (cfg.ct_scheme)");
+    if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_ct_stage: stage must be 1 or 2");
+    int rc;
+    if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
+        (rc = check_fields(ctx, U_0, "U_0")) || (rc = check_fields(ctx, P_out, "P_out")) ||
+        (rc = check_fields(ctx, U_out, "U_out"))) return rc;
+    for (const khb_fields* f : {Bf_s, Bf_0, Bf_out})
+        if (!f || !f->v[0] || !f->v[1] || !f->v[2]) return fail(KHB_ERR_ARG, "khb_ct_stage: NULL face field");
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_ct_stage: NULL flags");
+    return do_ct_stage(ctx, stage, dt, *P_s, *U_s, *U_0, *Bf_s, *Bf_0, *P_out, *U_out, *Bf_out, pflag, fflag, S(stream));
+}
+
+int khb_ct_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
+                int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_step: block is not B_CT (cfg.ct_scheme)");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
+    if (!Bf || !Bf->v[0] || !Bf->v[1] || !Bf->v[2]) return fail(KHB_ERR_ARG, "khb_ct_step: NULL face field");
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_ct_step: NULL flags");
+    khb_fields P1, U1, B1;
+    std::memset(&P1, 0, sizeof(P1)); std::memset(&U1, 0, sizeof(U1)); std::memset(&B1, 0, sizeof(B1));
+    for (int p = 0; p < ctx->nv; ++p) {
+        P1.v[p] = ctx->stageP + (size_t)p*ctx->d.N;
+        U1.v[p] = ctx->stageU + (size_t)p*ctx->d.N;
+    }
+    for (int x = 0; x < 3; ++x) B1.v[x] = ctx->ct_stageBf + (size_t)x*ctx->d.N;
+    if ((rc = do_ct_stage(ctx, 1, dt, *P, *U, *U, *Bf, *Bf, P1, U1, B1, pflag, fflag, S(stream)))) return rc;
+    return do_ct_stage(ctx, 2, dt, P1, U1, *U, B1, *Bf, *P, *U, *Bf, pflag, fflag, S(stream));
 }
 
 int khb_set_timestep(khb_ctx* ctx, double dt, double cfl, double dt_min, double max_dt_increase)
@@ -718,6 +794,7 @@ int khb_step_device_dt(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, i
                        void* stream)
 {
     KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_device_dt: a B_CT block steps with khb_ct_stage/khb_ct_step");
     if (!ctx->dt_state) return fail(KHB_ERR_STATE, "khb_step_device_dt: no device timestep (khb_set_timestep)");
     int rc;
     if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
@@ -742,6 +819,7 @@ int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32
                    void* stream)
 {
     KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_graph: a B_CT block steps with khb_ct_stage/khb_ct_step");
     cudaStream_t st = S(stream);
     if (!st) return fail(KHB_ERR_ARG, "khb_step_graph: needs a non-default stream to capture");
     if (!P || !U || !pflag || !fflag) return fail(KHB_ERR_ARG, "khb_step_graph: NULL argument");
@@ -990,6 +1068,7 @@ int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit
                    void* stream)
 {
     KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: EMHD with B_CT is not supported");
     int rc;
     if ((rc = emhd_flux_ready(ctx, emhd, "khb_imex_stage"))) return rc;
     if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_imex_stage: stage must be 1 or 2");

@@ -52,6 +52,12 @@ struct khb_ctx {
     double* adj_buf;
     int32_t* adj_flags;
     double* adj_red;       // partial sums of khb_flux_dot
+    // B_CT: zone-centred EMFs [3][N] of FT, the intermediate stage's face field [3][N], and the face
+    // field a zone pass in progress reads (set only inside khb_ct_stage)
+    void* ct_emfc;
+    double* ct_stageBf;
+    const double* ct_bf[3];
+    bool ct_active;
 };
 
 
@@ -65,5 +71,10 @@ int set_error(int code, const std::string& msg);
 // Flux fixes and ghost zones of one block, as khb_stage issues them
 int ctx_fix_flux(khb_ctx* ctx, cudaStream_t st);
 int ctx_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st);
+// B_CT stage pieces (khb_ct.cu): edge EMFs from the stage's face fluxes and primitives, and the face
+// update Bf_out = gam0 Bf_s + gam1 Bf_0 + beta dt dBf/dt
+int ct_emf(khb_ctx* ctx, const khb_fields& Ps, cudaStream_t st);
+int ct_face_update(khb_ctx* ctx, int stage, double dt, const khb_fields& Bs, const khb_fields& B0,
+                   const khb_fields& Bout, cudaStream_t st);
 
 } // namespace khb

@@ -118,7 +118,7 @@ template <int DIR> struct FluxMinBlocks<double, DIR> {
     static constexpr int value = (DIR == 3) ? KHB_FLUX64_X3_MINB : KHB_FLUX64_MINB;
 };
 template <int MODE_, typename FT> struct ZoneMinBlocks {
-    static constexpr int MODE = MODE_ & ~M_KASTAUN;
+    static constexpr int MODE = MODE_ & ~(M_KASTAUN | M_BCT);
     static constexpr int value = (MODE == M_UPDATE) ? (sizeof(FT) == 8 ? KHB_ZONE_UPDATE_MINB : KHB_ZONE_UPDATE32_MINB) :
                                  (MODE == M_UTOP) ? KHB_ZONE_INV_MINB :
                                  (MODE == M_ZONE_FLOORS) ? KHB_ZONE_FLOOR_MINB :
@@ -315,6 +315,19 @@ __device__ __forceinline__ void ct_divergence(const Dims& d, const Phys& ph, con
     }
 }
 
+// B_CT::BlockUtoP for one zone (b_ct.cpp:172-181): the zone B^i as the average of its two faces'
+// B^i = Bf / sqrt(-g)(face); along an inactive direction the single face's value
+__device__ __forceinline__ void ct_zone_b(const Dims& d, const DevGeom& g, const double* const Bf[3], long long c,
+                                          int j, int i, double Bp[3])
+{
+    const long long gi = (long long)j*g.G1 + i;
+    Bp[0] = (__ldg(Bf[0] + c) / __ldg(g.gdet[0] + gi) + __ldg(Bf[0] + c + 1) / __ldg(g.gdet[0] + gi + 1)) / 2;
+    Bp[1] = (d.ndim > 1) ? (__ldg(Bf[1] + c) / __ldg(g.gdet[1] + gi) + __ldg(Bf[1] + c + d.sj) / __ldg(g.gdet[1] + gi + g.G1)) / 2
+                         : __ldg(Bf[1] + c) / __ldg(g.gdet[1] + gi);
+    Bp[2] = (d.ndim > 2) ? (__ldg(Bf[2] + c) / __ldg(g.gdet[2] + gi) + __ldg(Bf[2] + c + d.sk) / __ldg(g.gdet[2] + gi)) / 2
+                         : __ldg(Bf[2] + c) / __ldg(g.gdet[2] + gi);
+}
+
 // MODE: compile-time mask of M_* steps (0: take the mask from the arguments at run time).  The
 // CFL reduction (M_DT) is always a run-time choice.
 // One zone of the zone pass; returns the zone's timestep for the CFL minimum (DBL_MAX if none)
@@ -347,8 +360,9 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
                 dudt[p] = -du / vol;
             }
             if (NV > 5) {
-                double dudt_b[3];
-                ct_divergence<FT>(d, ph, F1, F2, F3, c, j, dudt_b);
+                double dudt_b[3] = {0., 0., 0.};
+                // with B_CT the zone B follows the faces (below) and has no flux divergence
+                if (!(mode & M_BCT)) ct_divergence<FT>(d, ph, F1, F2, F3, c, j, dudt_b);
 #pragma unroll
                 for (int v = 0; v < 3; ++v) dudt[5 + v] = dudt_b[v];
             }
@@ -384,6 +398,13 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
                 double x = a.g0 * __ldg(a.Us.v[p] + c) + a.g1 * __ldg(a.U0.v[p] + c);
                 U[p] = 1.0 * x + bdt * dudt[p];
             }
+            if (NV > 5 && (mode & M_BCT)) {
+                // B_CT::BlockUtoP on the updated faces: sqrt(-g) B^i at the zone centre
+                double Bp[3];
+                ct_zone_b(d, g, a.Bf, c, j, i, Bp);
+#pragma unroll
+                for (int v = 0; v < 3; ++v) U[5 + v] = Bp[v] * G.gdet;
+            }
         } else {
 #pragma unroll
             for (int p = 0; p < NV; ++p) U[p] = a.Us.v[p][c];
@@ -401,8 +422,15 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
             pflag = pf % FF_GEOM_RHO;
             fflag = (pf / FF_GEOM_RHO) * FF_GEOM_RHO;
             if (NV > 5) {
+                if (mode & M_BCT) {
+                    double Bp[3];
+                    ct_zone_b(d, g, a.Bf, c, j, i, Bp);
 #pragma unroll
-                for (int v = 0; v < 3; ++v) P[5 + v] = U[5 + v] / G.gdet;
+                    for (int v = 0; v < 3; ++v) P[5 + v] = Bp[v];
+                } else {
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) P[5 + v] = U[5 + v] / G.gdet;
+                }
             }
         } else {
             pflag = a.pflag[c];

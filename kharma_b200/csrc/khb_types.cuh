@@ -53,6 +53,7 @@ struct Phys {
     int inverter;                          // KHB_INVERTER_*
     int fofc, fofc_polar_cells;            // first-order flux correction
     double fofc_r_mark;                    // r_horizon + fofc/eh_buffer (spherical coordinates)
+    int ct_scheme;                         // KHB_CT_* (B_CT face-centred field when nonzero)
     Prescription fl;
 };
 
@@ -63,6 +64,9 @@ enum { M_ZONE_CELL = M_UTOP | M_FLOORS | M_PTOU | M_FAILLIST, M_ZONE_FUSED = M_U
 enum { M_ZONE_FLOORS = M_FLOORS | M_PTOU | M_FAILLIST };
 // Inversion by the Kastaun scheme instead of 1D_W (a compile-time variant of the kernels with M_UTOP)
 enum { M_KASTAUN = 64 };
+// B_CT: the zone B comes from the face field (ZoneArgs::Bf) instead of the flux-CT divergence; run
+// through the run-time-mode kernel (MODE = 0)
+enum { M_BCT = 128 };
 
 struct Box {
     int lo_i, lo_j, lo_k, cnt_i, cnt_j, cnt_k;
@@ -98,6 +102,7 @@ struct ZoneArgs {
     int* fail_count;
     int* fail_list;
     int mode;
+    const double* Bf[3];       // B_CT: the stage output's face field (M_BCT), else unused
 };
 
 

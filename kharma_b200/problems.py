@@ -406,3 +406,24 @@ def add_ramps(spec, P, frac=0.05, seed=9):
         a, b, c = rng.uniform(0.5, 1.5, 3)
         P[q] += amp[q] * (a * X1 + (b * X2 if spec.nx2 > 1 else 0) + (c * X3 if spec.nx3 > 1 else 0))
     return P
+
+
+# ------------------------------------------------------------------------ B_CT face fields
+def ct_curl_faces(spec, B0=(1.0, 0.0, 0.0), amp=0.05):
+    """A face field sqrt(-g) B^d (3, n3, n2, n1) on a Cartesian Minkowski block (sqrt(-g) = 1): the
+    uniform B0 plus the discrete curl of A_3 = amp sin(2 pi x1) cos(2 pi x2) sampled at the zone
+    corners, so that the face divergence vanishes to rounding.  Face i of direction d is the lower
+    x_d face of zone i."""
+    assert spec.cart_minkowski
+    n3, n2, n1 = spec.shape
+    dx1, dx2, _ = spec.dx
+    g2 = spec.ng if spec.nx2 > 1 else 0
+    xf = spec.x1min + (np.arange(n1 + 1) - spec.ng) * dx1          # corner x1 of zone i (lower)
+    yf = spec.x2min + (np.arange(n2 + 1) - g2) * dx2
+    Y, X = np.meshgrid(yf, xf, indexing="ij")                     # (n2+1, n1+1)
+    A = amp * np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y)
+    Bf = np.zeros((3,) + spec.shape)
+    Bf[0] = B0[0] + ((A[1:, :-1] - A[:-1, :-1]) / dx2)[None]       # (A(i, j+1) - A(i, j)) / dx2
+    Bf[1] = B0[1] - ((A[:-1, 1:] - A[:-1, :-1]) / dx1)[None]       # -(A(i+1, j) - A(i, j)) / dx1
+    Bf[2] = B0[2]
+    return Bf

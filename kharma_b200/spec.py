@@ -90,6 +90,9 @@ class BlockSpec:
     fofc: bool = False
     fofc_polar_cells: int = 0
     fofc_eh_buffer: float = 0.1
+    # magnetic field transport (b_field/solver, b_field/ct_scheme): "none" = B_FluxCT (cell-centred B);
+    # "bs99", "gs05_0", "gs05_c" ("sg07") = B_CT with a face-centred field
+    b_ct: str = "none"
     # driver
     driver: str = "simple"
 
@@ -155,6 +158,7 @@ class BlockSpec:
         c.inverter = _lib.INVERTER[self.inverter]
         c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(self.fofc), self.fofc_polar_cells, self.fofc_eh_buffer
         c.r_horizon = self.r_horizon
+        c.ct_scheme = _lib.CT_SCHEME[self.b_ct]
         return c
 
     @property

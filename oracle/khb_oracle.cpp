@@ -98,6 +98,7 @@ struct Config {
     int32_t inverter;                               // 0 onedw, 1 kastaun (inverter/type)
     int32_t fofc, fofc_polar_cells;                 // fofc/on, fofc/polar_cells
     double fofc_eh_buffer, r_horizon;               // fofc/eh_buffer, coords.get_horizon()
+    int32_t ct_scheme;                              // 0 B_FluxCT; B_CT: 1 bs99, 2 gs05_0, 3 gs05_c (b_ct.cpp:65)
 };
 
 // ---------------------------------------------------------------- coordinates
@@ -1694,6 +1695,184 @@ static void stage(const Block& B, Fields& f, int s, double dt,
     finish_stage(B, P_n, U_n);
 }
 
+// ---------------------------------------------------------------- B_CT (b_ct/b_ct.cpp)
+// Face field arrays Bf[3][N]: sqrt(-g) B^d on the x_d faces, face i = left face of zone i.  2D and 3D
+// blocks with periodic or exchange faces; only the interior faces [is, ie+1] (along their own
+// direction) are state.
+static const int CT_BS99 = 1, CT_GS05_0 = 2, CT_GS05_C = 3;
+
+// B_CT::BlockUtoP for one zone (b_ct.cpp:172-181)
+static void ct_zone_b(const Block& B, const double* Bf, int k, int j, int i, double Bp[3])
+{
+    const size_t N = B.N, c = B.id(k, j, i);
+    const double* F1 = Bf; const double* F2 = Bf + N; const double* F3 = Bf + 2*N;
+    Bp[0] = (F1[c] / B.Gdet(face1, j, i) + F1[c + 1] / B.Gdet(face1, j, i + 1)) / 2;
+    Bp[1] = (B.ndim > 1) ? (F2[c] / B.Gdet(face2, j, i) + F2[c + B.n1] / B.Gdet(face2, j + 1, i)) / 2
+                         : F2[c] / B.Gdet(face2, j, i);
+    Bp[2] = (B.ndim > 2) ? (F3[c] / B.Gdet(face3, j, i) + F3[c + (size_t)B.n1*B.n2] / B.Gdet(face3, j, i)) / 2
+                         : F3[c] / B.Gdet(face3, j, i);
+}
+
+// B_CT::CalculateEMF (b_ct.cpp:262-410) into emf[3][N] (E1, E2, E3 at the edges of zone (k,j,i)'s
+// lower corner lines) over [is, ie+1] x [js, je+1] x [ks, ke(+1 in 3D)]
+static void ct_calculate_emf(const Block& B, double* F[3], const double* P, double* emf)
+{
+    const size_t N = B.N, sj = B.n1, sk = (size_t)B.n1*B.n2;
+    const size_t V1 = 5*N, V2 = 6*N, V3 = 7*N;
+    const int scheme = B.c.ct_scheme;
+    const int h3 = B.ndim > 2;
+    std::vector<double> emfc;
+    if (scheme != CT_BS99) {
+        // zone-centred EMF (b_ct.cpp:331-345) over the interior +-1
+        emfc.assign(3*N, 0.);
+        for (int k = B.ks - h3; k <= B.ke + h3; ++k) for (int j = B.js - 1; j <= B.je + 1; ++j)
+        for (int i = B.is - 1; i <= B.ie + 1; ++i) {
+            const size_t c = B.id(k, j, i);
+            double Pc[8];
+            load_cell(B, P, c, Pc);
+            FourVectors D;
+            calc_4vecs(B, Pc, true, j, i, center, D);
+            const double gdet = B.Gdet(center, j, i);
+            emfc[c]       = (D.bcon[2]*D.ucon[3] - D.bcon[3]*D.ucon[2]) * gdet;
+            emfc[N + c]   = (D.bcon[3]*D.ucon[1] - D.bcon[1]*D.ucon[3]) * gdet;
+            emfc[2*N + c] = (D.bcon[1]*D.ucon[2] - D.bcon[2]*D.ucon[1]) * gdet;
+        }
+    }
+    const double* f1 = F[0]; const double* f2 = F[1]; const double* f3 = F[2];
+    auto ec = [&](int v, size_t x) { return emfc[v*N + x]; };
+    for (int k = B.ks; k <= B.ke + h3; ++k) for (int j = B.js; j <= B.je + 1; ++j) for (int i = B.is; i <= B.ie + 1; ++i) {
+        const size_t c = B.id(k, j, i);
+        double e1, e2, e3;
+        if (B.ndim > 2) {
+            e1 = 0.25*(-f2[V3 + c - sk] - f2[V3 + c] + f3[V2 + c - sj] + f3[V2 + c]);
+            e2 = 0.25*(-f3[V1 + c - 1] - f3[V1 + c] + f1[V3 + c - sk] + f1[V3 + c]);
+            e3 = 0.25*(-f1[V2 + c - sj] - f1[V2 + c] + f2[V1 + c - 1] + f2[V1 + c]);
+        } else {
+            e1 = -f2[V3 + c];
+            e2 = f1[V3 + c];
+            e3 = 0.25*(-f1[V2 + c - sj] - f1[V2 + c] + f2[V1 + c - 1] + f2[V1 + c]);
+        }
+        if (scheme == CT_GS05_0) {
+            if (B.ndim > 2) {
+                e1 = 2 * e1 - 0.25*(ec(0, c) + ec(0, c - sj) + ec(0, c - sj) + ec(0, c - sk - sj));
+                e2 = 2 * e2 - 0.25*(ec(1, c) + ec(1, c - 1) + ec(1, c - sk) + ec(1, c - sk - 1));
+            }
+            e3 = 2 * e3 - 0.25*(ec(2, c) + ec(2, c - 1) + ec(2, c - sj) + ec(2, c - sj - 1));
+        } else if (scheme == CT_GS05_C) {
+            if (B.ndim > 2) {
+                const double e1_l3 = (f2[c - sk] >= 0.0) ? f3[V2 + c - sj] - ec(0, c - sk - sj) : f3[V2 + c] - ec(0, c - sk);
+                const double e1_r3 = (f2[c] >= 0.0) ? f3[V2 + c - sj] - ec(0, c - sj) : f3[V2 + c] - ec(0, c);
+                const double e1_l2 = (f3[c - sj] >= 0.0) ? -f2[V3 + c - sk] - ec(0, c - sk - sj) : -f2[V3 + c] - ec(0, c - sj);
+                const double e1_r2 = (f3[c] >= 0.0) ? -f2[V3 + c - sk] - ec(0, c - sk) : -f2[V3 + c] - ec(0, c);
+                e1 += 0.25*(e1_l3 + e1_r3 + e1_l2 + e1_r2);
+                const double e2_l3 = (f1[c - sk] >= 0.0) ? -f3[V1 + c - 1] - ec(1, c - sk - 1) : -f3[V1 + c] - ec(1, c - sk);
+                const double e2_r3 = (f1[c] >= 0.0) ? -f3[V1 + c - 1] - ec(1, c - 1) : -f3[V1 + c] - ec(1, c);
+                const double e2_l1 = (f3[c - 1] >= 0.0) ? f1[V3 + c - sk] - ec(1, c - sk - 1) : f1[V3 + c] - ec(1, c - 1);
+                const double e2_r1 = (f3[c] >= 0.0) ? f1[V3 + c - sk] - ec(1, c - sk) : f1[V3 + c] - ec(1, c);
+                e2 += 0.25*(e2_l3 + e2_r3 + e2_l1 + e2_r1);
+            }
+            const double e3_l2 = (f1[c - sj] >= 0.0) ? f2[V1 + c - 1] - ec(2, c - sj - 1) : f2[V1 + c] - ec(2, c - sj);
+            const double e3_r2 = (f1[c] >= 0.0) ? f2[V1 + c - 1] - ec(2, c - 1) : f2[V1 + c] - ec(2, c);
+            const double e3_l1 = (f2[c - 1] >= 0.0) ? -f1[V2 + c - sj] - ec(2, c - sj - 1) : -f1[V2 + c] - ec(2, c - 1);
+            const double e3_r1 = (f2[c] >= 0.0) ? -f1[V2 + c - sj] - ec(2, c - sj) : -f1[V2 + c] - ec(2, c);
+            e3 += 0.25*(e3_l2 + e3_r2 + e3_l1 + e3_r1);
+        }
+        emf[c] = e1; emf[N + c] = e2; emf[2*N + c] = e3;
+    }
+}
+
+// B_CT::AddSource (b_ct.cpp:412-470) and the face RK combination (WeightedSumDataFace twice)
+static void ct_update_faces(const Block& B, const double* emf, int s, double dt, const double* Bs, const double* B0,
+                            double* Bn)
+{
+    const size_t N = B.N, sj = B.n1, sk = (size_t)B.n1*B.n2;
+    const double g0 = RK_GAM0[s], g1 = RK_GAM1[s], bdt = RK_BETA[s] * dt;
+    const double L1 = B.c.dx1, L2 = B.c.dx2, L3 = B.c.dx3;
+    const bool d3 = B.ndim > 2;
+    auto E = [&](int v, size_t x) { return emf[v*N + x]; };
+    for (int k = B.ks; k <= B.ke + d3; ++k) for (int j = B.js; j <= B.je + 1; ++j) for (int i = B.is; i <= B.ie + 1; ++i) {
+        const size_t c = B.id(k, j, i);
+        if (j <= B.je && k <= B.ke) {
+            double db = (-L3 * E(2, c + sj) + L3 * E(2, c));
+            if (d3) db += (L2 * E(1, c + sk) - L2 * E(1, c));
+            db /= (L2 * L3);
+            const double x = g0 * Bs[c] + g1 * B0[c];
+            Bn[c] = 1.0 * x + bdt * db;
+        }
+        if (i <= B.ie && k <= B.ke) {
+            double db = (L3 * E(2, c + 1) - L3 * E(2, c));
+            if (d3) db += (-L1 * E(0, c + sk) + L1 * E(0, c));
+            db /= (L1 * L3);
+            const double x = g0 * Bs[N + c] + g1 * B0[N + c];
+            Bn[N + c] = 1.0 * x + bdt * db;
+        }
+        if (i <= B.ie && j <= B.je) {
+            const double db = (-L2 * E(1, c + 1) + L2 * E(1, c) + L1 * E(0, c + sj) - L1 * E(0, c)) / (L1 * L2);
+            const double x = g0 * Bs[2*N + c] + g1 * B0[2*N + c];
+            Bn[2*N + c] = 1.0 * x + bdt * db;
+        }
+    }
+}
+
+// One RK stage with B_CT (kharma_step.cpp:163-214, use_b_ct): fluxes, FixFlux without flux-CT, EMFs,
+// face update, the cell update, the zone B (and sqrt(-g) B) from the new faces, inversion, floors,
+// fixups, boundaries and P->U as stage() does
+static void ct_stage(const Block& B, Fields& f, int s, double dt, const double* P_s, const double* U_s,
+                     const double* U_0, const double* Bs, const double* B0, double* P_n, double* U_n, double* Bn,
+                     double* pflag, double* fflag)
+{
+    const size_t N = B.N, NV = (size_t)B.nv*N;
+    for (int d = 1; d <= B.ndim; ++d)
+        get_flux(B, d, P_s, f.F[d-1].data(), f.cmax[d-1].data(), f.cmin[d-1].data());
+    double* F[3] = {f.F[0].data(), f.F[1].data(), f.F[2].data()};
+    boundaries_fix_flux(B, F);
+    std::vector<double> emf(3*N, 0.);
+    ct_calculate_emf(B, F, P_s, emf.data());
+    ct_update_faces(B, emf.data(), s, dt, Bs, B0, Bn);
+    std::vector<double> dudt(NV, 0.);
+    flux_divergence(B, F, dudt.data());
+    add_geo_source(B, P_s, dudt.data());
+    const double g0 = RK_GAM0[s], g1 = RK_GAM1[s], bdt = RK_BETA[s] * dt;
+    for (size_t x = 0; x < NV; ++x) U_n[x] = g0 * U_s[x] + g1 * U_0[x];
+    for (size_t x = 0; x < NV; ++x) U_n[x] = 1.0 * U_n[x] + bdt * dudt[x];
+    // the zone B follows the faces (cons.B is derived, not updated by its flux divergence)
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        double Bp[3];
+        ct_zone_b(B, Bn, k, j, i, Bp);
+        const size_t c = B.id(k, j, i);
+        for (int v = 0; v < 3; ++v) U_n[(size_t)(5 + v)*N + c] = Bp[v] * B.Gdet(center, j, i);
+    }
+    // inversion guess and the ghost shell (exchange faces keep theirs; periodic ones are refreshed)
+    if (P_n != P_s) std::memcpy(P_n, P_s, NV*sizeof(double));
+    for (size_t x = 0; x < N; ++x) { pflag[x] = 0; fflag[x] = 0; }
+    block_utop(B, U_n, P_n, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        double Bp[3];
+        ct_zone_b(B, Bn, k, j, i, Bp);
+        for (int v = 0; v < 3; ++v) P_n[(size_t)(5 + v)*N + B.id(k, j, i)] = Bp[v];
+    }
+    if (B.c.floors_on) apply_grmhd_floors(B, P_n, U_n, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
+    {
+        int ks = B.ks, ke = B.ke, js = B.js, je = B.je, is = B.is, ie = B.ie;
+        for (int d = 1; d <= B.ndim; ++d)
+            if (B.c.bc[2*(d-1)] == BC_PERIODIC) {
+                periodic_fill(B, P_n, 5, d);
+                periodic_fill(B, pflag, 1, d);
+                if (d == 1) { is = 0; ie = B.n1 - 1; }
+                if (d == 2) { js = 0; je = B.n2 - 1; }
+                if (d == 3) { ks = 0; ke = B.n3 - 1; }
+            }
+        if (B.c.bc[0] == BC_EXCHANGE) is = 0;
+        if (B.c.bc[1] == BC_EXCHANGE) ie = B.n1 - 1;
+        if (B.ndim > 1 && B.c.bc[2] == BC_EXCHANGE) js = 0;
+        if (B.ndim > 1 && B.c.bc[3] == BC_EXCHANGE) je = B.n2 - 1;
+        if (B.ndim > 2 && B.c.bc[4] == BC_EXCHANGE) ks = 0;
+        if (B.ndim > 2 && B.c.bc[5] == BC_EXCHANGE) ke = B.n3 - 1;
+        fix_utop(B, P_n, U_n, pflag, ks, ke, js, je, is, ie);
+    }
+    finish_stage(B, P_n, U_n);
+}
+
 // ======================================================================== EMHD and the implicit solve
 // Extended GRMHD (emhd/) and the per-zone Newton solve (implicit/).  Zone state for these
 // functions is a 10-slot array: rho, u, u1..u3, B1..B3 (slots 0-7 as above), q~ (8), dP~ (9).
@@ -2736,6 +2915,72 @@ void orc_step(void* hp, double* P, double* U, double* pflag, double* fflag, doub
         const double ndt = clip(mn * B.c.cfl, B.c.dt_min, B.c.max_dt_increase * dt);
         *dt_next = std::min(2.0 * dt, ndt);
     }
+}
+
+// One RK2 step with B_CT in place on (P, U, Bf[3][N]); returns the next dt like orc_step
+void orc_ct_step(void* hp, double* P, double* U, double* Bf, double* pflag, double* fflag, double dt,
+                 double* dt_next, double* min_ndt_out)
+{
+    Handle* h = (Handle*)hp;
+    const Block& B = h->B;
+    const size_t NV = (size_t)B.nv*B.N;
+    h->P1.assign(P, P + NV); h->U1.assign(NV, 0.); h->U0.assign(U, U + NV);
+    std::vector<double> B0(Bf, Bf + 3*B.N), B1(Bf, Bf + 3*B.N);
+    ct_stage(B, h->f, 0, dt, P, h->U0.data(), h->U0.data(), B0.data(), B0.data(), h->P1.data(), h->U1.data(),
+             B1.data(), pflag, fflag);
+    ct_stage(B, h->f, 1, dt, h->P1.data(), h->U1.data(), h->U0.data(), B1.data(), B0.data(), P, U, Bf, pflag, fflag);
+    const double mn = min_ndt(B, h->f);
+    if (min_ndt_out) *min_ndt_out = mn;
+    if (dt_next) {
+        const double ndt = clip(mn * B.c.cfl, B.c.dt_min, B.c.max_dt_increase * dt);
+        *dt_next = std::min(2.0 * dt, ndt);
+    }
+}
+
+// B_CT::BlockUtoP over the interior
+void orc_ct_utop(void* hp, const double* Bf, double* P, double* U)
+{
+    const Block& B = ((Handle*)hp)->B;
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        double Bp[3];
+        ct_zone_b(B, Bf, k, j, i, Bp);
+        const size_t c = B.id(k, j, i);
+        for (int v = 0; v < 3; ++v) {
+            P[(size_t)(5 + v)*B.N + c] = Bp[v];
+            U[(size_t)(5 + v)*B.N + c] = Bp[v] * B.Gdet(center, j, i);
+        }
+    }
+}
+
+// B_CT::DangerousPtoU over the interior faces (the x3 faces of a 2D block: their zone's value)
+void orc_ct_faces_from_prims(void* hp, const double* P, double* Bf)
+{
+    const Block& B = ((Handle*)hp)->B;
+    const size_t N = B.N, sj = B.n1, sk = (size_t)B.n1*B.n2;
+    const int d3 = B.ndim > 2;
+    for (int k = B.ks; k <= B.ke + d3; ++k) for (int j = B.js; j <= B.je + 1; ++j) for (int i = B.is; i <= B.ie + 1; ++i) {
+        const size_t c = B.id(k, j, i);
+        if (j <= B.je && k <= B.ke) Bf[c] = B.Gdet(face1, j, i) * (P[5*N + c - 1] + P[5*N + c]) / 2;
+        if (i <= B.ie && k <= B.ke) Bf[N + c] = B.Gdet(face2, j, i) * (P[6*N + c - sj] + P[6*N + c]) / 2;
+        if (i <= B.ie && j <= B.je)
+            Bf[2*N + c] = d3 ? B.Gdet(face3, j, i) * (P[7*N + c - sk] + P[7*N + c]) / 2 : B.Gdet(face3, j, i) * P[7*N + c];
+    }
+}
+
+// max |face divergence| over the interior (b_ct.cpp:499-520)
+double orc_ct_max_divb(void* hp, const double* Bf)
+{
+    const Block& B = ((Handle*)hp)->B;
+    const size_t N = B.N, sj = B.n1, sk = (size_t)B.n1*B.n2;
+    double m = 0.;
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double du = (Bf[c + 1] - Bf[c]) / B.c.dx1;
+        if (B.ndim > 1) du += (Bf[N + c + sj] - Bf[N + c]) / B.c.dx2;
+        if (B.ndim > 2) du += (Bf[2*N + c + sk] - Bf[2*N + c]) / B.c.dx3;
+        m = std::max(m, std::fabs(du));
+    }
+    return m;
 }
 
 double orc_max_divb(void* hp, const double* U, int avoid_inner, int avoid_outer)

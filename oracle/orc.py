@@ -51,6 +51,7 @@ class Config(C.Structure):
         ("inverter", C.c_int32),
         ("fofc", C.c_int32), ("fofc_polar_cells", C.c_int32),
         ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
+        ("ct_scheme", C.c_int32),
     ]
 
 
@@ -85,6 +86,11 @@ def load():
     lib.orc_ptou.argtypes = [P, P, P]
     lib.orc_boundaries.argtypes = [P, P, P]
     lib.orc_step.argtypes = [P, P, P, P, P, C.c_double, P, P]
+    lib.orc_ct_step.argtypes = [P, P, P, P, P, P, C.c_double, P, P]
+    lib.orc_ct_utop.argtypes = [P, P, P, P]
+    lib.orc_ct_faces_from_prims.argtypes = [P, P, P]
+    lib.orc_ct_max_divb.restype = C.c_double
+    lib.orc_ct_max_divb.argtypes = [P, P]
     lib.orc_max_divb.restype = C.c_double
     lib.orc_max_divb.argtypes = [P, P, C.c_int, C.c_int]
     lib.orc_utop_cell.restype = C.c_int
@@ -137,6 +143,7 @@ def config_from_spec(spec):
     c.inverter = 1 if spec.inverter == "kastaun" else 0
     c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(spec.fofc), spec.fofc_polar_cells, spec.fofc_eh_buffer
     c.r_horizon = spec.r_horizon
+    c.ct_scheme = {"none": 0, "bs99": 1, "gs05_0": 2, "gs05_c": 3, "sg07": 3}[spec.b_ct]
     for name, _ in Prescription._fields_:
         setattr(c.floors, name, type(getattr(c.floors, name))(getattr(spec.floors, name)))
     return c
@@ -232,6 +239,35 @@ class Oracle:
         mn = C.c_double()
         self.lib.orc_step(self.h, _ptr(P), _ptr(U), _ptr(pflag), _ptr(fflag), dt, C.byref(dtn), C.byref(mn))
         return pflag, fflag, dtn.value, mn.value
+
+    # ---------------------------------------------------------------- B_CT (face fields (3, n3, n2, n1))
+    def ct_init_state(self, P, Bf=None):
+        """Same sequence as kharma_b200.block.Block.set_prims for a B_CT block: ghost zones, faces
+        from the zone B unless given, the zone B from the faces, ghost zones again, U = U(P)."""
+        P = np.ascontiguousarray(P, dtype=np.float64).copy()
+        U = self.ptou(P)
+        self.boundaries(P, U)
+        if Bf is None:
+            Bf = np.zeros((3,) + self.shape)
+            self.lib.orc_ct_faces_from_prims(self.h, _ptr(P), _ptr(Bf))
+        else:
+            Bf = np.ascontiguousarray(Bf, dtype=np.float64).copy()
+        self.lib.orc_ct_utop(self.h, _ptr(Bf), _ptr(P), _ptr(U))
+        self.boundaries(P, U)
+        self.lib.orc_ptou(self.h, _ptr(P), _ptr(U))
+        return P, U, Bf
+
+    def ct_step(self, P, U, Bf, dt):
+        """One RK2 step with B_CT in place; returns (pflag, fflag, dt_next, min_ndt)."""
+        pflag = np.zeros(self.shape)
+        fflag = np.zeros(self.shape)
+        dtn = C.c_double()
+        mn = C.c_double()
+        self.lib.orc_ct_step(self.h, _ptr(P), _ptr(U), _ptr(Bf), _ptr(pflag), _ptr(fflag), dt, C.byref(dtn), C.byref(mn))
+        return pflag, fflag, dtn.value, mn.value
+
+    def ct_max_divb(self, Bf):
+        return self.lib.orc_ct_max_divb(self.h, _ptr(Bf))
 
     def max_divb(self, U, avoid_inner=False, avoid_outer=False):
         return self.lib.orc_max_divb(self.h, _ptr(U), int(avoid_inner), int(avoid_outer))
