@@ -343,6 +343,42 @@ def batching(steps=20, warm=3):
     return out
 
 
+def b_ct_form(n=128, steps=20, warm=3):
+    """B_CT (face-centred field, gs05_c EMFs) against the flux-CT path on the same n^3 periodic MHD
+    fast mode (Minkowski, linear MC, LLF, 1D_W), fixed dt, steps launched back to back on one stream;
+    CUDA events."""
+    import dataclasses
+    import torch
+    from kharma_b200 import problems
+    from kharma_b200.block import Block
+    from kharma_b200.spec import mhdmodes_spec
+
+    out = {"workload": f"MHD fast mode {n}^3 periodic, Minkowski, linear MC, LLF, FP64"}
+    base = mhdmodes_spec(n, n, n, recon="linear_mc")
+    P0 = problems.mhdmodes(base, 3, amp=1e-2)
+    for name, spec in (("flux_ct", base), ("b_ct_gs05_c", dataclasses.replace(base, b_ct="gs05_c"))):
+        b = Block(spec)
+        b.set_prims(P0)
+        b.step(spec.dt_min)
+        dt = 0.5 * spec.cfl * b.min_ndt()
+        for _ in range(warm):
+            b.step(dt)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            b.step(dt)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms_per_step": ms, "zone_cycles_per_s": n ** 3 / (ms / 1000.0), "max_divb": b.max_divb()}
+        del b
+        torch.cuda.empty_cache()
+    out["b_ct_over_flux_ct_time"] = out["b_ct_gs05_c"]["ms_per_step"] / out["flux_ct"]["ms_per_step"]
+    return out
+
+
 def adjoint_form(n=192, steps=200, every=20, ndir=8):
     """The differentiation form on the adjoint workload's shape: an n^3 Bondi block (KS a = 0, MKS,
     r in [3, 30], x2 in [0.1, 0.9], all x3; linear MC, LLF, hydro) with exchange faces holding the
@@ -603,6 +639,10 @@ def gpu_arm(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_emhd:
         emhd = emhd_newton()
 
+    bct = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        bct = b_ct_form()
+
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
         del b, drv
@@ -628,7 +668,7 @@ def gpu_arm(args, rank, world, local_rank):
                           "parallelism": "single block" if world == 1 else f"x3 slabs x{world} (NCCL halo exchange)",
                           "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
-               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch,
+               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch, "b_ct": bct,
                "host_driven_step": host_driven}
         print(json.dumps(out), flush=True)
 

@@ -410,6 +410,23 @@ int khb_batch_autotune(khb_batch* batch, int reps, int32_t* kz_out, int32_t* per
 /* Device kernel launches issued for this batch so far (a graph replay counts its nodes). */
 int64_t khb_batch_launch_count(khb_batch* batch);
 
+/* Static mesh refinement over the blocks of a batch (Parthenon's boundary communication and flux
+ * correction for a refined mesh, kharma_step.cpp:157-214, with its cell-centred refinement operators):
+ * the blocks form one mesh whose ghost zones are filled from their neighbours after every stage and
+ * whose coarse faces on fine-coarse boundaries take the average of the fine fluxes before the update.
+ * ghost: n_ghost entries of 6 int32 {dst block, dst zone, op, src block, src zone, aux}, op 0 copy,
+ * 1 restriction (average of the 2^ndim fine zones from src zone upwards), 2 prolongation (src coarse
+ * zone plus minmod-limited slopes times +-1/4; aux bit d: + side along direction d+1); the first
+ * n_ghost_first entries are the copies and restrictions, the rest the prolongations.  The primitives
+ * are filled, then U = U(P) in those zones.  flux: n_flux entries {coarse block, direction, coarse
+ * face, fine block, fine face of lowest index, 0}.  Hydro blocks (nvar 5) with exchange faces.
+ * Every index is checked against the blocks' sizes.  Synchronizes the device. */
+int khb_batch_set_mesh(khb_batch* batch, const int32_t* ghost, int64_t n_ghost, int64_t n_ghost_first,
+                       const int32_t* flux, int64_t n_flux);
+
+/* Fill every block's ghost zones of the state (P, U) from the mesh (e.g. after initial data). */
+int khb_batch_mesh_exchange(khb_batch* batch, void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Extended MHD and the implicit solve (emhd/, implicit/)
  * ------------------------------------------------------------------------------------------- */

@@ -12,6 +12,7 @@ identical ghost inputs, as the per-block comparison with the oracle needs.
 import ctypes as C
 import math
 
+import numpy as np
 import torch
 
 from . import _lib, problems
@@ -147,6 +148,18 @@ class Batch:
 
     def launch_count(self):
         return int(self.lib.khb_batch_launch_count(self.h))
+
+    def set_mesh(self, ghost, n_ghost_first, flux):
+        """SMR tables (kharma_b200.mesh.SMRMesh.tables): ghost exchange after every stage and flux
+        correction before every update."""
+        ghost = np.ascontiguousarray(ghost, dtype=np.int32)
+        flux = np.ascontiguousarray(flux, dtype=np.int32)
+        _lib.check(self.lib.khb_batch_set_mesh(self.h, ghost.ctypes.data_as(C.c_void_p), len(ghost), int(n_ghost_first),
+                                               flux.ctypes.data_as(C.c_void_p), len(flux)), "khb_batch_set_mesh")
+
+    def mesh_exchange(self):
+        """Fill the ghost zones of every block's state from the mesh."""
+        _lib.check(self.lib.khb_batch_mesh_exchange(self.h, self.stream), "khb_batch_mesh_exchange")
 
     def state(self):
         """Host copies of every block's (P, U, pflag, fflag)."""

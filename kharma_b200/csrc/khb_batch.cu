@@ -39,6 +39,10 @@ struct khb_batch {
     double dt_host = 0.;                           // source of the timestep upload
     std::vector<int> needs_fix_flux, needs_bounds; // blocks with physical (or periodic) faces
     bool any_exchange = false;                     // some block carries its ghost shell over
+    // SMR: ghost-exchange and flux-correction tables (6 ints per entry) of the mesh the blocks form
+    int* mesh_ghost = nullptr;
+    int* mesh_flux = nullptr;
+    long long n_ghost = 0, n_ghost_first = 0, n_flux = 0;
     // CUDA graph of one step
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -201,6 +205,10 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
         if (rc) return rc;
         b->launches += b->ctx[x]->launches - l0;
     }
+    if (b->n_flux) {
+        Launch<FT>::mesh_flux(b->nv, desc, b->mesh_flux, b->n_flux, st);
+        KHB_BLAUNCHED(b, 1);
+    }
     if (b->any_exchange) {
         LaunchCommon::batch_ghost_copy(b->nv, b->fix, b->nb, stage, st);
         KHB_BLAUNCHED(b, 1);
@@ -230,6 +238,11 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
         int rc = ctx_boundaries(c, Po, Uo, st);
         if (rc) return rc;
         b->launches += c->launches - l0;
+    }
+    if (b->n_ghost) {
+        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, 0, b->n_ghost_first, stage, st);
+        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, b->n_ghost_first, b->n_ghost, stage, st);
+        KHB_BLAUNCHED(b, 2);
     }
     return KHB_OK;
 }
@@ -355,9 +368,78 @@ int khb_batch_destroy(khb_batch* b)
     if (!b) return KHB_OK;
     drop_graph(b);
     free_tables(b);
+    cudaFree(b->mesh_ghost);
+    cudaFree(b->mesh_flux);
     cudaFree(b->dt_dev);
     cudaFree(b->word);
     delete b;
+    return KHB_OK;
+}
+
+int khb_batch_set_mesh(khb_batch* b, const int32_t* ghost, int64_t n_ghost, int64_t n_ghost_first,
+                       const int32_t* flux, int64_t n_flux)
+{
+    if (!b) return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: NULL batch");
+    if (n_ghost < 0 || n_flux < 0 || n_ghost_first < 0 || n_ghost_first > n_ghost ||
+        (n_ghost && !ghost) || (n_flux && !flux))
+        return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: bad table sizes");
+    if (b->nv != 5) return set_error(KHB_ERR_UNSUPPORTED, "khb_batch_set_mesh: SMR meshes of hydro blocks (nvar 5) only");
+    // every index is checked here, so the kernels read and write inside the blocks' arrays
+    for (int64_t e = 0; e < n_ghost; ++e) {
+        const int32_t* t = ghost + 6 * e;
+        if (t[0] < 0 || t[0] >= b->nb || t[3] < 0 || t[3] >= b->nb || t[2] < 0 || t[2] > 2)
+            return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: ghost entry with a bad block or op");
+        const Dims& dd = b->ctx[t[0]]->d;
+        const Dims& ds = b->ctx[t[3]]->d;
+        if (t[1] < 0 || t[1] >= dd.N) return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: ghost entry outside its block");
+        // the source stencil: the zone, +1 per active direction (restrict), +-1 (prolong)
+        long long lo = t[4], hi = t[4];
+        const long long st[3] = {1, ds.sj, ds.sk};
+        for (int d = 0; d < ds.ndim; ++d) {
+            if (t[2] == 1) hi += st[d];
+            if (t[2] == 2) { lo -= st[d]; hi += st[d]; }
+        }
+        if (lo < 0 || hi >= ds.N) return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: ghost source outside its block");
+        if ((e < n_ghost_first) != (t[2] != 2))
+            return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: prolongations must follow copies and restrictions");
+    }
+    for (int64_t e = 0; e < n_flux; ++e) {
+        const int32_t* t = flux + 6 * e;
+        if (t[0] < 0 || t[0] >= b->nb || t[3] < 0 || t[3] >= b->nb || t[1] < 1 || t[1] > b->ndim)
+            return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: flux entry with a bad block or direction");
+        const Dims& dc = b->ctx[t[0]]->d;
+        const Dims& df = b->ctx[t[3]]->d;
+        const long long t1 = (t[1] == 1) ? df.sj : 1, t2 = (t[1] == 3) ? df.sj : df.sk;
+        const long long hi = t[4] + t1 + ((df.ndim > 2) ? t2 : 0);
+        if (t[2] < 0 || t[2] >= dc.N || t[4] < 0 || hi >= df.N)
+            return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: flux entry outside its blocks");
+    }
+    drop_graph(b);
+    cudaFree(b->mesh_ghost); cudaFree(b->mesh_flux);
+    b->mesh_ghost = nullptr; b->mesh_flux = nullptr;
+    b->n_ghost = b->n_ghost_first = b->n_flux = 0;
+    if (n_ghost) {
+        KHB_BCUDA(cudaMalloc((void**)&b->mesh_ghost, sizeof(int32_t) * 6 * (size_t)n_ghost));
+        KHB_BCUDA(cudaMemcpy(b->mesh_ghost, ghost, sizeof(int32_t) * 6 * (size_t)n_ghost, cudaMemcpyHostToDevice));
+    }
+    if (n_flux) {
+        KHB_BCUDA(cudaMalloc((void**)&b->mesh_flux, sizeof(int32_t) * 6 * (size_t)n_flux));
+        KHB_BCUDA(cudaMemcpy(b->mesh_flux, flux, sizeof(int32_t) * 6 * (size_t)n_flux, cudaMemcpyHostToDevice));
+    }
+    KHB_BCUDA(cudaDeviceSynchronize());
+    b->n_ghost = n_ghost; b->n_ghost_first = n_ghost_first; b->n_flux = n_flux;
+    return KHB_OK;
+}
+
+int khb_batch_mesh_exchange(khb_batch* b, void* stream)
+{
+    if (!b) return set_error(KHB_ERR_ARG, "khb_batch_mesh_exchange: NULL batch");
+    if (b->n_ghost) {
+        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, 0, b->n_ghost_first, 2, S(stream));
+        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, b->n_ghost_first, b->n_ghost, 2, S(stream));
+        b->launches += 2;
+        KHB_BCUDA(cudaGetLastError());
+    }
     return KHB_OK;
 }
 

@@ -1117,6 +1117,99 @@ k_batch_zone(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ 
     }
 }
 
+// ===================================================================================== SMR
+// Flux correction (Parthenon's flux-correction messages, kharma_step.cpp:183-195): each entry
+// replaces a coarse face's fluxes by the average of the 2^(ndim-1) fine fluxes through it.  Entry:
+// {coarse block, direction, coarse face, fine block, fine face of lowest index, -}.
+template <typename FT>
+__global__ void __launch_bounds__(128) k_mesh_flux(const BatchBlock<FT>* __restrict__ blocks,
+                                                   const int* __restrict__ table, long long n, int nv)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int* t = table + 6 * e;
+    const BatchBlock<FT>& C = blocks[__ldg(t)];
+    const BatchBlock<FT>& F = blocks[__ldg(t + 3)];
+    const int dir = __ldg(t + 1);
+    const long long cc = __ldg(t + 2), fc = __ldg(t + 4);
+    FT* Fc = C.F[dir - 1];
+    const FT* Ff = F.F[dir - 1];
+    const Dims& df = F.d;
+    // tangential strides in the fine block
+    const long long t1 = (dir == 1) ? df.sj : 1;
+    const long long t2 = (dir == 3) ? df.sj : df.sk;
+    const bool two = df.ndim > 2;
+    for (int p = 0; p < nv; ++p) {
+        const FT* f = Ff + p * df.N + fc;
+        FT v;
+        if (two) v = ((f[0] + f[t1]) + (f[t2] + f[t1 + t2])) * (FT)0.25;
+        else v = (f[0] + f[t1]) * (FT)0.5;
+        Fc[p * C.d.N + cc] = v;
+    }
+}
+
+#ifdef KHB_COMMON_KERNELS
+// SMR ghost zones (Parthenon's cell-centred refinement operators on a uniform grid): entries
+// {dst block, dst zone, op, src block, src zone, aux} fill the stage output's primitives of a ghost
+// zone by a copy, the average of the 2^ndim fine zones (restriction), or the coarse value plus a
+// minmod-limited slope times +-1/4 per active direction (prolongation; aux bit d: + side along
+// d+1), then set its conserved variables U = U(P).  Prolongations run in a second launch: they read
+// coarse ghost zones that copies and restrictions fill.
+__device__ __forceinline__ double minmod2(double a, double b)
+{
+    return (a * b > 0.) ? ((fabs(a) < fabs(b)) ? a : b) : 0.;
+}
+template <int NV>
+__global__ void __launch_bounds__(128) k_mesh_ghost(const FixupBlock* __restrict__ blocks, const int* __restrict__ table,
+                                                    long long begin, long long end, int stage)
+{
+    const long long e = begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= end) return;
+    const int s = stage - 1;
+    const int* t = table + 6 * e;
+    const FixupBlock& D = blocks[__ldg(t)];
+    const FixupBlock& S = blocks[__ldg(t + 3)];
+    const long long cd = __ldg(t + 1), cs = __ldg(t + 4);
+    const int op = __ldg(t + 2), aux = __ldg(t + 5);
+    const khb_fields& Ps = S.P[s];
+    const Dims& ds = S.d;
+    double P[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        const double* q = Ps.v[p];
+        if (op == 0) {
+            P[p] = q[cs];
+        } else if (op == 1) {
+            double r = (q[cs] + q[cs + 1]);
+            if (ds.ndim > 1) r = r + (q[cs + ds.sj] + q[cs + ds.sj + 1]);
+            if (ds.ndim > 2) r = r + ((q[cs + ds.sk] + q[cs + ds.sk + 1]) + (q[cs + ds.sk + ds.sj] + q[cs + ds.sk + ds.sj + 1]));
+            P[p] = r * ((ds.ndim > 2) ? 0.125 : (ds.ndim > 1) ? 0.25 : 0.5);
+        } else {
+            const double uc = q[cs];
+            double v = uc;
+            const long long st[3] = {1, ds.sj, ds.sk};
+            for (int d = 0; d < ds.ndim; ++d) {
+                const double sl = minmod2(uc - q[cs - st[d]], q[cs + st[d]] - uc);
+                v += ((aux >> d) & 1) ? 0.25 * sl : -0.25 * sl;
+            }
+            P[p] = v;
+        }
+    }
+    const khb_fields& Pd = D.P[s];
+    const khb_fields& Ud = D.U[s];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) Pd.v[p][cd] = P[p];
+    int k, j, i;
+    zone_kji(D.d, cd, k, j, i);
+    ZoneGeom G;
+    load_zone_geom(D.g, j, i, G);
+    double U[NV];
+    p_to_u_zone<NV>(G, D.ph.gam, P, U);
+#pragma unroll
+    for (int p = 0; p < NV; ++p) Ud.v[p][cd] = U[p];
+}
+#endif
+
 #ifdef KHB_COMMON_KERNELS
 // One row of CTAs per block (blockIdx.y), each walking that block's failed-zone list
 template <int NV>
@@ -1362,7 +1455,21 @@ int Launch<FT>::batch_zone(int nv, int mode, const BatchBlock<FT>* blocks, const
     return batch_zone_mode<5, FT, M_ZONE_CELL>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
 }
 
+template <typename FT>
+void Launch<FT>::mesh_flux(int nv, const BatchBlock<FT>* blocks, const int* table, long long n, cudaStream_t st)
+{
+    if (n > 0) k_mesh_flux<FT><<<blocks_for(n, 128), 128, 0, st>>>(blocks, table, n, nv);
+}
+
 #ifdef KHB_COMMON_KERNELS
+void LaunchCommon::mesh_ghost(int nv, const FixupBlock* blocks, const int* table, long long begin, long long end,
+                              int stage, cudaStream_t st)
+{
+    if (end <= begin) return;
+    if (nv == 8) k_mesh_ghost<8><<<blocks_for(end - begin, 128), 128, 0, st>>>(blocks, table, begin, end, stage);
+    else k_mesh_ghost<5><<<blocks_for(end - begin, 128), 128, 0, st>>>(blocks, table, begin, end, stage);
+}
+
 void LaunchCommon::batch_fixup(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st)
 {
     const dim3 grid(4, nblocks);

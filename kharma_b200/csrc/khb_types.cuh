@@ -162,6 +162,8 @@ struct Launch {
                           unsigned grid, int stage, cudaStream_t st);
     static int batch_zone(int nv, int mode, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
                           unsigned grid, int stage, int dtm, double beta, const double* dt, cudaStream_t st);
+    // SMR flux correction over the entries of a mesh's flux table (6 ints each)
+    static void mesh_flux(int nv, const BatchBlock<FT>* blocks, const int* table, long long n, cudaStream_t st);
 };
 
 // Zone-local FP64 work shared by both forms (compiled with the FP64 unit)
@@ -183,6 +185,9 @@ struct LaunchCommon {
     // Batched fixups (one CTA row per block) and the per-stage reset of the failed-zone counters
     // (and, when word != NULL, of the timestep minimum)
     static void batch_fixup(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st);
+    // SMR ghost zones of stage `stage`'s outputs from entries [begin, end) of a mesh's ghost table
+    static void mesh_ghost(int nv, const FixupBlock* blocks, const int* table, long long begin, long long end,
+                           int stage, cudaStream_t st);
     static void batch_reset(int* const* counts, int nblocks, unsigned long long* word, cudaStream_t st);
     // Per-stage reset of one block's failed-zone counter (and of the timestep minimum when word)
     static void stage_reset(int* count, unsigned long long* word, cudaStream_t st);

@@ -427,3 +427,29 @@ def ct_curl_faces(spec, B0=(1.0, 0.0, 0.0), amp=0.05):
     Bf[1] = B0[1] - ((A[:-1, 1:] - A[:-1, :-1]) / dx1)[None]       # -(A(i+1, j) - A(i, j)) / dx1
     Bf[2] = B0[2]
     return Bf
+
+
+
+# ------------------------------------------------------------------------ hydro entropy wave
+def entropy_wave(spec, amp=0.1, v=(0.3, 0.2, 0.1), t=0.0, gam=None):
+    """Hydro (5-variable) entropy wave on a periodic unit box in Minkowski space: rho = 1 + amp
+    sin(2 pi (x1 + x2 + x3 - (v1 + v2 + v3) t)) over the active directions, uniform pressure (u = 1)
+    and uniform 3-velocity v (primitive u^i = W v^i).  An exact solution, advected at v."""
+    n3, n2, n1 = spec.shape
+    x1, x2, x3 = cell_centers(spec)
+    X3, X2, X1 = np.meshgrid(x3, x2, x1, indexing="ij")
+    ph = X1 - v[0] * t
+    vv = [v[0], 0.0, 0.0]
+    if spec.nx2 > 1:
+        ph = ph + X2 - v[1] * t
+        vv[1] = v[1]
+    if spec.nx3 > 1:
+        ph = ph + X3 - v[2] * t
+        vv[2] = v[2]
+    W = 1.0 / math.sqrt(1.0 - sum(c * c for c in vv))
+    P = np.zeros((5, n3, n2, n1))
+    P[0] = 1.0 + amp * np.sin(2 * np.pi * ph)
+    P[1] = 1.0
+    for d in range(3):
+        P[2 + d] = W * vv[d]
+    return P

@@ -1,0 +1,127 @@
+"""Static mesh refinement through the batch (khb_batch_set_mesh): a two-level hydro mesh on a
+periodic box.
+
+* The ghost zones the library fills after an exchange equal, bitwise, the oracle-side restatement
+  built from whole-domain arrays (oracle/smr_ref.py).
+* With flux correction the mesh conserves mass to rounding, and energy and momentum as well as the
+  unrefined mesh does (the lock-step U = U(P) after the inversion limits both to the inversion's
+  tolerance); without it, mass is not conserved (the check has teeth).
+* A uniform state stays exactly uniform across the refinement boundary.
+* An entropy wave advected across the refined patch: the mesh's error lies between those of the
+  uniform coarse and uniform fine meshes.
+"""
+import dataclasses
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from kharma_b200 import problems
+from kharma_b200.mesh import SMRMesh, conserved_totals, smr_batch
+from kharma_b200.spec import BlockSpec
+
+pytestmark = pytest.mark.gpu
+
+_spec = importlib.util.spec_from_file_location(
+    "smr_ref", os.path.join(os.path.dirname(__file__), "..", "oracle", "smr_ref.py"))
+smr_ref = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(smr_ref)
+
+
+def base(nd, recon="linear_mc"):
+    return BlockSpec(nx1=16, nx2=16 if nd > 1 else 1, nx3=16 if nd > 2 else 1, x1min=0., x1max=1., x2min=0.,
+                     x2max=1., x3min=0., x3max=1., gam=5. / 3., nvar=5, recon=recon, cfl=0.8, dt_min=1e-4)
+
+
+def mesh_of(nd, refine=((0, 0, 0),), nx=16, nb=2, recon="linear_mc"):
+    return SMRMesh(base(nd, recon), (nb, nb, nb if nd > 2 else 1), (nx, nx, nx if nd > 2 else 1), refine=refine)
+
+
+def random_smooth(spec, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    P = problems.entropy_wave(spec, amp=0.1)
+    P[0] *= 1 + 0.05 * rng.standard_normal(P[0].shape)
+    P[1] *= 1 + 0.05 * rng.standard_normal(P[1].shape)
+    P[2:5] += 0.05 * rng.standard_normal(P[2:5].shape)
+    return P
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_exchange_matches_restatement(nd):
+    mesh = mesh_of(nd)
+    seeds = iter(range(1000))
+    b = smr_batch(mesh, lambda s: random_smooth(s, next(seeds)))
+    torch.cuda.synchronize()
+    P = [blk.P.cpu().numpy() for blk in b.blocks]
+    for n, ((mask, E), Pb) in enumerate(zip(smr_ref.expected_ghosts(mesh, P), P)):
+        got, want = Pb[:, mask], E[:, mask]
+        assert np.array_equal(got, want), (n, mesh.blocks[n].level, np.abs(got - want).max())
+
+
+def run(mesh, flux_correction, steps=10, init=None):
+    b = smr_batch(mesh, init or (lambda s: random_smooth(s, 3)), flux_correction=flux_correction)
+    t0 = conserved_totals(mesh, b)
+    dt = 0.2 * min(blk.spec.dx[0] for blk in mesh.blocks)
+    for _ in range(steps):
+        b.step(dt)
+    torch.cuda.synchronize()
+    assert not any(blk.pflag.any() for blk in b.blocks)
+    return b, t0, conserved_totals(mesh, b)
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_flux_correction_conserves(nd):
+    _, r0, r1 = run(mesh_of(nd, refine=()), True)
+    mesh = mesh_of(nd)
+    _, t0, t1 = run(mesh, True)
+    scale = np.abs(t0).max()
+    uniform = np.abs(r1 - r0) / scale
+    refined = np.abs(t1 - t0) / scale
+    print("relative change of the conserved totals, unrefined:", uniform, "refined:", refined)
+    assert refined[0] <= 1e-13
+    assert np.all(refined <= 10 * uniform + 1e-13)
+    _, u0, u1 = run(mesh, False)
+    print("refined without flux correction:", np.abs(u1 - u0) / scale)
+    assert np.abs(u1[0] - u0[0]) > 1e-9 * abs(u0[0])
+
+
+def test_uniform_state_stays_uniform():
+    mesh = mesh_of(2)
+
+    def uniform(s):
+        P = np.zeros((5,) + s.shape)
+        P[0], P[1], P[2], P[3] = 1.0, 2.0, 0.2, -0.1
+        return P
+
+    b, _, _ = run(mesh, True, steps=5, init=uniform)
+    for blk in b.blocks:
+        P = blk.P.cpu().numpy()
+        ref = uniform(blk.spec)
+        assert np.abs(P - ref).max() <= 1e-14
+
+
+def test_entropy_wave_error_between_coarse_and_fine():
+    """The wave crosses the refined patch: the L1 density error of the mesh (over all leaf zones,
+    volume-weighted) lies between the uniform-coarse and uniform-fine errors."""
+    t_end = 0.5
+    errs = {}
+    for name, mesh in (("coarse", mesh_of(2, refine=())), ("fine", mesh_of(2, refine=(), nb=4)),
+                       ("smr", mesh_of(2))):
+        b = smr_batch(mesh, lambda s: problems.entropy_wave(s, amp=0.1))
+        dx = min(blk.spec.dx[0] for blk in mesh.blocks)
+        n = int(np.ceil(t_end / (0.3 * dx)))
+        for _ in range(n):
+            b.step(t_end / n)
+        torch.cuda.synchronize()
+        e, vol = 0.0, 0.0
+        for k, (mb, blk) in enumerate(zip(mesh.blocks, b.blocks)):
+            ref = problems.entropy_wave(mb.spec, amp=0.1, t=t_end)
+            sl = mb.spec.interior
+            v = mesh.zone_volume(k)
+            e += np.abs(blk.P.cpu().numpy()[0][sl] - ref[0][sl]).sum() * v
+            vol += ref[0][sl].size * v
+        errs[name] = e / vol
+    print("entropy wave L1 errors:", errs)
+    assert errs["fine"] < errs["smr"] < errs["coarse"]

@@ -1,0 +1,42 @@
+"""SMR mesh tables (kharma_b200.mesh), CPU only: every ghost zone of every block gets exactly one
+entry, prolongations only feed fine blocks and come after the copies and restrictions, and the flux
+correction covers exactly the coarse faces that border refined blocks."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from kharma_b200.mesh import OP_COPY, OP_PROLONG, OP_RESTRICT, SMRMesh
+from kharma_b200.spec import BlockSpec
+
+
+def hydro_base(nd):
+    return BlockSpec(nx1=8, nx2=8 if nd > 1 else 1, nx3=8 if nd > 2 else 1, x1min=0., x1max=1., x2min=0., x2max=1.,
+                     x3min=0., x3max=1., gam=5. / 3., nvar=5, recon="linear_mc")
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_tables_cover_every_ghost_zone_once(nd):
+    nx = (8, 8, 8 if nd > 2 else 1)
+    nb = (2, 2, 2 if nd > 2 else 1)
+    mesh = SMRMesh(hydro_base(nd), nb, nx, refine=[(0, 0, 0)])
+    ghost, n_first, flux = mesh.tables()
+    assert np.all(ghost[:n_first, 2] != OP_PROLONG) and np.all(ghost[n_first:, 2] == OP_PROLONG)
+    for b, blk in enumerate(mesh.blocks):
+        n3, n2, n1 = blk.spec.shape
+        inside = np.zeros(n3 * n2 * n1, dtype=bool)
+        inside.reshape(n3, n2, n1)[blk.spec.interior] = True
+        dst = ghost[ghost[:, 0] == b, 1]
+        assert len(np.unique(dst)) == len(dst) == (~inside).sum()
+        assert not inside[dst].any()
+        ops = ghost[ghost[:, 0] == b, 2]
+        if blk.level == 0:
+            assert not (ops == OP_PROLONG).any()
+        else:
+            assert not (ops == OP_RESTRICT).any()
+    # coarse faces bordering the refined root block: in 2D the two x1 neighbours of (0,0) see it on
+    # both of their x1 faces (periodic), likewise the x2 neighbour; 16 faces per block side
+    nface = nx[0] * (nx[2] if nd > 2 else 1)
+    expect = (3 if nd > 2 else 2) * 2 * nface
+    assert len(flux) == expect
+    assert set(flux[:, 3]) <= {b for b, blk in enumerate(mesh.blocks) if blk.level == 1}
