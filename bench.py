@@ -343,6 +343,56 @@ def batching(steps=20, warm=3):
     return out
 
 
+def smr_form(steps=20, warm=3):
+    """Static mesh refinement through the batch: a 4 x 4 x 4 root grid of 32^3 hydro blocks on the
+    periodic unit box with the central 2 x 2 x 2 roots refined (56 coarse + 64 fine blocks, 3.9M
+    zones), entropy wave, linear MC, LLF, FP64, fixed dt; the CUDA-graph step with the ghost exchange
+    and flux correction, against the same blocks stepped without the mesh tables (ghost zones then
+    carry over unchanged).  CUDA events on the batch's stream."""
+    import numpy as np
+    import torch
+    from kharma_b200 import problems
+    from kharma_b200.mesh import SMRMesh, smr_batch
+    from kharma_b200.spec import BlockSpec
+
+    base = BlockSpec(nx1=32, nx2=32, nx3=32, x1min=0., x1max=1., x2min=0., x2max=1., x3min=0., x3max=1.,
+                     gam=5. / 3., nvar=5, recon="linear_mc")
+    refine = [(i, j, k) for i in (1, 2) for j in (1, 2) for k in (1, 2)]
+    mesh = SMRMesh(base, (4, 4, 4), (32, 32, 32), refine=refine)
+    b = smr_batch(mesh, lambda sp: problems.entropy_wave(sp, amp=0.1))
+    dt = 0.3 * min(blk.spec.dx[0] for blk in mesh.blocks)
+    ghost, n_first, flux = mesh.tables()
+
+    def timed(n):
+        with torch.cuda.stream(b.torch_stream):
+            for _ in range(warm):
+                b.step_graph(dt)
+            torch.cuda.synchronize()
+            l0 = b.launch_count()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(b.torch_stream)
+            for _ in range(n):
+                b.step_graph(dt)
+            e1.record(b.torch_stream)
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, (b.launch_count() - l0) / n
+
+    ms, launches = timed(steps)
+    out = {"workload": "periodic box, 4x4x4 root blocks of 32^3 with the central 2x2x2 refined: 56 coarse + 64 fine "
+                       "blocks, 3,932,160 zones, hydro entropy wave, linear MC, LLF, FP64",
+           "ghost_entries": int(len(ghost)), "flux_entries": int(len(flux)),
+           "graph_ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0), "launches_per_step": launches}
+    empty = np.zeros((0, 6), dtype=np.int32)
+    b.set_mesh(empty, 0, empty)
+    ms0, _ = timed(steps)
+    out["without_mesh_ms_per_step"] = ms0
+    out["mesh_overhead"] = ms / ms0 - 1.0
+    del b
+    torch.cuda.empty_cache()
+    return out
+
+
 def b_ct_form(n=128, steps=20, warm=3):
     """B_CT (face-centred field, gs05_c EMFs) against the flux-CT path on the same n^3 periodic MHD
     fast mode (Minkowski, linear MC, LLF, 1D_W), fixed dt, steps launched back to back on one stream;
@@ -639,9 +689,10 @@ def gpu_arm(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_emhd:
         emhd = emhd_newton()
 
-    bct = None
+    bct = smr = None
     if rank == 0 and world == 1 and not args.no_batch:
         bct = b_ct_form()
+        smr = smr_form()
 
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
@@ -668,7 +719,7 @@ def gpu_arm(args, rank, world, local_rank):
                           "parallelism": "single block" if world == 1 else f"x3 slabs x{world} (NCCL halo exchange)",
                           "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
-               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch, "b_ct": bct,
+               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch, "b_ct": bct, "smr": smr,
                "host_driven_step": host_driven}
         print(json.dumps(out), flush=True)
 

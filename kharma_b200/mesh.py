@@ -88,112 +88,117 @@ class SMRMesh:
         """Zones along each direction of the whole domain at a level (inactive directions: 1)."""
         return [self.nb[d] * self.nx[d] * (2 ** level if d < self.ndim else 1) for d in range(3)]
 
-    def _leaf(self, level, g):
-        """Block covering global zone g (3 ints, wrapped) at `level`, or None."""
-        loc = tuple(g[d] // self.nx[d] if d < self.ndim else 0 for d in range(3))
-        return self.index.get((level, loc))
+    def _owners(self, level):
+        """Block id per logical location at a level (-1 where that level has no block), (l3, l2, l1)."""
+        nl = [self.nb[d] * (2 ** level if d < self.ndim else 1) for d in range(3)]
+        own = np.full((nl[2], nl[1], nl[0]), -1, dtype=np.int64)
+        for n, b in enumerate(self.blocks):
+            if b.level == level:
+                own[b.loc[2], b.loc[1], b.loc[0]] = n
+        return own
 
-    def _local(self, b, g):
-        """Local zone index (k, j, i) in block b of the global zone g at b's level."""
-        blk = self.blocks[b]
-        ng = self.ng
-        i = g[0] - blk.loc[0] * self.nx[0] + ng
-        j = g[1] - blk.loc[1] * self.nx[1] + ng if self.ndim > 1 else 0
-        k = g[2] - blk.loc[2] * self.nx[2] + ng if self.ndim > 2 else 0
-        return k, j, i
-
-    def _zone(self, b, kji):
-        s = self.blocks[b].spec
-        n3, n2, n1 = s.shape
-        k, j, i = kji
+    def _zone_index(self, k, j, i):
+        n3, n2, n1 = self.blocks[0].spec.shape      # every block has the same shape
         return (k * n2 + j) * n1 + i
 
     def tables(self):
+        ng, ndim, nx = self.ng, self.ndim, self.nx
+        own = [self._owners(0), self._owners(1)]
         ghost_a, ghost_b, flux = [], [], []
-        ng, ndim = self.ng, self.ndim
+        act = [d < ndim for d in range(3)]
+
+        def local(src_loc, g):
+            # local (k, j, i) of global zone(s) g in blocks at logical locations src_loc
+            return tuple((g[d] - src_loc[d] * nx[d] + ng) if act[d] else np.zeros_like(g[d]) for d in (2, 1, 0))
+
         for b, blk in enumerate(self.blocks):
-            s = blk.spec
-            n3, n2, n1 = s.shape
+            n3, n2, n1 = blk.spec.shape
             L = blk.level
             tot = self._zones_at(L)
-            for k in range(n3):
-                for j in range(n2):
-                    for i in range(n1):
-                        inside = (ng <= i < ng + self.nx[0]) and (ndim < 2 or ng <= j < ng + self.nx[1]) and \
-                                 (ndim < 3 or ng <= k < ng + self.nx[2])
-                        if inside:
-                            continue
-                        g = [(blk.loc[0] * self.nx[0] + i - ng) % tot[0],
-                             ((blk.loc[1] * self.nx[1] + j - ng) % tot[1]) if ndim > 1 else 0,
-                             ((blk.loc[2] * self.nx[2] + k - ng) % tot[2]) if ndim > 2 else 0]
-                        dst = (k * n2 + j) * n1 + i
-                        src = self._leaf(L, g)
-                        if src is not None:
-                            ghost_a.append((b, dst, OP_COPY, src, self._zone(src, self._local(src, g)), 0))
-                            continue
-                        if L == 1:
-                            gc = [g[d] // 2 if d < ndim else 0 for d in range(3)]
-                            src = self._leaf(0, gc)
-                            assert src is not None, "mesh is not 2:1 balanced"
-                            aux = sum((g[d] % 2) << d for d in range(ndim))
-                            ghost_b.append((b, dst, OP_PROLONG, src, self._zone(src, self._local(src, gc)), aux))
-                            continue
-                        gf = [2 * g[d] if d < ndim else 0 for d in range(3)]
-                        src = self._leaf(1, gf)
-                        assert src is not None, "ghost zone with no covering block"
-                        ghost_a.append((b, dst, OP_RESTRICT, src, self._zone(src, self._local(src, gf)), 0))
+            K, J, I = np.meshgrid(np.arange(n3), np.arange(n2), np.arange(n1), indexing="ij")
+            inside = np.zeros((n3, n2, n1), dtype=bool)
+            inside[blk.spec.interior] = True
+            K, J, I = K[~inside], J[~inside], I[~inside]
+            dst = (K * n2 + J) * n1 + I
+            g = [(blk.loc[0] * nx[0] + I - ng) % tot[0],
+                 ((blk.loc[1] * nx[1] + J - ng) % tot[1]) if act[1] else np.zeros_like(I),
+                 ((blk.loc[2] * nx[2] + K - ng) % tot[2]) if act[2] else np.zeros_like(I)]
+            loc = [g[d] // nx[d] if act[d] else np.zeros_like(I) for d in range(3)]
+            src = own[L][loc[2], loc[1], loc[0]]
+            same = src >= 0
+            if same.any():
+                sl = [loc[d][same] for d in range(3)]
+                gs = [g[d][same] for d in range(3)]
+                k, j, i = local(sl, gs)
+                z = self._zone_index(k, j, i)
+                ghost_a.append(np.stack([np.full(same.sum(), b), dst[same], np.full(same.sum(), OP_COPY),
+                                         src[same], z, np.zeros(same.sum(), dtype=np.int64)], axis=1))
+            rest = ~same
+            if rest.any():
+                gr = [g[d][rest] for d in range(3)]
+                if L == 1:
+                    gc = [gr[d] // 2 if act[d] else gr[d] for d in range(3)]
+                    lc = [gc[d] // nx[d] if act[d] else gc[d] for d in range(3)]
+                    s0 = own[0][lc[2], lc[1], lc[0]]
+                    assert (s0 >= 0).all(), "mesh is not 2:1 balanced"
+                    k, j, i = local(lc, gc)
+                    z = self._zone_index(k, j, i)
+                    aux = sum((gr[d] % 2) << d for d in range(ndim))
+                    ghost_b.append(np.stack([np.full(rest.sum(), b), dst[rest], np.full(rest.sum(), OP_PROLONG),
+                                             s0, z, aux], axis=1))
+                else:
+                    gf = [2 * gr[d] if act[d] else gr[d] for d in range(3)]
+                    lf = [gf[d] // nx[d] if act[d] else gf[d] for d in range(3)]
+                    s1 = own[1][lf[2], lf[1], lf[0]]
+                    assert (s1 >= 0).all(), "ghost zone with no covering block"
+                    k, j, i = local(lf, gf)
+                    z = self._zone_index(k, j, i)
+                    ghost_a.append(np.stack([np.full(rest.sum(), b), dst[rest], np.full(rest.sum(), OP_RESTRICT),
+                                             s1, z, np.zeros(rest.sum(), dtype=np.int64)], axis=1))
             # flux correction: faces of a coarse block bordering fine blocks
-            if L == 0:
-                for d in range(ndim):
-                    for side in (0, 1):
-                        # global coarse index of the zone just across the face
-                        for t in self._face_positions(blk, d):
-                            gz = list(t)
-                            gz[d] = (blk.loc[d] * self.nx[d] + (self.nx[d] if side else -1)) % tot[d]
-                            if self._leaf(0, gz) is not None:
-                                continue
-                            # the coarse face (zone index of the zone above it) in this block
-                            ci = list(t)
-                            ci[d] = blk.loc[d] * self.nx[d] + (self.nx[d] if side else 0)
-                            kji = self._local_unwrapped(b, ci)
-                            cface = self._zone(b, kji)
-                            # the fine face: 2x the coarse face index, tangential 2x
-                            tot1 = self._zones_at(1)
-                            gf = [2 * t[e] if e < ndim else 0 for e in range(3)]
-                            gf[d] = (2 * ci[d]) % tot1[d]
-                            # the fine block owning the zone above (side 1) or below (side 0) the face
-                            gown = list(gf)
-                            if not side:
-                                gown[d] = (gf[d] - 1) % tot1[d]
-                            fb = self._leaf(1, gown)
-                            assert fb is not None
-                            fk, fj, fi = self._local(fb, gown)
-                            if not side:
-                                # the face above the fine zone below it
-                                fi, fj, fk = (fi + 1, fj, fk) if d == 0 else ((fi, fj + 1, fk) if d == 1 else (fi, fj, fk + 1))
-                            flux.append((b, d + 1, cface, fb, self._zone(fb, (fk, fj, fi)), 0))
-        ghost = np.array(ghost_a + ghost_b, dtype=np.int32).reshape(-1, 6)
-        flux = np.array(flux, dtype=np.int32).reshape(-1, 6)
-        return ghost, len(ghost_a), flux
-
-    def _face_positions(self, blk, d):
-        """Global (unwrapped) coarse zone indices of the zones along block blk's faces normal to d
-        (the normal coordinate is filled in by the caller)."""
-        rng = [range(blk.loc[e] * self.nx[e], (blk.loc[e] + 1) * self.nx[e]) if e < self.ndim else range(1)
-               for e in range(3)]
-        rng[d] = range(1)
-        for c in rng[2]:
-            for bb in rng[1]:
-                for a in rng[0]:
-                    yield (a, bb, c)
-
-    def _local_unwrapped(self, b, g):
-        blk = self.blocks[b]
-        ng = self.ng
-        i = g[0] - blk.loc[0] * self.nx[0] + ng
-        j = g[1] - blk.loc[1] * self.nx[1] + ng if self.ndim > 1 else 0
-        k = g[2] - blk.loc[2] * self.nx[2] + ng if self.ndim > 2 else 0
-        return k, j, i
+            if L != 0:
+                continue
+            tot1 = self._zones_at(1)
+            for d in range(ndim):
+                # tangential global coarse indices of the face's zones
+                rng = [np.arange(blk.loc[e] * nx[e], (blk.loc[e] + 1) * nx[e]) if act[e] else np.zeros(1, dtype=np.int64)
+                       for e in range(3)]
+                rng[d] = np.zeros(1, dtype=np.int64)
+                T3, T2, T1 = np.meshgrid(rng[2], rng[1], rng[0], indexing="ij")
+                t = [T1.ravel(), T2.ravel(), T3.ravel()]
+                for side in (0, 1):
+                    across = list(t)
+                    across[d] = np.full_like(t[0], (blk.loc[d] * nx[d] + (nx[d] if side else -1)) % tot[d])
+                    la = [across[e] // nx[e] if act[e] else across[e] for e in range(3)]
+                    if (own[0][la[2], la[1], la[0]] >= 0).all():
+                        continue
+                    assert (own[0][la[2], la[1], la[0]] < 0).all()
+                    ci = list(t)
+                    ci[d] = np.full_like(t[0], blk.loc[d] * nx[d] + (nx[d] if side else 0))
+                    k, j, i = local([np.full_like(t[0], blk.loc[e]) for e in range(3)], ci)
+                    cface = self._zone_index(k, j, i)
+                    gf = [2 * t[e] if act[e] else t[e] for e in range(3)]
+                    gf[d] = (2 * ci[d]) % tot1[d]
+                    gown = list(gf)
+                    if not side:
+                        gown[d] = (gf[d] - 1) % tot1[d]
+                    lo = [gown[e] // nx[e] if act[e] else gown[e] for e in range(3)]
+                    fb = own[1][lo[2], lo[1], lo[0]]
+                    assert (fb >= 0).all()
+                    fk, fj, fi = local(lo, gown)
+                    if not side:
+                        if d == 0:
+                            fi = fi + 1
+                        elif d == 1:
+                            fj = fj + 1
+                        else:
+                            fk = fk + 1
+                    fz = self._zone_index(fk, fj, fi)
+                    flux.append(np.stack([np.full(len(fb), b), np.full(len(fb), d + 1), cface, fb, fz,
+                                          np.zeros(len(fb), dtype=np.int64)], axis=1))
+        cat = lambda parts: (np.concatenate(parts) if parts else np.zeros((0, 6), dtype=np.int64)).astype(np.int32)
+        ga, gb = cat(ghost_a), cat(ghost_b)
+        return np.concatenate([ga, gb]), len(ga), cat(flux)
 
     # ------------------------------------------------------------------ helpers
     def zone_volume(self, b):
