@@ -44,8 +44,12 @@ enum { KHB_RHO = 0, KHB_UU = 1, KHB_U1 = 2, KHB_B1 = 5, KHB_Q = 8, KHB_DP = 9 };
 
 enum { KHB_OK = 0, KHB_ERR_ARG = -1, KHB_ERR_CUDA = -2, KHB_ERR_STATE = -3, KHB_ERR_UNSUPPORTED = -4 };
 
-/* Reconstruction schemes (flux/reconstruction.hpp:49) */
-enum { KHB_RECON_DONOR_CELL = 0, KHB_RECON_LINEAR_MC = 1, KHB_RECON_WENO5 = 2, KHB_RECON_PPM = 3 };
+/* Reconstruction schemes (flux/reconstruction.hpp:49, flux.cpp:75-122; donor_cell_c gives the same
+ * states as donor_cell).  linear_vl is Parthenon's simplified van Leer PLM on a uniform grid. */
+enum { KHB_RECON_DONOR_CELL = 0, KHB_RECON_LINEAR_MC = 1, KHB_RECON_WENO5 = 2, KHB_RECON_PPM = 3,
+       KHB_RECON_LINEAR_VL = 4, KHB_RECON_WENO5_LINEAR = 5, KHB_RECON_PPMX = 6, KHB_RECON_MP5 = 7 };
+/* WENO5 lowered to linear MC (flux/low_order_edges, flux/low_order_poles; reconstruction.hpp:694-771) */
+enum { KHB_RECON_LOWER_NONE = 0, KHB_RECON_LOWER_EDGES = 1, KHB_RECON_LOWER_POLES = 2 };
 /* Riemann solvers (flux/flux.hpp:110-121) */
 enum { KHB_FLUX_LLF = 0, KHB_FLUX_HLLE = 1 };
 /* Boundary types per face (boundaries/boundaries.cpp:57-368).  KHB_BC_EXCHANGE (any face of an
@@ -100,6 +104,10 @@ typedef struct {
     /* magnetic field transport: KHB_CT_NONE is B_FluxCT (cell-centred B, flux-CT); the others are
      * B_CT (face-centred B, edge EMFs, b_field/ct_scheme, b_ct.cpp:65-67) and need the khb_ct_* calls */
     int32_t ct_scheme;
+    /* KHB_RECON_LOWER_* (weno5 only), and flux/reconstruction_fallback: faces whose reconstructed
+     * states hit the geometric floors take the PPM states (weno5, weno5_linear, linear_vl, ppmx, mp5;
+     * needs floors) */
+    int32_t recon_lower, recon_fallback;
 } khb_config;
 
 /* B_CT EMF schemes (b_ct.cpp:65): Balsara & Spicer 1999 flux averaging, Gardiner & Stone 2005

@@ -14,7 +14,8 @@ MAX_VARS = 10
 Q, DP = 8, 9           # khb_fields slots of the EMHD variables
 
 # enums (include/khb.h)
-RECON = {"donor_cell": 0, "linear_mc": 1, "weno5": 2, "ppm": 3}
+RECON = {"donor_cell": 0, "donor_cell_c": 0, "linear_mc": 1, "weno5": 2, "ppm": 3, "linear_vl": 4, "weno5_linear": 5,
+         "ppmx": 6, "mp5": 7}
 FLUX = {"llf": 0, "hlle": 1}
 BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
@@ -62,6 +63,7 @@ class KhbConfig(C.Structure):
         ("fofc", C.c_int32), ("fofc_polar_cells", C.c_int32),
         ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
         ("ct_scheme", C.c_int32),
+        ("recon_lower", C.c_int32), ("recon_fallback", C.c_int32),
     ]
 
 

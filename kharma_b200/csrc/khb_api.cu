@@ -309,7 +309,7 @@ int khb::ctx_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, 
 int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why)
 {
     if (cfg->nvar != 5 && cfg->nvar != 8) { *why = "nvar must be 5 or 8"; return KHB_ERR_UNSUPPORTED; }
-    if (cfg->recon < 0 || cfg->recon > 3) { *why = "unknown reconstruction"; return KHB_ERR_UNSUPPORTED; }
+    if (cfg->recon < 0 || cfg->recon > KHB_RECON_MP5) { *why = "unknown reconstruction"; return KHB_ERR_UNSUPPORTED; }
     if (cfg->ng < 3) { *why = "need at least 3 ghost zones"; return KHB_ERR_ARG; }
     if (cfg->nx1 < 1 || cfg->nx2 < 1 || cfg->nx3 < 1) { *why = "bad block size"; return KHB_ERR_ARG; }
     if (cfg->nx2 == 1 && cfg->nx3 > 1) { *why = "x3 active with x2 inactive"; return KHB_ERR_UNSUPPORTED; }
@@ -377,6 +377,23 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
         if (cfg->fofc) { *why = "FOFC with B_CT is not supported"; return KHB_ERR_UNSUPPORTED; }
     }
     ph.ct_scheme = cfg->ct_scheme;
+    ph.recon_extra = (cfg->recon >= KHB_RECON_LINEAR_VL) ? cfg->recon - KHB_RECON_PPM : 0;
+    if (cfg->recon_lower < KHB_RECON_LOWER_NONE || cfg->recon_lower > KHB_RECON_LOWER_POLES) {
+        *why = "unknown recon_lower";
+        return KHB_ERR_ARG;
+    }
+    if (cfg->recon_lower && cfg->recon != KHB_RECON_WENO5) {
+        *why = "lowered reconstruction near edges or poles is a weno5 option";   // flux.cpp:82-83
+        return KHB_ERR_ARG;
+    }
+    ph.weno_lower = cfg->recon_lower;
+    if (cfg->recon_fallback && (cfg->recon == KHB_RECON_DONOR_CELL || cfg->recon == KHB_RECON_LINEAR_MC ||
+                                cfg->recon == KHB_RECON_PPM)) {
+        *why = "reconstruction_fallback applies to the high-order reconstructions";
+        return KHB_ERR_UNSUPPORTED;
+    }
+    if (cfg->recon_fallback && !cfg->floors_on) { *why = "reconstruction_fallback needs floors"; return KHB_ERR_ARG; }
+    ph.recon_fallback = cfg->recon_fallback;
     std::memcpy(&ph.fl, &cfg->floors, sizeof(khb_floors));
     return KHB_OK;
 }
@@ -1012,6 +1029,8 @@ int emhd_flux_ready(khb_ctx* ctx, const khb_emhd_params* emhd, const char* who)
     if (!ctx->F10[0]) return fail(KHB_ERR_STATE, std::string(who) + ": EMHD scratch not allocated (call khb_set_connection)");
     if (ctx->nv != 8) return fail(KHB_ERR_UNSUPPORTED, std::string(who) + ": the block must carry B (nvar = 8)");
     if (ctx->fp32) return fail(KHB_ERR_UNSUPPORTED, std::string(who) + ": the EMHD path is FP64 only");
+    if (ctx->cfg.recon > KHB_RECON_PPM || ctx->ph.weno_lower || ctx->ph.recon_fallback)
+        return fail(KHB_ERR_UNSUPPORTED, std::string(who) + ": EMHD fluxes use donor cell, linear MC, WENO5 or PPM");
     return KHB_OK;
 }
 void emhd_face_range(const Dims& d, int dir, int lo[3], int cnt[3])

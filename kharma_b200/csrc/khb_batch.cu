@@ -318,6 +318,11 @@ int khb_batch_create(khb_ctx* const* blocks, int nblocks, const khb_fields* P, c
         if (!c || !c->geom_set) { delete b; return set_error(KHB_ERR_STATE, "khb_batch_create: block without geometry"); }
         if (c->ph.fofc) { delete b; return set_error(KHB_ERR_UNSUPPORTED, "khb_batch_create: fofc blocks are stepped with khb_step"); }
         if (c->ph.ct_scheme) { delete b; return set_error(KHB_ERR_UNSUPPORTED, "khb_batch_create: B_CT blocks are stepped with khb_ct_step"); }
+        if (c->cfg.recon > KHB_RECON_PPM || c->ph.weno_lower || c->ph.recon_fallback) {
+            delete b;
+            return set_error(KHB_ERR_UNSUPPORTED, "khb_batch_create: batches use donor cell, linear MC, WENO5 or PPM "
+                                                  "without lowering or fallback");
+        }
         if (x == 0) {
             b->nv = c->nv; b->recon = c->cfg.recon; b->fp32 = c->fp32; b->ndim = c->d.ndim;
         } else if (c->nv != b->nv || c->cfg.recon != b->recon || c->fp32 != b->fp32 || c->d.ndim != b->ndim ||

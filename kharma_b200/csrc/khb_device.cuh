@@ -24,7 +24,14 @@ __device__ __forceinline__ double dsqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float  dabs(float x)   { return fabsf(x); }
 __device__ __forceinline__ double dabs(double x)  { return fabs(x); }
 
-enum { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3 };
+enum { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3,
+       // the further schemes of flux/reconstruction.hpp, one kernel variant that picks the scheme
+       // at run time from Phys::recon_extra
+       RECON_EXTRA = 4,
+       // WENO5 with its lowered variants or the floor fallback (a separate kernel variant, so that
+       // plain WENO5 keeps its code)
+       RECON_WENO5X = 5 };
+enum { EX_LINEAR_VL = 1, EX_WENO5_LINEAR = 2, EX_PPMX = 3, EX_MP5 = 4 };
 
 // ------------------------------------------------------------------ reconstruction
 // flux/reconstruction.hpp:52-56
@@ -110,6 +117,166 @@ __device__ __forceinline__ R recon_left(R x1, R x2, R x3, R x4, R x5)
         if ((qc*qd) >= R(0)) return x3;
         if (dabs(qd) >= R(2)*dabs(qc)) qlv = x3 - R(2)*qc;
         return qlv;
+    }
+}
+
+// ------------------------------------------------------------------ further reconstructions
+__device__ __forceinline__ double kcopysign(double a, double b) { return ::copysign(a, b); }
+__device__ __forceinline__ float kcopysign(float a, float b) { return copysignf(a, b); }
+// MC slope with a limiter coefficient (reconstruction.hpp:58-63)
+template <typename R>
+__device__ __forceinline__ R mc_alpha(R dm, R dp, R alpha)
+{
+    const R dc = (dm * dp > R(0)) ? R(0.5) * (dm + dp) : R(0);
+    return kcopysign(kmin(dabs(dc), alpha * kmin(dabs(dm), dabs(dp))), dc);
+}
+
+template <typename R>
+__device__ __forceinline__ R minmod_r(R a, R b) { return (a * b > R(0)) ? ((dabs(a) < dabs(b)) ? a : b) : R(0); }
+
+// Linearized WENO5 (reconstruction.hpp:209-268): both faces of the zone x3; formed in FP64 (its
+// epsilon, 1e-100, is below FP32's range)
+__device__ __forceinline__ void weno5_linear_lr(double x1, double x2, double x3, double x4, double x5,
+                                                double& lout, double& rout)
+{
+    const double a00 = 1.0 / 3.0, a01 = -7.0 / 6.0, a02 = 11.0 / 6.0;
+    const double a10 = -1.0 / 6.0, a11 = 5.0 / 6.0, a12 = 1.0 / 3.0;
+    const double a20 = 1.0 / 3.0, a21 = 5.0 / 6.0, a22 = -1.0 / 6.0;
+    const double g0 = 0.1, g1 = 0.6, g2 = 0.3;
+    const double eps = 1e-100, tt = 13.0 / 3.0;
+    double a = x1 - 2 * x2 + x3;
+    double b = x1 - 4.0 * x2 + 3.0 * x3;
+    double beta0 = tt * a * a + b * b + eps;
+    a = x2 - 2.0 * x3 + x4;
+    b = x4 - x2;
+    double beta1 = tt * a * a + b * b + eps;
+    a = x3 - 2.0 * x4 + x5;
+    b = x5 - 4.0 * x4 + 3.0 * x3;
+    double beta2 = tt * a * a + b * b + eps;
+    const double tau5 = fabs(beta2 - beta0);
+    beta0 = (beta0 + tau5) / beta0;
+    beta1 = (beta1 + tau5) / beta1;
+    beta2 = (beta2 + tau5) / beta2;
+    double w0 = g0 * beta0 + eps, w1 = g1 * beta1 + eps, w2 = g2 * beta2 + eps;
+    double wsum = 1.0 / (w0 + w1 + w2);
+    rout = w0 * (a00 * x1 + a01 * x2 + a02 * x3);
+    rout += w1 * (a10 * x2 + a11 * x3 + a12 * x4);
+    rout += w2 * (a20 * x3 + a21 * x4 + a22 * x5);
+    rout *= wsum;
+    const double alpha_r = 3.0 * wsum * w0 * w1 * w2 / (g2 * w0 * w1 + g1 * w0 * w2 + g0 * w1 * w2) + eps;
+    w0 = g0 * beta2 + eps; w1 = g1 * beta1 + eps; w2 = g2 * beta0 + eps;
+    wsum = 1.0 / (w0 + w1 + w2);
+    lout = w0 * (a00 * x5 + a01 * x4 + a02 * x3);
+    lout += w1 * (a10 * x4 + a11 * x3 + a12 * x2);
+    lout += w2 * (a20 * x3 + a21 * x2 + a22 * x1);
+    lout *= wsum;
+    const double alpha_l = 3.0 * wsum * w0 * w1 * w2 / (g2 * w0 * w1 + g1 * w0 * w2 + g0 * w1 * w2) + eps;
+    const double dq = mc_alpha<double>(x3 - x2, x4 - x3, 2.0);
+    const double alpha_lin = 2.0 * alpha_r * alpha_l / (alpha_r + alpha_l);
+    rout = alpha_lin * rout + (1.0 - alpha_lin) * (x3 + 0.5 * dq);
+    lout = alpha_lin * lout + (1.0 - alpha_lin) * (x3 - 0.5 * dq);
+}
+
+// MP5 (Suresh & Huynh 1997) as reconstruction.hpp:284-325 has it: the value at the face between
+// Fj and Fjp1
+template <typename R>
+__device__ __forceinline__ R mp5_subcalc(R Fjm2, R Fjm1, R Fj, R Fjp1, R Fjp2)
+{
+    const R alpha = R(4.0), epsm = R(1.e-12);
+    R f = R(2.0) * Fjm2 - R(13.0) * Fjm1 + R(47.0) * Fj + R(27.0) * Fjp1 - R(3.0) * Fjp2;
+    f /= R(60.0);
+    const R fMP = Fj + minmod_r(Fjp1 - Fj, alpha * (Fj - Fjm1));
+    if ((f - Fj) * (f - fMP) <= epsm) return f;
+    const R d2m = Fjm2 + Fj - R(2.0) * Fjm1;
+    const R d2 = Fjm1 + Fjp1 - R(2.0) * Fj;
+    const R d2p = Fj + Fjp2 - R(2.0) * Fjp1;
+    R scrh1 = minmod_r(R(4.0) * d2 - d2p, R(4.0) * d2p - d2);
+    R scrh2 = minmod_r(d2, d2p);
+    const R dMMp = minmod_r(scrh1, scrh2);
+    scrh1 = minmod_r(R(4.0) * d2m - d2, R(4.0) * d2 - d2m);
+    scrh2 = minmod_r(d2, d2m);
+    const R dMMm = minmod_r(scrh1, scrh2);
+    const R fUL = Fj + alpha * (Fj - Fjm1);
+    const R fAV = R(0.5) * (Fj + Fjp1);
+    const R fMD = fAV - R(0.5) * dMMp;
+    const R fLC = R(0.5) * (R(3.0) * Fj - Fjm1) + R(4.0 / 3.0) * dMMm;
+    scrh1 = kmin(kmin(Fj, Fjp1), fMD);
+    scrh2 = kmin(kmin(Fj, fUL), fLC);
+    const R mn = kmax(scrh1, scrh2);
+    scrh1 = kmax(kmax(Fj, Fjp1), fMD);
+    scrh2 = kmax(kmax(Fj, fUL), fLC);
+    const R mx = kmin(scrh1, scrh2);
+    return f + minmod_r(mn - f, mx - f);       // Median(f, mn, mx)
+}
+
+// PPMX, extremum-preserving PPM with Colella & Sekora limiters (reconstruction.hpp:403-495)
+template <typename R>
+__device__ __forceinline__ R sgn_r(R x) { return (x < R(0)) ? R(-1) : R(1); }
+template <typename R>
+__device__ __forceinline__ void ppmx_lr(R q_im2, R q_im1, R q_i, R q_ip1, R q_ip2, R& qlv, R& qrv)
+{
+    qlv = (R(7.) * (q_i + q_im1) - (q_im2 + q_ip1)) / R(12.0);
+    qrv = (R(7.) * (q_i + q_ip1) - (q_im1 + q_ip2)) / R(12.0);
+    R d2qc = R(3.0) * ((q_im1 + q_i) - R(2.0) * qlv);
+    R d2ql = (q_im2 + q_i) - R(2.0) * q_im1;
+    R d2qr = (q_im1 + q_ip1) - R(2.0) * q_i;
+    R d2qlim = R(0.0);
+    R lim_slope = kmin(dabs(d2ql), dabs(d2qr));
+    if (d2qc > R(0) && d2ql > R(0) && d2qr > R(0)) d2qlim = sgn_r(d2qc) * kmin(R(1.25) * lim_slope, dabs(d2qc));
+    if (d2qc < R(0) && d2ql < R(0) && d2qr < R(0)) d2qlim = sgn_r(d2qc) * kmin(R(1.25) * lim_slope, dabs(d2qc));
+    if (((q_im1 - qlv) * (q_i - qlv)) > R(0)) qlv = R(0.5) * (q_i + q_im1) - d2qlim / R(6.0);
+    d2qc = R(3.0) * ((q_i + q_ip1) - R(2.0) * qrv);
+    d2ql = d2qr;
+    d2qr = (q_i + q_ip2) - R(2.0) * q_ip1;
+    d2qlim = R(0.0);
+    lim_slope = kmin(dabs(d2ql), dabs(d2qr));
+    if (d2qc > R(0) && d2ql > R(0) && d2qr > R(0)) d2qlim = sgn_r(d2qc) * kmin(R(1.25) * lim_slope, dabs(d2qc));
+    if (d2qc < R(0) && d2ql < R(0) && d2qr < R(0)) d2qlim = sgn_r(d2qc) * kmin(R(1.25) * lim_slope, dabs(d2qc));
+    if (((q_i - qrv) * (q_ip1 - qrv)) > R(0)) qrv = R(0.5) * (q_i + q_ip1) - d2qlim / R(6.0);
+    const R qa = (qrv - q_i) * (q_i - qlv);
+    const R qb = (q_im1 - q_i) * (q_i - q_ip1);
+    if (qa <= R(0) || qb <= R(0)) {
+        const R d2q = R(6.0) * (qlv + qrv - R(2.0) * q_i);
+        const R c = (q_im1 + q_ip1) - R(2.0) * q_i;
+        const R l = (q_im2 + q_i) - R(2.0) * q_im1;
+        const R r = (q_i + q_ip2) - R(2.0) * q_ip1;
+        d2qlim = R(0.0);
+        lim_slope = kmin(dabs(l), dabs(r));
+        lim_slope = kmin(dabs(c), lim_slope);
+        if (c > R(0) && l > R(0) && r > R(0) && d2q > R(0)) d2qlim = sgn_r(d2q) * kmin(R(1.25) * lim_slope, dabs(d2q));
+        if (c < R(0) && l < R(0) && r < R(0) && d2q < R(0)) d2qlim = sgn_r(d2q) * kmin(R(1.25) * lim_slope, dabs(d2q));
+        R rho = R(0.0);
+        if (dabs(d2q) > R(1.0e-12) * kmax(dabs(q_im1), kmax(dabs(q_i), dabs(q_ip1)))) rho = d2qlim / d2q;
+        qlv = q_i + (qlv - q_i) * rho;
+        qrv = q_i + (qrv - q_i) * rho;
+    } else {
+        const R qc = qrv - q_i, qd = qlv - q_i;
+        if (dabs(qc) >= R(2.0) * dabs(qd)) qrv = q_i - R(2.0) * qd;
+        if (dabs(qd) >= R(2.0) * dabs(qc)) qlv = q_i - R(2.0) * qc;
+    }
+}
+
+// Right / left face value of zone x3 by the scheme `ex` (EX_*); linear van Leer is the simplified
+// VL limiter of Parthenon's PiecewiseLinear on a uniform grid (2 dql dqr / (dql + dqr) where the
+// one-sided differences agree in sign)
+template <typename R>
+__device__ __forceinline__ R recon_extra(int ex, bool right, R x1, R x2, R x3, R x4, R x5)
+{
+    if (ex == EX_LINEAR_VL) {
+        const R dql = x3 - x2, dqr = x4 - x3;
+        const R dq2 = dql * dqr;
+        const R dqm = (dq2 > R(0)) ? R(2.0) * dq2 / (dql + dqr) : R(0);
+        return right ? x3 + R(0.5) * dqm : x3 - R(0.5) * dqm;
+    } else if (ex == EX_WENO5_LINEAR) {
+        double l, r;
+        weno5_linear_lr(x1, x2, x3, x4, x5, l, r);
+        return (R)(right ? r : l);
+    } else if (ex == EX_PPMX) {
+        R l, r;
+        ppmx_lr<R>(x1, x2, x3, x4, x5, l, r);
+        return right ? r : l;
+    } else {
+        return right ? mp5_subcalc<R>(x1, x2, x3, x4, x5) : mp5_subcalc<R>(x5, x4, x3, x2, x1);
     }
 }
 

@@ -150,19 +150,55 @@ __device__ __forceinline__ void flux_face(const Dims& d, const DevGeom& g, const
 
     // reconstruction: left state = right face of zone c-st, right state = left face of zone c
     R Pl[NV], Pr[NV];
+    // WENO5 lowered to linear MC (reconstruction.hpp:694-771): near the X1 block edges for X1 faces
+    // (zones within 4 of the first and 2 of the last interior zone, as ReconstructX1's split of the
+    // [is-1, ie+2] zone range places them), or in the rows j <= 6 and j >= n2 - 6 for every direction
+    bool mc_l = false, mc_r = false;
+    if (RECON == RECON_WENO5X && ph.weno_lower) {
+        if (ph.weno_lower == 1) {
+            if (dir == 1) {
+                mc_l = (i - 1 <= d.is + 3) || (i - 1 >= d.ie - 2);
+                mc_r = (i <= d.is + 3) || (i >= d.ie - 2);
+            }
+        } else {
+            mc_l = mc_r = !(j > 6 && j < d.n2 - 6);
+        }
+    }
 #pragma unroll
     for (int p = 0; p < NV; ++p) {
         const double* q = P.v[p];
         const R x0 = (R)__ldg(q + c - 3*st), x1 = (R)__ldg(q + c - 2*st), x2 = (R)__ldg(q + c - st);
         const R x3 = (R)__ldg(q + c), x4 = (R)__ldg(q + c + st), x5 = (R)__ldg(q + c + 2*st);
-        Pl[p] = recon_right<RECON, R>(x0, x1, x2, x3, x4);
-        Pr[p] = recon_left<RECON, R>(x1, x2, x3, x4, x5);
+        if (RECON == RECON_EXTRA) {
+            Pl[p] = recon_extra<R>(ph.recon_extra, true, x0, x1, x2, x3, x4);
+            Pr[p] = recon_extra<R>(ph.recon_extra, false, x1, x2, x3, x4, x5);
+        } else if (RECON == RECON_WENO5X) {
+            Pl[p] = mc_l ? recon_right<RECON_MC, R>(x0, x1, x2, x3, x4) : recon_right<RECON_WENO5, R>(x0, x1, x2, x3, x4);
+            Pr[p] = mc_r ? recon_left<RECON_MC, R>(x1, x2, x3, x4, x5) : recon_left<RECON_WENO5, R>(x1, x2, x3, x4, x5);
+        } else {
+            Pl[p] = recon_right<RECON, R>(x0, x1, x2, x3, x4);
+            Pr[p] = recon_left<RECON, R>(x1, x2, x3, x4, x5);
+        }
     }
-    if (ph.recon_floors) {
-        // floors_functions.hpp:320-354 applied to both reconstructed states (get_flux.hpp:174-181)
+    constexpr bool HIGH = (RECON == RECON_WENO5X || RECON == RECON_EXTRA);
+    if (ph.recon_floors || (HIGH && ph.recon_fallback)) {
+        // floors_functions.hpp:301-333 applied to both reconstructed states (get_flux.hpp:174-181)
         const double rf = __ldg(g.floor_rho + (long long)j*g.n1 + i), uf = __ldg(g.floor_u + (long long)j*g.n1 + i);
+        const bool hit = ((R)rf > Pl[0]) || ((R)uf > Pl[1]) || ((R)rf > Pr[0]) || ((R)uf > Pr[1]);
         Pl[0] += kmax(R(0), (R)rf - Pl[0]); Pl[1] += kmax(R(0), (R)uf - Pl[1]);
         Pr[0] += kmax(R(0), (R)rf - Pr[0]); Pr[1] += kmax(R(0), (R)uf - Pr[1]);
+        if (HIGH && ph.recon_fallback && hit) {
+            // reconstruction_fallback (get_flux.hpp:185-199): a face whose states hit the floors
+            // takes the PPM states instead
+#pragma unroll
+            for (int p = 0; p < NV; ++p) {
+                const double* q = P.v[p];
+                const R x0 = (R)__ldg(q + c - 3*st), x1 = (R)__ldg(q + c - 2*st), x2 = (R)__ldg(q + c - st);
+                const R x3 = (R)__ldg(q + c), x4 = (R)__ldg(q + c + st), x5 = (R)__ldg(q + c + 2*st);
+                Pl[p] = recon_right<RECON_PPM, R>(x0, x1, x2, x3, x4);
+                Pr[p] = recon_left<RECON_PPM, R>(x1, x2, x3, x4, x5);
+            }
+        }
     }
 
     constexpr bool HAS_B = NV > 5;
@@ -1258,7 +1294,9 @@ static void flux_dir_recon(int recon, const Dims& d, const DevGeom& g, const Phy
     case RECON_DONOR: k_flux<DIR, RECON_DONOR, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
     case RECON_MC:    k_flux<DIR, RECON_MC, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
     case RECON_WENO5: k_flux<DIR, RECON_WENO5, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
-    default:          k_flux<DIR, RECON_PPM, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
+    case RECON_PPM:   k_flux<DIR, RECON_PPM, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
+    case RECON_WENO5X: k_flux<DIR, RECON_WENO5X, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
+    default:          k_flux<DIR, RECON_EXTRA, NV, FT, FT><<<nb, 128, 0, st>>>(d, g, ph, P, F, ctop, bx); break;
     }
 }
 
@@ -1275,8 +1313,12 @@ template <typename FT>
 void Launch<FT>::flux(int recon, int nv, int dir, const Dims& d, const DevGeom& g, const Phys& ph,
                       const khb_fields& P, FT* F, FT* ctop, const int lo[3], const int cnt[3], cudaStream_t st)
 {
-    if (nv == 8) flux_nv<8, FT>(recon, dir, d, g, ph, P, F, ctop, lo, cnt, st);
-    else flux_nv<5, FT>(recon, dir, d, g, ph, P, F, ctop, lo, cnt, st);
+    // the kernel variant: KHB_RECON_* 0-3 as they are, 4-7 through RECON_EXTRA, WENO5 with lowering
+    // or the floor fallback through RECON_WENO5X
+    const int kr = (recon > RECON_PPM) ? RECON_EXTRA
+                 : ((recon == RECON_WENO5 && (ph.weno_lower || ph.recon_fallback)) ? RECON_WENO5X : recon);
+    if (nv == 8) flux_nv<8, FT>(kr, dir, d, g, ph, P, F, ctop, lo, cnt, st);
+    else flux_nv<5, FT>(kr, dir, d, g, ph, P, F, ctop, lo, cnt, st);
 }
 
 template <typename FT>

@@ -54,6 +54,9 @@ struct Phys {
     int fofc, fofc_polar_cells;            // first-order flux correction
     double fofc_r_mark;                    // r_horizon + fofc/eh_buffer (spherical coordinates)
     int ct_scheme;                         // KHB_CT_* (B_CT face-centred field when nonzero)
+    int recon_extra;                       // EX_* scheme of the RECON_EXTRA flux kernels
+    int weno_lower;                        // WENO5 lowered to MC: 1 near X1 block edges, 2 near the poles
+    int recon_fallback;                    // faces whose reconstructed states hit the floors take PPM
     Prescription fl;
 };
 

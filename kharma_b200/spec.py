@@ -60,6 +60,9 @@ class BlockSpec:
     riemann: str = "llf"
     precision: str = "fp64"
     recon_floors: bool = False
+    low_order_edges: bool = False       # flux/low_order_edges (weno5 only)
+    low_order_poles: bool = False       # flux/low_order_poles (weno5 only)
+    recon_fallback: bool = False        # flux/reconstruction_fallback
     # coordinates (coordinate_embedding.hpp:119-210)
     base: str = "cartesian_minkowski"
     transform: str = "null"
@@ -159,6 +162,8 @@ class BlockSpec:
         c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(self.fofc), self.fofc_polar_cells, self.fofc_eh_buffer
         c.r_horizon = self.r_horizon
         c.ct_scheme = _lib.CT_SCHEME[self.b_ct]
+        c.recon_lower = 1 if self.low_order_edges else (2 if self.low_order_poles else 0)
+        c.recon_fallback = int(self.recon_fallback)
         return c
 
     @property

@@ -73,7 +73,8 @@ struct CoordSpec {
     double a, hslope, mks_smooth, poly_xt, poly_alpha, startx1;
 };
 
-enum Recon { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3 };
+enum Recon { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3, RECON_LINEAR_VL = 4,
+             RECON_WENO5_LINEAR = 5, RECON_PPMX = 6, RECON_MP5 = 7 };
 enum BC { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2, BC_EXCHANGE = 3 };
 // Exchange faces are internal block boundaries whose ghost zones the caller fills (Parthenon's
 // boundary communication); only outflow and reflecting faces are global "user" boundaries.
@@ -99,6 +100,8 @@ struct Config {
     int32_t fofc, fofc_polar_cells;                 // fofc/on, fofc/polar_cells
     double fofc_eh_buffer, r_horizon;               // fofc/eh_buffer, coords.get_horizon()
     int32_t ct_scheme;                              // 0 B_FluxCT; B_CT: 1 bs99, 2 gs05_0, 3 gs05_c (b_ct.cpp:65)
+    int32_t recon_lower;                            // weno5 lowered to MC: 1 low_order_edges, 2 low_order_poles
+    int32_t recon_fallback;                         // flux/reconstruction_fallback
 };
 
 // ---------------------------------------------------------------- coordinates
@@ -463,9 +466,152 @@ static inline double mc(double dm, double dp)
     return kmax(0.0, kmin(2.0, kmin(2*r, 0.5*(1+r))));
 }
 // Single-zone reconstruction: lout = value at the left face of the zone, rout = at the right face
+// reconstruction.hpp:58-63 (mc with a limiter coefficient) and 66-71 (MINMOD, Median)
+static inline double mc_alpha(double dm, double dp, double alpha)
+{
+    const double dc = (dm * dp > 0.0) * 0.5 * (dm + dp);
+    return std::copysign(std::min(std::fabs(dc), alpha * std::min(std::fabs(dm), std::fabs(dp))), dc);
+}
+static inline double minmod(double a, double b) { return a * b > 0.0 ? (std::fabs(a) < std::fabs(b) ? a : b) : 0.0; }
+static inline double median(double a, double b, double c) { return a + minmod(b - a, c - a); }
+
+// reconstruction.hpp:284-325
+static double mp5_subcalc(double Fjm2, double Fjm1, double Fj, double Fjp1, double Fjp2)
+{
+    const double alpha = 4.0, epsm = 1.e-12;
+    double f = 2.0 * Fjm2 - 13.0 * Fjm1 + 47.0 * Fj + 27.0 * Fjp1 - 3.0 * Fjp2;
+    f /= 60.0;
+    const double fMP = Fj + minmod(Fjp1 - Fj, alpha * (Fj - Fjm1));
+    if ((f - Fj) * (f - fMP) <= epsm) return f;
+    const double d2m = Fjm2 + Fj - 2.0 * Fjm1;
+    const double d2 = Fjm1 + Fjp1 - 2.0 * Fj;
+    const double d2p = Fj + Fjp2 - 2.0 * Fjp1;
+    double scrh1 = minmod(4.0 * d2 - d2p, 4.0 * d2p - d2);
+    double scrh2 = minmod(d2, d2p);
+    const double dMMp = minmod(scrh1, scrh2);
+    scrh1 = minmod(4.0 * d2m - d2, 4.0 * d2 - d2m);
+    scrh2 = minmod(d2, d2m);
+    const double dMMm = minmod(scrh1, scrh2);
+    const double fUL = Fj + alpha * (Fj - Fjm1);
+    const double fAV = 0.5 * (Fj + Fjp1);
+    const double fMD = fAV - 0.5 * dMMp;
+    const double fLC = 0.5 * (3.0 * Fj - Fjm1) + 4.0 / 3.0 * dMMm;
+    scrh1 = kmin(kmin(Fj, Fjp1), fMD);
+    scrh2 = kmin(kmin(Fj, fUL), fLC);
+    const double mn = kmax(scrh1, scrh2);
+    scrh1 = kmax(kmax(Fj, Fjp1), fMD);
+    scrh2 = kmax(kmax(Fj, fUL), fLC);
+    const double mx = kmin(scrh1, scrh2);
+    return median(f, mn, mx);
+}
+
+static inline double sgn(double x) { return (x < 0.0) ? -1.0 : 1.0; }
+
 static void recon_zone(int recon, double x1, double x2, double x3, double x4, double x5, double& lout, double& rout)
 {
     switch (recon) {
+    case RECON_LINEAR_VL: {
+        // Parthenon PiecewiseLinear, simplified van Leer limiter on a uniform grid
+        const double dql = x3 - x2, dqr = x4 - x3;
+        const double dq2 = dql * dqr;
+        double dqm = 0.0;
+        if (dq2 > 0.0) dqm = 2.0 * dq2 / (dql + dqr);
+        rout = x3 + 0.5 * dqm;
+        lout = x3 - 0.5 * dqm;
+        break;
+    }
+    case RECON_WENO5_LINEAR: {      // reconstruction.hpp:209-268
+        const double w5alpha[3][3] = {{1.0 / 3.0, -7.0 / 6.0, 11.0 / 6.0},
+                                      {-1.0 / 6.0, 5.0 / 6.0, 1.0 / 3.0},
+                                      {1.0 / 3.0, 5.0 / 6.0, -1.0 / 6.0}};
+        const double w5gamma[3] = {0.1, 0.6, 0.3};
+        const double eps = 1e-100, thirteen_thirds = 13.0 / 3.0;
+        double a = x1 - 2 * x2 + x3;
+        double b = x1 - 4.0 * x2 + 3.0 * x3;
+        double beta0 = thirteen_thirds * a * a + b * b + eps;
+        a = x2 - 2.0 * x3 + x4;
+        b = x4 - x2;
+        double beta1 = thirteen_thirds * a * a + b * b + eps;
+        a = x3 - 2.0 * x4 + x5;
+        b = x5 - 4.0 * x4 + 3.0 * x3;
+        double beta2 = thirteen_thirds * a * a + b * b + eps;
+        const double tau5 = std::fabs(beta2 - beta0);
+        beta0 = (beta0 + tau5) / beta0;
+        beta1 = (beta1 + tau5) / beta1;
+        beta2 = (beta2 + tau5) / beta2;
+        double w0 = w5gamma[0] * beta0 + eps, w1 = w5gamma[1] * beta1 + eps, w2 = w5gamma[2] * beta2 + eps;
+        double wsum = 1.0 / (w0 + w1 + w2);
+        rout = w0 * (w5alpha[0][0] * x1 + w5alpha[0][1] * x2 + w5alpha[0][2] * x3);
+        rout += w1 * (w5alpha[1][0] * x2 + w5alpha[1][1] * x3 + w5alpha[1][2] * x4);
+        rout += w2 * (w5alpha[2][0] * x3 + w5alpha[2][1] * x4 + w5alpha[2][2] * x5);
+        rout *= wsum;
+        const double alpha_r = 3.0 * wsum * w0 * w1 * w2 /
+                               (w5gamma[2] * w0 * w1 + w5gamma[1] * w0 * w2 + w5gamma[0] * w1 * w2) + eps;
+        w0 = w5gamma[0] * beta2 + eps; w1 = w5gamma[1] * beta1 + eps; w2 = w5gamma[2] * beta0 + eps;
+        wsum = 1.0 / (w0 + w1 + w2);
+        lout = w0 * (w5alpha[0][0] * x5 + w5alpha[0][1] * x4 + w5alpha[0][2] * x3);
+        lout += w1 * (w5alpha[1][0] * x4 + w5alpha[1][1] * x3 + w5alpha[1][2] * x2);
+        lout += w2 * (w5alpha[2][0] * x3 + w5alpha[2][1] * x2 + w5alpha[2][2] * x1);
+        lout *= wsum;
+        const double alpha_l = 3.0 * wsum * w0 * w1 * w2 /
+                               (w5gamma[2] * w0 * w1 + w5gamma[1] * w0 * w2 + w5gamma[0] * w1 * w2) + eps;
+        double dq = x4 - x3;
+        dq = mc_alpha(x3 - x2, dq, 2.0);
+        const double alpha_lin = 2.0 * alpha_r * alpha_l / (alpha_r + alpha_l);
+        rout = alpha_lin * rout + (1.0 - alpha_lin) * (x3 + 0.5 * dq);
+        lout = alpha_lin * lout + (1.0 - alpha_lin) * (x3 - 0.5 * dq);
+        break;
+    }
+    case RECON_MP5:
+        lout = mp5_subcalc(x5, x4, x3, x2, x1);
+        rout = mp5_subcalc(x1, x2, x3, x4, x5);
+        break;
+    case RECON_PPMX: {              // reconstruction.hpp:403-495
+        const double q_im2 = x1, q_im1 = x2, q_i = x3, q_ip1 = x4, q_ip2 = x5;
+        double qlv = (7.*(q_i + q_im1) - (q_im2 + q_ip1))/12.0;
+        double qrv = (7.*(q_i + q_ip1) - (q_im1 + q_ip2))/12.0;
+        double d2qc = 3.0*((q_im1 + q_i) - 2.0*qlv);
+        double d2ql = (q_im2 + q_i  ) - 2.0*q_im1;
+        double d2qr = (q_im1 + q_ip1) - 2.0*q_i;
+        double d2qlim = 0.0;
+        double lim_slope = std::min(std::fabs(d2ql), std::fabs(d2qr));
+        if (d2qc > 0.0 && d2ql > 0.0 && d2qr > 0.0) d2qlim = sgn(d2qc)*std::min(1.25*lim_slope, std::fabs(d2qc));
+        if (d2qc < 0.0 && d2ql < 0.0 && d2qr < 0.0) d2qlim = sgn(d2qc)*std::min(1.25*lim_slope, std::fabs(d2qc));
+        if (((q_im1 - qlv)*(q_i - qlv)) > 0.0) qlv = 0.5*(q_i + q_im1) - d2qlim/6.0;
+        d2qc = 3.0*((q_i + q_ip1) - 2.0*qrv);
+        d2ql = d2qr;
+        d2qr = (q_i + q_ip2) - 2.0*q_ip1;
+        d2qlim = 0.0;
+        lim_slope = std::min(std::fabs(d2ql), std::fabs(d2qr));
+        if (d2qc > 0.0 && d2ql > 0.0 && d2qr > 0.0) d2qlim = sgn(d2qc)*std::min(1.25*lim_slope, std::fabs(d2qc));
+        if (d2qc < 0.0 && d2ql < 0.0 && d2qr < 0.0) d2qlim = sgn(d2qc)*std::min(1.25*lim_slope, std::fabs(d2qc));
+        if (((q_i - qrv)*(q_ip1 - qrv)) > 0.0) qrv = 0.5*(q_i + q_ip1) - d2qlim/6.0;
+        const double qa = (qrv - q_i)*(q_i - qlv);
+        const double qb = (q_im1 - q_i)*(q_i - q_ip1);
+        if (qa <= 0.0 || qb <= 0.0) {
+            const double d2q = 6.0*(qlv + qrv - 2.0*q_i);
+            const double c2 = (q_im1 + q_ip1) - 2.0*q_i;
+            const double l2 = (q_im2 + q_i  ) - 2.0*q_im1;
+            const double r2 = (q_i   + q_ip2) - 2.0*q_ip1;
+            d2qlim = 0.0;
+            lim_slope = std::min(std::fabs(l2), std::fabs(r2));
+            lim_slope = std::min(std::fabs(c2), lim_slope);
+            if (c2 > 0.0 && l2 > 0.0 && r2 > 0.0 && d2q > 0.0) d2qlim = sgn(d2q)*std::min(1.25*lim_slope, std::fabs(d2q));
+            if (c2 < 0.0 && l2 < 0.0 && r2 < 0.0 && d2q < 0.0) d2qlim = sgn(d2q)*std::min(1.25*lim_slope, std::fabs(d2q));
+            double rho = 0.0;
+            if (std::fabs(d2q) > (1.0e-12)*std::max(std::fabs(q_im1), std::max(std::fabs(q_i), std::fabs(q_ip1))))
+                rho = d2qlim/d2q;
+            qlv = q_i + (qlv - q_i)*rho;
+            qrv = q_i + (qrv - q_i)*rho;
+        } else {
+            const double qc = qrv - q_i;
+            const double qd = qlv - q_i;
+            if (std::fabs(qc) >= 2.0*std::fabs(qd)) qrv = q_i - 2.0*qd;
+            if (std::fabs(qd) >= 2.0*std::fabs(qc)) qlv = q_i - 2.0*qc;
+        }
+        lout = qlv; rout = qrv;
+        break;
+    }
     case RECON_DONOR:
         rout = x3; lout = x3;
         break;
@@ -671,19 +817,38 @@ static void get_flux(const Block& B, int dir, const double* P, double* F, double
     for (int k = k0; k <= k1; ++k) for (int j = j0; j <= j1; ++j) for (int i = i0; i <= i1; ++i) {
         const size_t c = B.id(k, j, i);
         double Pl[8], Pr[8];
+        // weno5 lowered to MC (reconstruction.hpp:694-771): X1 faces near the block's X1 edges (zones
+        // [is-1, is+3] and [ie-2, ie+2] of ReconstructX1's range), or every face in rows j <= 6 and
+        // j >= n2 - 6
+        int rl = B.c.recon, rr = B.c.recon;
+        if (B.c.recon == RECON_WENO5 && B.c.recon_lower == 1 && d1) {
+            if (i - 1 <= B.is + 3 || i - 1 >= B.ie - 2) rl = RECON_MC;
+            if (i <= B.is + 3 || i >= B.ie - 2) rr = RECON_MC;
+        }
+        if (B.c.recon == RECON_WENO5 && B.c.recon_lower == 2 && !(j > 6 && j < B.n2 - 6)) rl = rr = RECON_MC;
         for (int p = 0; p < nv; ++p) {
             const double* q = P + (size_t)p*B.N;
             double l, r;
             // Left state: right face of zone c-1 (ReconstructX1 ql(i+1) / ReconstructX{2,3}l reconstruct_right)
-            recon_zone(B.c.recon, q[c - 3*st], q[c - 2*st], q[c - st], q[c], q[c + st], l, r);
+            recon_zone(rl, q[c - 3*st], q[c - 2*st], q[c - st], q[c], q[c + st], l, r);
             Pl[p] = r;
             // Right state: left face of zone c (qr(i) / reconstruct_left)
-            recon_zone(B.c.recon, q[c - 2*st], q[c - st], q[c], q[c + st], q[c + 2*st], l, r);
+            recon_zone(rr, q[c - 2*st], q[c - st], q[c], q[c + st], q[c + 2*st], l, r);
             Pr[p] = l;
         }
-        if (B.c.recon_floors) {    // get_flux.hpp:174-181
-            apply_geo_floors_local(B, Pl, j, i);
-            apply_geo_floors_local(B, Pr, j, i);
+        if (B.c.recon_floors || B.c.recon_fallback) {    // get_flux.hpp:174-199
+            int hit = apply_geo_floors_local(B, Pl, j, i);
+            hit |= apply_geo_floors_local(B, Pr, j, i);
+            if (B.c.recon_fallback && hit) {
+                for (int p = 0; p < nv; ++p) {
+                    const double* q = P + (size_t)p*B.N;
+                    double l, r;
+                    recon_zone(RECON_PPM, q[c - 3*st], q[c - 2*st], q[c - st], q[c], q[c + st], l, r);
+                    Pl[p] = r;
+                    recon_zone(RECON_PPM, q[c - 2*st], q[c - st], q[c], q[c + st], q[c + 2*st], l, r);
+                    Pr[p] = l;
+                }
+            }
         }
         FourVectors Dl, Dr;
         double Ul[8], Fl[8], Ur[8], Fr[8], cmaxL, cminL, cmaxR, cminR;

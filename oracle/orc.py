@@ -52,10 +52,12 @@ class Config(C.Structure):
         ("fofc", C.c_int32), ("fofc_polar_cells", C.c_int32),
         ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
         ("ct_scheme", C.c_int32),
+        ("recon_lower", C.c_int32), ("recon_fallback", C.c_int32),
     ]
 
 
-RECON = {"donor_cell": 0, "linear_mc": 1, "weno5": 2, "ppm": 3}
+RECON = {"donor_cell": 0, "donor_cell_c": 0, "linear_mc": 1, "weno5": 2, "ppm": 3, "linear_vl": 4, "weno5_linear": 5,
+         "ppmx": 6, "mp5": 7}
 BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
@@ -144,6 +146,8 @@ def config_from_spec(spec):
     c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(spec.fofc), spec.fofc_polar_cells, spec.fofc_eh_buffer
     c.r_horizon = spec.r_horizon
     c.ct_scheme = {"none": 0, "bs99": 1, "gs05_0": 2, "gs05_c": 3, "sg07": 3}[spec.b_ct]
+    c.recon_lower = 1 if spec.low_order_edges else (2 if spec.low_order_poles else 0)
+    c.recon_fallback = int(spec.recon_fallback and spec.floors_on)
     for name, _ in Prescription._fields_:
         setattr(c.floors, name, type(getattr(c.floors, name))(getattr(spec.floors, name)))
     return c
