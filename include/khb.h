@@ -56,7 +56,11 @@ enum { KHB_FLUX_LLF = 0, KHB_FLUX_HLLE = 1 };
  * active direction) marks a face whose ghost zones the caller fills from the neighbouring block
  * (Parthenon's boundary communication): khb_boundaries and the flux fixes leave it alone, and
  * khb_fix_utop reads the neighbour values there. */
-enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2, KHB_BC_EXCHANGE = 3 };
+enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2, KHB_BC_EXCHANGE = 3,
+       /* transmitting polar faces (one_block_transmit.cpp:43-137): X2 faces of a 3D block covering all
+        * of x3 (periodic, even nx3) in coordinates symmetric about the pole; a ghost zone takes the
+        * mirrored zone half-way round in x3 with u^2, u^3, B^2, B^3 inverted */
+       KHB_BC_TRANSMITTING = 4 };
 /* Floor injection frames (floors/floors.hpp:96) */
 enum { KHB_FRAME_FLUID = 0, KHB_FRAME_NORMAL = 1, KHB_FRAME_DRIFT = 2 };
 /* Arithmetic of reconstruction, Riemann fluxes and EMF averaging */

@@ -17,7 +17,10 @@ Q, DP = 8, 9           # khb_fields slots of the EMHD variables
 RECON = {"donor_cell": 0, "donor_cell_c": 0, "linear_mc": 1, "weno5": 2, "ppm": 3, "linear_vl": 4, "weno5_linear": 5,
          "ppmx": 6, "mp5": 7}
 FLUX = {"llf": 0, "hlle": 1}
-BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
+# "dirichlet" and "bondi" faces hold the ghost values the caller set (boundaries/dirichlet.cpp restores
+# the values saved at initialisation; the bondi faces, the analytic solution): the exchange face's
+# carry-over of the ghost shell gives the same ghost zones
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3, "transmitting": 4, "dirichlet": 3, "bondi": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 PREC = {"fp64": 0, "fp32_flux": 1}
 INVERTER = {"onedw": 0, "kastaun": 1}

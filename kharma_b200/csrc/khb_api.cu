@@ -318,7 +318,15 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
         return KHB_ERR_UNSUPPORTED;
     }
     for (int x = 0; x < 6; ++x) {
-        if (cfg->bc[x] < KHB_BC_PERIODIC || cfg->bc[x] > KHB_BC_EXCHANGE) { *why = "unknown boundary type"; return KHB_ERR_ARG; }
+        if (cfg->bc[x] < KHB_BC_PERIODIC || cfg->bc[x] > KHB_BC_TRANSMITTING) { *why = "unknown boundary type"; return KHB_ERR_ARG; }
+        if (cfg->bc[x] == KHB_BC_TRANSMITTING) {
+            // one_block_transmit.cpp:74-75 and boundaries.cpp:297-301
+            if (x != 2 && x != 3) { *why = "transmitting boundaries are X2 faces"; return KHB_ERR_UNSUPPORTED; }
+            if (cfg->nx3 < 2 || cfg->nx3 % 2 || cfg->bc[4] != KHB_BC_PERIODIC) {
+                *why = "transmitting polar boundaries need a 3D block over all of a periodic x3 (even nx3)";
+                return KHB_ERR_UNSUPPORTED;
+            }
+        }
         const bool active = x < 2 || (x < 4 ? cfg->nx2 > 1 : cfg->nx3 > 1);
         if (cfg->bc[x] == KHB_BC_EXCHANGE && !active) {
             *why = "exchange boundaries are supported on faces of active directions only";

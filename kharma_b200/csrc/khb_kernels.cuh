@@ -767,21 +767,24 @@ __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int
     }
     const int type = d.bc[face];
     const int offset = 2 * ref + (inner ? -1 : 1);
-    int ii = i, jj = j;
+    const bool transmit = type == KHB_BC_TRANSMITTING;
+    int ii = i, jj = j, kk = k;
     if (bdir == 1) ii = (type == KHB_BC_OUTFLOW) ? ref : offset - i;
     else           jj = (type == KHB_BC_OUTFLOW) ? ref : offset - j;
+    // transmitting: the mirrored zone half-way round in x3 (one_block_transmit.cpp:116-134)
+    if (transmit) kk = ((k - d.ks + d.nx3 / 2) % d.nx3) + d.ks;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
-    const long long s = ((long long)k*d.n2 + jj)*d.n1 + ii;
+    const long long s = ((long long)kk*d.n2 + jj)*d.n1 + ii;
     double Pz[5];
 #pragma unroll
     for (int p = 0; p < 5; ++p) {
-        const bool flip = (type == KHB_BC_REFLECTING) && (p == 1 + bdir);
+        const bool flip = ((type == KHB_BC_REFLECTING) && (p == 1 + bdir)) || (transmit && (p == 3 || p == 4));
         Pz[p] = (flip ? -1.0 : 1.0) * P.v[p][s];
     }
     if (NV > 5) {
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
-            const bool flip = (type == KHB_BC_REFLECTING) && (v == bdir - 1);
+            const bool flip = ((type == KHB_BC_REFLECTING) && (v == bdir - 1)) || (transmit && v >= 1);
             U.v[5 + v][c] = (flip ? -1.0 : 1.0) * U.v[5 + v][s];
         }
     }

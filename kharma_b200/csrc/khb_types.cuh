@@ -243,7 +243,10 @@ inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1)
 
 // A face of the global domain with a physical boundary condition (outflow or reflecting), as
 // opposed to a periodic face or an exchange face filled by the caller from a neighbouring block
-__host__ __device__ inline bool phys_face(int bc) { return bc == KHB_BC_OUTFLOW || bc == KHB_BC_REFLECTING; }
+__host__ __device__ inline bool phys_face(int bc)
+{
+    return bc == KHB_BC_OUTFLOW || bc == KHB_BC_REFLECTING || bc == KHB_BC_TRANSMITTING;
+}
 
 // Validate a khb_config and derive the block index ranges and physics parameters (no allocation).
 // Returns KHB_OK or a KHB_ERR_* code with a message in *why.

@@ -75,10 +75,10 @@ struct CoordSpec {
 
 enum Recon { RECON_DONOR = 0, RECON_MC = 1, RECON_WENO5 = 2, RECON_PPM = 3, RECON_LINEAR_VL = 4,
              RECON_WENO5_LINEAR = 5, RECON_PPMX = 6, RECON_MP5 = 7 };
-enum BC { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2, BC_EXCHANGE = 3 };
+enum BC { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2, BC_EXCHANGE = 3, BC_TRANSMIT = 4 };
 // Exchange faces are internal block boundaries whose ghost zones the caller fills (Parthenon's
 // boundary communication); only outflow and reflecting faces are global "user" boundaries.
-static inline bool phys_face(int bc) { return bc == BC_OUTFLOW || bc == BC_REFLECT; }
+static inline bool phys_face(int bc) { return bc == BC_OUTFLOW || bc == BC_REFLECT || bc == BC_TRANSMIT; }
 enum Frame { FRAME_FLUID = 0, FRAME_NORMAL = 1, FRAME_DRIFT = 2 };
 
 struct Config {
@@ -1604,14 +1604,18 @@ static void physical_face(const Block& B, double* P, double* U, int face)
         } else {
             if (bdir == 1) ii = offset - i; else if (bdir == 2) jj = offset - j; else kk = offset - k;
         }
+        // transmitting polar faces (one_block_transmit.cpp:116-134): half-way round in x3, u^2, u^3,
+        // B^2, B^3 inverted
+        const bool transmit = type == BC_TRANSMIT;
+        if (transmit) kk = ((k - B.ks + B.c.nx3 / 2) % B.c.nx3) + B.ks;
         const size_t s = B.id(kk, jj, ii);
         for (int p = 0; p < 5; ++p) {
-            const bool flip = (type == BC_REFLECT) && (p == 1 + bdir);
+            const bool flip = ((type == BC_REFLECT) && (p == 1 + bdir)) || (transmit && (p == 3 || p == 4));
             P[(size_t)p*N + c] = (flip ? -1.0 : 1.0) * P[(size_t)p*N + s];
         }
         if (B.nv > 5)
             for (int v = 0; v < 3; ++v) {
-                const bool flip = (type == BC_REFLECT) && (v == bdir - 1);
+                const bool flip = ((type == BC_REFLECT) && (v == bdir - 1)) || (transmit && v >= 1);
                 U[(size_t)(5 + v)*N + c] = (flip ? -1.0 : 1.0) * U[(size_t)(5 + v)*N + s];
             }
     }

@@ -58,7 +58,7 @@ class Config(C.Structure):
 
 RECON = {"donor_cell": 0, "donor_cell_c": 0, "linear_mc": 1, "weno5": 2, "ppm": 3, "linear_vl": 4, "weno5_linear": 5,
          "ppmx": 6, "mp5": 7}
-BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3}
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3, "transmitting": 4, "dirichlet": 3, "bondi": 3}
 FRAME = {"fluid": 0, "normal": 1, "drift": 2}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
 TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
