@@ -61,8 +61,11 @@ enum { KHB_BC_PERIODIC = 0, KHB_BC_OUTFLOW = 1, KHB_BC_REFLECTING = 2, KHB_BC_EX
         * of x3 (periodic, even nx3) in coordinates symmetric about the pole; a ghost zone takes the
         * mirrored zone half-way round in x3 with u^2, u^3, B^2, B^3 inverted */
        KHB_BC_TRANSMITTING = 4 };
-/* Floor injection frames (floors/floors.hpp:96) */
-enum { KHB_FRAME_FLUID = 0, KHB_FRAME_NORMAL = 1, KHB_FRAME_DRIFT = 2 };
+/* Floor injection frames (floors/floors.hpp:93, floors.cpp:66-91): the mixed frames take the normal
+ * frame inside frame_switch_r and the fluid frame outside it, or the drift frame where
+ * min(rho, u)/b^2 < frame_switch_beta and the normal frame elsewhere (floors_impl.hpp:84-106) */
+enum { KHB_FRAME_FLUID = 0, KHB_FRAME_NORMAL = 1, KHB_FRAME_DRIFT = 2, KHB_FRAME_MIXED_FLUID_NORMAL = 3,
+       KHB_FRAME_MIXED_NORMAL_DRIFT = 4 };
 /* Arithmetic of reconstruction, Riemann fluxes and EMF averaging */
 enum { KHB_PREC_FP64 = 0, KHB_PREC_FP32_FLUX = 1 };
 /* Primitive recovery (inverter/type, inverter.cpp:54-64): 1D_W of Noble et al. (2006) or the
@@ -112,6 +115,11 @@ typedef struct {
      * states hit the geometric floors take the PPM states (weno5, weno5_linear, linear_vl, ppmx, mp5;
      * needs floors) */
     int32_t recon_lower, recon_fallback;
+    /* floors_inner (floors.hpp:155-167): the prescription for r < floors.floors_switch_r when
+     * floors.radius_dependent_floors is set (for the floors, ceilings and the Kastaun inverter's
+     * floors); the switch points of the mixed injection frames */
+    khb_floors floors_inner;
+    double frame_switch_r, frame_switch_beta;
 } khb_config;
 
 /* B_CT EMF schemes (b_ct.cpp:65): Balsara & Spicer 1999 flux averaging, Gardiner & Stone 2005

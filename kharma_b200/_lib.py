@@ -21,7 +21,7 @@ FLUX = {"llf": 0, "hlle": 1}
 # the values saved at initialisation; the bondi faces, the analytic solution): the exchange face's
 # carry-over of the ghost shell gives the same ghost zones
 BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3, "transmitting": 4, "dirichlet": 3, "bondi": 3}
-FRAME = {"fluid": 0, "normal": 1, "drift": 2}
+FRAME = {"fluid": 0, "normal": 1, "drift": 2, "mixed": 3, "mixed_fluid_normal": 3, "mixed_normal_drift": 4}
 PREC = {"fp64": 0, "fp32_flux": 1}
 INVERTER = {"onedw": 0, "kastaun": 1}
 CT_SCHEME = {"none": 0, "bs99": 1, "gs05_0": 2, "gs05_c": 3, "sg07": 3}
@@ -67,6 +67,8 @@ class KhbConfig(C.Structure):
         ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
         ("ct_scheme", C.c_int32),
         ("recon_lower", C.c_int32), ("recon_fallback", C.c_int32),
+        ("floors_inner", KhbFloors),
+        ("frame_switch_r", C.c_double), ("frame_switch_beta", C.c_double),
     ]
 
 

@@ -403,6 +403,13 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
     if (cfg->recon_fallback && !cfg->floors_on) { *why = "reconstruction_fallback needs floors"; return KHB_ERR_ARG; }
     ph.recon_fallback = cfg->recon_fallback;
     std::memcpy(&ph.fl, &cfg->floors, sizeof(khb_floors));
+    std::memcpy(&ph.fl_inner, &cfg->floors_inner, sizeof(khb_floors));
+    if (cfg->floor_frame < KHB_FRAME_FLUID || cfg->floor_frame > KHB_FRAME_MIXED_NORMAL_DRIFT) {
+        *why = "unknown floor frame";
+        return KHB_ERR_ARG;
+    }
+    ph.frame_switch_r = cfg->frame_switch_r;
+    ph.frame_switch_beta = cfg->frame_switch_beta;
     return KHB_OK;
 }
 
@@ -515,8 +522,10 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
     // geometric floors per zone centre (floors_functions.hpp:96-104), x3-independent
     double* frho = h.data() + 4*per_loc + 65*n2n1;
     double* fu = frho + n2n1;
-    const khb_floors& f = ctx->cfg.floors;
     for (size_t x = 0; x < n2n1; ++x) {
+        // the inner prescription inside floors_switch_r (floors_functions.hpp:89-90)
+        const khb_floors& f = (ctx->cfg.floors.radius_dependent_floors && r_center[x] < ctx->cfg.floors.floors_switch_r)
+                                  ? ctx->cfg.floors_inner : ctx->cfg.floors;
         if (ctx->cfg.spherical) {
             const double r = r_center[x];
             const double rhoscal = (f.use_r_char) ? 1. / ((r*r) * (1 + r / f.r_char)) : 1. / std::sqrt(r*r*r);

@@ -61,6 +61,14 @@ __device__ __forceinline__ void load_zone_geom(const DevGeom& g, int j, int i, Z
     G.gdet = __ldg(g.gdet[3] + gi);
 }
 
+// The floor prescription of zone (j, i): the inner one inside floors_switch_r when radius-dependent
+// floors are on (floors_functions.hpp:56-57, 89-90; inverter.cpp:165-168)
+__device__ __forceinline__ const Prescription& floors_at(const Phys& ph, const DevGeom& g, int j, int i)
+{
+    return (ph.fl.radius_dependent_floors && __ldg(g.rcen + (long long)j*g.n1 + i) < ph.fl.floors_switch_r)
+               ? ph.fl_inner : ph.fl;
+}
+
 // Flux::p_to_u for one zone (all NV conserved variables), flux_functions.hpp:343-352
 template <int NV>
 __device__ __forceinline__ void p_to_u_zone(const ZoneGeom& G, double gam, const double* P, double* U)
@@ -453,7 +461,7 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
         for (int p = 0; p < NV; ++p) P[p] = a.Ps.v[p][c];
         if (mode & M_UTOP) {
             // inverter.cpp:163-181 then b_flux_ct.cpp:196-217
-            const int pf = (mode & M_KASTAUN) ? u_to_p_kastaun<NV>(G, gam, ph.fl, U, P, ph.iter_max, ph.err_tol)
+            const int pf = (mode & M_KASTAUN) ? u_to_p_kastaun<NV>(G, gam, floors_at(ph, g, j, i), U, P, ph.iter_max, ph.err_tol)
                                               : u_to_p_onedw<NV>(G, gam, U, P, ph.iter_max, ph.err_tol);
             pflag = pf % FF_GEOM_RHO;
             fflag = (pf / FF_GEOM_RHO) * FF_GEOM_RHO;
@@ -476,11 +484,21 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
             // floors.cpp:215-229 and floors_impl.hpp:77-125
             double rf, uf;
             const long long cg = (long long)j*g.n1 + i;
-            fflag |= determine_floors<NV>(G, ph.fl, __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), gam, P, rf, uf, D);
+            const Prescription& fl = floors_at(ph, g, j, i);
+            fflag |= determine_floors<NV>(G, fl, __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), gam, P, rf, uf, D);
             if (fflag) {
-                const int pl = apply_floors_frame<NV>(G, ph.frame, gam, P, U, rf, uf, 8, &D);
+                // mixed frames (floors_impl.hpp:84-106): by radius, or by min(rho, u)/b^2 of the
+                // state before the floors
+                int frame = ph.frame;
+                if (frame == KHB_FRAME_MIXED_FLUID_NORMAL) {
+                    frame = (__ldg(g.rcen + cg) > ph.frame_switch_r) ? KHB_FRAME_FLUID : KHB_FRAME_NORMAL;
+                } else if (frame == KHB_FRAME_MIXED_NORMAL_DRIFT) {
+                    const double mag_switch = kmin(P[0], P[1]) / dot4(D.bcon, D.bcov);
+                    frame = (mag_switch < ph.frame_switch_beta) ? KHB_FRAME_DRIFT : KHB_FRAME_NORMAL;
+                }
+                const int pl = apply_floors_frame<NV>(G, frame, gam, P, U, rf, uf, 8, &D);
                 if (pl) pflag = pl;
-                apply_ceilings(G, ph.fl, gam, P);
+                apply_ceilings(G, fl, gam, P);
                 // the fluid part of U(P) after the floors; the lock-step P->U below computes the same
                 // values from the same P, so it is formed here only when that step is not part of the pass
                 if (!(mode & M_PTOU)) {
@@ -585,14 +603,14 @@ __global__ void __launch_bounds__(128) k_fofc_guess(Dims d, DevGeom g, Phys ph, 
 #pragma unroll
         for (int v = 0; v < 3; ++v) Pg[5 + v] = Ug[5 + v] / G.gdet;
     }
-    const int pf = KAST ? u_to_p_kastaun<NV>(G, ph.gam, ph.fl, Ug, Pg, ph.iter_max, ph.err_tol)
+    const int pf = KAST ? u_to_p_kastaun<NV>(G, ph.gam, floors_at(ph, g, j, i), Ug, Pg, ph.iter_max, ph.err_tol)
                         : u_to_p_onedw<NV>(G, ph.gam, Ug, Pg, ph.iter_max, ph.err_tol);
     int ff = (pf / FF_GEOM_RHO) * FF_GEOM_RHO;
     if (ph.floors_on) {
         const long long cg = (long long)j*g.n1 + i;
         double rf, uf;
         FourVec<double> D;
-        ff |= determine_floors<NV>(G, ph.fl, __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), ph.gam, Pg, rf, uf, D);
+        ff |= determine_floors<NV>(G, floors_at(ph, g, j, i), __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), ph.gam, Pg, rf, uf, D);
     }
     const bool eh = ph.spherical && __ldg(g.rcen + (long long)j*g.n1 + i) < ph.fofc_r_mark;
     flag[c] = (ff != 0 || eh) ? 1 : 0;

@@ -58,6 +58,8 @@ struct Phys {
     int weno_lower;                        // WENO5 lowered to MC: 1 near X1 block edges, 2 near the poles
     int recon_fallback;                    // faces whose reconstructed states hit the floors take PPM
     Prescription fl;
+    Prescription fl_inner;                 // r < fl.floors_switch_r when fl.radius_dependent_floors
+    double frame_switch_r, frame_switch_beta;
 };
 
 enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST = 32 };

@@ -4,6 +4,7 @@ A BlockSpec carries what the Flux, B_FluxCT, Inverter, Floors, Boundaries and GR
 put in their Params for one meshblock, and converts it to the khb_config / khb_coords structs
 of the C ABI.  Defaults follow the reference's GetOrAdd* defaults (cited per field group).
 """
+from typing import Optional
 from dataclasses import dataclass, field
 import math
 
@@ -83,6 +84,11 @@ class BlockSpec:
     floors_on: bool = False
     floor_frame: str = "drift"
     floors: FloorSpec = field(default_factory=FloorSpec)
+    # floors_inner block (used inside floors.floors_switch_r when floors.radius_dependent_floors; None:
+    # the same as floors) and the switch points of the mixed injection frames
+    floors_inner: Optional[FloorSpec] = None
+    frame_switch_r: float = 50.0
+    frame_switch_beta: float = 10.0
     # inverter (inverter.cpp:46-115): 1D_W (8 iterations, 1e-8) or Kastaun (25, 1e-12)
     inverter: str = "onedw"
     iter_max: int = 8
@@ -158,6 +164,8 @@ class BlockSpec:
         c.fix_average_neighbors = int(self.fix_average_neighbors)
         c.fix_atmosphere = int(self.fix_atmosphere)
         c.floors = self.floors.to_struct()
+        c.floors_inner = (self.floors_inner or self.floors).to_struct()
+        c.frame_switch_r, c.frame_switch_beta = self.frame_switch_r, self.frame_switch_beta
         c.inverter = _lib.INVERTER[self.inverter]
         c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(self.fofc), self.fofc_polar_cells, self.fofc_eh_buffer
         c.r_horizon = self.r_horizon

@@ -79,7 +79,7 @@ enum BC { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2, BC_EXCHANGE = 3, BC_T
 // Exchange faces are internal block boundaries whose ghost zones the caller fills (Parthenon's
 // boundary communication); only outflow and reflecting faces are global "user" boundaries.
 static inline bool phys_face(int bc) { return bc == BC_OUTFLOW || bc == BC_REFLECT || bc == BC_TRANSMIT; }
-enum Frame { FRAME_FLUID = 0, FRAME_NORMAL = 1, FRAME_DRIFT = 2 };
+enum Frame { FRAME_FLUID = 0, FRAME_NORMAL = 1, FRAME_DRIFT = 2, FRAME_MIXED_FLUID_NORMAL = 3, FRAME_MIXED_NORMAL_DRIFT = 4 };
 
 struct Config {
     int32_t nx1, nx2, nx3, ng;
@@ -102,6 +102,8 @@ struct Config {
     int32_t ct_scheme;                              // 0 B_FluxCT; B_CT: 1 bs99, 2 gs05_0, 3 gs05_c (b_ct.cpp:65)
     int32_t recon_lower;                            // weno5 lowered to MC: 1 low_order_edges, 2 low_order_poles
     int32_t recon_fallback;                         // flux/reconstruction_fallback
+    Prescription floors_inner;                      // floors_inner (floors.hpp:155-167)
+    double frame_switch_r, frame_switch_beta;       // floors/frame_switch_r, floors/frame_switch_beta
 };
 
 // ---------------------------------------------------------------- coordinates
@@ -782,7 +784,9 @@ static inline double hlle(double fL, double fR, double cmax, double cmin, double
 // floors_functions.hpp:320-354 (local form; loc ignored for r as in the reference, which uses G.r(0,j,i))
 static int apply_geo_floors_local(const Block& B, double* P, int j, int i)
 {
-    const Prescription& f = B.c.floors;
+    // the inner prescription inside floors_switch_r (floors_functions.hpp:307-308)
+    const Prescription& f = (B.c.floors.radius_dependent_floors && B.rcen[(size_t)j*B.n1 + i] < B.c.floors.floors_switch_r)
+                                ? B.c.floors_inner : B.c.floors;
     double rhoflr_geom, uflr_geom;
     if (B.C.spherical()) {
         const double r = B.rcen[(size_t)j*B.n1 + i];
@@ -1132,10 +1136,17 @@ static int u_to_p_onedw(const Block& B, const double* U, double* P, int j, int i
 }
 
 // ---------------------------------------------------------------- floors
+// The prescription of zone (j, i): the inner one inside floors_switch_r with radius-dependent floors
+// (floors_functions.hpp:56-57, 89-90; inverter.cpp:165-168)
+static const Prescription& myfloors(const Block& B, int j, int i)
+{
+    return (B.c.floors.radius_dependent_floors && B.rcen[(size_t)j*B.n1 + i] < B.c.floors.floors_switch_r)
+               ? B.c.floors_inner : B.c.floors;
+}
 // floors_functions.hpp:84-160
 static int determine_floors(const Block& B, const double* P, int j, int i, double& rhoflr_max, double& uflr_max)
 {
-    const Prescription& f = B.c.floors;
+    const Prescription& f = myfloors(B, j, i);
     const double gam = B.c.gam;
     double rhoflr_geom, uflr_geom;
     if (B.C.spherical()) {
@@ -1176,7 +1187,7 @@ static int determine_floors(const Block& B, const double* P, int j, int i, doubl
 // floors_functions.hpp:50-82
 static void apply_ceilings(const Block& B, double* P, int j, int i)
 {
-    const Prescription& f = B.c.floors;
+    const Prescription& f = myfloors(B, j, i);
     const double gam = B.c.gam;
     const double gamma = lorentz_calc(B, P, j, i, center);
     const double ktot = (gam - 1.) * P[1] / std::pow(P[0], gam);
@@ -1191,11 +1202,21 @@ static void apply_ceilings(const Block& B, double* P, int j, int i)
 static int apply_floors_frame(const Block& B, double* P, double* U, int j, int i, double rhoflr_max, double uflr_max)
 {
     const double gam = B.c.gam;
-    if (B.c.floor_frame == FRAME_FLUID) {
+    // mixed frames (floors_impl.hpp:84-106): by radius, or by min(rho, u)/b^2 before the floors
+    int frame = B.c.floor_frame;
+    if (frame == FRAME_MIXED_FLUID_NORMAL) {
+        frame = (B.rcen[(size_t)j*B.n1 + i] > B.c.frame_switch_r) ? FRAME_FLUID : FRAME_NORMAL;
+    } else if (frame == FRAME_MIXED_NORMAL_DRIFT) {
+        FourVectors Dt;
+        calc_4vecs(B, P, B.nv > 5, j, i, center, Dt);
+        const double mag_switch = std::min(P[0], P[1]) / dot4(Dt.bcon, Dt.bcov);
+        frame = (mag_switch < B.c.frame_switch_beta) ? FRAME_DRIFT : FRAME_NORMAL;
+    }
+    if (frame == FRAME_FLUID) {
         P[0] += kmax(0., rhoflr_max - P[0]);
         P[1] += kmax(0., uflr_max - P[1]);
         return 0;
-    } else if (B.c.floor_frame == FRAME_DRIFT) {
+    } else if (frame == FRAME_DRIFT) {
         const double lapse2 = 1. / (-B.Gcon(center, j, i, 0, 0));
         double beta[4] = {0};
         beta[1] = lapse2 * B.Gcon(center, j, i, 0, 1);
@@ -1350,7 +1371,7 @@ static double illinois(F&& f, double zm, double zp, int max_iterations, double t
 static int u_to_p_kastaun(const Block& B, const double* U, double* P, int j, int i, int loc, int max_iterations,
                           double tol)
 {
-    const Prescription& fl = B.c.floors;
+    const Prescription& fl = myfloors(B, j, i);
     const double gam = B.c.gam;
     const double alpha = 1. / std::sqrt(-B.Gcon(loc, j, i, 0, 0));
     const double a_over_g = alpha / B.Gdet(loc, j, i);

@@ -53,13 +53,15 @@ class Config(C.Structure):
         ("fofc_eh_buffer", C.c_double), ("r_horizon", C.c_double),
         ("ct_scheme", C.c_int32),
         ("recon_lower", C.c_int32), ("recon_fallback", C.c_int32),
+        ("floors_inner", Prescription),
+        ("frame_switch_r", C.c_double), ("frame_switch_beta", C.c_double),
     ]
 
 
 RECON = {"donor_cell": 0, "donor_cell_c": 0, "linear_mc": 1, "weno5": 2, "ppm": 3, "linear_vl": 4, "weno5_linear": 5,
          "ppmx": 6, "mp5": 7}
 BC = {"periodic": 0, "outflow": 1, "reflecting": 2, "exchange": 3, "transmitting": 4, "dirichlet": 3, "bondi": 3}
-FRAME = {"fluid": 0, "normal": 1, "drift": 2}
+FRAME = {"fluid": 0, "normal": 1, "drift": 2, "mixed": 3, "mixed_fluid_normal": 3, "mixed_normal_drift": 4}
 BASE = {"cartesian_minkowski": 0, "spherical_minkowski": 1, "spherical_ks": 2, "spherical_bl": 3}
 TRANSFORM = {"null": 0, "eks": 1, "mks": 2, "fmks": 3}
 
@@ -148,8 +150,11 @@ def config_from_spec(spec):
     c.ct_scheme = {"none": 0, "bs99": 1, "gs05_0": 2, "gs05_c": 3, "sg07": 3}[spec.b_ct]
     c.recon_lower = 1 if spec.low_order_edges else (2 if spec.low_order_poles else 0)
     c.recon_fallback = int(spec.recon_fallback and spec.floors_on)
+    inner = spec.floors_inner if spec.floors_inner is not None else spec.floors
     for name, _ in Prescription._fields_:
         setattr(c.floors, name, type(getattr(c.floors, name))(getattr(spec.floors, name)))
+        setattr(c.floors_inner, name, type(getattr(c.floors_inner, name))(getattr(inner, name)))
+    c.frame_switch_r, c.frame_switch_beta = spec.frame_switch_r, spec.frame_switch_beta
     return c
 
 
