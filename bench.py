@@ -588,6 +588,7 @@ def gpu_arm(args, rank, world, local_rank):
     bench_stream = torch.cuda.Stream()
     torch.cuda.set_stream(bench_stream)          # graph capture needs a non-default stream
     b, drv, ms, launches, clocks = run(args.form, args.steps, args.warmup, sampler)
+    graph_ok = world == 1 and not args.slab_path
     host_driven = None
     if world == 1 and not args.slab_path:
         _, _, ms_h, _, _ = run(args.form, max(3, args.steps // 4), args.warmup, graph=False)
@@ -629,13 +630,13 @@ def gpu_arm(args, rank, world, local_rank):
         fp32["rel_l1_rho_after_100_steps"] = float((r32 - r64).abs().sum() / r64.abs().sum())
         del ref, f32
 
-    # end-to-end through the C ABI with host buffers: H2D of P and U, the step, D2H of P and U
+    # end-to-end through the C ABI with a host-resident state: khb_step_host copies the primitives in
+    # (pinned host memory), rebuilds U = U(P) on the device (the state's own U: the lock-step P -> U
+    # leaves U = U(P) after every step), replays the graph step and copies the primitives back
     e2e = None
     if not args.no_e2e:
         hP = torch.empty(b.P.shape, dtype=torch.float64, pin_memory=True)
-        hU = torch.empty(b.U.shape, dtype=torch.float64, pin_memory=True)
         hP.copy_(b.P)
-        hU.copy_(b.U)
         torch.cuda.synchronize()
         ke = max(3, args.steps // 2)
         if world > 1:
@@ -643,21 +644,26 @@ def gpu_arm(args, rank, world, local_rank):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(ke):
-            b.P.copy_(hP, non_blocking=True)
-            b.U.copy_(hU, non_blocking=True)
-            drv.step()                       # the graph-replayed step; its timestep stays on the device
-            hP.copy_(b.P, non_blocking=True)
-            hU.copy_(b.U, non_blocking=True)
+        if graph_ok:
+            for _ in range(ke):
+                drv.step_host(hP)
+        else:
+            for _ in range(ke):
+                b.P.copy_(hP, non_blocking=True)
+                b.ptou()
+                drv.step()
+                hP.copy_(b.P, non_blocking=True)
         e1.record()
         torch.cuda.synchronize()
         te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         ms_e = float(te.item()) / ke
-        nbytes = 2 * b.P.numel() * 8
+        nbytes = b.P.numel() * 8
         e2e = {"value": world * zones / (ms_e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": nbytes if world == 1 else nbytes + 8, "ms_per_step": ms_e}
+               "d2h_bytes_per_step": nbytes if world == 1 else nbytes + 8, "ms_per_step": ms_e,
+               "path": "khb_step_host (P in, U = U(P), graph step, P out)" if graph_ok else
+                       "P in, khb_ptou, host-driven step, P out"}
 
     # roofline of the dominant kernel, timed live with CUDA events
     peak, peak_kind = measured_peaks()

@@ -366,6 +366,15 @@ int khb_ct_faces_from_prims(khb_ctx* ctx, const khb_fields* P, const khb_fields*
  * |sum_d (Bf_d(+) - Bf_d(-)) / dx_d|.  Synchronizes the stream. */
 int khb_ct_max_divb(khb_ctx* ctx, const khb_fields* Bf, double* max_divb_host, void* stream);
 
+/* One step of a host-resident state (nv host arrays of the primitives, entire block, pinned for
+ * asynchronous copies), through the device state (P, U): the primitives are copied in, U = U(P) is
+ * rebuilt on the device (the lock-step P -> U of every stage leaves U = U(P) at the end of a step, so
+ * this is the state's own U, bit for bit), the step runs as khb_step_graph (device timestep; set it
+ * with khb_set_timestep; non-default stream), and the primitives are copied back into P_host.
+ * Launches and copies only; the caller synchronizes before reading P_host. */
+int khb_step_host(khb_ctx* ctx, double* const* P_host, const khb_fields* P, const khb_fields* U, int32_t* pflag,
+                  int32_t* fflag, void* stream);
+
 /* B_FluxCT::MaxDivB (b_flux_ct.cpp:566-607): max |corner divB| of the conserved field.
  * Synchronizes the stream. */
 int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void* stream);

@@ -227,6 +227,15 @@ class DeviceDriver:
                       b.stream), "khb_step_graph" if self.graph else "khb_step_device_dt")
         self.nstep += 1
 
+    def step_host(self, hP):
+        """One step of the host-resident primitives hP ((nvar, n3, n2, n1) float64, pinned CPU tensor),
+        in place (khb_step_host: P in, U = U(P), the graph step, P out).  Launches and copies only."""
+        b = self.block
+        ptrs = (C.c_void_p * b.spec.nvar)(*[hP[p].data_ptr() for p in range(b.spec.nvar)])
+        _lib.check(b.lib.khb_step_host(b.ctx, ptrs, b.Pf.ref, b.Uf.ref, C.c_void_p(b.pflag.data_ptr()),
+                                       C.c_void_p(b.fflag.data_ptr()), b.stream), "khb_step_host")
+        self.nstep += 1
+
     def timestep(self):
         """(next dt, time, dt of the last step); synchronizes."""
         dt, t, last = C.c_double(), C.c_double(), C.c_double()

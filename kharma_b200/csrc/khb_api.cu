@@ -881,6 +881,28 @@ int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32
     return KHB_OK;
 }
 
+int khb_step_host(khb_ctx* ctx, double* const* P_host, const khb_fields* P, const khb_fields* U, int32_t* pflag,
+                  int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_host: a B_CT block steps with khb_ct_stage/khb_ct_step");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
+    if (!P_host) return fail(KHB_ERR_ARG, "khb_step_host: NULL host state");
+    for (int p = 0; p < ctx->nv; ++p)
+        if (!P_host[p]) return fail(KHB_ERR_ARG, "khb_step_host: NULL host variable");
+    cudaStream_t st = S(stream);
+    const size_t bytes = sizeof(double) * (size_t)ctx->d.N;
+    // the primitives in; the lock-step P -> U at the end of every stage (zone pass, ghost zones, periodic
+    // images, fixups) leaves U = U(P) everywhere, so the conserved state is rebuilt, not copied
+    for (int p = 0; p < ctx->nv; ++p) KHB_CUDA(cudaMemcpyAsync(P->v[p], P_host[p], bytes, cudaMemcpyHostToDevice, st));
+    LaunchCommon::ptou(ctx->nv, ctx->d, ctx->g, ctx->ph, *P, *U, st);
+    KHB_LAUNCHED(ctx);
+    if ((rc = khb_step_graph(ctx, P, U, pflag, fflag, stream))) return rc;
+    for (int p = 0; p < ctx->nv; ++p) KHB_CUDA(cudaMemcpyAsync(P_host[p], P->v[p], bytes, cudaMemcpyDeviceToHost, st));
+    return KHB_OK;
+}
+
 int khb_get_min_ndt(khb_ctx* ctx, double* min_ndt_host, void* stream)
 {
     if (!ctx || !min_ndt_host) return fail(KHB_ERR_ARG, "khb_get_min_ndt: NULL argument");

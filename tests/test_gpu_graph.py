@@ -39,3 +39,33 @@ def test_graph_step_equals_host_driven_step(make):
     assert last == dts[-1] and dt_next == da.dt and t == sum(dts) or abs(t - sum(dts)) <= 1e-15 * t
     assert torch.equal(a.P, b.P) and torch.equal(a.U, b.U)
     assert torch.equal(a.pflag, b.pflag) and torch.equal(a.fflag, b.fflag)
+
+
+def test_step_host_matches_device_resident_steps():
+    """khb_step_host (primitives in, U = U(P), graph step, primitives out) leaves the same state as
+    the device-resident graph step, bit for bit: U = U(P) holds exactly after every step."""
+    import dataclasses
+    from kharma_b200 import problems
+    from kharma_b200.block import Block, DeviceDriver, build_geometry
+    from kharma_b200.spec import torus_spec
+    spec = torus_spec(32, 24, 8)
+    geom = build_geometry(spec)
+    P0 = problems.fm_torus(spec, geom, seed=5)
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        a = Block(spec, geometry=geom); a.set_prims(P0)
+        b = Block(spec, geometry=geom); b.set_prims(P0)
+        da, db = DeviceDriver(a), DeviceDriver(b)
+        hP = torch.empty(b.P.shape, dtype=torch.float64, pin_memory=True)
+        hP.copy_(b.P)
+        for _ in range(5):
+            da.step()
+            db.step_host(hP)
+        torch.cuda.synchronize()
+        assert torch.equal(a.P.cpu(), hP)
+        assert torch.equal(a.U, b.U)
+        # and the device state b holds satisfies U = U(P) exactly
+        U0 = b.U.clone()
+        b.ptou()
+        torch.cuda.synchronize()
+        assert torch.equal(U0, b.U)
