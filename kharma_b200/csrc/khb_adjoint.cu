@@ -48,9 +48,14 @@ __device__ __forceinline__ void face_side(const R gcov[4][4], const R* gcon0, R 
 // ---------------------------------------------------------------------------- face fluxes
 // Pbar += (dF/dP)^T Fbar for every face of the box (faces [s, e+1] along DIR, [s-1, e+1] across).
 // R: the arithmetic of the forward face kernel (double, or float in the FP32-flux form).
+// The hydro components of Fbar are formed here from Ubar_upd (zero outside the interior): the
+// transpose of U_upd(c) += bdt (area_d/vol) (F_d(c) - F_d(c+st)) gives Fbar_d(c) = area_d w (Ubar_upd(c) -
+// Ubar_upd(c-st)) with w = bdt/vol; the magnetic components (flux-CT) come scattered from k_adj_update
+// in Fbar; the objective's seed (scale * weight on the X1 mass flux) is added for DIR = 1.
 template <int DIR, int NV, int RECON, typename R>
 __global__ void __launch_bounds__(128) k_adj_flux(Dims d, DevGeom g, Phys ph, khb_fields P, const double* Fbar,
-                                                  khb_fields Pbar, Box bx)
+                                                  const double* Uupd, double w, double area, const double* seed,
+                                                  double seed_scale, khb_fields Pbar, Box bx)
 {
     int i, j, k;
     if (!box_cell(bx, blockIdx.x, i, j, k)) return;
@@ -59,7 +64,13 @@ __global__ void __launch_bounds__(128) k_adj_flux(Dims d, DevGeom g, Phys ph, kh
     double fb[NV];
     bool any = false;
 #pragma unroll
-    for (int p = 0; p < NV; ++p) { fb[p] = Fbar[p*d.N + c]; any |= fb[p] != 0.; }
+    for (int p = 0; p < 5; ++p) {
+        const double hi = area * (w * Uupd[p*d.N + c]), lo = -(area * (w * Uupd[p*d.N + c - st]));
+        fb[p] = (DIR == 1 && p == 0 && seed) ? (seed_scale * seed[c] + hi) + lo : hi + lo;
+        any |= fb[p] != 0.;
+    }
+#pragma unroll
+    for (int p = 5; p < NV; ++p) { fb[p] = Fbar[p*d.N + c]; any |= fb[p] != 0.; }
     if (!any) return;
     typedef Dual<R> DR;
     const int loc = DIR - 1;
@@ -169,8 +180,10 @@ __global__ void __launch_bounds__(128) k_adj_update(Dims d, DevGeom g, Phys ph, 
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     const long long N = d.N, sj = d.sj, sk = d.sk;
     double ub[NV];
+    bool any = false;
 #pragma unroll
-    for (int p = 0; p < NV; ++p) ub[p] = Ubar_upd[p*N + c];
+    for (int p = 0; p < NV; ++p) { ub[p] = Ubar_upd[p*N + c]; any |= ub[p] != 0.; }
+    if (!any) return;
 #pragma unroll
     for (int p = 0; p < NV; ++p) {
         Ubar_s.v[p][c] += g0 * ub[p];
@@ -178,14 +191,7 @@ __global__ void __launch_bounds__(128) k_adj_update(Dims d, DevGeom g, Phys ph, 
     }
     const double a1 = ph.dx2*ph.dx3, a2 = ph.dx1*ph.dx3, a3 = ph.dx1*ph.dx2;
     const double w = bdt / (ph.dx1*ph.dx2*ph.dx3);
-    // hydro divergence: U += bdt * -(a1 (F1(c+1) - F1(c)) + ...)/vol
-#pragma unroll
-    for (int p = 0; p < 5; ++p) {
-        const double u = w * ub[p];
-        atomicAdd(F1b + p*N + c + 1, -a1 * u); atomicAdd(F1b + p*N + c, a1 * u);
-        if (d.ndim >= 2) { atomicAdd(F2b + p*N + c + sj, -a2 * u); atomicAdd(F2b + p*N + c, a2 * u); }
-        if (d.ndim == 3) { atomicAdd(F3b + p*N + c + sk, -a3 * u); atomicAdd(F3b + p*N + c, a3 * u); }
-    }
+    // the hydro divergence's transpose is gathered per face by k_adj_flux
     if (NV > 5) {
         // flux-CT (b_flux_ct.cpp:307-370) as ct_divergence forms it: face B fluxes from corner EMFs,
         // EMFs from the raw B fluxes; transposed term by term
@@ -261,6 +267,18 @@ __global__ void __launch_bounds__(128) k_adj_update(Dims d, DevGeom g, Phys ph, 
             for (int b = 0; b < 4; ++b) gcov[a][b] = DD(G.gcov[a][b]);
         }
         const long long cg = (long long)j*g.n1 + i, cs = (long long)(d.n2)*g.n1;
+        // S_lam = sum_{mu,nu} T^mu_nu gdet Gamma^nu_{lam mu}, so sum_lam Ubar[1+lam] dS_lam/dP_q =
+        // sum_{mu,nu} dT^mu_nu/dP_q W[mu][nu] with W[mu][nu] = sum_lam Ubar[1+lam] gdet Gamma^nu_{lam mu}
+        double W[4][4];
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+#pragma unroll
+            for (int nu = 0; nu < 4; ++nu) {
+                double s = 0.;
+#pragma unroll
+                for (int lam = 0; lam < 4; ++lam) s += ub[1 + lam] * __ldg(g.gdet_conn + ((nu*4 + lam)*4 + mu)*cs + cg);
+                W[mu][nu] = s;
+            }
         double P0[NV];
 #pragma unroll
         for (int p = 0; p < NV; ++p) P0[p] = Ps.v[p][c];
@@ -270,19 +288,14 @@ __global__ void __launch_bounds__(128) k_adj_update(Dims d, DevGeom g, Phys ph, 
             for (int p = 0; p < NV; ++p) P[p] = DD(P0[p], (p == q) ? 1. : 0.);
             FourVec<DD> D;
             calc_4vecs<DD, (NV > 5)>(gcov, gcon0[0], gcon0, P, D);
-            DD new_du[4] = {DD(0.), DD(0.), DD(0.), DD(0.)};
+            double acc = 0.;
+#pragma unroll
             for (int mu = 0; mu < 4; ++mu) {
                 DD Tmu[4];
                 calc_tensor<DD, (NV > 5)>(P[0], P[1], DD(ph.gam - 1) * P[1], D, mu, Tmu);
 #pragma unroll
-                for (int nu = 0; nu < 4; ++nu)
-#pragma unroll
-                    for (int lam = 0; lam < 4; ++lam)
-                        new_du[lam] += Tmu[nu] * DD(__ldg(g.gdet_conn + ((nu*4 + lam)*4 + mu)*cs + cg));
+                for (int nu = 0; nu < 4; ++nu) acc += Tmu[nu].d * W[mu][nu];
             }
-            double acc = 0.;
-#pragma unroll
-            for (int lam = 0; lam < 4; ++lam) acc += ub[1 + lam] * new_du[lam].d;
             Pbar_s.v[q][c] += bdt * acc;
         }
     }
@@ -352,15 +365,19 @@ __global__ void __launch_bounds__(128) k_adj_cell(Dims d, DevGeom g, Phys ph, kh
     int i, j, k;
     if (!box_cell(bx, blockIdx.x, i, j, k)) return;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    double P[NV], J[NV][NV], y[NV], ubo[NV];
+    bool any = false;
+#pragma unroll
+    for (int p = 0; p < NV; ++p) { y[p] = Pbar_out.v[p][c]; ubo[p] = Ubar_out.v[p][c]; any |= (y[p] != 0.) | (ubo[p] != 0.); }
+    if (!any) return;                     // Ubar_upd stays zero (cleared before the launch)
     ZoneGeom G;
     load_zone_geom(g, j, i, G);
-    double P[NV], J[NV][NV], y[NV];
 #pragma unroll
-    for (int p = 0; p < NV; ++p) { P[p] = Pout.v[p][c]; y[p] = Pbar_out.v[p][c]; }
+    for (int p = 0; p < NV; ++p) P[p] = Pout.v[p][c];
     ptou_jacobian<NV>(G, ph.gam, P, J);
     solve_transposed<NV>(J, y);
 #pragma unroll
-    for (int p = 0; p < NV; ++p) Ubar_upd[p*d.N + c] = Ubar_out.v[p][c] + y[p];
+    for (int p = 0; p < NV; ++p) Ubar_upd[p*d.N + c] = ubo[p] + y[p];
 }
 
 // Pbar += J(P)^T Ubar over the whole block (the adjoint of U = U(P) of an initial state)
@@ -420,15 +437,6 @@ __global__ void k_adj_clear_ghosts(Dims d, khb_fields A)
     for (int p = 0; p < NV; ++p) A.v[p][t] = 0.;
 }
 
-// Seed of the objective: Fbar1[RHO] += scale * weight over all faces
-__global__ void k_adj_seed(long long N, const double* weight, double scale, double* F1b)
-{
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N) return;
-    const double w = weight[t];
-    if (w != 0.) F1b[t] += scale * w;
-}
-
 // Deterministic sum_f w[f] * F[f] (times scale) added to *out: fixed-size grid of partial sums,
 // then one block adds them in order.
 constexpr int kDotBlocks = 592, kDotThreads = 256;
@@ -452,13 +460,15 @@ __global__ void __launch_bounds__(kDotThreads) k_flux_dot_partial(long long N, c
         partial[blockIdx.x] = t;
     }
 }
+// one warp: lane l adds partials l, l+32, ... in order, then a fixed butterfly (deterministic)
 __global__ void k_flux_dot_final(const double* partial, int n, double scale, double* out)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double t = 0.;
-        for (int i = 0; i < n; ++i) t += partial[i];
-        *out += scale * t;
-    }
+    const int l = threadIdx.x;
+    double t = 0.;
+    for (int i = l; i < n; i += 32) t += partial[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (l == 0) *out += scale * t;
 }
 
 } // namespace khb
@@ -512,8 +522,17 @@ void fold(const Dims& d, const khb_fields& A, cudaStream_t st)
     k_adj_clear_ghosts<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, A);
 }
 
+// what k_adj_flux needs to form the hydro flux adjoints: Ubar_upd, bdt/vol, the objective's seed
+struct FluxAdj {
+    const double* Uupd;
+    double w;
+    const double* seed;
+    double seed_scale;
+};
+
 template <int DIR, int NV, typename R>
-void adj_flux_dir(const khb_ctx* ctx, const khb_fields& P, const double* Fb, const khb_fields& Pbar, cudaStream_t st)
+void adj_flux_dir(const khb_ctx* ctx, const khb_fields& P, const double* Fb, const FluxAdj& fa, const khb_fields& Pbar,
+                  cudaStream_t st)
 {
     const Dims& d = ctx->d;
     int lo[3], cnt[3];
@@ -527,15 +546,18 @@ void adj_flux_dir(const khb_ctx* ctx, const khb_fields& P, const double* Fb, con
         cnt[a] = hi - lo[a] + 1;
     }
     const Box bx = make_box(lo[0], lo[1], lo[2], cnt[0], cnt[1], cnt[2]);
+    const double a = (DIR == 1) ? ctx->ph.dx2 * ctx->ph.dx3 : ((DIR == 2) ? ctx->ph.dx1 * ctx->ph.dx3 : ctx->ph.dx1 * ctx->ph.dx2);
     if (ctx->cfg.recon == KHB_RECON_DONOR_CELL)
-        k_adj_flux<DIR, NV, RECON_DONOR, R><<<box_blocks(bx), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Fb, Pbar, bx);
+        k_adj_flux<DIR, NV, RECON_DONOR, R><<<box_blocks(bx), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Fb, fa.Uupd, fa.w, a,
+                                                                            fa.seed, fa.seed_scale, Pbar, bx);
     else
-        k_adj_flux<DIR, NV, RECON_MC, R><<<box_blocks(bx), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Fb, Pbar, bx);
+        k_adj_flux<DIR, NV, RECON_MC, R><<<box_blocks(bx), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Fb, fa.Uupd, fa.w, a,
+                                                                         fa.seed, fa.seed_scale, Pbar, bx);
 }
 
 // Adjoint of one stage.  Pbar_out/Ubar_out are read by the first kernel; with clear_out they are
 // zeroed right after, so that they can receive Ubar_0 (stage 2 passes the caller's arrays both ways).
-// Launches: memset, cell, [clear], [seed], update, ndim flux, 2-3 folds x 2.
+// Launches: memset, cell, [clear], update, ndim flux (the X1 one adds the objective seed), 2-3 folds x 2.
 template <int NV>
 int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Pout,
                      const khb_fields& Pbar_out, const khb_fields& Ubar_out, bool clear_out, const double* weight,
@@ -554,26 +576,27 @@ int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, c
             KHB_ACUDA(cudaMemsetAsync(Pbar_out.v[p], 0, sizeof(double) * N, st));
             KHB_ACUDA(cudaMemsetAsync(Ubar_out.v[p], 0, sizeof(double) * N, st));
         }
-    if (weight) k_adj_seed<<<blocks_for(d.N, 256), 256, 0, st>>>(d.N, weight, wscale, Fb[0]);
     const int s = stage - 1;
+    const double bdt = kRkBeta[s] * dt;
     k_adj_update<NV><<<box_blocks(zb), 128, 0, st>>>(d, ctx->g, ctx->ph, Uupd, Ps, kRkGam0[s], kRkGam1[s],
-                                                     kRkBeta[s] * dt, Fb[0], Fb[1], Fb[2], Pbar_s, Ubar_s, Ubar_0, zb);
+                                                     bdt, Fb[0], Fb[1], Fb[2], Pbar_s, Ubar_s, Ubar_0, zb);
+    const FluxAdj fa{Uupd, bdt / (ctx->ph.dx1 * ctx->ph.dx2 * ctx->ph.dx3), weight, wscale};
     for (int dir = 1; dir <= d.ndim; ++dir) {
         if (ctx->fp32) {
-            if (dir == 1) adj_flux_dir<1, NV, float>(ctx, Ps, Fb[0], Pbar_s, st);
-            else if (dir == 2) adj_flux_dir<2, NV, float>(ctx, Ps, Fb[1], Pbar_s, st);
-            else adj_flux_dir<3, NV, float>(ctx, Ps, Fb[2], Pbar_s, st);
+            if (dir == 1) adj_flux_dir<1, NV, float>(ctx, Ps, Fb[0], fa, Pbar_s, st);
+            else if (dir == 2) adj_flux_dir<2, NV, float>(ctx, Ps, Fb[1], fa, Pbar_s, st);
+            else adj_flux_dir<3, NV, float>(ctx, Ps, Fb[2], fa, Pbar_s, st);
         } else {
-            if (dir == 1) adj_flux_dir<1, NV, double>(ctx, Ps, Fb[0], Pbar_s, st);
-            else if (dir == 2) adj_flux_dir<2, NV, double>(ctx, Ps, Fb[1], Pbar_s, st);
-            else adj_flux_dir<3, NV, double>(ctx, Ps, Fb[2], Pbar_s, st);
+            if (dir == 1) adj_flux_dir<1, NV, double>(ctx, Ps, Fb[0], fa, Pbar_s, st);
+            else if (dir == 2) adj_flux_dir<2, NV, double>(ctx, Ps, Fb[1], fa, Pbar_s, st);
+            else adj_flux_dir<3, NV, double>(ctx, Ps, Fb[2], fa, Pbar_s, st);
         }
     }
     fold<NV>(d, Pbar_s, st);
     fold<NV>(d, Ubar_s, st);
     if (Ubar_0.v[0] != Ubar_s.v[0]) fold<NV>(d, Ubar_0, st);
     KHB_ACUDA(cudaGetLastError());
-    ctx->launches += 4 + d.ndim + (weight ? 1 : 0) + (clear_out ? 2 * NV : 0) + 2 * (Ubar_0.v[0] != Ubar_s.v[0] ? 3 : 2);
+    ctx->launches += 3 + d.ndim + (clear_out ? 2 * NV : 0) + 2 * (Ubar_0.v[0] != Ubar_s.v[0] ? 3 : 2);
     return KHB_OK;
 }
 

@@ -452,6 +452,27 @@ __device__ __forceinline__ double err_eqn(double gam, double Bsq, double D, doub
     return -Ep + Wp - p + 0.5 * Bsq + 0.5 * (Bsq * Qtsq - QdB * QdB) / ((Bsq + W)*(Bsq + W));
 }
 
+// The same residual with one division and one reciprocal square root in place of four divisions
+// and a square root: 1/gamma = rsqrt(1 + |utsq|), rho = D/gamma and w = W/gamma^2 by products,
+// (gam-1)/gam from the caller (gfac), (Bsq + W)^2 = WB^2.  Equal to err_eqn up to rounding (a few
+// ulp); used by the FP32-flux form's inversion, which has no bitwise contract with the reference.
+__device__ __forceinline__ double err_eqn_fast(double gfac, double Bsq, double D, double Ep, double QdB, double Qtsq,
+                                               double Wp, int& eflag)
+{
+    const double QdBsq = QdB * QdB;
+    const double W = Wp + D;
+    const double W2 = W * W;
+    const double WB = W + Bsq;
+    const double utsq = -((W + WB) * QdBsq + W2 * Qtsq) / (QdBsq * (W + WB) + W2 * (Qtsq - WB * WB));
+    double ig;                                   // 1/gamma; gamma = -1 for an unphysical utsq
+    if (utsq < -1.e-15 || utsq > 1.e7) { ig = -1.; eflag = ST_BAD_UT; }
+    else ig = rsqrt(1. + fabs(utsq));
+    const double w = W * (ig * ig);
+    const double rho = D * ig;
+    const double p = (w - rho) * gfac;
+    return -Ep + Wp - p + 0.5 * Bsq + 0.5 * (Bsq * Qtsq - QdBsq) / (WB * WB);
+}
+
 // Zone-centre geometry for the inversion, floors and P->U
 struct ZoneGeom {
     double gcov[4][4];
@@ -471,8 +492,10 @@ __device__ __forceinline__ void raise4(const ZoneGeom& G, const double* vcov, do
 }
 
 // onedw.hpp:89-233.  U: conserved zone values; P: guess on entry, updated only on success.
-// The iteration count is bounded by max_iterations.
-template <int NV>
+// The iteration count is bounded by max_iterations.  FAST (the FP32-flux form): the residual by
+// err_eqn_fast and the convergence tests |dW| < tol |Wp|, |err| < tol |Wp| without the divisions;
+// FP64 throughout, equal to the plain form up to rounding.
+template <int NV, bool FAST = false>
 __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, double* P, int max_iterations, double tol)
 {
     if (U[0] <= 0.) return ST_NEG_INPUT;
@@ -501,21 +524,25 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
     const double Qtsq = dot4(Qcon, Qcov) + Qdotn*Qdotn;
     const double Ep = -Qdotn - D;
     int eflag = ST_SUCCESS;
+    const double gfac = (gam - 1) / gam;
+    auto residual = [&](double Wq) {
+        return FAST ? err_eqn_fast(gfac, Bsq, D, Ep, QdB, Qtsq, Wq, eflag) : err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wq, eflag);
+    };
     double Wp, err;
     {
         const double gamma = lorentz(G.gcov, P[2], P[3], P[4]);
         if (gamma < 1) return ST_BAD_UT;
         const double rho = P[0], u = P[1];
         Wp = (rho + u + (gam - 1) * u) * gamma * gamma - rho * gamma;
-        err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+        err = residual(Wp);
     }
     double dW;
     {
         const double Wpm = (1. - 1.e-5) * Wp;
         const double h = Wp - Wpm;
         const double Wpp = Wp + h;
-        const double errm = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wpm, eflag);
-        const double errp = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wpp, eflag);
+        const double errm = residual(Wpm);
+        const double errp = residual(Wpp);
         const double dedW = (errp - errm) / (Wpp - Wpm);
         const double dedW2 = (errp - 2. * err + errm) / (h*h);
         const double f = kclip(0.5 * err * dedW2 / (dedW*dedW), -0.3, 0.3);
@@ -524,16 +551,16 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
     double Wp1 = Wp;
     double err1 = err;
     Wp += dW;
-    err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
+    err = residual(Wp);
     int iter = 0;
     for (iter = 0; iter < max_iterations; iter++) {
         dW = kclip((Wp1 - Wp) * err / (err - err1), -0.5*Wp, 2.0*Wp);
         Wp1 = Wp;
         err1 = err;
         Wp += dW;
-        if (fabs(dW / Wp) < tol) break;
-        err = err_eqn(gam, Bsq, D, Ep, QdB, Qtsq, Wp, eflag);
-        if (fabs(err / Wp) < tol) break;
+        if (FAST ? fabs(dW) < tol * fabs(Wp) : fabs(dW / Wp) < tol) break;
+        err = residual(Wp);
+        if (FAST ? fabs(err) < tol * fabs(Wp) : fabs(err / Wp) < tol) break;
     }
     if (iter == max_iterations) return ST_MAX_ITER;
     const double gamma = lorentz_calc_w(Bsq, D, QdB, Qtsq, Wp);

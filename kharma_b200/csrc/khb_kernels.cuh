@@ -462,7 +462,7 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
         if (mode & M_UTOP) {
             // inverter.cpp:163-181 then b_flux_ct.cpp:196-217
             const int pf = (mode & M_KASTAUN) ? u_to_p_kastaun<NV>(G, gam, floors_at(ph, g, j, i), U, P, ph.iter_max, ph.err_tol)
-                                              : u_to_p_onedw<NV>(G, gam, U, P, ph.iter_max, ph.err_tol);
+                                              : u_to_p_onedw<NV, (sizeof(FT) == 4)>(G, gam, U, P, ph.iter_max, ph.err_tol);
             pflag = pf % FF_GEOM_RHO;
             fflag = (pf / FF_GEOM_RHO) * FF_GEOM_RHO;
             if (NV > 5) {
