@@ -543,10 +543,17 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
         const double Wpp = Wp + h;
         const double errm = residual(Wpm);
         const double errp = residual(Wpp);
-        const double dedW = (errp - errm) / (Wpp - Wpm);
-        const double dedW2 = (errp - 2. * err + errm) / (h*h);
-        const double f = kclip(0.5 * err * dedW2 / (dedW*dedW), -0.3, 0.3);
-        dW = kclip(-err / dedW / (1. - f), -0.5*Wp, 2.0*Wp);
+        if (FAST) {
+            const double idedW = (Wpp - Wpm) / (errp - errm);
+            const double dedW2 = (errp - 2. * err + errm) / (h*h);
+            const double f = kclip(0.5 * err * dedW2 * (idedW*idedW), -0.3, 0.3);
+            dW = kclip(-err * idedW / (1. - f), -0.5*Wp, 2.0*Wp);
+        } else {
+            const double dedW = (errp - errm) / (Wpp - Wpm);
+            const double dedW2 = (errp - 2. * err + errm) / (h*h);
+            const double f = kclip(0.5 * err * dedW2 / (dedW*dedW), -0.3, 0.3);
+            dW = kclip(-err / dedW / (1. - f), -0.5*Wp, 2.0*Wp);
+        }
     }
     double Wp1 = Wp;
     double err1 = err;
@@ -563,10 +570,31 @@ __device__ int u_to_p_onedw(const ZoneGeom& G, double gam, const double* U, doub
         if (FAST ? fabs(err) < tol * fabs(Wp) : fabs(err / Wp) < tol) break;
     }
     if (iter == max_iterations) return ST_MAX_ITER;
+    const double W = Wp + D;
+    if (FAST) {
+        // gamma = 1/ig with ig = rsqrt(1 + |utsq|), as in err_eqn_fast
+        const double QdBsq = QdB * QdB, W2 = W * W, WB = W + Bsq;
+        const double utsq = -((W + WB) * QdBsq + W2 * Qtsq) / (QdBsq * (W + WB) + W2 * (Qtsq - WB * WB));
+        if (utsq < -1.e-15 || utsq > 1.e7) return ST_BAD_UT;
+        const double ig = rsqrt(1. + fabs(utsq));
+        const double rho = D * ig;
+        const double w = W * (ig * ig);
+        const double p = (w - rho) * gfac;
+        const double u = w - (rho + p);
+        if (rho < 0 && u < 0) return ST_NEG_RHOU;
+        else if (rho < 0) return ST_NEG_RHO;
+        else if (u < 0) return ST_NEG_U;
+        P[0] = rho;
+        P[1] = u;
+        const double pre = 1. / (ig * WB), qw = QdB / W;
+        P[2] = pre * (Qtcon[1] + qw * Bcon[1]);
+        P[3] = pre * (Qtcon[2] + qw * Bcon[2]);
+        P[4] = pre * (Qtcon[3] + qw * Bcon[3]);
+        return ST_SUCCESS;
+    }
     const double gamma = lorentz_calc_w(Bsq, D, QdB, Qtsq, Wp);
     if (gamma < 1) return ST_BAD_UT;
     const double rho = D / gamma;
-    const double W = Wp + D;
     const double w = W / (gamma*gamma);
     const double p = (w - rho) * (gam - 1) / gam;
     const double u = w - (rho + p);

@@ -50,13 +50,20 @@ __device__ __forceinline__ bool box_cell(const Box& b, unsigned blk, int& i, int
 }
 
 // Load the centre geometry of zone (j,i)
+// SYM: the upper triangles only, mirrored (10 values per metric held in registers instead of 16).
+// The host tables are symmetric to rounding, not bit for bit, so only the FP32-flux form, which has
+// no bitwise contract, reads them this way.
+template <bool SYM = false>
 __device__ __forceinline__ void load_zone_geom(const DevGeom& g, int j, int i, ZoneGeom& G)
 {
     const long long gi = (long long)j*g.G1 + i;
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
-        G.gcov[m/4][m%4] = __ldg(g.gcov[3] + m*g.gs + gi);
-        G.gcon[m/4][m%4] = __ldg(g.gcon[3] + m*g.gs + gi);
+        const int r = m/4, q = m%4;
+        if (SYM && q < r) continue;
+        G.gcov[r][q] = __ldg(g.gcov[3] + m*g.gs + gi);
+        G.gcon[r][q] = __ldg(g.gcon[3] + m*g.gs + gi);
+        if (SYM) { G.gcov[q][r] = G.gcov[r][q]; G.gcon[q][r] = G.gcon[r][q]; }
     }
     G.gdet = __ldg(g.gdet[3] + gi);
 }
@@ -96,7 +103,8 @@ template <> struct FaceTables<float> {
 // Resident 128-thread blocks per SM requested from the compiler for each kernel (register caps
 // of 65536 / (128 x blocks)), chosen by measurement on B200: FP64 faces 5 blocks along x1/x2 and 4
 // along x3, FP32 faces 8, the update half of the zone pass 4 (FP64 fluxes; no spills) or 5 (FP32
-// fluxes) and its inversion half 5.  Each can be overridden at build time.
+// fluxes) and its inversion half 5 (6 in the FP32-flux form, whose zone pass holds the metric's
+// upper triangles only).  Each can be overridden at build time.
 #ifndef KHB_FLUX64_MINB
 #define KHB_FLUX64_MINB 5
 #endif
@@ -115,6 +123,9 @@ template <> struct FaceTables<float> {
 #ifndef KHB_ZONE_CELL_MINB
 #define KHB_ZONE_CELL_MINB 5
 #endif
+#ifndef KHB_ZONE_CELL32_MINB
+#define KHB_ZONE_CELL32_MINB 6
+#endif
 #ifndef KHB_ZONE_INV_MINB
 #define KHB_ZONE_INV_MINB 6
 #endif
@@ -130,7 +141,7 @@ template <int MODE_, typename FT> struct ZoneMinBlocks {
     static constexpr int value = (MODE == M_UPDATE) ? (sizeof(FT) == 8 ? KHB_ZONE_UPDATE_MINB : KHB_ZONE_UPDATE32_MINB) :
                                  (MODE == M_UTOP) ? KHB_ZONE_INV_MINB :
                                  (MODE == M_ZONE_FLOORS) ? KHB_ZONE_FLOOR_MINB :
-                                 ((MODE & M_UTOP) ? KHB_ZONE_CELL_MINB : 1);
+                                 ((MODE & M_UTOP) ? (sizeof(FT) == 8 ? KHB_ZONE_CELL_MINB : KHB_ZONE_CELL32_MINB) : 1);
 };
 
 template <int DIR, int RECON, int NV, typename R, typename FT>
@@ -386,7 +397,7 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
         const long long N = d.N, sj = d.sj, sk = d.sk;
         const double gam = ph.gam;
         ZoneGeom G;
-        load_zone_geom(g, j, i, G);
+        load_zone_geom<(sizeof(FT) == 4)>(g, j, i, G);
 
         double U[NV], P[NV];
         if (mode & M_UPDATE) {
