@@ -59,6 +59,8 @@ def parse():
                     help="at N = 1, step the block through the x3-slab path (one slab, local exchange)")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="time the differentiation form (forward + checkpointed adjoint) and print only that")
+    ap.add_argument("--adjoint-shape", default="192,200,20,64",
+                    help="differentiation form: block size n (n^3), steps, checkpoint spacing, FD directions")
     ap.add_argument("--emhd-only", action="store_true",
                     help="run only the implicit EMHD Newton measurement and print its JSON object")
     return ap.parse_args()
@@ -429,7 +431,7 @@ def b_ct_form(n=128, steps=20, warm=3):
     return out
 
 
-def adjoint_form(n=192, steps=200, every=20, ndir=8):
+def adjoint_form(n=192, steps=200, every=20, ndir=64):
     """The differentiation form on the adjoint workload's shape: an n^3 Bondi block (KS a = 0, MKS,
     r in [3, 30], x2 in [0.1, 0.9], all x3; linear MC, LLF, hydro) with exchange faces holding the
     analytic solution, smooth seeded ramps on every variable (no flat neighbourhoods: the derivative
@@ -437,8 +439,8 @@ def adjoint_form(n=192, steps=200, every=20, ndir=8):
     flux through the x1 face layer nearest r = 5, checkpoints every `every` steps.  The FP32-flux
     form's forward run and adjoint are timed with CUDA events (the adjoint includes the recompute of
     each segment); its gradient is compared with the FP64 adjoint, and the FP64 adjoint with central
-    differences of the FP64 forward run on `ndir` seeded random directions (best of step sizes 1e-6,
-    1e-7, 1e-8 per direction)."""
+    differences of the FP64 forward run on `ndir` seeded random directions (step size 1e-7, retried
+    with 1e-6 and 1e-8 when the relative difference exceeds 1e-4; the best is kept)."""
     import math
     import numpy as np
     import torch
@@ -513,13 +515,15 @@ def adjoint_form(n=192, steps=200, every=20, ndir=8):
         v[sl] = torch.as_tensor(rng.standard_normal(tuple(v[sl].shape)) * scale[:, None, None, None], device="cuda")
         ad = float((g64 * v).sum())
         best = math.inf
-        for e in (1e-6, 1e-7, 1e-8):
+        for e in (1e-7, 1e-6, 1e-8):
             fd = (objective(P0 + e * v) - objective(P0 - e * v)) / (2 * e)
             best = min(best, abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
-            if best < 1e-7:
+            if best < 1e-4:
                 break
         rels.append(best)
-    out["fd_check_fp64"] = {"directions": ndir, "median_rel": float(np.median(rels)), "worst_rel": float(max(rels))}
+    if rels:
+        out["fd_check_fp64"] = {"directions": ndir, "median_rel": float(np.median(rels)),
+                                "worst_rel": float(max(rels)), "below_1e-4": int(sum(r < 1e-4 for r in rels))}
     return out
 
 
@@ -745,7 +749,8 @@ def main():
         return
     if args.adjoint_only:
         if rank == 0:
-            print(json.dumps({"adjoint": adjoint_form()}), flush=True)
+            n, steps, every, ndir = [int(x) for x in args.adjoint_shape.split(",")]
+            print(json.dumps({"adjoint": adjoint_form(n, steps, every, ndir)}), flush=True)
         return
     if world > 1:
         import torch.distributed as dist

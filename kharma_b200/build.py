@@ -10,6 +10,9 @@ Translation units and their arithmetic flags:
   khb_batch.cu     batches of meshblocks: tile tables, CUDA graph, autotuner
   khb_noalloc.cu   khb_max_divb_noalloc (static device scratch)   -fmad=false
   khb_emhd.cu      EMHD sources and the implicit Newton solve      -fmad=false
+  khb_adjoint.cu   discrete adjoint of the step (FP64 faces)      -fmad=false
+  khb_adjoint_fp32.cu  adjoint of the FP32-flux form's faces      as khb_fp32.cu
+  khb_ct.cu        B_CT (face-centred field, EMFs, face update)   -fmad=false
   khb_geometry.cpp host construction of the geometry tables
 The library is a plain shared object; the Python layer binds it with ctypes.
 """
@@ -29,10 +32,11 @@ UNITS = {
     "khb_noalloc.cu": ["-fmad=false"],
     "khb_emhd.cu": ["-fmad=false"],
     "khb_adjoint.cu": ["-fmad=false"],
+    "khb_adjoint_fp32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "khb_ct.cu": ["-fmad=false"],
     "khb_geometry.cpp": [],
 }
-HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", "khb_internal.hpp", "khb_dual.cuh", os.path.join("..", "..", "include", "khb.h")]
+HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", "khb_internal.hpp", "khb_dual.cuh", "khb_adjoint_flux.cuh", os.path.join("..", "..", "include", "khb.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
