@@ -512,6 +512,12 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
             pflag = a.pflag[c];
             fflag = a.fflag[c];
         }
+        if ((mode & M_UTOP) && (mode & (M_FLOORS | M_PTOU))) {
+            // reload the metric for floors and P->U instead of holding it through the inversion
+            // (the compiler barrier keeps the reload; measured 0.4% / 1.3% off the FP64 / FP32 step)
+            asm volatile("" ::: "memory");
+            load_zone_geom<(sizeof(FT) == 4)>(g, j, i, G);
+        }
         if ((mode & M_FLOORS) && ph.floors_on) {
             // floors.cpp:215-229 and floors_impl.hpp:77-125
             double rf, uf;
