@@ -333,8 +333,9 @@ int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, 
                      void* stream);
 
 /* ---------------------------------------------------------------------------------------------
- * B_CT: face-centred magnetic field (cfg.ct_scheme != KHB_CT_NONE; 2D and 3D blocks with periodic or
- * exchange faces).  Face fields are passed as khb_fields with v[0..2] = the conserved sqrt(-g) B^1,
+ * B_CT: face-centred magnetic field (cfg.ct_scheme != KHB_CT_NONE; 2D and 3D blocks; X1/X2 faces
+ * periodic, exchange, outflow or reflecting, X3 faces periodic or exchange; 4 ghost zones with
+ * physical faces).  Face fields are passed as khb_fields with v[0..2] = the conserved sqrt(-g) B^1,
  * B^2, B^3 on x1, x2, x3 faces, each [n3][n2][n1] like the zone arrays, face i being the left face
  * of zone i (faces of the interior, [is, ie+1] along their own direction, are the state; the cell
  * B slots of P and U are derived from them).
@@ -350,12 +351,22 @@ int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, cons
                  const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
                  const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream);
 
+/* Ghost zones of a B_CT block (KBoundaries::ApplyBoundary with B_CT, boundaries.cpp:369-500): with
+ * physical faces, the face field's ghost layers first — reflecting faces: tangential components
+ * mirrored, the normal one zero on the domain face and reflected beyond it (reflect_face_vector);
+ * outflow faces: tangential components copied, the normal one rebuilt outward for zero divergence
+ * (clean_face_B, b_ct_boundaries.cpp:190-262) — then the zone boundaries as khb_boundaries, with the
+ * ghost zones' B from their faces (B_CT::BlockUtoP over the boundary domain).  Without physical
+ * faces it is khb_boundaries.  Reflecting faces also zero the EMFs on their domain-face edges during
+ * each stage (zero_EMF, b_ct_boundaries.cpp:40-62). */
+int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf, void* stream);
+
 /* Full RK2 step with B_CT in place on (P, U, Bf), the intermediate stage in context scratch. */
 int khb_ct_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
                 int32_t* pflag, int32_t* fflag, void* stream);
 
 /* B_CT::BlockUtoP (b_ct.cpp:160-188) over the interior: zone B^i (P slots 5-7) as the average of the
- * two faces' B^i, zone sqrt(-g) B^i (U slots 5-7) from it.  Ghost zones: khb_boundaries. */
+ * two faces' B^i, zone sqrt(-g) B^i (U slots 5-7) from it.  Ghost zones: khb_ct_boundaries. */
 int khb_ct_utop(khb_ctx* ctx, const khb_fields* Bf, const khb_fields* P, const khb_fields* U, void* stream);
 
 /* B_CT::DangerousPtoU (b_ct.cpp:190-253): interior faces from the zone B of P (average of the two

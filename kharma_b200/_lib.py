@@ -139,6 +139,7 @@ SIGNATURES = {
     "khb_flux_dot": (_I, [_P, _I, _I, _P, _D, _P, _P]),
     "khb_ct_stage": (_I, [_P, _I, _D] + [C.POINTER(KhbFields)] * 8 + [_P, _P, _P]),
     "khb_ct_step": (_I, [_P, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_ct_boundaries": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
     "khb_ct_utop": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
     "khb_ct_faces_from_prims": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
     "khb_ct_max_divb": (_I, [_P, C.POINTER(KhbFields), C.POINTER(_D), _P]),

@@ -107,7 +107,8 @@ class Block:
             else:
                 self.Bf.copy_(torch.as_tensor(faces, dtype=torch.float64))
             _lib.check(self.lib.khb_ct_utop(self.ctx, self.Bff.ref, self.Pf.ref, self.Uf.ref, self.stream), "khb_ct_utop")
-            self.boundaries()
+            _lib.check(self.lib.khb_ct_boundaries(self.ctx, self.Pf.ref, self.Uf.ref, self.Bff.ref, self.stream),
+                       "khb_ct_boundaries")
         self.ptou()
 
     def ptou(self):

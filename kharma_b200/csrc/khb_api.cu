@@ -165,12 +165,25 @@ int launch_fixup(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, const i
     return KHB_OK;
 }
 
-int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
+// Bf: a B_CT block's faces; with physical faces their ghost layers are filled first and the ghost
+// zones of the physical directions take B from them
+int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st,
+                      const khb_fields* Bf = nullptr)
 {
     const Dims& d = ctx->d;
     const int nv = ctx->nv;
     const int cnt_k = d.ke - d.ks + 1;
     bool physical = false;
+    int ct_mask = 0;
+    if (Bf) {
+        if (phys_face(d.bc[0])) ct_mask |= 1;
+        if (d.ndim >= 2 && phys_face(d.bc[2])) ct_mask |= 2;
+        if (!ct_mask) Bf = nullptr;
+    }
+    if (Bf) {
+        const int rc = khb::ct_face_boundaries(ctx, *Bf, st);
+        if (rc) return rc;
+    }
     // X1 faces over the interior j range, then X2 faces over all i, then the corner fix
     for (int face = 0; face < 2; ++face) {
         if (!phys_face(d.bc[face])) continue;
@@ -191,7 +204,7 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
         }
     }
     if (physical) {
-        LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st);
+        LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask);
         KHB_LAUNCHED(ctx);
     }
     int pmask = 0;
@@ -294,7 +307,7 @@ int do_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const 
     ctx->ct_active = false;
     if (rc) return rc;
     if ((rc = launch_fixup(ctx, Pout, Uout, pflag, st))) return rc;
-    return launch_boundaries(ctx, Pout, Uout, st);
+    return launch_boundaries(ctx, Pout, Uout, st, &Bout);
 }
 
 } // namespace
@@ -380,11 +393,22 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
     if (cfg->ct_scheme != KHB_CT_NONE) {
         if (cfg->nvar != 8) { *why = "B_CT needs the magnetic field (nvar 8)"; return KHB_ERR_UNSUPPORTED; }
         if (d.ndim < 2) { *why = "B_CT blocks are 2D or 3D"; return KHB_ERR_UNSUPPORTED; }
-        for (int f = 0; f < 2 * d.ndim; ++f)
-            if (phys_face(cfg->bc[f])) { *why = "B_CT blocks have periodic or exchange faces only"; return KHB_ERR_UNSUPPORTED; }
+        bool physical = false;
+        for (int f = 0; f < 2 * d.ndim; ++f) {
+            if (!phys_face(cfg->bc[f])) continue;
+            physical = true;
+            // b_ct_boundaries.cpp: outflow (clean_face_B) and reflecting (reflect_face_vector,
+            // zero_EMF) X1/X2 faces; transmitting faces (average_EMF) are not built
+            if (f >= 4 || (cfg->bc[f] != KHB_BC_OUTFLOW && cfg->bc[f] != KHB_BC_REFLECTING)) {
+                *why = "B_CT blocks take outflow or reflecting X1/X2 faces, periodic or exchange faces otherwise";
+                return KHB_ERR_UNSUPPORTED;
+            }
+        }
+        if (physical && cfg->ng < 4) { *why = "B_CT with physical faces needs 4 ghost zones"; return KHB_ERR_UNSUPPORTED; }
         if (cfg->fofc) { *why = "FOFC with B_CT is not supported"; return KHB_ERR_UNSUPPORTED; }
     }
     ph.ct_scheme = cfg->ct_scheme;
+    if (cfg->ct_scheme != KHB_CT_NONE) ph.fix_polar_flux = 0;      // B_FluxCT's polar fix; not loaded with B_CT
     ph.recon_extra = (cfg->recon >= KHB_RECON_LINEAR_VL) ? cfg->recon - KHB_RECON_PPM : 0;
     if (cfg->recon_lower < KHB_RECON_LOWER_NONE || cfg->recon_lower > KHB_RECON_LOWER_POLES) {
         *why = "unknown recon_lower";
@@ -778,6 +802,16 @@ int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, cons
         if (!f || !f->v[0] || !f->v[1] || !f->v[2]) return fail(KHB_ERR_ARG, "khb_ct_stage: NULL face field");
     if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_ct_stage: NULL flags");
     return do_ct_stage(ctx, stage, dt, *P_s, *U_s, *U_0, *Bf_s, *Bf_0, *P_out, *U_out, *Bf_out, pflag, fflag, S(stream));
+}
+
+int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_boundaries: block is not B_CT (cfg.ct_scheme)");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
+    if (!Bf || !Bf->v[0] || !Bf->v[1] || !Bf->v[2]) return fail(KHB_ERR_ARG, "khb_ct_boundaries: NULL face field");
+    return launch_boundaries(ctx, *P, *U, S(stream), Bf);
 }
 
 int khb_ct_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,

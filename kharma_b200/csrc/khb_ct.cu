@@ -5,8 +5,11 @@
 // k_ct_faces (face change from the EMF circulation and the RK combination of the face field).  The
 // zone pass then takes the zone B from the updated faces (ct_zone_b in khb_kernels.cuh).  EMFs are
 // formed in the flux arithmetic FT (FP32 in the FP32-flux form); the face update is FP64.  Blocks are
-// 2D or 3D with periodic or exchange faces: only interior faces are state, and every EMF and
-// zone-centred EMF they need lies within the flux ranges and the ghost zones.
+// 2D or 3D.  Interior faces are the state; every EMF and zone-centred EMF they need lies within the
+// flux ranges and the ghost zones.  X1/X2 faces may be physical (outflow or reflecting): reflecting
+// faces zero the EMFs on their domain-face edges (zero_EMF), and after each stage the face field's
+// ghost layers are filled (k_ct_face_tangential, k_ct_face_reflect, k_ct_face_outflow with the
+// divergence cleaning) before the ghost zones take B from their faces (k_ghost_ptou).
 #include "khb_internal.hpp"
 #include "khb_kernels.cuh"
 
@@ -187,6 +190,111 @@ __global__ void __launch_bounds__(128) k_ct_divb(Dims d, Phys ph, khb_fields Bf,
     if ((threadIdx.x & 31) == 0) atomicMax(word, (unsigned long long)__double_as_longlong(v));
 }
 
+// ---- physical faces (boundaries.cpp:186-207 defaults, 432-490; b_ct_boundaries.cpp:40-262)
+// Index of the zone / face at position x along bdir and (a, b) across it (a the faster of the two)
+__device__ __forceinline__ long long ct_at(const Dims& d, int bdir, int x, int a, int b)
+{
+    int i, j, k;
+    if (bdir == 1) { i = x; j = a; k = b; } else if (bdir == 2) { i = a; j = x; k = b; } else { i = a; j = b; k = x; }
+    return ((long long)k*d.n2 + j)*d.n1 + i;
+}
+__host__ __device__ inline int ct_na(const Dims& d, int bdir) { return (bdir == 1) ? d.n2 : d.n1; }
+__host__ __device__ inline int ct_nb(const Dims& d, int bdir) { return (bdir == 3) ? d.n2 : d.n3; }
+__host__ __device__ inline int ct_nx(const Dims& d, int bdir) { return (bdir == 1) ? d.n1 : (bdir == 2) ? d.n2 : d.n3; }
+__host__ __device__ inline int ct_s(const Dims& d, int bdir) { return (bdir == 1) ? d.is : (bdir == 2) ? d.js : d.ks; }
+__host__ __device__ inline int ct_e(const Dims& d, int bdir) { return (bdir == 1) ? d.ie : (bdir == 2) ? d.je : d.ke; }
+
+// zero_EMF (b_ct_boundaries.cpp:40-62): the two EMF components along the domain face's edges, over
+// the whole face plane
+template <typename FT>
+__global__ void k_ct_zero_emf(Dims d, int bdir, int f, FT* emf)
+{
+    const int na = ct_na(d, bdir), nb = ct_nb(d, bdir);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)na*nb) return;
+    const long long c = ct_at(d, bdir, f, (int)(t % na), (int)(t / na));
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+        if (v != bdir - 1) emf[v*d.N + c] = (FT)0;
+}
+
+// The tangential face components of one face's ghost layers, as zones: outflow copies the first
+// interior layer, reflecting the mirror layer (no sign change)
+__global__ void k_ct_face_tangential(Dims d, khb_fields Bf, int bdir, int binner, int outflow)
+{
+    const int na = ct_na(d, bdir), nb = ct_nb(d, bdir);
+    const int s = ct_s(d, bdir), e = ct_e(d, bdir);
+    const int layers = binner ? s : ct_nx(d, bdir) - 1 - e;
+    const long long plane = (long long)na*nb;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2*layers*plane) return;
+    const int comp = (int)(t / (layers*plane));
+    const long long r = t - comp*(layers*plane);
+    const int l = (int)(r / plane);
+    const long long q = r - l*plane;
+    const int a = (int)(q % na), b = (int)(q / na);
+    const int v = (bdir == 1) ? 1 + comp : ((bdir == 2) ? 2*comp : comp);     // the components other than bdir-1
+    const int x = binner ? l : e + 1 + l;
+    const int src = outflow ? (binner ? s : e) : (binner ? 2*s - 1 - x : 2*e + 1 - x);
+    Bf.v[v][ct_at(d, bdir, x, a, b)] = Bf.v[v][ct_at(d, bdir, src, a, b)];
+}
+
+// reflect_face_vector (boundaries.cpp:458-479): the normal component zero on the domain face f and
+// minus the mirror face beyond it
+__global__ void k_ct_face_reflect(Dims d, khb_fields Bf, int bdir, int binner)
+{
+    const int na = ct_na(d, bdir), nb = ct_nb(d, bdir), nx = ct_nx(d, bdir);
+    const int f = binner ? ct_s(d, bdir) : ct_e(d, bdir) + 1;
+    const int layers = binner ? f + 1 : nx - f;
+    const long long plane = (long long)na*nb;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= layers*plane) return;
+    const int l = (int)(t / plane);
+    const long long q = t - l*plane;
+    const int a = (int)(q % na), b = (int)(q / na);
+    const int x = binner ? l : f + l;
+    const int m = 2*f - x;
+    if (m < 0 || m >= nx) return;
+    double* F = Bf.v[bdir - 1];
+    F[ct_at(d, bdir, x, a, b)] = (x == f) ? 0. : -F[ct_at(d, bdir, m, a, b)];
+}
+
+// Outflow normal component: the domain face copied outward (Parthenon's outflow), then clean_face_B
+// (DestructiveBoundaryClean, b_ct_boundaries.cpp:190-262): from the domain face outward each face
+// closes the zone between it and the previous face with zero divergence.  One thread per column
+// across the face, all layers in order; the cleaning covers the columns whose transverse upper faces
+// are stored (all but the last transverse layer).  X1 and X2 faces.
+__global__ void k_ct_face_outflow(Dims d, Phys ph, khb_fields Bf, int bdir, int binner)
+{
+    const int na = ct_na(d, bdir), nb = ct_nb(d, bdir), nx = ct_nx(d, bdir);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)na*nb) return;
+    const int a = (int)(t % na), b = (int)(t / na);
+    const int f = binner ? ct_s(d, bdir) : ct_e(d, bdir) + 1;
+    double* Fn = Bf.v[bdir - 1];
+    const double ff = Fn[ct_at(d, bdir, f, a, b)];
+    if (binner) { for (int x = 0; x < f; ++x) Fn[ct_at(d, bdir, x, a, b)] = ff; }
+    else { for (int x = f + 1; x < nx; ++x) Fn[ct_at(d, bdir, x, a, b)] = ff; }
+    const int d3 = d.ndim > 2;
+    if (a >= na - 1 || b >= nb - d3) return;
+    const double A1 = ph.dx2 * ph.dx3, A2 = ph.dx1 * ph.dx3, A3 = ph.dx1 * ph.dx2;
+    const int osign = binner ? -1 : 1;
+    const double nsign = (double)(-(-osign));
+    const double* Ft = Bf.v[(bdir == 1) ? 1 : 0];                 // the other in-plane component
+    const double* F3 = Bf.v[2];
+    const double At = (bdir == 1) ? A2 : A1, An = (bdir == 1) ? A1 : A2;
+    const long long up = (bdir == 1) ? d.sj : 1;                  // its upper face across the column
+    for (int layer = 0; layer < nx; ++layer) {
+        const int x = binner ? f - layer : f + layer;
+        if (x < 0 || x > nx - 1) break;
+        const int lf = binner ? x + 1 : x - 1, lc = binner ? x : x - 1;
+        const long long zc = ct_at(d, bdir, lc, a, b);
+        double nf = nsign * Fn[ct_at(d, bdir, lf, a, b)] * An - (Ft[zc + up] * At - Ft[zc] * At);
+        if (d3) nf -= F3[zc + d.sk] * A3 - F3[zc] * A3;
+        Fn[ct_at(d, bdir, x, a, b)] = (double)osign * nf / An;
+    }
+}
+
 namespace {
 
 Box interior_box(const Dims& d) { return make_box(d.is, d.js, d.ks, d.ie - d.is + 1, d.je - d.js + 1, d.ke - d.ks + 1); }
@@ -218,8 +326,47 @@ int ct_emf(khb_ctx* ctx, const khb_fields& Ps, cudaStream_t st)
 {
     if (ctx->fp32) edge_emf<float>(ctx, Ps, st); else edge_emf<double>(ctx, Ps, st);
     ctx->launches += 1 + (ctx->ph.ct_scheme != KHB_CT_BS99);
+    const Dims& d = ctx->d;
+    for (int face = 0; face < 2 * d.ndim; ++face) {
+        if (d.bc[face] != KHB_BC_REFLECTING) continue;
+        const int bdir = face / 2 + 1, binner = (face % 2) == 0;
+        const int f = binner ? ct_s(d, bdir) : ct_e(d, bdir) + 1;
+        const long long n = (long long)ct_na(d, bdir) * ct_nb(d, bdir);
+        if (ctx->fp32) k_ct_zero_emf<float><<<blocks_for(n, 128), 128, 0, st>>>(d, bdir, f, (float*)ctx->emf);
+        else k_ct_zero_emf<double><<<blocks_for(n, 128), 128, 0, st>>>(d, bdir, f, (double*)ctx->emf);
+        ctx->launches += 1;
+    }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? KHB_OK : set_error(KHB_ERR_CUDA, std::string("B_CT EMF: ") + cudaGetErrorString(e));
+}
+
+// The face field's ghost layers at the physical faces, in Parthenon's order (x1 faces, x2 faces, then
+// inner x1 again with fix_corner)
+int ct_face_boundaries(khb_ctx* ctx, const khb_fields& Bf, cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    auto one = [&](int face) {
+        const int bdir = face / 2 + 1, binner = (face % 2) == 0;
+        const int outflow = d.bc[face] == KHB_BC_OUTFLOW;
+        const long long plane = (long long)ct_na(d, bdir) * ct_nb(d, bdir);
+        const int layers = binner ? ct_s(d, bdir) : ct_nx(d, bdir) - 1 - ct_e(d, bdir);
+        k_ct_face_tangential<<<blocks_for(2 * layers * plane, 128), 128, 0, st>>>(d, Bf, bdir, binner, outflow);
+        if (outflow) {
+            k_ct_face_outflow<<<blocks_for(plane, 128), 128, 0, st>>>(d, ctx->ph, Bf, bdir, binner);
+        } else {
+            const int f = binner ? ct_s(d, bdir) : ct_e(d, bdir) + 1;
+            const int nl = binner ? f + 1 : ct_nx(d, bdir) - f;
+            k_ct_face_reflect<<<blocks_for(nl * plane, 128), 128, 0, st>>>(d, Bf, bdir, binner);
+        }
+        ctx->launches += 2;
+    };
+    for (int face = 0; face < 2 * d.ndim; ++face) {
+        if (!phys_face(d.bc[face])) continue;
+        one(face);
+        if (face == 3 && ctx->cfg.fix_corner_inner && phys_face(d.bc[0])) one(0);
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? KHB_OK : set_error(KHB_ERR_CUDA, std::string("B_CT face boundaries: ") + cudaGetErrorString(e));
 }
 
 int ct_face_update(khb_ctx* ctx, int stage, double dt, const khb_fields& Bs, const khb_fields& B0,

@@ -74,6 +74,7 @@ int ctx_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaS
 // B_CT stage pieces (khb_ct.cu): edge EMFs from the stage's face fluxes and primitives, and the face
 // update Bf_out = gam0 Bf_s + gam1 Bf_0 + beta dt dBf/dt
 int ct_emf(khb_ctx* ctx, const khb_fields& Ps, cudaStream_t st);
+int ct_face_boundaries(khb_ctx* ctx, const khb_fields& Bf, cudaStream_t st);
 int ct_face_update(khb_ctx* ctx, int stage, double dt, const khb_fields& Bs, const khb_fields& B0,
                    const khb_fields& Bout, cudaStream_t st);
 

@@ -894,9 +894,13 @@ __host__ __device__ inline unsigned plane_ghost_count(const Dims& d)
     return (unsigned)(d.n1 * d.n2) - (unsigned)((d.ie - d.is + 1) * (d.je - d.js + 1));
 }
 
-// B_P = B_U/gdet and U = U(P) on the X1/X2 ghost zones of the interior k range
+// B_P = B_U/gdet and U = U(P) on the X1/X2 ghost zones of the interior k range.  B_CT blocks with
+// physical faces (Bf.v[0] set): a zone outside the interior only along directions in ct_mask (bit
+// 0: X1, bit 1: X2) takes B from its faces (B_CT::BlockUtoP over the boundary domain, b_ct.cpp:
+// 160-188); the last ghost layer of a direction has its lower face only (the face array stops
+// there) and takes B from that face alone.
 template <int NV>
-__global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U)
+__global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, khb_fields Bf, int ct_mask)
 {
     const unsigned per = plane_ghost_count(d);
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -911,7 +915,20 @@ __global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_field
     double Pz[NV], Uz[NV];
 #pragma unroll
     for (int p = 0; p < 5; ++p) Pz[p] = P.v[p][c];
-    if (NV > 5) {
+    const bool gi = i < d.is || i > d.ie, gj = j < d.js || j > d.je;
+    const bool from_faces = NV > 5 && Bf.v[0] && !(gi && !(ct_mask & 1)) && !(gj && !(ct_mask & 2));
+    if (from_faces) {
+        const long long gi0 = (long long)j*g.G1 + i;
+        const double* F1 = Bf.v[0]; const double* F2 = Bf.v[1]; const double* F3 = Bf.v[2];
+        Pz[5] = (i == d.n1 - 1) ? F1[c] / __ldg(g.gdet[0] + gi0)
+                                : (F1[c] / __ldg(g.gdet[0] + gi0) + F1[c + 1] / __ldg(g.gdet[0] + gi0 + 1)) / 2;
+        Pz[6] = (d.ndim > 1 && j < d.n2 - 1) ? (F2[c] / __ldg(g.gdet[1] + gi0) + F2[c + d.sj] / __ldg(g.gdet[1] + gi0 + g.G1)) / 2
+                                             : F2[c] / __ldg(g.gdet[1] + gi0);
+        Pz[7] = (d.ndim > 2 && k < d.n3 - 1) ? (F3[c] / __ldg(g.gdet[2] + gi0) + F3[c + d.sk] / __ldg(g.gdet[2] + gi0)) / 2
+                                             : F3[c] / __ldg(g.gdet[2] + gi0);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) P.v[5 + v][c] = Pz[5 + v];
+    } else if (NV > 5) {
 #pragma unroll
         for (int v = 0; v < 3; ++v) { Pz[5 + v] = U.v[5 + v][c] / G.gdet; P.v[5 + v][c] = Pz[5 + v]; }
     }
@@ -1613,12 +1630,15 @@ void LaunchCommon::bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, c
 }
 
 void LaunchCommon::ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
-                              const khb_fields& U, cudaStream_t st)
+                              const khb_fields& U, cudaStream_t st, const khb_fields* Bf, int ct_mask)
 {
     const long long tot = (long long)plane_ghost_count(d)*(d.ke - d.ks + 1);
     if (tot == 0) return;
-    if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U);
-    else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U);
+    khb_fields F;
+    for (int x = 0; x < KHB_MAX_VARS; ++x) F.v[x] = nullptr;
+    if (Bf) for (int x = 0; x < 3; ++x) F.v[x] = Bf->v[x];
+    if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask);
+    else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask);
 }
 
 void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st)

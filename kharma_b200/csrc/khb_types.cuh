@@ -178,7 +178,7 @@ struct LaunchCommon {
     static void bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
                    int face, int lo_a, int cnt_a, int lo_k, int cnt_k, cudaStream_t st);
     static void ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
-                           const khb_fields& U, cudaStream_t st);
+                           const khb_fields& U, cudaStream_t st, const khb_fields* Bf = nullptr, int ct_mask = 0);
     static void periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st);
     static void ghost_copy(int nv, const Dims& d, const khb_fields& Pin, const khb_fields& Uin, const khb_fields& Pout,
                            const khb_fields& Uout, cudaStream_t st);

@@ -133,12 +133,14 @@ def _torus_rho(a, rin, rmax, gam, kappa, r, th):
     return np.where((lnh >= 0.) & (r >= rin), rho, 0.0)
 
 
-def fm_torus(spec, geom, rin=6.0, rmax=12.0, kappa=1e-3, beta_min=100.0, u_jitter=0.08, seed=1234):
+def fm_torus(spec, geom, rin=6.0, rmax=12.0, kappa=1e-3, beta_min=100.0, u_jitter=0.08, seed=1234, faces=False):
     """Fishbone-Moncrief torus + SANE field, on a spherical-KS FMKS block.
 
     geom: dict with the centre tables 'gcov', 'gcon' (arrays [7][n2+1][n1+1][4][4]) and 'gdet'
     from khb_build_geometry.  The field is A_phi = max(rho/rho_max - 0.2, 0) at zone corners,
     curled with the flux-CT averaged curl and normalised so max(p_gas)/max(p_B) = beta_min.
+    faces=True also returns the B_CT face field sqrt(-g) B^d (3, n3, n2, n1): the face curl of the
+    same A_phi with the same normalisation (B_CT's seeding, divergence-free to rounding).
     """
     gam, a = spec.gam, spec.a
     n3, n2, n1 = spec.shape
@@ -197,9 +199,10 @@ def fm_torus(spec, geom, rin=6.0, rmax=12.0, kappa=1e-3, beta_min=100.0, u_jitte
     rng = np.random.Generator(np.random.PCG64(seed))
     jit = rng.uniform(-u_jitter / 2, u_jitter / 2, size=P[1].shape)
     P[1] = np.where(P[0] > fl.rho_min_geom, P[1] * (1. + jit), P[1])
+    Bf = None
     if spec.nvar > 5:
-        _seed_sane(spec, geom, P, a, rin, rmax, gam, kappa, rho_max, beta_min)
-    return P
+        Bf = _seed_sane(spec, geom, P, a, rin, rmax, gam, kappa, rho_max, beta_min)
+    return (P, Bf) if faces else P
 
 
 def _seed_sane(spec, geom, P, a, rin, rmax, gam, kappa, rho_norm, beta_min):
@@ -234,6 +237,11 @@ def _seed_sane(spec, geom, P, a, rin, rmax, gam, kappa, rho_norm, beta_min):
     beta_now = p_max / (0.5 * bsq_max)
     norm = math.sqrt(beta_now / beta_min)
     P[5:8] *= norm
+    # the face curl (A_3 at the corners of face i's lower edge): sqrt(-g) B^1 on x1 faces, B^2 on x2
+    Bf = np.zeros((3,) + spec.shape)
+    Bf[0] = (norm * (A[1:, :-1] - A[:-1, :-1]) / dx2)[None]
+    Bf[1] = (-norm * (A[:-1, 1:] - A[:-1, :-1]) / dx1)[None]
+    return Bf
 
 
 def _bsq(P, gcov, gcon):

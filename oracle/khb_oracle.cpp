@@ -2004,6 +2004,154 @@ static void ct_update_faces(const Block& B, const double* emf, int s, double dt,
     }
 }
 
+// ---- B_CT at physical faces (boundaries.cpp:186-207 defaults, 432-490; b_ct_boundaries.cpp:40-262)
+// Reflecting faces zero the EMFs on the edges lying in the domain face (zero_EMF), before the face
+// update.  After the stage, each physical face (x1 faces, x2 faces, then inner x1 again with
+// fix_corner) fills the face field's ghost layers: tangential components copy as zones do
+// (outflow: the first interior layer; reflecting: the mirror zone, no sign change), the normal
+// component is the reflected face vector (reflect_face_vector: zero on the domain face, minus the
+// mirror face beyond it) or, on outflow faces, is rebuilt layer by layer outward from the domain face
+// so that every zone it closes has zero divergence (clean_face_B, DestructiveBoundaryClean).  The
+// ghost zones then take B from their faces (B_CT::BlockUtoP over the boundary domain).  The arrays
+// hold faces 0..n-1 per direction (face n, the top of the last ghost layer, is not stored): the
+// cleaning leaves the last transverse ghost layer as copied, and the last ghost zone layer takes its
+// normal B from its one stored face; with ng >= 4 neither reaches an interior flux.
+static void ct_zero_boundary_emf(const Block& B, double* emf)
+{
+    const size_t N = B.N;
+    for (int face = 0; face < 2*B.ndim; ++face) {
+        if (B.c.bc[face] != BC_REFLECT) continue;
+        const int bdir = face / 2 + 1;
+        const bool binner = (face % 2) == 0;
+        const int f = (bdir == 1) ? (binner ? B.is : B.ie + 1) : (bdir == 2) ? (binner ? B.js : B.je + 1)
+                                                                            : (binner ? B.ks : B.ke + 1);
+        for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+            const int x = (bdir == 1) ? i : (bdir == 2) ? j : k;
+            if (x != f) continue;
+            for (int v = 0; v < 3; ++v)
+                if (v != bdir - 1) emf[(size_t)v*N + B.id(k, j, i)] = 0.;
+        }
+    }
+}
+
+static void ct_face_boundary(const Block& B, double* Bf, int face)
+{
+    const size_t N = B.N;
+    const int bdir = face / 2 + 1;
+    const bool binner = (face % 2) == 0;
+    const int type = B.c.bc[face];
+    const int n[3] = {B.n1, B.n2, B.n3};
+    const int s = (bdir == 1) ? B.is : (bdir == 2) ? B.js : B.ks;
+    const int e = (bdir == 1) ? B.ie : (bdir == 2) ? B.je : B.ke;
+    const int nb = n[bdir - 1];
+    const int f = binner ? s : e + 1;                       // the domain face
+    auto at = [&](int v, int k, int j, int i) -> double& { return Bf[(size_t)v*N + B.id(k, j, i)]; };
+    auto idx = [&](int k, int j, int i) { return (bdir == 1) ? i : (bdir == 2) ? j : k; };
+    auto moved = [&](int k, int j, int i, int x) {
+        if (bdir == 1) i = x; else if (bdir == 2) j = x; else k = x;
+        return B.id(k, j, i);
+    };
+    // tangential components: zone-like ghost layers (Parthenon's outflow / reflect)
+    for (int v = 0; v < 3; ++v) {
+        if (v == bdir - 1) continue;
+        for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+            const int x = idx(k, j, i);
+            if (binner ? x >= s : x <= e) continue;
+            const int src = (type == BC_OUTFLOW) ? (binner ? s : e) : (binner ? 2*s - 1 - x : 2*e + 1 - x);
+            at(v, k, j, i) = Bf[(size_t)v*N + moved(k, j, i, src)];
+        }
+    }
+    const int v = bdir - 1;
+    if (type == BC_REFLECT) {
+        // reflect_face_vector (boundaries.cpp:458-479): zero on the domain face, minus the mirror face
+        for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+            const int x = idx(k, j, i);
+            if (binner ? x > f : x < f) continue;
+            const int m = 2*f - x;
+            if (m < 0 || m >= nb) continue;
+            at(v, k, j, i) = (x == f) ? 0. : -Bf[(size_t)v*N + moved(k, j, i, m)];
+        }
+        return;
+    }
+    // outflow: Parthenon's copy of the domain face into the ghost faces, then clean_face_B
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+        const int x = idx(k, j, i);
+        if (binner ? x >= f : x <= f) continue;
+        at(v, k, j, i) = Bf[(size_t)v*N + moved(k, j, i, f)];
+    }
+    // DestructiveBoundaryClean (b_ct_boundaries.cpp:190-262): from the domain face outward, each face
+    // closes the zone between it and the previous one with zero divergence
+    const double A1 = B.c.dx2 * B.c.dx3, A2 = B.c.dx1 * B.c.dx3, A3 = B.c.dx1 * B.c.dx2;
+    const int osign = binner ? -1 : 1;
+    const double nsign = (double)(-(-osign));
+    const int d3 = B.ndim > 2;
+    for (int layer = 0; layer < nb; ++layer) {
+        const int x = binner ? f - layer : f + layer;
+        if (x < 0 || x > nb - 1) break;
+        const int lf = binner ? x + 1 : x - 1, lc = binner ? x : x - 1;
+        if (bdir == 1) {
+            for (int k = 0; k < B.n3 - d3; ++k) for (int j = 0; j < B.n2 - 1; ++j) {
+                double nf = nsign * at(0, k, j, lf) * A1 - (at(1, k, j + 1, lc) * A2 - at(1, k, j, lc) * A2);
+                if (d3) nf -= at(2, k + 1, j, lc) * A3 - at(2, k, j, lc) * A3;
+                at(0, k, j, x) = (double)osign * nf / A1;
+            }
+        } else {
+            for (int k = 0; k < B.n3 - d3; ++k) for (int i = 0; i < B.n1 - 1; ++i) {
+                double nf = nsign * at(1, k, lf, i) * A2 - (at(0, k, lc, i + 1) * A1 - at(0, k, lc, i) * A1);
+                if (d3) nf -= at(2, k + 1, lc, i) * A3 - at(2, k, lc, i) * A3;
+                at(1, k, x, i) = (double)osign * nf / A2;
+            }
+        }
+    }
+}
+
+// Ghost zones of the physical directions: B from the faces, sqrt(-g) B as conserved B
+static void ct_ghost_zone_b(const Block& B, const double* Bf, double* P, double* U)
+{
+    const size_t N = B.N;
+    const bool ph1 = phys_face(B.c.bc[0]), ph2 = B.ndim > 1 && phys_face(B.c.bc[2]);
+    const bool ph3 = B.ndim > 2 && phys_face(B.c.bc[4]);
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+        const bool gi = i < B.is || i > B.ie, gj = j < B.js || j > B.je, gk = k < B.ks || k > B.ke;
+        if (!((gi && ph1) || (gj && ph2) || (gk && ph3))) continue;
+        if ((gi && !ph1) || (gj && !ph2) || (gk && !ph3)) continue;     // periodic images fill these
+        double Bp[3];
+        const size_t c = B.id(k, j, i);
+        const double* F1 = Bf; const double* F2 = Bf + N; const double* F3 = Bf + 2*N;
+        Bp[0] = (i == B.n1 - 1) ? F1[c] / B.Gdet(face1, j, i)
+                                : (F1[c] / B.Gdet(face1, j, i) + F1[c + 1] / B.Gdet(face1, j, i + 1)) / 2;
+        Bp[1] = (B.ndim > 1 && j < B.n2 - 1) ? (F2[c] / B.Gdet(face2, j, i) + F2[c + B.n1] / B.Gdet(face2, j + 1, i)) / 2
+                                             : F2[c] / B.Gdet(face2, j, i);
+        Bp[2] = (B.ndim > 2 && k < B.n3 - 1) ? (F3[c] / B.Gdet(face3, j, i) + F3[c + (size_t)B.n1*B.n2] / B.Gdet(face3, j, i)) / 2
+                                             : F3[c] / B.Gdet(face3, j, i);
+        for (int v = 0; v < 3; ++v) {
+            P[(size_t)(5 + v)*N + c] = Bp[v];
+            U[(size_t)(5 + v)*N + c] = Bp[v] * B.Gdet(center, j, i);
+        }
+    }
+}
+
+// The ghost zones of a B_CT block with physical faces: faces first, then the zone boundaries as
+// apply_boundaries fills them, with the zone B of the physical directions' ghost zones from the faces
+// (before the periodic images are taken again)
+static bool ct_has_physical(const Block& B)
+{
+    for (int face = 0; face < 2*B.ndim; ++face) if (phys_face(B.c.bc[face])) return true;
+    return false;
+}
+static void ct_apply_boundaries(const Block& B, double* P, double* U, double* Bf)
+{
+    for (int face = 0; face < 2*B.ndim; ++face) {
+        if (!phys_face(B.c.bc[face])) continue;
+        ct_face_boundary(B, Bf, face);
+        if (face == 3 && B.c.fix_corner_inner && phys_face(B.c.bc[0])) ct_face_boundary(B, Bf, 0);
+    }
+    apply_boundaries(B, P, U);
+    ct_ghost_zone_b(B, Bf, P, U);
+    for (int d = 1; d <= B.ndim; ++d)
+        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, B.nv, d); periodic_fill(B, U, B.nv, d); }
+}
+
 // One RK stage with B_CT (kharma_step.cpp:163-214, use_b_ct): fluxes, FixFlux without flux-CT, EMFs,
 // face update, the cell update, the zone B (and sqrt(-g) B) from the new faces, inversion, floors,
 // fixups, boundaries and P->U as stage() does
@@ -2018,6 +2166,7 @@ static void ct_stage(const Block& B, Fields& f, int s, double dt, const double* 
     boundaries_fix_flux(B, F);
     std::vector<double> emf(3*N, 0.);
     ct_calculate_emf(B, F, P_s, emf.data());
+    ct_zero_boundary_emf(B, emf.data());
     ct_update_faces(B, emf.data(), s, dt, Bs, B0, Bn);
     std::vector<double> dudt(NV, 0.);
     flux_divergence(B, F, dudt.data());
@@ -2060,7 +2209,11 @@ static void ct_stage(const Block& B, Fields& f, int s, double dt, const double* 
         if (B.ndim > 2 && B.c.bc[5] == BC_EXCHANGE) ke = B.n3 - 1;
         fix_utop(B, P_n, U_n, pflag, ks, ke, js, je, is, ie);
     }
-    finish_stage(B, P_n, U_n);
+    if (!ct_has_physical(B)) { finish_stage(B, P_n, U_n); return; }
+    ct_apply_boundaries(B, P_n, U_n, Bn);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i)
+        p_to_u_cell(B, P_n, U_n, B.id(k, j, i), j, i);
 }
 
 // ======================================================================== EMHD and the implicit solve
@@ -3125,6 +3278,15 @@ void orc_ct_step(void* hp, double* P, double* U, double* Bf, double* pflag, doub
         const double ndt = clip(mn * B.c.cfl, B.c.dt_min, B.c.max_dt_increase * dt);
         *dt_next = std::min(2.0 * dt, ndt);
     }
+}
+
+// Ghost zones of a B_CT block (khb_ct_boundaries): with physical faces the face field's ghost layers
+// and the ghost zones' B from them, else the zone boundaries alone
+void orc_ct_boundaries(void* hp, double* P, double* U, double* Bf)
+{
+    const Block& B = ((Handle*)hp)->B;
+    if (ct_has_physical(B)) ct_apply_boundaries(B, P, U, Bf);
+    else apply_boundaries(B, P, U);
 }
 
 // B_CT::BlockUtoP over the interior

@@ -93,6 +93,7 @@ def load():
     lib.orc_ct_step.argtypes = [P, P, P, P, P, P, C.c_double, P, P]
     lib.orc_ct_utop.argtypes = [P, P, P, P]
     lib.orc_ct_faces_from_prims.argtypes = [P, P, P]
+    lib.orc_ct_boundaries.argtypes = [P, P, P, P]
     lib.orc_ct_max_divb.restype = C.c_double
     lib.orc_ct_max_divb.argtypes = [P, P]
     lib.orc_max_divb.restype = C.c_double
@@ -262,7 +263,7 @@ class Oracle:
         else:
             Bf = np.ascontiguousarray(Bf, dtype=np.float64).copy()
         self.lib.orc_ct_utop(self.h, _ptr(Bf), _ptr(P), _ptr(U))
-        self.boundaries(P, U)
+        self.lib.orc_ct_boundaries(self.h, _ptr(P), _ptr(U), _ptr(Bf))
         self.lib.orc_ptou(self.h, _ptr(P), _ptr(U))
         return P, U, Bf
 
