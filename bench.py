@@ -397,8 +397,8 @@ def smr_form(steps=20, warm=3):
 
 def b_ct_form(n=128, steps=20, warm=3):
     """B_CT (face-centred field, gs05_c EMFs) against the flux-CT path on the same n^3 periodic MHD
-    fast mode (Minkowski, linear MC, LLF, 1D_W), fixed dt, steps launched back to back on one stream;
-    CUDA events."""
+    fast mode (Minkowski, linear MC, LLF, 1D_W) and on the n^3 FM torus, fixed dt, steps launched back
+    to back on one stream; CUDA events."""
     import dataclasses
     import torch
     from kharma_b200 import problems
@@ -428,6 +428,34 @@ def b_ct_form(n=128, steps=20, warm=3):
         del b
         torch.cuda.empty_cache()
     out["b_ct_over_flux_ct_time"] = out["b_ct_gs05_c"]["ms_per_step"] / out["flux_ct"]["ms_per_step"]
+    # the FM torus workload with B_CT (outflow X1, reflecting X2 faces: zero_EMF, the face field's
+    # ghost layers and their divergence cleaning each stage) beside the same torus with flux-CT
+    from kharma_b200.block import build_geometry
+    from kharma_b200.spec import torus_spec
+    tspec = torus_spec(n, n, n)
+    geom = build_geometry(tspec)
+    P0t, Bf0 = problems.fm_torus(tspec, geom, faces=True)
+    torus = {"workload": f"FM torus FMKS {n}^3 (outflow X1, reflecting X2, periodic X3, drift floors), MC, LLF, FP64"}
+    for name, spec in (("flux_ct", tspec), ("b_ct_gs05_c", dataclasses.replace(tspec, b_ct="gs05_c"))):
+        b = Block(spec, geometry=geom)
+        b.set_prims(P0t, faces=Bf0 if spec.b_ct != "none" else None)
+        dt = 1e-3
+        for _ in range(warm):
+            b.step(dt)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            b.step(dt)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        torus[name] = {"ms_per_step": ms, "zone_cycles_per_s": n ** 3 / (ms / 1000.0), "max_divb": b.max_divb()}
+        del b
+        torch.cuda.empty_cache()
+    torus["b_ct_over_flux_ct_time"] = torus["b_ct_gs05_c"]["ms_per_step"] / torus["flux_ct"]["ms_per_step"]
+    out["torus"] = torus
     return out
 
 
