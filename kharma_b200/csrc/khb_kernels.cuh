@@ -101,15 +101,15 @@ template <> struct FaceTables<float> {
 };
 
 // Resident 128-thread blocks per SM requested from the compiler for each kernel (register caps
-// of 65536 / (128 x blocks)), chosen by measurement on B200: FP64 faces 5 blocks along x1/x2 and 4
-// along x3, FP32 faces 8, the update half of the zone pass 4 (FP64 fluxes; no spills) or 5 (FP32
+// of 65536 / (128 x blocks)), chosen by measurement on B200: FP64 faces 6 blocks along x1/x2 and 5
+// along x3 (with the L2 prefetch of each zone's primitives; 5 and 4 before it), FP32 faces 8, the update half of the zone pass 4 (FP64 fluxes; no spills) or 5 (FP32
 // fluxes) and its inversion half 5 (6 in the FP32-flux form, whose zone pass holds the metric's
 // upper triangles only).  Each can be overridden at build time.
 #ifndef KHB_FLUX64_MINB
-#define KHB_FLUX64_MINB 5
+#define KHB_FLUX64_MINB 6
 #endif
 #ifndef KHB_FLUX64_X3_MINB
-#define KHB_FLUX64_X3_MINB 4
+#define KHB_FLUX64_X3_MINB 5
 #endif
 #ifndef KHB_FLUX32_MINB
 #define KHB_FLUX32_MINB 8
