@@ -392,6 +392,18 @@ def smr_form(steps=20, warm=3):
     out["mesh_overhead"] = ms / ms0 - 1.0
     del b
     torch.cuda.empty_cache()
+    # three levels: the central 2 x 2 x 2 of the refined blocks refined again
+    refine3 = refine + [(1, (i, j, k)) for i in (3, 4) for j in (3, 4) for k in (3, 4)]
+    mesh = SMRMesh(base, (4, 4, 4), (32, 32, 32), refine=refine3)
+    b = smr_batch(mesh, lambda sp: problems.entropy_wave(sp, amp=0.1))
+    dt = 0.3 * min(blk.spec.dx[0] for blk in mesh.blocks)
+    ms3, launches3 = timed(steps)
+    out["three_levels"] = {"workload": f"the same with the central 2x2x2 level-1 blocks refined again: 56 + 56 + 64 "
+                                       f"blocks, {mesh.zones:,} zones",
+                           "graph_ms_per_step": ms3, "zone_cycles_per_s": mesh.zones / (ms3 / 1000.0),
+                           "launches_per_step": launches3}
+    del b
+    torch.cuda.empty_cache()
     return out
 
 

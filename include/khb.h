@@ -456,8 +456,10 @@ int64_t khb_batch_launch_count(khb_batch* batch);
  * whose coarse faces on fine-coarse boundaries take the average of the fine fluxes before the update.
  * ghost: n_ghost entries of 6 int32 {dst block, dst zone, op, src block, src zone, aux}, op 0 copy,
  * 1 restriction (average of the 2^ndim fine zones from src zone upwards), 2 prolongation (src coarse
- * zone plus minmod-limited slopes times +-1/4; aux bit d: + side along direction d+1); the first
- * n_ghost_first entries are the copies and restrictions, the rest the prolongations.  The primitives
+ * zone plus minmod-limited slopes times +-1/4; aux bit d: + side along direction d+1, aux bits 8 and
+ * up: the prolongation phase, the destination level less one); the first n_ghost_first entries are
+ * the copies and restrictions, the rest the prolongations in phase order, each phase launched after
+ * the previous one (a level's prolongations read coarse ghost zones the coarser level's filled).  The primitives
  * are filled, then U = U(P) in those zones.  flux: n_flux entries {coarse block, direction, coarse
  * face, fine block, fine face of lowest index, 0}.  Hydro blocks (nvar 5) with exchange faces.
  * Every index is checked against the blocks' sizes.  Synchronizes the device. */

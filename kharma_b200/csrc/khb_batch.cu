@@ -43,6 +43,7 @@ struct khb_batch {
     int* mesh_ghost = nullptr;
     int* mesh_flux = nullptr;
     long long n_ghost = 0, n_ghost_first = 0, n_flux = 0;
+    std::vector<long long> ghost_phase_end;        // ends of the prolongation phases (one per level)
     // CUDA graph of one step
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -53,6 +54,18 @@ struct khb_batch {
 namespace {
 
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+// The mesh's ghost exchange: copies and restrictions, then the prolongations level by level
+void enqueue_mesh_ghost(khb_batch* b, int stage, cudaStream_t st)
+{
+    LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, 0, b->n_ghost_first, stage, st);
+    long long begin = b->n_ghost_first;
+    for (long long end : b->ghost_phase_end) {
+        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, begin, end, stage, st);
+        begin = end;
+    }
+    b->launches += 1 + (int64_t)b->ghost_phase_end.size();
+}
 
 #define KHB_BCUDA(call)                                                                  \
     do {                                                                                 \
@@ -240,9 +253,8 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
         b->launches += c->launches - l0;
     }
     if (b->n_ghost) {
-        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, 0, b->n_ghost_first, stage, st);
-        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, b->n_ghost_first, b->n_ghost, stage, st);
-        KHB_BLAUNCHED(b, 2);
+        enqueue_mesh_ghost(b, stage, st);
+        KHB_BLAUNCHED(b, 0);
     }
     return KHB_OK;
 }
@@ -407,7 +419,15 @@ int khb_batch_set_mesh(khb_batch* b, const int32_t* ghost, int64_t n_ghost, int6
         if (lo < 0 || hi >= ds.N) return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: ghost source outside its block");
         if ((e < n_ghost_first) != (t[2] != 2))
             return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: prolongations must follow copies and restrictions");
+        if (t[2] == 2) {
+            const int phase = t[5] >> 8;
+            if (phase < 0 || (e > n_ghost_first && phase < (ghost[6 * (e - 1) + 5] >> 8)))
+                return set_error(KHB_ERR_ARG, "khb_batch_set_mesh: prolongations must come in phase order");
+        }
     }
+    std::vector<long long> phase_end;
+    for (int64_t e = n_ghost_first; e < n_ghost; ++e)
+        if (e + 1 == n_ghost || (ghost[6 * (e + 1) + 5] >> 8) != (ghost[6 * e + 5] >> 8)) phase_end.push_back(e + 1);
     for (int64_t e = 0; e < n_flux; ++e) {
         const int32_t* t = flux + 6 * e;
         if (t[0] < 0 || t[0] >= b->nb || t[3] < 0 || t[3] >= b->nb || t[1] < 1 || t[1] > b->ndim)
@@ -423,6 +443,7 @@ int khb_batch_set_mesh(khb_batch* b, const int32_t* ghost, int64_t n_ghost, int6
     cudaFree(b->mesh_ghost); cudaFree(b->mesh_flux);
     b->mesh_ghost = nullptr; b->mesh_flux = nullptr;
     b->n_ghost = b->n_ghost_first = b->n_flux = 0;
+    b->ghost_phase_end.clear();
     if (n_ghost) {
         KHB_BCUDA(cudaMalloc((void**)&b->mesh_ghost, sizeof(int32_t) * 6 * (size_t)n_ghost));
         KHB_BCUDA(cudaMemcpy(b->mesh_ghost, ghost, sizeof(int32_t) * 6 * (size_t)n_ghost, cudaMemcpyHostToDevice));
@@ -433,6 +454,7 @@ int khb_batch_set_mesh(khb_batch* b, const int32_t* ghost, int64_t n_ghost, int6
     }
     KHB_BCUDA(cudaDeviceSynchronize());
     b->n_ghost = n_ghost; b->n_ghost_first = n_ghost_first; b->n_flux = n_flux;
+    b->ghost_phase_end = phase_end;
     return KHB_OK;
 }
 
@@ -440,9 +462,7 @@ int khb_batch_mesh_exchange(khb_batch* b, void* stream)
 {
     if (!b) return set_error(KHB_ERR_ARG, "khb_batch_mesh_exchange: NULL batch");
     if (b->n_ghost) {
-        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, 0, b->n_ghost_first, 2, S(stream));
-        LaunchCommon::mesh_ghost(b->nv, b->fix, b->mesh_ghost, b->n_ghost_first, b->n_ghost, 2, S(stream));
-        b->launches += 2;
+        enqueue_mesh_ghost(b, 2, S(stream));
         KHB_BCUDA(cudaGetLastError());
     }
     return KHB_OK;

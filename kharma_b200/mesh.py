@@ -1,5 +1,5 @@
-"""Static mesh refinement (SMR): a two-level block mesh on a periodic Cartesian domain, stepped as one
-batch with ghost-zone exchange and flux correction between blocks (khb_batch_set_mesh).
+"""Static mesh refinement (SMR): a multi-level block mesh on a periodic Cartesian domain, stepped as
+one batch with ghost-zone exchange and flux correction between blocks (khb_batch_set_mesh).
 
 Parthenon owns mesh refinement in the reference (KHARMA only enables it, kharma.cpp:381-382, and
 tasks the flux-correction messages, kharma_step.cpp:157-195); its cell-centred operators are
@@ -13,15 +13,17 @@ restated here as the algorithms it documents:
   * flux correction: a coarse face on a fine-coarse boundary takes the average of the 2^(ndim-1)
     fine fluxes through it before the update, so the mesh conserves what the uniform scheme does.
 Ghost zones are filled from primitives (then U = U(P) there); every block has the same zone count,
-as Parthenon requires, and the fine blocks cover whole coarse blocks (2:1 in each active direction).
-Scope: hydro (5 variables), 2 levels, periodic domain.
+as Parthenon requires, and the fine blocks cover whole coarse blocks (2:1 in each active direction,
+neighbouring blocks at most one level apart).  Scope: hydro (5 variables), periodic domain, any
+number of levels.
 
 `SMRMesh.tables()` gives the device tables khb_batch_set_mesh takes:
   ghost entries (int32 x 6): dst block, dst zone, op (0 copy, 1 restrict, 2 prolong), src block,
     src zone (copy: the zone; restrict: the fine zone of lowest index; prolong: the coarse zone),
-    aux (prolong: bit d set when the fine zone lies on the + side of the coarse centre along d+1);
-    copies and restrictions first, then prolongations (which read coarse ghost zones filled by the
-    first group);
+    aux (prolong: bit d set when the fine zone lies on the + side of the coarse centre along d+1,
+    and the prolongation phase, the destination level less one, in bits 8 and up);
+    copies and restrictions first, then the prolongations level by level (each reads coarse ghost
+    zones that the copies, the restrictions or the previous level's prolongations filled);
   flux entries (int32 x 6): coarse block, direction, coarse face (zone index of the zone above it),
     fine block, fine face of lowest index, 0.
 """
@@ -44,8 +46,10 @@ class MeshBlock:
 
 class SMRMesh:
     """Root grid of nb = (nb1, nb2, nb3) blocks of nx = (nx1, nx2, nx3) zones over `base`'s domain
-    (a Cartesian Minkowski BlockSpec supplying the physics options and the domain extent); root
-    blocks whose logical location is in `refine` are replaced by their 2^ndim children."""
+    (a Cartesian Minkowski BlockSpec supplying the physics options and the domain extent); a block
+    named in `refine` is replaced by its 2^ndim children one level up.  Entries are root locations
+    (l1, l2, l3), or (level, (l1, l2, l3)) for a block of that level (its logical location at that
+    level); refinements apply recursively, coarsest first."""
 
     def __init__(self, base: BlockSpec, nb, nx, refine=()):
         assert base.cart_minkowski and base.nvar == 5, "SMR: Cartesian Minkowski hydro blocks"
@@ -59,18 +63,28 @@ class SMRMesh:
         lo = (base.x1min, base.x2min, base.x3min)
         hi = (base.x1max, base.x2max, base.x3max)
         self.lo, self.size = lo, tuple(hi[d] - lo[d] for d in range(3))
-        refine = {tuple(r) for r in refine}
+        ref = set()
+        for r in refine:
+            if len(r) == 2 and isinstance(r[1], (tuple, list)):
+                ref.add((int(r[0]), tuple(int(x) for x in r[1])))
+            else:
+                ref.add((0, tuple(int(x) for x in r)))
         self.blocks = []
+
+        def place(level, loc):
+            if (level, loc) not in ref:
+                self._add(level, loc)
+                return
+            for c3 in range(2 if self.ndim > 2 else 1):
+                for c2 in range(2 if self.ndim > 1 else 1):
+                    for c1 in range(2):
+                        place(level + 1, (2 * loc[0] + c1, 2 * loc[1] + c2, 2 * loc[2] + c3))
+
         for l3 in range(self.nb[2]):
             for l2 in range(self.nb[1]):
                 for l1 in range(self.nb[0]):
-                    if (l1, l2, l3) in refine:
-                        for c3 in range(2 if self.ndim > 2 else 1):
-                            for c2 in range(2 if self.ndim > 1 else 1):
-                                for c1 in range(2):
-                                    self._add(1, (2 * l1 + c1, 2 * l2 + c2, 2 * l3 + c3))
-                    else:
-                        self._add(0, (l1, l2, l3))
+                    place(0, (l1, l2, l3))
+        self.levels = 1 + max(b.level for b in self.blocks)
         self.index = {(b.level, b.loc): n for n, b in enumerate(self.blocks)}
 
     def _add(self, level, loc):
@@ -103,13 +117,21 @@ class SMRMesh:
 
     def tables(self):
         ng, ndim, nx = self.ng, self.ndim, self.nx
-        own = [self._owners(0), self._owners(1)]
-        ghost_a, ghost_b, flux = [], [], []
+        own = [self._owners(L) for L in range(self.levels)]
+        ghost_a, flux = [], []
+        ghost_b = [[] for _ in range(self.levels)]      # prolongations by destination level
         act = [d < ndim for d in range(3)]
 
         def local(src_loc, g):
             # local (k, j, i) of global zone(s) g in blocks at logical locations src_loc
             return tuple((g[d] - src_loc[d] * nx[d] + ng) if act[d] else np.zeros_like(g[d]) for d in (2, 1, 0))
+
+        def owner(level, g):
+            # block id owning global zones g at `level` (-1: none), with the logical locations
+            if level < 0 or level >= self.levels:
+                return np.full(len(g[0]), -1, dtype=np.int64), None
+            lo = [g[d] // nx[d] if act[d] else g[d] for d in range(3)]
+            return own[level][lo[2], lo[1], lo[0]], lo
 
         for b, blk in enumerate(self.blocks):
             n3, n2, n1 = blk.spec.shape
@@ -123,8 +145,7 @@ class SMRMesh:
             g = [(blk.loc[0] * nx[0] + I - ng) % tot[0],
                  ((blk.loc[1] * nx[1] + J - ng) % tot[1]) if act[1] else np.zeros_like(I),
                  ((blk.loc[2] * nx[2] + K - ng) % tot[2]) if act[2] else np.zeros_like(I)]
-            loc = [g[d] // nx[d] if act[d] else np.zeros_like(I) for d in range(3)]
-            src = own[L][loc[2], loc[1], loc[0]]
+            src, loc = owner(L, g)
             same = src >= 0
             if same.any():
                 sl = [loc[d][same] for d in range(3)]
@@ -134,33 +155,38 @@ class SMRMesh:
                 ghost_a.append(np.stack([np.full(same.sum(), b), dst[same], np.full(same.sum(), OP_COPY),
                                          src[same], z, np.zeros(same.sum(), dtype=np.int64)], axis=1))
             rest = ~same
-            if rest.any():
-                gr = [g[d][rest] for d in range(3)]
-                if L == 1:
-                    gc = [gr[d] // 2 if act[d] else gr[d] for d in range(3)]
-                    lc = [gc[d] // nx[d] if act[d] else gc[d] for d in range(3)]
-                    s0 = own[0][lc[2], lc[1], lc[0]]
-                    assert (s0 >= 0).all(), "mesh is not 2:1 balanced"
-                    k, j, i = local(lc, gc)
-                    z = self._zone_index(k, j, i)
-                    aux = sum((gr[d] % 2) << d for d in range(ndim))
-                    ghost_b.append(np.stack([np.full(rest.sum(), b), dst[rest], np.full(rest.sum(), OP_PROLONG),
-                                             s0, z, aux], axis=1))
-                else:
-                    gf = [2 * gr[d] if act[d] else gr[d] for d in range(3)]
-                    lf = [gf[d] // nx[d] if act[d] else gf[d] for d in range(3)]
-                    s1 = own[1][lf[2], lf[1], lf[0]]
-                    assert (s1 >= 0).all(), "ghost zone with no covering block"
-                    k, j, i = local(lf, gf)
-                    z = self._zone_index(k, j, i)
-                    ghost_a.append(np.stack([np.full(rest.sum(), b), dst[rest], np.full(rest.sum(), OP_RESTRICT),
-                                             s1, z, np.zeros(rest.sum(), dtype=np.int64)], axis=1))
-            # flux correction: faces of a coarse block bordering fine blocks
-            if L != 0:
+            if not rest.any():
                 continue
-            tot1 = self._zones_at(1)
+            gr = [g[d][rest] for d in range(3)]
+            dr = dst[rest]
+            # a coarser neighbour: prolongation from level L-1
+            gc = [gr[d] // 2 if act[d] else gr[d] for d in range(3)]
+            s0, lc = owner(L - 1, gc)
+            # a finer neighbour: restriction from level L+1
+            gf = [2 * gr[d] if act[d] else gr[d] for d in range(3)]
+            s1, lf = owner(L + 1, gf)
+            assert ((s0 >= 0) ^ (s1 >= 0)).all(), "mesh is not 2:1 balanced"
+            pm, rm = s0 >= 0, s1 >= 0
+            if pm.any():
+                k, j, i = local([lc[d][pm] for d in range(3)], [gc[d][pm] for d in range(3)])
+                z = self._zone_index(k, j, i)
+                aux = sum((gr[d][pm] % 2) << d for d in range(ndim)) + ((L - 1) << 8)
+                ghost_b[L].append(np.stack([np.full(pm.sum(), b), dr[pm], np.full(pm.sum(), OP_PROLONG),
+                                            s0[pm], z, aux], axis=1))
+            if rm.any():
+                k, j, i = local([lf[d][rm] for d in range(3)], [gf[d][rm] for d in range(3)])
+                z = self._zone_index(k, j, i)
+                ghost_a.append(np.stack([np.full(rm.sum(), b), dr[rm], np.full(rm.sum(), OP_RESTRICT),
+                                         s1[rm], z, np.zeros(rm.sum(), dtype=np.int64)], axis=1))
+        # flux correction: faces of a block bordering finer blocks
+        for b, blk in enumerate(self.blocks):
+            L = blk.level
+            if L + 1 >= self.levels:
+                continue
+            tot = self._zones_at(L)
+            tot1 = self._zones_at(L + 1)
             for d in range(ndim):
-                # tangential global coarse indices of the face's zones
+                # tangential global indices (level L) of the face's zones
                 rng = [np.arange(blk.loc[e] * nx[e], (blk.loc[e] + 1) * nx[e]) if act[e] else np.zeros(1, dtype=np.int64)
                        for e in range(3)]
                 rng[d] = np.zeros(1, dtype=np.int64)
@@ -169,22 +195,21 @@ class SMRMesh:
                 for side in (0, 1):
                     across = list(t)
                     across[d] = np.full_like(t[0], (blk.loc[d] * nx[d] + (nx[d] if side else -1)) % tot[d])
-                    la = [across[e] // nx[e] if act[e] else across[e] for e in range(3)]
-                    if (own[0][la[2], la[1], la[0]] >= 0).all():
-                        continue
-                    assert (own[0][la[2], la[1], la[0]] < 0).all()
+                    if (owner(L, across)[0] >= 0).all():
+                        continue                            # same level
+                    if (owner(L - 1, [across[e] // 2 if act[e] else across[e] for e in range(3)])[0] >= 0).all():
+                        continue                            # a coarser neighbour corrects this face
                     ci = list(t)
                     ci[d] = np.full_like(t[0], blk.loc[d] * nx[d] + (nx[d] if side else 0))
                     k, j, i = local([np.full_like(t[0], blk.loc[e]) for e in range(3)], ci)
                     cface = self._zone_index(k, j, i)
-                    gf = [2 * t[e] if act[e] else t[e] for e in range(3)]
-                    gf[d] = (2 * ci[d]) % tot1[d]
-                    gown = list(gf)
+                    gfz = [2 * t[e] if act[e] else t[e] for e in range(3)]
+                    gfz[d] = (2 * ci[d]) % tot1[d]
+                    gown = list(gfz)
                     if not side:
-                        gown[d] = (gf[d] - 1) % tot1[d]
-                    lo = [gown[e] // nx[e] if act[e] else gown[e] for e in range(3)]
-                    fb = own[1][lo[2], lo[1], lo[0]]
-                    assert (fb >= 0).all()
+                        gown[d] = (gfz[d] - 1) % tot1[d]
+                    fb, lo = owner(L + 1, gown)
+                    assert (fb >= 0).all(), "mesh is not 2:1 balanced"
                     fk, fj, fi = local(lo, gown)
                     if not side:
                         if d == 0:
@@ -197,7 +222,8 @@ class SMRMesh:
                     flux.append(np.stack([np.full(len(fb), b), np.full(len(fb), d + 1), cface, fb, fz,
                                           np.zeros(len(fb), dtype=np.int64)], axis=1))
         cat = lambda parts: (np.concatenate(parts) if parts else np.zeros((0, 6), dtype=np.int64)).astype(np.int32)
-        ga, gb = cat(ghost_a), cat(ghost_b)
+        ga = cat(ghost_a)
+        gb = cat([x for lev in ghost_b for x in lev])
         return np.concatenate([ga, gb]), len(ga), cat(flux)
 
     # ------------------------------------------------------------------ helpers

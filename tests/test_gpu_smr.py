@@ -1,5 +1,5 @@
-"""Static mesh refinement through the batch (khb_batch_set_mesh): a two-level hydro mesh on a
-periodic box.
+"""Static mesh refinement through the batch (khb_batch_set_mesh): two- and three-level hydro meshes on
+a periodic box.
 
 * The ghost zones the library fills after an exchange equal, bitwise, the oracle-side restatement
   built from whole-domain arrays (oracle/smr_ref.py).
@@ -125,3 +125,36 @@ def test_entropy_wave_error_between_coarse_and_fine():
         errs[name] = e / vol
     print("entropy wave L1 errors:", errs)
     assert errs["fine"] < errs["smr"] < errs["coarse"]
+
+
+def three_level(nd, nx=8):
+    """4^nd roots of nx^nd zones, the central 2^nd refined, the central 2^nd of those refined again."""
+    c = [(a, b, e) for a in (1, 2) for b in (1, 2) for e in ((1, 2) if nd > 2 else (0,))]
+    f = [(1, (a, b, e)) for a in (3, 4) for b in (3, 4) for e in ((3, 4) if nd > 2 else (0,))]
+    return SMRMesh(base(nd), (4, 4, 4 if nd > 2 else 1), (nx, nx, nx if nd > 2 else 1), refine=c + f)
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_three_levels_exchange_matches_restatement(nd):
+    """The level-2 ghost zones prolongated from level-1 zones, some of which are level-1 ghost zones
+    prolongated from level 0 in the phase before: bitwise against the whole-domain restatement."""
+    mesh = three_level(nd)
+    seeds = iter(range(1000))
+    b = smr_batch(mesh, lambda s: random_smooth(s, next(seeds)))
+    torch.cuda.synchronize()
+    P = [blk.P.cpu().numpy() for blk in b.blocks]
+    for n, ((mask, E), Pb) in enumerate(zip(smr_ref.expected_ghosts(mesh, P), P)):
+        got, want = Pb[:, mask], E[:, mask]
+        assert np.array_equal(got, want), (n, mesh.blocks[n].level, np.abs(got - want).max())
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_three_levels_conserve(nd):
+    mesh = three_level(nd)
+    _, t0, t1 = run(mesh, True, steps=6)
+    scale = np.abs(t0).max()
+    refined = np.abs(t1 - t0) / scale
+    print("three levels, relative change of the conserved totals:", refined)
+    assert refined[0] <= 1e-13
+    _, u0, u1 = run(mesh, False, steps=6)
+    assert np.abs(u1[0] - u0[0]) > 1e-9 * abs(u0[0])

@@ -40,3 +40,49 @@ def test_tables_cover_every_ghost_zone_once(nd):
     expect = (3 if nd > 2 else 2) * 2 * nface
     assert len(flux) == expect
     assert set(flux[:, 3]) <= {b for b, blk in enumerate(mesh.blocks) if blk.level == 1}
+
+
+def three_level(nd, nx=8):
+    """4^nd roots; the central 2^nd refined; the central 2^nd of those refined again."""
+    c = [(a, b, e) for a in (1, 2) for b in (1, 2) for e in ((1, 2) if nd > 2 else (0,))]
+    f = [(1, (a, b, e)) for a in (3, 4) for b in (3, 4) for e in ((3, 4) if nd > 2 else (0,))]
+    return SMRMesh(hydro_base(nd) if nx == 8 else dataclasses.replace(hydro_base(nd), nx1=nx),
+                   (4, 4, 4 if nd > 2 else 1), (nx, nx, nx if nd > 2 else 1), refine=c + f)
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_three_level_tables(nd):
+    mesh = three_level(nd)
+    assert mesh.levels == 3
+    ghost, n_first, flux = mesh.tables()
+    assert np.all(ghost[:n_first, 2] != OP_PROLONG) and np.all(ghost[n_first:, 2] == OP_PROLONG)
+    # prolongation phases: the destination level less one, in order
+    phase = ghost[n_first:, 5] >> 8
+    assert np.all(np.diff(phase) >= 0) and set(phase) == {0, 1}
+    level = np.array([blk.level for blk in mesh.blocks])
+    assert np.all(level[ghost[n_first:, 0]] == phase + 1)
+    assert np.all(level[ghost[n_first:, 3]] == phase)
+    for b, blk in enumerate(mesh.blocks):
+        n3, n2, n1 = blk.spec.shape
+        inside = np.zeros(n3 * n2 * n1, dtype=bool)
+        inside.reshape(n3, n2, n1)[blk.spec.interior] = True
+        mine = ghost[ghost[:, 0] == b]
+        assert len(np.unique(mine[:, 1])) == len(mine) == (~inside).sum()
+        src_level = level[mine[:, 3]]
+        assert np.all(np.abs(src_level - blk.level) <= 1)
+        assert np.all((mine[:, 2] == OP_RESTRICT) == (src_level == blk.level + 1))
+        assert np.all((mine[:, 2] == OP_PROLONG) == (src_level == blk.level - 1))
+    # flux correction at both coarse-fine interfaces, each fine face block one level up
+    assert set(level[flux[:, 0]]) == {0, 1}
+    assert np.all(level[flux[:, 3]] == level[flux[:, 0]] + 1)
+    # every coarse face on a fine-coarse boundary once: 2^nd refined blocks' surfaces, per interface
+    per_face = 8 ** (nd - 1)
+    ring = 2 * nd * 2 ** (nd - 1)            # coarse faces (block faces) around a 2^nd patch
+    assert len(flux) == 2 * ring * per_face
+
+
+def test_unbalanced_mesh_is_rejected():
+    # a level-2 patch touching level-0 blocks
+    mesh = SMRMesh(hydro_base(2), (2, 2, 1), (8, 8, 1), refine=[(0, 0, 0), (1, (0, 0, 0))])
+    with pytest.raises(AssertionError, match="2:1"):
+        mesh.tables()
