@@ -674,13 +674,15 @@ def gpu_arm(args, rank, world, local_rank):
         fp32["rel_l1_rho_after_100_steps"] = float((r32 - r64).abs().sum() / r64.abs().sum())
         del ref, f32
 
-    # end-to-end through the C ABI with a host-resident state: khb_step_host copies the primitives in
-    # (pinned host memory), rebuilds U = U(P) on the device (the state's own U: the lock-step P -> U
-    # leaves U = U(P) after every step), replays the graph step and copies the primitives back
+    # end-to-end through the C ABI with a host-resident state: khb_step_host_interior copies the
+    # interior primitives in (pinned host memory), rebuilds U = U(P) and the ghost zones on the device
+    # (the state's own: the lock-step P -> U and the boundaries leave both as functions of the
+    # interior after every step), replays the graph step and copies the interior primitives back
     e2e = None
     if not args.no_e2e:
-        hP = torch.empty(b.P.shape, dtype=torch.float64, pin_memory=True)
-        hP.copy_(b.P)
+        isl = (slice(None),) + spec.interior
+        hP = torch.empty(b.P.shape if not graph_ok else b.P[isl].shape, dtype=torch.float64, pin_memory=True)
+        hP.copy_(b.P if not graph_ok else b.P[isl])
         torch.cuda.synchronize()
         ke = max(3, args.steps // 2)
         if world > 1:
@@ -690,7 +692,7 @@ def gpu_arm(args, rank, world, local_rank):
         e0.record()
         if graph_ok:
             for _ in range(ke):
-                drv.step_host(hP)
+                drv.step_host_interior(hP)
         else:
             for _ in range(ke):
                 b.P.copy_(hP, non_blocking=True)
@@ -703,11 +705,11 @@ def gpu_arm(args, rank, world, local_rank):
         if world > 1:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         ms_e = float(te.item()) / ke
-        nbytes = b.P.numel() * 8
+        nbytes = hP.numel() * 8
         e2e = {"value": world * zones / (ms_e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes if world == 1 else nbytes + 8, "ms_per_step": ms_e,
-               "path": "khb_step_host (P in, U = U(P), graph step, P out)" if graph_ok else
-                       "P in, khb_ptou, host-driven step, P out"}
+               "path": "khb_step_host_interior (interior P in, U = U(P) and ghost zones rebuilt, graph step, "
+                       "interior P out)" if graph_ok else "P in, khb_ptou, host-driven step, P out"}
 
     # roofline of the dominant kernel, timed live with CUDA events
     peak, peak_kind = measured_peaks()

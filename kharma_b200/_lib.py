@@ -133,6 +133,7 @@ SIGNATURES = {
     "khb_step_device_dt": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
     "khb_step_graph": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
     "khb_step_host": (_I, [_P, C.POINTER(_P), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_step_host_interior": (_I, [_P, C.POINTER(_P), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
     "khb_adjoint_step": (_I, [_P, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
                               C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _D, _P]),
     "khb_adjoint_ptou": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),

@@ -237,6 +237,15 @@ class DeviceDriver:
                                        C.c_void_p(b.fflag.data_ptr()), b.stream), "khb_step_host")
         self.nstep += 1
 
+    def step_host_interior(self, hP):
+        """step_host for host primitives holding the interior only ((nvar, nx3, nx2, nx1) float64,
+        pinned, contiguous per variable): khb_step_host_interior rebuilds the ghost zones on the device."""
+        b = self.block
+        ptrs = (C.c_void_p * b.spec.nvar)(*[hP[p].data_ptr() for p in range(b.spec.nvar)])
+        _lib.check(b.lib.khb_step_host_interior(b.ctx, ptrs, b.Pf.ref, b.Uf.ref, C.c_void_p(b.pflag.data_ptr()),
+                                                C.c_void_p(b.fflag.data_ptr()), b.stream), "khb_step_host_interior")
+        self.nstep += 1
+
     def timestep(self):
         """(next dt, time, dt of the last step); synchronizes."""
         dt, t, last = C.c_double(), C.c_double(), C.c_double()

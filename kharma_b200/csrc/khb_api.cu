@@ -165,6 +165,22 @@ int launch_fixup(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, const i
     return KHB_OK;
 }
 
+// The interior zones of a block to / from a packed [nv][nx3][nx2][nx1] buffer (unpack: buffer -> P)
+__global__ void k_interior_pack(Dims d, khb_fields P, int nv, double* buf, int unpack)
+{
+    const long long nint = (long long)d.nx1 * d.nx2 * d.nx3;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nint) return;
+    const int i = (int)(t % d.nx1);
+    const long long r = t / d.nx1;
+    const int j = (int)(r % d.nx2), k = (int)(r / d.nx2);
+    const long long c = ((long long)(k + d.ks) * d.n2 + (j + d.js)) * d.n1 + (i + d.is);
+    for (int p = 0; p < nv; ++p) {
+        if (unpack) P.v[p][c] = buf[p * nint + t];
+        else buf[p * nint + t] = P.v[p][c];
+    }
+}
+
 // Bf: a B_CT block's faces; with physical faces their ghost layers are filled first and the ghost
 // zones of the physical directions take B from them
 int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st,
@@ -934,6 +950,41 @@ int khb_step_host(khb_ctx* ctx, double* const* P_host, const khb_fields* P, cons
     KHB_LAUNCHED(ctx);
     if ((rc = khb_step_graph(ctx, P, U, pflag, fflag, stream))) return rc;
     for (int p = 0; p < ctx->nv; ++p) KHB_CUDA(cudaMemcpyAsync(P_host[p], P->v[p], bytes, cudaMemcpyDeviceToHost, st));
+    return KHB_OK;
+}
+
+int khb_step_host_interior(khb_ctx* ctx, double* const* P_host, const khb_fields* P, const khb_fields* U,
+                           int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_NEED_GEOM(ctx);
+    if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_host_interior: a B_CT block steps with khb_ct_stage/khb_ct_step");
+    if (has_exchange_face(ctx->d))
+        return fail(KHB_ERR_UNSUPPORTED, "khb_step_host_interior: exchange faces hold the caller's ghost zones; use khb_step_host");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
+    if (!P_host) return fail(KHB_ERR_ARG, "khb_step_host_interior: NULL host state");
+    for (int p = 0; p < ctx->nv; ++p)
+        if (!P_host[p]) return fail(KHB_ERR_ARG, "khb_step_host_interior: NULL host variable");
+    cudaStream_t st = S(stream);
+    const Dims& d = ctx->d;
+    const long long nint = (long long)d.nx1 * d.nx2 * d.nx3;
+    const size_t bytes = sizeof(double) * (size_t)nint;
+    // the stage scratch is free before and after the step: it carries the packed interiors
+    double* buf = ctx->stageP;
+    for (int p = 0; p < ctx->nv; ++p)
+        KHB_CUDA(cudaMemcpyAsync(buf + (size_t)p * nint, P_host[p], bytes, cudaMemcpyHostToDevice, st));
+    k_interior_pack<<<blocks_for(nint, 256), 256, 0, st>>>(d, *P, ctx->nv, buf, 1);
+    KHB_LAUNCHED(ctx);
+    // U = U(P) on the interior (the ghost zones' values are rebuilt next), then the ghost zones
+    // exactly as the step's last stage leaves them: boundaries of the interior, U = U(P) there
+    LaunchCommon::ptou(ctx->nv, d, ctx->g, ctx->ph, *P, *U, st);
+    KHB_LAUNCHED(ctx);
+    if ((rc = launch_boundaries(ctx, *P, *U, st))) return rc;
+    if ((rc = khb_step_graph(ctx, P, U, pflag, fflag, stream))) return rc;
+    k_interior_pack<<<blocks_for(nint, 256), 256, 0, st>>>(d, *P, ctx->nv, buf, 0);
+    KHB_LAUNCHED(ctx);
+    for (int p = 0; p < ctx->nv; ++p)
+        KHB_CUDA(cudaMemcpyAsync(P_host[p], buf + (size_t)p * nint, bytes, cudaMemcpyDeviceToHost, st));
     return KHB_OK;
 }
 

@@ -69,3 +69,36 @@ def test_step_host_matches_device_resident_steps():
         b.ptou()
         torch.cuda.synchronize()
         assert torch.equal(U0, b.U)
+
+
+def test_step_host_interior_matches_device_resident_steps():
+    """khb_step_host_interior (interior primitives in, ghost zones rebuilt on the device, graph step,
+    interior primitives out) leaves the device-resident graph step's state, bit for bit, ghost zones
+    included; blocks with exchange faces are refused."""
+    import dataclasses
+    from kharma_b200 import _lib, problems
+    from kharma_b200.block import Block, DeviceDriver, build_geometry
+    from kharma_b200.spec import mhdmodes_spec, torus_spec
+    spec = torus_spec(32, 24, 8)
+    geom = build_geometry(spec)
+    P0 = problems.fm_torus(spec, geom, seed=5)
+    sl = (slice(None),) + spec.interior
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        a = Block(spec, geometry=geom); a.set_prims(P0)
+        b = Block(spec, geometry=geom); b.set_prims(P0)
+        da, db = DeviceDriver(a), DeviceDriver(b)
+        hP = torch.empty(b.P[sl].shape, dtype=torch.float64, pin_memory=True)
+        hP.copy_(b.P[sl])
+        for _ in range(5):
+            da.step()
+            db.step_host_interior(hP)
+        torch.cuda.synchronize()
+        assert torch.equal(a.P[sl].cpu(), hP)
+        assert torch.equal(a.P, b.P) and torch.equal(a.U, b.U)
+        ex = Block(dataclasses.replace(mhdmodes_spec(16, 16, 1), bc=("exchange",) * 4 + ("periodic",) * 2))
+        ex.set_prims(problems.mhdmodes(ex.spec, 3))
+        dex = DeviceDriver(ex)
+        h = torch.empty(ex.P[(slice(None),) + ex.spec.interior].shape, dtype=torch.float64, pin_memory=True)
+        with pytest.raises(_lib.KhbError, match="exchange"):
+            dex.step_host_interior(h)
