@@ -334,7 +334,7 @@ int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, 
 
 /* ---------------------------------------------------------------------------------------------
  * B_CT: face-centred magnetic field (cfg.ct_scheme != KHB_CT_NONE; 2D and 3D blocks; X1/X2 faces
- * periodic, exchange, outflow or reflecting, X3 faces periodic or exchange; 4 ghost zones with
+ * periodic, exchange, outflow, reflecting or transmitting, X3 faces periodic or exchange; 4 ghost zones with
  * physical faces).  Face fields are passed as khb_fields with v[0..2] = the conserved sqrt(-g) B^1,
  * B^2, B^3 on x1, x2, x3 faces, each [n3][n2][n1] like the zone arrays, face i being the left face
  * of zone i (faces of the interior, [is, ie+1] along their own direction, are the state; the cell
@@ -355,10 +355,12 @@ int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, cons
  * physical faces, the face field's ghost layers first — reflecting faces: tangential components
  * mirrored, the normal one zero on the domain face and reflected beyond it (reflect_face_vector);
  * outflow faces: tangential components copied, the normal one rebuilt outward for zero divergence
- * (clean_face_B, b_ct_boundaries.cpp:190-262) — then the zone boundaries as khb_boundaries, with the
+ * (clean_face_B, b_ct_boundaries.cpp:190-262); transmitting X2 faces: the mirror rows half-way
+ * round in x3 (one_block_transmit.cpp:60-143) — then the zone boundaries as khb_boundaries, with the
  * ghost zones' B from their faces (B_CT::BlockUtoP over the boundary domain).  Without physical
- * faces it is khb_boundaries.  Reflecting faces also zero the EMFs on their domain-face edges during
- * each stage (zero_EMF, b_ct_boundaries.cpp:40-62). */
+ * faces it is khb_boundaries.  During each stage reflecting faces zero the EMFs on their domain-face
+ * edges (zero_EMF, b_ct_boundaries.cpp:40-62) and transmitting ones average them (average_EMF,
+ * b_ct_boundaries.cpp:64-186). */
 int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf, void* stream);
 
 /* Full RK2 step with B_CT in place on (P, U, Bf), the intermediate stage in context scratch. */

@@ -413,10 +413,11 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
         for (int f = 0; f < 2 * d.ndim; ++f) {
             if (!phys_face(cfg->bc[f])) continue;
             physical = true;
-            // b_ct_boundaries.cpp: outflow (clean_face_B) and reflecting (reflect_face_vector,
-            // zero_EMF) X1/X2 faces; transmitting faces (average_EMF) are not built
-            if (f >= 4 || (cfg->bc[f] != KHB_BC_OUTFLOW && cfg->bc[f] != KHB_BC_REFLECTING)) {
-                *why = "B_CT blocks take outflow or reflecting X1/X2 faces, periodic or exchange faces otherwise";
+            // b_ct_boundaries.cpp: outflow (clean_face_B), reflecting (reflect_face_vector,
+            // zero_EMF) and transmitting (average_EMF, X2 faces only as for the zones) X1/X2 faces
+            if (f >= 4 || (cfg->bc[f] != KHB_BC_OUTFLOW && cfg->bc[f] != KHB_BC_REFLECTING &&
+                           cfg->bc[f] != KHB_BC_TRANSMITTING)) {
+                *why = "B_CT blocks take outflow, reflecting or transmitting X1/X2 faces, periodic or exchange faces otherwise";
                 return KHB_ERR_UNSUPPORTED;
             }
         }

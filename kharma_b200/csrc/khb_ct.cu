@@ -204,10 +204,10 @@ __host__ __device__ inline int ct_nx(const Dims& d, int bdir) { return (bdir == 
 __host__ __device__ inline int ct_s(const Dims& d, int bdir) { return (bdir == 1) ? d.is : (bdir == 2) ? d.js : d.ks; }
 __host__ __device__ inline int ct_e(const Dims& d, int bdir) { return (bdir == 1) ? d.ie : (bdir == 2) ? d.je : d.ke; }
 
-// zero_EMF (b_ct_boundaries.cpp:40-62): the two EMF components along the domain face's edges, over
-// the whole face plane
+// zero_EMF (b_ct_boundaries.cpp:40-62): the EMF components in mask (bit v: E(v+1)) on the domain
+// face's edges, over the whole face plane
 template <typename FT>
-__global__ void k_ct_zero_emf(Dims d, int bdir, int f, FT* emf)
+__global__ void k_ct_zero_emf(Dims d, int bdir, int f, int mask, FT* emf)
 {
     const int na = ct_na(d, bdir), nb = ct_nb(d, bdir);
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -215,7 +215,48 @@ __global__ void k_ct_zero_emf(Dims d, int bdir, int f, FT* emf)
     const long long c = ct_at(d, bdir, f, (int)(t % na), (int)(t / na));
 #pragma unroll
     for (int v = 0; v < 3; ++v)
-        if (v != bdir - 1) emf[v*d.N + c] = (FT)0;
+        if (mask & (1 << v)) emf[v*d.N + c] = (FT)0;
+}
+
+// average_EMF on a transmitting X2 face (b_ct_boundaries.cpp:64-186, 3D): E1 on the polar face
+// replaced by its average over the interior x3 edges, summed over k upwards (the reference's team
+// reduction has no fixed order), every k set.  One thread per i.
+template <typename FT>
+__global__ void k_ct_average_emf1(Dims d, int jf, FT* emf)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n1) return;
+    double sum = 0.;
+    for (int k = d.ks; k <= d.ke; ++k) sum += (double)emf[((long long)k*d.n2 + jf)*d.n1 + i];
+    const double av = sum / (d.ke + 1 - d.ks);
+    for (int k = 0; k < d.n3; ++k) emf[((long long)k*d.n2 + jf)*d.n1 + i] = (FT)av;
+}
+
+// OneBlockTransmit on the face field (one_block_transmit.cpp:60-143), X2 faces: the mirror face
+// half-way round in x3; F1 copied, F3 inverted over the ghost rows, F2 inverted beyond the polar face
+// and zero on it.  One thread per (k, row, i) of the rows j < js (or > je) and the polar face row.
+__global__ void k_ct_face_transmit(Dims d, khb_fields Bf, int binner)
+{
+    const int s = d.js, e = d.je, f = binner ? s : e + 1;
+    const int rows = binner ? s + 1 : d.n2 - f;                   // ghost rows plus the polar face row
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)rows * d.n1 * d.n3) return;
+    const int i = (int)(t % d.n1);
+    const long long r = t / d.n1;
+    const int l = (int)(r % rows), k = (int)(r / rows);
+    const int j = binner ? l : f + l;
+    const int ki = ((k - d.ks + d.nx3 / 2) % d.nx3) + d.ks;
+    if (ki < 0 || ki >= d.n3) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    if (binner ? j < s : j > e) {
+        const int ji = binner ? 2*s - 1 - j : 2*e + 1 - j;
+        const long long m = ((long long)ki*d.n2 + ji)*d.n1 + i;
+        Bf.v[0][c] = Bf.v[0][m];
+        Bf.v[2][c] = -Bf.v[2][m];
+    }
+    const int ji = 2*f - j;
+    if (ji < 0 || ji >= d.n2) return;
+    Bf.v[1][c] = (j == f) ? 0. : -Bf.v[1][((long long)ki*d.n2 + ji)*d.n1 + i];
 }
 
 // The tangential face components of one face's ghost layers, as zones: outflow copies the first
@@ -328,12 +369,28 @@ int ct_emf(khb_ctx* ctx, const khb_fields& Ps, cudaStream_t st)
     ctx->launches += 1 + (ctx->ph.ct_scheme != KHB_CT_BS99);
     const Dims& d = ctx->d;
     for (int face = 0; face < 2 * d.ndim; ++face) {
+        if (d.bc[face] == KHB_BC_TRANSMITTING) {
+            const int jf = (face == 2) ? d.js : d.je + 1;
+            const long long n = (long long)d.n1 * d.n3;
+            if (ctx->ph.spherical) {                     // E3 only (component mask 4)
+                if (ctx->fp32) k_ct_zero_emf<float><<<blocks_for(n, 128), 128, 0, st>>>(d, 2, jf, 4, (float*)ctx->emf);
+                else k_ct_zero_emf<double><<<blocks_for(n, 128), 128, 0, st>>>(d, 2, jf, 4, (double*)ctx->emf);
+                ctx->launches += 1;
+            }
+            if (d.ndim > 2) {
+                if (ctx->fp32) k_ct_average_emf1<float><<<blocks_for(d.n1, 128), 128, 0, st>>>(d, jf, (float*)ctx->emf);
+                else k_ct_average_emf1<double><<<blocks_for(d.n1, 128), 128, 0, st>>>(d, jf, (double*)ctx->emf);
+                ctx->launches += 1;
+            }
+            continue;
+        }
         if (d.bc[face] != KHB_BC_REFLECTING) continue;
         const int bdir = face / 2 + 1, binner = (face % 2) == 0;
         const int f = binner ? ct_s(d, bdir) : ct_e(d, bdir) + 1;
         const long long n = (long long)ct_na(d, bdir) * ct_nb(d, bdir);
-        if (ctx->fp32) k_ct_zero_emf<float><<<blocks_for(n, 128), 128, 0, st>>>(d, bdir, f, (float*)ctx->emf);
-        else k_ct_zero_emf<double><<<blocks_for(n, 128), 128, 0, st>>>(d, bdir, f, (double*)ctx->emf);
+        const int mask = 7 & ~(1 << (bdir - 1));        // the two components along the face
+        if (ctx->fp32) k_ct_zero_emf<float><<<blocks_for(n, 128), 128, 0, st>>>(d, bdir, f, mask, (float*)ctx->emf);
+        else k_ct_zero_emf<double><<<blocks_for(n, 128), 128, 0, st>>>(d, bdir, f, mask, (double*)ctx->emf);
         ctx->launches += 1;
     }
     const cudaError_t e = cudaGetLastError();
@@ -347,6 +404,12 @@ int ct_face_boundaries(khb_ctx* ctx, const khb_fields& Bf, cudaStream_t st)
     const Dims& d = ctx->d;
     auto one = [&](int face) {
         const int bdir = face / 2 + 1, binner = (face % 2) == 0;
+        if (d.bc[face] == KHB_BC_TRANSMITTING) {
+            const int rows = binner ? d.js + 1 : d.n2 - (d.je + 1);
+            k_ct_face_transmit<<<blocks_for((long long)rows * d.n1 * d.n3, 128), 128, 0, st>>>(d, Bf, binner);
+            ctx->launches += 1;
+            return;
+        }
         const int outflow = d.bc[face] == KHB_BC_OUTFLOW;
         const long long plane = (long long)ct_na(d, bdir) * ct_nb(d, bdir);
         const int layers = binner ? ct_s(d, bdir) : ct_nx(d, bdir) - 1 - ct_e(d, bdir);

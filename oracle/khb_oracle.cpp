@@ -2020,6 +2020,23 @@ static void ct_zero_boundary_emf(const Block& B, double* emf)
 {
     const size_t N = B.N;
     for (int face = 0; face < 2*B.ndim; ++face) {
+        if (B.c.bc[face] == BC_TRANSMIT) {
+            // average_EMF (b_ct_boundaries.cpp:64-186) on a transmitting X2 face: E3 zero on the polar
+            // face (spherical coordinates: the edges have no length), E1 replaced by its average over
+            // the interior x3 edges (3D; in 2D E1 is left alone).  The reference's team reduction has
+            // no fixed order; the sum here runs over k upwards.
+            const int jf = (face == 2) ? B.js : B.je + 1;
+            if (B.C.spherical())
+                for (int k = 0; k < B.n3; ++k) for (int i = 0; i < B.n1; ++i) emf[2*N + B.id(k, jf, i)] = 0.;
+            if (B.ndim > 2)
+                for (int i = 0; i < B.n1; ++i) {
+                    double sum = 0.;
+                    for (int k = B.ks; k <= B.ke; ++k) sum += emf[B.id(k, jf, i)];
+                    const double av = sum / (B.ke + 1 - B.ks);
+                    for (int k = 0; k < B.n3; ++k) emf[B.id(k, jf, i)] = av;
+                }
+            continue;
+        }
         if (B.c.bc[face] != BC_REFLECT) continue;
         const int bdir = face / 2 + 1;
         const bool binner = (face % 2) == 0;
@@ -2053,7 +2070,7 @@ static void ct_face_boundary(const Block& B, double* Bf, int face)
     };
     // tangential components: zone-like ghost layers (Parthenon's outflow / reflect)
     for (int v = 0; v < 3; ++v) {
-        if (v == bdir - 1) continue;
+        if (v == bdir - 1 || type == BC_TRANSMIT) continue;
         for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
             const int x = idx(k, j, i);
             if (binner ? x >= s : x <= e) continue;
@@ -2062,6 +2079,27 @@ static void ct_face_boundary(const Block& B, double* Bf, int face)
         }
     }
     const int v = bdir - 1;
+    if (type == BC_TRANSMIT) {
+        // OneBlockTransmit on the face field (one_block_transmit.cpp:60-143, X2 faces): the mirror
+        // face half-way round in x3; F2 and F3 inverted, F2 zero on the polar face itself
+        const int nx3 = B.c.nx3;
+        auto ki_of = [&](int k) { return ((k - B.ks + nx3 / 2) % nx3) + B.ks; };
+        for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
+            const int ki = ki_of(k);
+            if (ki < 0 || ki >= B.n3) continue;
+            if (binner ? j < s : j > e) {                  // F1 and F3: zone-like layers
+                const int ji = binner ? 2*s - 1 - j : 2*e + 1 - j;
+                at(0, k, j, i) = Bf[B.id(ki, ji, i)];
+                at(2, k, j, i) = -Bf[2*N + B.id(ki, ji, i)];
+            }
+            if (binner ? j <= f : j >= f) {                // F2: the polar face and beyond
+                const int ji = 2*f - j;
+                if (ji < 0 || ji >= nb) continue;
+                at(1, k, j, i) = (j == f) ? 0. : -Bf[N + B.id(ki, ji, i)];
+            }
+        }
+        return;
+    }
     if (type == BC_REFLECT) {
         // reflect_face_vector (boundaries.cpp:458-479): zero on the domain face, minus the mirror face
         for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {

@@ -7,10 +7,10 @@
 * The 2D fast mode converges at second order with B_CT, as the reference's mhdmodes test requires
   of the flux-CT path.
 * The FP32-flux form with B_CT against FP64 B_CT.
-* Physical faces (b_ct_boundaries.cpp, boundaries.cpp:432-490): the FM torus (outflow X1 with
-  inflow checks, reflecting X2, periodic X3, drift floors) with B_CT against the oracle's
-  restatement of zero_EMF, reflect_face_vector, clean_face_B and the ghost zones' B from their
-  faces — primitives, conserved variables and every stored face to 1e-12 (floors call pow), flags
+* Physical faces (b_ct_boundaries.cpp, boundaries.cpp:432-490, one_block_transmit.cpp): the FM
+  torus (outflow X1 with inflow checks, reflecting or transmitting X2, periodic X3, drift floors)
+  with B_CT against the oracle's restatement of zero_EMF, average_EMF, reflect_face_vector,
+  clean_face_B, the transmitted face rows and the ghost zones' B from their faces — primitives, conserved variables and every stored face to 1e-12 (floors call pow), flags
   identical; the face divergence of the torus's face curl stays at rounding over 100 steps.
 """
 import dataclasses
@@ -160,6 +160,10 @@ TORI = {
     "torus3d_mc_gs05_c": lambda: dataclasses.replace(torus_spec(24, 16, 8), b_ct="gs05_c"),
     "torus3d_mc_bs99": lambda: dataclasses.replace(torus_spec(24, 16, 8), b_ct="bs99"),
     "torus3d_weno5_gs05_0": lambda: dataclasses.replace(torus_spec(24, 16, 8, recon="weno5"), b_ct="gs05_0"),
+    # transmitting poles (average_EMF, the face field's transmitted ghost rows): MKS over all of x3
+    "torus3d_mks_transmitting_gs05_c": lambda: dataclasses.replace(
+        torus_spec(24, 16, 16), transform="mks", b_ct="gs05_c",
+        bc=("outflow", "outflow", "transmitting", "transmitting", "periodic", "periodic")),
 }
 
 
