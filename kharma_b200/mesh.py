@@ -12,7 +12,8 @@ restated here as the algorithms it documents:
     cover (RestrictCellAverage on a uniform grid);
   * flux correction: a coarse face on a fine-coarse boundary takes the average of the 2^(ndim-1)
     fine fluxes through it before the update, so the mesh conserves what the uniform scheme does.
-Ghost zones are filled from primitives (then U = U(P) there); every block has the same zone count,
+Ghost zones are filled from primitives (then U = U(P) there), as KHARMA's simple and imex drivers
+exchange them (sync_prims, kharma_driver.cpp:109-110); every block has the same zone count,
 as Parthenon requires, and the fine blocks cover whole coarse blocks (2:1 in each active direction,
 neighbouring blocks at most one level apart).  Scope: hydro (5 variables), periodic domain, any
 number of levels.
