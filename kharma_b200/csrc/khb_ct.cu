@@ -6,10 +6,11 @@
 // zone pass then takes the zone B from the updated faces (ct_zone_b in khb_kernels.cuh).  EMFs are
 // formed in the flux arithmetic FT (FP32 in the FP32-flux form); the face update is FP64.  Blocks are
 // 2D or 3D.  Interior faces are the state; every EMF and zone-centred EMF they need lies within the
-// flux ranges and the ghost zones.  X1/X2 faces may be physical (outflow or reflecting): reflecting
-// faces zero the EMFs on their domain-face edges (zero_EMF), and after each stage the face field's
-// ghost layers are filled (k_ct_face_tangential, k_ct_face_reflect, k_ct_face_outflow with the
-// divergence cleaning) before the ghost zones take B from their faces (k_ghost_ptou).
+// flux ranges and the ghost zones.  X1/X2 faces may be physical (outflow, reflecting, or transmitting
+// X2 faces): reflecting faces zero the EMFs on their domain-face edges (zero_EMF), transmitting ones
+// average them (average_EMF), and after each stage the face field's ghost layers are filled
+// (k_ct_face_tangential, k_ct_face_reflect, k_ct_face_outflow with the divergence cleaning,
+// k_ct_face_transmit) before the ghost zones take B from their faces (k_ghost_ptou).
 #include "khb_internal.hpp"
 #include "khb_kernels.cuh"
 
