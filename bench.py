@@ -736,6 +736,13 @@ def gpu_arm(args, rank, world, local_rank):
                              "frac": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9 / peak,
                              "alg_bytes_per_zone_cycle": B_ALG_PER_ZC},
                     "kernel_ms_per_launch": {k: round(v[0], 4) for k, v in ktimes.items()}}
+        if (n1, n2, n3) == (128, 128, 128):
+            # the bound that applies to the FP64 path: FP64-pipe activity of its kernels on this
+            # workload (ncu sm__pipe_fp64_cycles_active as a fraction of peak, from the full capture
+            # of the stage-2 kernels of this build); not timed live
+            roofline["fp64_pipe"] = {"source": "ncu capture of this workload", "k_flux_x1": 0.427,
+                                     "k_flux_x2": 0.390, "k_flux_x3": 0.382, "k_zone_update": 0.241,
+                                     "k_zone_cell": 0.382}
 
     emhd = None
     if rank == 0 and world == 1 and not args.no_emhd:
