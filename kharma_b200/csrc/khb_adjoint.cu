@@ -263,9 +263,10 @@ __global__ void __launch_bounds__(128) k_adj_ptou(Dims d, DevGeom g, Phys ph, kh
     }
 }
 
-// Ghost-zone adjoints: a zone outside the interior only in periodic directions is a copy of its
-// image, so its adjoint is added to the image; any other ghost zone is the caller's constant.  All
-// ghost adjoints are zeroed afterwards (two launches: fold, then clear).
+// Ghost-zone adjoints: a zone outside the interior along a periodic direction is a copy of its
+// image, so its adjoint is added to the image (first); a zone of a physical face's ghost layers is
+// a function of its source zone (k_adj_bc, next); any other ghost zone is the caller's constant.  All
+// ghost adjoints are zeroed afterwards.
 template <int NV>
 __global__ void k_adj_fold(Dims d, khb_fields A, int pmask)
 {
@@ -273,15 +274,19 @@ __global__ void k_adj_fold(Dims d, khb_fields A, int pmask)
     if (t >= d.N) return;
     int k, j, i;
     zone_kji(d, t, k, j, i);
-    const bool gi = i < d.is || i > d.ie, gj = j < d.js || j > d.je, gk = k < d.ks || k > d.ke;
+    // k_periodic copies every zone outside the interior along a periodic direction from its image,
+    // wrapping the periodic directions only (the image may lie in another direction's ghost zones)
+    const bool gi = (pmask & 1) && (i < d.is || i > d.ie), gj = (pmask & 2) && (j < d.js || j > d.je);
+    const bool gk = (pmask & 4) && (k < d.ks || k > d.ke);
     if (!(gi || gj || gk)) return;
-    if ((gi && !(pmask & 1)) || (gj && !(pmask & 2)) || (gk && !(pmask & 4))) return;
     const int ii = gi ? i + ((i < d.is) ? d.nx1 : -d.nx1) : i;
     const int jj = gj ? j + ((j < d.js) ? d.nx2 : -d.nx2) : j;
     const int kk = gk ? k + ((k < d.ks) ? d.nx3 : -d.nx3) : k;
     const long long s = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+    // a periodic ghost zone is never an image, so zeroing it here races with nothing; the physical
+    // faces' adjoint then sees only what their own fills contributed
 #pragma unroll
-    for (int p = 0; p < NV; ++p) atomicAdd(A.v[p] + s, A.v[p][t]);
+    for (int p = 0; p < NV; ++p) { atomicAdd(A.v[p] + s, A.v[p][t]); A.v[p][t] = 0.; }
 }
 template <int NV>
 __global__ void k_adj_clear_ghosts(Dims d, khb_fields A)
@@ -294,6 +299,71 @@ __global__ void k_adj_clear_ghosts(Dims d, khb_fields A)
     if (interior) return;
 #pragma unroll
     for (int p = 0; p < NV; ++p) A.v[p][t] = 0.;
+}
+
+// Adjoint of one physical face's ghost fill k_bc (hydro): the ghost zone's primitives are its
+// source zone's, the normal velocity inverted on reflecting faces, and on X1 faces with inflow checks
+// the velocity passed through inflow_fix (its Jacobian by three dual evaluations).  Pbar(source) +=
+// J^T Pbar(ghost), then Pbar(ghost) = 0.  Same thread layout and index logic as k_bc.
+__global__ void k_adj_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields Pbar, int face,
+                         int lo_a, int cnt_a, int lo_k, int cnt_k)
+{
+    const int bdir = face / 2 + 1;
+    const bool inner = (face % 2) == 0;
+    const int ng = (bdir == 1) ? d.is : d.js;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ng*cnt_a*cnt_k) return;
+    const int gidx = (int)(t % ng);
+    const long long r = t / ng;
+    const int aidx = lo_a + (int)(r % cnt_a);
+    const int k = lo_k + (int)(r / cnt_a);
+    int i, j, ref;
+    if (bdir == 1) { j = aidx; ref = inner ? d.is : d.ie; i = inner ? gidx : d.ie + 1 + gidx; }
+    else { i = aidx; ref = inner ? d.js : d.je; j = inner ? gidx : d.je + 1 + gidx; }
+    const int type = d.bc[face];
+    const int offset = 2 * ref + (inner ? -1 : 1);
+    int ii = i, jj = j;
+    if (bdir == 1) ii = (type == KHB_BC_OUTFLOW) ? ref : offset - i;
+    else           jj = (type == KHB_BC_OUTFLOW) ? ref : offset - j;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long s = ((long long)k*d.n2 + jj)*d.n1 + ii;
+    double pb[5];
+    bool any = false;
+#pragma unroll
+    for (int p = 0; p < 5; ++p) { pb[p] = Pbar.v[p][c]; Pbar.v[p][c] = 0.; any |= pb[p] != 0.; }
+    if (!any) return;
+    double sgn[5];
+#pragma unroll
+    for (int p = 0; p < 5; ++p) sgn[p] = ((type == KHB_BC_REFLECTING) && (p == 1 + bdir)) ? -1.0 : 1.0;
+    const bool inflow = (face == 0 && ph.check_inflow_in) || (face == 1 && ph.check_inflow_out);
+    if (inflow) {
+        typedef Dual<double> DD;
+        ZoneGeom G;
+        load_zone_geom(g, j, i, G);
+        DD gcov[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) gcov[a][b] = DD(G.gcov[a][b]);
+        double u0[3];
+#pragma unroll
+        for (int v = 0; v < 3; ++v) u0[v] = sgn[2 + v] * P.v[2 + v][s];
+        double ub[3] = {0., 0., 0.};
+        for (int q = 0; q < 3; ++q) {
+            DD u[3];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) u[v] = DD(u0[v], (v == q) ? 1. : 0.);
+            inflow_fix<DD>(G, gcov, u, inner);
+            double acc = 0.;
+#pragma unroll
+            for (int v = 0; v < 3; ++v) acc += u[v].d * pb[2 + v];
+            ub[q] = acc;
+        }
+#pragma unroll
+        for (int v = 0; v < 3; ++v) pb[2 + v] = ub[v];
+    }
+#pragma unroll
+    for (int p = 0; p < 5; ++p) atomicAdd(Pbar.v[p] + s, sgn[p] * pb[p]);
 }
 
 // Deterministic sum_f w[f] * F[f] (times scale) added to *out: fixed-size grid of partial sums,
@@ -352,8 +422,14 @@ int adj_supported(const khb_ctx* ctx, const char* who)
     if (ctx->ph.riemann != 0) return set_error(KHB_ERR_UNSUPPORTED, w + ": LLF fluxes only");
     if (ctx->cfg.recon != KHB_RECON_LINEAR_MC && ctx->cfg.recon != KHB_RECON_DONOR_CELL)
         return set_error(KHB_ERR_UNSUPPORTED, w + ": linear MC or donor-cell reconstruction only");
-    for (int f = 0; f < 2 * d.ndim; ++f)
-        if (phys_face(d.bc[f])) return set_error(KHB_ERR_UNSUPPORTED, w + ": periodic or exchange faces only");
+    for (int f = 0; f < 2 * d.ndim; ++f) {
+        if (!phys_face(d.bc[f])) continue;
+        // outflow / reflecting X1 and X2 faces of hydro blocks (their ghost fills, inflow checks and
+        // flux fixes are differentiated); MHD flux-CT polar fixes and transmitting faces are not
+        if (ctx->nv != 5) return set_error(KHB_ERR_UNSUPPORTED, w + ": physical faces on hydro blocks only");
+        if (f >= 4 || (d.bc[f] != KHB_BC_OUTFLOW && d.bc[f] != KHB_BC_REFLECTING))
+            return set_error(KHB_ERR_UNSUPPORTED, w + ": physical faces must be outflow or reflecting X1/X2 faces");
+    }
     return KHB_OK;
 }
 
@@ -374,10 +450,31 @@ khb_fields slice_fields(double* base, long long N, int nv)
     return f;
 }
 
-template <int NV>
-void fold(const Dims& d, const khb_fields& A, cudaStream_t st)
+// The adjoint of launch_boundaries' ghost fills in reverse order (inner x1 again with fix_corner,
+// x2 faces, x1 faces), for a stage input P
+void bc_adjoint(const khb_ctx* ctx, const khb_fields& P, const khb_fields& Pbar, cudaStream_t st)
 {
+    const Dims& d = ctx->d;
+    const int cnt_k = d.ke - d.ks + 1;
+    auto one = [&](int face, int lo_a, int cnt_a) {
+        const int ng = (face < 2) ? d.is : d.js;
+        k_adj_bc<<<blocks_for((long long)ng * cnt_a * cnt_k, 128), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Pbar, face,
+                                                                                 lo_a, cnt_a, d.ks, cnt_k);
+    };
+    if (d.ndim >= 2 && ctx->cfg.fix_corner_inner && phys_face(d.bc[0]) && phys_face(d.bc[3])) one(0, 0, d.n2);
+    if (d.ndim >= 2)
+        for (int face = 3; face >= 2; --face)
+            if (phys_face(d.bc[face])) one(face, 0, d.n1);
+    for (int face = 1; face >= 0; --face)
+        if (phys_face(d.bc[face])) one(face, d.js, d.je - d.js + 1);
+}
+
+template <int NV>
+void fold(const khb_ctx* ctx, const khb_fields& A, cudaStream_t st, const khb_fields* P = nullptr)
+{
+    const Dims& d = ctx->d;
     k_adj_fold<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, A, pmask_of(d));
+    if (P) bc_adjoint(ctx, *P, A, st);
     k_adj_clear_ghosts<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, A);
 }
 
@@ -458,9 +555,9 @@ int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, c
             else adj_flux_dir<3, NV, double>(ctx, Ps, Fb[2], fa, Pbar_s, st);
         }
     }
-    fold<NV>(d, Pbar_s, st);
-    fold<NV>(d, Ubar_s, st);
-    if (Ubar_0.v[0] != Ubar_s.v[0]) fold<NV>(d, Ubar_0, st);
+    fold<NV>(ctx, Pbar_s, st, &Ps);
+    fold<NV>(ctx, Ubar_s, st);
+    if (Ubar_0.v[0] != Ubar_s.v[0]) fold<NV>(ctx, Ubar_0, st);
     KHB_ACUDA(cudaGetLastError());
     ctx->launches += 3 + d.ndim + (clear_out ? 2 * NV : 0) + 2 * (Ubar_0.v[0] != Ubar_s.v[0] ? 3 : 2);
     return KHB_OK;

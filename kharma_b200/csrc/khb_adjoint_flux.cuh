@@ -43,6 +43,10 @@ __global__ void __launch_bounds__(128) k_adj_flux(Dims d, DevGeom g, Phys ph, kh
     if (!box_cell(bx, blockIdx.x, i, j, k)) return;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     const long long st = (DIR == 1) ? 1 : ((DIR == 2) ? d.sj : d.sk);
+    // KBoundaries::FixFlux zero_polar_flux (boundaries.cpp:672-684): these faces carry no flux
+    if (DIR == 2 && ph.zero_polar_flux &&
+        ((j == d.js && phys_face(d.bc[2])) || (j == d.je + 1 && phys_face(d.bc[3]))))
+        return;
     double fb[NV];
     bool any = false;
 #pragma unroll
@@ -84,6 +88,19 @@ __global__ void __launch_bounds__(128) k_adj_flux(Dims d, DevGeom g, Phys ph, kh
     R Uv[2][NV], Fv[2][NV], cmx[2], cmn[2];
     face_side<R, NV, DIR>(gcov, gcon0, gcondd, gdet, gam, Pl, Uv[0], Fv[0], cmx[0], cmn[0]);
     face_side<R, NV, DIR>(gcov, gcon0, gcondd, gdet, gam, Pr, Uv[1], Fv[1], cmx[1], cmn[1]);
+    // KBoundaries::FixFlux inflow checks (boundaries.cpp:611-660): the X1 domain faces' mass flux
+    // clipped to outflow; where the clip acted, the flux no longer depends on the state
+    if (DIR == 1) {
+        const bool in = i == d.is && ph.check_inflow_in && phys_face(d.bc[0]);
+        const bool out = i == d.ie + 1 && ph.check_inflow_out && phys_face(d.bc[1]);
+        if (in || out) {
+            const R cmax = kmax(kmax(R(0), cmx[0]), cmx[1]);
+            const R cmin = -kmin(kmin(R(0), cmn[0]), cmn[1]);
+            const R ctp = kmax(cmax, cmin);
+            const R f0 = R(0.5) * (Fv[0][0] + Fv[1][0] - ctp * (Uv[1][0] - Uv[0][0]));
+            if ((in && f0 > R(0)) || (out && f0 < R(0))) fb[0] = 0.;
+        }
+    }
     // dual geometry
     DR Dgcov[4][4], Dgcon0[4];
 #pragma unroll

@@ -801,6 +801,31 @@ __global__ void k_fixup(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, 
         fixup_zone<NV>(d, g, ph, P, U, pflag, fail_list[t]);
 }
 
+// KBoundaries::check_inflow (boundaries.hpp:101-136) on a ghost zone's u^i (u[0..2]): where the
+// flow enters the domain, the 3-velocity is reset to the normal observer's radial drift and the
+// Lorentz factor rebuilt.  R: double, or Dual<double> for its Jacobian (gcov in R).
+template <typename R>
+__device__ __forceinline__ void inflow_fix(const ZoneGeom& G, const R gcov[4][4], R* u, bool inner)
+{
+    R uvec[3] = {u[0], u[1], u[2]};
+    R gamma = lorentz(gcov, uvec[0], uvec[1], uvec[2]);
+    const double alpha = 1. / sqrt(-G.gcon[0][0]);
+    const R ucon1 = uvec[0] - gamma * R(alpha) * R(G.gcon[0][1]);
+    if (((ucon1 > R(0.)) && inner) || ((ucon1 < R(0.)) && !inner)) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) uvec[v] = uvec[v] / gamma;
+        const double beta1 = G.gcon[0][1] * alpha * alpha;
+        uvec[0] = R(beta1 / alpha);
+        const R vsq = gcov[1][1] * uvec[0] * uvec[0] + gcov[2][2] * uvec[1] * uvec[1] +
+                      gcov[3][3] * uvec[2] * uvec[2] +
+                      R(2.) * (gcov[1][2] * uvec[0] * uvec[1] + gcov[1][3] * uvec[0] * uvec[2] +
+                               gcov[2][3] * uvec[1] * uvec[2]);
+        gamma = R(1.) / dsqrt(R(1.) - vsq);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) u[v] = uvec[v] * gamma;
+    }
+}
+
 // ===================================================================================== boundaries
 // Parthenon's outflow/reflecting functions (unvendored) as KHARMA applies them: fluid primitives
 // and the conserved field; then the inflow check (boundaries.hpp:101-136).  dir = 1 or 2.
@@ -854,23 +879,7 @@ __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int
     if (inflow) {
         ZoneGeom G;
         load_zone_geom(g, j, i, G);
-        double uvec[3] = {Pz[2], Pz[3], Pz[4]};
-        double gamma = lorentz(G.gcov, uvec[0], uvec[1], uvec[2]);
-        const double alpha = 1. / sqrt(-G.gcon[0][0]);
-        const double ucon1 = uvec[0] - gamma * alpha * G.gcon[0][1];
-        if (((ucon1 > 0.) && inner) || ((ucon1 < 0.) && !inner)) {
-#pragma unroll
-            for (int v = 0; v < 3; ++v) uvec[v] /= gamma;
-            const double beta1 = G.gcon[0][1] * alpha * alpha;
-            uvec[0] = beta1 / alpha;
-            const double vsq = G.gcov[1][1] * uvec[0] * uvec[0] + G.gcov[2][2] * uvec[1] * uvec[1] +
-                               G.gcov[3][3] * uvec[2] * uvec[2] +
-                               2. * (G.gcov[1][2] * uvec[0] * uvec[1] + G.gcov[1][3] * uvec[0] * uvec[2] +
-                                     G.gcov[2][3] * uvec[1] * uvec[2]);
-            gamma = 1./sqrt(1. - vsq);
-#pragma unroll
-            for (int v = 0; v < 3; ++v) Pz[2 + v] = uvec[v] * gamma;
-        }
+        inflow_fix<double>(G, G.gcov, Pz + 2, inner);
     }
 #pragma unroll
     for (int p = 0; p < 5; ++p) P.v[p][c] = Pz[p];

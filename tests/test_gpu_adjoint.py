@@ -8,8 +8,9 @@ Checks:
     in FMKS coordinates, the periodic MHD linear-mode box with a functional of the final state);
   * the FP32-flux form's adjoint against the FP64 adjoint;
   * checkpoint spacing does not change the gradient (recompute reproduces the forward states).
-Floors, fixups, FOFC and physical boundaries are outside the differentiated scope; the cases
-below keep every inversion successful (the harness raises otherwise).
+Floors, fixups, FOFC, and physical boundaries of MHD blocks are outside the differentiated scope
+(outflow and reflecting faces of hydro blocks are in it); the cases below keep every inversion
+successful (the harness raises otherwise).
 
 The MC limiter and the LLF speed maxima are piecewise smooth: the adjoint is the derivative of the
 branch each face takes.  Central differences agree with it where a perturbation crosses no branch
@@ -150,6 +151,18 @@ def torus_block_case(precision="fp64"):
 def test_adjoint_bondi_vs_fd():
     b, P0, dts, w = bondi_case()
     check_fd(b, P0, dts, w, None, ndir=64, seed=1)
+
+
+def test_adjoint_bondi_physical_faces_vs_fd():
+    """Outflow X1 faces with inflow checks (the outer face takes inflow: its ghost velocities are
+    reset and its mass flux clipped), reflecting X2 faces with zero polar fluxes and the corner fix,
+    periodic X3: the ghost fills' and flux fixes' adjoints against central differences."""
+    b, P0, dts, w = bondi_case()
+    spec = dataclasses.replace(b.spec, bc=("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"),
+                               check_inflow_inner_x1=True, check_inflow_outer_x1=True, zero_polar_flux=True,
+                               fix_corner_inner=True)
+    bp = Block(spec, geometry=b.geom)
+    check_fd(bp, P0, dts, w, None, ndir=16, seed=3)
 
 
 def test_adjoint_torus_block_mhd_vs_fd():
