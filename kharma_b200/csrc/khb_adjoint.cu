@@ -301,11 +301,12 @@ __global__ void k_adj_clear_ghosts(Dims d, khb_fields A)
     for (int p = 0; p < NV; ++p) A.v[p][t] = 0.;
 }
 
-// Adjoint of one physical face's ghost fill k_bc (hydro): the ghost zone's primitives are its
+// Adjoint of one physical face's ghost fill k_bc: the ghost zone's fluid primitives are its
 // source zone's, the normal velocity inverted on reflecting faces, and on X1 faces with inflow checks
 // the velocity passed through inflow_fix (its Jacobian by three dual evaluations).  Pbar(source) +=
 // J^T Pbar(ghost), then Pbar(ghost) = 0.  Same thread layout and index logic as k_bc.
-__global__ void k_adj_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields Pbar, int face,
+template <int NV>
+__global__ void k_adj_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields Pbar, khb_fields Ubar, int face,
                          int lo_a, int cnt_a, int lo_k, int cnt_k)
 {
     const int bdir = face / 2 + 1;
@@ -327,6 +328,17 @@ __global__ void k_adj_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields Pb
     else           jj = (type == KHB_BC_OUTFLOW) ? ref : offset - j;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     const long long s = ((long long)k*d.n2 + jj)*d.n1 + ii;
+    if (NV > 5) {
+        // k_bc's U_B copy (the normal component inverted on reflecting faces); the ghost B_P = U_B/gdet
+        // of k_ghost_ptou was moved into Ubar by k_adj_ghost_b before these passes
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const double ub = Ubar.v[5 + v][c];
+            Ubar.v[5 + v][c] = 0.;
+            const double fl = ((type == KHB_BC_REFLECTING) && (v == bdir - 1)) ? -1.0 : 1.0;
+            if (ub != 0.) atomicAdd(Ubar.v[5 + v] + s, fl * ub);
+        }
+    }
     double pb[5];
     bool any = false;
 #pragma unroll
@@ -364,6 +376,48 @@ __global__ void k_adj_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields Pb
     }
 #pragma unroll
     for (int p = 0; p < 5; ++p) atomicAdd(Pbar.v[p] + s, sgn[p] * pb[p]);
+}
+
+// The adjoint of k_ghost_ptou's B_P = U_B / gdet on the X1/X2 ghost zones of the interior k range of
+// the physical directions (Ubar_B += Pbar_B / gdet, Pbar_B = 0); same enumeration as k_ghost_ptou
+__global__ void k_adj_ghost_b(Dims d, DevGeom g, khb_fields Pbar, khb_fields Ubar)
+{
+    const unsigned per = plane_ghost_count(d);
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned kk = t / per;
+    if (kk >= (unsigned)(d.ke - d.ks + 1)) return;
+    int j, i;
+    if (!plane_ghost(d, t - kk * per, j, i)) return;
+    const long long c = ((long long)(d.ks + (int)kk)*d.n2 + j)*d.n1 + i;
+    const double gdet = __ldg(g.gdet[3] + (long long)j*g.G1 + i);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const double pb = Pbar.v[5 + v][c];
+        Pbar.v[5 + v][c] = 0.;
+        Ubar.v[5 + v][c] += pb / gdet;
+    }
+}
+
+// The adjoint of B_FluxCT's polar flux fix (k_fix_flux_x2 with fix_polar_flux, b_flux_ct.cpp:372-418):
+// the X1 and X3 B2 fluxes of the ghost row beside the polar face are minus those of the first
+// interior row, so their adjoints move there with a sign and are cleared.  One thread per (k, i).
+__global__ void k_adj_fix_polar(Dims d, double* F1b, double* F3b, int inner)
+{
+    const int ni = d.ie - d.is + 3;
+    const int nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ni*nk) return;
+    const int i = d.is - 1 + t % ni;
+    const int k = (d.ndim > 2) ? d.ks - 1 + t / ni : d.ks;
+    const int j = inner ? d.js : d.je + 1;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i, N = d.N;
+    const long long gh = inner ? c - d.sj : c, in = inner ? c : c - d.sj;     // written row, read row
+    F1b[6*N + in] -= F1b[6*N + gh];
+    F1b[6*N + gh] = 0.;
+    if (d.ndim > 2) {
+        F3b[6*N + in] -= F3b[6*N + gh];
+        F3b[6*N + gh] = 0.;
+    }
 }
 
 // Deterministic sum_f w[f] * F[f] (times scale) added to *out: fixed-size grid of partial sums,
@@ -424,9 +478,8 @@ int adj_supported(const khb_ctx* ctx, const char* who)
         return set_error(KHB_ERR_UNSUPPORTED, w + ": linear MC or donor-cell reconstruction only");
     for (int f = 0; f < 2 * d.ndim; ++f) {
         if (!phys_face(d.bc[f])) continue;
-        // outflow / reflecting X1 and X2 faces of hydro blocks (their ghost fills, inflow checks and
-        // flux fixes are differentiated); MHD flux-CT polar fixes and transmitting faces are not
-        if (ctx->nv != 5) return set_error(KHB_ERR_UNSUPPORTED, w + ": physical faces on hydro blocks only");
+        // outflow / reflecting X1 and X2 faces (their ghost fills, inflow checks and flux fixes,
+        // flux-CT's polar B-flux fix included, are differentiated); transmitting faces are not
         if (f >= 4 || (d.bc[f] != KHB_BC_OUTFLOW && d.bc[f] != KHB_BC_REFLECTING))
             return set_error(KHB_ERR_UNSUPPORTED, w + ": physical faces must be outflow or reflecting X1/X2 faces");
     }
@@ -452,14 +505,20 @@ khb_fields slice_fields(double* base, long long N, int nv)
 
 // The adjoint of launch_boundaries' ghost fills in reverse order (inner x1 again with fix_corner,
 // x2 faces, x1 faces), for a stage input P
-void bc_adjoint(const khb_ctx* ctx, const khb_fields& P, const khb_fields& Pbar, cudaStream_t st)
+template <int NV>
+void bc_adjoint(const khb_ctx* ctx, const khb_fields& P, const khb_fields& Pbar, const khb_fields& Ubar,
+                cudaStream_t st)
 {
     const Dims& d = ctx->d;
     const int cnt_k = d.ke - d.ks + 1;
+    if (NV > 5) {
+        const long long tot = (long long)plane_ghost_count(d) * cnt_k;
+        if (tot) k_adj_ghost_b<<<blocks_for(tot, 128), 128, 0, st>>>(d, ctx->g, Pbar, Ubar);
+    }
     auto one = [&](int face, int lo_a, int cnt_a) {
         const int ng = (face < 2) ? d.is : d.js;
-        k_adj_bc<<<blocks_for((long long)ng * cnt_a * cnt_k, 128), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Pbar, face,
-                                                                                 lo_a, cnt_a, d.ks, cnt_k);
+        k_adj_bc<NV><<<blocks_for((long long)ng * cnt_a * cnt_k, 128), 128, 0, st>>>(d, ctx->g, ctx->ph, P, Pbar, Ubar,
+                                                                                     face, lo_a, cnt_a, d.ks, cnt_k);
     };
     if (d.ndim >= 2 && ctx->cfg.fix_corner_inner && phys_face(d.bc[0]) && phys_face(d.bc[3])) one(0, 0, d.n2);
     if (d.ndim >= 2)
@@ -470,12 +529,27 @@ void bc_adjoint(const khb_ctx* ctx, const khb_fields& P, const khb_fields& Pbar,
 }
 
 template <int NV>
-void fold(const khb_ctx* ctx, const khb_fields& A, cudaStream_t st, const khb_fields* P = nullptr)
+void fold(const khb_ctx* ctx, const khb_fields& A, cudaStream_t st)
 {
     const Dims& d = ctx->d;
     k_adj_fold<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, A, pmask_of(d));
-    if (P) bc_adjoint(ctx, *P, A, st);
     k_adj_clear_ghosts<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, A);
+}
+
+// The stage input's ghost adjoints: periodic images first, then (physical faces) the ghost fills'
+// transposes, which move Pbar (and for MHD the ghost B into Ubar) to the source zones, then cleared
+template <int NV>
+void fold_input(const khb_ctx* ctx, const khb_fields& P, const khb_fields& Pbar, const khb_fields& Ubar,
+                cudaStream_t st)
+{
+    const Dims& d = ctx->d;
+    k_adj_fold<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, Pbar, pmask_of(d));
+    k_adj_fold<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, Ubar, pmask_of(d));
+    bool physical = false;
+    for (int f = 0; f < 2 * d.ndim; ++f) physical |= phys_face(d.bc[f]);
+    if (physical) bc_adjoint<NV>(ctx, P, Pbar, Ubar, st);
+    k_adj_clear_ghosts<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, Pbar);
+    k_adj_clear_ghosts<NV><<<blocks_for(d.N, 256), 256, 0, st>>>(d, Ubar);
 }
 
 // what k_adj_flux needs to form the hydro flux adjoints: Ubar_upd, bdt/vol, the objective's seed
@@ -543,6 +617,12 @@ int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, c
     const double bdt = kRkBeta[s] * dt;
     k_adj_update<NV><<<box_blocks(zb), 128, 0, st>>>(d, ctx->g, ctx->ph, Uupd, Ps, kRkGam0[s], kRkGam1[s],
                                                      bdt, Fb[0], Fb[1], Fb[2], Pbar_s, Ubar_s, Ubar_0, zb);
+    if (NV > 5 && d.ndim >= 2 && ctx->ph.fix_polar_flux)
+        for (int face = 2; face <= 3; ++face) {
+            if (!phys_face(d.bc[face])) continue;
+            const int ni = d.ie - d.is + 3, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+            k_adj_fix_polar<<<blocks_for((long long)ni * nk, 128), 128, 0, st>>>(d, Fb[0], Fb[2], face == 2);
+        }
     const FluxAdj fa{Uupd, bdt / (ctx->ph.dx1 * ctx->ph.dx2 * ctx->ph.dx3), weight, wscale};
     for (int dir = 1; dir <= d.ndim; ++dir) {
         if (ctx->fp32) {
@@ -555,8 +635,7 @@ int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, c
             else adj_flux_dir<3, NV, double>(ctx, Ps, Fb[2], fa, Pbar_s, st);
         }
     }
-    fold<NV>(ctx, Pbar_s, st, &Ps);
-    fold<NV>(ctx, Ubar_s, st);
+    fold_input<NV>(ctx, Ps, Pbar_s, Ubar_s, st);
     if (Ubar_0.v[0] != Ubar_s.v[0]) fold<NV>(ctx, Ubar_0, st);
     KHB_ACUDA(cudaGetLastError());
     ctx->launches += 3 + d.ndim + (clear_out ? 2 * NV : 0) + 2 * (Ubar_0.v[0] != Ubar_s.v[0] ? 3 : 2);

@@ -47,6 +47,9 @@ __global__ void __launch_bounds__(128) k_adj_flux(Dims d, DevGeom g, Phys ph, kh
     if (DIR == 2 && ph.zero_polar_flux &&
         ((j == d.js && phys_face(d.bc[2])) || (j == d.je + 1 && phys_face(d.bc[3]))))
         return;
+    // B_FluxCT's polar fix zeroes the X2 B1 and B3 fluxes on the polar faces
+    const bool polar_b = NV > 5 && DIR == 2 && ph.fix_polar_flux &&
+                         ((j == d.js && phys_face(d.bc[2])) || (j == d.je + 1 && phys_face(d.bc[3])));
     double fb[NV];
     bool any = false;
 #pragma unroll
@@ -56,7 +59,10 @@ __global__ void __launch_bounds__(128) k_adj_flux(Dims d, DevGeom g, Phys ph, kh
         any |= fb[p] != 0.;
     }
 #pragma unroll
-    for (int p = 5; p < NV; ++p) { fb[p] = Fbar[p*d.N + c]; any |= fb[p] != 0.; }
+    for (int p = 5; p < NV; ++p) {
+        fb[p] = (polar_b && p != 6) ? 0. : Fbar[p*d.N + c];
+        any |= fb[p] != 0.;
+    }
     if (!any) return;
     typedef Dual<R> DR;
     const int loc = DIR - 1;

@@ -208,6 +208,48 @@ def test_adjoint_cartesian_exchange_mhd_vs_fd():
     check_fd(b, P0, dts, None, Pw, ndir=8, seed=5)
 
 
+def test_adjoint_cartesian_physical_faces_mhd_vs_fd():
+    """Minkowski MHD block with outflow X1 faces (inflow checks), reflecting X2 faces (zero polar
+    fluxes, the corner fix) and periodic X3: the ghost fills of P and of U_B (the ghost B_P = U_B/gdet)
+    and the flux fixes, against central differences of a final-state objective (donor-cell faces)."""
+    spec = dataclasses.replace(mhdmodes_spec(12, 12, 8, recon="donor_cell"),
+                               bc=("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"),
+                               check_inflow_inner_x1=True, check_inflow_outer_x1=True, zero_polar_flux=True,
+                               fix_corner_inner=True)
+    b = Block(spec)
+    P0 = torch.as_tensor(ramps(spec, problems.mhdmodes(spec, 3, amp=1e-2)), device="cuda")
+    rng = np.random.Generator(np.random.PCG64(9))
+    Pw = np.zeros(tuple(P0.shape))
+    sl = (slice(None),) + spec.interior
+    Pw[sl] = rng.standard_normal(Pw[sl].shape)
+    Pw = torch.as_tensor(Pw, device="cuda")
+    dts = [stable_dt(b, P0)] * 6
+    check_fd(b, P0, dts, None, Pw, ndir=8, seed=6)
+
+
+def test_adjoint_polar_mhd_vs_fd():
+    """A magnetized FMKS block on the pole (reflecting X2 faces with B_FluxCT's polar B-flux fix and
+    zero polar fluxes, outflow X1 faces with inflow checks, floors off; a ramped magnetized gas),
+    final-state objective."""
+    full = torus_spec(128, 128, 64)
+    spec = dataclasses.replace(full, nx1=12, nx2=8, nx3=8, x1min=math.log(13.0), x1max=math.log(18.0),
+                               x2min=0.0, x2max=0.1, x3min=0.0, x3max=math.pi / 4, floors_on=False,
+                               recon="donor_cell")
+    geom = build_geometry(spec)
+    # a gas at rest with a radial field, ramped in every variable (the torus itself is atmosphere here)
+    P = np.zeros((8,) + spec.shape)
+    P[0], P[1], P[5] = 1.0, 0.1, 0.05
+    P0 = torch.as_tensor(ramps(spec, P), device="cuda")
+    b = Block(spec, geometry=geom)
+    rng = np.random.Generator(np.random.PCG64(10))
+    Pw = np.zeros(tuple(P0.shape))
+    sl = (slice(None),) + spec.interior
+    Pw[sl] = rng.standard_normal(Pw[sl].shape)
+    Pw = torch.as_tensor(Pw, device="cuda")
+    dts = [stable_dt(Block(spec, geometry=geom), P0)] * 4
+    check_fd(b, P0, dts, None, Pw, ndir=8, seed=7, tol=1e-4)
+
+
 def test_adjoint_donor_cell_vs_fd():
     b, P0, dts, w = bondi_case()
     spec = dataclasses.replace(b.spec, recon="donor_cell")
