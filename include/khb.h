@@ -313,10 +313,13 @@ int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32
  * weights of dx2 dx3 on one x1 face layer, the RK2-consistent mass through that layer in the step).
  * The intermediate stage is recomputed from (P_n, U_n) into the context's stage scratch; the
  * inversion is differentiated by the implicit-function theorem at the converged state; periodic
- * ghost-zone adjoints are folded into their images, exchange ghost zones are constants.  Supported:
- * LLF fluxes with linear MC or donor-cell reconstruction, periodic or exchange faces, floors,
- * recon floors and FOFC off (KHB_ERR_UNSUPPORTED otherwise).  Ghost zones of Pbar/Ubar are zero on
- * return.  Scratch (6 nv N doubles, 2 N flags) is allocated on the first call. */
+ * ghost-zone adjoints are folded into their images, exchange ghost zones are constants, and the
+ * ghost fills of outflow/reflecting X1/X2 faces (inflow checks, the corner fix, the ghost B of MHD
+ * blocks) and the flux fixes (the X1 mass-flux clip, zero polar fluxes, B_FluxCT's polar B-flux fix,
+ * boundaries.cpp:369-690, b_flux_ct.cpp:372-418) are transposed.  Supported: LLF fluxes with linear MC
+ * or donor-cell reconstruction, periodic, exchange, outflow or reflecting faces, floors, recon floors
+ * and FOFC off (KHB_ERR_UNSUPPORTED otherwise).  Ghost zones of Pbar/Ubar are zero on return.
+ * Scratch (6 nv N doubles, 2 N flags) is allocated on the first call. */
 int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_fields* U_n,
                      const khb_fields* P_np1, const khb_fields* Pbar, const khb_fields* Ubar,
                      const double* rho_flux1_weight, double weight_scale, void* stream);
