@@ -160,6 +160,8 @@ TORI = {
     "torus3d_mc_gs05_c": lambda: dataclasses.replace(torus_spec(24, 16, 8), b_ct="gs05_c"),
     "torus3d_mc_bs99": lambda: dataclasses.replace(torus_spec(24, 16, 8), b_ct="bs99"),
     "torus3d_weno5_gs05_0": lambda: dataclasses.replace(torus_spec(24, 16, 8, recon="weno5"), b_ct="gs05_0"),
+    # the reference's default inverter
+    "torus3d_mc_kastaun_gs05_c": lambda: dataclasses.replace(torus_spec(24, 16, 8, inverter="kastaun"), b_ct="gs05_c"),
     # transmitting poles (average_EMF, the face field's transmitted ghost rows): MKS over all of x3
     "torus3d_mks_transmitting_gs05_c": lambda: dataclasses.replace(
         torus_spec(24, 16, 16), transform="mks", b_ct="gs05_c",
