@@ -176,6 +176,10 @@ class Block:
         _lib.check(self.lib.khb_apply_floors(self.ctx, Fields(P).ref, Fields(U).ref, C.c_void_p(pflag.data_ptr()),
                                              C.c_void_p(fflag.data_ptr()), self.stream), "khb_apply_floors")
 
+    def fix_utop(self, P, U, pflag):
+        _lib.check(self.lib.khb_fix_utop(self.ctx, Fields(P).ref, Fields(U).ref, C.c_void_p(pflag.data_ptr()),
+                                         self.stream), "khb_fix_utop")
+
 
 class Driver:
     """Step loop with the reference's timestep schedule.

@@ -1823,6 +1823,30 @@ static void fofc_correct(const Block& B, Fields& f, int s, double dt, const doub
     }
 }
 
+// FixUtoP as a stage runs it (inverter.hpp:83-89, fixup.cpp:47-156) over the physical range: periodic
+// ghosts of P and pflag are filled first so that they serve as neighbours, and across exchange faces
+// the neighbour's values in the ghost zones are valid neighbours (their flags are the caller's; zero
+// unless it exchanges them)
+static void stage_fix_utop(const Block& B, double* P_n, double* U_n, double* pflag)
+{
+    int ks = B.ks, ke = B.ke, js = B.js, je = B.je, is = B.is, ie = B.ie;
+    for (int d = 1; d <= B.ndim; ++d)
+        if (B.c.bc[2*(d-1)] == BC_PERIODIC) {
+            periodic_fill(B, P_n, 5, d);
+            periodic_fill(B, pflag, 1, d);
+            if (d == 1) { is = 0; ie = B.n1 - 1; }
+            if (d == 2) { js = 0; je = B.n2 - 1; }
+            if (d == 3) { ks = 0; ke = B.n3 - 1; }
+        }
+    if (B.c.bc[0] == BC_EXCHANGE) is = 0;
+    if (B.c.bc[1] == BC_EXCHANGE) ie = B.n1 - 1;
+    if (B.ndim > 1 && B.c.bc[2] == BC_EXCHANGE) js = 0;
+    if (B.ndim > 1 && B.c.bc[3] == BC_EXCHANGE) je = B.n2 - 1;
+    if (B.ndim > 2 && B.c.bc[4] == BC_EXCHANGE) ks = 0;
+    if (B.ndim > 2 && B.c.bc[5] == BC_EXCHANGE) ke = B.n3 - 1;
+    fix_utop(B, P_n, U_n, pflag, ks, ke, js, je, is, ie);
+}
+
 // One stage.  P_s/U_s: stage-start state; U_0: step-start conserved state; outputs P_n/U_n.
 static void stage(const Block& B, Fields& f, int s, double dt,
                   const double* P_s, const double* U_s, const double* U_0,
@@ -1860,27 +1884,8 @@ static void stage(const Block& B, Fields& f, int s, double dt,
     for (size_t x = 0; x < N; ++x) { pflag[x] = 0; fflag[x] = 0; }
     block_utop(B, U_n, P_n, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
     if (B.c.floors_on) apply_grmhd_floors(B, P_n, U_n, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
-    // 9. FixUtoP over the physical range: periodic ghosts of P and pflag are needed as neighbours
-    {
-        int ks = B.ks, ke = B.ke, js = B.js, je = B.je, is = B.is, ie = B.ie;
-        for (int d = 1; d <= B.ndim; ++d)
-            if (B.c.bc[2*(d-1)] == BC_PERIODIC) {
-                periodic_fill(B, P_n, 5, d);
-                periodic_fill(B, pflag, 1, d);
-                if (d == 1) { is = 0; ie = B.n1 - 1; }
-                if (d == 2) { js = 0; je = B.n2 - 1; }
-                if (d == 3) { ks = 0; ke = B.n3 - 1; }
-            }
-        // exchange faces: the neighbour's values in the ghost zones are valid neighbours (their
-        // flags are the caller's; zero unless it exchanges them)
-        if (B.c.bc[0] == BC_EXCHANGE) is = 0;
-        if (B.c.bc[1] == BC_EXCHANGE) ie = B.n1 - 1;
-        if (B.ndim > 1 && B.c.bc[2] == BC_EXCHANGE) js = 0;
-        if (B.ndim > 1 && B.c.bc[3] == BC_EXCHANGE) je = B.n2 - 1;
-        if (B.ndim > 2 && B.c.bc[4] == BC_EXCHANGE) ks = 0;
-        if (B.ndim > 2 && B.c.bc[5] == BC_EXCHANGE) ke = B.n3 - 1;
-        fix_utop(B, P_n, U_n, pflag, ks, ke, js, je, is, ie);
-    }
+    // 9. FixUtoP over the physical range
+    stage_fix_utop(B, P_n, U_n, pflag);
     // 10-11. boundaries, then U = U(P) over the entire block
     finish_stage(B, P_n, U_n);
 }
@@ -2229,24 +2234,7 @@ static void ct_stage(const Block& B, Fields& f, int s, double dt, const double* 
         for (int v = 0; v < 3; ++v) P_n[(size_t)(5 + v)*N + B.id(k, j, i)] = Bp[v];
     }
     if (B.c.floors_on) apply_grmhd_floors(B, P_n, U_n, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
-    {
-        int ks = B.ks, ke = B.ke, js = B.js, je = B.je, is = B.is, ie = B.ie;
-        for (int d = 1; d <= B.ndim; ++d)
-            if (B.c.bc[2*(d-1)] == BC_PERIODIC) {
-                periodic_fill(B, P_n, 5, d);
-                periodic_fill(B, pflag, 1, d);
-                if (d == 1) { is = 0; ie = B.n1 - 1; }
-                if (d == 2) { js = 0; je = B.n2 - 1; }
-                if (d == 3) { ks = 0; ke = B.n3 - 1; }
-            }
-        if (B.c.bc[0] == BC_EXCHANGE) is = 0;
-        if (B.c.bc[1] == BC_EXCHANGE) ie = B.n1 - 1;
-        if (B.ndim > 1 && B.c.bc[2] == BC_EXCHANGE) js = 0;
-        if (B.ndim > 1 && B.c.bc[3] == BC_EXCHANGE) je = B.n2 - 1;
-        if (B.ndim > 2 && B.c.bc[4] == BC_EXCHANGE) ks = 0;
-        if (B.ndim > 2 && B.c.bc[5] == BC_EXCHANGE) ke = B.n3 - 1;
-        fix_utop(B, P_n, U_n, pflag, ks, ke, js, je, is, ie);
-    }
+    stage_fix_utop(B, P_n, U_n, pflag);
     if (!ct_has_physical(B)) { finish_stage(B, P_n, U_n); return; }
     ct_apply_boundaries(B, P_n, U_n, Bn);
 #pragma omp parallel for collapse(2) schedule(static)
@@ -3259,6 +3247,12 @@ void orc_utop(void* hp, const double* U, double* P, double* pflag, double* fflag
     block_utop(B, U, P, pflag, fflag, B.ks, B.ke, B.js, B.je, B.is, B.ie);
 }
 // Floors::ApplyGRMHDFloors over the interior
+// Inverter::MeshFixUtoP on a block after its inversion and floors (P, U, pflag as the stage leaves them)
+void orc_fix_utop(void* hp, double* P, double* U, double* pflag)
+{
+    const Block& B = ((Handle*)hp)->B;
+    stage_fix_utop(B, P, U, pflag);
+}
 void orc_floors(void* hp, double* P, double* U, double* pflag, double* fflag)
 {
     const Block& B = ((Handle*)hp)->B;

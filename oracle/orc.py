@@ -87,6 +87,7 @@ def load():
     lib.orc_fix_flux.argtypes = [P, P, P, P]
     lib.orc_utop.argtypes = [P, P, P, P, P]
     lib.orc_floors.argtypes = [P, P, P, P, P]
+    lib.orc_fix_utop.argtypes = [P, P, P, P]
     lib.orc_ptou.argtypes = [P, P, P]
     lib.orc_boundaries.argtypes = [P, P, P]
     lib.orc_step.argtypes = [P, P, P, P, P, C.c_double, P, P]
@@ -240,6 +241,10 @@ class Oracle:
 
     def floors(self, P, U, pflag, fflag):
         self.lib.orc_floors(self.h, _ptr(P), _ptr(U), _ptr(pflag), _ptr(fflag))
+
+    def fix_utop(self, P, U, pflag):
+        """FixUtoP in place as a stage runs it (periodic images of P and pflag filled first)."""
+        self.lib.orc_fix_utop(self.h, _ptr(P), _ptr(U), _ptr(pflag))
 
     def step(self, P, U, dt):
         """One RK2 step in place; returns (pflag, fflag, dt_next, min_ndt)."""
