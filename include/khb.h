@@ -404,16 +404,19 @@ int khb_step_host_interior(khb_ctx* ctx, double* const* P_host, const khb_fields
  * Synchronizes the stream. */
 int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void* stream);
 
-/* No counterpart in the reference.  For callers that cannot allocate device memory (a step
- * recorded into a CUDA graph, a framework that hands out memory only from its own pool, or a
- * diagnostic hook holding only the field pointers and no context): the same maximum as
- * khb_max_divb, computed without a context and without any allocation.  The per-block partial
+/* No counterpart in the reference.  For callers that cannot allocate device memory (a framework
+ * that hands out device memory only from its own pre-reserved pool, or a diagnostic hook holding
+ * only the field pointers and no context, since creating a context allocates its scratch): the
+ * same maximum as khb_max_divb, computed without a context and without any allocation (0 for
+ * blocks without B, nvar < 8, and for 1D blocks, as khb_max_divb returns).  The per-block partial
  * maxima live in a file-scope __device__ array of 16384 doubles (128 KiB, held by every GPU that
  * loads the library until exit), so blocks with more than 256 * 16384 corners are rejected with
- * KHB_ERR_ARG.  The result is written asynchronously to *max_divb_out (device memory); nothing is
- * synchronized.  The first call on a device looks the array's address up (cudaGetSymbolAddress)
- * with that device current -- make it before any stream capture.  Calls that overlap on the GPU
- * share the array and race; serialize them.  Errors: khb_noalloc_last_error(). */
+ * KHB_ERR_ARG.  The result is written asynchronously to *max_divb_out (device memory); the host
+ * does not wait for the stream.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress) with that device current and keeps it for the life of the process: make
+ * that first call before any stream capture begins, and do not call this again on a device after
+ * cudaDeviceReset (the kept address belongs to the destroyed context).  Calls that overlap on the
+ * GPU share the array and race; serialize them.  Errors: khb_noalloc_last_error(). */
 int khb_max_divb_noalloc(const khb_config* cfg, const khb_fields* U, double* max_divb_out, void* stream);
 const char* khb_noalloc_last_error(void);
 

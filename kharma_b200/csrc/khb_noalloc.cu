@@ -1,20 +1,21 @@
 // khb_noalloc.cu -- khb_max_divb_noalloc: the divB diagnostic for callers that cannot allocate.
 //
-// Some callers cannot call cudaMalloc: a step being recorded into a CUDA graph (an allocation
-// would synchronize the device and is not capturable), a host framework that hands out device
-// memory only from its own pre-reserved pool, or a diagnostic hook that holds only the field
-// pointers and no khb_ctx (creating a context allocates its scratch).  This entry point needs
-// no context and allocates nothing.  Its scratch -- one partial maximum per thread block -- is a
-// file-scope __device__ array of KHB_NOALLOC_MAX_PARTIALS doubles (128 KiB) that every GPU which
-// loads the library holds until the process exits.  Blocks with more corners than
+// Some callers cannot call cudaMalloc: a host framework that hands out device memory only from
+// its own pre-reserved pool, or a diagnostic hook that holds only the field pointers and no
+// khb_ctx (creating a context allocates its scratch).  This entry point needs no context and
+// allocates nothing.  Its scratch -- one partial maximum per thread block -- is a file-scope
+// __device__ array of KHB_NOALLOC_MAX_PARTIALS doubles (128 KiB) that every GPU which loads the
+// library holds until the process exits.  Blocks with more corners than
 // 256 * KHB_NOALLOC_MAX_PARTIALS are rejected.
 //
 // Host code may not pass the array's name to a kernel: on the host it is only a stand-in, not a
 // device address.  The first call on each device therefore looks the address up with
-// cudaGetSymbolAddress while that device is current; make that first call before any stream
-// capture begins.  All calls share the one array and it keeps the last call's contents: every
-// partial the reduction reads is written by the same call, so nothing needs clearing, but calls
-// that overlap on the GPU (concurrent streams, or several host threads) race on it.
+// cudaGetSymbolAddress while that device is current, and keeps it for the life of the process
+// (so that first call belongs before any stream capture, and a cudaDeviceReset, which unloads the
+// module, ends its validity).  All calls share the one array and it keeps the last call's
+// contents: every partial the reduction reads is written by the same call, so nothing needs
+// clearing, but calls that overlap on the GPU (concurrent streams, or several host threads) race
+// on it.
 #include "khb_kernels.cuh"
 
 #include <mutex>
@@ -66,16 +67,15 @@ extern "C" int khb_max_divb_noalloc(const khb_config* cfg, const khb_fields* U, 
     const char* why = nullptr;
     int rc = khb::derive_block(cfg, d, ph, &why);
     if (rc) return noalloc_fail(rc, why);
-    if (cfg->nvar < 8) return noalloc_fail(KHB_ERR_ARG, "khb_max_divb_noalloc: needs the B field (nvar = 8)");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cfg->nvar < 8 || d.ndim < 2) {
+        // no field, or no corners: 0, as khb_max_divb returns.  All-zero bytes are +0.0; the
+        // memset is stream-ordered and the host does not wait for it.
+        const cudaError_t e = cudaMemsetAsync(max_divb_out, 0, sizeof(double), st);
+        return e == cudaSuccess ? KHB_OK : noalloc_fail(KHB_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    }
     for (int v = 5; v < 8; ++v)
         if (!U->v[v]) return noalloc_fail(KHB_ERR_ARG, "khb_max_divb_noalloc: NULL B_U pointer");
-    cudaStream_t st = (cudaStream_t)stream;
-    if (d.ndim < 2) {
-        const double zero = 0.;
-        cudaError_t e = cudaMemcpyAsync(max_divb_out, &zero, sizeof(double), cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // the host source is on this stack frame
-        return e == cudaSuccess ? KHB_OK : noalloc_fail(KHB_ERR_CUDA, cudaGetErrorString(e));
-    }
     // same corner range as khb_max_divb (b_flux_ct.cpp:554-564)
     const int avoid_in = khb::phys_face(d.bc[0]), avoid_out = khb::phys_face(d.bc[1]);
     const int i_lo = d.is + avoid_in, i_hi = d.ie + !avoid_out;

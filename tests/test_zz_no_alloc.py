@@ -1,11 +1,13 @@
 """khb_max_divb_noalloc: the divB diagnostic for callers that cannot allocate device memory.
 
-Callers inside a CUDA-graph capture, callers whose device memory comes only from their own
-framework's pool, and diagnostic hooks that hold field pointers but no khb_ctx cannot use
-khb_max_divb (it needs a context, and creating one allocates).  The no-allocation variant keeps
-its per-block partial maxima in a static device array; this test checks, through the C ABI, that
-two calls in a row return what the context-based entry point returns.  It lives in its own file so
-that a run stopping at the first failure has already run every other test.
+Callers whose device memory comes only from their own framework's pre-reserved pool, and diagnostic
+hooks that hold field pointers but no khb_ctx, cannot use khb_max_divb (it needs a context, and
+creating one allocates).  The no-allocation variant keeps its per-block partial maxima in a static
+device array; these tests check, through the C ABI, that two calls in a row return what the
+context-based entry point returns (relative 1e-12), that both equal the oracle's maximum on a field
+with O(1) divergence, and that blocks without a field or without corners give 0 as khb_max_divb does.
+The file is collected last, so that a run stopping at the first failure has already run every
+other test.
 """
 import ctypes as C
 
@@ -15,7 +17,7 @@ import torch
 
 from kharma_b200 import _lib, problems
 from kharma_b200.block import Block
-from kharma_b200.spec import mhdmodes_spec, torus_spec
+from kharma_b200.spec import bondi_spec, mhdmodes_spec, torus_spec
 
 pytestmark = pytest.mark.gpu
 
@@ -52,6 +54,32 @@ def test_noalloc_divb_matches_context_version(spec):
         assert abs(got - ref) <= RTOL * max(abs(ref), 1e-300), f"call {call}: {got} vs {ref}"
         # move the state on so the second call sees different data
         b.step(dt)
+
+
+@pytest.mark.parametrize("spec", [mhdmodes_spec(24, 20, 16), torus_spec(32, 24, 8)], ids=["cart3d", "torus3d"])
+def test_noalloc_divb_matches_oracle(oracle_mod, spec):
+    o = oracle_mod.Oracle(spec)
+    b = Block(spec, geometry=o.geometry())
+    rng = np.random.default_rng(5)
+    phys = lambda bc: bc in ("outflow", "reflecting", "transmitting")
+    out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    for call in range(2):
+        U = np.zeros((spec.nvar,) + spec.shape)
+        U[5:8] = rng.uniform(-1.0, 1.0, size=(3,) + spec.shape)
+        b.U.copy_(torch.from_numpy(U))
+        ref = o.max_divb(U, avoid_inner=phys(spec.bc[0]), avoid_outer=phys(spec.bc[1]))
+        got = noalloc_divb(b, out)
+        assert ref > 1.0
+        assert abs(got - ref) <= RTOL * ref, f"call {call}: {got} vs {ref}"
+
+
+@pytest.mark.parametrize("spec", [mhdmodes_spec(32, 1, 1), bondi_spec(16, 8, 8, 3.0, 30.0)], ids=["1d", "hydro"])
+def test_noalloc_divb_zero_without_corners_or_field(spec):
+    """A 1D block has no corners and a hydro block (nvar = 5) no field: 0, as khb_max_divb gives."""
+    b = Block(spec)
+    out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    assert noalloc_divb(b, out) == 0.0
+    assert b.max_divb() == 0.0
 
 
 def test_noalloc_rejects_oversized_block():
