@@ -75,6 +75,32 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def detail(name, obj):
+    """A bulky secondary measurement on its own stdout line, ahead of the final JSON line."""
+    print(f"detail {name}: " + json.dumps(obj), flush=True)
+
+
+def profile_traffic(kernel, size, form):
+    """DRAM bytes per launch of `kernel` (dram__bytes_read.sum + dram__bytes_write.sum) from the
+    committed ncu summary of this workload, which states it on a line
+    `traffic_per_launch_bytes: <kernel> <form> <n1>x<n2>x<n3> <bytes>`; None when no summary covers it."""
+    want = (kernel, form, "x".join(str(x) for x in size))
+    pdir = os.path.join(ROOT, "profiles")
+    try:
+        names = sorted(os.listdir(pdir))
+    except OSError:
+        return None, None
+    for name in names:
+        if not name.endswith(".md"):
+            continue
+        with open(os.path.join(pdir, name)) as f:
+            for ln in f:
+                t = ln.strip().strip("`").split()
+                if len(t) == 5 and t[0] == "traffic_per_launch_bytes:" and tuple(t[1:4]) == want:
+                    return float(t[4]), "profiles/" + name
+    return None, None
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -89,7 +115,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -135,54 +161,92 @@ def make_state(spec):
 
 
 # ----------------------------------------------------------------------------------- CPU side
-def cpu_sample(n1, n2, n3_sample, steps, warm=1):
-    """Oracle (all host threads) on a k-slab of the torus; returns zone-cycles/s and details."""
+def _oracle_block(n1, n2, n3):
+    """The oracle (the CPU restatement of the reference hot path) on the benchmark block."""
+    # the OpenMP runtime reads OMP_PROC_BIND when the oracle library is first loaded
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    from kharma_b200 import problems
     from kharma_b200.spec import torus_spec
     from oracle import orc
-    spec = torus_spec(n1, n2, n3_sample)
+    spec = torus_spec(n1, n2, n3)
     o = orc.Oracle(spec)
-    from kharma_b200 import problems
     P, U = o.init_state(problems.fm_torus(spec, o.geometry(), seed=1234))
+    return orc, o, spec, P, U
+
+
+def _host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def cpu_baseline_block(n1, n2, n3, runs=5):
+    """The oracle on the same n1 x n2 x n3 block as the GPU arm: one warm-up step, then `runs` RK2
+    steps timed one by one on all host threads (median reported), then one step on one thread."""
+    orc, o, spec, P, U = _oracle_block(n1, n2, n3)
+    threads = orc.set_threads(0)
     dt = spec.dt_min
-    for _ in range(warm):
+    _, _, dt, _ = o.step(P, U, dt)
+    per = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
         _, _, dt, _ = o.step(P, U, dt)
+        per.append(time.perf_counter() - t0)
+    zones = n1 * n2 * n3
+    med = statistics.median(per)
+    orc.set_threads(1)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        _, _, dt, _ = o.step(P, U, dt)
-    el = time.perf_counter() - t0
-    zones = n1 * n2 * n3_sample
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return zones * steps / el, threads, el
+    o.step(P, U, dt)
+    one = time.perf_counter() - t0
+    orc.set_threads(threads)
+    return {"value": zones / med, "unit": UNIT, "cores": threads, "kind": "port",
+            "single_thread_value": zones / one,
+            "sample": f"oracle port, same {n1}x{n2}x{n3} block, {threads} threads ({_cpu_model()}): median of {runs} "
+                      f"RK2 steps after 1 warm-up ({min(per):.2f}-{max(per):.2f} s); 1 thread: {one:.2f} s/step"}
 
 
 def reference_arm(args, rank, world):
+    """The reference's algorithm on the host cores: the oracle port (kharma.host cannot be built), on
+    the GPU arm's block and metric, all host threads, W warm-up steps then K timed RK2 steps."""
     if rank != 0:
         return
     n1, n2, n3 = [int(x) for x in args.size.split(",")]
-    n3s = max(8, n3 // 4)
-    from kharma_b200.spec import torus_spec
-    from oracle import orc
-    from kharma_b200 import problems
-    spec = torus_spec(n1, n2, n3s)
-    o = orc.Oracle(spec)
-    P, U = o.init_state(problems.fm_torus(spec, o.geometry(), seed=1234))
+    orc, o, spec, P, U = _oracle_block(n1, n2, n3)
+    threads = orc.set_threads(0)
     dt = spec.dt_min
     for _ in range(args.warmup):
         _, _, dt, _ = o.step(P, U, dt)
-    t0 = time.perf_counter()
+    per = []
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         _, _, dt, _ = o.step(P, U, dt)
-    el = time.perf_counter() - t0
-    v = n1 * n2 * n3s * args.steps / el
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = (f"oracle port of the reference hot path, {threads} OpenMP threads, {n1}x{n2}x{n3s} slab of the "
-              f"{n1}x{n2}x{n3} torus (same per-zone work), {args.steps} RK2 steps after {args.warmup} warm-up")
+        per.append(time.perf_counter() - t0)
+    el = sum(per)
+    zones = n1 * n2 * n3
+    v = zones * args.steps / el
+    sample = (f"oracle port of the reference hot path, {threads} OpenMP threads ({_cpu_model()}), the same "
+              f"{n1}x{n2}x{n3} block, {args.steps} RK2 steps after {args.warmup} warm-up; median step "
+              f"{statistics.median(per):.3f} s")
     out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic", "config": {"workload": f"FM torus FMKS {n1}x{n2}x{n3} (slab sample)",
-                                            "recon": "linear_mc", "flux": "llf", "b_field": "flux_ct"},
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+           "data": "synthetic", "config": {"workload": f"FM torus FMKS {n1}x{n2}x{n3} one meshblock",
+                                            "recon": "linear_mc", "flux": "llf", "b_field": "flux_ct",
+                                            "inverter": "onedw", "floors": "drift"},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                            "median_step_value": zones / statistics.median(per)},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -266,8 +330,8 @@ def emhd_newton(n=128, reps=3):
     fail = sol.scalar_field()
     scale = float(Ud[:, k, j, i].abs().max()) / dt
 
-    def solve(jac, rel):
-        sol.set_implicit(ImplicitSpec(min_nonlinear_iter=1, max_nonlinear_iter=16, rootfind_tol=rel * scale,
+    def solve(jac, rel, max_iter=16):
+        sol.set_implicit(ImplicitSpec(min_nonlinear_iter=1, max_nonlinear_iter=max_iter, rootfind_tol=rel * scale,
                                       jacobian=jac))
         times = []
         for r in range(reps + 1):
@@ -293,9 +357,30 @@ def emhd_newton(n=128, reps=3):
     for jac in ("fd", "exact"):
         out[jac] = solve(jac, 1e-10)
     out["exact_vs_fd_wall_time"] = out["fd"]["ms_per_solve"] / out["exact"]["ms_per_solve"]
-    # a tighter tolerance, where the forward-difference Jacobian's error starts to cost iterations
-    out["tolerance_1e-12"] = {jac: solve(jac, 1e-12) for jac in ("fd", "exact")}
+    # iterations and time to tolerance over a sweep of relative tolerances (max residual norm over
+    # max|U|/dt), and at the reference's own convention: an absolute rootfind_tol of 1e-12 on the
+    # zone's residual L2 norm (implicit.cpp:101, 502-554)
+    sweep = {}
+    for rel in (1e-8, 1e-9, 1e-10, 1e-11, 1e-12, 1e-13):
+        sweep["%.0e" % rel] = {jac: solve(jac, rel) for jac in ("fd", "exact")}
+    # the reference's defaults: at most 3 iterations to an absolute 1e-12, which lies below this state's
+    # round-off floor of the residual, so both forms stop at 3: compared is the residual they reach
+    sweep["abs_1e-12_max3"] = {jac: solve(jac, 1e-12 / scale, max_iter=3) for jac in ("fd", "exact")}
+    out["sweep"] = {k: {jac: {"iterations": v[jac]["iterations"], "ms_per_solve": round(v[jac]["ms_per_solve"], 3),
+                              "final_max_norm": v[jac]["max_norm_per_iteration"][-1],
+                              "failed_zones": v[jac]["failed_zones"]} for jac in v} for k, v in sweep.items()}
     return out
+
+
+def emhd_summary(e):
+    """The implicit-solve figures the final line carries: iterations and ms per solve to 1e-10 (relative)
+    and over the tolerance sweep, forward-difference vs exact Jacobian."""
+    return {"tol_rel": 1e-10, "fd_iterations": e["fd"]["iterations"], "exact_iterations": e["exact"]["iterations"],
+            "fd_ms": round(e["fd"]["ms_per_solve"], 3), "exact_ms": round(e["exact"]["ms_per_solve"], 3),
+            "exact_vs_fd_wall_time": round(e["exact_vs_fd_wall_time"], 3),
+            "sweep_iterations_fd_exact": {k: [v["fd"]["iterations"], v["exact"]["iterations"]]
+                                          for k, v in e["sweep"].items()},
+            "ref_defaults_final_norm_fd_exact": [e["sweep"]["abs_1e-12_max3"][j]["final_max_norm"] for j in ("fd", "exact")]}
 
 
 def batching(steps=20, warm=3):
@@ -708,8 +793,7 @@ def gpu_arm(args, rank, world, local_rank):
         nbytes = hP.numel() * 8
         e2e = {"value": world * zones / (ms_e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes if world == 1 else nbytes + 8, "ms_per_step": ms_e,
-               "path": "khb_step_host_interior (interior P in, U = U(P) and ghost zones rebuilt, graph step, "
-                       "interior P out)" if graph_ok else "P in, khb_ptou, host-driven step, P out"}
+               "path": "khb_step_host_interior" if graph_ok else "P in, khb_ptou, host-driven step, P out"}
 
     # roofline of the dominant kernel, timed live with CUDA events
     peak, peak_kind = measured_peaks()
@@ -726,60 +810,46 @@ def gpu_arm(args, rank, world, local_rank):
         # per zone per launch on average); a flux pass reads P once (nv doubles per zone).
         per_zone = {"k_zone": 4.5 * nv * 8}.get(dom, nv * 8)
         ach = per_zone * zones / (ms_launch / 1000.0) / 1e9
-        # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on
-        # this workload: the stage-2 zone pass, update and cell kernels together
-        traffic = {"k_zone": 1479.0e6}.get(dom) if (n1, n2, n3) == (128, 128, 128) else None
+        traffic, tsrc = profile_traffic(dom, (n1, n2, n3), args.form)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
+                    "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic, "traffic_source": tsrc,
                     "alg_bytes_per_zone_per_launch": per_zone,
-                    "step": {"achieved": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9,
-                             "frac": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9 / peak,
-                             "alg_bytes_per_zone_cycle": B_ALG_PER_ZC},
-                    "kernel_ms_per_launch": {k: round(v[0], 4) for k, v in ktimes.items()}}
-        if (n1, n2, n3) == (128, 128, 128):
-            # the bound that applies to the FP64 path: FP64-pipe activity of its kernels on this
-            # workload (ncu sm__pipe_fp64_cycles_active as a fraction of peak, from the full capture
-            # of the stage-2 kernels of this build); not timed live
-            roofline["fp64_pipe"] = {"source": "ncu capture of this workload", "k_flux_x1": 0.427,
-                                     "k_flux_x2": 0.390, "k_flux_x3": 0.382, "k_zone_update": 0.241,
-                                     "k_zone_cell": 0.382}
+                    "step_frac": B_ALG_PER_ZC * zones / (ms_step / 1000.0) / 1e9 / peak}
+        detail("kernel_ms_per_launch", {k: round(v[0], 4) for k, v in ktimes.items()})
 
     emhd = None
     if rank == 0 and world == 1 and not args.no_emhd:
         emhd = emhd_newton()
+        detail("emhd_newton", emhd)
 
-    bct = smr = None
     if rank == 0 and world == 1 and not args.no_batch:
-        bct = b_ct_form()
-        smr = smr_form()
-
-    batch = None
-    if rank == 0 and world == 1 and not args.no_batch:
+        detail("b_ct", b_ct_form())
+        detail("smr", smr_form())
         del b, drv
         torch.cuda.empty_cache()
-        batch = batching()
+        detail("batching", batching())
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        n3s = max(8, n3 // 2)
-        v_cpu, threads, el = cpu_sample(n1, n2, n3s, steps=8)
-        cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"oracle port, {threads} OpenMP threads, {n1}x{n2}x{n3s} slab of the torus "
-                         f"(same per-zone work), 8 RK2 steps after 1 warm-up ({el:.1f} s)"}
+        cpu = cpu_baseline_block(n1, n2, n3)
 
     if rank == 0:
+        if host_driven:
+            detail("host_driven_step", host_driven)
+        if fp32 and "kernel_ms_per_launch" in fp32:
+            detail("fp32_flux_kernel_ms_per_launch", fp32.pop("kernel_ms_per_launch"))
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                "config": {"workload": (f"FM torus FMKS {n1}x{n2}x{n3} one meshblock per GPU" if world == 1 else
                                        f"FM torus FMKS {n1}x{n2}x{n3 * world}, one {n1}x{n2}x{n3} x3 slab per GPU"),
                           "recon": "linear_mc", "flux": "llf", "b_field": "flux_ct", "inverter": "onedw",
-                          "floors": "drift",
+                          "floors": "drift", "form": args.form,
                           "parallelism": "single block" if world == 1 else f"x3 slabs x{world} (NCCL halo exchange)",
-                          "l2": "state (P,U: 2 x 8 x 136^3 doubles = 322 MB) larger than L2"},
+                          "l2": "state 322 MB > L2, no flush"},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
-               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu, "emhd_newton": emhd, "batching": batch, "b_ct": bct, "smr": smr,
-               "host_driven_step": host_driven}
+               "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu,
+               "emhd_newton": emhd_summary(emhd) if emhd else None}
         print(json.dumps(out), flush=True)
 
 
@@ -794,7 +864,9 @@ def main():
     import torch
     if args.emhd_only:
         if rank == 0:
-            print(json.dumps({"emhd_newton": emhd_newton()}), flush=True)
+            e = emhd_newton()
+            detail("emhd_newton", e)
+            print(json.dumps({"emhd_newton": emhd_summary(e)}), flush=True)
         return
     if args.adjoint_only:
         if rank == 0:

@@ -33,6 +33,7 @@
 #include <vector>
 #include <algorithm>
 #include <limits>
+#include <omp.h>
 
 namespace orc {
 
@@ -3188,6 +3189,15 @@ void* orc_create(const Config* cfg, const CoordSpec* cs)
     return h;
 }
 void orc_destroy(void* hp) { delete (Handle*)hp; }
+
+// OpenMP threads of the following parallel regions (the CPU baseline's one-thread run); returns the
+// previous maximum
+int orc_set_threads(int n)
+{
+    const int prev = omp_get_max_threads();
+    if (n > 0) omp_set_num_threads(n);
+    return prev;
+}
 
 void orc_get_dims(void* hp, int32_t* dims)
 {

@@ -80,6 +80,8 @@ def load():
     lib.orc_create.restype = P
     lib.orc_create.argtypes = [C.POINTER(Config), C.POINTER(CoordSpec)]
     lib.orc_destroy.argtypes = [P]
+    lib.orc_set_threads.restype = C.c_int
+    lib.orc_set_threads.argtypes = [C.c_int]
     lib.orc_get_dims.argtypes = [P, P]
     lib.orc_get_geometry.argtypes = [P, P, P, P, P, P]
     lib.orc_set_geometry.argtypes = [P, P, P, P, P, P]
@@ -115,6 +117,11 @@ def load():
     lib.orc_imex_stage.argtypes = [P, P, P, C.c_int, C.c_double, P, P, P, P, P, P, P, P, P]
     _lib = lib
     return lib
+
+
+def set_threads(n):
+    """OpenMP threads of the oracle's parallel loops from now on; returns the previous maximum."""
+    return int(load().orc_set_threads(int(n)))
 
 
 def _ptr(a):
