@@ -846,7 +846,8 @@ def gpu_arm(args, rank, world, local_rank):
                           "recon": "linear_mc", "flux": "llf", "b_field": "flux_ct", "inverter": "onedw",
                           "floors": "drift", "form": args.form,
                           "parallelism": "single block" if world == 1 else f"x3 slabs x{world} (NCCL halo exchange)",
-                          "l2": "state 322 MB > L2, no flush"},
+                          "l2": (f"state {2 * spec.nvar * spec.shape[0] * spec.shape[1] * spec.shape[2] * 8 / 1e6:.0f} MB "
+                                 f"{'>' if 2 * spec.nvar * np.prod(spec.shape) * 8 > 126e6 else '<'} L2 (126 MB), no flush")},
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
                "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu,
                "emhd_newton": emhd_summary(emhd) if emhd else None}
