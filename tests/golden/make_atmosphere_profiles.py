@@ -5,15 +5,18 @@ files atmosphere_soln_{rCoords,rho,u,phi}.txt, one row per radial zone including
 zones, and checks rCoords against its grid to 1e-10.  Its test harness keeps one set per
 resolution under tests/conducting_atmosphere/conducting_atmosphere_<n1>_default/.
 
-Run from the repository root with the reference checkout at REF (default /root/reference):
-    python tests/golden/make_atmosphere_profiles.py [REF]
+Run from the repository root with the path of a KHARMA checkout, as an argument or in the
+environment variable KHARMA_REF:
+    python tests/golden/make_atmosphere_profiles.py <path to kharma>
 """
 import os
 import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KHARMA_REF")
+if not REF:
+    sys.exit("usage: make_atmosphere_profiles.py <path to a KHARMA checkout> (or set KHARMA_REF)")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "atmosphere_profiles.npz")
 
 arrays = {}
