@@ -61,6 +61,43 @@ def mhdmodes(spec, nmode=3, amp=1e-4):
     return P
 
 
+# The 2D EMHD wave of prob/emhd/emhdmodes.hpp:56-160: mean state rho 1, u 2, B (0.1, 0.3, 0), wavevector
+# (2 pi, 4 pi, 0), conduction and viscosity with the sound-speed closure; eigenvector coefficients of
+# cos(phi) and sin(phi) per primitive (rho, u, u1, u2, u3, B1, B2, B3, q, dP) and the complex
+# frequency (decay rate omega_real, angular frequency omega_imag) as the problem defines them
+# (the B coefficients come through the "wave" field seed, prob/seed_B.hpp:160-169).
+EMHD_MODE = {
+    "mean": (1.0, 2.0, 0.0, 0.0, 0.0, 0.1, 0.3, 0.0, 0.0, 0.0),
+    "cos": (-0.518522524082246, 0.5516170736393813, 0.008463122479547856, -0.16175466371870734, 0.0,
+            -0.05973794979640743, 0.02986897489820372, 0.0, 0.5233486841539436, 0.2909106062057657),
+    "sin": (0.1792647678001878, 0.0, -0.011862022608466367, 0.034828080823603294, 0.0,
+            0.03351707506150924, -0.016758537530754618, 0.0, -0.04767672501939603, -0.02159452055336572),
+    "omega_real": -0.5533585207638141, "omega_imag": -3.6262571286888425, "k1": 2 * np.pi, "k2": 4 * np.pi,
+}
+
+
+def emhdmodes(spec, amp=1e-8, t=0.0):
+    """The EMHD wave on the periodic unit square (emhdmodes.hpp:129-157 without higher-order terms):
+    10-slot primitives over the whole block at time t (t = 0: the initial state; later times: the
+    analytic solution tests/emhdmodes/check.py compares with, phase advanced by omega_imag t and
+    amplitude scaled by exp(omega_real t))."""
+    m = EMHD_MODE
+    n3, n2, n1 = spec.shape
+    x1, x2, _ = cell_centers(spec)
+    X1, X2 = np.meshgrid(x1, x2, indexing="xy")          # (n2, n1)
+    phi = m["k1"] * X1 + m["k2"] * X2 + m["omega_imag"] * t
+    c, s = np.cos(phi), np.sin(phi)
+    decay = np.exp(m["omega_real"] * t)
+    P = np.zeros((10, n3, n2, n1))
+    for v in range(10):
+        if v in (5, 6, 7):
+            # the wave seed adds amp_B cos + amp2_B sin with amp_B = amp * coefficient
+            P[v] = m["mean"][v] + ((amp * m["cos"][v]) * c + (amp * m["sin"][v]) * s) * decay
+        else:
+            P[v] = m["mean"][v] + (amp * (m["cos"][v] * c + m["sin"][v] * s)) * decay
+    return P
+
+
 def mhdmodes_period(nmode=3):
     return 2 * np.pi / MODES_DIR3[nmode]["omega"]
 

@@ -5,6 +5,9 @@ tests/mhdmodes/run.sh + check.py in the reference run the 2D linear modes (k = (
 power of resolution with slope in [-2.15, -1.94] ([-2.3, -1.94] for u2/u3).  The eigenvectors and
 frequencies come from kharma/prob/mhdmodes.hpp:140-190.  The configuration here is the reference's
 `*_onedw` case: WENO5, LLF, flux-CT, simple driver, 1D_W inversion, CFL 0.9, dt_min 1e-4.
+The reference's Bondi steady-state test (tests/bondi) and EMHD linear-mode test (tests/emhdmodes)
+pin the spherical hydro path (inflow check, polar faces, KS/MKS geometry, both inverters) and the
+EMHD ImEx path the same way, below.
 """
 import numpy as np
 import pytest
@@ -65,3 +68,110 @@ def test_oracle_divb_roundoff(oracle_mod):
     for _ in range(10):
         _, _, dt, _ = o.step(P, U, dt)
     assert o.max_divb(U) < 1e-12 + 10 * d0
+
+
+# ---------------------------------------------------------------------------- Bondi steady state
+# tests/bondi/run.sh + check.py: the 2D Bondi flow (pars/bondi/bondi.par: KS a = 0 in MKS hslope 0.3,
+# r in [3, 30], gamma 5/3, WENO5, hydro, floors off, outer X1 face holding the analytic solution,
+# inner X1 outflow with the inflow check, reflecting polar faces with zero polar fluxes) run to
+# t = 50 from the analytic solution at 16, 24, 32, 48, 64 zones per side; the L1 drift from the
+# initial state of the x2-averaged rho, u and u^1 must fall with slope in [-2.2, -1.85].
+BONDI_RES = [16, 24, 32, 48, 64]
+
+
+def bondi_pin_spec(n, **kw):
+    import dataclasses
+    import math
+    from kharma_b200.spec import bondi_spec
+    spec = bondi_spec(n, n, 1, math.log(3.0), math.log(30.0), 0.0, 1.0, recon="weno5",
+                      bc=("outflow", "exchange", "reflecting", "reflecting", "periodic", "periodic"))
+    return dataclasses.replace(spec, check_inflow_inner_x1=True, check_inflow_outer_x1=False,
+                               zero_polar_flux=True, **kw)
+
+
+def bondi_drift(P, P0, spec):
+    """check.py's figure: mean over r of |<P_end>_x2 - <P_start>_x2| for rho, u, u^1."""
+    sl = spec.interior
+    return [float(np.mean(np.abs(np.mean(P[v][sl], axis=1) - np.mean(P0[v][sl], axis=1)))) for v in (0, 1, 2)]
+
+
+def bondi_slopes(L):
+    L = np.array(L)
+    return [np.polyfit(np.log(BONDI_RES), np.log(L[:, v]), 1)[0] for v in range(3)]
+
+
+@pytest.mark.parametrize("variant", [{}, {"inverter": "kastaun", "iter_max": 25, "err_tol": 1e-12},
+                                     {"recon": "linear_mc"}], ids=["base", "kastaun", "linear_mc"])
+def test_oracle_bondi_converges_like_reference(oracle_mod, variant):
+    L = []
+    for n in BONDI_RES:
+        spec = bondi_pin_spec(n, **variant)
+        o = oracle_mod.Oracle(spec)
+        P, U = o.init_state(problems.bondi(spec, o.geometry()))
+        P0 = P.copy()
+        t, dt = 0.0, spec.dt_min
+        while t < 50.0:
+            dt = min(dt, 50.0 - t)
+            _, _, dtn, _ = o.step(P, U, dt)
+            t += dt
+            dt = dtn
+        L.append(bondi_drift(P, P0, spec))
+    for name, p in zip(("rho", "u", "u1"), bondi_slopes(L)):
+        assert -2.2 <= p <= -1.85, f"{name}: slope {p:.3f}; L1 {np.array(L)}"
+
+
+# ---------------------------------------------------------------------------- EMHD linear mode
+# tests/emhdmodes/run.sh + check.py: the 2D EMHD wave (prob/emhd/emhdmodes.hpp; pars/emhd/emhdmodes.par:
+# periodic unit square, Minkowski, gamma 4/3, sound-speed closure with conduction and viscosity,
+# tau = 1, alphas 1, amplitude 1e-8, ImEx (vl2) with the forward-difference Newton solve, 3
+# iterations, rootfind_tol 1e-20) run to t = 2 with WENO5 at 32, 64, 128; the L1 error of every
+# perturbed primitive against the damped analytic wave must fall with slope in [-3.3, -1.6].
+EMHD_RES = [32, 64, 128]
+
+
+def emhd_mode_setup(n, recon):
+    from kharma_b200.spec import BlockSpec, EmhdSpec, ImplicitSpec
+    spec = BlockSpec(nx1=n, nx2=n, nx3=1, x1min=0., x1max=1., x2min=0., x2max=1., x3min=0., x3max=1.,
+                     gam=4.0 / 3.0, nvar=8, recon=recon, riemann="llf", cfl=0.9, driver="imex")
+    emhd = EmhdSpec(closure_type="soundspeed", higher_order_terms=False, tau=1.0, conduction_alpha=1.0,
+                    viscosity_alpha=1.0)
+    imp = ImplicitSpec(min_nonlinear_iter=1, max_nonlinear_iter=3, rootfind_tol=1e-20)
+    return spec, emhd, imp
+
+
+def emhd_next_dt(spec, mn, dt):
+    return min(2.0 * dt, min(max(mn * spec.cfl, spec.dt_min), spec.max_dt_increase * dt))
+
+
+def emhd_errors(P, spec, t):
+    ref = problems.emhdmodes(spec, t=t)
+    sl = spec.interior
+    return [float(np.mean(np.abs(P[v][sl] - ref[v][sl]))) for v in range(10)]
+
+
+def emhd_slopes(L, res):
+    L = np.array(L)
+    m = problems.EMHD_MODE
+    return {v: np.polyfit(np.log(res), np.log(L[:, v]), 1)[0] for v in range(10)
+            if m["cos"][v] != 0 or m["sin"][v] != 0}
+
+
+def test_oracle_emhd_mode_converges_like_reference(oracle_mod):
+    L = []
+    for n in EMHD_RES:
+        spec, emhd, imp = emhd_mode_setup(n, "weno5")
+        o = oracle_mod.Oracle(spec)
+        P = problems.emhdmodes(spec)
+        U = o.emhd_ptou(emhd, P)
+        sn, sf = np.zeros(spec.shape), np.zeros(spec.shape)
+        t, dt = 0.0, spec.dt_min
+        while t < 2.0:
+            dt = min(dt, 2.0 - t)
+            P1, U1, _, _ = o.imex_stage(emhd, imp, 1, dt, P, U, P, U, sn, sf)
+            P, U, _, mn = o.imex_stage(emhd, imp, 2, dt, P, U, P1, U1, sn, sf)
+            t += dt
+            dt = emhd_next_dt(spec, mn, dt)
+        L.append(emhd_errors(P, spec, t))
+    names = ["rho", "u", "u1", "u2", "u3", "B1", "B2", "B3", "q", "dP"]
+    for v, p in emhd_slopes(L, EMHD_RES).items():
+        assert -3.3 <= p <= -1.6, f"{names[v]}: slope {p:.3f}; L1 {np.array(L)[:, v]}"
