@@ -58,13 +58,18 @@ class LocalExchange:
 
 
 class DistExchange:
-    """One slab per rank of the default process group; neighbours rank -/+ 1 (periodic)."""
+    """One slab per rank of the default process group; neighbours rank -/+ 1 (periodic).
 
-    def __init__(self):
+    host_staged: device slices travel through host buffers (a backend without device point-to-point
+    support, such as gloo, with the slabs on GPUs); otherwise the field arrays' own slices are sent
+    (NCCL between GPUs, or gloo with CPU tensors)."""
+
+    def __init__(self, host_staged=False):
         import torch.distributed as dist
         self.dist = dist
         self.rank = dist.get_rank()
         self.world = dist.get_world_size()
+        self.host_staged = host_staged
 
     def exchange(self, arrays, spec, nplanes):
         """arrays: this rank's list of (n3, n2, n1) (or (nv, n3, n2, n1)) arrays."""
@@ -77,18 +82,30 @@ class DistExchange:
         views = []
         for a in arrays:
             views += [a[v] for v in range(a.shape[0])] if a.dim() == 4 else [a]
+        stage = self.host_staged and views and views[0].is_cuda
+        if stage:
+            torch.cuda.current_stream().synchronize()
+            sends = [(a[slo].cpu(), a[shi].cpu()) for a in views]
+            recvs = [(torch.empty_like(lo), torch.empty_like(hi)) for lo, hi in sends]
+        else:
+            sends = [(a[slo], a[shi]) for a in views]
+            recvs = [(a[rhi], a[rlo]) for a in views]
         ops = []
         # Per peer the k-th send matches the k-th receive: send (low planes -> left, high planes ->
         # right) and receive (high ghosts <- right, low ghosts <- left) in this order, so that with
         # two ranks (left == right) the low planes still land in the peer's high ghosts.
-        for a in views:
-            ops.append(dist.P2POp(dist.isend, a[slo], left))
-            ops.append(dist.P2POp(dist.isend, a[shi], right))
-        for a in views:
-            ops.append(dist.P2POp(dist.irecv, a[rhi], right))
-            ops.append(dist.P2POp(dist.irecv, a[rlo], left))
+        for lo, hi in sends:
+            ops.append(dist.P2POp(dist.isend, lo, left))
+            ops.append(dist.P2POp(dist.isend, hi, right))
+        for into_hi, into_lo in recvs:
+            ops.append(dist.P2POp(dist.irecv, into_hi, right))
+            ops.append(dist.P2POp(dist.irecv, into_lo, left))
         for req in dist.batch_isend_irecv(ops):
             req.wait()
+        if stage:
+            for a, (into_hi, into_lo) in zip(views, recvs):
+                a[rhi].copy_(into_hi)
+                a[rlo].copy_(into_lo)
 
 
 class SlabBlock:
