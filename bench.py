@@ -417,10 +417,16 @@ def batching(steps=20, warm=3):
             r["per_block_ms_per_step"] = timed(lambda: b.step_per_block(dt), max(3, steps // 4))
             r["batched_ms_per_step"] = timed(lambda: b.step(dt), steps)
             tune, pers = b.autotune(3)
-            r["autotune"] = {"planes_per_cta": tune, "persistent": pers}
-            l0 = b.launch_count()
-            r["graph_ms_per_step"] = timed(lambda: b.step_graph(dt), steps)
-            r["launches_per_step"] = (b.launch_count() - l0) / (steps + warm)
+            plan = b.plan()
+            r["autotune"] = {"planes_per_cta": tune, "persistent": pers, "plan": plan}
+            # both launch plans with the tuned tile shapes: one launch per kernel per stage, and three
+            for p in (1 - plan, plan):
+                b.set_plan(p)
+                l0 = b.launch_count()
+                r[f"graph_ms_per_step_plan{p}"] = timed(lambda: b.step_graph(dt), steps)
+                r[f"launches_per_step_plan{p}"] = (b.launch_count() - l0) / (steps + warm)
+            r["graph_ms_per_step"] = r[f"graph_ms_per_step_plan{plan}"]
+            r["launches_per_step"] = r[f"launches_per_step_plan{plan}"]
         for k in ("per_block", "batched", "graph"):
             r[k + "_zone_cycles_per_s"] = zones / (r[k + "_ms_per_step"] / 1000.0)
         r["speedup_graph_vs_per_block"] = r["per_block_ms_per_step"] / r["graph_ms_per_step"]
@@ -466,10 +472,15 @@ def smr_form(steps=20, warm=3):
         return e0.elapsed_time(e1) / n, (b.launch_count() - l0) / n
 
     ms, launches = timed(steps)
+    b.set_plan(1)
+    ms_f, launches_f = timed(steps)
+    b.set_plan(0)
     out = {"workload": "periodic box, 4x4x4 root blocks of 32^3 with the central 2x2x2 refined: 56 coarse + 64 fine "
                        "blocks, 3,932,160 zones, hydro entropy wave, linear MC, LLF, FP64",
            "ghost_entries": int(len(ghost)), "flux_entries": int(len(flux)),
-           "graph_ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0), "launches_per_step": launches}
+           "graph_ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0), "launches_per_step": launches,
+           "fused_plan": {"graph_ms_per_step": ms_f, "zone_cycles_per_s": mesh.zones / (ms_f / 1000.0),
+                          "launches_per_step": launches_f}}
     empty = np.zeros((0, 6), dtype=np.int32)
     b.set_mesh(empty, 0, empty)
     ms0, _ = timed(steps)

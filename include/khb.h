@@ -459,10 +459,19 @@ int khb_batch_classes(khb_batch* batch, int32_t* nclasses, int32_t* sizes, int32
 int khb_batch_set_tuning(khb_batch* batch, int size_class, int kz, int persistent);
 
 /* Autotuner: for each class in turn, time reps runs of a stage-1 pass with each tile shape and
- * keep the fastest; then the same for the launch mode.  Stage 1 writes only the contexts' stage
- * scratch, the flags and the failed-zone lists, so the state is unchanged.  Writes the chosen kz
- * per class and the launch mode.  Synchronizes. */
+ * keep the fastest; then the same for the launch mode and the launch plan.  Stage 1 writes only the
+ * contexts' stage scratch, the flags and the failed-zone lists, so the state is unchanged.  Writes
+ * the chosen kz per class and the launch mode (the plan: khb_batch_get_plan).  Synchronizes. */
 int khb_batch_autotune(khb_batch* batch, int reps, int32_t* kz_out, int32_t* persistent_out, void* stream);
+
+/* Launch plan of a stage (results bitwise the same): 0 (the default) launches each kernel once per
+ * stage for all blocks (counter reset, faces per direction, ghost-shell copy, update half, cell
+ * half, fixups: 8 launches per stage for blocks with exchange faces); 1 fuses them into three (all
+ * faces of all directions with the resets and ghost-shell copies, the whole zone pass, fixups).
+ * Blocks with physical faces add their per-block flux fixes and boundary launches, SMR meshes the
+ * flux correction and ghost exchange, in either plan.  A captured graph is captured again. */
+int khb_batch_set_plan(khb_batch* batch, int plan);
+int khb_batch_get_plan(khb_batch* batch, int32_t* plan);
 
 /* Device kernel launches issued for this batch so far (a graph replay counts its nodes). */
 int64_t khb_batch_launch_count(khb_batch* batch);

@@ -149,6 +149,15 @@ class Batch:
     def launch_count(self):
         return int(self.lib.khb_batch_launch_count(self.h))
 
+    def set_plan(self, plan):
+        """0: one launch per kernel per stage; 1: three launches per stage (khb_batch_set_plan)."""
+        _lib.check(self.lib.khb_batch_set_plan(self.h, int(plan)), "khb_batch_set_plan")
+
+    def plan(self):
+        out = C.c_int32()
+        _lib.check(self.lib.khb_batch_get_plan(self.h, C.byref(out)), "khb_batch_get_plan")
+        return int(out.value)
+
     def set_mesh(self, ghost, n_ghost_first, flux):
         """SMR tables (kharma_b200.mesh.SMRMesh.tables): ghost exchange after every stage and flux
         correction before every update."""

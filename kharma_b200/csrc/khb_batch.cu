@@ -25,15 +25,21 @@ struct khb_batch {
     std::vector<std::array<int, 3>> class_size;    // (nx1, nx2, nx3) of each class
     std::vector<int> class_kz;                     // planes per CTA (0 = default)
     int persistent = 0;                            // 1: grid of (SMs x resident CTAs), CTAs loop over tiles
+    // launch plan: 0 one launch per kernel per stage (counter reset, faces per direction, ghost-shell
+    // copy, update half, cell half, fixups); 1 fused: three launches per stage (all faces with the
+    // resets and shell copies, the whole zone pass, fixups), plus the per-block launches of physical
+    // faces and the mesh kernels of SMR meshes
+    int plan = 0;
     int nsm = 0;
     // device tables
     void* desc = nullptr;                          // BatchBlock<FT>[nb]
     FixupBlock* fix = nullptr;                     // FixupBlock[nb]
     int** counts = nullptr;                        // fail_count pointer of each block
-    int* tiles[4] = {nullptr, nullptr, nullptr, nullptr};
-    unsigned ntiles[4] = {0, 0, 0, 0};
-    unsigned grid[4] = {0, 0, 0, 0};               // 0: one CTA per tile
-    int occ[5] = {0, 0, 0, 0, 0};                  // resident CTAs per SM: flux x1..x3, update, cell
+    int* tiles[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // x1-x3 faces, zones, fused-plan faces
+    unsigned ntiles[5] = {0, 0, 0, 0, 0};
+    unsigned grid[5] = {0, 0, 0, 0, 0};            // 0: one CTA per tile
+    unsigned grid_fused_zone = 0;
+    int occ[7] = {0, 0, 0, 0, 0, 0, 0};            // resident CTAs per SM: flux x1..x3, update, cell, faces, zone pass
     double* dt_dev = nullptr;
     unsigned long long* word = nullptr;            // minimum zone timestep (bit pattern)
     double dt_host = 0.;                           // source of the timestep upload
@@ -87,7 +93,7 @@ void free_tables(khb_batch* b)
     cudaFree(b->desc); b->desc = nullptr;
     cudaFree(b->fix); b->fix = nullptr;
     cudaFree(b->counts); b->counts = nullptr;
-    for (int x = 0; x < 4; ++x) { cudaFree(b->tiles[x]); b->tiles[x] = nullptr; }
+    for (int x = 0; x < 5; ++x) { cudaFree(b->tiles[x]); b->tiles[x] = nullptr; }
 }
 
 void drop_graph(khb_batch* b)
@@ -120,7 +126,7 @@ int build_tables(khb_batch* b)
     std::vector<BatchBlock<FT>> desc(b->nb);
     std::vector<FixupBlock> fix(b->nb);
     std::vector<int*> counts(b->nb);
-    std::vector<int> tiles[4];
+    std::vector<int> tiles[5];
     for (int x = 0; x < b->nb; ++x) {
         khb_ctx* c = b->ctx[x];
         const Dims& d = c->d;
@@ -164,6 +170,20 @@ int build_tables(khb_batch* b)
             const unsigned n = box_blocks(bx);
             tiles[q].insert(tiles[q].end(), n, x);
         }
+        // the fused plan's table: this block's faces of every direction, then its ghost shell in
+        // tiles of 128 zones when it has an exchange face (entry = block | kind << 28)
+        bool exch = false;
+        for (int f = 0; f < 2 * d.ndim; ++f) if (d.bc[f] == KHB_BC_EXCHANGE) exch = true;
+        for (int q = 0; q < 4; ++q) {
+            B.tile0c[q] = (unsigned)tiles[4].size();
+            unsigned n = 0;
+            if (q < 3 && q + 1 <= b->ndim) n = box_blocks(B.fbox[q]);
+            if (q == 3 && exch) {
+                const long long shell = d.N - (long long)(d.ie - d.is + 1) * (d.je - d.js + 1) * (d.ke - d.ks + 1);
+                n = (unsigned)((shell + 127) / 128);
+            }
+            tiles[4].insert(tiles[4].end(), n, x | (q << 28));
+        }
         fix[x].d = d; fix[x].g = c->g; fix[x].ph = c->ph;
         fix[x].exch = 0;
         for (int f = 0; f < 2 * d.ndim; ++f) if (d.bc[f] == KHB_BC_EXCHANGE) fix[x].exch = 1;
@@ -178,7 +198,8 @@ int build_tables(khb_batch* b)
     KHB_BCUDA(cudaMemcpy(b->fix, fix.data(), sizeof(FixupBlock) * b->nb, cudaMemcpyHostToDevice));
     KHB_BCUDA(cudaMalloc((void**)&b->counts, sizeof(int*) * b->nb));
     KHB_BCUDA(cudaMemcpy(b->counts, counts.data(), sizeof(int*) * b->nb, cudaMemcpyHostToDevice));
-    for (int q = 0; q < 4; ++q) {
+    if (b->nb >= (1 << 28)) return set_error(KHB_ERR_ARG, "khb_batch: too many blocks for the fused plan's table");
+    for (int q = 0; q < 5; ++q) {
         b->ntiles[q] = (unsigned)tiles[q].size();
         if (tiles[q].empty()) continue;
         KHB_BCUDA(cudaMalloc((void**)&b->tiles[q], sizeof(int) * tiles[q].size()));
@@ -189,52 +210,21 @@ int build_tables(khb_batch* b)
     // batched kernel reads them
     KHB_BCUDA(cudaDeviceSynchronize());
     // persistent grids: every SM holds as many CTAs as the kernel's registers allow
-    for (int q = 0; q < 4; ++q) {
-        const int occ = (q < 3) ? b->occ[q] : std::min(b->occ[3], b->occ[4]);
+    for (int q = 0; q < 5; ++q) {
+        const int occ = (q < 3) ? b->occ[q] : ((q == 3) ? std::min(b->occ[3], b->occ[4]) : b->occ[5]);
         const unsigned full = (unsigned)(b->nsm * std::max(occ, 1));
         b->grid[q] = b->persistent ? std::min(b->ntiles[q], full) : 0;
     }
+    b->grid_fused_zone = b->persistent ? std::min(b->ntiles[3], (unsigned)(b->nsm * std::max(b->occ[6], 1))) : 0;
     drop_graph(b);
     return KHB_OK;
 }
 
 int rebuild(khb_batch* b) { return b->fp32 ? build_tables<float>(b) : build_tables<double>(b); }
 
-template <typename FT>
-int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
+// The boundaries of blocks with physical or periodic faces (per-block launches of the context)
+int enqueue_bounds(khb_batch* b, int s, cudaStream_t st)
 {
-    const int stage = s + 1;
-    const BatchBlock<FT>* desc = (const BatchBlock<FT>*)b->desc;
-    LaunchCommon::batch_reset(b->counts, b->nb, s == 1 ? b->word : nullptr, st);
-    KHB_BLAUNCHED(b, 1);
-    for (int dir = 1; dir <= b->ndim; ++dir) {
-        Launch<FT>::batch_flux(b->recon, b->nv, dir, desc, b->tiles[dir - 1], b->ntiles[dir - 1], b->grid[dir - 1],
-                               stage, st);
-        KHB_BLAUNCHED(b, 1);
-    }
-    for (int x : b->needs_fix_flux) {
-        const int64_t l0 = b->ctx[x]->launches;
-        int rc = ctx_fix_flux(b->ctx[x], st);
-        if (rc) return rc;
-        b->launches += b->ctx[x]->launches - l0;
-    }
-    if (b->n_flux) {
-        Launch<FT>::mesh_flux(b->nv, desc, b->mesh_flux, b->n_flux, st);
-        KHB_BLAUNCHED(b, 1);
-    }
-    if (b->any_exchange) {
-        LaunchCommon::batch_ghost_copy(b->nv, b->fix, b->nb, stage, st);
-        KHB_BLAUNCHED(b, 1);
-    }
-    Launch<FT>::batch_zone(b->nv, M_UPDATE, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage, 0, kRkBeta[s],
-                           b->dt_dev, st);
-    KHB_BLAUNCHED(b, 1);
-    const int cell = M_ZONE_CELL | ((b->ctx[0]->ph.inverter == KHB_INVERTER_KASTAUN) ? M_KASTAUN : 0);
-    Launch<FT>::batch_zone(b->nv, cell, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage,
-                           s == 1 ? M_DT : 0, kRkBeta[s], b->dt_dev, st);
-    KHB_BLAUNCHED(b, 1);
-    LaunchCommon::batch_fixup(b->nv, b->fix, b->nb, stage, st);
-    KHB_BLAUNCHED(b, 1);
     for (int x : b->needs_bounds) {
         khb_ctx* c = b->ctx[x];
         khb_fields Po, Uo;
@@ -252,6 +242,83 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
         if (rc) return rc;
         b->launches += c->launches - l0;
     }
+    return KHB_OK;
+}
+
+int enqueue_fix_flux(khb_batch* b, cudaStream_t st)
+{
+    for (int x : b->needs_fix_flux) {
+        const int64_t l0 = b->ctx[x]->launches;
+        int rc = ctx_fix_flux(b->ctx[x], st);
+        if (rc) return rc;
+        b->launches += b->ctx[x]->launches - l0;
+    }
+    return KHB_OK;
+}
+
+// The fused plan: faces of all directions (with the resets and shell copies), the whole zone pass,
+// fixups; the same device functions on the same data as the one-kernel-per-launch plan
+template <typename FT>
+int enqueue_stage_fused(khb_batch* b, int s, cudaStream_t st)
+{
+    const int stage = s + 1;
+    const BatchBlock<FT>* desc = (const BatchBlock<FT>*)b->desc;
+    Launch<FT>::batch_flux_all(b->recon, b->nv, desc, b->tiles[4], b->ntiles[4], b->grid[4], stage, b->counts, b->nb,
+                               s == 1 ? b->word : nullptr, st);
+    KHB_BLAUNCHED(b, 1);
+    int rc;
+    if ((rc = enqueue_fix_flux(b, st))) return rc;
+    if (b->n_flux) {
+        Launch<FT>::mesh_flux(b->nv, desc, b->mesh_flux, b->n_flux, st);
+        KHB_BLAUNCHED(b, 1);
+    }
+    const int fused = M_ZONE_FUSED | ((b->ctx[0]->ph.inverter == KHB_INVERTER_KASTAUN) ? M_KASTAUN : 0);
+    Launch<FT>::batch_zone(b->nv, fused, desc, b->tiles[3], b->ntiles[3], b->grid_fused_zone, stage,
+                           s == 1 ? M_DT : 0, kRkBeta[s], b->dt_dev, st);
+    KHB_BLAUNCHED(b, 1);
+    LaunchCommon::batch_fixup(b->nv, b->fix, b->nb, stage, st);
+    KHB_BLAUNCHED(b, 1);
+    if ((rc = enqueue_bounds(b, s, st))) return rc;
+    if (b->n_ghost) {
+        enqueue_mesh_ghost(b, stage, st);
+        KHB_BLAUNCHED(b, 0);
+    }
+    return KHB_OK;
+}
+
+template <typename FT>
+int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
+{
+    if (b->plan == 1) return enqueue_stage_fused<FT>(b, s, st);
+    const int stage = s + 1;
+    const BatchBlock<FT>* desc = (const BatchBlock<FT>*)b->desc;
+    LaunchCommon::batch_reset(b->counts, b->nb, s == 1 ? b->word : nullptr, st);
+    KHB_BLAUNCHED(b, 1);
+    for (int dir = 1; dir <= b->ndim; ++dir) {
+        Launch<FT>::batch_flux(b->recon, b->nv, dir, desc, b->tiles[dir - 1], b->ntiles[dir - 1], b->grid[dir - 1],
+                               stage, st);
+        KHB_BLAUNCHED(b, 1);
+    }
+    int rc;
+    if ((rc = enqueue_fix_flux(b, st))) return rc;
+    if (b->n_flux) {
+        Launch<FT>::mesh_flux(b->nv, desc, b->mesh_flux, b->n_flux, st);
+        KHB_BLAUNCHED(b, 1);
+    }
+    if (b->any_exchange) {
+        LaunchCommon::batch_ghost_copy(b->nv, b->fix, b->nb, stage, st);
+        KHB_BLAUNCHED(b, 1);
+    }
+    Launch<FT>::batch_zone(b->nv, M_UPDATE, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage, 0, kRkBeta[s],
+                           b->dt_dev, st);
+    KHB_BLAUNCHED(b, 1);
+    const int cell = M_ZONE_CELL | ((b->ctx[0]->ph.inverter == KHB_INVERTER_KASTAUN) ? M_KASTAUN : 0);
+    Launch<FT>::batch_zone(b->nv, cell, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage,
+                           s == 1 ? M_DT : 0, kRkBeta[s], b->dt_dev, st);
+    KHB_BLAUNCHED(b, 1);
+    LaunchCommon::batch_fixup(b->nv, b->fix, b->nb, stage, st);
+    KHB_BLAUNCHED(b, 1);
+    if ((rc = enqueue_bounds(b, s, st))) return rc;
     if (b->n_ghost) {
         enqueue_mesh_ghost(b, stage, st);
         KHB_BLAUNCHED(b, 0);
@@ -283,6 +350,10 @@ int query_occupancy(khb_batch* b)
     for (int m = 0; m < 2; ++m)
         b->occ[3 + m] = b->fp32 ? Launch<float>::batch_zone(b->nv, modes[m], nullptr, nullptr, 0, 0, 1, 0, 1., nullptr, 0)
                                 : Launch<double>::batch_zone(b->nv, modes[m], nullptr, nullptr, 0, 0, 1, 0, 1., nullptr, 0);
+    b->occ[5] = b->fp32 ? Launch<float>::batch_flux_all(b->recon, b->nv, nullptr, nullptr, 0, 0, 1, nullptr, 0, nullptr, 0)
+                        : Launch<double>::batch_flux_all(b->recon, b->nv, nullptr, nullptr, 0, 0, 1, nullptr, 0, nullptr, 0);
+    b->occ[6] = b->fp32 ? Launch<float>::batch_zone(b->nv, M_ZONE_FUSED, nullptr, nullptr, 0, 0, 1, 0, 1., nullptr, 0)
+                        : Launch<double>::batch_zone(b->nv, M_ZONE_FUSED, nullptr, nullptr, 0, 0, 1, 0, 1., nullptr, 0);
     KHB_BCUDA(cudaGetLastError());
     return KHB_OK;
 }
@@ -569,9 +640,36 @@ int khb_batch_autotune(khb_batch* b, int reps, int32_t* kz_out, int32_t* persist
     }
     b->persistent = best_p;
     if ((rc = rebuild(b))) return rc;
+    // then the launch plan (the tables serve both)
+    int best_plan = 0;
+    best_ms = 1e30f;
+    for (int plan : {0, 1}) {
+        b->plan = plan;
+        float ms = 0.f;
+        if ((rc = time_stage1(b, reps, st, &ms))) return rc;
+        if (ms < best_ms) { best_ms = ms; best_plan = plan; }
+    }
+    b->plan = best_plan;
+    drop_graph(b);
     b->launches = l0;
     if (kz_out) for (size_t q = 0; q < b->class_size.size(); ++q) kz_out[q] = b->class_kz[q];
     if (persistent_out) *persistent_out = b->persistent;
+    return KHB_OK;
+}
+
+int khb_batch_set_plan(khb_batch* b, int plan)
+{
+    if (!b) return set_error(KHB_ERR_ARG, "khb_batch_set_plan: NULL batch");
+    if (plan != 0 && plan != 1) return set_error(KHB_ERR_ARG, "khb_batch_set_plan: plan must be 0 or 1");
+    b->plan = plan;
+    drop_graph(b);
+    return KHB_OK;
+}
+
+int khb_batch_get_plan(khb_batch* b, int32_t* plan)
+{
+    if (!b || !plan) return set_error(KHB_ERR_ARG, "khb_batch_get_plan: NULL argument");
+    *plan = b->plan;
     return KHB_OK;
 }
 

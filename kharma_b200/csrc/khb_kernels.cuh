@@ -1229,7 +1229,8 @@ k_batch_zone(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ 
             if (threadIdx.x == 0) {
                 sb.za[s].bdt = beta * __ldg(dt);      // as the single-block path forms beta * dt
                 sb.za[s].mode = dtm;
-                if (MODE & M_UTOP) sb.za[s].Us = sb.za[s].Uout;   // the inversion reads the updated state
+                // the cell half inverts the state the update half wrote (the fused pass keeps it in registers)
+                if ((MODE & M_UTOP) && !(MODE & M_UPDATE)) sb.za[s].Us = sb.za[s].Uout;
             }
             __syncthreads();
             cur = b;
@@ -1240,6 +1241,55 @@ k_batch_zone(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ 
         if (dtm & M_DT) {
             block_min_ndt(ndt_zone, sb.za[s].ndt_word);
             __syncthreads();          // wmin is reused by the next tile of this CTA
+        }
+    }
+}
+
+// The fused plan's first launch of a stage (Launch<FT>::batch_flux_all): the faces of all directions
+// of every block and the ghost-shell copies of blocks with exchange faces, one table of 128-wide
+// tiles; CTA 0 first resets the failed-zone counters and the timestep minimum the zone pass fills.
+// The launch bound is the x3 faces' (the largest register need of the three directions).
+#ifndef KHB_BATCH_FLUXALL_MINB
+#define KHB_BATCH_FLUXALL_MINB KHB_FLUX64_X3_MINB
+#endif
+template <typename R> struct FluxAllMinBlocks { static constexpr int value = KHB_FLUX32_MINB; };
+template <> struct FluxAllMinBlocks<double> { static constexpr int value = KHB_BATCH_FLUXALL_MINB; };
+template <int RECON, int NV, typename R, typename FT>
+__global__ void __launch_bounds__(128, FluxAllMinBlocks<R>::value)
+k_batch_flux_all(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ tiles, unsigned ntiles, int stage,
+                 int* const* __restrict__ counts, int nblocks, unsigned long long* word)
+{
+    __shared__ __align__(16) BatchBlock<FT> sb;
+    if (blockIdx.x == 0) {
+        for (int x = threadIdx.x; x < nblocks; x += blockDim.x) *counts[x] = 0;
+        if (threadIdx.x == 0 && word) *word = 0x7FEFFFFFFFFFFFFFull;     // bit pattern of DBL_MAX
+    }
+    const int s = stage - 1;
+    int cur = -1;
+    for (unsigned t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int e = __ldg(tiles + t);
+        const int b = e & 0x0fffffff, kind = (e >> 28) & 3;
+        if (b != cur) {
+            __syncthreads();
+            stage_desc(sb, blocks + b);
+            __syncthreads();
+            cur = b;
+        }
+        const unsigned lt = t - sb.tile0c[kind];
+        int i, j, k;
+        if (kind == 3) {
+            long long c;
+            if (shell_zone(sb.d, lt * 128u + threadIdx.x, c))
+                copy_zone<NV>(sb.za[s].Ps, sb.za[s].Us, sb.za[s].Pout, sb.za[s].Uout, c);
+        } else if (kind == 0) {
+            if (box_cell(sb.fbox[0], lt, i, j, k))
+                flux_face<1, RECON, NV, R, FT>(sb.d, sb.g, sb.ph, sb.Pin[s], sb.F[0], sb.ctop[0], i, j, k);
+        } else if (kind == 1) {
+            if (box_cell(sb.fbox[1], lt, i, j, k))
+                flux_face<2, RECON, NV, R, FT>(sb.d, sb.g, sb.ph, sb.Pin[s], sb.F[1], sb.ctop[1], i, j, k);
+        } else {
+            if (box_cell(sb.fbox[2], lt, i, j, k))
+                flux_face<3, RECON, NV, R, FT>(sb.d, sb.g, sb.ph, sb.Pin[s], sb.F[2], sb.ctop[2], i, j, k);
         }
     }
 }
@@ -1560,6 +1610,40 @@ int Launch<FT>::batch_flux(int recon, int nv, int dir, const BatchBlock<FT>* blo
                      : batch_flux_nv<5, FT>(recon, dir, blocks, tiles, ntiles, grid, stage, st);
 }
 
+template <int NV, typename FT>
+static int batch_flux_all_nv(int recon, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles, unsigned grid,
+                             int stage, int* const* counts, int nblocks, unsigned long long* word, cudaStream_t st)
+{
+    const void* fn;
+    switch (recon) {
+    case RECON_DONOR: fn = (const void*)k_batch_flux_all<RECON_DONOR, NV, FT, FT>; break;
+    case RECON_MC:    fn = (const void*)k_batch_flux_all<RECON_MC, NV, FT, FT>; break;
+    case RECON_WENO5: fn = (const void*)k_batch_flux_all<RECON_WENO5, NV, FT, FT>; break;
+    default:          fn = (const void*)k_batch_flux_all<RECON_PPM, NV, FT, FT>; break;
+    }
+    if (ntiles == 0) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, 0);
+        return occ;
+    }
+    const unsigned nb = grid ? grid : ntiles;
+    switch (recon) {
+    case RECON_DONOR: k_batch_flux_all<RECON_DONOR, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage, counts, nblocks, word); break;
+    case RECON_MC:    k_batch_flux_all<RECON_MC, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage, counts, nblocks, word); break;
+    case RECON_WENO5: k_batch_flux_all<RECON_WENO5, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage, counts, nblocks, word); break;
+    default:          k_batch_flux_all<RECON_PPM, NV, FT, FT><<<nb, 128, 0, st>>>(blocks, tiles, ntiles, stage, counts, nblocks, word); break;
+    }
+    return 0;
+}
+template <typename FT>
+int Launch<FT>::batch_flux_all(int recon, int nv, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
+                               unsigned grid, int stage, int* const* counts, int nblocks, unsigned long long* word,
+                               cudaStream_t st)
+{
+    return (nv == 8) ? batch_flux_all_nv<8, FT>(recon, blocks, tiles, ntiles, grid, stage, counts, nblocks, word, st)
+                     : batch_flux_all_nv<5, FT>(recon, blocks, tiles, ntiles, grid, stage, counts, nblocks, word, st);
+}
+
 template <int NV, typename FT, int MODE>
 static int batch_zone_mode(const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles, unsigned grid, int stage,
                            int dtm, double beta, const double* dt, cudaStream_t st)
@@ -1576,6 +1660,14 @@ template <typename FT>
 int Launch<FT>::batch_zone(int nv, int mode, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
                            unsigned grid, int stage, int dtm, double beta, const double* dt, cudaStream_t st)
 {
+    if ((mode & ~M_KASTAUN) == M_ZONE_FUSED) {
+        // the fused plan: update and cell halves in one pass
+        const bool kast = mode & M_KASTAUN;
+        if (nv == 8) return kast ? batch_zone_mode<8, FT, M_ZONE_FUSED | M_KASTAUN>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st)
+                                 : batch_zone_mode<8, FT, M_ZONE_FUSED>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+        return kast ? batch_zone_mode<5, FT, M_ZONE_FUSED | M_KASTAUN>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st)
+                    : batch_zone_mode<5, FT, M_ZONE_FUSED>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
+    }
     if (nv == 8) {
         if (mode == M_UPDATE) return batch_zone_mode<8, FT, M_UPDATE>(blocks, tiles, ntiles, grid, stage, dtm, beta, dt, st);
         if (mode & M_KASTAUN)

@@ -128,6 +128,7 @@ struct BatchBlock {
     Box fbox[3];
     Box zbox;
     unsigned tile0[4];
+    unsigned tile0c[4];        // first tile of each kind in the fused plan's combined table (x1-x3 faces, shell)
 };
 
 // What the batched fixup reads of each block (independent of the flux precision)
@@ -167,6 +168,13 @@ struct Launch {
                           unsigned grid, int stage, cudaStream_t st);
     static int batch_zone(int nv, int mode, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
                           unsigned grid, int stage, int dtm, double beta, const double* dt, cudaStream_t st);
+    // The fused plan's first launch of a stage: every block's faces along all directions and the
+    // ghost-shell copies of blocks with exchange faces from one table (entry = block | kind << 28,
+    // kind 0-2 faces along x1-x3, 3 the shell), after CTA 0 has reset the failed-zone counters
+    // (counts[0..nblocks)) and, when word is given, the timestep minimum
+    static int batch_flux_all(int recon, int nv, const BatchBlock<FT>* blocks, const int* tiles, unsigned ntiles,
+                              unsigned grid, int stage, int* const* counts, int nblocks, unsigned long long* word,
+                              cudaStream_t st);
     // SMR flux correction over the entries of a mesh's flux table (6 ints each)
     static void mesh_flux(int nv, const BatchBlock<FT>* blocks, const int* table, long long n, cudaStream_t st);
 };

@@ -2,7 +2,8 @@
 per stage (khb_batch_step), replayed from a CUDA graph (khb_batch_step_graph), after autotuning.
 
 Requirements: a batch step is bitwise identical to khb_step on each block in turn (the per-block
-launch path), in both precisions; graph replay and any tile shape chosen by the autotuner change
+launch path), in both precisions and both launch plans (one launch per kernel per stage, or three
+launches per stage); graph replay and any tile shape or plan chosen by the autotuner change
 nothing; autotuning leaves the state alone; and each block matches the CPU oracle stepped with the
 same ghost inputs to 1e-12 per variable (max |gpu - oracle| <= 1e-12 max |oracle|), flags exactly.
 The mesh here has the production block counts (8 + 48 + 128) with 16^3, 8^3 and 4^3 blocks.
@@ -26,10 +27,12 @@ def assert_same(a, b):
             assert np.array_equal(sa[q], sb[q]), f"block {x} array {q} differs"
 
 
+@pytest.mark.parametrize("plan", [0, 1])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_flux"])
-def test_batch_step_equals_per_block_steps(precision):
+def test_batch_step_equals_per_block_steps(precision, plan):
     specs = bondi_smr_layout(SMALL, precision=precision)
     a, b = Batch(specs), Batch(specs)
+    a.set_plan(plan)
     for dt in DTS:
         a.step(dt)
         b.step_per_block(dt)
@@ -83,3 +86,19 @@ def test_batch_blocks_match_oracle(oracle_mod):
                 assert np.max(np.abs(got - ref)) <= 1e-12 * scale, f"block {pick[x]} variable {v}"
         assert np.array_equal(pg[sl], pflag[sl].astype(np.int32))
         assert np.array_equal(fg[sl], fflag[sl].astype(np.int32))
+
+
+@pytest.mark.parametrize("persistent", [0, 1])
+def test_fused_plan_three_launches_per_stage(persistent):
+    """The fused plan replays a step of the exchange-face Bondi mesh as 6 graph nodes (3 per stage),
+    bitwise equal to the one-launch-per-kernel plan, flat or persistent grid."""
+    specs = bondi_smr_layout(SMALL)
+    a, b = Batch(specs), Batch(specs)
+    b.set_tuning(-1, 0, persistent)
+    b.set_plan(1)
+    l0 = b.launch_count()
+    for dt in DTS:
+        a.step(dt)
+        b.step_graph(dt)
+    assert_same(a, b)
+    assert (b.launch_count() - l0) / len(DTS) == 6
