@@ -120,6 +120,9 @@ typedef struct {
      * floors); the switch points of the mixed injection frames */
     khb_floors floors_inner;
     double frame_switch_r, frame_switch_beta;
+    /* fofc/use_glf (replaced faces take the speed-of-light Lax-Friedrichs speeds, fofc.cpp:200-205) and
+     * fofc/use_source_term (the guess update also takes the geometric source, kharma_driver.cpp:308-312) */
+    int32_t fofc_use_glf, fofc_use_source_term;
 } khb_config;
 
 /* B_CT EMF schemes (b_ct.cpp:65): Balsara & Spicer 1999 flux averaging, Gardiner & Stone 2005

@@ -69,6 +69,7 @@ class KhbConfig(C.Structure):
         ("recon_lower", C.c_int32), ("recon_fallback", C.c_int32),
         ("floors_inner", KhbFloors),
         ("frame_switch_r", C.c_double), ("frame_switch_beta", C.c_double),
+        ("fofc_use_glf", C.c_int32), ("fofc_use_source_term", C.c_int32),
     ]
 
 

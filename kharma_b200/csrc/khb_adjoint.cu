@@ -670,6 +670,7 @@ int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_f
                      const khb_fields* P_np1, const khb_fields* Pbar, const khb_fields* Ubar,
                      const double* rho_flux1_weight, double weight_scale, void* stream)
 {
+    KHB_RANGE("khb_adjoint_step");
     if (!ctx || !ctx->geom_set) return set_error(KHB_ERR_STATE, "khb_adjoint_step: context without geometry");
     if (!P_n || !U_n || !P_np1 || !Pbar || !Ubar) return set_error(KHB_ERR_ARG, "khb_adjoint_step: NULL argument");
     for (int p = 0; p < ctx->nv; ++p)
@@ -696,6 +697,7 @@ int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_f
 
 int khb_flux_dot(khb_ctx* ctx, int dir, int var, const double* weight, double scale, double* out, void* stream)
 {
+    KHB_RANGE("khb_flux_dot");
     if (!ctx || !weight || !out) return set_error(KHB_ERR_ARG, "khb_flux_dot: NULL argument");
     if (dir < 1 || dir > ctx->d.ndim) return set_error(KHB_ERR_ARG, "khb_flux_dot: inactive direction");
     if (var < 0 || var >= ctx->nv) return set_error(KHB_ERR_ARG, "khb_flux_dot: bad variable");
@@ -719,6 +721,7 @@ int khb_flux_dot(khb_ctx* ctx, int dir, int var, const double* weight, double sc
 
 int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, const khb_fields* Pbar, void* stream)
 {
+    KHB_RANGE("khb_adjoint_ptou");
     if (!ctx || !ctx->geom_set) return set_error(KHB_ERR_STATE, "khb_adjoint_ptou: context without geometry");
     if (!P || !Ubar || !Pbar) return set_error(KHB_ERR_ARG, "khb_adjoint_ptou: NULL argument");
     for (int p = 0; p < ctx->nv; ++p)

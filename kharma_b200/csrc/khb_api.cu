@@ -404,6 +404,8 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
     ph.fofc = cfg->fofc;
     ph.fofc_polar_cells = cfg->fofc_polar_cells;
     ph.fofc_r_mark = cfg->r_horizon + cfg->fofc_eh_buffer;
+    ph.fofc_glf = cfg->fofc_use_glf != 0;
+    ph.fofc_source = cfg->fofc_use_source_term != 0;
     if (cfg->fofc && cfg->fofc_polar_cells < 0) { *why = "fofc_polar_cells must be >= 0"; return KHB_ERR_ARG; }
     if (cfg->ct_scheme < KHB_CT_NONE || cfg->ct_scheme > KHB_CT_GS05_C) { *why = "unknown ct_scheme"; return KHB_ERR_ARG; }
     if (cfg->ct_scheme != KHB_CT_NONE) {
@@ -612,6 +614,7 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
 
 int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream)
 {
+    KHB_RANGE("khb_get_flux");
     KHB_NEED_GEOM(ctx);
     if (dir < 1 || dir > ctx->d.ndim) return fail(KHB_ERR_ARG, "khb_get_flux: dir out of range");
     int rc;
@@ -622,6 +625,7 @@ int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream)
 int khb_fofc(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
              const khb_fields* U_0, void* stream)
 {
+    KHB_RANGE("khb_fofc");
     KHB_NEED_GEOM(ctx);
     if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_fofc: stage must be 1 or 2");
     if (!ctx->ph.fofc) return fail(KHB_ERR_STATE, "khb_fofc: the context was created with fofc off");
@@ -633,12 +637,14 @@ int khb_fofc(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const kh
 
 int khb_fix_flux(khb_ctx* ctx, void* stream)
 {
+    KHB_RANGE("khb_fix_flux");
     KHB_NEED_GEOM(ctx);
     return launch_fix_flux(ctx, ctx->ph, S(stream));
 }
 
 int khb_flux_ct(khb_ctx* ctx, void* stream)
 {
+    KHB_RANGE("khb_flux_ct");
     KHB_NEED_GEOM(ctx);
     if (ctx->nv < 8 || ctx->d.ndim < 2) return KHB_OK;
     if (ctx->fp32)
@@ -672,6 +678,7 @@ int khb_copy_flux(khb_ctx* ctx, int dir, const khb_fields* F_out, double* ctop_o
 int khb_update(khb_ctx* ctx, const khb_fields* P_s, const khb_fields* U_s, const khb_fields* U_0,
                double gam0, double gam1, double beta_dt, const khb_fields* U_out, void* stream)
 {
+    KHB_RANGE("khb_update");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
@@ -686,6 +693,7 @@ int khb_update(khb_ctx* ctx, const khb_fields* P_s, const khb_fields* U_s, const
 
 int khb_utop(khb_ctx* ctx, const khb_fields* U, const khb_fields* P, int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_utop");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
@@ -700,6 +708,7 @@ int khb_utop(khb_ctx* ctx, const khb_fields* U, const khb_fields* P, int32_t* pf
 
 int khb_apply_floors(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_apply_floors");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
@@ -714,6 +723,7 @@ int khb_apply_floors(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int
 
 int khb_fix_utop(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const int32_t* pflag, void* stream)
 {
+    KHB_RANGE("khb_fix_utop");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
@@ -731,6 +741,7 @@ int khb_fix_utop(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const i
 
 int khb_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* stream)
 {
+    KHB_RANGE("khb_boundaries");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
@@ -739,6 +750,7 @@ int khb_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void*
 
 int khb_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* stream)
 {
+    KHB_RANGE("khb_ptou");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
@@ -751,6 +763,7 @@ int khb_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const k
               const khb_fields* U_0, const khb_fields* P_out, const khb_fields* U_out,
               int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_stage");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_stage: a B_CT block steps with khb_ct_stage/khb_ct_step");
     if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_stage: stage must be 1 or 2");
@@ -766,6 +779,7 @@ int khb_zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, con
                   const khb_fields* U_0, const khb_fields* P_out, const khb_fields* U_out,
                   int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_zone_pass");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_zone_pass: a B_CT block steps with khb_ct_stage/khb_ct_step");
     if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_zone_pass: stage must be 1 or 2");
@@ -779,6 +793,7 @@ int khb_zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, con
 
 int khb_fix_utop_list(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const int32_t* pflag, void* stream)
 {
+    KHB_RANGE("khb_fix_utop_list");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_fields(ctx, U, "U")) || (rc = check_fields(ctx, P, "P"))) return rc;
@@ -789,6 +804,7 @@ int khb_fix_utop_list(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, co
 int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
              int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_step");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step: a B_CT block steps with khb_ct_stage/khb_ct_step");
     int rc;
@@ -808,6 +824,7 @@ int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, cons
                  const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
                  const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_ct_stage");
     KHB_NEED_GEOM(ctx);
     if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_stage: block is not B_CT (cfg.ct_scheme)");
     if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_ct_stage: stage must be 1 or 2");
@@ -823,6 +840,7 @@ int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, cons
 
 int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf, void* stream)
 {
+    KHB_RANGE("khb_ct_boundaries");
     KHB_NEED_GEOM(ctx);
     if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_boundaries: block is not B_CT (cfg.ct_scheme)");
     int rc;
@@ -834,6 +852,7 @@ int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, co
 int khb_ct_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
                 int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_ct_step");
     KHB_NEED_GEOM(ctx);
     if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_step: block is not B_CT (cfg.ct_scheme)");
     int rc;
@@ -878,6 +897,7 @@ int khb_get_timestep(khb_ctx* ctx, double* dt_next, double* t, double* dt_last, 
 int khb_step_device_dt(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag,
                        void* stream)
 {
+    KHB_RANGE("khb_step_device_dt");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_device_dt: a B_CT block steps with khb_ct_stage/khb_ct_step");
     if (!ctx->dt_state) return fail(KHB_ERR_STATE, "khb_step_device_dt: no device timestep (khb_set_timestep)");
@@ -903,6 +923,7 @@ int khb_step_device_dt(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, i
 int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32_t* pflag, int32_t* fflag,
                    void* stream)
 {
+    KHB_RANGE("khb_step_graph");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_graph: a B_CT block steps with khb_ct_stage/khb_ct_step");
     cudaStream_t st = S(stream);
@@ -935,6 +956,7 @@ int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32
 int khb_step_host(khb_ctx* ctx, double* const* P_host, const khb_fields* P, const khb_fields* U, int32_t* pflag,
                   int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_step_host");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_host: a B_CT block steps with khb_ct_stage/khb_ct_step");
     int rc;
@@ -957,6 +979,7 @@ int khb_step_host(khb_ctx* ctx, double* const* P_host, const khb_fields* P, cons
 int khb_step_host_interior(khb_ctx* ctx, double* const* P_host, const khb_fields* P, const khb_fields* U,
                            int32_t* pflag, int32_t* fflag, void* stream)
 {
+    KHB_RANGE("khb_step_host_interior");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_step_host_interior: a B_CT block steps with khb_ct_stage/khb_ct_step");
     if (has_exchange_face(ctx->d))
@@ -1001,6 +1024,7 @@ int khb_get_min_ndt(khb_ctx* ctx, double* min_ndt_host, void* stream)
 
 int khb_max_divb(khb_ctx* ctx, const khb_fields* U, double* max_divb_host, void* stream)
 {
+    KHB_RANGE("khb_max_divb");
     KHB_NEED_GEOM(ctx);
     if (!U || !max_divb_host) return fail(KHB_ERR_ARG, "khb_max_divb: NULL argument");
     if (ctx->nv < 8 || ctx->d.ndim < 2) { *max_divb_host = 0.; return KHB_OK; }
@@ -1078,6 +1102,7 @@ int khb_set_connection(khb_ctx* ctx, const double* conn)
 
 int khb_emhd_ptou(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* U, void* stream)
 {
+    KHB_RANGE("khb_emhd_ptou");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_emhd(emhd)) || (rc = check_fields10(emhd, P, "P")) || (rc = check_fields10(emhd, U, "U"))) return rc;
@@ -1090,6 +1115,7 @@ int khb_emhd_ptou(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P
 int khb_emhd_add_source(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* dUdt,
                         void* stream)
 {
+    KHB_RANGE("khb_emhd_add_source");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_emhd(emhd)) || (rc = check_fields10(emhd, P, "P")) || (rc = check_fields10(emhd, dUdt, "dUdt")))
@@ -1131,6 +1157,7 @@ int khb_implicit_step(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_impli
                       const khb_fields* src, const khb_fields* P_solver, double* solve_norm, double* solve_fail,
                       double dt, void* stream)
 {
+    KHB_RANGE("khb_implicit_step");
     KHB_NEED_GEOM(ctx);
     ImpFields f;
     int rc;
@@ -1180,6 +1207,7 @@ khb_fields fields_of(double* base, long long N)
 
 int khb_get_flux_emhd(khb_ctx* ctx, const khb_emhd_params* emhd, int dir, const khb_fields* P, void* stream)
 {
+    KHB_RANGE("khb_get_flux_emhd");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = emhd_flux_ready(ctx, emhd, "khb_get_flux_emhd")) || (rc = check_fields10(emhd, P, "P"))) return rc;
@@ -1211,6 +1239,7 @@ int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit
                    const khb_fields* P_out, const khb_fields* U_out, double* solve_norm, double* solve_fail,
                    void* stream)
 {
+    KHB_RANGE("khb_imex_stage");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: EMHD with B_CT is not supported");
     int rc;
@@ -1279,6 +1308,7 @@ int khb_implicit_jacobian(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_i
                           const khb_fields* src, const khb_fields* P_solver, double dt, double* jacobian,
                           double* residual, void* stream)
 {
+    KHB_RANGE("khb_implicit_jacobian");
     KHB_NEED_GEOM(ctx);
     ImpFields f;
     int rc;
@@ -1294,6 +1324,7 @@ int khb_implicit_jacobian(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_i
 int khb_fix_solve(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_fields* P, const khb_fields* U,
                   const double* solve_fail, void* stream)
 {
+    KHB_RANGE("khb_fix_solve");
     KHB_NEED_GEOM(ctx);
     int rc;
     if ((rc = check_emhd(emhd)) || (rc = check_fields10(emhd, P, "P")) || (rc = check_fields10(emhd, U, "U"))) return rc;

@@ -531,6 +531,7 @@ int khb_batch_set_mesh(khb_batch* b, const int32_t* ghost, int64_t n_ghost, int6
 
 int khb_batch_mesh_exchange(khb_batch* b, void* stream)
 {
+    KHB_RANGE("khb_batch_mesh_exchange");
     if (!b) return set_error(KHB_ERR_ARG, "khb_batch_mesh_exchange: NULL batch");
     if (b->n_ghost) {
         enqueue_mesh_ghost(b, 2, S(stream));
@@ -541,6 +542,7 @@ int khb_batch_mesh_exchange(khb_batch* b, void* stream)
 
 int khb_batch_step(khb_batch* b, double dt, void* stream)
 {
+    KHB_RANGE("khb_batch_step");
     if (!b) return set_error(KHB_ERR_ARG, "khb_batch_step: NULL batch");
     int rc;
     if ((rc = upload_dt(b, dt, S(stream)))) return rc;
@@ -550,6 +552,7 @@ int khb_batch_step(khb_batch* b, double dt, void* stream)
 
 int khb_batch_step_graph(khb_batch* b, double dt, void* stream)
 {
+    KHB_RANGE("khb_batch_step_graph");
     if (!b) return set_error(KHB_ERR_ARG, "khb_batch_step_graph: NULL batch");
     cudaStream_t st = S(stream);
     if (!st) return set_error(KHB_ERR_ARG, "khb_batch_step_graph: needs a non-default stream to capture");
@@ -609,6 +612,7 @@ int khb_batch_set_tuning(khb_batch* b, int size_class, int kz, int persistent)
 
 int khb_batch_autotune(khb_batch* b, int reps, int32_t* kz_out, int32_t* persistent_out, void* stream)
 {
+    KHB_RANGE("khb_batch_autotune");
     if (!b || reps < 1) return set_error(KHB_ERR_ARG, "khb_batch_autotune: bad argument");
     cudaStream_t st = S(stream);
     int rc;

@@ -468,6 +468,7 @@ extern "C" {
 
 int khb_ct_utop(khb_ctx* ctx, const khb_fields* Bf, const khb_fields* P, const khb_fields* U, void* stream)
 {
+    KHB_RANGE("khb_ct_utop");
     int rc;
     if ((rc = ct_check(ctx, "khb_ct_utop"))) return rc;
     if (!faces_ok(Bf) || !P || !U) return set_error(KHB_ERR_ARG, "khb_ct_utop: NULL argument");
@@ -480,6 +481,7 @@ int khb_ct_utop(khb_ctx* ctx, const khb_fields* Bf, const khb_fields* P, const k
 
 int khb_ct_faces_from_prims(khb_ctx* ctx, const khb_fields* P, const khb_fields* Bf, void* stream)
 {
+    KHB_RANGE("khb_ct_faces_from_prims");
     int rc;
     if ((rc = ct_check(ctx, "khb_ct_faces_from_prims"))) return rc;
     if (!faces_ok(Bf) || !P) return set_error(KHB_ERR_ARG, "khb_ct_faces_from_prims: NULL argument");
@@ -492,6 +494,7 @@ int khb_ct_faces_from_prims(khb_ctx* ctx, const khb_fields* P, const khb_fields*
 
 int khb_ct_max_divb(khb_ctx* ctx, const khb_fields* Bf, double* max_divb_host, void* stream)
 {
+    KHB_RANGE("khb_ct_max_divb");
     int rc;
     if ((rc = ct_check(ctx, "khb_ct_max_divb"))) return rc;
     if (!faces_ok(Bf) || !max_divb_host) return set_error(KHB_ERR_ARG, "khb_ct_max_divb: NULL argument");

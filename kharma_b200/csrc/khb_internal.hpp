@@ -6,6 +6,19 @@
 
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
+// A named NVTX range around one C-ABI call, the counterpart of the reference's Flag/EndFlag timer
+// regions (types.hpp:286-293): it shows each call on a profiler's timeline and costs a test of an
+// unset pointer when no profiler is attached (header-only NVTX v3, no library to link)
+struct KhbRange {
+    explicit KhbRange(const char* name) { nvtxRangePushA(name); }
+    ~KhbRange() { nvtxRangePop(); }
+    KhbRange(const KhbRange&) = delete;
+    KhbRange& operator=(const KhbRange&) = delete;
+};
+#define KHB_RANGE(name) KhbRange khb_range_scope_(name)
+
 struct khb_ctx {
     khb_config cfg;
     khb::Dims d;

@@ -393,6 +393,30 @@ __device__ __forceinline__ void ct_zone_b(const Dims& d, const DevGeom& g, const
                          : __ldg(Bf[2] + c) / __ldg(g.gdet[2] + gi);
 }
 
+// The geometric source of one zone (flux.cpp:413-441): new_du[lam] = sum over mu, nu of
+// T^mu_nu gdet Gamma^nu_lam mu for the UU and U1-U3 components, from the zone's primitives Ps
+template <int NV>
+__device__ __forceinline__ void geo_source(const Dims& d, const DevGeom& g, const ZoneGeom& G, double gam,
+                                           const double* Ps, int j, int i, double new_du[4])
+{
+    FourVec<double> D;
+    const double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
+    calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, Ps, D);
+#pragma unroll
+    for (int lam = 0; lam < 4; ++lam) new_du[lam] = 0.;
+    const long long cg = (long long)j*g.n1 + i, cs = (long long)(d.n2)*g.n1;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        double Tmu[4];
+        calc_tensor<double, (NV > 5)>(Ps[0], Ps[1], (gam - 1) * Ps[1], D, mu, Tmu);
+#pragma unroll
+        for (int nu = 0; nu < 4; ++nu)
+#pragma unroll
+            for (int lam = 0; lam < 4; ++lam)
+                new_du[lam] += Tmu[nu] * __ldg(g.gdet_conn + ((nu*4 + lam)*4 + mu)*cs + cg);
+    }
+}
+
 // MODE: compile-time mask of M_* steps (0: take the mask from the arguments at run time).  The
 // CFL reduction (M_DT) is always a run-time choice.
 // One zone of the zone pass; returns the zone's timestep for the CFL minimum (DBL_MAX if none)
@@ -453,21 +477,8 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
                 double Ps[NV];
 #pragma unroll
                 for (int p = 0; p < NV; ++p) Ps[p] = __ldg(a.Ps.v[p] + c);
-                FourVec<double> D;
-                const double gcon0[4] = {G.gcon[0][0], G.gcon[0][1], G.gcon[0][2], G.gcon[0][3]};
-                calc_4vecs<double, (NV > 5)>(G.gcov, G.gcon[0][0], gcon0, Ps, D);
-                double new_du[4] = {0., 0., 0., 0.};
-                const long long cg = (long long)j*g.n1 + i, cs = (long long)(d.n2)*g.n1;
-#pragma unroll
-                for (int mu = 0; mu < 4; ++mu) {
-                    double Tmu[4];
-                    calc_tensor<double, (NV > 5)>(Ps[0], Ps[1], (gam - 1) * Ps[1], D, mu, Tmu);
-#pragma unroll
-                    for (int nu = 0; nu < 4; ++nu)
-#pragma unroll
-                        for (int lam = 0; lam < 4; ++lam)
-                            new_du[lam] += Tmu[nu] * __ldg(g.gdet_conn + ((nu*4 + lam)*4 + mu)*cs + cg);
-                }
+                double new_du[4];
+                geo_source<NV>(d, g, G, gam, Ps, j, i, new_du);
                 dudt[1] += new_du[0];
                 dudt[2] += new_du[1];
                 dudt[3] += new_du[2];
@@ -632,16 +643,26 @@ __global__ void __launch_bounds__(128) k_fofc_guess(Dims d, DevGeom g, Phys ph, 
     const double vol = ph.dx1*ph.dx2*ph.dx3;
     ZoneGeom G;
     load_zone_geom(g, j, i, G);
-    double Ug[NV], Pg[NV];
+    double Ug[NV], Pg[NV], dudt[NV];
 #pragma unroll
     for (int p = 0; p < NV; ++p) {
         double du = (a1 * ldf(F1, p*N + c + 1) - a1 * ldf(F1, p*N + c));
         if (d.ndim >= 2) du += a2 * ldf(F2, p*N + c + sj) - a2 * ldf(F2, p*N + c);
         if (d.ndim == 3) du += a3 * ldf(F3, p*N + c + sk) - a3 * ldf(F3, p*N + c);
-        const double dudt = -du / vol;
-        const double x = g0 * Us.v[p][c] + g1 * U0.v[p][c];
-        Ug[p] = 1.0 * x + bdt * dudt;
+        dudt[p] = -du / vol;
         Pg[p] = Ps.v[p][c];
+    }
+    // fofc/use_source_term: the guess also takes the geometric source of P_s (kharma_driver.cpp:308-312)
+    if (ph.fofc_source && !ph.cart_minkowski) {
+        double new_du[4];
+        geo_source<NV>(d, g, G, ph.gam, Pg, j, i, new_du);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) dudt[1 + v] += new_du[v];
+    }
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        const double x = g0 * Us.v[p][c] + g1 * U0.v[p][c];
+        Ug[p] = 1.0 * x + bdt * dudt[p];
     }
     if (NV > 5) {
 #pragma unroll
@@ -721,8 +742,9 @@ __global__ void __launch_bounds__(128) k_fofc_replace(Dims d, DevGeom g, Phys ph
     prim_to_flux<R, NV>(Pr, D, gam, gdet, 0, Ur);
     prim_to_flux<R, NV>(Pr, D, gam, gdet, DIR, Fr);
     vchar<R, HAS_B>(Pr, D, gam, gcon0[0], gcon0[DIR], gcondd, DIR, cmaxR, cminR);
-    const R cmax = kmax(kmax(R(0), cmaxL), cmaxR);
-    const R cmin = -kmin(kmin(R(0), cminL), cminR);
+    // fofc/use_glf: the speed-of-light Lax-Friedrichs speeds (fofc.cpp:200-205)
+    const R cmax = ph.fofc_glf ? R(1) : kmax(kmax(R(0), cmaxL), cmaxR);
+    const R cmin = ph.fofc_glf ? R(1) : -kmin(kmin(R(0), cminL), cminR);
     const R ctp = kmax(cmax, cmin);
 #pragma unroll
     for (int p = 0; p < NV; ++p) F[p*d.N + c] = (FT)(R(0.5) * (Fl[p] + Fr[p] - ctp * (Ur[p] - Ul[p])));

@@ -60,6 +60,7 @@ struct Phys {
     Prescription fl;
     Prescription fl_inner;                 // r < fl.floors_switch_r when fl.radius_dependent_floors
     double frame_switch_r, frame_switch_beta;
+    int fofc_glf, fofc_source;             // fofc/use_glf, fofc/use_source_term
 };
 
 enum { M_UPDATE = 1, M_UTOP = 2, M_FLOORS = 4, M_PTOU = 8, M_DT = 16, M_FAILLIST = 32 };

@@ -99,6 +99,8 @@ class BlockSpec:
     fofc: bool = False
     fofc_polar_cells: int = 0
     fofc_eh_buffer: float = 0.1
+    fofc_use_glf: bool = False               # fofc/use_glf: speed-of-light LF speeds on replaced faces
+    fofc_use_source_term: bool = False       # fofc/use_source_term: the guess takes the geometric source
     # magnetic field transport (b_field/solver, b_field/ct_scheme): "none" = B_FluxCT (cell-centred B);
     # "bs99", "gs05_0", "gs05_c" ("sg07") = B_CT with a face-centred field
     b_ct: str = "none"
@@ -168,6 +170,7 @@ class BlockSpec:
         c.frame_switch_r, c.frame_switch_beta = self.frame_switch_r, self.frame_switch_beta
         c.inverter = _lib.INVERTER[self.inverter]
         c.fofc, c.fofc_polar_cells, c.fofc_eh_buffer = int(self.fofc), self.fofc_polar_cells, self.fofc_eh_buffer
+        c.fofc_use_glf, c.fofc_use_source_term = int(self.fofc_use_glf), int(self.fofc_use_source_term)
         c.r_horizon = self.r_horizon
         c.ct_scheme = _lib.CT_SCHEME[self.b_ct]
         c.recon_lower = 1 if self.low_order_edges else (2 if self.low_order_poles else 0)

@@ -105,6 +105,7 @@ struct Config {
     int32_t recon_fallback;                         // flux/reconstruction_fallback
     Prescription floors_inner;                      // floors_inner (floors.hpp:155-167)
     double frame_switch_r, frame_switch_beta;       // floors/frame_switch_r, floors/frame_switch_beta
+    int32_t fofc_use_glf, fofc_use_source_term;     // fofc/use_glf, fofc/use_source_term
 };
 
 // ---------------------------------------------------------------- coordinates
@@ -984,6 +985,22 @@ static void flux_divergence(const Block& B, double* F[3], double* dudt)
     }
 }
 // flux.cpp:395-444
+// The geometric source T^mu_lam gdet Gamma^lam_nu mu of one zone (flux.cpp:413-441) into new_du[4]
+// (the UU and U1-U3 components)
+static void geo_source_cell(const Block& B, const double* Pc, int j, int i, double new_du[4])
+{
+    FourVectors D;
+    calc_4vecs(B, Pc, B.nv > 5, j, i, center, D);
+    double Tmu[4] = {0};
+    for (int x = 0; x < 4; ++x) new_du[x] = 0.;
+    for (int mu = 0; mu < 4; ++mu) {
+        calc_tensor(Pc[0], Pc[1], (B.c.gam - 1) * Pc[1], D, mu, B.nv > 5, Tmu);
+        for (int nu = 0; nu < 4; ++nu)
+            for (int lam = 0; lam < 4; ++lam)
+                new_du[lam] += Tmu[nu] * B.GdetConn(j, i, nu, lam, mu);
+    }
+}
+
 static void add_geo_source(const Block& B, const double* P, double* dudt)
 {
     if (B.C.cart_minkowski()) return;
@@ -993,15 +1010,8 @@ static void add_geo_source(const Block& B, const double* P, double* dudt)
         const size_t c = B.id(k, j, i);
         double Pc[8];
         for (int p = 0; p < B.nv; ++p) Pc[p] = P[(size_t)p*N + c];
-        FourVectors D;
-        calc_4vecs(B, Pc, B.nv > 5, j, i, center, D);
-        double Tmu[4] = {0}, new_du[4] = {0};
-        for (int mu = 0; mu < 4; ++mu) {
-            calc_tensor(Pc[0], Pc[1], (B.c.gam - 1) * Pc[1], D, mu, B.nv > 5, Tmu);
-            for (int nu = 0; nu < 4; ++nu)
-                for (int lam = 0; lam < 4; ++lam)
-                    new_du[lam] += Tmu[nu] * B.GdetConn(j, i, nu, lam, mu);
-        }
+        double new_du[4];
+        geo_source_cell(B, Pc, j, i, new_du);
         dudt[1*N + c] += new_du[0];
         for (int v = 0; v < 3; ++v) dudt[(size_t)(2 + v)*N + c] += new_du[1 + v];
     }
@@ -1756,16 +1766,26 @@ static void fofc_correct(const Block& B, Fields& f, int s, double dt, const doub
 #pragma omp parallel for collapse(2) schedule(dynamic, 4)
     for (int k = k0; k <= k1; ++k) for (int j = j0; j <= j1; ++j) for (int i = i0; i <= i1; ++i) {
         const size_t c = B.id(k, j, i);
-        double Ug[8], Pg[8];
+        double Ug[8], Pg[8], dudt[8];
         for (size_t p = 0; p < nv; ++p) {
             const size_t pc = p*N + c;
             double du = (a1 * f.F[0][pc + 1] - a1 * f.F[0][pc]);
             if (B.ndim >= 2) du += a2 * f.F[1][pc + sj] - a2 * f.F[1][pc];
             if (B.ndim == 3) du += a3 * f.F[2][pc + sk] - a3 * f.F[2][pc];
-            const double dudt = -du / vol;
-            double x = g0 * U_s[pc] + g1 * U_0[pc];
-            Ug[p] = 1.0 * x + bdt * dudt;
+            dudt[p] = -du / vol;
             Pg[p] = P_s[pc];
+        }
+        // fofc/use_source_term: the guess also takes the geometric source of P_s
+        // (kharma_driver.cpp:308-312, over the entire block)
+        if (B.c.fofc_use_source_term && !B.C.cart_minkowski()) {
+            double new_du[4];
+            geo_source_cell(B, Pg, j, i, new_du);
+            for (int v = 0; v < 4; ++v) dudt[1 + v] += new_du[v];
+        }
+        for (size_t p = 0; p < nv; ++p) {
+            const size_t pc = p*N + c;
+            double x = g0 * U_s[pc] + g1 * U_0[pc];
+            Ug[p] = 1.0 * x + bdt * dudt[p];
         }
         if (nv > 5) for (int v = 0; v < 3; ++v) Pg[5 + v] = Ug[5 + v] / B.Gdet(center, j, i);
         const int pf = u_to_p(B, Ug, Pg, j, i, center, B.c.iter_max, B.c.err_tol);
@@ -1815,8 +1835,9 @@ static void fofc_correct(const Block& B, Fields& f, int s, double dt, const doub
             prim_to_flux(B, Pr, Dr, j, i, 0, Ur, loc);
             prim_to_flux(B, Pr, Dr, j, i, dir, Fr, loc);
             vchar(B, Pr, Dr, j, i, loc, dir, cmaxR, cminR);
-            const double cmax = kmax(kmax(0., cmaxL), cmaxR);
-            const double cmin = -kmin(kmin(0., cminL), cminR);
+            // fofc/use_glf: the global (speed of light) Lax-Friedrichs speeds on replaced faces (fofc.cpp:200-205)
+            const double cmax = B.c.fofc_use_glf ? 1. : kmax(kmax(0., cmaxL), cmaxR);
+            const double cmin = B.c.fofc_use_glf ? 1. : -kmin(kmin(0., cminL), cminR);
             f.cmax[dir-1][c] = cmax;
             f.cmin[dir-1][c] = cmin;
             for (size_t p = 0; p < nv; ++p) f.F[dir-1][p*N + c] = llf(Fl[p], Fr[p], cmax, cmin, Ul[p], Ur[p]);

@@ -55,6 +55,7 @@ class Config(C.Structure):
         ("recon_lower", C.c_int32), ("recon_fallback", C.c_int32),
         ("floors_inner", Prescription),
         ("frame_switch_r", C.c_double), ("frame_switch_beta", C.c_double),
+        ("fofc_use_glf", C.c_int32), ("fofc_use_source_term", C.c_int32),
     ]
 
 
@@ -164,6 +165,7 @@ def config_from_spec(spec):
         setattr(c.floors, name, type(getattr(c.floors, name))(getattr(spec.floors, name)))
         setattr(c.floors_inner, name, type(getattr(c.floors_inner, name))(getattr(inner, name)))
     c.frame_switch_r, c.frame_switch_beta = spec.frame_switch_r, spec.frame_switch_beta
+    c.fofc_use_glf, c.fofc_use_source_term = int(spec.fofc_use_glf), int(spec.fofc_use_source_term)
     return c
 
 

@@ -3,6 +3,8 @@
 Tolerance for the FP64 path: for every variable v, max |x_gpu - x_oracle| <= 1e-12 * max |x_oracle,v|
 (per-variable relative L-infinity).  Inversion and floor flags must agree bit for bit.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -123,6 +125,9 @@ FULL = {
     # first-order flux correction on (the production SANE deck's setting, pars/tori_3d/sane.par:80-81)
     "torus3d_mc_fofc": lambda: torus_spec(32, 24, 8, fofc=True),
     "torus3d_mc_128_fofc": lambda: torus_spec(128, 128, 128, fofc=True),
+    # the FOFC options: speed-of-light LF speeds on replaced faces, geometric source in the guess
+    "torus3d_mc_fofc_glf": lambda: dataclasses.replace(torus_spec(32, 24, 8, fofc=True), fofc_use_glf=True),
+    "torus3d_mc_fofc_src": lambda: dataclasses.replace(torus_spec(32, 24, 8, fofc=True), fofc_use_source_term=True),
 }
 CASES.update(FULL)
 
@@ -130,7 +135,8 @@ CASES.update(FULL)
 @pytest.mark.parametrize("name,nsteps", [("mhdmodes3d_weno5", 10), ("mhdmodes2d_ppm_hlle", 10), ("torus3d_mc", 5),
                                          ("mhdmodes3d_weno5_64", 10), ("torus3d_mc_128", 3),
                                          ("torus2d_mc_128", 10), ("torus3d_mc_kastaun", 10),
-                                         ("torus3d_mc_fofc", 10), ("torus3d_mc_128_fofc", 3)])
+                                         ("torus3d_mc_fofc", 10), ("torus3d_mc_128_fofc", 3),
+                                         ("torus3d_mc_fofc_glf", 10), ("torus3d_mc_fofc_src", 10)])
 def test_step_parity(oracle_mod, name, nsteps):
     spec = CASES[name]()
     o, b, Po, Uo = make_pair(oracle_mod, spec, initial(oracle_mod, name, spec))
