@@ -223,6 +223,21 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
         LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask);
         KHB_LAUNCHED(ctx);
     }
+    // X3 faces last (Parthenon's face order), over the whole (j, i) plane: their ghost planes copy
+    // the boundary planes with the X1/X2 ghost zones already filled; then B_P and U = U(P) there
+    int kplanes = 0;
+    if (d.ndim >= 3) {
+        for (int face = 4; face < 6; ++face) {
+            if (!phys_face(d.bc[face])) continue;
+            kplanes |= 1 << (face - 4);
+            LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, 0, d.n1 * d.n2, 0, 1, st);
+            KHB_LAUNCHED(ctx);
+        }
+        if (kplanes) {
+            LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st, nullptr, 0, kplanes);
+            KHB_LAUNCHED(ctx);
+        }
+    }
     int pmask = 0;
     if (d.bc[0] == KHB_BC_PERIODIC) pmask |= 1;
     if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) pmask |= 2;

@@ -857,29 +857,37 @@ __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int
 {
     const int bdir = face / 2 + 1;
     const bool inner = (face % 2) == 0;
-    const int ng = (bdir == 1) ? d.is : d.js;
+    const int ng = (bdir == 1) ? d.is : ((bdir == 2) ? d.js : d.ks);
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ng*cnt_a*cnt_k) return;
     const int gidx = (int)(t % ng);
     const long long r = t / ng;
     const int aidx = lo_a + (int)(r % cnt_a);
-    const int k = lo_k + (int)(r / cnt_a);
-    int i, j, ref;
+    int i, j, k, ref;
     if (bdir == 1) {
         j = aidx;
+        k = lo_k + (int)(r / cnt_a);
         ref = inner ? d.is : d.ie;
         i = inner ? gidx : d.ie + 1 + gidx;
-    } else {
+    } else if (bdir == 2) {
         i = aidx;
+        k = lo_k + (int)(r / cnt_a);
         ref = inner ? d.js : d.je;
         j = inner ? gidx : d.je + 1 + gidx;
+    } else {
+        // X3 faces: a runs over the whole (j, i) plane
+        j = aidx / d.n1;
+        i = aidx - j * d.n1;
+        ref = inner ? d.ks : d.ke;
+        k = inner ? gidx : d.ke + 1 + gidx;
     }
     const int type = d.bc[face];
     const int offset = 2 * ref + (inner ? -1 : 1);
     const bool transmit = type == KHB_BC_TRANSMITTING;
     int ii = i, jj = j, kk = k;
-    if (bdir == 1) ii = (type == KHB_BC_OUTFLOW) ? ref : offset - i;
-    else           jj = (type == KHB_BC_OUTFLOW) ? ref : offset - j;
+    if (bdir == 1)      ii = (type == KHB_BC_OUTFLOW) ? ref : offset - i;
+    else if (bdir == 2) jj = (type == KHB_BC_OUTFLOW) ? ref : offset - j;
+    else                kk = (type == KHB_BC_OUTFLOW) ? ref : offset - k;
     // transmitting: the mirrored zone half-way round in x3 (one_block_transmit.cpp:116-134)
     if (transmit) kk = ((k - d.ks + d.nx3 / 2) % d.nx3) + d.ks;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
@@ -936,16 +944,29 @@ __host__ __device__ inline unsigned plane_ghost_count(const Dims& d)
 // 0: X1, bit 1: X2) takes B from its faces (B_CT::BlockUtoP over the boundary domain, b_ct.cpp:
 // 160-188); the last ghost layer of a direction has its lower face only (the face array stops
 // there) and takes B from that face alone.
+// kplanes: the ghost planes of physical X3 faces instead (whole (j, i) planes below ks and above ke)
 template <int NV>
-__global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, khb_fields Bf, int ct_mask)
+__global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, khb_fields Bf, int ct_mask,
+                             int kplanes)
 {
-    const unsigned per = plane_ghost_count(d);
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned kk = t / per;
-    if (kk >= (unsigned)(d.ke - d.ks + 1)) return;
-    int j, i;
-    if (!plane_ghost(d, t - kk * per, j, i)) return;
-    const int k = d.ks + (int)kk;
+    int j, i, k;
+    if (kplanes) {
+        const unsigned plane = (unsigned)(d.n1 * d.n2);
+        const unsigned kp = t / plane, r = t - kp * plane;
+        const unsigned below = (kplanes & 1) ? (unsigned)d.ks : 0u;
+        const unsigned above = (kplanes & 2) ? (unsigned)(d.n3 - 1 - d.ke) : 0u;
+        if (kp >= below + above) return;
+        k = (kp < below) ? (int)kp : d.ke + 1 + (int)(kp - below);
+        j = (int)(r / (unsigned)d.n1);
+        i = (int)(r - (unsigned)j * (unsigned)d.n1);
+    } else {
+        const unsigned per = plane_ghost_count(d);
+        const unsigned kk = t / per;
+        if (kk >= (unsigned)(d.ke - d.ks + 1)) return;
+        if (!plane_ghost(d, t - kk * per, j, i)) return;
+        k = d.ks + (int)kk;
+    }
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     ZoneGeom G;
     load_zone_geom(g, j, i, G);
@@ -1752,22 +1773,24 @@ void LaunchCommon::fixup(int nv, const Dims& d, const DevGeom& g, const Phys& ph
 void LaunchCommon::bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
                       int face, int lo_a, int cnt_a, int lo_k, int cnt_k, cudaStream_t st)
 {
-    const int ng = (face < 2) ? d.is : d.js;
+    const int ng = (face < 2) ? d.is : ((face < 4) ? d.js : d.ks);
     const unsigned nb = blocks_for((long long)ng*cnt_a*cnt_k, 128);
     if (nv == 8) k_bc<8><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
     else k_bc<5><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
 }
 
 void LaunchCommon::ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
-                              const khb_fields& U, cudaStream_t st, const khb_fields* Bf, int ct_mask)
+                              const khb_fields& U, cudaStream_t st, const khb_fields* Bf, int ct_mask, int kplanes)
 {
-    const long long tot = (long long)plane_ghost_count(d)*(d.ke - d.ks + 1);
+    const long long plane = (long long)d.n1 * d.n2;
+    const long long tot = kplanes ? plane * (((kplanes & 1) ? d.ks : 0) + ((kplanes & 2) ? d.n3 - 1 - d.ke : 0))
+                                  : (long long)plane_ghost_count(d)*(d.ke - d.ks + 1);
     if (tot == 0) return;
     khb_fields F;
     for (int x = 0; x < KHB_MAX_VARS; ++x) F.v[x] = nullptr;
     if (Bf) for (int x = 0; x < 3; ++x) F.v[x] = Bf->v[x];
-    if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask);
-    else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask);
+    if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes);
+    else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes);
 }
 
 void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st)

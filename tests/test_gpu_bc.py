@@ -46,3 +46,34 @@ def test_transmitting_ghosts_are_mirrored_images():
             ki = ((k - ng + n3 // 2) % n3) + ng
             assert np.array_equal(P[:5, k, jg, ng:-ng], sp * P[:5, ki, js, ng:-ng])
             assert np.array_equal(U[5:, k, jg, ng:-ng], sb * U[5:, ki, js, ng:-ng])
+
+
+# Physical X3 faces (KBoundaries on inner/outer_x3, boundaries.cpp:369-589; Parthenon's face order
+# x1, x2, x3): the X3 ghost planes copy (outflow) or mirror with u^3 and B^3 inverted (reflecting)
+# the boundary planes over the whole (j, i) plane, after the X1/X2 faces.
+X3_CASES = {
+    "outflow": ("periodic", "periodic", "periodic", "periodic", "outflow", "outflow"),
+    "reflecting": ("periodic", "periodic", "periodic", "periodic", "reflecting", "reflecting"),
+    "mixed": ("outflow", "outflow", "periodic", "periodic", "reflecting", "outflow"),
+}
+
+
+@pytest.mark.parametrize("name", list(X3_CASES))
+def test_x3_physical_faces_match_oracle(oracle_mod, name):
+    from kharma_b200.spec import mhdmodes_spec
+    spec = dataclasses.replace(mhdmodes_spec(16, 12, 12, recon="linear_mc"), bc=X3_CASES[name])
+    # seeded smooth ramps on every variable, so that the state varies along x3 and u^3, B^3 are nonzero
+    P0 = problems.add_ramps(spec, problems.mhdmodes(spec, 3, amp=1e-2))
+    o, b, Po, Uo = make_pair(oracle_mod, spec, P0)
+    worst, flags_equal = run_steps(o, b, Po, Uo, 5, spec)
+    assert np.all(worst <= RTOL), worst
+    assert flags_equal
+    # the ghost planes themselves, after the last step's boundaries
+    P, U = b.P.cpu().numpy(), b.U.cpu().numpy()
+    assert np.max(np.abs(P - Po)) <= RTOL * np.max(np.abs(Po))
+    assert np.max(np.abs(U - Uo)) <= RTOL * np.max(np.abs(Uo))
+    ng, ke = spec.ng, spec.ng + spec.nx3 - 1
+    if name == "reflecting":
+        for g in range(ng):
+            assert np.array_equal(P[4, ng - 1 - g], -P[4, ng + g])          # u^3 inverted
+            assert np.array_equal(P[0, ke + 1 + g], P[0, ke - g])
