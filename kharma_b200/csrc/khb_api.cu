@@ -194,6 +194,7 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
     if (Bf) {
         if (phys_face(d.bc[0])) ct_mask |= 1;
         if (d.ndim >= 2 && phys_face(d.bc[2])) ct_mask |= 2;
+        if (d.ndim >= 3 && phys_face(d.bc[4])) ct_mask |= 4;
         if (!ct_mask) Bf = nullptr;
     }
     if (Bf) {
@@ -234,7 +235,7 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
             KHB_LAUNCHED(ctx);
         }
         if (kplanes) {
-            LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st, nullptr, 0, kplanes);
+            LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask, kplanes);
             KHB_LAUNCHED(ctx);
         }
     }
@@ -430,11 +431,10 @@ int khb::derive_block(const khb_config* cfg, Dims& d, Phys& ph, const char** why
         for (int f = 0; f < 2 * d.ndim; ++f) {
             if (!phys_face(cfg->bc[f])) continue;
             physical = true;
-            // b_ct_boundaries.cpp: outflow (clean_face_B), reflecting (reflect_face_vector,
-            // zero_EMF) and transmitting (average_EMF, X2 faces only as for the zones) X1/X2 faces
-            if (f >= 4 || (cfg->bc[f] != KHB_BC_OUTFLOW && cfg->bc[f] != KHB_BC_REFLECTING &&
-                           cfg->bc[f] != KHB_BC_TRANSMITTING)) {
-                *why = "B_CT blocks take outflow, reflecting or transmitting X1/X2 faces, periodic or exchange faces otherwise";
+            // b_ct_boundaries.cpp: outflow (clean_face_B) and reflecting (reflect_face_vector,
+            // zero_EMF) faces in every direction, transmitting (average_EMF) X2 faces as for the zones
+            if (cfg->bc[f] != KHB_BC_OUTFLOW && cfg->bc[f] != KHB_BC_REFLECTING && cfg->bc[f] != KHB_BC_TRANSMITTING) {
+                *why = "B_CT blocks take outflow, reflecting or transmitting faces, periodic or exchange faces otherwise";
                 return KHB_ERR_UNSUPPORTED;
             }
         }

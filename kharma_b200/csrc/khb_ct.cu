@@ -305,7 +305,7 @@ __global__ void k_ct_face_reflect(Dims d, khb_fields Bf, int bdir, int binner)
 // (DestructiveBoundaryClean, b_ct_boundaries.cpp:190-262): from the domain face outward each face
 // closes the zone between it and the previous face with zero divergence.  One thread per column
 // across the face, all layers in order; the cleaning covers the columns whose transverse upper faces
-// are stored (all but the last transverse layer).  X1 and X2 faces.
+// are stored (all but the last transverse layer).
 __global__ void k_ct_face_outflow(Dims d, Phys ph, khb_fields Bf, int bdir, int binner)
 {
     const int na = ct_na(d, bdir), nb = ct_nb(d, bdir), nx = ct_nx(d, bdir);
@@ -318,10 +318,25 @@ __global__ void k_ct_face_outflow(Dims d, Phys ph, khb_fields Bf, int bdir, int 
     if (binner) { for (int x = 0; x < f; ++x) Fn[ct_at(d, bdir, x, a, b)] = ff; }
     else { for (int x = f + 1; x < nx; ++x) Fn[ct_at(d, bdir, x, a, b)] = ff; }
     const int d3 = d.ndim > 2;
-    if (a >= na - 1 || b >= nb - d3) return;
+    if (a >= na - 1 || b >= nb - ((bdir == 3) ? 1 : d3)) return;
     const double A1 = ph.dx2 * ph.dx3, A2 = ph.dx1 * ph.dx3, A3 = ph.dx1 * ph.dx2;
     const int osign = binner ? -1 : 1;
     const double nsign = (double)(-(-osign));
+    if (bdir == 3) {
+        // X3 faces (b_ct_boundaries.cpp:249-268): both in-plane components close the zone
+        const double* F1 = Bf.v[0];
+        const double* F2 = Bf.v[1];
+        for (int layer = 0; layer < nx; ++layer) {
+            const int x = binner ? f - layer : f + layer;
+            if (x < 0 || x > nx - 1) break;
+            const int lf = binner ? x + 1 : x - 1, lc = binner ? x : x - 1;
+            const long long zc = ct_at(d, 3, lc, a, b);
+            const double nf = nsign * Fn[ct_at(d, 3, lf, a, b)] * A3 - (F1[zc + 1] * A1 - F1[zc] * A1)
+                              - (F2[zc + d.sj] * A2 - F2[zc] * A2);
+            Fn[ct_at(d, 3, x, a, b)] = (double)osign * nf / A3;
+        }
+        return;
+    }
     const double* Ft = Bf.v[(bdir == 1) ? 1 : 0];                 // the other in-plane component
     const double* F3 = Bf.v[2];
     const double At = (bdir == 1) ? A2 : A1, An = (bdir == 1) ? A1 : A2;

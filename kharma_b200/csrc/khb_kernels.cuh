@@ -941,7 +941,7 @@ __host__ __device__ inline unsigned plane_ghost_count(const Dims& d)
 
 // B_P = B_U/gdet and U = U(P) on the X1/X2 ghost zones of the interior k range.  B_CT blocks with
 // physical faces (Bf.v[0] set): a zone outside the interior only along directions in ct_mask (bit
-// 0: X1, bit 1: X2) takes B from its faces (B_CT::BlockUtoP over the boundary domain, b_ct.cpp:
+// 0: X1, bit 1: X2, bit 2: X3) takes B from its faces (B_CT::BlockUtoP over the boundary domain, b_ct.cpp:
 // 160-188); the last ghost layer of a direction has its lower face only (the face array stops
 // there) and takes B from that face alone.
 // kplanes: the ghost planes of physical X3 faces instead (whole (j, i) planes below ks and above ke)
@@ -973,8 +973,9 @@ __global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_field
     double Pz[NV], Uz[NV];
 #pragma unroll
     for (int p = 0; p < 5; ++p) Pz[p] = P.v[p][c];
-    const bool gi = i < d.is || i > d.ie, gj = j < d.js || j > d.je;
-    const bool from_faces = NV > 5 && Bf.v[0] && !(gi && !(ct_mask & 1)) && !(gj && !(ct_mask & 2));
+    const bool gi = i < d.is || i > d.ie, gj = j < d.js || j > d.je, gk = k < d.ks || k > d.ke;
+    const bool from_faces = NV > 5 && Bf.v[0] && !(gi && !(ct_mask & 1)) && !(gj && !(ct_mask & 2)) &&
+                            !(gk && !(ct_mask & 4));
     if (from_faces) {
         const long long gi0 = (long long)j*g.G1 + i;
         const double* F1 = Bf.v[0]; const double* F2 = Bf.v[1]; const double* F3 = Bf.v[2];

@@ -2160,6 +2160,15 @@ static void ct_face_boundary(const Block& B, double* Bf, int face)
                 if (d3) nf -= at(2, k + 1, j, lc) * A3 - at(2, k, j, lc) * A3;
                 at(0, k, j, x) = (double)osign * nf / A1;
             }
+        } else if (bdir == 3) {
+            // X3 faces (b_ct_boundaries.cpp:249-268), layers along k over the face plane (the
+            // reference's loop takes its k range from the face's i bounds, which only its intent, the
+            // k layers, can mean)
+            for (int j = 0; j < B.n2 - 1; ++j) for (int i = 0; i < B.n1 - 1; ++i) {
+                const double nf = nsign * at(2, lf, j, i) * A3 - (at(0, lc, j, i + 1) * A1 - at(0, lc, j, i) * A1)
+                                  - (at(1, lc, j + 1, i) * A2 - at(1, lc, j, i) * A2);
+                at(2, x, j, i) = (double)osign * nf / A3;
+            }
         } else {
             for (int k = 0; k < B.n3 - d3; ++k) for (int i = 0; i < B.n1 - 1; ++i) {
                 double nf = nsign * at(1, k, lf, i) * A2 - (at(0, k, lc, i + 1) * A1 - at(0, k, lc, i) * A1);

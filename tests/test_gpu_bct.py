@@ -13,6 +13,7 @@
   clean_face_B, the transmitted face rows and the ghost zones' B from their faces — primitives, conserved variables and every stored face to 1e-12 (floors call pow), flags
   identical; the face divergence of the torus's face curl stays at rounding over 100 steps.
 """
+import ctypes as C
 import dataclasses
 
 import numpy as np
@@ -150,9 +151,10 @@ def test_ct_entry_points_check_the_block_kind():
         _lib.check(lib.khb_ct_step(plain.ctx, 1e-3, plain.Pf.ref, plain.Uf.ref, b.Bff.ref,
                                    C.c_void_p(plain.pflag.data_ptr()), C.c_void_p(plain.fflag.data_ptr()),
                                    plain.stream), "khb_ct_step")
-    with pytest.raises(_lib.KhbError, match="X1/X2"):
+    # transmitting faces are X2 faces only (one_block_transmit.cpp:74-75)
+    with pytest.raises(_lib.KhbError, match="X2 faces"):
         Block(dataclasses.replace(ct_spec((16, 16, 8), "linear_mc", "gs05_c"),
-                                  bc=("periodic", "periodic", "periodic", "periodic", "outflow", "outflow")))
+                                  bc=("periodic", "periodic", "periodic", "periodic", "transmitting", "transmitting")))
 
 
 TORI = {
@@ -238,3 +240,42 @@ def test_ct_torus_fp32_flux_form(oracle_mod):
     assert err <= 1e-5
     scale = float(b32.Bf.abs().max()) / min(spec64.dx[:2])
     assert b32.max_divb() < 1e-12 * scale
+
+
+# Physical X3 faces with B_CT (b_ct_boundaries.cpp:40-62 zero_EMF, 190-268 clean_face_B; the
+# reflect_face_vector of boundaries.cpp:458-479 along x3): Cartesian 3D blocks, the face field a
+# discrete curl, 5 steps against the oracle, every stored face included
+X3_CT = {
+    "outflow": ("periodic", "periodic", "periodic", "periodic", "outflow", "outflow"),
+    "reflecting": ("periodic", "periodic", "periodic", "periodic", "reflecting", "reflecting"),
+    "mixed": ("outflow", "outflow", "periodic", "periodic", "reflecting", "outflow"),
+}
+
+
+@pytest.mark.parametrize("name", list(X3_CT))
+def test_ct_x3_physical_faces(oracle_mod, name):
+    spec = ct_spec((12, 12, 12), "linear_mc", "gs05_c", bc=X3_CT[name])
+    P0 = problems.add_ramps(spec, problems.mhdmodes(spec, 3, amp=1e-2))
+    Bf0 = problems.ct_curl_faces(spec)
+    o = oracle_mod.Oracle(spec)
+    b = Block(spec, geometry=o.geometry())
+    b.set_prims(P0, faces=Bf0)
+    Po, Uo, Bfo = o.ct_init_state(P0, Bf0)
+    dt = 0.5 * spec.dt_min
+    sl = spec.interior
+    for step in range(5):
+        pf_o, ff_o, dtn, mn_o = o.ct_step(Po, Uo, Bfo, dt)
+        b.step(dt)
+        mn_g = b.min_ndt()
+        P, U, Bf = b.P.cpu().numpy(), b.U.cpu().numpy(), b.Bf.cpu().numpy()
+        for what, x, y in (("P", P, Po), ("U", U, Uo), ("Bf", Bf, Bfo)):
+            err = rel_err(x, y)
+            assert np.all(err <= RTOL), (name, step, what, err)
+        assert np.array_equal(b.pflag.cpu().numpy()[sl], pf_o[sl].astype(np.int32))
+        assert abs(mn_g - mn_o) <= RTOL * abs(mn_o)
+        dt = dtn
+    # the face divergence of the interior zones stays at rounding
+    out = C.c_double()
+    _lib.check(b.lib.khb_ct_max_divb(b.ctx, b.Bff.ref, C.byref(out), b.stream), "khb_ct_max_divb")
+    scale = np.max(np.abs(Bf)) / min(spec.dx)
+    assert out.value <= 1e-12 * scale, (out.value, scale)

@@ -74,3 +74,24 @@ def test_schemes_agree_on_a_smooth_mode(oracle_mod):
     pert = np.abs(P0[:, 0] - P0[:, 0].mean(axis=(1, 2), keepdims=True)).max()
     for a in ("gs05_0", "gs05_c"):
         assert np.abs(out[a] - out["bs99"]).max() < 0.05 * pert
+
+
+def test_x3_outflow_cleaning_closes_the_ghost_zones(oracle_mod):
+    """Outflow X3 faces (clean_face_B along x3, b_ct_boundaries.cpp:249-268): after the boundaries
+    every ghost zone whose faces are all stored, in the X3 ghost layers, has zero face divergence to
+    rounding, and the interior field keeps its rounding-level divergence over 5 steps."""
+    spec = dataclasses.replace(mhdmodes_spec(12, 12, 12, recon="linear_mc"), b_ct="gs05_c",
+                               bc=("periodic", "periodic", "periodic", "periodic", "outflow", "outflow"))
+    P0 = problems.add_ramps(spec, problems.mhdmodes(spec, 3, amp=1e-2))
+    Bf0 = problems.ct_curl_faces(spec)
+    o, P, U, Bf = run(oracle_mod, spec, P0, Bf0, 5)
+    assert o.ct_max_divb(Bf) < 1e-12
+    dx1, dx2, dx3 = spec.dx
+    F1, F2, F3 = Bf
+    # zone (k, j, i) closed by faces i, i+1 / j, j+1 / k, k+1 (all stored for i < n1-1, j < n2-1, k < n3-1)
+    div = ((F1[:-1, :-1, 1:] - F1[:-1, :-1, :-1]) / dx1 + (F2[:-1, 1:, :-1] - F2[:-1, :-1, :-1]) / dx2
+           + (F3[1:, :-1, :-1] - F3[:-1, :-1, :-1]) / dx3)
+    ng = spec.ng
+    scale = np.abs(Bf).max() / min(spec.dx)
+    for kz in list(range(0, ng)) + list(range(ng + spec.nx3, spec.shape[0] - 1)):
+        assert np.abs(div[kz]).max() < 1e-12 * scale, kz
