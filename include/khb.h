@@ -587,6 +587,18 @@ int khb_set_tuning(khb_ctx* ctx, const char* key, int value);
 /* Number of device kernel launches issued through this context so far (for accounting). */
 int64_t khb_launch_count(khb_ctx* ctx);
 
+/* No counterpart in the reference.  The bounds-checked build of this library (kharma_b200/lib/
+ * libkhb_checked.so, compiled with KHB_BOUNDS_CHECK=1): the stencil loads and stores of the face
+ * kernels, the zone pass's flux and corner-EMF loads, the fixups' neighbours, the boundary and
+ * periodic-image copies and the geometry indices are checked against their arrays; an index outside
+ * is replaced by 0 (so the access stays inside the array and nothing traps) and the first one is
+ * recorded in the context's status word as site << 48 | its low 48 bits (sites: 1 face stencil, 2
+ * face store, 3 zone-pass flux, 4 corner EMF, 5 fixup neighbour, 6 boundary copy, 7 periodic image,
+ * 8 geometry).  khb_bounds_checked: 1 in that build, 0 in the regular one (whose checks compile away
+ * and whose status stays 0).  khb_bounds_status reads the word and clears it; synchronizes. */
+int khb_bounds_checked(void);
+int khb_bounds_status(khb_ctx* ctx, uint64_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

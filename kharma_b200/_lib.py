@@ -178,6 +178,8 @@ SIGNATURES = {
     "khb_batch_autotune": (_I, [_P, _I, _P, C.POINTER(C.c_int32), _P]),
     "khb_batch_launch_count": (C.c_int64, [_P]),
     "khb_batch_set_plan": (_I, [_P, _I]),
+    "khb_bounds_checked": (_I, []),
+    "khb_bounds_status": (_I, [_P, C.POINTER(C.c_uint64), _P]),
     "khb_batch_get_plan": (_I, [_P, C.POINTER(C.c_int32)]),
     "khb_batch_set_mesh": (_I, [_P, _P, C.c_int64, C.c_int64, _P, C.c_int64]),
     "khb_batch_mesh_exchange": (_I, [_P, _P]),

@@ -1,6 +1,7 @@
 """Build libkhb.so in-tree for sm_100a with nvcc.
 
-    python -m kharma_b200.build
+    python -m kharma_b200.build              (lib/libkhb.so)
+    python -m kharma_b200.build --checked    (lib/libkhb_checked.so, KHB_BOUNDS_CHECK=1)
 
 Translation units and their arithmetic flags:
   khb_fp64.cu      FP64 path (fluxes, zone pass, ghost zones)      -fmad=false
@@ -46,19 +47,32 @@ def _deps_mtime():
     return max(os.path.getmtime(p) for p in paths)
 
 
-def build(force=False, extra=(), out=OUT, verbose=False, jobs=4):
-    os.makedirs(OBJ, exist_ok=True)
+CHECKED_OUT = os.path.join(HERE, "lib", "libkhb_checked.so")
+CHECKED_OBJ = os.path.join(HERE, "lib", "obj_checked")
+
+
+def build_checked(force=False, verbose=False):
+    """The bounds-checked build (KHB_BOUNDS_CHECK=1, khb_bounds_status in include/khb.h)."""
+    return build(force=force, extra_flags=["-DKHB_BOUNDS_CHECK=1"], out=CHECKED_OUT, obj=CHECKED_OBJ,
+                 verbose=verbose)
+
+
+def build(force=False, extra=(), out=OUT, verbose=False, jobs=4, extra_flags=(), obj=None):
+    """Compile the units whose sources or headers changed and link out.  extra: flags that also force
+    a full rebuild; extra_flags: flags of a build variant kept in its own object directory obj."""
+    OBJ_DIR = obj or OBJ
+    os.makedirs(OBJ_DIR, exist_ok=True)
     hdr_t = _deps_mtime()
     procs = []
     objs = []
     for src, flags in UNITS.items():
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ, src + ".o")
+        o = os.path.join(OBJ_DIR, src + ".o")
         objs.append(o)
         stale = force or extra or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_t)
         if not stale:
             continue
-        cmd = ["nvcc", *ARCH, *COMMON, *flags, *extra, "-c", s, "-o", o]
+        cmd = ["nvcc", *ARCH, *COMMON, *flags, *extra, *extra_flags, "-c", s, "-o", o]
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
@@ -84,5 +98,8 @@ def build(force=False, extra=(), out=OUT, verbose=False, jobs=4):
 
 
 if __name__ == "__main__":
-    extra = [a for a in sys.argv[1:] if a.startswith("-")]
-    print(build(force=True, extra=extra, verbose=True))
+    if "--checked" in sys.argv[1:]:
+        print(build_checked(force=True, verbose=True))
+    else:
+        extra = [a for a in sys.argv[1:] if a.startswith("-")]
+        print(build(force=True, extra=extra, verbose=True))

@@ -517,6 +517,8 @@ int khb_create(const khb_config* cfg, khb_ctx** out)
     if (e == cudaSuccess && cfg->fofc) e = alloc((void**)&c->fofc_flag, sizeof(int32_t) * N);
     if (e == cudaSuccess && cfg->ct_scheme) e = alloc(&c->ct_emfc, fs * 3 * N);
     if (e == cudaSuccess && cfg->ct_scheme) e = alloc((void**)&c->ct_stageBf, sizeof(double) * 3 * N);
+    // words[3]: the status word of the bounds-checked build (every kernel sees it through Dims)
+    if (e == cudaSuccess) c->d.chk = c->words + 3;
     // the memsets above run on the legacy default stream, which the caller's (non-blocking) streams
     // do not wait for: finish them before the context is handed out
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -1069,6 +1071,19 @@ int khb_set_tuning(khb_ctx* ctx, const char* key, int value)
 }
 
 int64_t khb_launch_count(khb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int khb_bounds_checked(void) { return KHB_BOUNDS_CHECK ? 1 : 0; }
+
+int khb_bounds_status(khb_ctx* ctx, uint64_t* status, void* stream)
+{
+    if (!ctx || !status) return fail(KHB_ERR_ARG, "khb_bounds_status: NULL argument");
+    unsigned long long w = 0;
+    KHB_CUDA(cudaMemcpyAsync(&w, ctx->words + 3, sizeof(w), cudaMemcpyDeviceToHost, S(stream)));
+    KHB_CUDA(cudaMemsetAsync(ctx->words + 3, 0, sizeof(w), S(stream)));
+    KHB_CUDA(cudaStreamSynchronize(S(stream)));
+    *status = (uint64_t)w;
+    return KHB_OK;
+}
 
 // ---------------------------------------------------------------------------- EMHD and implicit solve
 static int check_emhd(const khb_emhd_params* e)

@@ -152,7 +152,7 @@ __device__ __forceinline__ void flux_face(const Dims& d, const DevGeom& g, const
                                           FT* __restrict__ F, FT* __restrict__ ctop, int i, int j, int k)
 {
     constexpr int dir = DIR;
-    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    const long long c = kchk(d, ((long long)k*d.n2 + j)*d.n1 + i, d.N, CHK_FLUX_STORE);
     const long long st = (dir == 1) ? 1 : ((dir == 2) ? d.sj : d.sk);
     const int loc = dir - 1;
     const R gam = (R)ph.gam;
@@ -164,7 +164,7 @@ __device__ __forceinline__ void flux_face(const Dims& d, const DevGeom& g, const
         for (int p = 0; p < NV; ++p) prefetch_l2(P.v[p] + c);
     }
     // geometry at the face
-    const long long gi = (long long)j*g.G1 + i;
+    const long long gi = kchk(d, (long long)j*g.G1 + i, g.gs, CHK_GEOM);
     const auto* tcov = FaceTables<R>::gcov(g, loc);
     const auto* tcon = FaceTables<R>::gcon(g, loc);
     R gcov[4][4];
@@ -195,8 +195,9 @@ __device__ __forceinline__ void flux_face(const Dims& d, const DevGeom& g, const
 #pragma unroll
     for (int p = 0; p < NV; ++p) {
         const double* q = P.v[p];
-        const R x0 = (R)__ldg(q + c - 3*st), x1 = (R)__ldg(q + c - 2*st), x2 = (R)__ldg(q + c - st);
-        const R x3 = (R)__ldg(q + c), x4 = (R)__ldg(q + c + st), x5 = (R)__ldg(q + c + 2*st);
+        const R x0 = (R)__ldg(q + kchk(d, c - 3*st, d.N, CHK_FLUX_STENCIL)), x1 = (R)__ldg(q + kchk(d, c - 2*st, d.N, CHK_FLUX_STENCIL));
+        const R x2 = (R)__ldg(q + kchk(d, c - st, d.N, CHK_FLUX_STENCIL)), x3 = (R)__ldg(q + c);
+        const R x4 = (R)__ldg(q + kchk(d, c + st, d.N, CHK_FLUX_STENCIL)), x5 = (R)__ldg(q + kchk(d, c + 2*st, d.N, CHK_FLUX_STENCIL));
         if (RECON == RECON_EXTRA) {
             Pl[p] = recon_extra<R>(ph.recon_extra, true, x0, x1, x2, x3, x4);
             Pr[p] = recon_extra<R>(ph.recon_extra, false, x1, x2, x3, x4, x5);
@@ -221,8 +222,9 @@ __device__ __forceinline__ void flux_face(const Dims& d, const DevGeom& g, const
 #pragma unroll
             for (int p = 0; p < NV; ++p) {
                 const double* q = P.v[p];
-                const R x0 = (R)__ldg(q + c - 3*st), x1 = (R)__ldg(q + c - 2*st), x2 = (R)__ldg(q + c - st);
-                const R x3 = (R)__ldg(q + c), x4 = (R)__ldg(q + c + st), x5 = (R)__ldg(q + c + 2*st);
+                const R x0 = (R)__ldg(q + kchk(d, c - 3*st, d.N, CHK_FLUX_STENCIL)), x1 = (R)__ldg(q + kchk(d, c - 2*st, d.N, CHK_FLUX_STENCIL));
+                const R x2 = (R)__ldg(q + kchk(d, c - st, d.N, CHK_FLUX_STENCIL)), x3 = (R)__ldg(q + c);
+                const R x4 = (R)__ldg(q + kchk(d, c + st, d.N, CHK_FLUX_STENCIL)), x5 = (R)__ldg(q + kchk(d, c + 2*st, d.N, CHK_FLUX_STENCIL));
                 Pl[p] = recon_right<RECON_PPM, R>(x0, x1, x2, x3, x4);
                 Pr[p] = recon_left<RECON_PPM, R>(x1, x2, x3, x4, x5);
             }
@@ -330,13 +332,18 @@ __device__ __forceinline__ void ct_divergence(const Dims& d, const Phys& ph, con
     double fb[3][3][2];   // [face dir][B component][lo/hi face]
     if (d.ndim >= 2) {
         const long long B1 = 5*N, B2 = 6*N, B3 = 7*N;
+        // corner EMFs; the checked build verifies the furthest reaches of each (x itself, x - sj or
+        // x - sk, x - 1) against the field's extent
         auto e3 = [&](long long x) -> FT {
+            x = kchk(d, x, N, CHK_ZONE_CT); kchk(d, x - sj, N, CHK_ZONE_CT); kchk(d, x - 1, N, CHK_ZONE_CT);
             return (FT)0.25 * (__ldg(F1 + B2 + x) + __ldg(F1 + B2 + x - sj) - __ldg(F2 + B1 + x) - __ldg(F2 + B1 + x - 1));
         };
         auto e1 = [&](long long x) -> FT {
+            x = kchk(d, x, N, CHK_ZONE_CT); kchk(d, x - sk, N, CHK_ZONE_CT); kchk(d, x - sj, N, CHK_ZONE_CT);
             return (FT)0.25 * (__ldg(F2 + B3 + x) + __ldg(F2 + B3 + x - sk) - __ldg(F3 + B2 + x) - __ldg(F3 + B2 + x - sj));
         };
         auto e2 = [&](long long x) -> FT {
+            x = kchk(d, x, N, CHK_ZONE_CT); kchk(d, x - 1, N, CHK_ZONE_CT); kchk(d, x - sk, N, CHK_ZONE_CT);
             return (FT)0.25 * (__ldg(F3 + B1 + x) + __ldg(F3 + B1 + x - 1) - __ldg(F1 + B3 + x) - __ldg(F1 + B3 + x - sk));
         };
         const bool d3 = d.ndim > 2;
@@ -427,9 +434,13 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
     const int mode = MODE ? (MODE | (a.mode & M_DT)) : a.mode;
     double ndt_zone = 1.7976931348623157e308;
     {
-        const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+        const long long c = kchk(d, ((long long)k*d.n2 + j)*d.n1 + i, d.N, CHK_ZONE_FLUX);
         const long long N = d.N, sj = d.sj, sk = d.sk;
         const double gam = ph.gam;
+        kchk(d, c + 1, N, CHK_ZONE_FLUX);
+        if (d.ndim >= 2) kchk(d, c + sj, N, CHK_ZONE_FLUX);
+        if (d.ndim == 3) kchk(d, c + sk, N, CHK_ZONE_FLUX);
+        kchk(d, (long long)j*g.G1 + i, g.gs, CHK_GEOM);
         ZoneGeom G;
         load_zone_geom<(sizeof(FT) == 4)>(g, j, i, G);
 
@@ -787,7 +798,7 @@ __device__ __forceinline__ void fixup_zone(const Dims& d, const DevGeom& g, cons
                     if (bc == KHB_BC_PERIODIC) kk += (kk < d.ks) ? d.nx3 : -d.nx3;
                     else if (bc != KHB_BC_EXCHANGE) continue;
                 }
-                const long long cn = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+                const long long cn = kchk(d, ((long long)kk*d.n2 + jj)*d.n1 + ii, d.N, CHK_FIXUP);
                 if (!(pflag[cn] > 0)) {
                     const double w = 1./(abs(l) + abs(m) + abs(nn) + 1);
                     wsum += w;
@@ -890,8 +901,8 @@ __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int
     else                kk = (type == KHB_BC_OUTFLOW) ? ref : offset - k;
     // transmitting: the mirrored zone half-way round in x3 (one_block_transmit.cpp:116-134)
     if (transmit) kk = ((k - d.ks + d.nx3 / 2) % d.nx3) + d.ks;
-    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
-    const long long s = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+    const long long c = kchk(d, ((long long)k*d.n2 + j)*d.n1 + i, d.N, CHK_BC);
+    const long long s = kchk(d, ((long long)kk*d.n2 + jj)*d.n1 + ii, d.N, CHK_BC);
     double Pz[5];
 #pragma unroll
     for (int p = 0; p < 5; ++p) {
@@ -1028,7 +1039,7 @@ __global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
     if ((pmask & 2) && (j < d.js || j > d.je)) { jj += (j < d.js) ? d.nx2 : -d.nx2; any = true; }
     if ((pmask & 4) && (k < d.ks || k > d.ke)) { kk += (k < d.ks) ? d.nx3 : -d.nx3; any = true; }
     if (!any) return;
-    const long long s = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+    const long long s = kchk(d, ((long long)kk*d.n2 + jj)*d.n1 + ii, d.N, CHK_PERIODIC);
 #pragma unroll
     for (int p = 0; p < NV; ++p) {
         if (NV > 8 && !P.v[p]) continue;       // EMHD slots that are not evolved

@@ -26,7 +26,34 @@ struct Dims {
     long long N;
     long long sj, sk;
     int bc[6];
+    // status word of the bounds-checked build (KHB_BOUNDS_CHECK): the first out-of-range index a
+    // checked access met, with its site; unused otherwise
+    unsigned long long* chk;
 };
+
+// Sites of the bounds-checked accesses (the top 16 bits of the status word)
+enum { CHK_FLUX_STENCIL = 1, CHK_FLUX_STORE = 2, CHK_ZONE_FLUX = 3, CHK_ZONE_CT = 4, CHK_FIXUP = 5,
+       CHK_BC = 6, CHK_PERIODIC = 7, CHK_GEOM = 8 };
+
+// Index check of the bounds-checked build (-DKHB_BOUNDS_CHECK=1, the stand-in for a memory checker):
+// an index outside [0, n) is recorded in the status word (site << 48 | low 48 bits of the index, the
+// first one wins) and replaced by 0, so the access stays inside its array and nothing traps.  In the
+// regular build it is the identity.
+#ifndef KHB_BOUNDS_CHECK
+#define KHB_BOUNDS_CHECK 0
+#endif
+__host__ __device__ __forceinline__ long long kchk(const Dims& d, long long x, long long n, int site)
+{
+#if KHB_BOUNDS_CHECK && defined(__CUDA_ARCH__)
+    if (x < 0 || x >= n) {
+        if (d.chk) atomicCAS(d.chk, 0ull, ((unsigned long long)site << 48) | ((unsigned long long)x & 0xffffffffffffull));
+        return 0;
+    }
+#else
+    (void)d; (void)n; (void)site;
+#endif
+    return x;
+}
 
 struct DevGeom {
     int G1, G2, n1;
