@@ -148,9 +148,11 @@ enum { KHB_JACOBIAN_FD = 0, KHB_JACOBIAN_EXACT = 1 };
 enum { KHB_SOLVE_CONVERGED = 0, KHB_SOLVE_FAIL = 1, KHB_SOLVE_BEYOND_TOL = 2, KHB_SOLVE_BACKTRACK = 3 };
 
 /* EMHD::EMHD_parameters (emhd/emhd.hpp:60-84) with the package switches emhd/conduction and
- * emhd/viscosity (emhd.cpp:60-72); q~ is evolved iff conduction, dP~ iff viscosity. */
+ * emhd/viscosity (emhd.cpp:60-72); q~ is evolved iff conduction, dP~ iff viscosity.
+ * stability_limits: emhd/stability_limits (emhd.cpp:118-125), the heat-flux and pressure-anisotropy
+ * limits an ImEx stage applies after the implicit solve. */
 typedef struct {
-    int32_t closure, higher_order_terms, feedback, conduction, viscosity, pad;
+    int32_t closure, higher_order_terms, feedback, conduction, viscosity, stability_limits;
     double tau, conduction_alpha, viscosity_alpha, kappa, eta;
 } khb_emhd_params;
 
@@ -549,17 +551,30 @@ int khb_copy_flux_emhd(khb_ctx* ctx, int dir, const khb_fields* F_out, double* c
 
 /* One ImEx stage (driver/imex_step.cpp:58-356) of the vl2 integrator the implicit package forces
  * (implicit.cpp:96; stage 1: beta 1/2, stage 2: beta 1, both from the step-start state):
- * EMHD fluxes, flux-CT, divergence, the geometric source with the EMHD tensor and EMHD::AddSource
- * into dU/dt; the explicit update of B and B_P = B_U/gdet; the implicit guess copied from the
- * sub-step state; Implicit::Step with beta dt (fluid and EMHD variables); FixSolve; periodic ghost
- * zones; P -> U with the EMHD tensor over the whole block.  P_out/U_out must not alias P_sub/U_sub;
- * exchange faces carry the sub-step ghost zones over.  Floors and physical (outflow/reflecting)
- * faces on the EMHD state are rejected (KHB_ERR_UNSUPPORTED).  The last stage accumulates the zone
- * timestep minimum (khb_get_min_ndt). */
+ * EMHD fluxes, flux-CT, the flux fixes of physical faces (boundaries.cpp:611-690: X1 inflow checks,
+ * zero polar fluxes of all 10 slots), divergence, the geometric source with the EMHD tensor and
+ * EMHD::AddSource into dU/dt; the explicit update of B and B_P = B_U/gdet; the implicit guess copied
+ * from the sub-step state; Implicit::Step with beta dt (fluid and EMHD variables); the floors
+ * (imex_step.cpp:269; fluid or drift frame) and the EMHD stability limits (emhd_limits.hpp:55-130)
+ * over the interior; FixSolve; the ghost zones of the 10-slot state (periodic images and the
+ * outflow/reflecting faces, q~ and dP~ copied as the density); P -> U with the EMHD tensor over the
+ * whole block.  P_out/U_out must not alias P_sub/U_sub; exchange faces carry the sub-step ghost zones
+ * over.  Floors or stability limits need the flag arrays: use khb_imex_stage_flags (KHB_ERR_ARG
+ * here).  The last stage accumulates the zone timestep minimum (khb_get_min_ndt). */
 int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp, int stage, double dt,
                    const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub, const khb_fields* U_sub,
                    const khb_fields* P_out, const khb_fields* U_out, double* solve_norm, double* solve_fail,
                    void* stream);
+
+/* khb_imex_stage with the stage's flag fields ([N] int32 each, device): fflag the floor bits
+ * (KHB_FFLAG_*) and eflag the EMHD limit bits (1 heat flux, 2 pressure anisotropy above, 4 below;
+ * emhd_limits.hpp:38-40) of the interior zones, written every call (zeros where the floors or the
+ * limits are off; either may be NULL while its step is off).  The normal-observer and mixed floor
+ * frames are rejected (KHB_ERR_UNSUPPORTED) on the EMHD state. */
+int khb_imex_stage_flags(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp, int stage,
+                         double dt, const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub,
+                         const khb_fields* U_sub, const khb_fields* P_out, const khb_fields* U_out,
+                         double* solve_norm, double* solve_fail, int32_t* fflag, int32_t* eflag, void* stream);
 
 /* Iterations taken by the last khb_implicit_step and the maximum solve_norm of each (max_norms
  * has room for max_nonlinear_iter values).  Synchronizes the stream. */

@@ -87,7 +87,7 @@ class KhbFields(C.Structure):
 
 class KhbEmhdParams(C.Structure):
     _fields_ = [("closure", C.c_int32), ("higher_order_terms", C.c_int32), ("feedback", C.c_int32),
-                ("conduction", C.c_int32), ("viscosity", C.c_int32), ("pad", C.c_int32),
+                ("conduction", C.c_int32), ("viscosity", C.c_int32), ("stability_limits", C.c_int32),
                 ("tau", C.c_double), ("conduction_alpha", C.c_double), ("viscosity_alpha", C.c_double),
                 ("kappa", C.c_double), ("eta", C.c_double)]
 
@@ -167,6 +167,10 @@ SIGNATURES = {
     "khb_imex_stage": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbImplicitParams), _I, _D,
                             C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
                             C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
+    "khb_imex_stage_flags": (_I, [_P, C.POINTER(KhbEmhdParams), C.POINTER(KhbImplicitParams), _I, _D,
+                                  C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields),
+                                  C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P, _P,
+                                  _P]),
     "khb_batch_create": (_I, [C.POINTER(_P), _I, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(_P),
                               C.POINTER(_P), C.POINTER(_P)]),
     "khb_batch_destroy": (_I, [_P]),

@@ -70,14 +70,16 @@ int launch_flux(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
 }
 
 template <typename FT>
-int launch_fix_flux_t(khb_ctx* ctx, const Phys& ph, cudaStream_t st)
+int launch_fix_flux_t(khb_ctx* ctx, const Phys& ph, cudaStream_t st, FT* F1 = nullptr, FT* F2 = nullptr,
+                      FT* F3 = nullptr, int nv = 0)
 {
+    // default: the context's flux arrays; the EMHD stage passes its 10-slot arrays (nv = 10)
     const Dims& d = ctx->d;
-    FT* F1 = (FT*)ctx->F[0]; FT* F2 = (FT*)ctx->F[1]; FT* F3 = (FT*)ctx->F[2];
-    if (d.ndim >= 2 && (ph.zero_polar_flux || (ctx->nv > 5 && ph.fix_polar_flux))) {
+    if (!F1) { F1 = (FT*)ctx->F[0]; F2 = (FT*)ctx->F[1]; F3 = (FT*)ctx->F[2]; nv = ctx->nv; }
+    if (d.ndim >= 2 && (ph.zero_polar_flux || (nv > 5 && ph.fix_polar_flux))) {
         for (int face = 2; face <= 3; ++face) {
             if (!phys_face(d.bc[face])) continue;
-            Launch<FT>::fix_flux_x2(ctx->nv, d, ph, F1, F2, F3, face == 2, st);
+            Launch<FT>::fix_flux_x2(nv, d, ph, F1, F2, F3, face == 2, st);
             KHB_LAUNCHED(ctx);
         }
     }
@@ -183,11 +185,14 @@ __global__ void k_interior_pack(Dims d, khb_fields P, int nv, double* buf, int u
 
 // Bf: a B_CT block's faces; with physical faces their ghost layers are filled first and the ghost
 // zones of the physical directions take B from them
+// nv_state: 10 for the EMHD state (its scalar slots q~, dP~ copied as the density is), else the
+// context's nvar
 int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st,
-                      const khb_fields* Bf = nullptr)
+                      const khb_fields* Bf = nullptr, int nv_state = 0)
 {
     const Dims& d = ctx->d;
-    const int nv = ctx->nv;
+    const int nv = nv_state ? nv_state : ctx->nv;
+    const int nv_ptou = (nv == 10) ? 8 : nv;     // ghost B_P and (GRMHD) U; the EMHD U is formed later
     const int cnt_k = d.ke - d.ks + 1;
     bool physical = false;
     int ct_mask = 0;
@@ -221,7 +226,7 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
         }
     }
     if (physical) {
-        LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask);
+        LaunchCommon::ghost_ptou(nv_ptou, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask);
         KHB_LAUNCHED(ctx);
     }
     // X3 faces last (Parthenon's face order), over the whole (j, i) plane: their ghost planes copy
@@ -235,7 +240,7 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
             KHB_LAUNCHED(ctx);
         }
         if (kplanes) {
-            LaunchCommon::ghost_ptou(nv, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask, kplanes);
+            LaunchCommon::ghost_ptou(nv_ptou, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask, kplanes);
             KHB_LAUNCHED(ctx);
         }
     }
@@ -1269,6 +1274,15 @@ int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit
                    const khb_fields* P_out, const khb_fields* U_out, double* solve_norm, double* solve_fail,
                    void* stream)
 {
+    return khb_imex_stage_flags(ctx, emhd, imp, stage, dt, P_full, U_full, P_sub, U_sub, P_out, U_out, solve_norm,
+                                solve_fail, nullptr, nullptr, stream);
+}
+
+int khb_imex_stage_flags(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit_params* imp, int stage,
+                         double dt, const khb_fields* P_full, const khb_fields* U_full, const khb_fields* P_sub,
+                         const khb_fields* U_sub, const khb_fields* P_out, const khb_fields* U_out,
+                         double* solve_norm, double* solve_fail, int32_t* fflag, int32_t* eflag, void* stream)
+{
     KHB_RANGE("khb_imex_stage");
     KHB_NEED_GEOM(ctx);
     if (ctx->ph.ct_scheme) return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: EMHD with B_CT is not supported");
@@ -1281,18 +1295,26 @@ int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit
     if (P_out->v[0] == P_sub->v[0] || U_out->v[0] == U_sub->v[0])
         return fail(KHB_ERR_ARG, "khb_imex_stage: the output state must not alias the sub-step state");
     if (!solve_norm || !solve_fail) return fail(KHB_ERR_ARG, "khb_imex_stage: NULL solve_norm/solve_fail");
-    if (ctx->ph.floors_on) return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: floors on the EMHD state are not supported");
+    if (ctx->ph.floors_on && !fflag)
+        return fail(KHB_ERR_ARG, "khb_imex_stage: floors on the EMHD state write their flags (khb_imex_stage_flags)");
+    if (emhd->stability_limits && !eflag)
+        return fail(KHB_ERR_ARG, "khb_imex_stage: the EMHD stability limits write their flags (khb_imex_stage_flags)");
+    if (ctx->ph.floors_on && ctx->ph.frame != KHB_FRAME_FLUID && ctx->ph.frame != KHB_FRAME_DRIFT)
+        return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: floors on the EMHD state in the fluid or drift frame only "
+                                         "(the normal frame re-inverts a conserved state the implicit solve does not form)");
     const Dims& d = ctx->d;
-    for (int f = 0; f < 2 * d.ndim; ++f)
-        if (phys_face(d.bc[f]))
-            return fail(KHB_ERR_UNSUPPORTED, "khb_imex_stage: physical boundaries of the EMHD state are not supported "
-                                             "(use periodic or exchange faces)");
+    bool physical = false;
+    for (int f = 0; f < 2 * d.ndim; ++f) physical |= phys_face(d.bc[f]);
     cudaStream_t st = S(stream);
     const int s = stage - 1;
     // vl2, which the implicit package forces (implicit.cpp:96): gam0 = {0, 0}, gam1 = {1, 1}, beta = {1/2, 1}
     const double g0 = 0.0, g1 = 1.0, beta = (stage == 1) ? 0.5 : 1.0, bdt = beta * dt;
     for (int dir = 1; dir <= d.ndim; ++dir)
         if ((rc = khb_get_flux_emhd(ctx, emhd, dir, P_sub, stream))) return rc;
+    // FixFlux on the physical faces (polar B-flux fix, zero polar fluxes of all 10 slots, X1 inflow
+    // checks); flux-CT, and the polar zeroing after it, run inside the divergence kernel
+    if (physical && (rc = launch_fix_flux_t<double>(ctx, ctx->ph, st, ctx->F10[0], ctx->F10[1], ctx->F10[2], 10)))
+        return rc;
     if (stage == 2)
         KHB_CUDA(cudaMemcpyAsync(ctx->words, &ctx->dbl_max_bits, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
     khb_fields du = fields_of(ctx->dudt10, d.N);
@@ -1309,14 +1331,33 @@ int khb_imex_stage(khb_ctx* ctx, const khb_emhd_params* emhd, const khb_implicit
     (void)s;
     if ((rc = khb_implicit_step(ctx, emhd, imp, P_full, U_full, P_sub, &du, P_out, solve_norm, solve_fail, bdt,
                                 stream))) return rc;
-    if ((rc = khb_fix_solve(ctx, emhd, P_out, U_out, solve_fail, stream))) return rc;
-    int pmask = 0;
-    if (d.bc[0] == KHB_BC_PERIODIC) pmask |= 1;
-    if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) pmask |= 2;
-    if (d.ndim >= 3 && d.bc[4] == KHB_BC_PERIODIC) pmask |= 4;
-    if (pmask) {
-        LaunchCommon::periodic(10, d, *P_out, *U_out, pmask, st);
+    // Packages::MeshApplyFloors over the interior (imex_step.cpp:269): the GRMHD floors, then the EMHD
+    // package's stability limits
+    if (ctx->ph.floors_on) {
+        LaunchEmhd::floors(d, ctx->g, ctx->ph, *P_out, fflag, st);
         KHB_LAUNCHED(ctx);
+    } else if (fflag) {
+        KHB_CUDA(cudaMemsetAsync(fflag, 0, sizeof(int32_t) * (size_t)d.N, st));
+    }
+    if (emhd->stability_limits) {
+        LaunchEmhd::limits(d, ctx->g, ctx->ph.gam, *emhd, *P_out, eflag, st);
+        KHB_LAUNCHED(ctx);
+    } else if (eflag) {
+        KHB_CUDA(cudaMemsetAsync(eflag, 0, sizeof(int32_t) * (size_t)d.N, st));
+    }
+    if ((rc = khb_fix_solve(ctx, emhd, P_out, U_out, solve_fail, stream))) return rc;
+    // ApplyBoundaryConditionsOnCoarseOrFineMD (imex_step.cpp:297-298) on the 10-slot state
+    if (physical) {
+        if ((rc = launch_boundaries(ctx, *P_out, *U_out, st, nullptr, 10))) return rc;
+    } else {
+        int pmask = 0;
+        if (d.bc[0] == KHB_BC_PERIODIC) pmask |= 1;
+        if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) pmask |= 2;
+        if (d.ndim >= 3 && d.bc[4] == KHB_BC_PERIODIC) pmask |= 4;
+        if (pmask) {
+            LaunchCommon::periodic(10, d, *P_out, *U_out, pmask, st);
+            KHB_LAUNCHED(ctx);
+        }
     }
     return khb_emhd_ptou(ctx, emhd, P_out, U_out, stream);
 }

@@ -9,6 +9,7 @@
 //                      path), backtracking, line search, update, residual norm and the block maximum
 //   k_implicit_jacobian  residual and Jacobian only (the split "implicit_jacobian" kernel's output)
 //   k_fix_solve_avg / k_fix_solve_apply   Implicit::FixSolve neighbour averaging and P->U
+//   k_emhd_floors / k_emhd_limits   the floors and the EMHD stability limits of an ImEx stage
 //
 // The Newton state of a zone stays in registers for a whole iteration; the Jacobian (at most 7x7)
 // is never written to memory.  Successive iterations are separate launches that read the previous
@@ -1378,6 +1379,77 @@ static void flux_emhd_hd(int recon, int dir, const Dims& d, const DevGeom& g, co
     else if (dir == 2) flux_emhd_dir<2, HQ, HD>(recon, d, g, ph, E, P, F, ctop, bx, st);
     else flux_emhd_dir<3, HQ, HD>(recon, d, g, ph, E, P, F, ctop, bx, st);
 }
+// Packages::MeshApplyFloors on the EMHD state over the interior (imex_step.cpp:269): the GRMHD floors
+// in the fluid or drift frame (floors.cpp:215-229, floors_impl.hpp:77-125), which change the fluid
+// primitives only, and the ceilings; the stage's final P -> U over the whole block forms U.  Floor
+// bits into fflag.
+__global__ void __launch_bounds__(128) k_emhd_floors(Dims d, DevGeom g, Phys ph, khb_fields P, int32_t* fflag)
+{
+    int k, j, i;
+    long long c;
+    if (!interior_zone(d, (long long)blockIdx.x * blockDim.x + threadIdx.x, k, j, i, c)) return;
+    ZoneGeom G;
+    load_zone_geom(g, j, i, G);
+    double Pz[8], Uz[8] = {0., 0., 0., 0., 0., 0., 0., 0.};   // the fluid and drift frames leave U alone
+#pragma unroll
+    for (int p = 0; p < 8; ++p) Pz[p] = P.v[p][c];
+    const long long cg = (long long)j*g.n1 + i;
+    const Prescription& fl = floors_at(ph, g, j, i);
+    double rf, uf;
+    FourVec<double> D;
+    const int ff = determine_floors<8>(G, fl, __ldg(g.floor_rho + cg), __ldg(g.floor_u + cg), ph.gam, Pz, rf, uf, D);
+    if (ff) {
+        apply_floors_frame<8>(G, ph.frame, ph.gam, Pz, Uz, rf, uf, 8, &D);
+        apply_ceilings(G, fl, ph.gam, Pz);
+#pragma unroll
+        for (int p = 0; p < 5; ++p) P.v[p][c] = Pz[p];
+    }
+    fflag[c] = ff;
+}
+
+// EMHD::ApplyEMHDLimits / apply_instability_limits (emhd.cpp:399-428, emhd_limits.hpp:55-130) over
+// the interior: q~ scaled so that |q| <= 1.07 rho cs^3, dP~ to the mirror and firehose bounds; the
+// limit bits (1 q, 2 dP above, 4 dP below) into eflag.  The reference's closing p_to_u is the
+// stage's final P -> U.
+__global__ void __launch_bounds__(128) k_emhd_limits(Dims d, DevGeom g, double gam, EmhdArgs E, khb_fields P,
+                                                    int32_t* eflag)
+{
+    int k, j, i;
+    long long c;
+    if (!interior_zone(d, (long long)blockIdx.x * blockDim.x + threadIdx.x, k, j, i, c)) return;
+    CenterGeom G;
+    load_center(g, j, i, G);
+    double Pz[10];
+    load10(P, c, Pz);
+    const double rho = Pz[0], uu = Pz[1];
+    const double qtilde = E.conduction ? Pz[8] : 0., dPtilde = E.viscosity ? Pz[9] : 0.;
+    const double pg = (gam - 1.) * uu;
+    const double Theta = pg / rho;
+    const double cs = sqrt(gam * pg / (rho + (gam * uu)));
+    FourVec<double> D;
+    calc_4vecs<double, true>(G.gcov, G.gcon0[0], G.gcon0, Pz, D);
+    const double bsq = kmax(dot4(D.bcon, D.bcov), SMALL);
+    double q, dP;
+    convert_q_dP(E, qtilde, dPtilde, rho, Theta, cs*cs, q, dP);
+    int ef = 0;
+    if (E.conduction) {
+        const double qmax = 1.07 * rho * cs*cs*cs;
+        const double max_frac = kmax(fabs(q) / qmax, 1.);
+        if (fabs(q) / qmax > 1.) ef |= 1;
+        P.v[8][c] = Pz[8] / max_frac;
+    }
+    if (E.viscosity) {
+        const double dP_comp_ratio = kmax(pg - 2./3. * dP, SMALL) / kmax(pg + 1./3. * dP, SMALL);
+        const double dP_plus = kmin(1.07 * 0.5 * bsq * dP_comp_ratio, 1.49 * pg);
+        const double dP_minus = kmax(-1.07 * bsq, -2.99 * pg);
+        if (dP > 0. && (dP / dP_plus > 1.)) ef |= 2;
+        else if (dP < 0. && (dP / dP_minus > 1.)) ef |= 4;
+        if (dP > 0.) P.v[9][c] = Pz[9] * (1. / kmax(dP / dP_plus, 1.));
+        else P.v[9][c] = Pz[9] * (1. / kmax(dP / dP_minus, 1.));
+    }
+    eflag[c] = ef;
+}
+
 void LaunchEmhd::flux(int recon, int dir, const Dims& d, const DevGeom& g, const Phys& ph, const EmhdArgs& E,
                       const khb_fields& P, double* F, double* ctop, const int lo[3], const int cnt[3], cudaStream_t st)
 {
@@ -1438,6 +1510,20 @@ void LaunchEmhd::implicit_jacobian(const Dims& d, const DevGeom& g, double gam, 
                                    cudaStream_t st)
 {
     KHB_DISPATCH_HD(E, jac_hd, d, g, gam, E, ip, f, dt, jac, res, st);
+}
+
+void LaunchEmhd::floors(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, int32_t* fflag,
+                        cudaStream_t st)
+{
+    const long long nz = (long long)d.nx1 * d.nx2 * d.nx3;
+    k_emhd_floors<<<blocks_for(nz, 128), 128, 0, st>>>(d, g, ph, P, fflag);
+}
+
+void LaunchEmhd::limits(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,
+                        int32_t* eflag, cudaStream_t st)
+{
+    const long long nz = (long long)d.nx1 * d.nx2 * d.nx3;
+    k_emhd_limits<<<blocks_for(nz, 128), 128, 0, st>>>(d, g, gam, E, P, eflag);
 }
 
 void LaunchEmhd::fix_solve(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,

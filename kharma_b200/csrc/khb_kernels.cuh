@@ -861,7 +861,8 @@ __device__ __forceinline__ void inflow_fix(const ZoneGeom& G, const R gcov[4][4]
 
 // ===================================================================================== boundaries
 // Parthenon's outflow/reflecting functions (unvendored) as KHARMA applies them: fluid primitives
-// and the conserved field; then the inflow check (boundaries.hpp:101-136).  dir = 1 or 2.
+// and the conserved field; then the inflow check (boundaries.hpp:101-136).  NV = 10: the EMHD state,
+// whose scalar primitives q~, dP~ (slots 8, 9) are copied as the density is.
 template <int NV>
 __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int face,
                      int lo_a, int cnt_a, int lo_k, int cnt_k)
@@ -908,6 +909,10 @@ __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int
     for (int p = 0; p < 5; ++p) {
         const bool flip = ((type == KHB_BC_REFLECTING) && (p == 1 + bdir)) || (transmit && (p == 3 || p == 4));
         Pz[p] = (flip ? -1.0 : 1.0) * P.v[p][s];
+    }
+    if (NV == 10) {                          // slots that are not evolved may be NULL
+        if (P.v[8]) P.v[8][c] = P.v[8][s];
+        if (P.v[9]) P.v[9][c] = P.v[9][s];
     }
     if (NV > 5) {
 #pragma unroll
@@ -1522,7 +1527,8 @@ void Launch<FT>::fix_flux_x2(int nv, const Dims& d, const Phys& ph, FT* F1, FT* 
 {
     const int ni = d.ie - d.is + 3, nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
     const unsigned nb = blocks_for((long long)ni*nk, 128);
-    if (nv == 8) k_fix_flux_x2<8, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
+    if (nv == 10) k_fix_flux_x2<10, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
+    else if (nv == 8) k_fix_flux_x2<8, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
     else k_fix_flux_x2<5, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
 }
 
@@ -1787,7 +1793,8 @@ void LaunchCommon::bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, c
 {
     const int ng = (face < 2) ? d.is : ((face < 4) ? d.js : d.ks);
     const unsigned nb = blocks_for((long long)ng*cnt_a*cnt_k, 128);
-    if (nv == 8) k_bc<8><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
+    if (nv == 10) k_bc<10><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
+    else if (nv == 8) k_bc<8><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
     else k_bc<5><<<nb, 128, 0, st>>>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k);
 }
 

@@ -276,6 +276,11 @@ struct LaunchEmhd {
     static void implicit_jacobian(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E,
                                   const ImplicitArgs& ip, const ImpFields& f, double dt, double* jac, double* res,
                                   cudaStream_t st);
+    // ImEx stage: floors (fluid/drift frame) and stability limits over the interior, flag bits out
+    static void floors(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, int32_t* fflag,
+                       cudaStream_t st);
+    static void limits(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,
+                       int32_t* eflag, cudaStream_t st);
     static void fix_solve(const Dims& d, const DevGeom& g, double gam, const EmhdArgs& E, const khb_fields& P,
                           const khb_fields& U, const double* solve_fail, double* scratch, cudaStream_t st);
 };

@@ -46,6 +46,8 @@ class ImplicitSolver:
         self.implicit = implicit or ImplicitSpec()
         self._e = emhd.to_struct()
         self._i = self.implicit.to_struct()
+        # EMHD::eflag (emhd.cpp:162-165): the stability-limit bits of the last ImEx stage
+        self.eflag = torch.zeros(self.spec.shape, dtype=torch.int32, device=block.device)
         conn = build_connection(self.spec) if conn is None else np.ascontiguousarray(conn, dtype=np.float64)
         _lib.check(self.lib.khb_set_connection(block.ctx, conn.ctypes.data_as(C.c_void_p)), "khb_set_connection")
 
@@ -111,13 +113,23 @@ class ImplicitSolver:
                                                self.block.stream), "khb_copy_flux_emhd")
         return F, ctop
 
-    def imex_stage(self, stage, dt, P_full, U_full, P_sub, U_sub, P_out, U_out, solve_norm, solve_fail):
-        """One ImEx stage (vl2): fluxes, sources, explicit B update, Newton solve, FixSolve, P -> U."""
-        _lib.check(self.lib.khb_imex_stage(self.block.ctx, C.byref(self._e), C.byref(self._i), stage, float(dt),
-                                           Fields(P_full).ref, Fields(U_full).ref, Fields(P_sub).ref,
-                                           Fields(U_sub).ref, Fields(P_out).ref, Fields(U_out).ref,
-                                           C.c_void_p(solve_norm.data_ptr()), C.c_void_p(solve_fail.data_ptr()),
-                                           self.block.stream), "khb_imex_stage")
+    def imex_stage(self, stage, dt, P_full, U_full, P_sub, U_sub, P_out, U_out, solve_norm, solve_fail,
+                   fflag=None, eflag=None):
+        """One ImEx stage (vl2): fluxes, flux fixes, sources, explicit B update, Newton solve, floors and
+        EMHD limits, FixSolve, ghost zones, P -> U.  fflag/eflag (int32 fields) receive the floor and
+        limit bits of the interior; the block's own fflag and this solver's eflag are used when the
+        floors or the limits are on and none is given."""
+        if fflag is None and self.block.spec.floors_on:
+            fflag = self.block.fflag
+        if eflag is None and self.emhd.stability_limits:
+            eflag = self.eflag
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        _lib.check(self.lib.khb_imex_stage_flags(self.block.ctx, C.byref(self._e), C.byref(self._i), stage,
+                                                 float(dt), Fields(P_full).ref, Fields(U_full).ref,
+                                                 Fields(P_sub).ref, Fields(U_sub).ref, Fields(P_out).ref,
+                                                 Fields(U_out).ref, C.c_void_p(solve_norm.data_ptr()),
+                                                 C.c_void_p(solve_fail.data_ptr()), ptr(fflag), ptr(eflag),
+                                                 self.block.stream), "khb_imex_stage_flags")
 
     def imex_step(self, P, U, dt, solve_norm, solve_fail):
         """One vl2 ImEx step in place on (P, U) through an intermediate state."""

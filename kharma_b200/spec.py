@@ -261,6 +261,8 @@ class EmhdSpec:
     viscosity_alpha: float = 1.0
     kappa: float = 1.0
     eta: float = 1.0
+    # emhd/stability_limits (emhd.cpp:118-125): limit q and dP to the instability bounds after the solve
+    stability_limits: bool = False
 
     @property
     def nfvar(self):
@@ -272,6 +274,7 @@ class EmhdSpec:
         s.closure = _lib.CLOSURE[self.closure_type]
         s.higher_order_terms, s.feedback = int(self.higher_order_terms), int(self.feedback)
         s.conduction, s.viscosity = int(self.conduction), int(self.viscosity)
+        s.stability_limits = int(self.stability_limits)
         s.tau, s.conduction_alpha, s.viscosity_alpha = self.tau, self.conduction_alpha, self.viscosity_alpha
         s.kappa, s.eta = self.kappa, self.eta
         return s

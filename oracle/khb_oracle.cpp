@@ -939,8 +939,10 @@ static void flux_ct(const Block& B, double* F1, double* F2, double* F3)
     }
 }
 // boundaries.cpp:611-690 (check_inflow flux limiting on X1, zero_flux on X2 poles)
-static void boundaries_fix_flux(const Block& B, double* F[3])
+// nvars: the variables whose fluxes the polar faces zero (8, or 10 with the EMHD slots)
+static void boundaries_fix_flux(const Block& B, double* F[3], int nvars = 0)
 {
+    if (nvars <= 0) nvars = B.nv;
     const size_t N = B.N;
     for (int face = 0; face < 4; ++face) {
         const int bdir = face / 2 + 1;
@@ -961,7 +963,7 @@ static void boundaries_fix_flux(const Block& B, double* F[3])
                 f = binner ? kmin(f, 0.) : kmax(f, 0.);
             }
             if (zero_flux)
-                for (int p = 0; p < B.nv; ++p) F[bdir-1][(size_t)p*N + c] = 0.;
+                for (int p = 0; p < nvars; ++p) F[bdir-1][(size_t)p*N + c] = 0.;
         }
     }
 }
@@ -1614,8 +1616,9 @@ static void check_inflow(const Block& B, double* P, size_t c, int j, int i, bool
         for (int v = 0; v < 3; ++v) P[(size_t)(2 + v)*B.N + c] = uvec[v];
     }
 }
-// One physical face: P (fluid primitives, vars 0-4) and U_B (vars 5-7 of U)
-static void physical_face(const Block& B, double* P, double* U, int face)
+// One physical face: P (fluid primitives, vars 0-4) and U_B (vars 5-7 of U); emhd: also the scalar
+// primitives q~, dP~ (slots 8, 9), copied as the density is (no sign change)
+static void physical_face(const Block& B, double* P, double* U, int face, bool emhd = false)
 {
     const int bdir = face / 2 + 1;
     const bool binner = (face % 2) == 0;
@@ -1645,6 +1648,8 @@ static void physical_face(const Block& B, double* P, double* U, int face)
             const bool flip = ((type == BC_REFLECT) && (p == 1 + bdir)) || (transmit && (p == 3 || p == 4));
             P[(size_t)p*N + c] = (flip ? -1.0 : 1.0) * P[(size_t)p*N + s];
         }
+        if (emhd)
+            for (int p = 8; p < 10; ++p) P[(size_t)p*N + c] = P[(size_t)p*N + s];
         if (B.nv > 5)
             for (int v = 0; v < 3; ++v) {
                 const bool flip = ((type == BC_REFLECT) && (v == bdir - 1)) || (transmit && v >= 1);
@@ -1658,18 +1663,20 @@ static void physical_face(const Block& B, double* P, double* U, int face)
 }
 // Fill all ghost zones: physical faces in the order Parthenon applies them (x1, x2, then the
 // fix_corner re-application of inner x1: boundaries.cpp:538-559), then periodic directions.
-static void apply_boundaries(const Block& B, double* P, double* U)
+// emhd: P and U hold the 10 slots of the EMHD state (the scalar slots q~, dP~ filled as well)
+static void apply_boundaries(const Block& B, double* P, double* U, bool emhd = false)
 {
+    const int nvars = emhd ? 10 : B.nv;
     // periodic directions first, so physical faces see filled corners exactly as after a sync
     for (int d = 1; d <= B.ndim; ++d)
-        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, B.nv, d); periodic_fill(B, U, B.nv, d); }
+        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, nvars, d); periodic_fill(B, U, nvars, d); }
     for (int face = 0; face < 2*B.ndim; ++face) {
         if (!phys_face(B.c.bc[face])) continue;
-        physical_face(B, P, U, face);
-        if (face == 3 && B.c.fix_corner_inner && phys_face(B.c.bc[0])) physical_face(B, P, U, 0);
+        physical_face(B, P, U, face, emhd);
+        if (face == 3 && B.c.fix_corner_inner && phys_face(B.c.bc[0])) physical_face(B, P, U, 0, emhd);
     }
     for (int d = 1; d <= B.ndim; ++d)
-        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, B.nv, d); periodic_fill(B, U, B.nv, d); }
+        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, P, nvars, d); periodic_fill(B, U, nvars, d); }
     // B_P = B_U/gdet in the ghost zones (BoundaryUtoP of B_FluxCT)
     if (B.nv > 5)
         for (int k = 0; k < B.n3; ++k) for (int j = 0; j < B.n2; ++j) for (int i = 0; i < B.n1; ++i) {
@@ -2280,8 +2287,8 @@ static void ct_stage(const Block& B, Fields& f, int s, double dt, const double* 
 static const int IQ = 8, IDP = 9, NVE = 10;
 
 enum Closure { CL_CONSTANT = 0, CL_SOUNDSPEED = 1, CL_KAPPA_ETA = 2, CL_TORUS = 3 };   // emhd.hpp:58
-struct EmhdParams {            // emhd.hpp:60-84 plus the package switches of emhd.cpp:60-72
-    int32_t type, higher_order_terms, feedback, conduction, viscosity, pad;
+struct EmhdParams {            // emhd.hpp:60-84 plus the package switches of emhd.cpp:60-72, 118-125
+    int32_t type, higher_order_terms, feedback, conduction, viscosity, stability_limits;
     double tau, conduction_alpha, viscosity_alpha, kappa, eta;
 };
 struct ImplicitParams {        // implicit.cpp:99-119 (jacobian: 0 finite difference, 1 exact)
@@ -3148,12 +3155,63 @@ static double min_ndt_from(const Block& B, const std::vector<double> cmax[3], co
     }
     return m;
 }
+// EMHD::ApplyEMHDLimits / apply_instability_limits (emhd.cpp:399-428, emhd_limits.hpp:55-130) over
+// the interior: the heat flux limited to 1.07 rho cs^3 and the pressure anisotropy to the mirror and
+// firehose bounds, by scaling q~ and dP~; returns the eflag bits per zone in eflag (HIT_Q_LIMIT 1,
+// HIT_DP_MAX_LIMIT 2, HIT_DP_MIN_LIMIT 4).  The reference's closing p_to_u is covered by the stage's
+// final P -> U over the whole block.
+static void emhd_limits(const Block& B, const EmhdParams& ep, double gam, double* P, double* eflag)
+{
+    const size_t N = B.N;
+    for (int k = B.ks; k <= B.ke; ++k) for (int j = B.js; j <= B.je; ++j) for (int i = B.is; i <= B.ie; ++i) {
+        const size_t c = B.id(k, j, i);
+        double Pc[NVE];
+        for (int v = 0; v < NVE; ++v) Pc[v] = P[(size_t)v*N + c];
+        int ef = 0;
+        const double rho = Pc[0], uu = Pc[1];
+        const double qtilde = ep.conduction ? Pc[IQ] : 0., dPtilde = ep.viscosity ? Pc[IDP] : 0.;
+        const double pg = (gam - 1.) * uu;
+        const double Theta = pg / rho;
+        const double cs = std::sqrt(gam * pg / (rho + (gam * uu)));
+        FV<double> D;
+        calc_4vecs_t(B, Pc, j, i, D);
+        const double bsq = kmax(tdot(D.bcon, D.bcov), SMALL);
+        // (the reference also evaluates the closure here; nothing below uses it)
+        double q, dP;
+        convert_prims_to_q_dP_t(qtilde, dPtilde, rho, Theta, cs*cs, ep, q, dP);
+        if (ep.conduction) {
+            const double qmax = 1.07 * rho * cs*cs*cs;
+            const double max_frac = kmax(std::fabs(q) / qmax, 1.);
+            if (std::fabs(q) / qmax > 1.) ef |= 1;
+            P[(size_t)IQ*N + c] = Pc[IQ] / max_frac;
+        }
+        if (ep.viscosity) {
+            const double dP_comp_ratio = kmax(pg - 2./3. * dP, SMALL) / kmax(pg + 1./3. * dP, SMALL);
+            const double dP_plus = kmin(1.07 * 0.5 * bsq * dP_comp_ratio, 1.49 * pg);
+            const double dP_minus = kmax(-1.07 * bsq, -2.99 * pg);
+            if (dP > 0. && (dP / dP_plus > 1.)) ef |= 2;
+            else if (dP < 0. && (dP / dP_minus > 1.)) ef |= 4;
+            if (dP > 0.) P[(size_t)IDP*N + c] = Pc[IDP] * (1. / kmax(dP / dP_plus, 1.));
+            else P[(size_t)IDP*N + c] = Pc[IDP] * (1. / kmax(dP / dP_minus, 1.));
+        }
+        if (eflag) eflag[c] = ef;
+    }
+}
+
+static bool has_physical_face(const Block& B)
+{
+    for (int face = 0; face < 2*B.ndim; ++face) if (phys_face(B.c.bc[face])) return true;
+    return false;
+}
+
 // One ImEx stage (s = 0, 1).  All arrays [10][N]; ghost zones of Pout/Uout start as copies of the
-// sub-step state (the guess copy) and periodic faces are refreshed; other faces must be exchange
-// faces (the caller's).  Returns the Newton iterations; *min_ndt from this stage's fluxes.
+// sub-step state (the guess copy); periodic and physical faces are filled, exchange faces are the
+// caller's.  fflag / eflag (optional, [N]): the floor and EMHD-limit bits of the interior zones.
+// Returns the Newton iterations; *min_ndt from this stage's fluxes.
 static int imex_stage(const Block& B, const EmhdParams& ep, const ImplicitParams& ip, int s, double dt,
                       const double* Pfull, const double* Ufull, const double* Psub, const double* Usub,
-                      double* Pout, double* Uout, double* solve_norm, double* solve_fail, double* min_ndt_out)
+                      double* Pout, double* Uout, double* solve_norm, double* solve_fail, double* min_ndt_out,
+                      double* fflag = nullptr, double* eflag = nullptr)
 {
     const size_t N = B.N, NA = (size_t)NVE*N;
     const double gam = B.c.gam;
@@ -3169,6 +3227,9 @@ static int imex_stage(const Block& B, const EmhdParams& ep, const ImplicitParams
         if (phys_face(B.c.bc[3])) zero_boundary_flux_x2(B, F[0], F[1], F[2], false);
     }
     flux_ct(B, F[0], F[1], F[2]);
+    // KBoundaries::FixFlux on the physical faces: inflow checks on X1, zero polar fluxes of every
+    // variable, q~ and dP~ included (boundaries.cpp:611-690)
+    boundaries_fix_flux(B, F, NVE);
     std::vector<double> dudt(NA, 0.);
     emhd_dudt(B, ep, F, Psub, dudt.data());
     // solver state: the sub-step state everywhere; explicit update of B over the interior
@@ -3190,9 +3251,26 @@ static int imex_stage(const Block& B, const EmhdParams& ep, const ImplicitParams
                                     solve_fail, bdt, nullptr);
     std::memcpy(Pout, Psol.data(), NA*sizeof(double));
     std::memcpy(Uout, Usol.data(), NA*sizeof(double));
+    // Packages::MeshApplyFloors over the interior (imex_step.cpp:269): the GRMHD floors (fluid and
+    // drift frames change P only; the U they form is replaced by the stage's final P -> U), then the
+    // EMHD package's stability limits
+    if (fflag) for (size_t x = 0; x < N; ++x) fflag[x] = 0.;
+    if (eflag) for (size_t x = 0; x < N; ++x) eflag[x] = 0.;
+    if (B.c.floors_on) {
+        std::vector<double> pflag_tmp(N, 0.), fflag_tmp(N, 0.);
+        apply_grmhd_floors(B, Pout, Uout, pflag_tmp.data(), fflag ? fflag : fflag_tmp.data(),
+                           B.ks, B.ke, B.js, B.je, B.is, B.ie);
+    }
+    if (ep.stability_limits) emhd_limits(B, ep, gam, Pout, eflag);
     fix_solve(B, ep, gam, Pout, Uout, solve_fail);
-    for (int d = 1; d <= B.ndim; ++d)
-        if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, Pout, NVE, d); periodic_fill(B, Uout, NVE, d); }
+    // ApplyBoundaryConditionsOnCoarseOrFineMD (imex_step.cpp:297-298): periodic images and the physical
+    // faces of the 10-slot state, B_P from U_B in the ghost zones
+    if (has_physical_face(B)) {
+        apply_boundaries(B, Pout, Uout, true);
+    } else {
+        for (int d = 1; d <= B.ndim; ++d)
+            if (B.c.bc[2*(d-1)] == BC_PERIODIC) { periodic_fill(B, Pout, NVE, d); periodic_fill(B, Uout, NVE, d); }
+    }
     emhd_ptou(B, ep, gam, Pout, Uout);
     if (min_ndt_out) *min_ndt_out = min_ndt_from(B, cmx, cmn);
     return iters;
@@ -3430,6 +3508,15 @@ int orc_imex_stage(void* hp, const EmhdParams* ep, const ImplicitParams* ip, int
 {
     return imex_stage(((Handle*)hp)->B, *ep, *ip, stage - 1, dt, Pfull, Ufull, Psub, Usub, Pout, Uout,
                       solve_norm, solve_fail, min_ndt);
+}
+// The same with the floor and EMHD-limit flags of the interior zones ([N] each)
+int orc_imex_stage_flags(void* hp, const EmhdParams* ep, const ImplicitParams* ip, int stage, double dt,
+                         const double* Pfull, const double* Ufull, const double* Psub, const double* Usub,
+                         double* Pout, double* Uout, double* solve_norm, double* solve_fail, double* min_ndt,
+                         double* fflag, double* eflag)
+{
+    return imex_stage(((Handle*)hp)->B, *ep, *ip, stage - 1, dt, Pfull, Ufull, Psub, Usub, Pout, Uout,
+                      solve_norm, solve_fail, min_ndt, fflag, eflag);
 }
 
 // ---- EMHD and the implicit solve.  All field arrays are [10][N] (slots rho..B3, q, dP).

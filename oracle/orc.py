@@ -116,6 +116,8 @@ def load():
     lib.orc_get_flux_emhd.argtypes = [P, P, C.c_int, P, P, P, P]
     lib.orc_imex_stage.restype = C.c_int
     lib.orc_imex_stage.argtypes = [P, P, P, C.c_int, C.c_double, P, P, P, P, P, P, P, P, P]
+    lib.orc_imex_stage_flags.restype = C.c_int
+    lib.orc_imex_stage_flags.argtypes = [P, P, P, C.c_int, C.c_double, P, P, P, P, P, P, P, P, P, P, P]
     _lib = lib
     return lib
 
@@ -358,10 +360,22 @@ class Oracle:
                                      _ptr(solve_norm), _ptr(solve_fail), C.byref(mn))
         return Pout, Uout, it, mn.value
 
+    def imex_stage_flags(self, emhd, imp, stage, dt, Pfull, Ufull, Psub, Usub, solve_norm, solve_fail):
+        """imex_stage with the interior floor and EMHD-limit flags: (Pout, Uout, iterations, min zone dt,
+        fflag, eflag)."""
+        Pout, Uout = self.zeros10(), self.zeros10()
+        fflag, eflag = np.zeros(self.shape), np.zeros(self.shape)
+        mn = C.c_double()
+        it = self.lib.orc_imex_stage_flags(self.h, C.byref(emhd_params(emhd)), C.byref(implicit_params(imp)), stage,
+                                           dt, _ptr(Pfull), _ptr(Ufull), _ptr(Psub), _ptr(Usub), _ptr(Pout),
+                                           _ptr(Uout), _ptr(solve_norm), _ptr(solve_fail), C.byref(mn),
+                                           _ptr(fflag), _ptr(eflag))
+        return Pout, Uout, it, mn.value, fflag, eflag
+
 
 class EmhdParams(C.Structure):
     _fields_ = [("type", C.c_int32), ("higher_order_terms", C.c_int32), ("feedback", C.c_int32),
-                ("conduction", C.c_int32), ("viscosity", C.c_int32), ("pad", C.c_int32),
+                ("conduction", C.c_int32), ("viscosity", C.c_int32), ("stability_limits", C.c_int32),
                 ("tau", C.c_double), ("conduction_alpha", C.c_double), ("viscosity_alpha", C.c_double),
                 ("kappa", C.c_double), ("eta", C.c_double)]
 
@@ -381,6 +395,7 @@ def emhd_params(e):
     s.type = CLOSURE[e.closure_type]
     s.higher_order_terms, s.feedback = int(e.higher_order_terms), int(e.feedback)
     s.conduction, s.viscosity = int(e.conduction), int(e.viscosity)
+    s.stability_limits = int(getattr(e, "stability_limits", False))
     s.tau, s.conduction_alpha, s.viscosity_alpha = e.tau, e.conduction_alpha, e.viscosity_alpha
     s.kappa, s.eta = e.kappa, e.eta
     return s

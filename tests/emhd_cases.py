@@ -60,3 +60,34 @@ def implicit(jacobian="fd", **kw):
     base = dict(min_nonlinear_iter=1, max_nonlinear_iter=8, rootfind_tol=1e-10, jacobian=jacobian)
     base.update(kw)
     return ImplicitSpec(**base)
+
+
+# A block with every ImEx boundary and limit step in play: the atmosphere's own faces (outflow X1
+# with inflow checks, reflecting X2 with the polar flux fixes and the corner fix, periodic X3),
+# geometric density floors that bind in the inner part of the block, the EMHD stability limits on,
+# a monopole field strong enough for the anisotropy bounds to matter, and q~ / dP~ raised in seeded
+# zones so that the limit bits are hit.
+LIMITS_CASES = {
+    # closure, B10, q~ factor, dP~ amplitude (in units of u)
+    "constant": ("constant", 5e5, 5000.0, 2.0),
+    "kappa_eta_ho": ("kappa_eta_ho", 2e6, 5000.0, 30.0),
+}
+
+
+def atmosphere_limits_case(name, n1=64, n2=6, n3=1, seed=3):
+    """(spec, emhd, P) for LIMITS_CASES[name] on an n1 x n2 x n3 atmosphere block."""
+    import dataclasses
+    from kharma_b200.block import build_geometry
+    from kharma_b200.spec import FloorSpec
+    variant, B10, qfac, dpamp = LIMITS_CASES[name]
+    emhd = dataclasses.replace(EMHD_VARIANTS[variant], stability_limits=True)
+    spec = dataclasses.replace(atmosphere_spec(n1, n2, n3), floors_on=True, floor_frame="drift",
+                               floors=FloorSpec(rho_min_geom=8000.0, u_min_geom=1e-8),
+                               check_inflow_inner_x1=True, check_inflow_outer_x1=True,
+                               zero_polar_flux=True, fix_polar_flux=True, fix_corner_inner=True)
+    P = problems.conducting_atmosphere(spec, build_geometry(spec), emhd, profile(n1), jitter=1e-3, seed=seed,
+                                       B10=B10)
+    m = np.random.Generator(np.random.PCG64(seed + 8)).uniform(size=P.shape[1:])
+    P[8] *= np.where(m < 0.2, qfac, 1.0)
+    P[9] = np.where(m > 0.85, dpamp, np.where(m > 0.7, -dpamp, 0.0)) * P[1]
+    return spec, emhd, P

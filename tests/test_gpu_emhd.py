@@ -239,3 +239,85 @@ def test_imex_step_matches_oracle(oracle_mod, variant):
         assert rel_err(Ug[s][sl[1:]], U[s][sl[1:]]) <= tol, f"U slot {s}"
     assert np.array_equal(sf_d.cpu().numpy()[spec.interior], sf[spec.interior])
     assert abs(mn_d - mn) <= 1e-12 * abs(mn)
+
+
+@pytest.mark.parametrize("shape", ["2d", "3d"])
+@pytest.mark.parametrize("name", ["constant", "kappa_eta_ho"])
+def test_imex_floors_limits_physical_faces_match_oracle(oracle_mod, name, shape):
+    """Two vl2 ImEx steps on a block with outflow X1 (inflow checks), reflecting X2 (polar flux fixes,
+    corner fix) and periodic X3 faces, drift-frame floors and the EMHD stability limits: the flux fixes
+    of all 10 slots, the floors and limits after the solve, FixSolve and the 10-slot ghost zones
+    (imex_step.cpp:58-356).  Primitives and conserved variables over the whole block, ghost zones
+    included, within 1e-12 of the oracle per slot; floor and limit flags and solver status equal; the
+    zone timestep minimum within 1e-12."""
+    from emhd_cases import atmosphere_limits_case
+    n1, n2, n3 = SHAPES[shape]
+    spec, emhd, P = atmosphere_limits_case(name, n1, n2, n3)
+    o = oracle_mod.Oracle(spec)
+    b = Block(spec, geometry=o.geometry())
+    sol = ImplicitSolver(b, emhd, conn=o.connection())
+    U = o.emhd_ptou(emhd, P)
+    imp = implicit("fd", max_nonlinear_iter=3, rootfind_tol=1e-12)
+    sol.set_implicit(imp)
+    dt = 0.5
+    Pd, Ud = dev(P), dev(U)
+    sn_d, sf_d = sol.scalar_field(), sol.scalar_field()
+    sn, sf = np.zeros(spec.shape), np.zeros(spec.shape)
+    sl = spec.interior
+    seen = 0
+    for _ in range(2):
+        P1, U1, _, _, ff1, ef1 = o.imex_stage_flags(emhd, imp, 1, dt, P, U, P, U, sn, sf)
+        P1d, U1d = sol.zeros(), sol.zeros()
+        sol.imex_stage(1, dt, Pd, Ud, Pd, Ud, P1d, U1d, sn_d, sf_d)
+        assert np.array_equal(b.fflag.cpu().numpy()[sl], ff1[sl].astype(np.int32))
+        assert np.array_equal(sol.eflag.cpu().numpy()[sl], ef1[sl].astype(np.int32))
+        P, U, _, mn, ff2, ef2 = o.imex_stage_flags(emhd, imp, 2, dt, P, U, P1, U1, sn, sf)
+        P2d, U2d = sol.zeros(), sol.zeros()
+        sol.imex_stage(2, dt, Pd, Ud, P1d, U1d, P2d, U2d, sn_d, sf_d)
+        assert np.array_equal(b.fflag.cpu().numpy()[sl], ff2[sl].astype(np.int32))
+        assert np.array_equal(sol.eflag.cpu().numpy()[sl], ef2[sl].astype(np.int32))
+        seen |= int(np.bitwise_or.reduce(ef2[sl].astype(int), axis=None))
+        Pd, Ud = P2d, U2d
+        mn_d = b.min_ndt()
+        assert abs(mn_d - mn) <= 1e-12 * abs(mn)
+        Pg, Ug = Pd.cpu().numpy(), Ud.cpu().numpy()
+        for s in slots(emhd):
+            assert rel_err(Pg[s], P[s]) <= 1e-12, f"P slot {s}: {rel_err(Pg[s], P[s])}"
+            assert rel_err(Ug[s], U[s]) <= 1e-12, f"U slot {s}: {rel_err(Ug[s], U[s])}"
+        assert np.array_equal(sf_d.cpu().numpy()[sl], sf[sl])
+    assert seen & 1 and seen & 2
+
+
+def test_imex_stage_flag_arguments(oracle_mod):
+    """khb_imex_stage_flags without flag fields rejects floors or limits that would write them
+    (KHB_ERR_ARG), and the normal-observer floor frame is rejected on the EMHD state
+    (KHB_ERR_UNSUPPORTED)."""
+    import ctypes as C
+    import dataclasses
+    from emhd_cases import atmosphere_limits_case
+    from kharma_b200.block import Fields
+    OK, ERR_ARG, ERR_UNSUPPORTED = 0, -1, -4      # khb.h return codes
+    spec, emhd, P = atmosphere_limits_case("constant")
+    o = oracle_mod.Oracle(spec)
+    U = o.emhd_ptou(emhd, P)
+
+    def call(spec, emhd, with_flags):
+        b = Block(spec, geometry=o.geometry())
+        sol = ImplicitSolver(b, emhd, conn=o.connection())
+        Pd, Ud = dev(P), dev(U)
+        Po, Uo = sol.zeros(), sol.zeros()
+        sn, sf = sol.scalar_field(), sol.scalar_field()
+        fl = [C.c_void_p(b.fflag.data_ptr()), C.c_void_p(sol.eflag.data_ptr())] if with_flags else [None, None]
+        rc = sol.lib.khb_imex_stage_flags(b.ctx, C.byref(sol._e), C.byref(sol._i), 1, 0.5, Fields(Pd).ref,
+                                          Fields(Ud).ref, Fields(Pd).ref, Fields(Ud).ref, Fields(Po).ref,
+                                          Fields(Uo).ref, C.c_void_p(sn.data_ptr()), C.c_void_p(sf.data_ptr()),
+                                          fl[0], fl[1], b.stream)
+        torch.cuda.synchronize()
+        return rc
+
+    assert call(spec, emhd, True) == OK
+    assert call(spec, emhd, False) == ERR_ARG
+    assert call(dataclasses.replace(spec, floors_on=False), emhd, False) == ERR_ARG   # the limits are on
+    assert call(dataclasses.replace(spec, floors_on=False), dataclasses.replace(emhd, stability_limits=False),
+                False) == OK
+    assert call(dataclasses.replace(spec, floor_frame="normal"), emhd, True) == ERR_UNSUPPORTED

@@ -185,3 +185,53 @@ def test_imex_keeps_conducting_atmosphere_in_equilibrium(oracle_mod):
     assert not (sf[sl] == 1).any()
     for v in (0, 1, 8):
         assert np.max(np.abs(P[v][sl] - P0[v][sl])) / np.max(np.abs(P0[v][sl])) < 1e-4, v
+
+
+@pytest.mark.parametrize("name", ["constant", "kappa_eta_ho"])
+def test_imex_stage_floors_limits_and_physical_faces(oracle_mod, name):
+    """An ImEx stage on a block with physical faces, floors and the EMHD stability limits
+    (imex_step.cpp:269-298, emhd_limits.hpp:55-130): the limit bits are all hit, a zone the heat-flux
+    limit scaled holds |q| = 1.07 rho cs^3 (constant closure: q = q~), and the ghost zones of q~ / dP~
+    copy the boundary zones (outflow X1) or their mirror images (reflecting X2) without a sign change."""
+    import dataclasses
+    from emhd_cases import atmosphere_limits_case
+    spec, emhd, P = atmosphere_limits_case(name)
+    o = oracle_mod.Oracle(spec)
+    U = o.emhd_ptou(emhd, P)
+    imp = implicit("fd", max_nonlinear_iter=3, rootfind_tol=1e-12)
+    sn, sf = np.zeros(spec.shape), np.zeros(spec.shape)
+    Pout, Uout, _, _, ff, ef = o.imex_stage_flags(emhd, imp, 1, 0.5, P, U, P, U, sn, sf)
+    sl = spec.interior
+    ef_i, ff_i = ef[sl].astype(int), ff[sl].astype(int)
+    assert (ef_i & 1).any() and (ef_i & 2).any() and (ef_i & 4).any()
+    assert ff_i.any() and not ff_i.all()
+    assert np.isfinite(Pout).all() and np.isfinite(Uout).all()
+    ok = sf[sl] != 1          # zones FixSolve left alone
+    gam = spec.gam
+
+    def qmax(Q):
+        rho, u = Q[0][sl], Q[1][sl]
+        return 1.07 * rho * np.sqrt(gam * (gam - 1.) * u / (rho + gam * u)) ** 3
+
+    if name == "constant":
+        hit = ((ef_i & 1) != 0) & ok
+        assert hit.any()
+        np.testing.assert_allclose(np.abs(Pout[8][sl][hit]), qmax(Pout)[hit], rtol=1e-12)
+        assert np.all(np.abs(Pout[8][sl][ok]) <= qmax(Pout)[ok] * (1 + 1e-12))
+    # the same stage without the limits leaves the flags clear (and, constant closure, the bound broken)
+    free = dataclasses.replace(emhd, stability_limits=False)
+    sn2, sf2 = np.zeros(spec.shape), np.zeros(spec.shape)
+    Pfree, _, _, _, _, ef2 = o.imex_stage_flags(free, imp, 1, 0.5, P, U, P, U, sn2, sf2)
+    assert not ef2.any()
+    if name == "constant":
+        assert np.any(np.abs(Pfree[8][sl]) > qmax(Pfree) * (1 + 1e-6))
+    # ghost zones of the scalar slots (2D block: one k plane)
+    ng = spec.ng
+    js, je, is_, ie = ng, ng + spec.nx2 - 1, ng, ng + spec.nx1 - 1
+    for s in (8, 9):
+        A = Pout[s][0]
+        for g in range(ng):
+            np.testing.assert_array_equal(A[js:je + 1, g], A[js:je + 1, is_])
+            np.testing.assert_array_equal(A[js:je + 1, ie + 1 + g], A[js:je + 1, ie])
+            np.testing.assert_array_equal(A[g, is_:ie + 1], A[2 * js - 1 - g, is_:ie + 1])
+            np.testing.assert_array_equal(A[je + 1 + g, is_:ie + 1], A[je - g, is_:ie + 1])
