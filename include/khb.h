@@ -316,15 +316,20 @@ int khb_step_graph(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, int32
  * none) adds the objective sum over stages of weight_scale * sum_faces weight[f] * F1[rho][f] of
  * the raw x1 face fluxes ([N] doubles, indexed like the zone arrays; with weight_scale = dt/2 and
  * weights of dx2 dx3 on one x1 face layer, the RK2-consistent mass through that layer in the step).
- * The intermediate stage is recomputed from (P_n, U_n) into the context's stage scratch; the
- * inversion is differentiated by the implicit-function theorem at the converged state; periodic
+ * Both stages are recomputed from (P_n, U_n) (the intermediate one into the context's stage
+ * scratch); the inversion is differentiated by the implicit-function theorem at the converged
+ * state; the floors (fluid or drift frame, floors_functions.hpp:50-252) through the Jacobian of the
+ * floor map at the inverted primitives before the floors, which the recompute keeps; a zone whose
+ * inversion failed through its fixup (fixup.cpp:47-156: the weighted neighbour average, its
+ * geometric floors and the zone's own B); periodic
  * ghost-zone adjoints are folded into their images, exchange ghost zones are constants, and the
  * ghost fills of outflow/reflecting X1/X2 faces (inflow checks, the corner fix, the ghost B of MHD
  * blocks) and the flux fixes (the X1 mass-flux clip, zero polar fluxes, B_FluxCT's polar B-flux fix,
  * boundaries.cpp:369-690, b_flux_ct.cpp:372-418) are transposed.  Supported: LLF fluxes with linear MC
- * or donor-cell reconstruction, periodic, exchange, outflow or reflecting faces, floors, recon floors
- * and FOFC off (KHB_ERR_UNSUPPORTED otherwise).  Ghost zones of Pbar/Ubar are zero on return.
- * Scratch (6 nv N doubles, 2 N flags) is allocated on the first call. */
+ * or donor-cell reconstruction, periodic, exchange, outflow or reflecting faces, floors off or in the
+ * fluid or drift frame with the 1D_W inverter, recon floors and FOFC off (KHB_ERR_UNSUPPORTED
+ * otherwise).  Ghost zones of Pbar/Ubar are zero on return.  Scratch (8 nv N doubles, 4 N flags;
+ * with floors 10 N doubles more) is allocated on the first call. */
 int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_fields* U_n,
                      const khb_fields* P_np1, const khb_fields* Pbar, const khb_fields* Ubar,
                      const double* rho_flux1_weight, double weight_scale, void* stream);

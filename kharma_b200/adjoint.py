@@ -16,8 +16,9 @@ with U_0 = U(P_0) (khb_adjoint_ptou).  Memory: one state per checkpoint plus one
 the longest segment.
 
 The timestep sequence is an input: the adjoint is that of the run at those dts (the CFL control
-that chose them is not differentiated).  Inversion failures (and so fixups) make the run
-non-differentiable; `forward` raises if any zone failed.
+that chose them is not differentiated).  Zones whose inversion fails take their fixup (an average of
+the neighbours) and are differentiated through it; `forward` counts them (`Run.failures`), since
+the objective is not differentiable where a perturbation turns a failure into a success.
 """
 import ctypes as C
 
@@ -25,10 +26,6 @@ import torch
 
 from . import _lib
 from .block import Block, Fields
-
-
-class NotDifferentiable(RuntimeError):
-    pass
 
 
 class Run:
@@ -44,6 +41,7 @@ class Run:
         self.Us = torch.empty_like(block.U)
         self.Psf, self.Usf = Fields(self.Ps), Fields(self.Us)
         self.checkpoints = []
+        self.failures = 0
 
     # ------------------------------------------------------------- forward
     def _stage(self, stage, dt, Pin, Uin, U0, Pout, Uout):
@@ -81,8 +79,7 @@ class Run:
             if n % self.K == 0:
                 self.checkpoints.append((b.P.clone(), b.U.clone()))
             self._step(dt, fails, J)
-        if int(fails.item()):
-            raise NotDifferentiable(f"{int(fails.item())} zone inversions failed: fixups are not differentiated")
+        self.failures = int(fails.item())
         if self.Pw is not None:
             J = J + (self.Pw * b.P).sum()
         if self.Uw is not None:

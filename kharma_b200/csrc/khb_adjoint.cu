@@ -13,8 +13,11 @@
 //   Fbar += transpose of the divergence (and of flux-CT), Pbar_s += beta dt (dS/dP)^T Ubar_upd,
 //   Pbar_s += (dF/dP_stencil)^T Fbar                      (per face, scattered with atomics).
 // Local Jacobians come from the same templated device functions the forward kernels use, evaluated
-// on Dual numbers with one unit tangent per input.  Out of scope (rejected): floors, failed-zone
-// fixups, physical boundaries (outflow/reflecting faces), WENO5/PPM, HLLE.  Periodic ghost zones are
+// on Dual numbers with one unit tangent per input.  With floors (fluid or drift frame, 1D_W), the
+// recompute keeps each stage's inverted primitives before the floors, and a floored zone's adjoint
+// passes through the floor map's Jacobian (k_adj_cell); a zone whose inversion failed takes the
+// adjoint of its fixup (k_adj_fixup).  Out of scope (rejected): normal-frame and mixed-frame floors,
+// reconstruction floors, FOFC, transmitting faces, WENO5/PPM, HLLE.  Periodic ghost zones are
 // copies of their images, so their adjoints are folded into the images; exchange ghost zones are
 // the caller's constants and their adjoints are dropped.  The timestep is taken as given (the
 // forward run's sequence).
@@ -216,14 +219,208 @@ __device__ __forceinline__ void solve_transposed(double A[N][N], double b[N])
     }
 }
 
-// Ubar_upd = Ubar_out + J(P_out)^-T Pbar_out over the interior (zero elsewhere)
+// ---------------------------------------------------------------------------- floors
+// The floors of one zone on dual numbers: the operations of determine_floors, apply_floors_frame
+// (fluid and drift frames) and apply_ceilings (floors_functions.hpp:50-252, floors_impl.hpp:77-125)
+// in the same order, every branch taken by the value as the forward evaluation takes it.  Called
+// only for zones the forward run floored (fflag != 0), as the forward applies the frame and the
+// ceilings only there.  P: rho, u, u1-u3 (and B1-B3); the fluid primitives are replaced.
 template <int NV>
-__global__ void __launch_bounds__(128) k_adj_cell(Dims d, DevGeom g, Phys ph, khb_fields Pout, khb_fields Pbar_out,
-                                                  khb_fields Ubar_out, double* Ubar_upd, Box bx)
+__device__ void floors_dual(const ZoneGeom& G, const Prescription& f, double rhoflr_geom, double uflr_geom,
+                            double gam, int frame, Dual<double>* P)
+{
+    typedef Dual<double> DD;
+    DD gcov[4][4], gcon0[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        gcon0[a] = DD(G.gcon[0][a]);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) gcov[a][b] = DD(G.gcov[a][b]);
+    }
+    // determine_floors: the floor values
+    FourVec<DD> D;
+    calc_4vecs<DD, (NV > 5)>(gcov, gcon0[0], gcon0, P, D);
+    const DD bsq = dot4(D.bcon, D.bcov);
+    const DD rhoflr_b = bsq / DD(f.bsq_over_rho_max);
+    const DD uflr_b = bsq / DD(f.bsq_over_u_max);
+    const DD uflr_max = kmax(DD(uflr_geom), uflr_b);
+    DD rhoflr_max;
+    if (!f.temp_adjust_u) {
+        const DD rhoflr_temp = kmax(P[1], uflr_max) / DD(f.u_over_rho_max);
+        rhoflr_max = kmax(kmax(DD(rhoflr_geom), rhoflr_b), rhoflr_temp);
+    } else {
+        rhoflr_max = kmax(DD(rhoflr_geom), rhoflr_b);
+    }
+    // apply_floors_frame
+    if (frame == KHB_FRAME_FLUID) {
+        P[0] += kmax(DD(0.), rhoflr_max - P[0]);
+        P[1] += kmax(DD(0.), uflr_max - P[1]);
+    } else {
+        const double lapse2 = 1. / (-G.gcon[0][0]);
+        double beta[4] = {0., 0., 0., 0.};
+        beta[1] = lapse2 * G.gcon[0][1];
+        beta[2] = lapse2 * G.gcon[0][2];
+        beta[3] = lapse2 * G.gcon[0][3];
+        const DD rho = P[0], uu = P[1];
+        const DD pg = DD(gam - 1.) * uu;
+        const DD w_old = kmax(rho + uu + pg, DD(1e-20));
+        DD Bcon[4] = {DD(0.), DD(0.), DD(0.), DD(0.)}, Bcov[4] = {DD(0.), DD(0.), DD(0.), DD(0.)};
+        if (NV > 5) { Bcon[1] = P[5]; Bcon[2] = P[6]; Bcon[3] = P[7]; }
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+#pragma unroll
+            for (int nu = 0; nu < 4; ++nu) Bcov[mu] += gcov[mu][nu] * Bcon[nu];
+        const DD Bsq = kmax(dot4(Bcon, Bcov), DD(1e-20));
+        const DD B_mag = dsqrt(Bsq);
+        DD Qcov[4];
+        Qcov[0] = w_old * D.ucon[0] * D.ucov[0] + pg;
+        Qcov[1] = w_old * D.ucon[0] * D.ucov[1];
+        Qcov[2] = w_old * D.ucon[0] * D.ucov[2];
+        Qcov[3] = w_old * D.ucon[0] * D.ucov[3];
+        const DD QdotB = dot4(Bcon, Qcov);
+        DD vpar = QdotB / (B_mag * w_old * D.ucon[0] * D.ucon[0]);
+        DD ucon_dr[4] = {DD(0.), DD(0.), DD(0.), DD(0.)};
+        ucon_dr[0] = DD(1.) / dsqrt(DD(1.) / (D.ucon[0] * D.ucon[0]) + vpar * vpar);
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+            ucon_dr[mu] = D.ucon[mu] * (ucon_dr[0] / D.ucon[0]) - (vpar * Bcon[mu] * ucon_dr[0] / B_mag);
+        P[0] = kmax(rho, rhoflr_max);
+        P[1] = kmax(uu, uflr_max);
+        const DD pg_new = DD(gam - 1.) * P[1];
+        const DD w_new = P[0] + P[1] + pg_new;
+        const DD x = (DD(2.) * QdotB) / (B_mag * w_new * ucon_dr[0]);
+        vpar = x / (DD(1.) + dsqrt(DD(1.) + x * x)) * (DD(1.) / ucon_dr[0]);
+        DD uc[4];
+        uc[0] = DD(1.) / dsqrt(DD(1.) / (ucon_dr[0] * ucon_dr[0]) - vpar * vpar);
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) uc[mu] = ucon_dr[mu] * (uc[0] / ucon_dr[0]) + (vpar * Bcon[mu] * uc[0] / B_mag);
+        P[2] = uc[1] + (DD(beta[1]) * uc[0]);
+        P[3] = uc[2] + (DD(beta[2]) * uc[0]);
+        P[4] = uc[3] + (DD(beta[3]) * uc[0]);
+    }
+    // apply_ceilings
+    const DD gamma = lorentz(gcov, P[2], P[3], P[4]);
+    if (gamma.v > f.gamma_max) {
+        const DD fr = dsqrt(DD(f.gamma_max * f.gamma_max - 1.) / (gamma * gamma - DD(1.)));
+#pragma unroll
+        for (int v = 0; v < 3; ++v) P[2 + v] *= fr;
+    }
+    if (ktot_above(gam, P[0].v, P[1].v, f.ktot_max)) {
+        // d pow(rho, gam) = gam pow(rho, gam) / rho d rho
+        const double pw = pow(P[0].v, gam);
+        const DD rg(pw, gam * pw / P[0].v * P[0].d);
+        const DD ktot = DD(gam - 1.) * P[1] / rg;
+        P[1] = DD(f.ktot_max) / ktot * P[1];
+    }
+    if (f.temp_adjust_u && P[1].v / P[0].v > f.u_over_rho_max) P[1] = DD(f.u_over_rho_max) * P[0];
+}
+
+// Adjoint of FixUtoP (fixup.cpp:47-156 as fixup_zone runs it): a failed zone (pflag > 0) takes the
+// 1/(Manhattan + 1)-weighted average of its good neighbours' fluid primitives (the neighbourhood of
+// fixup_zone: periodic directions wrap, exchange faces reach the caller's ghost zones, physical
+// faces end it), raised to the geometric floors, keeps the B of its own update (B_P = U_B/sqrt(-g))
+// and forms U = U(P).  With t = Pbar_out + J(P_fix)^T Ubar_out, its adjoint goes to the good interior
+// neighbours' Pbar_out (fluid, by weight; a neighbour across an exchange face is the caller's
+// constant), and to its own updated B (Ubar_upd_B = t_B / sqrt(-g)); its fluid update is discarded.
+// Runs before k_adj_cell, which then sees the neighbours' complete Pbar_out and skips failed zones.
+template <int NV>
+__global__ void __launch_bounds__(128) k_adj_fixup(Dims d, DevGeom g, Phys ph, khb_fields Pout, khb_fields Pbar_out,
+                                                   khb_fields Ubar_out, const int32_t* pflag, double* Ubar_upd,
+                                                   Box bx)
 {
     int i, j, k;
     if (!box_cell(bx, blockIdx.x, i, j, k)) return;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    if (!(pflag[c] > 0)) return;
+    double P[NV], J[NV][NV], t[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) P[p] = Pout.v[p][c];
+    ZoneGeom G;
+    load_zone_geom(g, j, i, G);
+    ptou_jacobian<NV>(G, ph.gam, P, J);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double s = Pbar_out.v[q][c];
+#pragma unroll
+        for (int p = 0; p < NV; ++p) s += J[p][q] * Ubar_out.v[p][c];
+        t[q] = s;
+    }
+    // B: from the zone's own update
+#pragma unroll
+    for (int v = 5; v < NV; ++v) Ubar_upd[v*d.N + c] = t[v] / G.gdet;
+    if (!ph.fix_avg) return;             // the atmosphere values depend on the geometry alone
+    // a good neighbour of fixup_zone's neighbourhood: x the zone it reads, inside whether x is an
+    // interior zone (else a ghost zone across an exchange face)
+    auto neighbour = [&](int l, int m, int nn, long long& x, bool& inside) -> bool {
+        int ii = i + l, jj = j + m, kk = k + nn;
+        inside = true;
+        if (ii < d.is || ii > d.ie) {
+            const int bc = d.bc[(ii < d.is) ? 0 : 1];
+            if (bc == KHB_BC_PERIODIC) ii += (ii < d.is) ? d.nx1 : -d.nx1;
+            else if (bc != KHB_BC_EXCHANGE) return false;
+            else inside = false;
+        }
+        if (jj < d.js || jj > d.je) {
+            const int bc = d.bc[(jj < d.js) ? 2 : 3];
+            if (d.ndim < 2) return false;
+            if (bc == KHB_BC_PERIODIC) jj += (jj < d.js) ? d.nx2 : -d.nx2;
+            else if (bc != KHB_BC_EXCHANGE) return false;
+            else inside = false;
+        }
+        if (kk < d.ks || kk > d.ke) {
+            const int bc = d.bc[(kk < d.ks) ? 4 : 5];
+            if (d.ndim < 3) return false;
+            if (bc == KHB_BC_PERIODIC) kk += (kk < d.ks) ? d.nx3 : -d.nx3;
+            else if (bc != KHB_BC_EXCHANGE) return false;
+            else inside = false;
+        }
+        x = ((long long)kk*d.n2 + jj)*d.n1 + ii;
+        return !(pflag[x] > 0);
+    };
+    double wsum = 0., sum[2] = {0., 0.};
+    for (int nn = -1; nn <= 1; nn++) for (int m = -1; m <= 1; m++) for (int l = -1; l <= 1; l++) {
+        long long x;
+        bool inside;
+        if (!neighbour(l, m, nn, x, inside)) continue;
+        const double w = 1./(abs(l) + abs(m) + abs(nn) + 1);
+        wsum += w;
+        sum[0] += w * Pout.v[0][x];
+        sum[1] += w * Pout.v[1][x];
+    }
+    if (wsum < 1.e-10) return;
+    // the geometric floors of the average: where one raised it, that component is a constant
+    const long long cg = (long long)j*g.n1 + i;
+    const double rf = g.floor_rho[cg], uf = g.floor_u[cg];
+    double tf[5];
+#pragma unroll
+    for (int p = 0; p < 5; ++p) tf[p] = t[p] / wsum;
+    if (0. < rf - sum[0]/wsum) tf[0] = 0.;
+    if (0. < uf - sum[1]/wsum) tf[1] = 0.;
+    for (int nn = -1; nn <= 1; nn++) for (int m = -1; m <= 1; m++) for (int l = -1; l <= 1; l++) {
+        long long x;
+        bool inside;
+        if (!neighbour(l, m, nn, x, inside) || !inside) continue;
+        const double w = 1./(abs(l) + abs(m) + abs(nn) + 1);
+#pragma unroll
+        for (int p = 0; p < 5; ++p) atomicAdd(Pbar_out.v[p] + x, w * tf[p]);
+    }
+}
+
+// Ubar_upd = Ubar_out + J(P_out)^-T Pbar_out over the interior (zero elsewhere).  With floors (fflag
+// set, Pinv the stage's inverted fluid primitives before the floors, [5][N]), a floored zone has
+// P_out = Floors(P_inv) and U_out = U(P_out), so there
+//   Ubar_upd = J(P_inv)^-T DFloors(P_inv)^T (Pbar_out + J(P_out)^T Ubar_out)
+// (the floor Jacobian by one dual evaluation per input); zones the floors left alone keep the first
+// form.
+template <int NV>
+__global__ void __launch_bounds__(128) k_adj_cell(Dims d, DevGeom g, Phys ph, khb_fields Pout, khb_fields Pbar_out,
+                                                  khb_fields Ubar_out, double* Ubar_upd, const double* Pinv,
+                                                  const int32_t* fflag, const int32_t* pflag, Box bx)
+{
+    int i, j, k;
+    if (!box_cell(bx, blockIdx.x, i, j, k)) return;
+    const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
+    if (pflag && pflag[c] > 0) return;    // a failed zone: k_adj_fixup
     double P[NV], J[NV][NV], y[NV], ubo[NV];
     bool any = false;
 #pragma unroll
@@ -233,6 +430,44 @@ __global__ void __launch_bounds__(128) k_adj_cell(Dims d, DevGeom g, Phys ph, kh
     load_zone_geom(g, j, i, G);
 #pragma unroll
     for (int p = 0; p < NV; ++p) P[p] = Pout.v[p][c];
+    if (fflag && fflag[c]) {
+        // Pbar_out + J(P_out)^T Ubar_out
+        ptou_jacobian<NV>(G, ph.gam, P, J);
+        double t[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = y[q];
+#pragma unroll
+            for (int p = 0; p < NV; ++p) s += J[p][q] * ubo[p];
+            t[q] = s;
+        }
+        // the inverted state; B is not changed by the floors
+        double Pi[NV];
+#pragma unroll
+        for (int p = 0; p < 5; ++p) Pi[p] = Pinv[p*d.N + c];
+#pragma unroll
+        for (int p = 5; p < NV; ++p) Pi[p] = P[p];
+        const long long cg = (long long)j*g.n1 + i;
+        const Prescription& fl = floors_at(ph, g, j, i);
+        const double rfg = __ldg(g.floor_rho + cg), ufg = __ldg(g.floor_u + cg);
+        // s = DFloors^T t: column q of DFloors from the tangent seeded on input q
+        double s[NV];
+        for (int q = 0; q < NV; ++q) {
+            Dual<double> X[NV];
+#pragma unroll
+            for (int p = 0; p < NV; ++p) X[p] = Dual<double>(Pi[p], (p == q) ? 1. : 0.);
+            floors_dual<NV>(G, fl, rfg, ufg, ph.gam, ph.frame, X);
+            double acc = 0.;
+#pragma unroll
+            for (int p = 0; p < NV; ++p) acc += X[p].d * t[p];
+            s[q] = acc;
+        }
+        ptou_jacobian<NV>(G, ph.gam, Pi, J);
+        solve_transposed<NV>(J, s);
+#pragma unroll
+        for (int p = 0; p < NV; ++p) Ubar_upd[p*d.N + c] = s[p];
+        return;
+    }
     ptou_jacobian<NV>(G, ph.gam, P, J);
     solve_transposed<NV>(J, y);
 #pragma unroll
@@ -470,7 +705,11 @@ int adj_supported(const khb_ctx* ctx, const char* who)
 {
     const Dims& d = ctx->d;
     const std::string w(who);
-    if (ctx->ph.floors_on || ctx->ph.recon_floors) return set_error(KHB_ERR_UNSUPPORTED, w + ": floors are not differentiated");
+    if (ctx->ph.recon_floors) return set_error(KHB_ERR_UNSUPPORTED, w + ": reconstruction floors are not differentiated");
+    if (ctx->ph.floors_on && ctx->ph.frame != KHB_FRAME_FLUID && ctx->ph.frame != KHB_FRAME_DRIFT)
+        return set_error(KHB_ERR_UNSUPPORTED, w + ": floors are differentiated in the fluid and drift frames only");
+    if (ctx->ph.floors_on && ctx->ph.inverter != KHB_INVERTER_ONEDW)
+        return set_error(KHB_ERR_UNSUPPORTED, w + ": floors are differentiated with the 1D_W inverter only");
     if (ctx->ph.fofc) return set_error(KHB_ERR_UNSUPPORTED, w + ": first-order flux correction is not differentiated");
     if (ctx->ph.ct_scheme) return set_error(KHB_ERR_UNSUPPORTED, w + ": B_CT is not differentiated");
     if (ctx->ph.riemann != 0) return set_error(KHB_ERR_UNSUPPORTED, w + ": LLF fluxes only");
@@ -599,7 +838,7 @@ template <int NV>
 int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Pout,
                      const khb_fields& Pbar_out, const khb_fields& Ubar_out, bool clear_out, const double* weight,
                      double wscale, const khb_fields& Pbar_s, const khb_fields& Ubar_s, const khb_fields& Ubar_0,
-                     cudaStream_t st)
+                     const double* pinv, const int32_t* fflag, const int32_t* pflag, cudaStream_t st)
 {
     const Dims& d = ctx->d;
     const size_t N = (size_t)d.N;
@@ -607,7 +846,12 @@ int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, c
     double* Uupd = ctx->adj_buf + 3 * NV * N;
     KHB_ACUDA(cudaMemsetAsync(ctx->adj_buf, 0, sizeof(double) * 4 * NV * N, st));
     const Box zb = make_box(d.is, d.js, d.ks, d.ie - d.is + 1, d.je - d.js + 1, d.ke - d.ks + 1);
-    k_adj_cell<NV><<<box_blocks(zb), 128, 0, st>>>(d, ctx->g, ctx->ph, Pout, Pbar_out, Ubar_out, Uupd, zb);
+    if (pflag) {
+        k_adj_fixup<NV><<<box_blocks(zb), 128, 0, st>>>(d, ctx->g, ctx->ph, Pout, Pbar_out, Ubar_out, pflag, Uupd, zb);
+        ctx->launches += 1;
+    }
+    k_adj_cell<NV><<<box_blocks(zb), 128, 0, st>>>(d, ctx->g, ctx->ph, Pout, Pbar_out, Ubar_out, Uupd, pinv, fflag,
+                                                   pflag, zb);
     if (clear_out)
         for (int p = 0; p < NV; ++p) {
             KHB_ACUDA(cudaMemsetAsync(Pbar_out.v[p], 0, sizeof(double) * N, st));
@@ -642,10 +886,13 @@ int adjoint_stage_nv(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, c
     return KHB_OK;
 }
 
+// pinv/fflag/pflag: per stage, the inverted fluid primitives before the floors, the floor flags and
+// the inversion flags of the recomputed stages (NULL where the stage was not recomputed)
 template <int NV>
 int adjoint_step_nv(khb_ctx* ctx, double dt, const khb_fields& Pn, const khb_fields& Pstar,
                     const khb_fields& Pnp1, const khb_fields& Pbar, const khb_fields& Ubar, const double* weight,
-                    double wscale, cudaStream_t st)
+                    double wscale, const double* const pinv[2], const int32_t* const fflag[2],
+                    const int32_t* const pflag[2], cudaStream_t st)
 {
     const size_t N = (size_t)ctx->d.N;
     const khb_fields Pbar_star = slice_fields(ctx->adj_buf + 4 * NV * N, ctx->d.N, NV);
@@ -655,11 +902,11 @@ int adjoint_step_nv(khb_ctx* ctx, double dt, const khb_fields& Pn, const khb_fie
     int rc;
     // stage 2: (P*, U*, U^n) -> (P^{n+1}, U^{n+1}); the caller's arrays turn into the adjoint of U^n
     if ((rc = adjoint_stage_nv<NV>(ctx, 2, dt, Pstar, Pnp1, Pbar, Ubar, true, weight, wscale, Pbar_star, Ubar_star,
-                                   Ubar, st)))
+                                   Ubar, pinv[1], fflag[1], pflag[1], st)))
         return rc;
     // stage 1: (P^n, U^n, U^n) -> (P*, U*)
     return adjoint_stage_nv<NV>(ctx, 1, dt, Pn, Pstar, Pbar_star, Ubar_star, false, weight, wscale, Pbar, Ubar, Ubar,
-                                st);
+                                pinv[0], fflag[0], pflag[0], st);
 }
 
 } // namespace
@@ -687,12 +934,48 @@ int khb_adjoint_step(khb_ctx* ctx, double dt, const khb_fields* P_n, const khb_f
         KHB_ACUDA(cudaMemset(ctx->adj_flags, 0, sizeof(int32_t) * 2 * (size_t)d.N));
         KHB_ACUDA(cudaDeviceSynchronize());
     }
-    // recompute the intermediate stage (P*, U*) into the context's stage scratch
+    const bool floors = ctx->ph.floors_on;
+    if (!ctx->adj_s2) {
+        KHB_ACUDA(cudaMalloc((void**)&ctx->adj_s2, sizeof(double) * 2 * ctx->nv * (size_t)d.N));
+        KHB_ACUDA(cudaMalloc((void**)&ctx->adj_flags2, sizeof(int32_t) * 2 * (size_t)d.N));
+        KHB_ACUDA(cudaMemset(ctx->adj_s2, 0, sizeof(double) * 2 * ctx->nv * (size_t)d.N));
+        KHB_ACUDA(cudaMemset(ctx->adj_flags2, 0, sizeof(int32_t) * 2 * (size_t)d.N));
+        KHB_ACUDA(cudaDeviceSynchronize());
+    }
+    if (floors && !ctx->adj_pf) {
+        KHB_ACUDA(cudaMalloc((void**)&ctx->adj_pf, sizeof(double) * 10 * (size_t)d.N));
+        KHB_ACUDA(cudaMemset(ctx->adj_pf, 0, sizeof(double) * 10 * (size_t)d.N));
+        KHB_ACUDA(cudaDeviceSynchronize());
+    }
+    // recompute both stages: the intermediate state (P*, U*) into the context's stage scratch, and
+    // each stage's inversion flags (failed zones take the fixup's adjoint) and, with floors, its
+    // inverted primitives before the floors and its floor flags
+    struct PrefloorScope {
+        khb_ctx* c;
+        ~PrefloorScope() { c->prefloor_dst = nullptr; }
+    } scope{ctx};
     const khb_fields Pstar = slice_fields(ctx->stageP, d.N, ctx->nv), Ustar = slice_fields(ctx->stageU, d.N, ctx->nv);
+    ctx->prefloor_dst = floors ? ctx->adj_pf : nullptr;
     if ((rc = khb_stage(ctx, 1, dt, P_n, U_n, U_n, &Pstar, &Ustar, ctx->adj_flags, ctx->adj_flags + d.N, stream)))
         return rc;
-    if (ctx->nv == 8) return adjoint_step_nv<8>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, st);
-    return adjoint_step_nv<5>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, st);
+    const khb_fields P2 = slice_fields(ctx->adj_s2, d.N, ctx->nv);
+    const khb_fields U2 = slice_fields(ctx->adj_s2 + (size_t)ctx->nv * d.N, d.N, ctx->nv);
+    ctx->prefloor_dst = floors ? ctx->adj_pf + 5 * (size_t)d.N : nullptr;
+    if ((rc = khb_stage(ctx, 2, dt, &Pstar, &Ustar, U_n, &P2, &U2, ctx->adj_flags2, ctx->adj_flags2 + d.N, stream)))
+        return rc;
+    ctx->prefloor_dst = nullptr;
+    const double* pinv[2] = {nullptr, nullptr};
+    const int32_t* ffl[2] = {nullptr, nullptr};
+    const int32_t* pfl[2] = {ctx->adj_flags, ctx->adj_flags2};
+    if (floors) {
+        pinv[0] = ctx->adj_pf; pinv[1] = ctx->adj_pf + 5 * (size_t)d.N;
+        ffl[0] = ctx->adj_flags + d.N; ffl[1] = ctx->adj_flags2 + d.N;
+    }
+    if (ctx->nv == 8)
+        return adjoint_step_nv<8>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, pinv, ffl,
+                                  pfl, st);
+    return adjoint_step_nv<5>(ctx, dt, *P_n, Pstar, *P_np1, *Pbar, *Ubar, rho_flux1_weight, weight_scale, pinv, ffl,
+                              pfl, st);
 }
 
 int khb_flux_dot(khb_ctx* ctx, int dir, int var, const double* weight, double scale, double* out, void* stream)

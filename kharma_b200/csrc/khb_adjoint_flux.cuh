@@ -9,11 +9,35 @@
 
 namespace khb {
 
+// The MC-limited slope mc_lim(dm, dp) dp (reconstruction.hpp:52-56, 107-123)
+template <typename R>
+__device__ __forceinline__ R mc_slope(R dm, R dp) { return mc_lim<R>(dm, dp) * dp; }
+// On dual numbers: the value as the forward forms it, the tangent from the homogeneous form of the
+// branch the value takes (0, 2 dm, (1 + r)/2 dp = (dm + dp)/2, or 2 dp), so that the tangent of
+// r = dm/dp, which overflows where dp is tiny (a field at the bottom of the double range), is never
+// formed.  Ties follow kmin/kmax as the forward's mc_lim resolves them.
+template <typename T>
+__device__ __forceinline__ Dual<T> mc_slope(Dual<T> dm, Dual<T> dp)
+{
+    const T v = mc_lim<T>(dm.v, dp.v) * dp.v;
+    if (!(fabs(dp.v) > T(0))) return Dual<T>(v, T(1.5) * dp.d);      // r = 2: phi = 3/2
+    const T r = dm.v / dp.v;
+    const T t2r = T(2) * r, thalf = T(0.5) * (T(1) + r);
+    const bool inner_half = thalf < t2r;                    // kmin(2r, (1+r)/2)
+    const T inner = inner_half ? thalf : t2r;
+    const bool mid_two = !(inner < T(2));                   // kmin(2, inner)
+    const T mid = mid_two ? T(2) : inner;
+    if (!(T(0) < mid)) return Dual<T>(v, T(0));             // kmax(0, mid) = 0
+    if (mid_two) return Dual<T>(v, T(2) * dp.d);
+    if (inner_half) return Dual<T>(v, T(0.5) * (dm.d + dp.d));
+    return Dual<T>(v, T(2) * dm.d);
+}
+
 // MC face values of a zone from its left, centre and right values (reconstruction.hpp:107-123)
 template <typename R>
-__device__ __forceinline__ R mc_right(R xm, R x0, R xp) { return x0 + R(0.5) * (mc_lim<R>(x0 - xm, xp - x0) * (xp - x0)); }
+__device__ __forceinline__ R mc_right(R xm, R x0, R xp) { return x0 + R(0.5) * mc_slope(x0 - xm, xp - x0); }
 template <typename R>
-__device__ __forceinline__ R mc_left(R xm, R x0, R xp) { return x0 - R(0.5) * (mc_lim<R>(x0 - xm, xp - x0) * (xp - x0)); }
+__device__ __forceinline__ R mc_left(R xm, R x0, R xp) { return x0 - R(0.5) * mc_slope(x0 - xm, xp - x0); }
 
 // One side of a face in arithmetic R: conserved state, flux and signal speeds (get_flux.hpp:219-331)
 template <typename R, int NV, int DIR>

@@ -291,7 +291,10 @@ int zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const kh
     zc.g0 = kRkGam0[s]; zc.g1 = kRkGam1[s]; zc.bdt = kRkBeta[s] * dt;
     zc.dt_dev = ctx->dt_active; zc.beta = kRkBeta[s];
     const int dtm = (stage == 2) ? M_DT : 0;
-    if (!ctx->zone_split) {
+    // the adjoint's recompute keeps the primitives between the inversion and the floors (the split
+    // passes are bitwise the fused one)
+    const bool snap = ctx->prefloor_dst && ctx->ph.floors_on;
+    if (!ctx->zone_split && !snap) {
         zc.mode = M_ZONE_FUSED | dtm;
         return launch_zone(ctx, zc, st);
     }
@@ -299,12 +302,16 @@ int zone_pass(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const kh
     zc.mode = M_UPDATE;
     if ((rc = launch_zone(ctx, zc, st))) return rc;
     zc.Us = Uout;          // the updated conserved state is the inversion's input
-    if (ctx->zone_split == 1) {
+    if (ctx->zone_split == 1 && !snap) {
         zc.mode = M_ZONE_CELL | dtm;
         return launch_zone(ctx, zc, st);
     }
     zc.mode = M_UTOP;
     if ((rc = launch_zone(ctx, zc, st))) return rc;
+    if (snap)
+        for (int p = 0; p < 5; ++p)
+            KHB_CUDA(cudaMemcpyAsync(ctx->prefloor_dst + (size_t)p * ctx->d.N, Pout.v[p], sizeof(double) * (size_t)ctx->d.N,
+                                     cudaMemcpyDeviceToDevice, st));
     zc.Ps = Pout;          // floors start from the inverted primitives and their flags
     zc.mode = M_ZONE_FLOORS | dtm;
     return launch_zone(ctx, zc, st);
@@ -548,6 +555,7 @@ int khb_destroy(khb_ctx* c)
     cudaFree(c->fofc_flag);
     cudaFree(c->dt_state);
     cudaFree(c->adj_buf); cudaFree(c->adj_flags); cudaFree(c->adj_red);
+    cudaFree(c->adj_pf); cudaFree(c->adj_s2); cudaFree(c->adj_flags2);
     cudaFree(c->ct_emfc); cudaFree(c->ct_stageBf);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->graph) cudaGraphDestroy(c->graph);

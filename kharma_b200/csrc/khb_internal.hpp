@@ -65,6 +65,14 @@ struct khb_ctx {
     double* adj_buf;
     int32_t* adj_flags;
     double* adj_red;       // partial sums of khb_flux_dot
+    // adjoint through the floors: the fluid primitives each recomputed stage inverted, before the
+    // floors changed them ([2 stages][5][N]), the recomputed second stage ([2][nv][N]: P, U) and its
+    // flags ([2][N]: pflag, fflag); prefloor_dst, set only while the adjoint recomputes a stage, makes
+    // the zone pass run split and copy its inverted primitives there before the floors
+    double* adj_pf;
+    double* adj_s2;
+    int32_t* adj_flags2;
+    double* prefloor_dst;
     // B_CT: zone-centred EMFs [3][N] of FT, the intermediate stage's face field [3][N], and the face
     // field a zone pass in progress reads (set only inside khb_ct_stage)
     void* ct_emfc;

@@ -7,6 +7,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+# Under pytest-xdist every worker would start an OpenMP team of all cores in the oracle library, and
+# their spinning threads oversubscribe the host by the worker count: one thread per worker instead
+# (read when the library is first loaded).
+if os.environ.get("PYTEST_XDIST_WORKER"):
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a) and the built libkhb.so")

@@ -8,9 +8,9 @@ Checks:
     in FMKS coordinates, the periodic MHD linear-mode box with a functional of the final state);
   * the FP32-flux form's adjoint against the FP64 adjoint;
   * checkpoint spacing does not change the gradient (recompute reproduces the forward states).
-Floors, fixups, FOFC, and physical boundaries of MHD blocks are outside the differentiated scope
-(outflow and reflecting faces of hydro blocks are in it); the cases below keep every inversion
-successful (the harness raises otherwise).
+Floors in the fluid and drift frames, and outflow and reflecting X1/X2 faces, are differentiated;
+fixups, FOFC, normal-frame floors and transmitting faces are outside the differentiated scope; the
+cases below keep every inversion successful (the harness raises otherwise).
 
 The MC limiter and the LLF speed maxima are piecewise smooth: the adjoint is the derivative of the
 branch each face takes.  Central differences agree with it where a perturbation crosses no branch
@@ -171,6 +171,126 @@ def test_adjoint_torus_block_mhd_vs_fd():
     check_fd(b, P0, dts, w, None, ndir=8, seed=2, tol=1e-4)
 
 
+@pytest.mark.parametrize("frame", ["drift", "fluid"])
+def test_adjoint_torus_block_floors_vs_fd(frame):
+    """The magnetized torus block with the floors on and the geometric density floor raised so that
+    they bind on about half of the zones at every stage (drift frame: density, internal energy and
+    velocity change; fluid frame: density and internal energy): the floors' adjoint (one dual
+    evaluation of the floor map per input at the inverted, pre-floor primitives the recompute keeps)
+    against central differences."""
+    b, P0, dts, w = torus_block_case()
+    spec = dataclasses.replace(b.spec, floors_on=True, floor_frame=frame,
+                               floors=dataclasses.replace(b.spec.floors, rho_min_geom=50.0))
+    bf = Block(spec, geometry=b.geom)
+    bf.set_prims(P0)
+    bf.step(dts[0])
+    floored = float((bf.fflag[spec.interior] != 0).float().mean())
+    assert 0.2 < floored < 0.8, floored
+    check_fd(bf, P0, dts, w, None, ndir=8, seed=5, tol=1e-4)
+
+
+def test_adjoint_through_fixups_vs_fd():
+    """Inversion failures and FixUtoP: three zones of the torus block's initial conserved state are
+    poisoned (two hot, 1D_W max_iter; one with negative D, neg_input) after U = U(P0), so that their
+    inversions fail and the fixup replaces them by the weighted average of their neighbours; the
+    adjoint through the fixup (to the neighbours' primitives and the zone's own B) against central
+    differences in directions that leave the poisoned zones' P0 alone (their U0 is not U(P0))."""
+    import poison_cases
+    b, P0, dts, w = torus_block_case()
+    spec = b.spec
+    ng = spec.ng
+    zs = [(ng + 3, ng + 4, ng + 5), (ng + 4, ng + 7, ng + 6), (ng + 5, ng + 5, ng + 8)]
+    kinds = ["hot", "hot", "neg_D"]
+
+    def prepare(P):
+        b.set_prims(P)
+        U = b.U.cpu().numpy()
+        for z, kind in zip(zs, kinds):
+            U[(slice(0, 8),) + z] = poison_cases.POISONS[kind](U[(slice(0, 8),) + z])
+        b.U.copy_(torch.as_tensor(U, device="cuda"))
+
+    def objective_p(P):
+        prepare(P)
+        return Run(b, dts, weight=w, checkpoint_every=5).forward()
+
+    prepare(P0)
+    P0_full = b.P.clone()
+    run = Run(b, dts, weight=w, checkpoint_every=5)
+    J = run.forward()
+    assert run.failures >= len(zs), run.failures
+    g = run.gradient_prims(P0_full)
+    rng = np.random.Generator(np.random.PCG64(7))
+    sl = (slice(None),) + spec.interior
+    scale = P0[sl].pow(2).mean(dim=(1, 2, 3)).sqrt().cpu().numpy() + 1e-6
+    rels = []
+    for _ in range(8):
+        v = np.zeros(tuple(P0.shape))
+        v[sl] = rng.standard_normal(v[sl].shape) * scale[:, None, None, None]
+        for z in zs:
+            v[(slice(None),) + z] = 0.
+        v = torch.as_tensor(v, device="cuda")
+        ad = float((g * v).sum())
+        best = math.inf
+        for e in (1e-6, 1e-7, 1e-8):
+            fd = (objective_p(P0 + e * v) - objective_p(P0 - e * v)) / (2 * e)
+            best = min(best, abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+            if best < 1e-7:
+                break
+        rels.append(best)
+    rels = np.array(rels)
+    print(f"J = {J:.6e}, {run.failures} failed inversions; adjoint vs central FD: median {np.median(rels):.1e}, "
+          f"worst {rels.max():.1e}")
+    assert rels.max() < 1e-4
+    assert np.median(rels) < 1e-6
+
+
+@pytest.mark.parametrize("nsteps,tol,tol_median", [(1, 1e-4, 1e-5), (6, 2e-3, 5e-4)])
+def test_adjoint_fm_torus_floored_vs_fd(nsteps, tol, tol_median):
+    """The adjoint workload's physics on a small FM torus block (FMKS a = 0.9375, SANE field, u jittered
+    +-4%, linear MC, LLF, flux-CT, 1D_W, drift-frame floors and ceilings, outflow X1 faces with inflow
+    checks, reflecting X2 faces with both polar flux fixes and the corner fix, periodic X3; a few
+    hundred inversions fail and are fixed up): gradient of the mass through r = 5 with respect to the
+    initial internal-energy perturbation, against central differences in directions of that
+    perturbation field (u (1 + eps xi) where the jitter acts, rho above the floor).  Outside the torus
+    the initial state is exactly axisymmetric, so its x3 MC slopes sit at the limiter's non-smooth
+    point (both differences zero) and a perturbation there has no derivative; the perturbation
+    field's support avoids that.  Over several steps central differences themselves stop
+    converging below about 1e-4 (the inverter's 1e-8 tolerance, zones hovering at the floors): the
+    bar widens with the steps."""
+    spec = torus_spec(32, 24, 8)
+    geom = build_geometry(spec)
+    P0 = torch.as_tensor(problems.fm_torus(spec, geom, seed=11), device="cuda")
+    b = Block(spec, geometry=geom)
+    dts = [stable_dt(Block(spec, geometry=geom), P0)] * nsteps
+    w = mdot_weight(spec)
+    J, g = gradient(b, P0, dts, w)
+    run = Run(b, dts, weight=w)
+    b.set_prims(P0)
+    run.forward()
+    b.set_prims(P0)
+    b.step(dts[0])
+    assert int((b.fflag[spec.interior] != 0).sum()) > 0
+    jittered = P0[0] > spec.floors.rho_min_geom
+    rng = np.random.Generator(np.random.PCG64(9))
+    rels = []
+    for _ in range(8):
+        v = torch.zeros_like(P0)
+        xi = torch.as_tensor(rng.standard_normal(tuple(P0[1][spec.interior].shape)), device="cuda")
+        v[1][spec.interior] = xi * P0[1][spec.interior]
+        v[1] = torch.where(jittered, v[1], torch.zeros_like(v[1]))
+        ad = float((g * v).sum())
+        best = math.inf
+        for e in (1e-5, 1e-6, 1e-7):
+            fd = (objective(b, P0 + e * v, dts, w) - objective(b, P0 - e * v, dts, w)) / (2 * e)
+            best = min(best, abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+        rels.append(best)
+    rels = np.array(rels)
+    print(f"J = {J:.6e}, {run.failures} failed inversions; adjoint vs central FD (u perturbation field, {nsteps} "
+          f"steps): median {np.median(rels):.1e}, worst {rels.max():.1e}")
+    assert rels.max() < tol
+    assert np.median(rels) < tol_median
+
+
 @pytest.mark.parametrize("recon", ["donor_cell", "linear_mc"])
 def test_adjoint_mhdmodes_periodic_final_state_vs_fd(recon):
     """Periodic MHD box (flux-CT, folded periodic ghost adjoints) with a smooth mode along every
@@ -290,4 +410,13 @@ def test_adjoint_rejects_unsupported():
     run = Run(b, [0.01], weight=None, Pw=torch.ones_like(b.P))
     run.forward()
     with pytest.raises(_lib.KhbError, match="reconstruction"):
+        run.adjoint()
+    # floors in the normal-observer frame (their re-inversion is not differentiated)
+    tb, P0, dts, w = torus_block_case()
+    spec = dataclasses.replace(tb.spec, floors_on=True, floor_frame="normal")
+    nb = Block(spec, geometry=tb.geom)
+    nb.set_prims(P0)
+    run = Run(nb, dts[:1], weight=w)
+    run.forward()
+    with pytest.raises(_lib.KhbError, match="drift frames"):
         run.adjoint()
