@@ -376,6 +376,49 @@ int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, cons
  * b_ct_boundaries.cpp:64-186). */
 int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf, void* stream);
 
+/* khb_ct_stage in two halves, for a mesh whose blocks exchange corrections between them
+ * (kharma_step.cpp:163-214: the flux and EMF corrections of a multilevel mesh run between
+ * CalculateEMF and the update): khb_ct_stage_fluxes forms the face fluxes, their fixes and the edge
+ * EMFs in context scratch; khb_ct_stage_update the face update, the zone pass, fixups and ghost
+ * zones from them.  Same arguments and checks as khb_ct_stage. */
+int khb_ct_stage_fluxes(khb_ctx* ctx, const khb_fields* P_s, void* stream);
+int khb_ct_stage_update(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+                        const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
+                        const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag,
+                        void* stream);
+
+/* B_CT::BlockUtoP over every ghost zone (b_ct.cpp:160-188 on the boundary domain): B^i as the average
+ * of the zone's two faces (the last ghost layer of a direction, whose upper face the arrays do not
+ * hold, from its lower face) and U = U(P); for blocks whose face field's ghost layers the caller
+ * filled (an SMR mesh's exchange). */
+int khb_ct_ghost_from_faces(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
+                            void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * SMR meshes of B_CT blocks (KHARMA's default field transport on multilevel meshes,
+ * kharma.cpp:376-395): tables from kharma_b200/ctmesh.py.  Blocks: FP64, Cartesian Minkowski,
+ * one shape, 2D or 3D, every face an exchange face.  Per stage: khb_ct_stage_fluxes on every
+ * block, khb_ctmesh_correct (the fluid fluxes of coarse faces on a fine-coarse boundary become the
+ * mean of the fine fluxes, and coarse edge EMFs that coincide with fine edges the mean of the fine
+ * EMFs along them: Parthenon's flux correction, kharma_step.cpp:183-194), khb_ct_stage_update on
+ * every block, then khb_ctmesh_exchange on the stage output (ghost-zone fluid primitives by copy,
+ * restriction or minmod prolongation; ghost faces by copy, area-average restriction (RestrictAverage),
+ * minmod prolongation onto faces shared with coarse faces (ProlongateSharedMinMod) and Olivares'
+ * divergence-preserving prolongation inside coarse zones (ProlongateInternalOlivares,
+ * b_ct_functions.hpp:151-200)) and khb_ct_ghost_from_faces on every block.  Tables: ghost zones
+ * (int32 x 6, the hydro mesh's format) with the end of each phase (copies and restrictions, then
+ * one phase per destination level); ghost faces (int32 x 8) with phase ends; fluxes and EMFs
+ * (int32 x 6).  P and Bf of khb_ctmesh_exchange are arrays of nblocks fields.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct khb_ctmesh khb_ctmesh;
+int khb_ctmesh_create(khb_ctx* const* ctxs, int nblocks, const int32_t* cell, int64_t n_cell,
+                      const int64_t* cell_ends, int n_cell_phases, const int32_t* face, int64_t n_face,
+                      const int64_t* face_ends, int n_face_phases, const int32_t* flux, int64_t n_flux,
+                      const int32_t* emf, int64_t n_emf, khb_ctmesh** out);
+int khb_ctmesh_destroy(khb_ctmesh* mesh);
+int khb_ctmesh_correct(khb_ctmesh* mesh, void* stream);
+int khb_ctmesh_exchange(khb_ctmesh* mesh, const khb_fields* P, const khb_fields* Bf, void* stream);
+
 /* Full RK2 step with B_CT in place on (P, U, Bf), the intermediate stage in context scratch. */
 int khb_ct_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
                 int32_t* pflag, int32_t* fflag, void* stream);

@@ -14,6 +14,7 @@ Translation units and their arithmetic flags:
   khb_adjoint.cu   discrete adjoint of the step (FP64 faces)      -fmad=false
   khb_adjoint_fp32.cu  adjoint of the FP32-flux form's faces      as khb_fp32.cu
   khb_ct.cu        B_CT (face-centred field, EMFs, face update)   -fmad=false
+  khb_ctmesh.cu    SMR meshes of B_CT blocks (corrections, exchange)  -fmad=false
   khb_geometry.cpp host construction of the geometry tables
 The library is a plain shared object; the Python layer binds it with ctypes.
 """
@@ -35,6 +36,7 @@ UNITS = {
     "khb_adjoint.cu": ["-fmad=false"],
     "khb_adjoint_fp32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "khb_ct.cu": ["-fmad=false"],
+    "khb_ctmesh.cu": ["-fmad=false"],
     "khb_geometry.cpp": [],
 }
 HEADERS = ["khb_device.cuh", "khb_kernels.cuh", "khb_types.cuh", "khb_internal.hpp", "khb_dual.cuh", "khb_adjoint_flux.cuh", os.path.join("..", "..", "include", "khb.h")]

@@ -334,15 +334,22 @@ int do_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb
 
 // One stage of a B_CT block: fluxes and their fixes, edge EMFs and the face update, then the zone pass
 // with the zone B from the new faces (M_BCT), fixups and ghost zones
-int do_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
-                const khb_fields& U0, const khb_fields& Bs, const khb_fields& B0, const khb_fields& Pout,
-                const khb_fields& Uout, const khb_fields& Bout, int32_t* pflag, int32_t* fflag, cudaStream_t st)
+// The first half of a B_CT stage: face fluxes, their fixes and the edge EMFs, in context scratch
+int ct_stage_fluxes(khb_ctx* ctx, const khb_fields& Ps, cudaStream_t st)
 {
     int rc;
     for (int dir = 1; dir <= ctx->d.ndim; ++dir)
         if ((rc = launch_flux(ctx, dir, Ps, st))) return rc;
     if ((rc = launch_fix_flux(ctx, ctx->ph, st))) return rc;
-    if ((rc = khb::ct_emf(ctx, Ps, st))) return rc;
+    return khb::ct_emf(ctx, Ps, st);
+}
+
+// The second half: the face update from the EMFs, the zone pass, fixups and ghost zones
+int ct_stage_update(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+                    const khb_fields& U0, const khb_fields& Bs, const khb_fields& B0, const khb_fields& Pout,
+                    const khb_fields& Uout, const khb_fields& Bout, int32_t* pflag, int32_t* fflag, cudaStream_t st)
+{
+    int rc;
     if ((rc = khb::ct_face_update(ctx, stage, dt, Bs, B0, Bout, st))) return rc;
     if ((rc = launch_ghost_copy(ctx, Ps, Us, Pout, Uout, st))) return rc;
     for (int x = 0; x < 3; ++x) ctx->ct_bf[x] = Bout.v[x];
@@ -352,6 +359,15 @@ int do_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const 
     if (rc) return rc;
     if ((rc = launch_fixup(ctx, Pout, Uout, pflag, st))) return rc;
     return launch_boundaries(ctx, Pout, Uout, st, &Bout);
+}
+
+int do_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+                const khb_fields& U0, const khb_fields& Bs, const khb_fields& B0, const khb_fields& Pout,
+                const khb_fields& Uout, const khb_fields& Bout, int32_t* pflag, int32_t* fflag, cudaStream_t st)
+{
+    int rc;
+    if ((rc = ct_stage_fluxes(ctx, Ps, st))) return rc;
+    return ct_stage_update(ctx, stage, dt, Ps, Us, U0, Bs, B0, Pout, Uout, Bout, pflag, fflag, st);
 }
 
 } // namespace
@@ -850,22 +866,79 @@ int khb_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U,
     return do_stage(ctx, 2, dt, P1, U1, *U, *P, *U, pflag, fflag, S(stream));
 }
 
+static int check_ct_stage_args(khb_ctx* ctx, const char* who, int stage, const khb_fields* P_s,
+                               const khb_fields* U_s, const khb_fields* U_0, const khb_fields* Bf_s,
+                               const khb_fields* Bf_0, const khb_fields* P_out, const khb_fields* U_out,
+                               const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag)
+{
+    const std::string w(who);
+    if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, w + ": block is not B_CT (cfg.ct_scheme)");
+    if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, w + ": stage must be 1 or 2");
+    int rc;
+    if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
+        (rc = check_fields(ctx, U_0, "U_0")) || (rc = check_fields(ctx, P_out, "P_out")) ||
+        (rc = check_fields(ctx, U_out, "U_out"))) return rc;
+    for (const khb_fields* f : {Bf_s, Bf_0, Bf_out})
+        if (!f || !f->v[0] || !f->v[1] || !f->v[2]) return fail(KHB_ERR_ARG, w + ": NULL face field");
+    if (!pflag || !fflag) return fail(KHB_ERR_ARG, w + ": NULL flags");
+    return KHB_OK;
+}
+
 int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
                  const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
                  const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream)
 {
     KHB_RANGE("khb_ct_stage");
     KHB_NEED_GEOM(ctx);
-    if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_stage: block is not B_CT (cfg.ct_scheme)");
-    if (stage != 1 && stage != 2) return fail(KHB_ERR_ARG, "khb_ct_stage: stage must be 1 or 2");
     int rc;
-    if ((rc = check_fields(ctx, P_s, "P_s")) || (rc = check_fields(ctx, U_s, "U_s")) ||
-        (rc = check_fields(ctx, U_0, "U_0")) || (rc = check_fields(ctx, P_out, "P_out")) ||
-        (rc = check_fields(ctx, U_out, "U_out"))) return rc;
-    for (const khb_fields* f : {Bf_s, Bf_0, Bf_out})
-        if (!f || !f->v[0] || !f->v[1] || !f->v[2]) return fail(KHB_ERR_ARG, "khb_ct_stage: NULL face field");
-    if (!pflag || !fflag) return fail(KHB_ERR_ARG, "khb_ct_stage: NULL flags");
+    if ((rc = check_ct_stage_args(ctx, "khb_ct_stage", stage, P_s, U_s, U_0, Bf_s, Bf_0, P_out, U_out, Bf_out,
+                                  pflag, fflag))) return rc;
     return do_ct_stage(ctx, stage, dt, *P_s, *U_s, *U_0, *Bf_s, *Bf_0, *P_out, *U_out, *Bf_out, pflag, fflag, S(stream));
+}
+
+int khb_ct_stage_fluxes(khb_ctx* ctx, const khb_fields* P_s, void* stream)
+{
+    KHB_RANGE("khb_ct_stage_fluxes");
+    KHB_NEED_GEOM(ctx);
+    if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_stage_fluxes: block is not B_CT (cfg.ct_scheme)");
+    int rc;
+    if ((rc = check_fields(ctx, P_s, "P_s"))) return rc;
+    return ct_stage_fluxes(ctx, *P_s, S(stream));
+}
+
+int khb_ct_stage_update(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
+                        const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
+                        const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag,
+                        void* stream)
+{
+    KHB_RANGE("khb_ct_stage_update");
+    KHB_NEED_GEOM(ctx);
+    int rc;
+    if ((rc = check_ct_stage_args(ctx, "khb_ct_stage_update", stage, P_s, U_s, U_0, Bf_s, Bf_0, P_out, U_out,
+                                  Bf_out, pflag, fflag))) return rc;
+    return ct_stage_update(ctx, stage, dt, *P_s, *U_s, *U_0, *Bf_s, *Bf_0, *P_out, *U_out, *Bf_out, pflag, fflag,
+                           S(stream));
+}
+
+int khb_ct_ghost_from_faces(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
+                            void* stream)
+{
+    KHB_RANGE("khb_ct_ghost_from_faces");
+    KHB_NEED_GEOM(ctx);
+    if (!ctx->ph.ct_scheme) return fail(KHB_ERR_STATE, "khb_ct_ghost_from_faces: block is not B_CT (cfg.ct_scheme)");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P")) || (rc = check_fields(ctx, U, "U"))) return rc;
+    if (!Bf || !Bf->v[0] || !Bf->v[1] || !Bf->v[2]) return fail(KHB_ERR_ARG, "khb_ct_ghost_from_faces: NULL face field");
+    const Dims& d = ctx->d;
+    cudaStream_t st = S(stream);
+    // the X1/X2 ghost zones of the interior k range, then (3D) both X3 ghost planes
+    LaunchCommon::ghost_ptou(ctx->nv, d, ctx->g, ctx->ph, *P, *U, st, Bf, 7);
+    KHB_LAUNCHED(ctx);
+    if (d.ndim > 2) {
+        LaunchCommon::ghost_ptou(ctx->nv, d, ctx->g, ctx->ph, *P, *U, st, Bf, 7, 3);
+        KHB_LAUNCHED(ctx);
+    }
+    return KHB_OK;
 }
 
 int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf, void* stream)

@@ -1,0 +1,384 @@
+"""Static mesh refinement of magnetized blocks with a face-centred field (B_CT): the tables and the
+driver of an SMR mesh of Cartesian Minkowski MHD blocks stepped with B_CT.
+
+KHARMA defaults multilevel meshes to B_CT (kharma.cpp:376-395): the field lives on faces and its
+divergence stays at round-off only if every block sees the same field across a fine-coarse
+boundary.  Parthenon (unvendored) and KHARMA's B_CT package do that with three pieces, restated
+here as tables the library executes:
+
+  * EMF correction (kharma_step.cpp:183-194, Parthenon's flux correction of edge variables): an
+    edge of a coarse block that coincides with edges of finer blocks takes the average of the fine
+    edge EMFs along it (one fine edge where the edge direction is inactive), so that the coarse face
+    on the boundary changes by the average of the fine faces' changes;
+  * the hydro flux correction of the cell-centred variables (the coarse face takes the average of
+    the fine fluxes through it, SMRMesh.tables());
+  * the face field's ghost exchange: same-level faces copied; a coarse block's ghost face covered by
+    finer blocks is the area average of the 2^(ndim-1) fine faces on it (RestrictAverage; 4 in 2D
+    for the x3 field, which is zone-centred there); a fine block's ghost face on a coarse face is the
+    coarse value plus minmod-limited tangential slopes times +-1/4 (ProlongateSharedMinMod), and a
+    fine face inside a coarse zone follows the divergence-preserving operator of Olivares et al.
+    (ProlongateInternalOlivares, b_ct_functions.hpp:151-200) from the shared faces around it, its
+    sub-face element el lying (el % 2) zones up along the next direction and (el // 2) along the
+    third (the reference's offsets exchange the two, which in 3D leaves the fine zones with a
+    divergence; in 2D both give the same faces).
+The cell-centred fluid primitives are exchanged as in SMRMesh; the ghost zones then take B from
+their faces and U = U(P).
+
+Face table entries (int32 x 8): dst block, face direction d (0: x1, 1: x2, 2: x3), dst face (flat
+index in the [n3][n2][n1] face array, face i being the left face of zone i), op, src block, src face,
+aux, phase.  op 0 copy; 1 restriction (src: the fine face of lowest tangential indices); 2 shared
+prolongation (src: the coarse face; aux bit a: + side along axis a); 3 internal prolongation (src
+block = dst block, src: the lowest fine zone of the coarse zone, aux: Olivares' sub-face element).
+phase 0 holds copies and restrictions; a prolongation into a level-L block has phase 2L-1 (shared)
+or 2L (internal), so that each reads only faces earlier phases filled.  Internal faces whose
+operator would read past the face arrays (the arrays stop at face n-1 along each direction, where
+Parthenon stores face n) are left unfilled; they lie in the outermost ghost layer, which no
+reconstruction stencil reaches.
+
+EMF table entries (int32 x 6): coarse block, edge direction e, coarse edge (flat), fine block, fine
+edge (flat, the sub-edge of lowest index along e), 0.  Edges follow the library's layout: E1 at
+(i centre, j face, k face), E2 at (i face, j centre, k face), E3 at (i face, j face, k centre).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .mesh import SMRMesh
+
+FOP_COPY, FOP_RESTRICT, FOP_SHARED, FOP_INTERNAL = 0, 1, 2, 3
+
+
+class _Geo:
+    """Index helpers of an SMRMesh: level-L global coordinates, owners of zones and faces."""
+
+    def __init__(self, mesh: SMRMesh):
+        self.m = mesh
+        self.ng, self.nx, self.ndim = mesh.ng, mesh.nx, mesh.ndim
+        self.act = [a < mesh.ndim for a in range(3)]
+        self.own = [mesh._owners(L) for L in range(mesh.levels)]
+        self.shape = mesh.blocks[0].spec.shape        # (n3, n2, n1)
+
+    def tot(self, L):
+        return self.m._zones_at(L)
+
+    def zone_owner(self, L, g):
+        """Block owning level-L zones g (list of 3 arrays, x1..x3; periodic); -1 where none."""
+        if L < 0 or L >= self.m.levels:
+            return np.full(len(g[0]), -1, dtype=np.int64)
+        t = self.tot(L)
+        lo = [(g[a] % t[a]) // self.nx[a] if self.act[a] else np.zeros_like(g[a]) for a in range(3)]
+        return self.own[L][lo[2], lo[1], lo[0]]
+
+    def local(self, b, L, g):
+        """Local (x1, x2, x3) indices in block b of level-L global zones g that b owns."""
+        blk = self.m.blocks[b]
+        t = self.tot(L)
+        return [((g[a] - blk.loc[a] * self.nx[a]) % t[a]) + self.ng if self.act[a] else np.zeros_like(g[a])
+                for a in range(3)]
+
+    def flat(self, loc3):
+        n3, n2, n1 = self.shape
+        return (loc3[2] * n2 + loc3[1]) * n1 + loc3[0]
+
+    def face_owner(self, L, d, g):
+        """Owner and local indices of level-L faces of direction d at global coordinates g (g[d] the
+        face index: the face between zones g[d]-1 and g[d]).  The block holding zone g[d] takes it
+        (its lower face), else the block holding zone g[d]-1 (its upper face)."""
+        if not self.act[d]:
+            b = self.zone_owner(L, g)
+            return b, [np.where(b >= 0, x, 0) for x in self._locals(b, L, g)]
+        hi = list(g)
+        lo = list(g)
+        lo[d] = g[d] - 1
+        bh = self.zone_owner(L, hi)
+        bl = self.zone_owner(L, lo)
+        b = np.where(bh >= 0, bh, bl)
+        lh = self._locals(bh, L, hi)
+        ll = self._locals(bl, L, lo)
+        ll[d] = ll[d] + 1
+        loc = [np.where(bh >= 0, lh[a], ll[a]) for a in range(3)]
+        return b, loc
+
+    def _locals(self, bs, L, g):
+        out = [np.zeros_like(g[0]) for _ in range(3)]
+        for b in np.unique(bs[bs >= 0]):
+            m = bs == b
+            lb = self.local(int(b), L, [g[a][m] for a in range(3)])
+            for a in range(3):
+                out[a][m] = lb[a]
+        return out
+
+
+def face_tables(mesh: SMRMesh):
+    """(entries int32 [n, 8], phase boundaries: entries of phase p are [ends[p-1], ends[p]), number of
+    internal faces skipped at the array ends)."""
+    G = _Geo(mesh)
+    ng, nx, act = G.ng, G.nx, G.act
+    n3, n2, n1 = G.shape
+    dims = (n1, n2, n3)
+    rows = []
+    skipped = 0
+    for b, blk in enumerate(mesh.blocks):
+        L = blk.level
+        t = G.tot(L)
+        K, J, I = np.meshgrid(np.arange(n3), np.arange(n2), np.arange(n1), indexing="ij")
+        loc3 = [I.ravel(), J.ravel(), K.ravel()]
+        for d in range(3):
+            # owned faces: [ng, ng + nx] along an active d, the interior across
+            owned = np.ones(len(loc3[0]), dtype=bool)
+            for a in range(3):
+                if not act[a]:
+                    continue
+                hi = ng + nx[a] if a == d else ng + nx[a] - 1
+                owned &= (loc3[a] >= ng) & (loc3[a] <= hi)
+            sel = ~owned
+            lg = [loc3[a][sel] for a in range(3)]
+            dst = G.flat(lg)
+            g = [((blk.loc[a] * nx[a] + lg[a] - ng) % t[a]) if act[a] else np.zeros_like(lg[a]) for a in range(3)]
+            n = len(dst)
+            ent = np.full((n, 8), -1, dtype=np.int64)
+            ent[:, 0] = b
+            ent[:, 1] = d
+            ent[:, 2] = dst
+            done = np.zeros(n, dtype=bool)
+            # same level: copy
+            sb, sl = G.face_owner(L, d, g)
+            m = sb >= 0
+            ent[m, 3] = FOP_COPY
+            ent[m, 4] = sb[m]
+            ent[m, 5] = G.flat([sl[a][m] for a in range(3)])
+            ent[m, 6] = 0
+            ent[m, 7] = 0
+            done |= m
+            # finer: restriction from the fine face of lowest tangential indices
+            if L + 1 < mesh.levels:
+                gf = [2 * g[a] if act[a] else g[a] for a in range(3)]
+                fb, fl = G.face_owner(L + 1, d, gf)
+                m = (~done) & (fb >= 0)
+                ent[m, 3] = FOP_RESTRICT
+                ent[m, 4] = fb[m]
+                ent[m, 5] = G.flat([fl[a][m] for a in range(3)])
+                ent[m, 6] = 0
+                ent[m, 7] = 0
+                done |= m
+            rest = ~done
+            if rest.any():
+                assert L > 0, "ghost face with no source: the mesh is not 2:1 balanced"
+                shared = rest.copy()
+                if act[d]:
+                    shared &= (g[d] % 2) == 0
+                internal = rest & ~shared
+                # shared faces: the coarse face and its tangential neighbours
+                if shared.any():
+                    gc = [g[a][shared] // 2 if act[a] else g[a][shared] for a in range(3)]
+                    cb, cl = G.face_owner(L - 1, d, gc)
+                    assert (cb >= 0).all(), "mesh is not 2:1 balanced"
+                    aux = np.zeros(int(shared.sum()), dtype=np.int64)
+                    for a in range(3):
+                        if act[a] and a != d:
+                            aux |= (g[a][shared] % 2) << a
+                    ent[shared, 3] = FOP_SHARED
+                    ent[shared, 4] = cb
+                    ent[shared, 5] = G.flat(cl)
+                    ent[shared, 6] = aux
+                    ent[shared, 7] = 2 * L - 1
+                if internal.any():
+                    nxt, thd = (d + 1) % 3, (d + 2) % 3
+                    base = [lg[a][internal] - (g[a][internal] % 2) if act[a] else lg[a][internal] for a in range(3)]
+                    base[d] = lg[d][internal] - 1
+                    par = lambda a: (g[a][internal] % 2) if act[a] else np.ones(int(internal.sum()), dtype=np.int64)
+                    # element: (el % 2) along nxt, (el // 2) along thd; where a direction is inactive the
+                    # operator writes the face twice and the later element stays
+                    elem = 2 * par(thd) + par(nxt)
+                    # the operator reads faces up to base + 2 along every active direction
+                    fits = np.ones(int(internal.sum()), dtype=bool)
+                    for a in range(3):
+                        if act[a]:
+                            fits &= base[a] + 2 <= dims[a] - 1
+                    idx = np.nonzero(internal)[0]
+                    skipped += int((~fits).sum())
+                    ok = idx[fits]
+                    ent[ok, 3] = FOP_INTERNAL
+                    ent[ok, 4] = b
+                    ent[ok, 5] = G.flat([base[a][fits] for a in range(3)])
+                    ent[ok, 6] = elem[fits]
+                    ent[ok, 7] = 2 * L
+                    ent = np.delete(ent, idx[~fits], axis=0)
+            rows.append(ent)
+    ent = np.concatenate(rows) if rows else np.zeros((0, 8), dtype=np.int64)
+    ent = ent[np.argsort(ent[:, 7], kind="stable")]
+    nph = int(ent[:, 7].max()) + 1 if len(ent) else 0
+    ends = np.array([int((ent[:, 7] <= p).sum()) for p in range(nph)], dtype=np.int64)
+    return ent.astype(np.int32), ends, skipped
+
+
+def emf_table(mesh: SMRMesh):
+    """EMF correction entries (int32 [n, 6])."""
+    G = _Geo(mesh)
+    ng, nx, act = G.ng, G.nx, G.act
+    rows = []
+    for b, blk in enumerate(mesh.blocks):
+        L = blk.level
+        if L + 1 >= mesh.levels:
+            continue
+        t = G.tot(L)
+        for e in range(3):
+            # the block's edges: zones along e, nodes across
+            rng = []
+            for a in range(3):
+                if not act[a]:
+                    rng.append(np.zeros(1, dtype=np.int64))
+                elif a == e:
+                    rng.append(np.arange(ng, ng + nx[a]))
+                else:
+                    rng.append(np.arange(ng, ng + nx[a] + 1))
+            Z3, Z2, Z1 = np.meshgrid(rng[2], rng[1], rng[0], indexing="ij")
+            lc = [Z1.ravel(), Z2.ravel(), Z3.ravel()]
+            bnd = np.zeros(len(lc[0]), dtype=bool)
+            for a in range(3):
+                if act[a] and a != e:
+                    bnd |= (lc[a] == ng) | (lc[a] == ng + nx[a])
+            lc = [x[bnd] for x in lc]
+            if not len(lc[0]):
+                continue
+            g = [((blk.loc[a] * nx[a] + lc[a] - ng) % t[a]) if act[a] else np.zeros_like(lc[a]) for a in range(3)]
+            # fine edge of lowest index along e; the fine zones around it
+            gf = [2 * g[a] if act[a] else g[a] for a in range(3)]
+            trans = [a for a in range(3) if a != e and act[a]]
+            fb = np.full(len(g[0]), -1, dtype=np.int64)
+            fl = [np.zeros_like(g[0]) for _ in range(3)]
+            for shifts in ([(0, 0), (0, -1), (-1, 0), (-1, -1)] if len(trans) == 2 else [(0,), (-1,)]):
+                z = list(gf)
+                for a, s in zip(trans, shifts):
+                    z[a] = gf[a] + s
+                ob = G.zone_owner(L + 1, z)
+                take = (fb < 0) & (ob >= 0)
+                if not take.any():
+                    continue
+                zl = G._locals(np.where(take, ob, -1), L + 1, z)
+                for a in range(3):
+                    v = zl[a]
+                    if a in trans and shifts[trans.index(a)] == -1:
+                        v = v + 1          # the zone below the node: its upper node
+                    fl[a] = np.where(take, v, fl[a])
+                fb = np.where(take, ob, fb)
+            m = fb >= 0
+            if not m.any():
+                continue
+            n = int(m.sum())
+            rows.append(np.stack([np.full(n, b), np.full(n, e), G.flat([x[m] for x in lc]), fb[m],
+                                  G.flat([x[m] for x in fl]), np.zeros(n, dtype=np.int64)], axis=1))
+    ent = np.concatenate(rows) if rows else np.zeros((0, 6), dtype=np.int64)
+    return ent.astype(np.int32)
+
+
+def cell_phase_ends(ghost, n_first):
+    """Phase ends of SMRMesh.tables()'s ghost-zone entries: copies and restrictions, then the
+    prolongations of each destination level (aux >> 8 = level - 1)."""
+    ends = [int(n_first)]
+    if len(ghost) > n_first:
+        ph = ghost[n_first:, 5] >> 8
+        for p in range(int(ph.max()) + 1):
+            ends.append(int(n_first + (ph <= p).sum()))
+    return np.array(ends, dtype=np.int64)
+
+
+class CTMesh:
+    """An SMRMesh of B_CT MHD blocks stepped with RK2: per block khb_ct_stage_fluxes, the mesh's flux
+    and EMF corrections, khb_ct_stage_update, then the ghost exchange of the stage output.
+    P_blocks: each block's primitives (8, n3, n2, n1) over the whole block; Bf_blocks: each block's
+    face field (3, n3, n2, n1), or None to interpolate it from the zone B."""
+
+    def __init__(self, mesh: SMRMesh, P_blocks, Bf_blocks=None, emf_correction=True, flux_correction=True):
+        import torch
+        from .block import Block, Fields
+        self.torch = torch
+        self.mesh = mesh
+        self.blocks = []
+        for n, blk in enumerate(mesh.blocks):
+            b = Block(blk.spec)
+            b.set_prims(P_blocks[n], faces=None if Bf_blocks is None else Bf_blocks[n])
+            self.blocks.append(b)
+        self.lib = self.blocks[0].lib
+        self.P1 = [torch.zeros_like(b.P) for b in self.blocks]
+        self.U1 = [torch.zeros_like(b.U) for b in self.blocks]
+        self.Bf1 = [torch.zeros_like(b.Bf) for b in self.blocks]
+        self.F1 = [(Fields(p), Fields(u), Fields(f)) for p, u, f in zip(self.P1, self.U1, self.Bf1)]
+        ghost, n_first, flux = mesh.tables()
+        cell_ends = cell_phase_ends(ghost, n_first)
+        face, face_ends, self.skipped_faces = face_tables(mesh)
+        emf = emf_table(mesh)
+        if not flux_correction:
+            flux = flux[:0]
+        if not emf_correction:
+            emf = emf[:0]
+        self.tables = {"cell": ghost, "face": face, "flux": flux, "emf": emf}
+        self._keep = [np.ascontiguousarray(x) for x in (ghost, cell_ends, face, face_ends, flux, emf)]
+        g, ce, f, fe, fl, em = self._keep
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        ctxs = (C.c_void_p * len(self.blocks))(*[b.ctx.value for b in self.blocks])
+        m = C.c_void_p()
+        _lib.check(self.lib.khb_ctmesh_create(ctxs, len(self.blocks), ptr(g), len(g), ptr(ce), len(ce), ptr(f), len(f),
+                                              ptr(fe), len(fe), ptr(fl), len(fl), ptr(em), len(em), C.byref(m)),
+                   "khb_ctmesh_create")
+        self.m = m
+        self.exchange(0)
+
+    def __del__(self):
+        try:
+            if getattr(self, "m", None):
+                self.lib.khb_ctmesh_destroy(self.m)
+                self.m = None
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return self.blocks[0].stream
+
+    def _state(self, s):
+        """(P, U, Bf) Fields of every block: s = 0 the state, 1 the intermediate stage."""
+        if s == 0:
+            return [(b.Pf, b.Uf, b.Bff) for b in self.blocks]
+        return self.F1
+
+    def exchange(self, s):
+        """Ghost zones and ghost faces of state s, then B and U = U(P) in every block's ghost zones."""
+        st = self._state(s)
+        P = (_lib.KhbFields * len(st))(*[x[0].s for x in st])
+        B = (_lib.KhbFields * len(st))(*[x[2].s for x in st])
+        _lib.check(self.lib.khb_ctmesh_exchange(self.m, C.cast(P, C.c_void_p), C.cast(B, C.c_void_p), self.stream),
+                   "khb_ctmesh_exchange")
+        for b, (Pf, Uf, Bff) in zip(self.blocks, st):
+            _lib.check(self.lib.khb_ct_ghost_from_faces(b.ctx, Pf.ref, Uf.ref, Bff.ref, self.stream),
+                       "khb_ct_ghost_from_faces")
+
+    def step(self, dt):
+        for stage in (1, 2):
+            src = self._state(stage - 1)
+            out = self._state(1 if stage == 1 else 0)
+            st0 = self._state(0)
+            for b, (Ps, _, _) in zip(self.blocks, src):
+                _lib.check(self.lib.khb_ct_stage_fluxes(b.ctx, Ps.ref, self.stream), "khb_ct_stage_fluxes")
+            _lib.check(self.lib.khb_ctmesh_correct(self.m, self.stream), "khb_ctmesh_correct")
+            for b, (Ps, Us, Bs), (_, U0, B0), (Po, Uo, Bo) in zip(self.blocks, src, st0, out):
+                _lib.check(self.lib.khb_ct_stage_update(b.ctx, stage, float(dt), Ps.ref, Us.ref, U0.ref, Bs.ref,
+                                                        B0.ref, Po.ref, Uo.ref, Bo.ref,
+                                                        C.c_void_p(b.pflag.data_ptr()),
+                                                        C.c_void_p(b.fflag.data_ptr()), self.stream),
+                           "khb_ct_stage_update")
+            self.exchange(1 if stage == 1 else 0)
+
+    def max_divb(self):
+        """Max over the blocks of khb_ct_max_divb (interior zones)."""
+        return max(b.max_divb() for b in self.blocks)
+
+    def conserved_totals(self):
+        """Sum over the blocks' interiors of U times the zone volume, per variable."""
+        tot = np.zeros(8)
+        for n, (blk, b) in enumerate(zip(self.mesh.blocks, self.blocks)):
+            U = b.U.cpu().numpy()
+            sl = (slice(None),) + blk.spec.interior
+            tot += U[sl].reshape(8, -1).sum(axis=1) * self.mesh.zone_volume(n)
+        return tot

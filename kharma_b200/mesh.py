@@ -53,7 +53,8 @@ class SMRMesh:
     level); refinements apply recursively, coarsest first."""
 
     def __init__(self, base: BlockSpec, nb, nx, refine=()):
-        assert base.cart_minkowski and base.nvar == 5, "SMR: Cartesian Minkowski hydro blocks"
+        assert base.cart_minkowski and (base.nvar == 5 or base.b_ct != "none"), \
+            "SMR: Cartesian Minkowski hydro blocks, or MHD blocks with B_CT"
         self.base = base
         self.nb = tuple(nb)
         self.nx = tuple(nx)

@@ -1,0 +1,186 @@
+"""SMR meshes of B_CT MHD blocks (khb_ctmesh_*, kharma_b200/ctmesh.py) on a periodic box.
+
+* After an exchange every ghost face the tables fill and every ghost zone's fluid primitives equal,
+  bitwise, the oracle-side restatement from whole-domain level arrays (oracle/smr_ref.py), on random
+  fields, for two- and three-level 2D and two-level 3D meshes.
+* One level of blocks steps bitwise as one block of the whole box (khb_ct_step).
+* A refined mesh evolving a magnetized entropy wave keeps every block's face divergence at round-off,
+  in the interior and in the ghost zones the exchange fills, and conserves mass to rounding; a coarse
+  face on a fine-coarse boundary stays the mean of the fine faces on it only with the EMF
+  correction (the check has teeth).
+"""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from ctmesh_cases import MESHES, base, curl_faces_levels, cut, fluid_levels, level_dx, random_levels
+from kharma_b200 import ctmesh
+from kharma_b200.block import Block
+from kharma_b200.mesh import SMRMesh
+
+pytestmark = pytest.mark.gpu
+
+_spec = importlib.util.spec_from_file_location(
+    "smr_ref", os.path.join(os.path.dirname(__file__), "..", "oracle", "smr_ref.py"))
+smr_ref = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(smr_ref)
+
+
+@pytest.mark.parametrize("name", list(MESHES))
+def test_exchange_matches_restatement(name):
+    mesh = MESHES[name]()
+    P = cut(mesh, random_levels(mesh, 8, seed=3, positive=True))
+    Bf = cut(mesh, random_levels(mesh, 3, seed=4))
+    m = ctmesh.CTMesh(mesh, P, Bf)          # the constructor exchanges once
+    # put the random fields back (set_prims rebuilt the zone B) and exchange again
+    for b, p, f in zip(m.blocks, P, Bf):
+        b.P.copy_(torch.as_tensor(p))
+        b.Bf.copy_(torch.as_tensor(f))
+    m.exchange(0)
+    torch.cuda.synchronize()
+    exp_f = smr_ref.expected_face_ghosts(mesh, Bf, level_dx(mesh))
+    exp_c = smr_ref.expected_ghosts(mesh, [p[:5] for p in P])
+    face = m.tables["face"]
+    for n, b in enumerate(m.blocks):
+        got = b.Bf.cpu().numpy().reshape(3, -1)
+        mine = face[face[:, 0] == n]
+        for d in range(3):
+            x = mine[mine[:, 1] == d, 2]
+            assert np.array_equal(got[d][x], exp_f[n][d].reshape(-1)[x]), f"block {n} faces {d}"
+        mask, E = exp_c[n]
+        Pg = b.P.cpu().numpy()
+        for v in range(5):
+            assert np.array_equal(Pg[v][mask], E[v][mask]), f"block {n} var {v}"
+
+
+def uniform_mesh_and_block(nd):
+    """2x2(x2) blocks of one level and the one block of the whole box, same state."""
+    mesh = SMRMesh(base(nd, nx=16), (2, 2, 2 if nd > 2 else 1), (16, 16, 16 if nd > 2 else 1))
+    big = base(nd, nx=32)
+    return mesh, big
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_one_level_steps_as_one_block(nd):
+    mesh, big = uniform_mesh_and_block(nd)
+    Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh)
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    one = SMRMesh(big, (1, 1, 1), (32, 32, 32 if nd > 2 else 1))
+    Pb, Fb = cut(one, Pl), cut(one, Fl)
+    b = Block(big)
+    b.set_prims(Pb[0], faces=Fb[0])
+    b.step(0.005)
+    m.step(0.005)
+    b.step(0.005)
+    m.step(0.005)
+    torch.cuda.synchronize()
+    ng = big.ng
+    for n, (blk, mb) in enumerate(zip(mesh.blocks, m.blocks)):
+        sl = []
+        for a in (2, 1, 0):
+            if a < mesh.ndim:
+                sl.append(slice(ng + blk.loc[a] * 16, ng + blk.loc[a] * 16 + 16))
+            else:
+                sl.append(slice(0, 1))
+        sl = tuple(sl)
+        assert np.array_equal(mb.P.cpu().numpy()[(slice(None),) + blk.spec.interior], b.P.cpu().numpy()[(slice(None),) + sl])
+        for d in range(3):
+            # the faces a block owns: its interior plus its upper boundary face
+            hi = [slice(s.start, s.stop + (1 if (2 - ax) == d and d < mesh.ndim else 0)) for ax, s in enumerate(sl)]
+            own = [slice(s.start, s.stop + (1 if (2 - ax) == d and d < mesh.ndim else 0)) for ax, s in enumerate(blk.spec.interior)]
+            assert np.array_equal(mb.Bf[d].cpu().numpy()[tuple(own)], b.Bf[d].cpu().numpy()[tuple(hi)]), f"block {n} face {d}"
+
+
+def interface_mismatch(m):
+    """Max over the faces of coarse blocks on a fine-coarse boundary of |coarse face - mean of the fine
+    faces on it| (each block's own faces)."""
+    mesh = m.mesh
+    G = ctmesh._Geo(mesh)
+    ng, nx, act = G.ng, G.nx, G.act
+    Bf = [b.Bf.cpu().numpy() for b in m.blocks]
+    worst = 0.
+    for b, blk in enumerate(mesh.blocks):
+        L = blk.level
+        if L + 1 >= mesh.levels:
+            continue
+        t = G.tot(L)
+        for d in range(mesh.ndim):
+            tr = [a for a in range(3) if act[a] and a != d]
+            for side in (ng, ng + nx[d]):
+                rng = [np.arange(ng, ng + nx[a]) if a in tr else np.zeros(1, dtype=np.int64) for a in range(3)]
+                rng[d] = np.array([side])
+                Z3, Z2, Z1 = np.meshgrid(rng[2], rng[1], rng[0], indexing="ij")
+                lc = [Z1.ravel(), Z2.ravel(), Z3.ravel()]
+                g = [((blk.loc[a] * nx[a] + lc[a] - ng) % t[a]) if act[a] else lc[a] for a in range(3)]
+                gf = [2 * g[a] if act[a] else g[a] for a in range(3)]
+                fb, fl = G.face_owner(L + 1, d, gf)
+                for n in np.nonzero(fb >= 0)[0]:
+                    f = Bf[int(fb[n])][d]
+                    x = [int(fl[a][n]) for a in range(3)]
+                    vals = []
+                    for o in range(1 << len(tr)):
+                        y = list(x)
+                        for q, a in enumerate(tr):
+                            y[a] += (o >> q) & 1
+                        vals.append(f[y[2], y[1], y[0]])
+                    mean = float(np.mean(vals))
+                    worst = max(worst, abs(Bf[b][d][lc[2][n], lc[1][n], lc[0][n]] - mean))
+    return worst
+
+
+def ghost_divb(m, depth=2):
+    """Max |div B| dx over the zones within `depth` layers of each block's interior (ghost zones
+    included), from the block's face arrays."""
+    worst = 0.
+    nd = m.mesh.ndim
+    for blk, b in zip(m.mesh.blocks, m.blocks):
+        F = b.Bf.cpu().numpy()
+        dx = blk.spec.dx
+        ng = blk.spec.ng
+        n3, n2, n1 = blk.spec.shape
+        lo = ng - depth
+        rng = [slice(lo, n1 - ng + depth), slice(lo, n2 - ng + depth), slice(lo, n3 - ng + depth) if nd > 2 else slice(0, 1)]
+        div = np.zeros(F[0][rng[2], rng[1], rng[0]].shape)
+        for d in range(nd):
+            s_hi = list(rng)
+            s_hi[d] = slice(rng[d].start + 1, rng[d].stop + 1)
+            div += (F[d][s_hi[2], s_hi[1], s_hi[0]] - F[d][rng[2], rng[1], rng[0]]) / dx[d]
+        worst = max(worst, float(np.abs(div).max() * min(dx[:nd])))
+    return worst
+
+
+@pytest.mark.parametrize("name", ["2d_two_levels", "2d_three_levels", "3d_two_levels"])
+def test_refined_mesh_keeps_divb_and_mass(name):
+    mesh = MESHES[name]()
+    Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh)
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    m0 = m.conserved_totals()
+    d0 = ghost_divb(m)
+    dt = 0.4 * min(min(b.spec.dx[:mesh.ndim]) for b in mesh.blocks)
+    for _ in range(10):
+        m.step(dt)
+    torch.cuda.synchronize()
+    m1 = m.conserved_totals()
+    scale = max(float(np.abs(b.Bf.cpu().numpy()).max()) for b in m.blocks)
+    print(name, "divB interior", m.max_divb(), "ghost-layer divB*dx", ghost_divb(m), "start", d0,
+          "mass change", (m1[0] - m0[0]) / m0[0], "interface mismatch", interface_mismatch(m))
+    assert m.max_divb() * min(min(b.spec.dx[:mesh.ndim]) for b in mesh.blocks) < 1e-13 * scale
+    assert ghost_divb(m) < 1e-13 * scale
+    assert abs(m1[0] - m0[0]) < 1e-13 * abs(m0[0])
+    assert interface_mismatch(m) < 1e-13 * scale
+
+
+def test_emf_correction_has_teeth():
+    mesh = MESHES["2d_two_levels"]()
+    Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh)
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl), emf_correction=False)
+    dt = 0.4 * min(min(b.spec.dx[:2]) for b in mesh.blocks)
+    for _ in range(10):
+        m.step(dt)
+    torch.cuda.synchronize()
+    scale = max(float(np.abs(b.Bf.cpu().numpy()).max()) for b in m.blocks)
+    print("without EMF correction: interface mismatch", interface_mismatch(m), "ghost-layer divB*dx", ghost_divb(m))
+    assert interface_mismatch(m) > 1e-8 * scale
