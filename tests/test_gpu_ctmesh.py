@@ -184,3 +184,43 @@ def test_emf_correction_has_teeth():
     scale = max(float(np.abs(b.Bf.cpu().numpy()).max()) for b in m.blocks)
     print("without EMF correction: interface mismatch", interface_mismatch(m), "ghost-layer divB*dx", ghost_divb(m))
     assert interface_mismatch(m) > 1e-8 * scale
+
+
+def test_fast_mode_across_refinement():
+    """The 2D fast magnetosonic mode (k = (2 pi, 2 pi, 0), the reference's mhdmodes) run for one period
+    on a mesh whose central quarter is refined: its L1 error in B1 lies between those of the uniform
+    coarse (64^2) and uniform fine (128^2) runs."""
+    from kharma_b200 import problems
+    nmode = 3
+    mesh = SMRMesh(base(2), (4, 4, 1), (16, 16, 1), refine=[(1, 1, 0), (1, 2, 0), (2, 1, 0), (2, 2, 0)])
+    m = ctmesh.CTMesh(mesh, [problems.mhdmodes(blk.spec, nmode) for blk in mesh.blocks])
+    tlim = problems.mhdmodes_period(nmode)
+
+    def run(step, dx_min):
+        dt0 = 0.4 * dx_min
+        n = int(np.ceil(tlim / dt0))
+        for _ in range(n):
+            step(tlim / n)
+
+    run(m.step, 1.0 / 128)
+
+    def l1(blocks_specs):
+        err, vol = 0., 0.
+        for spec, P in blocks_specs:
+            ref = problems.mhdmodes_analytic(spec, nmode)
+            sl = spec.interior
+            dv = spec.dx[0] * spec.dx[1]
+            err += np.abs(P[5][sl] - ref[5][sl]).sum() * dv
+            vol += P[5][sl].size * dv
+        return err / vol
+
+    e_mesh = l1([(blk.spec, b.P.cpu().numpy()) for blk, b in zip(mesh.blocks, m.blocks)])
+    errs = {}
+    for n in (64, 128):
+        spec = base(2, nx=n)
+        b = Block(spec)
+        b.set_prims(problems.mhdmodes(spec, nmode))
+        run(b.step, 1.0 / 128)
+        errs[n] = l1([(spec, b.P.cpu().numpy())])
+    print("fast mode L1(B1): coarse", errs[64], "refined mesh", e_mesh, "fine", errs[128])
+    assert errs[128] < e_mesh < errs[64]
