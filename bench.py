@@ -511,8 +511,10 @@ def smr_b_ct_form(steps=5, warm=2):
     central 2 x 2 x 2 refined (56 + 64 blocks, 3.9M zones), magnetized entropy wave (faces the curl of
     a vector potential), linear MC, LLF, gs05_c EMFs, FP64, fixed dt; each stage runs every block's
     khb_ct_stage_fluxes, the flux and EMF corrections, every block's khb_ct_stage_update and the
-    exchange, launched block by block from the host; against the same blocks stepped alone
-    (khb_ct_step).  CUDA events on the current stream; max face divergence after the run."""
+    exchange, launched block by block from the host (eager) or replayed from a CUDA graph of the whole
+    step, the per-block work spread over 8 streams; against the same blocks stepped alone (khb_ct_step,
+    eager, one stream).  CUDA events on the current
+    stream; max face divergence after the run."""
     import torch
     from kharma_b200 import ctmesh
     from kharma_b200.ctmesh import curl_faces_levels, cut, fluid_levels
@@ -523,7 +525,7 @@ def smr_b_ct_form(steps=5, warm=2):
                         gam=4. / 3., nvar=8, recon="linear_mc", riemann="llf", b_ct="gs05_c", driver="kharma")
     refine = [(i, j, k) for i in (1, 2) for j in (1, 2) for k in (1, 2)]
     mesh = SMRMesh(ct_base, (4, 4, 4), (32, 32, 32), refine=refine)
-    m = ctmesh.CTMesh(mesh, cut(mesh, fluid_levels(mesh)), cut(mesh, curl_faces_levels(mesh)))
+    m = ctmesh.CTMesh(mesh, cut(mesh, fluid_levels(mesh)), cut(mesh, curl_faces_levels(mesh)), streams=8)
     dt = 0.3 * min(blk.spec.dx[0] for blk in mesh.blocks)
 
     def timed(step):
@@ -540,13 +542,14 @@ def smr_b_ct_form(steps=5, warm=2):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps
 
-    ms = timed(lambda: m.step(dt))
+    ms_eager = timed(lambda: m.step(dt))
+    ms = timed(lambda: m.step_graph(dt))
     divb = m.max_divb() * min(mesh.blocks[0].spec.dx)
     ms_alone = timed(lambda: [b.step(dt) for b in m.blocks])
     out = {"workload": f"B_CT MHD mesh: 4x4x4 root blocks of 32^3, central 2x2x2 refined: {len(mesh.blocks)} blocks, "
                        f"{mesh.zones:,} zones, magnetized entropy wave, linear MC, LLF, gs05_c, FP64",
-           "ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0),
-           "blocks_alone_ms_per_step": ms_alone, "mesh_overhead": ms / ms_alone - 1.0,
+           "graph_ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0), "eager_ms_per_step": ms_eager,
+           "blocks_alone_eager_one_stream_ms_per_step": ms_alone,
            "max_face_divb_dx_after": divb,
            "face_entries": int(len(m.tables["face"])), "emf_entries": int(len(m.tables["emf"]))}
     del m

@@ -408,7 +408,9 @@ int khb_ct_ghost_from_faces(khb_ctx* ctx, const khb_fields* P, const khb_fields*
  * b_ct_functions.hpp:151-200)) and khb_ct_ghost_from_faces on every block.  Tables: ghost zones
  * (int32 x 6, the hydro mesh's format) with the end of each phase (copies and restrictions, then
  * one phase per destination level); ghost faces (int32 x 8) with phase ends; fluxes and EMFs
- * (int32 x 6).  P and Bf of khb_ctmesh_exchange are arrays of nblocks fields.
+ * (int32 x 6).  P and Bf of khb_ctmesh_exchange are arrays of nblocks fields; the first exchange of a
+ * state (its set of P and Bf pointers) uploads that state's descriptors and waits for the copy, later
+ * ones, and every khb_ctmesh_correct, only launch kernels.
  * --------------------------------------------------------------------------------------------- */
 typedef struct khb_ctmesh khb_ctmesh;
 int khb_ctmesh_create(khb_ctx* const* ctxs, int nblocks, const int32_t* cell, int64_t n_cell,

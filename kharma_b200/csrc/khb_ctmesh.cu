@@ -198,7 +198,15 @@ using namespace khb;
 struct khb_ctmesh {
     std::vector<khb_ctx*> ctx;
     CtmDims d;
-    CtmBlock* dev_blocks = nullptr;     // per call: the state the exchange works on
+    CtmBlock* dev_blocks = nullptr;     // the contexts' flux and EMF scratch (khb_ctmesh_correct)
+    // descriptors of each state an exchange has worked on, keyed by the first block's first
+    // primitive pointer: uploaded on the first exchange of a state, reused after (no transfer, no
+    // host wait, so that later calls can be captured in a CUDA graph)
+    struct State {
+        std::vector<CtmBlock> host;
+        CtmBlock* dev;
+    };
+    std::vector<State> states;
     std::vector<CtmBlock> host_blocks;
     int* cell = nullptr;
     long long n_cell = 0;
@@ -230,8 +238,9 @@ int upload(int** dst, const int32_t* src, long long n, int width)
     return KHB_OK;
 }
 
-// the descriptors of one state (per block P, Bf) plus the contexts' flux and EMF scratch
-int set_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, cudaStream_t st)
+// The descriptors of one state (per block P, Bf; NULL for the scratch-only set) plus the contexts'
+// flux and EMF scratch, uploaded synchronously into dev
+int upload_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, CtmBlock* dev)
 {
     const int n = (int)m->ctx.size();
     for (int b = 0; b < n; ++b) {
@@ -244,9 +253,31 @@ int set_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, cudaStr
         c.emf = (double*)x->emf;
         c.dx[0] = x->ph.dx1; c.dx[1] = x->ph.dx2; c.dx[2] = x->ph.dx3;
     }
-    KHB_MCUDA(cudaMemcpyAsync(m->dev_blocks, m->host_blocks.data(), sizeof(CtmBlock) * n, cudaMemcpyHostToDevice, st));
-    // the host copy is reused by the next call: let this one land first
-    KHB_MCUDA(cudaStreamSynchronize(st));
+    KHB_MCUDA(cudaMemcpy(dev, m->host_blocks.data(), sizeof(CtmBlock) * n, cudaMemcpyHostToDevice));
+    return KHB_OK;
+}
+
+// The device descriptors of state (P, Bf): uploaded on the first call with these pointers, found by
+// comparing the host copies afterwards (no device access)
+int state_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, CtmBlock** out)
+{
+    const int n = (int)m->ctx.size();
+    for (auto& s : m->states) {
+        bool same = true;
+        for (int b = 0; b < n && same; ++b) {
+            for (int p = 0; p < 8; ++p) same &= s.host[b].P[p] == P[b].v[p];
+            for (int q = 0; q < 3; ++q) same &= s.host[b].Bf[q] == Bf[b].v[q];
+        }
+        if (same) { *out = s.dev; return KHB_OK; }
+    }
+    khb_ctmesh::State s;
+    s.dev = nullptr;
+    KHB_MCUDA(cudaMalloc((void**)&s.dev, sizeof(CtmBlock) * n));
+    int rc;
+    if ((rc = upload_blocks(m, P, Bf, s.dev))) { cudaFree(s.dev); return rc; }
+    s.host = m->host_blocks;
+    m->states.push_back(s);
+    *out = s.dev;
     return KHB_OK;
 }
 
@@ -317,7 +348,8 @@ int khb_ctmesh_create(khb_ctx* const* ctxs, int nblocks, const int32_t* cell, in
     int rc;
     cudaError_t e = cudaMalloc((void**)&m->dev_blocks, sizeof(CtmBlock) * nblocks);
     if (e != cudaSuccess) { delete m; return ctm_fail(KHB_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
-    if ((rc = upload(&m->cell, cell, n_cell, 6)) || (rc = upload(&m->face, face, n_face, 8)) ||
+    if ((rc = upload_blocks(m, nullptr, nullptr, m->dev_blocks)) || (rc = upload(&m->cell, cell, n_cell, 6)) ||
+        (rc = upload(&m->face, face, n_face, 8)) ||
         (rc = upload(&m->flux, flux, n_flux, 6)) || (rc = upload(&m->emf, emf, n_emf, 6))) {
         cudaFree(m->dev_blocks); cudaFree(m->cell); cudaFree(m->face); cudaFree(m->flux); cudaFree(m->emf);
         delete m;
@@ -330,6 +362,7 @@ int khb_ctmesh_create(khb_ctx* const* ctxs, int nblocks, const int32_t* cell, in
 int khb_ctmesh_destroy(khb_ctmesh* m)
 {
     if (!m) return KHB_OK;
+    for (auto& s : m->states) cudaFree(s.dev);
     cudaFree(m->dev_blocks); cudaFree(m->cell); cudaFree(m->face); cudaFree(m->flux); cudaFree(m->emf);
     delete m;
     return KHB_OK;
@@ -340,8 +373,6 @@ int khb_ctmesh_correct(khb_ctmesh* m, void* stream)
     KHB_RANGE("khb_ctmesh_correct");
     if (!m) return ctm_fail(KHB_ERR_ARG, "khb_ctmesh_correct: NULL mesh");
     cudaStream_t st = (cudaStream_t)stream;
-    int rc;
-    if ((rc = set_blocks(m, nullptr, nullptr, st))) return rc;
     if (m->n_flux) k_ctm_flux<<<blocks_for(m->n_flux, 128), 128, 0, st>>>(m->dev_blocks, m->d, m->flux, m->n_flux);
     if (m->n_emf) k_ctm_emf<<<blocks_for(m->n_emf, 128), 128, 0, st>>>(m->dev_blocks, m->d, m->emf, m->n_emf);
     KHB_MCUDA(cudaGetLastError());
@@ -360,15 +391,16 @@ int khb_ctmesh_exchange(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf
     }
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
-    if ((rc = set_blocks(m, P, Bf, st))) return rc;
+    CtmBlock* blocks = nullptr;
+    if ((rc = state_blocks(m, P, Bf, &blocks))) return rc;
     long long lo = 0;
     for (long long hi : m->cell_ends) {
-        if (hi > lo) k_ctm_cell<<<blocks_for(hi - lo, 128), 128, 0, st>>>(m->dev_blocks, m->d, m->cell, lo, hi);
+        if (hi > lo) k_ctm_cell<<<blocks_for(hi - lo, 128), 128, 0, st>>>(blocks, m->d, m->cell, lo, hi);
         lo = hi;
     }
     lo = 0;
     for (long long hi : m->face_ends) {
-        if (hi > lo) k_ctm_face<<<blocks_for(hi - lo, 128), 128, 0, st>>>(m->dev_blocks, m->d, m->face, lo, hi);
+        if (hi > lo) k_ctm_face<<<blocks_for(hi - lo, 128), 128, 0, st>>>(blocks, m->d, m->face, lo, hi);
         lo = hi;
     }
     KHB_MCUDA(cudaGetLastError());

@@ -290,7 +290,8 @@ class CTMesh:
     P_blocks: each block's primitives (8, n3, n2, n1) over the whole block; Bf_blocks: each block's
     face field (3, n3, n2, n1), or None to interpolate it from the zone B."""
 
-    def __init__(self, mesh: SMRMesh, P_blocks, Bf_blocks=None, emf_correction=True, flux_correction=True):
+    def __init__(self, mesh: SMRMesh, P_blocks, Bf_blocks=None, emf_correction=True, flux_correction=True,
+                 streams=1):
         import torch
         from .block import Block, Fields
         self.torch = torch
@@ -323,6 +324,10 @@ class CTMesh:
                                               ptr(fe), len(fe), ptr(fl), len(fl), ptr(em), len(em), C.byref(m)),
                    "khb_ctmesh_create")
         self.m = m
+        self._graph = None
+        # the per-block work of each phase is spread over this many streams (blocks are independent
+        # there), joined before the mesh-wide corrections and exchange
+        self.streams = [torch.cuda.Stream() for _ in range(max(0, int(streams) - 1))]
         self.exchange(0)
 
     def __del__(self):
@@ -343,6 +348,19 @@ class CTMesh:
             return [(b.Pf, b.Uf, b.Bff) for b in self.blocks]
         return self.F1
 
+    def _per_block(self, fn):
+        """fn(n, block) for every block, block n on stream n mod (1 + extra streams), joined back."""
+        torch = self.torch
+        main = torch.cuda.current_stream()
+        lanes = [main] + self.streams
+        for s in self.streams:
+            s.wait_stream(main)
+        for n, b in enumerate(self.blocks):
+            with torch.cuda.stream(lanes[n % len(lanes)]):
+                fn(n, b)
+        for s in self.streams:
+            main.wait_stream(s)
+
     def exchange(self, s):
         """Ghost zones and ghost faces of state s, then B and U = U(P) in every block's ghost zones."""
         st = self._state(s)
@@ -350,25 +368,52 @@ class CTMesh:
         B = (_lib.KhbFields * len(st))(*[x[2].s for x in st])
         _lib.check(self.lib.khb_ctmesh_exchange(self.m, C.cast(P, C.c_void_p), C.cast(B, C.c_void_p), self.stream),
                    "khb_ctmesh_exchange")
-        for b, (Pf, Uf, Bff) in zip(self.blocks, st):
-            _lib.check(self.lib.khb_ct_ghost_from_faces(b.ctx, Pf.ref, Uf.ref, Bff.ref, self.stream),
+
+        def ghosts(n, b):
+            Pf, Uf, Bff = st[n]
+            _lib.check(self.lib.khb_ct_ghost_from_faces(b.ctx, Pf.ref, Uf.ref, Bff.ref, b.stream),
                        "khb_ct_ghost_from_faces")
+        self._per_block(ghosts)
 
     def step(self, dt):
         for stage in (1, 2):
             src = self._state(stage - 1)
             out = self._state(1 if stage == 1 else 0)
             st0 = self._state(0)
-            for b, (Ps, _, _) in zip(self.blocks, src):
-                _lib.check(self.lib.khb_ct_stage_fluxes(b.ctx, Ps.ref, self.stream), "khb_ct_stage_fluxes")
-            _lib.check(self.lib.khb_ctmesh_correct(self.m, self.stream), "khb_ctmesh_correct")
-            for b, (Ps, Us, Bs), (_, U0, B0), (Po, Uo, Bo) in zip(self.blocks, src, st0, out):
+
+            def fluxes(n, b):
+                _lib.check(self.lib.khb_ct_stage_fluxes(b.ctx, src[n][0].ref, b.stream), "khb_ct_stage_fluxes")
+
+            def update(n, b):
+                (Ps, Us, Bs), (_, U0, B0), (Po, Uo, Bo) = src[n], st0[n], out[n]
                 _lib.check(self.lib.khb_ct_stage_update(b.ctx, stage, float(dt), Ps.ref, Us.ref, U0.ref, Bs.ref,
                                                         B0.ref, Po.ref, Uo.ref, Bo.ref,
                                                         C.c_void_p(b.pflag.data_ptr()),
-                                                        C.c_void_p(b.fflag.data_ptr()), self.stream),
+                                                        C.c_void_p(b.fflag.data_ptr()), b.stream),
                            "khb_ct_stage_update")
+
+            self._per_block(fluxes)
+            _lib.check(self.lib.khb_ctmesh_correct(self.m, self.stream), "khb_ctmesh_correct")
+            self._per_block(update)
             self.exchange(1 if stage == 1 else 0)
+
+    def step_graph(self, dt):
+        """One step replayed from a CUDA graph of the whole mesh step (captured on the first call for
+        this dt, after one eager step that also registers both states' descriptors with the library)."""
+        torch = self.torch
+        if self._graph is not None and self._graph_dt == dt:
+            self._graph.replay()
+            return
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self.step(dt)
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.step(dt)
+        self._graph, self._graph_dt = g, dt
 
     def max_divb(self):
         """Max over the blocks of khb_ct_max_divb (interior zones)."""
