@@ -60,9 +60,11 @@ class LocalExchange:
 class DistExchange:
     """One slab per rank of the default process group; neighbours rank -/+ 1 (periodic).
 
-    host_staged: device slices travel through host buffers (a backend without device point-to-point
-    support, such as gloo, with the slabs on GPUs); otherwise the field arrays' own slices are sent
-    (NCCL between GPUs, or gloo with CPU tensors)."""
+    The planes of all arrays bound for one neighbour are packed (as bytes, whatever their types) into
+    one buffer, so that an exchange is two sends and two receives however many variables it carries.
+    host_staged: the packed buffers travel through host memory (a backend without device
+    point-to-point support, such as gloo, with the slabs on GPUs); otherwise they are sent from where
+    they are (NCCL between GPUs, or gloo with CPU tensors)."""
 
     def __init__(self, host_staged=False):
         import torch.distributed as dist
@@ -82,30 +84,32 @@ class DistExchange:
         views = []
         for a in arrays:
             views += [a[v] for v in range(a.shape[0])] if a.dim() == 4 else [a]
-        stage = self.host_staged and views and views[0].is_cuda
+        # each variable's plane range is contiguous: pack them byte-wise, one buffer per neighbour
+        as_bytes = lambda t: t.reshape(-1).view(torch.uint8)
+        send_lo = torch.cat([as_bytes(a[slo]) for a in views])
+        send_hi = torch.cat([as_bytes(a[shi]) for a in views])
+        stage = self.host_staged and send_lo.is_cuda
         if stage:
             torch.cuda.current_stream().synchronize()
-            sends = [(a[slo].cpu(), a[shi].cpu()) for a in views]
-            recvs = [(torch.empty_like(lo), torch.empty_like(hi)) for lo, hi in sends]
-        else:
-            sends = [(a[slo], a[shi]) for a in views]
-            recvs = [(a[rhi], a[rlo]) for a in views]
-        ops = []
+            send_lo, send_hi = send_lo.cpu(), send_hi.cpu()
+        recv_hi, recv_lo = torch.empty_like(send_lo), torch.empty_like(send_hi)
         # Per peer the k-th send matches the k-th receive: send (low planes -> left, high planes ->
         # right) and receive (high ghosts <- right, low ghosts <- left) in this order, so that with
         # two ranks (left == right) the low planes still land in the peer's high ghosts.
-        for lo, hi in sends:
-            ops.append(dist.P2POp(dist.isend, lo, left))
-            ops.append(dist.P2POp(dist.isend, hi, right))
-        for into_hi, into_lo in recvs:
-            ops.append(dist.P2POp(dist.irecv, into_hi, right))
-            ops.append(dist.P2POp(dist.irecv, into_lo, left))
+        ops = [dist.P2POp(dist.isend, send_lo, left), dist.P2POp(dist.isend, send_hi, right),
+               dist.P2POp(dist.irecv, recv_hi, right), dist.P2POp(dist.irecv, recv_lo, left)]
         for req in dist.batch_isend_irecv(ops):
             req.wait()
         if stage:
-            for a, (into_hi, into_lo) in zip(views, recvs):
-                a[rhi].copy_(into_hi)
-                a[rlo].copy_(into_lo)
+            dev = views[0].device
+            recv_hi, recv_lo = recv_hi.to(dev), recv_lo.to(dev)
+        off = 0
+        for a in views:
+            hi, lo = a[rhi], a[rlo]
+            n = hi.numel() * hi.element_size()
+            as_bytes(hi).copy_(recv_hi[off:off + n])
+            as_bytes(lo).copy_(recv_lo[off:off + n])
+            off += n
 
 
 class SlabBlock:
