@@ -243,7 +243,9 @@ int khb_fix_utop(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const i
 
 /* Physical and periodic boundary conditions for P (fluid primitives) and the conserved field,
  * then B_P = B_U/gdet and U = U(P) in every ghost zone (boundaries.cpp:369-589 with Parthenon's
- * outflow/reflecting functions, and Flux::MeshPtoU on the ghosts). */
+ * outflow/reflecting functions, and Flux::MeshPtoU on the ghosts).  A block with exchange faces: the
+ * conditions over the whole transverse range, after the caller's exchange, and B_P, U only past its
+ * physical faces. */
 int khb_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, void* stream);
 
 /* Flux::MeshPtoU (flux.cpp:276-322) over the whole block. */
@@ -359,7 +361,10 @@ int khb_adjoint_ptou(khb_ctx* ctx, const khb_fields* P, const khb_fields* Ubar, 
  * B_CT::AddSource (b_ct.cpp:412-470: face changes from the EMF circulation) and the face update
  * Bf_out = gam0 Bf_s + gam1 Bf_0 + beta dt dBf/dt (kharma_driver.cpp:339-387, WeightedSumDataFace),
  * then the zone pass with the zone B taken from the updated faces (B_CT::BlockUtoP,
- * b_ct.cpp:160-188) instead of the flux-CT divergence, fixups and ghost zones as khb_stage. */
+ * b_ct.cpp:160-188) instead of the flux-CT divergence, fixups and ghost zones as khb_stage.  A block
+ * with exchange faces (a block of a mesh) gets no ghost zones here: the caller exchanges, then calls
+ * khb_ct_ghost_from_faces and, for physical faces, khb_ct_boundaries (the reference's sync, MeshUtoP
+ * over the entire block, then its domain conditions: kharma_step.cpp:209-249). */
 int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,
                  const khb_fields* U_0, const khb_fields* Bf_s, const khb_fields* Bf_0, const khb_fields* P_out,
                  const khb_fields* U_out, const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream);
@@ -371,7 +376,9 @@ int khb_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, cons
  * (clean_face_B, b_ct_boundaries.cpp:190-262); transmitting X2 faces: the mirror rows half-way
  * round in x3 (one_block_transmit.cpp:60-143) — then the zone boundaries as khb_boundaries, with the
  * ghost zones' B from their faces (B_CT::BlockUtoP over the boundary domain).  Without physical
- * faces it is khb_boundaries.  During each stage reflecting faces zero the EMFs on their domain-face
+ * faces it is khb_boundaries.  On a block with exchange faces the conditions run over the whole
+ * transverse range (the ghost rows the exchange filled included) and B and U = U(P) are rebuilt past
+ * the physical faces only.  During each stage reflecting faces zero the EMFs on their domain-face
  * edges (zero_EMF, b_ct_boundaries.cpp:40-62) and transmitting ones average them (average_EMF,
  * b_ct_boundaries.cpp:64-186). */
 int khb_ct_boundaries(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf, void* stream);
@@ -397,7 +404,8 @@ int khb_ct_ghost_from_faces(khb_ctx* ctx, const khb_fields* P, const khb_fields*
 /* ---------------------------------------------------------------------------------------------
  * SMR meshes of B_CT blocks (KHARMA's default field transport on multilevel meshes,
  * kharma.cpp:376-395): tables from kharma_b200/ctmesh.py.  Blocks: FP64, Cartesian Minkowski,
- * one shape, 2D or 3D, every face an exchange face.  Per stage: khb_ct_stage_fluxes on every
+ * one shape, 2D or 3D; every face an exchange face or an outflow/reflecting domain face, which the
+ * block applies with khb_ct_boundaries after the exchange (no table entry reaches past it).  Per stage: khb_ct_stage_fluxes on every
  * block, khb_ctmesh_correct (the fluid fluxes of coarse faces on a fine-coarse boundary become the
  * mean of the fine fluxes, and coarse edge EMFs that coincide with fine edges the mean of the fine
  * EMFs along them: Parthenon's flux correction, kharma_step.cpp:183-194), khb_ct_stage_update on
@@ -542,12 +550,15 @@ int64_t khb_batch_launch_count(khb_batch* batch);
  * the copies and restrictions, the rest the prolongations in phase order, each phase launched after
  * the previous one (a level's prolongations read coarse ghost zones the coarser level's filled).  The primitives
  * are filled, then U = U(P) in those zones.  flux: n_flux entries {coarse block, direction, coarse
- * face, fine block, fine face of lowest index, 0}.  Hydro blocks (nvar 5) with exchange faces.
- * Every index is checked against the blocks' sizes.  Synchronizes the device. */
+ * face, fine block, fine face of lowest index, 0}.  Hydro blocks (nvar 5) with exchange faces; a
+ * block on an outflow or reflecting domain face applies it after each exchange, over the ghost rows
+ * the exchange filled (no entry reaches past it).  Every index is checked against the blocks' sizes.
+ * Synchronizes the device. */
 int khb_batch_set_mesh(khb_batch* batch, const int32_t* ghost, int64_t n_ghost, int64_t n_ghost_first,
                        const int32_t* flux, int64_t n_flux);
 
-/* Fill every block's ghost zones of the state (P, U) from the mesh (e.g. after initial data). */
+/* Fill every block's ghost zones of the state (P, U) from the mesh (e.g. after initial data), then
+ * the physical domain faces of the blocks on them. */
 int khb_batch_mesh_exchange(khb_batch* batch, void* stream);
 
 /* ---------------------------------------------------------------------------------------------

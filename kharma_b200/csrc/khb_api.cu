@@ -193,13 +193,28 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
     const Dims& d = ctx->d;
     const int nv = nv_state ? nv_state : ctx->nv;
     const int nv_ptou = (nv == 10) ? 8 : nv;     // ghost B_P and (GRMHD) U; the EMHD U is formed later
-    const int cnt_k = d.ke - d.ks + 1;
+    // the transverse range of a face's pass: the interior, or every zone along a direction with an
+    // exchange face (a block of a mesh: its ghost rows hold the neighbours' zones, and Parthenon
+    // applies the condition over them after the exchange)
+    const bool xj = d.ndim >= 2 && (d.bc[2] == KHB_BC_EXCHANGE || d.bc[3] == KHB_BC_EXCHANGE);
+    const bool xk = d.ndim >= 3 && (d.bc[4] == KHB_BC_EXCHANGE || d.bc[5] == KHB_BC_EXCHANGE);
+    const int lo_k = xk ? 0 : d.ks;
+    const int cnt_k = xk ? d.n3 : d.ke - d.ks + 1;
+    // a block of a mesh: B and U = U(P) over the boundary domains of its physical faces only
+    int pfaces = 0;
+    bool exch = false;
+    for (int f = 0; f < 2 * d.ndim; ++f) {
+        if (phys_face(d.bc[f])) pfaces |= 1 << f;
+        exch = exch || d.bc[f] == KHB_BC_EXCHANGE;
+    }
+    if (!exch) pfaces = 0;
     bool physical = false;
     int ct_mask = 0;
     if (Bf) {
-        if (phys_face(d.bc[0])) ct_mask |= 1;
-        if (d.ndim >= 2 && phys_face(d.bc[2])) ct_mask |= 2;
-        if (d.ndim >= 3 && phys_face(d.bc[4])) ct_mask |= 4;
+        // a direction with a physical face on either side (a block of a mesh may have one on one side only)
+        if (phys_face(d.bc[0]) || phys_face(d.bc[1])) ct_mask |= 1;
+        if (d.ndim >= 2 && (phys_face(d.bc[2]) || phys_face(d.bc[3]))) ct_mask |= 2;
+        if (d.ndim >= 3 && (phys_face(d.bc[4]) || phys_face(d.bc[5]))) ct_mask |= 4;
         if (!ct_mask) Bf = nullptr;
     }
     if (Bf) {
@@ -210,24 +225,29 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
     for (int face = 0; face < 2; ++face) {
         if (!phys_face(d.bc[face])) continue;
         physical = true;
-        LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, d.js, d.je - d.js + 1, d.ks, cnt_k, st);
+        LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, xj ? 0 : d.js, xj ? d.n2 : d.je - d.js + 1, lo_k, cnt_k, st);
         KHB_LAUNCHED(ctx);
     }
     if (d.ndim >= 2) {
         for (int face = 2; face < 4; ++face) {
             if (!phys_face(d.bc[face])) continue;
             physical = true;
-            LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, 0, d.n1, d.ks, cnt_k, st);
+            LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, face, 0, d.n1, lo_k, cnt_k, st);
             KHB_LAUNCHED(ctx);
         }
         if (ctx->cfg.fix_corner_inner && phys_face(d.bc[0]) && phys_face(d.bc[3])) {
-            LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, 0, 0, d.n2, d.ks, cnt_k, st);
+            LaunchCommon::bc(nv, d, ctx->g, ctx->ph, P, U, 0, 0, d.n2, lo_k, cnt_k, st);
             KHB_LAUNCHED(ctx);
         }
     }
     if (physical) {
-        LaunchCommon::ghost_ptou(nv_ptou, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask);
+        LaunchCommon::ghost_ptou(nv_ptou, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask, 0, pfaces);
         KHB_LAUNCHED(ctx);
+        if (xk) {
+            // the X1/X2 passes also filled the X3 ghost planes' corners
+            LaunchCommon::ghost_ptou(nv_ptou, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask, 3, pfaces);
+            KHB_LAUNCHED(ctx);
+        }
     }
     // X3 faces last (Parthenon's face order), over the whole (j, i) plane: their ghost planes copy
     // the boundary planes with the X1/X2 ghost zones already filled; then B_P and U = U(P) there
@@ -240,7 +260,7 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
             KHB_LAUNCHED(ctx);
         }
         if (kplanes) {
-            LaunchCommon::ghost_ptou(nv_ptou, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask, kplanes);
+            LaunchCommon::ghost_ptou(nv_ptou, d, ctx->g, ctx->ph, P, U, st, Bf, ct_mask, kplanes, pfaces);
             KHB_LAUNCHED(ctx);
         }
     }
@@ -358,6 +378,9 @@ int ct_stage_update(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, co
     ctx->ct_active = false;
     if (rc) return rc;
     if ((rc = launch_fixup(ctx, Pout, Uout, pflag, st))) return rc;
+    // a block of a mesh takes its physical faces after the exchange (khb_ct_boundaries), so that the
+    // faces it sends are those of the update, as in the reference's sync before its domain conditions
+    if (has_exchange_face(ctx->d)) return KHB_OK;
     return launch_boundaries(ctx, Pout, Uout, st, &Bout);
 }
 

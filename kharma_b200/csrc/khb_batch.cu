@@ -278,12 +278,13 @@ int enqueue_stage_fused(khb_batch* b, int s, cudaStream_t st)
     KHB_BLAUNCHED(b, 1);
     LaunchCommon::batch_fixup(b->nv, b->fix, b->nb, stage, st);
     KHB_BLAUNCHED(b, 1);
-    if ((rc = enqueue_bounds(b, s, st))) return rc;
+    // the mesh's exchange, then the physical faces over the ghost rows it filled (the reference's
+    // sync before its domain conditions, kharma_step.cpp:209-249)
     if (b->n_ghost) {
         enqueue_mesh_ghost(b, stage, st);
         KHB_BLAUNCHED(b, 0);
     }
-    return KHB_OK;
+    return enqueue_bounds(b, s, st);
 }
 
 template <typename FT>
@@ -318,12 +319,13 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
     KHB_BLAUNCHED(b, 1);
     LaunchCommon::batch_fixup(b->nv, b->fix, b->nb, stage, st);
     KHB_BLAUNCHED(b, 1);
-    if ((rc = enqueue_bounds(b, s, st))) return rc;
+    // the mesh's exchange, then the physical faces over the ghost rows it filled (the reference's
+    // sync before its domain conditions, kharma_step.cpp:209-249)
     if (b->n_ghost) {
         enqueue_mesh_ghost(b, stage, st);
         KHB_BLAUNCHED(b, 0);
     }
-    return KHB_OK;
+    return enqueue_bounds(b, s, st);
 }
 
 int enqueue_stage_any(khb_batch* b, int s, cudaStream_t st)
@@ -536,6 +538,8 @@ int khb_batch_mesh_exchange(khb_batch* b, void* stream)
     if (b->n_ghost) {
         enqueue_mesh_ghost(b, 2, S(stream));
         KHB_BCUDA(cudaGetLastError());
+        int rc;
+        if ((rc = enqueue_bounds(b, 1, S(stream)))) return rc;
     }
     return KHB_OK;
 }

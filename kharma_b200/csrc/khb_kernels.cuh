@@ -960,10 +960,12 @@ __host__ __device__ inline unsigned plane_ghost_count(const Dims& d)
 // 0: X1, bit 1: X2, bit 2: X3) takes B from its faces (B_CT::BlockUtoP over the boundary domain, b_ct.cpp:
 // 160-188); the last ghost layer of a direction has its lower face only (the face array stops
 // there) and takes B from that face alone.
-// kplanes: the ghost planes of physical X3 faces instead (whole (j, i) planes below ks and above ke)
+// kplanes: the ghost planes of physical X3 faces instead (whole (j, i) planes below ks and above ke).
+// pfaces (nonzero): a zone is taken only if it lies past a face whose bit is set (the boundary
+// domains inner_x1 ... outer_x3 of those faces; the exchanged ghost zones keep their values)
 template <int NV>
 __global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, khb_fields Bf, int ct_mask,
-                             int kplanes)
+                             int kplanes, int pfaces)
 {
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     int j, i, k;
@@ -983,6 +985,9 @@ __global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_field
         if (!plane_ghost(d, t - kk * per, j, i)) return;
         k = d.ks + (int)kk;
     }
+    if (pfaces && !(((pfaces & 1) && i < d.is) || ((pfaces & 2) && i > d.ie) || ((pfaces & 4) && j < d.js) ||
+                    ((pfaces & 8) && j > d.je) || ((pfaces & 16) && k < d.ks) || ((pfaces & 32) && k > d.ke)))
+        return;
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     ZoneGeom G;
     load_zone_geom(g, j, i, G);
@@ -1799,7 +1804,8 @@ void LaunchCommon::bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, c
 }
 
 void LaunchCommon::ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
-                              const khb_fields& U, cudaStream_t st, const khb_fields* Bf, int ct_mask, int kplanes)
+                              const khb_fields& U, cudaStream_t st, const khb_fields* Bf, int ct_mask, int kplanes,
+                              int pfaces)
 {
     const long long plane = (long long)d.n1 * d.n2;
     const long long tot = kplanes ? plane * (((kplanes & 1) ? d.ks : 0) + ((kplanes & 2) ? d.n3 - 1 - d.ke : 0))
@@ -1808,8 +1814,8 @@ void LaunchCommon::ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phy
     khb_fields F;
     for (int x = 0; x < KHB_MAX_VARS; ++x) F.v[x] = nullptr;
     if (Bf) for (int x = 0; x < 3; ++x) F.v[x] = Bf->v[x];
-    if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes);
-    else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes);
+    if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes, pfaces);
+    else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes, pfaces);
 }
 
 void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st)

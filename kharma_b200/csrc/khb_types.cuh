@@ -214,10 +214,12 @@ struct LaunchCommon {
     static void bc(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P, const khb_fields& U,
                    int face, int lo_a, int cnt_a, int lo_k, int cnt_k, cudaStream_t st);
     // kplanes: the ghost planes of physical X3 faces (bit 0: below ks, bit 1: above ke) instead of
-    // the X1/X2 ghost zones of the interior planes
+    // the X1/X2 ghost zones of the interior planes.  pfaces (nonzero): only the zones past the faces
+    // whose bits are set (bit f: face f = inner/outer X1, X2, X3), the boundary domains of a block
+    // whose other faces are exchanged
     static void ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
                            const khb_fields& U, cudaStream_t st, const khb_fields* Bf = nullptr, int ct_mask = 0,
-                           int kplanes = 0);
+                           int kplanes = 0, int pfaces = 0);
     static void periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st);
     static void ghost_copy(int nv, const Dims& d, const khb_fields& Pin, const khb_fields& Uin, const khb_fields& Pout,
                            const khb_fields& Uout, cudaStream_t st);

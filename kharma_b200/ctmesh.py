@@ -63,12 +63,21 @@ class _Geo:
         return self.m._zones_at(L)
 
     def zone_owner(self, L, g):
-        """Block owning level-L zones g (list of 3 arrays, x1..x3; periodic); -1 where none."""
+        """Block owning level-L zones g (list of 3 arrays, x1..x3; periodic directions wrap); -1 where
+        none, or past a physical domain face."""
         if L < 0 or L >= self.m.levels:
             return np.full(len(g[0]), -1, dtype=np.int64)
         t = self.tot(L)
-        lo = [(g[a] % t[a]) // self.nx[a] if self.act[a] else np.zeros_like(g[a]) for a in range(3)]
-        return self.own[L][lo[2], lo[1], lo[0]]
+        ok = np.ones(len(g[0]), dtype=bool)
+        for a in range(3):
+            if self.act[a] and not self.m.periodic[a]:
+                ok &= (g[a] >= 0) & (g[a] < t[a])
+        lo = [(np.clip(g[a], 0, t[a] - 1) if not self.m.periodic[a] else g[a] % t[a]) // self.nx[a]
+              if self.act[a] else np.zeros_like(g[a]) for a in range(3)]
+        return np.where(ok, self.own[L][lo[2], lo[1], lo[0]], -1)
+
+    def wrap(self, v, a, t):
+        return v % t if self.m.periodic[a] else v
 
     def local(self, b, L, g):
         """Local (x1, x2, x3) indices in block b of level-L global zones g that b owns."""
@@ -134,8 +143,16 @@ def face_tables(mesh: SMRMesh):
                 owned &= (loc3[a] >= ng) & (loc3[a] <= hi)
             sel = ~owned
             lg = [loc3[a][sel] for a in range(3)]
+            g = [G.wrap(blk.loc[a] * nx[a] + lg[a] - ng, a, t[a]) if act[a] else np.zeros_like(lg[a]) for a in range(3)]
+            # faces past a physical domain face are the block's own boundary condition's (the domain
+            # face itself, at index t along d, belongs to the last block)
+            keep = np.ones(len(lg[0]), dtype=bool)
+            for a in range(3):
+                if act[a] and not mesh.periodic[a]:
+                    keep &= (g[a] >= 0) & (g[a] <= (t[a] if a == d else t[a] - 1))
+            lg = [x[keep] for x in lg]
+            g = [x[keep] for x in g]
             dst = G.flat(lg)
-            g = [((blk.loc[a] * nx[a] + lg[a] - ng) % t[a]) if act[a] else np.zeros_like(lg[a]) for a in range(3)]
             n = len(dst)
             ent = np.full((n, 8), -1, dtype=np.int64)
             ent[:, 0] = b
@@ -242,7 +259,7 @@ def emf_table(mesh: SMRMesh):
             lc = [x[bnd] for x in lc]
             if not len(lc[0]):
                 continue
-            g = [((blk.loc[a] * nx[a] + lc[a] - ng) % t[a]) if act[a] else np.zeros_like(lc[a]) for a in range(3)]
+            g = [G.wrap(blk.loc[a] * nx[a] + lc[a] - ng, a, t[a]) if act[a] else np.zeros_like(lc[a]) for a in range(3)]
             # fine edge of lowest index along e; the fine zones around it
             gf = [2 * g[a] if act[a] else g[a] for a in range(3)]
             trans = [a for a in range(3) if a != e and act[a]]
@@ -302,6 +319,7 @@ class CTMesh:
             b.set_prims(P_blocks[n], faces=None if Bf_blocks is None else Bf_blocks[n])
             self.blocks.append(b)
         self.lib = self.blocks[0].lib
+        self._physical = [any(x not in ("exchange", "periodic") for x in blk.spec.bc) for blk in mesh.blocks]
         self.P1 = [torch.zeros_like(b.P) for b in self.blocks]
         self.U1 = [torch.zeros_like(b.U) for b in self.blocks]
         self.Bf1 = [torch.zeros_like(b.Bf) for b in self.blocks]
@@ -371,8 +389,14 @@ class CTMesh:
 
         def ghosts(n, b):
             Pf, Uf, Bff = st[n]
+            # B from the exchanged faces in every ghost zone (MeshUtoP over the entire block, before the
+            # domain conditions: kharma_step.cpp:233-249)
             _lib.check(self.lib.khb_ct_ghost_from_faces(b.ctx, Pf.ref, Uf.ref, Bff.ref, b.stream),
                        "khb_ct_ghost_from_faces")
+            if self._physical[n]:
+                # then the physical domain faces, over the ghost rows the exchange filled; they
+                # recompute B and U only past those faces
+                _lib.check(self.lib.khb_ct_boundaries(b.ctx, Pf.ref, Uf.ref, Bff.ref, b.stream), "khb_ct_boundaries")
         self._per_block(ghosts)
 
     def step(self, dt):
@@ -450,11 +474,13 @@ def level_dx(mesh):
     return [mesh.blocks[[b.level for b in mesh.blocks].index(L)].spec.dx for L in range(mesh.levels)]
 
 
-def curl_faces_levels(mesh, B0=(1.0, 0.5, 0.25), amp=0.05):
+def curl_faces_levels(mesh, B0=(1.0, 0.5, 0.25), amp=0.05, walls=False):
     """Whole-domain face arrays (3, t3, t2, t1) per level: B0 plus the discrete curl of
     A = amp (sin(2 pi x2) cos(2 pi x3), sin(2 pi x3) cos(2 pi x1), sin(2 pi x1) cos(2 pi x2)) sampled at
     each level's edges from integer corner indices, so that every level's field is divergence-free to
-    rounding and a coarse face equals the mean of the fine faces on it to rounding."""
+    rounding and a coarse face equals the mean of the fine faces on it to rounding.  walls (2D): no
+    normal field on the x1 and x2 domain faces, as reflecting faces require: A_3 = amp sin(2 pi x1)
+    sin(2 pi x2) and B0 along x3 only."""
     out = []
     for L in range(mesh.levels):
         t = mesh._zones_at(L)
@@ -466,7 +492,9 @@ def curl_faces_levels(mesh, B0=(1.0, 0.5, 0.25), amp=0.05):
         Z = np.zeros_like(X1)
         A1 = amp * np.sin(2 * np.pi * X2) * (np.cos(2 * np.pi * X3) if d3 else 1.0)      # at (i c, j f, k f)
         A2 = amp * (np.sin(2 * np.pi * X3) if d3 else Z) * np.cos(2 * np.pi * X1)       # at (i f, j c, k f)
-        A3 = amp * np.sin(2 * np.pi * X1) * np.cos(2 * np.pi * X2)                      # at (i f, j f, k c)
+        A3 = amp * np.sin(2 * np.pi * X1) * (np.sin if walls else np.cos)(2 * np.pi * X2)   # at (i f, j f, k c)
+        if walls:
+            B0 = (0.0, 0.0, B0[2])
         n3 = t[2]
         k1 = slice(0, n3) if d3 else slice(0, 1)
         F = np.zeros((3, n3, t[1], t[0]))

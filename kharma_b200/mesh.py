@@ -15,8 +15,12 @@ restated here as the algorithms it documents:
 Ghost zones are filled from primitives (then U = U(P) there), as KHARMA's simple and imex drivers
 exchange them (sync_prims, kharma_driver.cpp:109-110); every block has the same zone count,
 as Parthenon requires, and the fine blocks cover whole coarse blocks (2:1 in each active direction,
-neighbouring blocks at most one level apart).  Scope: hydro (5 variables), periodic domain, any
-number of levels.
+neighbouring blocks at most one level apart).  Scope: hydro blocks (5 variables) through the batch,
+MHD blocks with B_CT through kharma_b200/ctmesh.py; any number of levels; each direction periodic, or
+outflow/reflecting on the domain faces (a block on such a face keeps it; ghost entries stop at it and
+the block's boundary condition fills what lies beyond, after the exchange; refined blocks keep a
+coarse block between them and a physical domain face, since prolongation near it would read
+boundary values of the previous stage).
 
 `SMRMesh.tables()` gives the device tables khb_batch_set_mesh takes:
   ghost entries (int32 x 6): dst block, dst zone, op (0 copy, 1 restrict, 2 prolong), src block,
@@ -62,6 +66,15 @@ class SMRMesh:
         assert all(self.nb[d] == 1 or nx[d] > 1 for d in range(3))
         assert all(nx[d] >= 8 for d in range(self.ndim)), "SMR: at least 8 zones per active direction"
         self.ng = base.ng
+        # directions whose domain faces are physical (outflow or reflecting): blocks on those faces
+        # keep them, and no ghost entry reaches past them
+        self.periodic = tuple(d >= self.ndim or base.bc[2 * d] == "periodic" for d in range(3))
+        for d in range(self.ndim):
+            if not self.periodic[d]:
+                assert base.bc[2 * d] in ("outflow", "reflecting") and base.bc[2 * d + 1] in ("outflow", "reflecting"), \
+                    "SMR: domain faces periodic, outflow or reflecting"
+            else:
+                assert base.bc[2 * d + 1] == "periodic", "SMR: a periodic direction is periodic on both faces"
         lo = (base.x1min, base.x2min, base.x3min)
         hi = (base.x1max, base.x2max, base.x3max)
         self.lo, self.size = lo, tuple(hi[d] - lo[d] for d in range(3))
@@ -93,10 +106,22 @@ class SMRMesh:
         f = 2 ** level
         ext = [self.size[d] / (self.nb[d] * (f if d < self.ndim else 1)) for d in range(3)]
         x0 = [self.lo[d] + loc[d] * ext[d] for d in range(3)]
+        nl = [self.nb[d] * (f if d < self.ndim else 1) for d in range(3)]
+
+        def face_bc(face):
+            d, upper = face // 2, face % 2
+            if d >= self.ndim:
+                return "periodic"
+            at_edge = (loc[d] == nl[d] - 1) if upper else (loc[d] == 0)
+            return self.base.bc[face] if (at_edge and not self.periodic[d]) else "exchange"
         spec = dataclasses.replace(self.base, nx1=self.nx[0], nx2=self.nx[1], nx3=self.nx[2],
                                    x1min=x0[0], x1max=x0[0] + ext[0], x2min=x0[1], x2max=x0[1] + ext[1],
                                    x3min=x0[2], x3max=x0[2] + ext[2],
-                                   bc=tuple("exchange" if f // 2 < self.ndim else "periodic" for f in range(6)))
+                                   bc=tuple(face_bc(face) for face in range(6)))
+        # prolongation reads coarse zones up to one past the fine ghost zones: a coarse block between a
+        # refined block and a physical domain face keeps those reads inside the domain
+        assert level == 0 or all(x in ("exchange", "periodic") for x in spec.bc), \
+            "SMR: refined blocks keep a coarse block between them and a physical domain face"
         self.blocks.append(MeshBlock(level, loc, spec))
 
     # ------------------------------------------------------------------ topology
@@ -129,11 +154,20 @@ class SMRMesh:
             return tuple((g[d] - src_loc[d] * nx[d] + ng) if act[d] else np.zeros_like(g[d]) for d in (2, 1, 0))
 
         def owner(level, g):
-            # block id owning global zones g at `level` (-1: none), with the logical locations
+            # block id owning global zones g at `level` (-1: none, or outside a physical domain face),
+            # with the logical locations
             if level < 0 or level >= self.levels:
                 return np.full(len(g[0]), -1, dtype=np.int64), None
-            lo = [g[d] // nx[d] if act[d] else g[d] for d in range(3)]
-            return own[level][lo[2], lo[1], lo[0]], lo
+            t = self._zones_at(level)
+            ok = np.ones(len(g[0]), dtype=bool)
+            for d in range(3):
+                if act[d] and not self.periodic[d]:
+                    ok &= (g[d] >= 0) & (g[d] < t[d])
+            lo = [np.clip(g[d], 0, t[d] - 1) // nx[d] if act[d] else g[d] for d in range(3)]
+            return np.where(ok, own[level][lo[2], lo[1], lo[0]], -1), lo
+
+        def wrap(v, d, t):
+            return v % t if self.periodic[d] else v
 
         for b, blk in enumerate(self.blocks):
             n3, n2, n1 = blk.spec.shape
@@ -143,10 +177,17 @@ class SMRMesh:
             inside = np.zeros((n3, n2, n1), dtype=bool)
             inside[blk.spec.interior] = True
             K, J, I = K[~inside], J[~inside], I[~inside]
+            g = [wrap(blk.loc[0] * nx[0] + I - ng, 0, tot[0]),
+                 wrap(blk.loc[1] * nx[1] + J - ng, 1, tot[1]) if act[1] else np.zeros_like(I),
+                 wrap(blk.loc[2] * nx[2] + K - ng, 2, tot[2]) if act[2] else np.zeros_like(I)]
+            # ghost zones past a physical domain face are the block's own boundary condition's
+            keep = np.ones(len(I), dtype=bool)
+            for d in range(3):
+                if act[d] and not self.periodic[d]:
+                    keep &= (g[d] >= 0) & (g[d] < tot[d])
+            K, J, I = K[keep], J[keep], I[keep]
+            g = [x[keep] for x in g]
             dst = (K * n2 + J) * n1 + I
-            g = [(blk.loc[0] * nx[0] + I - ng) % tot[0],
-                 ((blk.loc[1] * nx[1] + J - ng) % tot[1]) if act[1] else np.zeros_like(I),
-                 ((blk.loc[2] * nx[2] + K - ng) % tot[2]) if act[2] else np.zeros_like(I)]
             src, loc = owner(L, g)
             same = src >= 0
             if same.any():
@@ -196,7 +237,9 @@ class SMRMesh:
                 t = [T1.ravel(), T2.ravel(), T3.ravel()]
                 for side in (0, 1):
                     across = list(t)
-                    across[d] = np.full_like(t[0], (blk.loc[d] * nx[d] + (nx[d] if side else -1)) % tot[d])
+                    across[d] = np.full_like(t[0], wrap(blk.loc[d] * nx[d] + (nx[d] if side else -1), d, tot[d]))
+                    if not self.periodic[d] and not (0 <= across[d][0] < tot[d]):
+                        continue                            # a physical domain face
                     if (owner(L, across)[0] >= 0).all():
                         continue                            # same level
                     if (owner(L - 1, [across[e] // 2 if act[e] else across[e] for e in range(3)])[0] >= 0).all():

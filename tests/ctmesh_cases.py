@@ -9,10 +9,14 @@ from kharma_b200.mesh import SMRMesh
 from kharma_b200.spec import BlockSpec
 
 
-def base(nd, nx=16, b_ct="gs05_c"):
+def base(nd, nx=16, b_ct="gs05_c", bc=("periodic",) * 6):
     return BlockSpec(nx1=nx, nx2=nx, nx3=nx if nd > 2 else 1, x1min=0., x1max=1., x2min=0., x2max=1., x3min=0.,
                      x3max=1., gam=4. / 3., nvar=8, recon="linear_mc", riemann="llf", cfl=0.8, dt_min=1e-4,
-                     b_ct=b_ct, driver="kharma")
+                     b_ct=b_ct, driver="kharma", bc=bc)
+
+
+WALLS = ("reflecting", "reflecting", "reflecting", "reflecting", "periodic", "periodic")
+OPEN = ("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic")
 
 
 REFINE_2D = [(1, 1, 0), (1, 2, 0), (2, 1, 0), (2, 2, 0)]
@@ -25,6 +29,8 @@ MESHES = {
                                                            (1, (4, 4, 0))]),
     # 2x2x2 root blocks of 8^3, one refined
     "3d_two_levels": lambda: SMRMesh(base(3, nx=8), (2, 2, 2), (8, 8, 8), refine=[(1, 1, 1)]),
+    # reflecting walls on the x1 and x2 domain faces, the central 2x2 of 4x4 roots refined
+    "2d_two_levels_walls": lambda: SMRMesh(base(2, bc=WALLS), (4, 4, 1), (16, 16, 1), refine=REFINE_2D),
 }
 
 

@@ -100,7 +100,21 @@ def test_face_table_covers_every_ghost_face_once(name):
             if a < mesh.ndim:
                 per *= nx[a] + (1 if a == d else 0)
         owned += per
-    assert len(face) + skipped == len(mesh.blocks) * (3 * N - owned)
+    if all(mesh.periodic):
+        assert len(face) + skipped == len(mesh.blocks) * (3 * N - owned)
+    else:
+        # no entry reaches past a physical domain face
+        G = ctmesh._Geo(mesh)
+        for e in face[:: max(1, len(face) // 2000)]:
+            blk = mesh.blocks[int(e[0])]
+            d = int(e[1])
+            k, r = divmod(int(e[2]), n1 * n2)
+            j, i = divmod(r, n1)
+            t = mesh._zones_at(blk.level)
+            for a, x in enumerate((i, j, k)):
+                if a < mesh.ndim and not mesh.periodic[a]:
+                    gg = blk.loc[a] * nx[a] + x - ng
+                    assert 0 <= gg <= (t[a] if a == d else t[a] - 1)
     assert np.all(np.diff(face[:, 7]) >= 0) and ends[-1] == len(face)
     assert face[:, 3].min() >= 0 and face[:, 3].max() <= 3
     assert np.all((face[:, 2] >= 0) & (face[:, 2] < N) & (face[:, 5] >= 0) & (face[:, 5] < N))
@@ -168,3 +182,11 @@ def test_emf_entries_pair_coinciding_edges(name):
             lo_c = (cblk.spec.x1min, cblk.spec.x2min, cblk.spec.x3min)[a] + (cl - ng) * cblk.spec.dx[a]
             lo_f = (fblk.spec.x1min, fblk.spec.x2min, fblk.spec.x3min)[a] + (fl - ng) * fblk.spec.dx[a]
             assert abs(((lo_c - lo_f) + 0.5) % 1.0 - 0.5) < 1e-12
+
+
+def test_refined_block_on_a_physical_face_is_rejected():
+    from ctmesh_cases import WALLS, base
+    from kharma_b200.mesh import SMRMesh
+    with pytest.raises(AssertionError, match="physical domain face"):
+        SMRMesh(base(2, bc=WALLS), (2, 2, 1), (16, 16, 1), refine=[(0, 0, 0)])
+    SMRMesh(base(2, bc=WALLS), (4, 4, 1), (16, 16, 1), refine=[(1, 1, 0)])

@@ -17,7 +17,7 @@ import pytest
 import torch
 
 from ctmesh_cases import MESHES, base, curl_faces_levels, cut, fluid_levels, level_dx, random_levels
-from kharma_b200 import ctmesh
+from kharma_b200 import _lib, ctmesh
 from kharma_b200.block import Block
 from kharma_b200.mesh import SMRMesh
 
@@ -33,7 +33,13 @@ _spec.loader.exec_module(smr_ref)
 def test_exchange_matches_restatement(name):
     mesh = MESHES[name]()
     P = cut(mesh, random_levels(mesh, 8, seed=3, positive=True))
-    Bf = cut(mesh, random_levels(mesh, 3, seed=4))
+    Fr = random_levels(mesh, 3, seed=4)
+    for F in Fr:
+        # reflecting domain faces carry no normal field
+        for d in range(mesh.ndim):
+            if not mesh.periodic[d]:
+                F[d][(slice(None),) * (2 - d) + (0,)] = 0.
+    Bf = cut(mesh, Fr)
     m = ctmesh.CTMesh(mesh, P, Bf)          # the constructor exchanges once
     # put the random fields back (set_prims rebuilt the zone B) and exchange again
     for b, p, f in zip(m.blocks, P, Bf):
@@ -51,6 +57,11 @@ def test_exchange_matches_restatement(name):
             x = mine[mine[:, 1] == d, 2]
             assert np.array_equal(got[d][x], exp_f[n][d].reshape(-1)[x]), f"block {n} faces {d}"
         mask, E = exp_c[n]
+        # the ghost zones the exchange fills (past a physical domain face: the block's own condition)
+        filled = np.zeros(mask.size, dtype=bool)
+        cell = m.tables["cell"]
+        filled[cell[cell[:, 0] == n, 1]] = True
+        mask = mask & filled.reshape(mask.shape)
         Pg = b.P.cpu().numpy()
         for v in range(5):
             assert np.array_equal(Pg[v][mask], E[v][mask]), f"block {n} var {v}"
@@ -240,3 +251,69 @@ def test_graph_step_equals_eager_step():
     torch.cuda.synchronize()
     for x, y in zip(a.blocks, b.blocks):
         assert torch.equal(x.P, y.P) and torch.equal(x.U, y.U) and torch.equal(x.Bf, y.Bf)
+
+
+@pytest.mark.parametrize("bc", ["walls", "open"])
+def test_one_level_with_physical_faces_steps_as_one_block(bc):
+    """2x2 blocks of one level with physical domain faces (reflecting walls, or outflow X1 with
+    reflecting X2): the blocks on the domain faces keep them, applied after the exchange over the
+    ghost rows it fills; the mesh steps bitwise as the single block with those faces."""
+    from ctmesh_cases import OPEN, WALLS
+    faces = WALLS if bc == "walls" else OPEN
+    mesh = SMRMesh(base(2, nx=16, bc=faces), (2, 2, 1), (16, 16, 1))
+    big = base(2, nx=32, bc=faces)
+    Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh, walls=True)
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    one = SMRMesh(big, (1, 1, 1), (32, 32, 1))
+    b = Block(big)
+    b.set_prims(cut(one, Pl)[0], faces=cut(one, Fl)[0])
+
+    def settle(blk):
+        # zone B from the faces as the domain conditions left them (the outflow condition rebuilds
+        # the domain face for zero divergence), then U = U(P): the same starting state in the blocks'
+        # interiors and in the ghost rows the exchange fills from them
+        _lib.check(blk.lib.khb_ct_utop(blk.ctx, blk.Bff.ref, blk.Pf.ref, blk.Uf.ref, blk.stream), "khb_ct_utop")
+        blk.ptou()
+    settle(b)
+    _lib.check(b.lib.khb_ct_boundaries(b.ctx, b.Pf.ref, b.Uf.ref, b.Bff.ref, b.stream), "khb_ct_boundaries")
+    for mb in m.blocks:
+        settle(mb)
+    torch.cuda.synchronize()
+    m.exchange(0)
+    for _ in range(3):
+        b.step(0.005)
+        m.step(0.005)
+    torch.cuda.synchronize()
+    ng = big.ng
+    for n, (blk, mb) in enumerate(zip(mesh.blocks, m.blocks)):
+        sl = (slice(0, 1), slice(ng + blk.loc[1] * 16, ng + blk.loc[1] * 16 + 16),
+              slice(ng + blk.loc[0] * 16, ng + blk.loc[0] * 16 + 16))
+        assert np.array_equal(mb.P.cpu().numpy()[(slice(None),) + blk.spec.interior],
+                              b.P.cpu().numpy()[(slice(None),) + sl]), f"block {n}"
+        for d in range(2):
+            own = list(blk.spec.interior)
+            hi = list(sl)
+            own[2 - d] = slice(own[2 - d].start, own[2 - d].stop + 1)
+            hi[2 - d] = slice(hi[2 - d].start, hi[2 - d].stop + 1)
+            assert np.array_equal(mb.Bf[d].cpu().numpy()[tuple(own)], b.Bf[d].cpu().numpy()[tuple(hi)]), f"block {n} face {d}"
+
+
+def test_refined_mesh_with_walls_keeps_divb_and_mass():
+    """Reflecting walls on the x1 and x2 domain faces, the central quarter refined: after 10 steps
+    every block keeps its face divergence at round-off in the interior and in the exchanged ghost
+    layers away from the walls, and the mesh conserves mass to rounding (no flux crosses a wall)."""
+    mesh = MESHES["2d_two_levels_walls"]()
+    Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh, walls=True)
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    m0 = m.conserved_totals()
+    dt = 0.4 / 128
+    for _ in range(10):
+        m.step(dt)
+    torch.cuda.synchronize()
+    m1 = m.conserved_totals()
+    scale = max(float(np.abs(b.Bf.cpu().numpy()).max()) for b in m.blocks)
+    print("walls: divB interior", m.max_divb(), "mass change", (m1[0] - m0[0]) / m0[0],
+          "interface mismatch", interface_mismatch(m))
+    assert m.max_divb() * (1.0 / 128) < 1e-13 * scale
+    assert abs(m1[0] - m0[0]) < 1e-13 * abs(m0[0])
+    assert interface_mismatch(m) < 1e-13 * scale

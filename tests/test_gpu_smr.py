@@ -1,5 +1,5 @@
 """Static mesh refinement through the batch (khb_batch_set_mesh): two- and three-level hydro meshes on
-a periodic box.
+a periodic box, and one-level meshes with outflow or reflecting domain faces.
 
 * The ghost zones the library fills after an exchange equal, bitwise, the oracle-side restatement
   built from whole-domain arrays (oracle/smr_ref.py).
@@ -9,6 +9,7 @@ a periodic box.
 * A uniform state stays exactly uniform across the refinement boundary.
 * An entropy wave advected across the refined patch: the mesh's error lies between those of the
   uniform coarse and uniform fine meshes.
+* 2x2 blocks with physical domain faces step bitwise as one block of the whole domain.
 """
 import dataclasses
 import importlib.util
@@ -158,3 +159,38 @@ def test_three_levels_conserve(nd):
     assert refined[0] <= 1e-13
     _, u0, u1 = run(mesh, False, steps=6)
     assert np.abs(u1[0] - u0[0]) > 1e-9 * abs(u0[0])
+
+
+@pytest.mark.parametrize("faces", [("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"),
+                                   ("reflecting",) * 4 + ("periodic",) * 2])
+def test_one_level_with_physical_faces_steps_as_one_block(faces):
+    """2x2 blocks of one level whose outer faces are the domain's outflow or reflecting faces: each
+    block on a domain face applies it after the exchange, over the ghost rows the exchange filled;
+    the mesh steps bitwise as one block of the whole domain with those faces."""
+    from kharma_b200.batch import Batch
+    spec = dataclasses.replace(base(2), bc=faces)
+    mesh = SMRMesh(spec, (2, 2, 1), (16, 16, 1))
+    big = dataclasses.replace(spec, nx1=32, nx2=32)
+    ng = big.ng
+    Pbig = problems.entropy_wave(big, amp=0.1)
+    J, I = np.meshgrid(np.arange(Pbig.shape[2]), np.arange(Pbig.shape[3]), indexing="ij")
+    Pbig[2] += 0.05 * np.sin(2 * np.pi * (J - ng + 0.5) / 32)
+    Pbig[3] += 0.05 * np.cos(2 * np.pi * (I - ng + 0.5) / 32)
+
+    def init(s):
+        lx, ly = round(s.x1min * 2), round(s.x2min * 2)
+        return Pbig[:, :, ly * 16:ly * 16 + 16 + 2 * ng, lx * 16:lx * 16 + 16 + 2 * ng]
+    b = smr_batch(mesh, init)
+    one = Batch([big], init=None)
+    with torch.cuda.stream(one.torch_stream):
+        one.blocks[0].set_prims(Pbig)
+    dt = 0.2 / 32
+    for _ in range(5):
+        b.step(dt)
+        one.step(dt)
+    torch.cuda.synchronize()
+    Pone = one.blocks[0].P.cpu().numpy()
+    for n, (blk, mb) in enumerate(zip(mesh.blocks, b.blocks)):
+        sl = (slice(None), slice(0, 1), slice(ng + blk.loc[1] * 16, ng + blk.loc[1] * 16 + 16),
+              slice(ng + blk.loc[0] * 16, ng + blk.loc[0] * 16 + 16))
+        assert np.array_equal(mb.P.cpu().numpy()[(slice(None),) + blk.spec.interior], Pone[sl]), f"block {n}"
