@@ -558,8 +558,20 @@ int khb_batch_set_mesh(khb_batch* batch, const int32_t* ghost, int64_t n_ghost, 
                        const int32_t* flux, int64_t n_flux);
 
 /* Fill every block's ghost zones of the state (P, U) from the mesh (e.g. after initial data), then
- * the physical domain faces of the blocks on them. */
+ * the physical domain faces of the blocks on them.  With KHB_SYNC_CONSERVED: U and P (the seeds) by
+ * the entries, then the inversion, floors and U = U(P) in those ghost zones. */
 int khb_batch_mesh_exchange(khb_batch* batch, void* stream);
+
+/* What a mesh's exchange moves (kharma_driver.cpp:109-118: sync_prims = driver_type != kharma).
+ * KHB_SYNC_PRIMS (the simple and ImEx drivers, the default): after each stage, the primitives by
+ * the entries, then U = U(P) there.  KHB_SYNC_CONSERVED (the kharma driver): between the update and
+ * the inversion of each stage, the updated conserved variables and, as the inversion's seeds, the
+ * stage's input primitives (GRMHD sync_utop_seed, grmhd.cpp:159-165), both by the entries; then the
+ * ghost zones are inverted, floored and given U = U(P) as the interior is (MeshUtoP and
+ * MeshApplyFloors over the entire block, kharma_step.cpp:233-236).  The conserved exchange runs the
+ * plain launch plan (the fused one inverts in the pass that updates). */
+enum { KHB_SYNC_PRIMS = 0, KHB_SYNC_CONSERVED = 1 };
+int khb_batch_set_mesh_sync(khb_batch* batch, int mode);
 
 /* ---------------------------------------------------------------------------------------------
  * Extended MHD and the implicit solve (emhd/, implicit/)

@@ -195,6 +195,7 @@ SIGNATURES = {
     "khb_batch_get_plan": (_I, [_P, C.POINTER(C.c_int32)]),
     "khb_batch_set_mesh": (_I, [_P, _P, C.c_int64, C.c_int64, _P, C.c_int64]),
     "khb_batch_mesh_exchange": (_I, [_P, _P]),
+    "khb_batch_set_mesh_sync": (_I, [_P, C.c_int]),
 }
 
 _lib = None

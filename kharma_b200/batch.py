@@ -166,6 +166,12 @@ class Batch:
         _lib.check(self.lib.khb_batch_set_mesh(self.h, ghost.ctypes.data_as(C.c_void_p), len(ghost), int(n_ghost_first),
                                                flux.ctypes.data_as(C.c_void_p), len(flux)), "khb_batch_set_mesh")
 
+    def set_mesh_sync(self, conserved):
+        """What the mesh's exchange moves: primitives (the simple and ImEx drivers), or conserved
+        variables with the primitives as inversion seeds, the ghost zones then inverted (the kharma
+        driver; kharma_driver.cpp:109-118)."""
+        _lib.check(self.lib.khb_batch_set_mesh_sync(self.h, 1 if conserved else 0), "khb_batch_set_mesh_sync")
+
     def mesh_exchange(self):
         """Fill the ghost zones of every block's state from the mesh."""
         _lib.check(self.lib.khb_batch_mesh_exchange(self.h, self.stream), "khb_batch_mesh_exchange")

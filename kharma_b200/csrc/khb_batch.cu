@@ -50,6 +50,8 @@ struct khb_batch {
     int* mesh_flux = nullptr;
     long long n_ghost = 0, n_ghost_first = 0, n_flux = 0;
     std::vector<long long> ghost_phase_end;        // ends of the prolongation phases (one per level)
+    // exchange of conserved variables with seeds (the kharma driver), else of primitives
+    bool sync_cons = false;
     // CUDA graph of one step
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -71,6 +73,25 @@ void enqueue_mesh_ghost(khb_batch* b, int stage, cudaStream_t st)
         begin = end;
     }
     b->launches += 1 + (int64_t)b->ghost_phase_end.size();
+}
+
+// The kharma driver's exchange in the same phases (conserved variables and inversion seeds), then
+// the inversion, floors and U = U(P) of every ghost zone it filled.  Stage s (0, 1): between the
+// update and the cell half of the zone pass; s = -1: outside a stage, on the blocks' state.
+template <typename FT>
+void enqueue_mesh_cons(khb_batch* b, int s, cudaStream_t st)
+{
+    const int seed_sel = (s < 0) ? 0 : s, u_sel = (s < 0) ? 1 : s;
+    LaunchCommon::mesh_ghost_cons(b->nv, b->fix, b->mesh_ghost, 0, b->n_ghost_first, seed_sel, u_sel, st);
+    long long begin = b->n_ghost_first;
+    for (long long end : b->ghost_phase_end) {
+        LaunchCommon::mesh_ghost_cons(b->nv, b->fix, b->mesh_ghost, begin, end, seed_sel, u_sel, st);
+        begin = end;
+    }
+    const bool kast = b->ctx[0]->ph.inverter == KHB_INVERTER_KASTAUN;
+    Launch<FT>::mesh_ghost_cell(b->nv, kast, (const BatchBlock<FT>*)b->desc, b->mesh_ghost, b->n_ghost,
+                                (s < 0) ? 1 : s, s < 0, st);
+    b->launches += 2 + (int64_t)b->ghost_phase_end.size();
 }
 
 #define KHB_BCUDA(call)                                                                  \
@@ -290,7 +311,8 @@ int enqueue_stage_fused(khb_batch* b, int s, cudaStream_t st)
 template <typename FT>
 int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
 {
-    if (b->plan == 1) return enqueue_stage_fused<FT>(b, s, st);
+    // the fused plan inverts in the pass that updates: the kharma driver's exchange needs the plain one
+    if (b->plan == 1 && !(b->sync_cons && b->n_ghost)) return enqueue_stage_fused<FT>(b, s, st);
     const int stage = s + 1;
     const BatchBlock<FT>* desc = (const BatchBlock<FT>*)b->desc;
     LaunchCommon::batch_reset(b->counts, b->nb, s == 1 ? b->word : nullptr, st);
@@ -313,6 +335,13 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
     Launch<FT>::batch_zone(b->nv, M_UPDATE, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage, 0, kRkBeta[s],
                            b->dt_dev, st);
     KHB_BLAUNCHED(b, 1);
+    const bool cons = b->sync_cons && b->n_ghost;
+    if (cons) {
+        // the kharma driver: the updated conserved state and the seeds cross before any inversion
+        // (kharma_step.cpp:209-236), and the ghost zones are inverted like the interior
+        enqueue_mesh_cons<FT>(b, s, st);
+        KHB_BLAUNCHED(b, 0);
+    }
     const int cell = M_ZONE_CELL | ((b->ctx[0]->ph.inverter == KHB_INVERTER_KASTAUN) ? M_KASTAUN : 0);
     Launch<FT>::batch_zone(b->nv, cell, desc, b->tiles[3], b->ntiles[3], b->grid[3], stage,
                            s == 1 ? M_DT : 0, kRkBeta[s], b->dt_dev, st);
@@ -321,7 +350,7 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
     KHB_BLAUNCHED(b, 1);
     // the mesh's exchange, then the physical faces over the ghost rows it filled (the reference's
     // sync before its domain conditions, kharma_step.cpp:209-249)
-    if (b->n_ghost) {
+    if (b->n_ghost && !cons) {
         enqueue_mesh_ghost(b, stage, st);
         KHB_BLAUNCHED(b, 0);
     }
@@ -536,11 +565,26 @@ int khb_batch_mesh_exchange(khb_batch* b, void* stream)
     KHB_RANGE("khb_batch_mesh_exchange");
     if (!b) return set_error(KHB_ERR_ARG, "khb_batch_mesh_exchange: NULL batch");
     if (b->n_ghost) {
-        enqueue_mesh_ghost(b, 2, S(stream));
+        if (b->sync_cons) {
+            if (b->fp32) enqueue_mesh_cons<float>(b, -1, S(stream));
+            else enqueue_mesh_cons<double>(b, -1, S(stream));
+        } else {
+            enqueue_mesh_ghost(b, 2, S(stream));
+        }
         KHB_BCUDA(cudaGetLastError());
         int rc;
         if ((rc = enqueue_bounds(b, 1, S(stream)))) return rc;
     }
+    return KHB_OK;
+}
+
+int khb_batch_set_mesh_sync(khb_batch* b, int mode)
+{
+    if (!b) return set_error(KHB_ERR_ARG, "khb_batch_set_mesh_sync: NULL batch");
+    if (mode != KHB_SYNC_PRIMS && mode != KHB_SYNC_CONSERVED)
+        return set_error(KHB_ERR_ARG, "khb_batch_set_mesh_sync: mode is KHB_SYNC_PRIMS or KHB_SYNC_CONSERVED");
+    if (b->sync_cons != (mode == KHB_SYNC_CONSERVED)) drop_graph(b);      // a captured step runs the other exchange
+    b->sync_cons = mode == KHB_SYNC_CONSERVED;
     return KHB_OK;
 }
 

@@ -1310,6 +1310,30 @@ k_batch_zone(const BatchBlock<FT>* __restrict__ blocks, const int* __restrict__ 
     }
 }
 
+// The cell half of the zone pass (inversion from the seed, floors, U = U(P)) on the ghost zones of a
+// mesh's exchange entries, after the kharma driver's exchange: MeshUtoP and MeshApplyFloors over the
+// entire block (kharma_step.cpp:233-236).  Stage s's arguments of the destination block, its updated
+// U as the state to invert; standalone (an exchange outside a stage): the seeds are the block's
+// state primitives, which the zone also writes.  No timestep and no failed-zone list: FixUtoP works
+// on the interior.
+template <int NV, typename FT, int MODE>
+__global__ void __launch_bounds__(128) k_mesh_ghost_cell(const BatchBlock<FT>* __restrict__ blocks,
+                                                         const int* __restrict__ table, long long n, int s,
+                                                         int standalone)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int* t = table + 6 * e;
+    const BatchBlock<FT>& B = blocks[__ldg(t)];
+    ZoneArgs<FT> a = B.za[s];
+    a.Us = a.Uout;
+    if (standalone) a.Ps = B.za[0].Ps;
+    a.mode = 0;
+    int k, j, i;
+    zone_kji(B.d, __ldg(t + 1), k, j, i);
+    zone_body<NV, FT, MODE>(B.d, B.g, B.ph, a, i, j, k);
+}
+
 // The fused plan's first launch of a stage (Launch<FT>::batch_flux_all): the faces of all directions
 // of every block and the ghost-shell copies of blocks with exchange faces, one table of 128-wide
 // tiles; CTA 0 first resets the failed-zone counters and the timestep minimum the zone pass fills.
@@ -1401,6 +1425,25 @@ __device__ __forceinline__ double minmod2(double a, double b)
 {
     return (a * b > 0.) ? ((fabs(a) < fabs(b)) ? a : b) : 0.;
 }
+// One variable of a ghost entry: op 0 copy, 1 restriction, 2 prolongation (q: the source array)
+__device__ __forceinline__ double mesh_op(const double* q, long long cs, int op, int aux, const Dims& ds)
+{
+    if (op == 0) return q[cs];
+    if (op == 1) {
+        double r = (q[cs] + q[cs + 1]);
+        if (ds.ndim > 1) r = r + (q[cs + ds.sj] + q[cs + ds.sj + 1]);
+        if (ds.ndim > 2) r = r + ((q[cs + ds.sk] + q[cs + ds.sk + 1]) + (q[cs + ds.sk + ds.sj] + q[cs + ds.sk + ds.sj + 1]));
+        return r * ((ds.ndim > 2) ? 0.125 : (ds.ndim > 1) ? 0.25 : 0.5);
+    }
+    const double uc = q[cs];
+    double v = uc;
+    const long long st[3] = {1, ds.sj, ds.sk};
+    for (int d = 0; d < ds.ndim; ++d) {
+        const double sl = minmod2(uc - q[cs - st[d]], q[cs + st[d]] - uc);
+        v += ((aux >> d) & 1) ? 0.25 * sl : -0.25 * sl;
+    }
+    return v;
+}
 template <int NV>
 __global__ void __launch_bounds__(128) k_mesh_ghost(const FixupBlock* __restrict__ blocks, const int* __restrict__ table,
                                                     long long begin, long long end, int stage)
@@ -1414,29 +1457,9 @@ __global__ void __launch_bounds__(128) k_mesh_ghost(const FixupBlock* __restrict
     const long long cd = __ldg(t + 1), cs = __ldg(t + 4);
     const int op = __ldg(t + 2), aux = __ldg(t + 5);
     const khb_fields& Ps = S.P[s];
-    const Dims& ds = S.d;
     double P[NV];
 #pragma unroll
-    for (int p = 0; p < NV; ++p) {
-        const double* q = Ps.v[p];
-        if (op == 0) {
-            P[p] = q[cs];
-        } else if (op == 1) {
-            double r = (q[cs] + q[cs + 1]);
-            if (ds.ndim > 1) r = r + (q[cs + ds.sj] + q[cs + ds.sj + 1]);
-            if (ds.ndim > 2) r = r + ((q[cs + ds.sk] + q[cs + ds.sk + 1]) + (q[cs + ds.sk + ds.sj] + q[cs + ds.sk + ds.sj + 1]));
-            P[p] = r * ((ds.ndim > 2) ? 0.125 : (ds.ndim > 1) ? 0.25 : 0.5);
-        } else {
-            const double uc = q[cs];
-            double v = uc;
-            const long long st[3] = {1, ds.sj, ds.sk};
-            for (int d = 0; d < ds.ndim; ++d) {
-                const double sl = minmod2(uc - q[cs - st[d]], q[cs + st[d]] - uc);
-                v += ((aux >> d) & 1) ? 0.25 * sl : -0.25 * sl;
-            }
-            P[p] = v;
-        }
-    }
+    for (int p = 0; p < NV; ++p) P[p] = mesh_op(Ps.v[p], cs, op, aux, S.d);
     const khb_fields& Pd = D.P[s];
     const khb_fields& Ud = D.U[s];
 #pragma unroll
@@ -1449,6 +1472,36 @@ __global__ void __launch_bounds__(128) k_mesh_ghost(const FixupBlock* __restrict
     p_to_u_zone<NV>(G, D.ph.gam, P, U);
 #pragma unroll
     for (int p = 0; p < NV; ++p) Ud.v[p][cd] = U[p];
+}
+
+// The kharma driver's exchange (sync_prims false, kharma_driver.cpp:109-118): the conserved variables
+// by the entry's operator, and the fluid primitives too as the seed of the ghost zone's inversion
+// (GRMHD sync_utop_seed, grmhd.cpp:159-165).  Runs between the update and the inversion: the
+// updated U of stage s sits in U[u_sel], the seeds (the stage's input primitives) in Pin[seed_sel];
+// the ghost zone's values go to the same arrays, where later phases and the inversion read them.
+template <int NV>
+__global__ void __launch_bounds__(128) k_mesh_ghost_cons(const FixupBlock* __restrict__ blocks,
+                                                         const int* __restrict__ table, long long begin,
+                                                         long long end, int seed_sel, int u_sel)
+{
+    const long long e = begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= end) return;
+    const int* t = table + 6 * e;
+    const FixupBlock& D = blocks[__ldg(t)];
+    const FixupBlock& S = blocks[__ldg(t + 3)];
+    const long long cd = __ldg(t + 1), cs = __ldg(t + 4);
+    const int op = __ldg(t + 2), aux = __ldg(t + 5);
+    double P[NV], U[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        P[p] = mesh_op(S.Pin[seed_sel].v[p], cs, op, aux, S.d);
+        U[p] = mesh_op(S.U[u_sel].v[p], cs, op, aux, S.d);
+    }
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        D.Pin[seed_sel].v[p][cd] = P[p];
+        D.U[u_sel].v[p][cd] = U[p];
+    }
 }
 #endif
 
@@ -1752,6 +1805,22 @@ void Launch<FT>::mesh_flux(int nv, const BatchBlock<FT>* blocks, const int* tabl
     if (n > 0) k_mesh_flux<FT><<<blocks_for(n, 128), 128, 0, st>>>(blocks, table, n, nv);
 }
 
+template <typename FT>
+void Launch<FT>::mesh_ghost_cell(int nv, bool kastaun, const BatchBlock<FT>* blocks, const int* table, long long n,
+                                 int s, int standalone, cudaStream_t st)
+{
+    if (n <= 0) return;
+    constexpr int C = M_UTOP | M_FLOORS | M_PTOU;
+    const unsigned nb = blocks_for(n, 128);
+    if (nv == 8) {
+        if (kastaun) k_mesh_ghost_cell<8, FT, C | M_KASTAUN><<<nb, 128, 0, st>>>(blocks, table, n, s, standalone);
+        else k_mesh_ghost_cell<8, FT, C><<<nb, 128, 0, st>>>(blocks, table, n, s, standalone);
+    } else {
+        if (kastaun) k_mesh_ghost_cell<5, FT, C | M_KASTAUN><<<nb, 128, 0, st>>>(blocks, table, n, s, standalone);
+        else k_mesh_ghost_cell<5, FT, C><<<nb, 128, 0, st>>>(blocks, table, n, s, standalone);
+    }
+}
+
 #ifdef KHB_COMMON_KERNELS
 void LaunchCommon::mesh_ghost(int nv, const FixupBlock* blocks, const int* table, long long begin, long long end,
                               int stage, cudaStream_t st)
@@ -1759,6 +1828,14 @@ void LaunchCommon::mesh_ghost(int nv, const FixupBlock* blocks, const int* table
     if (end <= begin) return;
     if (nv == 8) k_mesh_ghost<8><<<blocks_for(end - begin, 128), 128, 0, st>>>(blocks, table, begin, end, stage);
     else k_mesh_ghost<5><<<blocks_for(end - begin, 128), 128, 0, st>>>(blocks, table, begin, end, stage);
+}
+
+void LaunchCommon::mesh_ghost_cons(int nv, const FixupBlock* blocks, const int* table, long long begin,
+                                   long long end, int seed_sel, int u_sel, cudaStream_t st)
+{
+    if (end <= begin) return;
+    if (nv == 8) k_mesh_ghost_cons<8><<<blocks_for(end - begin, 128), 128, 0, st>>>(blocks, table, begin, end, seed_sel, u_sel);
+    else k_mesh_ghost_cons<5><<<blocks_for(end - begin, 128), 128, 0, st>>>(blocks, table, begin, end, seed_sel, u_sel);
 }
 
 void LaunchCommon::batch_fixup(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st)

@@ -205,6 +205,8 @@ struct Launch {
                               cudaStream_t st);
     // SMR flux correction over the entries of a mesh's flux table (6 ints each)
     static void mesh_flux(int nv, const BatchBlock<FT>* blocks, const int* table, long long n, cudaStream_t st);
+    static void mesh_ghost_cell(int nv, bool kastaun, const BatchBlock<FT>* blocks, const int* table, long long n,
+                                int s, int standalone, cudaStream_t st);
 };
 
 // Zone-local FP64 work shared by both forms (compiled with the FP64 unit)
@@ -234,6 +236,10 @@ struct LaunchCommon {
     // SMR ghost zones of stage `stage`'s outputs from entries [begin, end) of a mesh's ghost table
     static void mesh_ghost(int nv, const FixupBlock* blocks, const int* table, long long begin, long long end,
                            int stage, cudaStream_t st);
+    // The same entries on conserved variables (U[u_sel]) and inversion seeds (Pin[seed_sel]), the
+    // kharma driver's exchange; Launch<FT>::mesh_ghost_cell then inverts those ghost zones
+    static void mesh_ghost_cons(int nv, const FixupBlock* blocks, const int* table, long long begin, long long end,
+                                int seed_sel, int u_sel, cudaStream_t st);
     static void batch_reset(int* const* counts, int nblocks, unsigned long long* word, cudaStream_t st);
     // Per-stage reset of one block's failed-zone counter (and of the timestep minimum when word)
     static void stage_reset(int* count, unsigned long long* word, cudaStream_t st);

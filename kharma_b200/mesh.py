@@ -13,7 +13,10 @@ restated here as the algorithms it documents:
   * flux correction: a coarse face on a fine-coarse boundary takes the average of the 2^(ndim-1)
     fine fluxes through it before the update, so the mesh conserves what the uniform scheme does.
 Ghost zones are filled from primitives (then U = U(P) there), as KHARMA's simple and imex drivers
-exchange them (sync_prims, kharma_driver.cpp:109-110); every block has the same zone count,
+exchange them (sync_prims, kharma_driver.cpp:109-110), or, for blocks of the kharma driver, from
+the updated conserved variables with the primitives as the inversion's seeds, the ghost zones then
+inverted, floored and given U = U(P) like the interior (kharma_step.cpp:209-236); every block has the
+same zone count,
 as Parthenon requires, and the fine blocks cover whole coarse blocks (2:1 in each active direction,
 neighbouring blocks at most one level apart).  Scope: hydro blocks (5 variables) through the batch,
 MHD blocks with B_CT through kharma_b200/ctmesh.py; any number of levels; each direction periodic, or
@@ -281,10 +284,11 @@ class SMRMesh:
         return len(self.blocks) * self.nx[0] * self.nx[1] * self.nx[2]
 
 
-def smr_batch(mesh: SMRMesh, init, flux_correction=True, device="cuda"):
+def smr_batch(mesh: SMRMesh, init, flux_correction=True, device="cuda", conserved=None):
     """A Batch of the mesh's blocks with initial primitives init(spec) -> (5, n3, n2, n1) per block,
     the mesh tables set and the ghost zones exchanged.  flux_correction=False leaves the coarse
-    faces on fine-coarse boundaries uncorrected (for tests of conservation)."""
+    faces on fine-coarse boundaries uncorrected (for tests of conservation).  conserved: the
+    kharma driver's exchange of conserved variables (default: when the blocks' driver is kharma)."""
     import torch
     from .batch import Batch
     b = Batch([blk.spec for blk in mesh.blocks], init=None, device=device)
@@ -295,7 +299,10 @@ def smr_batch(mesh: SMRMesh, init, flux_correction=True, device="cuda"):
     if not flux_correction:
         flux = flux[:0]
     b.set_mesh(ghost, n_first, flux)
+    # the initial ghost zones from the initial primitives; the steps' exchanges as the driver's
+    b.set_mesh_sync(False)
     b.mesh_exchange()
+    b.set_mesh_sync(mesh.base.driver == "kharma" if conserved is None else conserved)
     return b
 
 

@@ -10,6 +10,9 @@ a periodic box, and one-level meshes with outflow or reflecting domain faces.
 * An entropy wave advected across the refined patch: the mesh's error lies between those of the
   uniform coarse and uniform fine meshes.
 * 2x2 blocks with physical domain faces step bitwise as one block of the whole domain.
+* The kharma driver's exchange (conserved variables and inversion seeds, the ghost zones inverted
+  like the interior): ghost zones equal the oracle's inversion of the restated conserved state from
+  the restated seed; one level steps bitwise as one block; conservation and uniformity as above.
 """
 import dataclasses
 import importlib.util
@@ -61,8 +64,9 @@ def test_exchange_matches_restatement(nd):
         assert np.array_equal(got, want), (n, mesh.blocks[n].level, np.abs(got - want).max())
 
 
-def run(mesh, flux_correction, steps=10, init=None):
-    b = smr_batch(mesh, init or (lambda s: random_smooth(s, 3)), flux_correction=flux_correction)
+def run(mesh, flux_correction, steps=10, init=None, conserved=None):
+    b = smr_batch(mesh, init or (lambda s: random_smooth(s, 3)), flux_correction=flux_correction,
+                  conserved=conserved)
     t0 = conserved_totals(mesh, b)
     dt = 0.2 * min(blk.spec.dx[0] for blk in mesh.blocks)
     for _ in range(steps):
@@ -72,23 +76,24 @@ def run(mesh, flux_correction, steps=10, init=None):
     return b, t0, conserved_totals(mesh, b)
 
 
-@pytest.mark.parametrize("nd", [2, 3])
-def test_flux_correction_conserves(nd):
-    _, r0, r1 = run(mesh_of(nd, refine=()), True)
+@pytest.mark.parametrize("nd,conserved", [(2, False), (3, False), (2, True), (3, True)])
+def test_flux_correction_conserves(nd, conserved):
+    _, r0, r1 = run(mesh_of(nd, refine=()), True, conserved=conserved)
     mesh = mesh_of(nd)
-    _, t0, t1 = run(mesh, True)
+    _, t0, t1 = run(mesh, True, conserved=conserved)
     scale = np.abs(t0).max()
     uniform = np.abs(r1 - r0) / scale
     refined = np.abs(t1 - t0) / scale
     print("relative change of the conserved totals, unrefined:", uniform, "refined:", refined)
     assert refined[0] <= 1e-13
     assert np.all(refined <= 10 * uniform + 1e-13)
-    _, u0, u1 = run(mesh, False)
+    _, u0, u1 = run(mesh, False, conserved=conserved)
     print("refined without flux correction:", np.abs(u1 - u0) / scale)
     assert np.abs(u1[0] - u0[0]) > 1e-9 * abs(u0[0])
 
 
-def test_uniform_state_stays_uniform():
+@pytest.mark.parametrize("conserved", [False, True])
+def test_uniform_state_stays_uniform(conserved):
     mesh = mesh_of(2)
 
     def uniform(s):
@@ -96,7 +101,7 @@ def test_uniform_state_stays_uniform():
         P[0], P[1], P[2], P[3] = 1.0, 2.0, 0.2, -0.1
         return P
 
-    b, _, _ = run(mesh, True, steps=5, init=uniform)
+    b, _, _ = run(mesh, True, steps=5, init=uniform, conserved=conserved)
     for blk in b.blocks:
         P = blk.P.cpu().numpy()
         ref = uniform(blk.spec)
@@ -161,14 +166,18 @@ def test_three_levels_conserve(nd):
     assert np.abs(u1[0] - u0[0]) > 1e-9 * abs(u0[0])
 
 
-@pytest.mark.parametrize("faces", [("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"),
+@pytest.mark.parametrize("driver", ["simple", "kharma"])
+@pytest.mark.parametrize("faces", [("periodic",) * 6,
+                                   ("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"),
                                    ("reflecting",) * 4 + ("periodic",) * 2])
-def test_one_level_with_physical_faces_steps_as_one_block(faces):
-    """2x2 blocks of one level whose outer faces are the domain's outflow or reflecting faces: each
-    block on a domain face applies it after the exchange, over the ghost rows the exchange filled;
-    the mesh steps bitwise as one block of the whole domain with those faces."""
+def test_one_level_steps_as_one_block(faces, driver):
+    """2x2 blocks of one level, the domain periodic or with outflow or reflecting faces: each block on
+    a domain face applies it after the exchange, over the ghost rows the exchange filled; the mesh
+    steps bitwise as one block of the whole domain with those faces.  With the kharma driver the
+    exchange moves the updated conserved variables and the seeds, and each ghost zone's inversion
+    repeats its source zone's."""
     from kharma_b200.batch import Batch
-    spec = dataclasses.replace(base(2), bc=faces)
+    spec = dataclasses.replace(base(2), bc=faces, driver=driver)
     mesh = SMRMesh(spec, (2, 2, 1), (16, 16, 1))
     big = dataclasses.replace(spec, nx1=32, nx2=32)
     ng = big.ng
@@ -194,3 +203,43 @@ def test_one_level_with_physical_faces_steps_as_one_block(faces):
         sl = (slice(None), slice(0, 1), slice(ng + blk.loc[1] * 16, ng + blk.loc[1] * 16 + 16),
               slice(ng + blk.loc[0] * 16, ng + blk.loc[0] * 16 + 16))
         assert np.array_equal(mb.P.cpu().numpy()[(slice(None),) + blk.spec.interior], Pone[sl]), f"block {n}"
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_conserved_exchange_matches_restatement(oracle_mod, nd):
+    """The kharma driver's exchange outside a stage (khb_batch_mesh_exchange with KHB_SYNC_CONSERVED):
+    on block states whose U is not U(P), so that every inversion moves its seed, each ghost zone's
+    primitives equal the oracle's inversion of the restated conserved state (copy, restriction or
+    prolongation of the blocks' U) from the restated seed, with no failure, and its U is U(P)."""
+    mesh = mesh_of(nd)
+    seeds = iter(range(1000))
+    b = smr_batch(mesh, lambda s: random_smooth(s, next(seeds)), conserved=True)
+    torch.cuda.synchronize()
+    rng = np.random.Generator(np.random.PCG64(11))
+    P, U = [], []
+    for blk in b.blocks:
+        u = blk.U.cpu().numpy()
+        u = u * (1 + 1e-3 * rng.standard_normal(u.shape))
+        blk.U.copy_(torch.as_tensor(u))
+        P.append(blk.P.cpu().numpy())
+        U.append(u)
+    torch.cuda.synchronize()
+    b.mesh_exchange()
+    torch.cuda.synchronize()
+    o = oracle_mod.Oracle(mesh.blocks[0].spec)
+    worst, checked = 0.0, 0
+    for n, ((mask, Eu), (_, Ep), blk) in enumerate(zip(smr_ref.expected_ghosts(mesh, U),
+                                                       smr_ref.expected_ghosts(mesh, P), b.blocks)):
+        Pg, Ug = blk.P.cpu().numpy(), blk.U.cpu().numpy()
+        pf = blk.pflag.cpu().numpy()
+        for k, j, i in np.argwhere(mask):
+            uz = np.ascontiguousarray(Eu[:, k, j, i])
+            pz = np.ascontiguousarray(Ep[:, k, j, i])
+            flag = o.lib.orc_utop_cell(o.h, int(j), int(i), oracle_mod._ptr(uz), oracle_mod._ptr(pz))
+            assert flag == 0 and pf[k, j, i] == 0
+            worst = max(worst, float(np.max(np.abs(Pg[:, k, j, i] - pz) / np.maximum(np.abs(pz), 1.0))))
+            checked += 1
+        Uo = o.ptou(Pg)
+        assert np.array_equal(Ug[:, mask], Uo[:, mask]), n
+    print("conserved exchange:", checked, "ghost zones, worst relative P difference", worst)
+    assert checked > 0 and worst <= 1e-12
