@@ -429,6 +429,24 @@ int khb_ctmesh_destroy(khb_ctmesh* mesh);
 int khb_ctmesh_correct(khb_ctmesh* mesh, void* stream);
 int khb_ctmesh_exchange(khb_ctmesh* mesh, const khb_fields* P, const khb_fields* Bf, void* stream);
 
+/* The kharma driver's stage on a B_CT mesh (sync_prims false, kharma_driver.cpp:109-118;
+ * kharma_step.cpp:209-249): khb_ct_stage_fluxes and khb_ctmesh_correct as above, then
+ * khb_ct_stage_update_part(part 1) on every block (face update, ghost-shell copy, the update half of
+ * the zone pass: U_out holds the updated conserved state), khb_ctmesh_exchange_cons (ghost-zone fluid
+ * U and seed primitives P_s by the cell entries — GRMHD sync_utop_seed, grmhd.cpp:159-165 — ghost
+ * faces by the face entries, then every entry's ghost zone inverted from its seed with B and U_B from
+ * its faces, floored and given U = U(P), as MeshUtoP and MeshApplyFloors over the entire block do),
+ * khb_ct_stage_update_part(part 2) on every block (the cell half over the interior and the fixups),
+ * and khb_ct_boundaries on blocks with physical faces.  The seeds of the ghost zones are written into
+ * P_s (whose ghost zones the stage's fluxes have already read).  Arrays per block as
+ * khb_ctmesh_exchange; descriptors cached per pointer set in the same way. */
+int khb_ct_stage_update_part(khb_ctx* ctx, int part, int stage, double dt, const khb_fields* P_s,
+                             const khb_fields* U_s, const khb_fields* U_0, const khb_fields* Bf_s,
+                             const khb_fields* Bf_0, const khb_fields* P_out, const khb_fields* U_out,
+                             const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream);
+int khb_ctmesh_exchange_cons(khb_ctmesh* mesh, const khb_fields* P_s, const khb_fields* U, const khb_fields* P_out,
+                             const khb_fields* Bf, int32_t* const* pflag, int32_t* const* fflag, void* stream);
+
 /* Full RK2 step with B_CT in place on (P, U, Bf), the intermediate stage in context scratch. */
 int khb_ct_step(khb_ctx* ctx, double dt, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,
                 int32_t* pflag, int32_t* fflag, void* stream);

@@ -142,12 +142,14 @@ SIGNATURES = {
     "khb_ct_stage": (_I, [_P, _I, _D] + [C.POINTER(KhbFields)] * 8 + [_P, _P, _P]),
     "khb_ct_stage_fluxes": (_I, [_P, C.POINTER(KhbFields), _P]),
     "khb_ct_stage_update": (_I, [_P, _I, _D] + [C.POINTER(KhbFields)] * 8 + [_P, _P, _P]),
+    "khb_ct_stage_update_part": (_I, [_P, _I, _I, _D] + [C.POINTER(KhbFields)] * 8 + [_P, _P, _P]),
     "khb_ct_ghost_from_faces": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
     "khb_ctmesh_create": (_I, [C.POINTER(_P), _I, _P, C.c_int64, _P, _I, _P, C.c_int64, _P, _I, _P, C.c_int64, _P,
                                C.c_int64, C.POINTER(_P)]),
     "khb_ctmesh_destroy": (_I, [_P]),
     "khb_ctmesh_correct": (_I, [_P, _P]),
     "khb_ctmesh_exchange": (_I, [_P, _P, _P, _P]),
+    "khb_ctmesh_exchange_cons": (_I, [_P] * 8),
     "khb_ct_step": (_I, [_P, _D, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P, _P, _P]),
     "khb_ct_boundaries": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),
     "khb_ct_utop": (_I, [_P, C.POINTER(KhbFields), C.POINTER(KhbFields), C.POINTER(KhbFields), _P]),

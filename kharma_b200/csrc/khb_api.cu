@@ -384,6 +384,40 @@ int ct_stage_update(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, co
     return launch_boundaries(ctx, Pout, Uout, st, &Bout);
 }
 
+// ct_stage_update in two parts around the kharma driver's exchange of a mesh: part 1 the face update,
+// the ghost-shell copy and the update half of the zone pass (U_out: the updated conserved state, its
+// B from the new faces); part 2 the cell half (inversion from P_s, floors, U = U(P)) and the fixups
+int ct_stage_update_part(khb_ctx* ctx, int part, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
+                         const khb_fields& U0, const khb_fields& Bs, const khb_fields& B0, const khb_fields& Pout,
+                         const khb_fields& Uout, const khb_fields& Bout, int32_t* pflag, int32_t* fflag, cudaStream_t st)
+{
+    const int s = stage - 1;
+    int rc;
+    ZoneCall zc;
+    zc.Ps = Ps; zc.Us = Us; zc.U0 = U0; zc.Pout = Pout; zc.Uout = Uout;
+    zc.pflag = pflag; zc.fflag = fflag;
+    zc.g0 = kRkGam0[s]; zc.g1 = kRkGam1[s]; zc.bdt = kRkBeta[s] * dt;
+    zc.dt_dev = ctx->dt_active; zc.beta = kRkBeta[s];
+    for (int x = 0; x < 3; ++x) ctx->ct_bf[x] = Bout.v[x];
+    if (part == 1) {
+        if ((rc = khb::ct_face_update(ctx, stage, dt, Bs, B0, Bout, st))) return rc;
+        if ((rc = launch_ghost_copy(ctx, Ps, Us, Pout, Uout, st))) return rc;
+        LaunchCommon::stage_reset(ctx->fail_count, stage == 2 ? ctx->words : nullptr, st);
+        KHB_LAUNCHED(ctx);
+        zc.mode = M_UPDATE;
+    } else {
+        zc.Us = Uout;          // the updated conserved state is the inversion's input
+        zc.mode = M_ZONE_CELL | ((stage == 2) ? M_DT : 0);
+    }
+    ctx->ct_active = true;
+    rc = launch_zone(ctx, zc, st);
+    ctx->ct_active = false;
+    if (rc || part == 1) return rc;
+    if ((rc = launch_fixup(ctx, Pout, Uout, pflag, st))) return rc;
+    if (has_exchange_face(ctx->d)) return KHB_OK;
+    return launch_boundaries(ctx, Pout, Uout, st, &Bout);
+}
+
 int do_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const khb_fields& Us,
                 const khb_fields& U0, const khb_fields& Bs, const khb_fields& B0, const khb_fields& Pout,
                 const khb_fields& Uout, const khb_fields& Bout, int32_t* pflag, int32_t* fflag, cudaStream_t st)
@@ -941,6 +975,22 @@ int khb_ct_stage_update(khb_ctx* ctx, int stage, double dt, const khb_fields* P_
                                   Bf_out, pflag, fflag))) return rc;
     return ct_stage_update(ctx, stage, dt, *P_s, *U_s, *U_0, *Bf_s, *Bf_0, *P_out, *U_out, *Bf_out, pflag, fflag,
                            S(stream));
+}
+
+int khb_ct_stage_update_part(khb_ctx* ctx, int part, int stage, double dt, const khb_fields* P_s,
+                             const khb_fields* U_s, const khb_fields* U_0, const khb_fields* Bf_s,
+                             const khb_fields* Bf_0, const khb_fields* P_out, const khb_fields* U_out,
+                             const khb_fields* Bf_out, int32_t* pflag, int32_t* fflag, void* stream)
+{
+    KHB_RANGE("khb_ct_stage_update_part");
+    KHB_NEED_GEOM(ctx);
+    if (part != 1 && part != 2) return fail(KHB_ERR_ARG, "khb_ct_stage_update_part: part is 1 or 2");
+    int rc;
+    if ((rc = check_ct_stage_args(ctx, "khb_ct_stage_update_part", stage, P_s, U_s, U_0, Bf_s, Bf_0, P_out, U_out,
+                                  Bf_out, pflag, fflag))) return rc;
+    if (ctx->fp32) return fail(KHB_ERR_UNSUPPORTED, "khb_ct_stage_update_part: FP64 blocks only");
+    return ct_stage_update_part(ctx, part, stage, dt, *P_s, *U_s, *U_0, *Bf_s, *Bf_0, *P_out, *U_out, *Bf_out,
+                                pflag, fflag, S(stream));
 }
 
 int khb_ct_ghost_from_faces(khb_ctx* ctx, const khb_fields* P, const khb_fields* U, const khb_fields* Bf,

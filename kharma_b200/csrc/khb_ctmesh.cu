@@ -10,7 +10,11 @@
 //                slopes, +-1/4) and onto faces inside a coarse zone (Olivares et al.'s
 //                divergence-preserving operator, b_ct_functions.hpp:151-200)
 // after which each block's ghost zones take B from their faces and U = U(P)
-// (khb_ct_ghost_from_faces).  All blocks have one shape, FP64 fluxes and the Minkowski metric of a
+// (khb_ct_ghost_from_faces).  The kharma driver's exchange (khb_ctmesh_exchange_cons) moves the
+// updated conserved fluid variables and the seed primitives by the same entries, between the update
+// and the inversion, then inverts each ghost zone like the interior:
+//   k_ctm_cell_cons    ghost-zone U (fluid) and seed P (fluid) by the entries
+//   k_ctm_ghost_cell   B and U_B from the faces, inversion, floors, U = U(P) (the zone pass's cell half)  All blocks have one shape, FP64 fluxes and the Minkowski metric of a
 // uniform Cartesian grid (areas and lengths are products of the zone widths).
 #include "khb_internal.hpp"
 #include "khb_kernels.cuh"
@@ -32,6 +36,15 @@ struct CtmBlock {
 struct CtmDims {
     int n1, n2, n3, ndim;
     long long N, sj, sk;
+};
+
+// What the ghost cell pass of one block reads: the block's shape, metric and physics, and its
+// zone-pass arguments (Ps the seeds, Us = Uout the updated state, Pout, flags, Bf the faces)
+struct CtmZoneBlock {
+    Dims d;
+    DevGeom g;
+    Phys ph;
+    ZoneArgs<double> a;
 };
 
 __device__ __forceinline__ double ctm_minmod(double a, double b)
@@ -104,6 +117,60 @@ __global__ void __launch_bounds__(128) k_ctm_cell(const CtmBlock* __restrict__ B
         }
         D.P[p][cd] = v;
     }
+}
+
+// The kharma driver's exchange of a B_CT mesh: the fluid part of the updated conserved state (U) and of
+// the seed primitives (P) by the entry's operator, into the destination's same arrays
+__global__ void __launch_bounds__(128) k_ctm_cell_cons(const CtmBlock* __restrict__ Bu, const CtmBlock* __restrict__ Bs,
+                                                       CtmDims d, const int* __restrict__ t6, long long begin,
+                                                       long long end)
+{
+    const long long e = begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= end) return;
+    const int* t = t6 + 6 * e;
+    const long long cd = __ldg(t + 1), cs = __ldg(t + 4);
+    const int op = __ldg(t + 2), aux = __ldg(t + 5);
+    const long long st[3] = {1, d.sj, d.sk};
+    for (int w = 0; w < 2; ++w) {
+        const CtmBlock* B = w ? Bs : Bu;
+        const CtmBlock& D = B[__ldg(t)];
+        const CtmBlock& S = B[__ldg(t + 3)];
+        for (int p = 0; p < 5; ++p) {
+            const double* q = S.P[p];
+            double v;
+            if (op == 0) {
+                v = q[cs];
+            } else if (op == 1) {
+                double r = (q[cs] + q[cs + 1]);
+                if (d.ndim > 1) r = r + (q[cs + d.sj] + q[cs + d.sj + 1]);
+                if (d.ndim > 2) r = r + ((q[cs + d.sk] + q[cs + d.sk + 1]) + (q[cs + d.sk + d.sj] + q[cs + d.sk + d.sj + 1]));
+                v = r * ((d.ndim > 2) ? 0.125 : (d.ndim > 1) ? 0.25 : 0.5);
+            } else {
+                const double uc = q[cs];
+                v = uc;
+                for (int a = 0; a < d.ndim; ++a) {
+                    const double sl = ctm_minmod(uc - q[cs - st[a]], q[cs + st[a]] - uc);
+                    v += ((aux >> a) & 1) ? 0.25 * sl : -0.25 * sl;
+                }
+            }
+            D.P[p][cd] = v;
+        }
+    }
+}
+
+// The ghost zones of the cell entries, each inverted as the zone pass's cell half inverts the
+// interior (MeshUtoP and MeshApplyFloors over the entire block, kharma_step.cpp:233-236)
+template <int MODE>
+__global__ void __launch_bounds__(128) k_ctm_ghost_cell(const CtmZoneBlock* __restrict__ Z, const int* __restrict__ t6,
+                                                        long long n)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int* t = t6 + 6 * e;
+    const CtmZoneBlock& B = Z[__ldg(t)];
+    int k, j, i;
+    zone_kji(B.d, __ldg(t + 1), k, j, i);
+    zone_body<8, double, MODE>(B.d, B.g, B.ph, B.a, i, j, k);
 }
 
 // One term of Olivares' operator (b_ct_functions.hpp, F<diff_face, diff_side, offset>): the
@@ -208,6 +275,12 @@ struct khb_ctmesh {
     };
     std::vector<State> states;
     std::vector<CtmBlock> host_blocks;
+    // the ghost cell pass's descriptors of each (seeds, U, Pout, Bf) set, cached the same way
+    struct ZoneState {
+        std::vector<CtmZoneBlock> host;
+        CtmZoneBlock* dev;
+    };
+    std::vector<ZoneState> zstates;
     int* cell = nullptr;
     long long n_cell = 0;
     std::vector<long long> cell_ends;   // copies and restrictions, then one phase per destination level
@@ -257,8 +330,8 @@ int upload_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, CtmB
     return KHB_OK;
 }
 
-// The device descriptors of state (P, Bf): uploaded on the first call with these pointers, found by
-// comparing the host copies afterwards (no device access)
+// The device descriptors of state (P, Bf; Bf NULL: P only): uploaded on the first call with these
+// pointers, found by comparing the host copies afterwards (no device access)
 int state_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, CtmBlock** out)
 {
     const int n = (int)m->ctx.size();
@@ -266,7 +339,7 @@ int state_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, CtmBl
         bool same = true;
         for (int b = 0; b < n && same; ++b) {
             for (int p = 0; p < 8; ++p) same &= s.host[b].P[p] == P[b].v[p];
-            for (int q = 0; q < 3; ++q) same &= s.host[b].Bf[q] == Bf[b].v[q];
+            for (int q = 0; q < 3; ++q) same &= s.host[b].Bf[q] == (Bf ? Bf[b].v[q] : nullptr);
         }
         if (same) { *out = s.dev; return KHB_OK; }
     }
@@ -277,6 +350,48 @@ int state_blocks(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf, CtmBl
     if ((rc = upload_blocks(m, P, Bf, s.dev))) { cudaFree(s.dev); return rc; }
     s.host = m->host_blocks;
     m->states.push_back(s);
+    *out = s.dev;
+    return KHB_OK;
+}
+
+bool same_fields(const khb_fields& a, const khb_fields& b, int n)
+{
+    for (int p = 0; p < n; ++p) if (a.v[p] != b.v[p]) return false;
+    return true;
+}
+
+// The ghost cell pass's descriptors of (P_s, U, P_out, Bf, flags): uploaded on first use, then reused
+int zone_blocks(khb_ctmesh* m, const khb_fields* Ps, const khb_fields* U, const khb_fields* Pout, const khb_fields* Bf,
+                int32_t* const* pflag, int32_t* const* fflag, CtmZoneBlock** out)
+{
+    const int n = (int)m->ctx.size();
+    for (auto& s : m->zstates) {
+        bool same = true;
+        for (int b = 0; b < n && same; ++b) {
+            const ZoneArgs<double>& a = s.host[b].a;
+            same = same_fields(a.Ps, Ps[b], 8) && same_fields(a.Us, U[b], 8) && same_fields(a.Pout, Pout[b], 8) &&
+                   a.Bf[0] == Bf[b].v[0] && a.Bf[1] == Bf[b].v[1] && a.Bf[2] == Bf[b].v[2] &&
+                   a.pflag == pflag[b] && a.fflag == fflag[b];
+        }
+        if (same) { *out = s.dev; return KHB_OK; }
+    }
+    khb_ctmesh::ZoneState s;
+    s.host.resize(n);
+    for (int b = 0; b < n; ++b) {
+        CtmZoneBlock& z = s.host[b];
+        std::memset((void*)&z, 0, sizeof(z));
+        const khb_ctx* c = m->ctx[b];
+        z.d = c->d; z.g = c->g; z.ph = c->ph;
+        z.a.Ps = Ps[b]; z.a.Us = U[b]; z.a.U0 = U[b]; z.a.Pout = Pout[b]; z.a.Uout = U[b];
+        z.a.pflag = pflag[b]; z.a.fflag = fflag[b];
+        for (int q = 0; q < 3; ++q) z.a.Bf[q] = Bf[b].v[q];
+        z.a.mode = 0;
+    }
+    s.dev = nullptr;
+    KHB_MCUDA(cudaMalloc((void**)&s.dev, sizeof(CtmZoneBlock) * n));
+    cudaError_t e = cudaMemcpy(s.dev, s.host.data(), sizeof(CtmZoneBlock) * n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { cudaFree(s.dev); return ctm_fail(KHB_ERR_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e)); }
+    m->zstates.push_back(s);
     *out = s.dev;
     return KHB_OK;
 }
@@ -363,6 +478,7 @@ int khb_ctmesh_destroy(khb_ctmesh* m)
 {
     if (!m) return KHB_OK;
     for (auto& s : m->states) cudaFree(s.dev);
+    for (auto& s : m->zstates) cudaFree(s.dev);
     cudaFree(m->dev_blocks); cudaFree(m->cell); cudaFree(m->face); cudaFree(m->flux); cudaFree(m->emf);
     delete m;
     return KHB_OK;
@@ -402,6 +518,49 @@ int khb_ctmesh_exchange(khb_ctmesh* m, const khb_fields* P, const khb_fields* Bf
     for (long long hi : m->face_ends) {
         if (hi > lo) k_ctm_face<<<blocks_for(hi - lo, 128), 128, 0, st>>>(blocks, m->d, m->face, lo, hi);
         lo = hi;
+    }
+    KHB_MCUDA(cudaGetLastError());
+    return KHB_OK;
+}
+
+int khb_ctmesh_exchange_cons(khb_ctmesh* m, const khb_fields* P_s, const khb_fields* U, const khb_fields* P_out,
+                             const khb_fields* Bf, int32_t* const* pflag, int32_t* const* fflag, void* stream)
+{
+    KHB_RANGE("khb_ctmesh_exchange_cons");
+    if (!m || !P_s || !U || !P_out || !Bf || !pflag || !fflag)
+        return ctm_fail(KHB_ERR_ARG, "khb_ctmesh_exchange_cons: NULL argument");
+    for (size_t b = 0; b < m->ctx.size(); ++b) {
+        for (int p = 0; p < 8; ++p)
+            if (!P_s[b].v[p] || !U[b].v[p] || !P_out[b].v[p])
+                return ctm_fail(KHB_ERR_ARG, "khb_ctmesh_exchange_cons: NULL variable pointer");
+        for (int q = 0; q < 3; ++q)
+            if (!Bf[b].v[q]) return ctm_fail(KHB_ERR_ARG, "khb_ctmesh_exchange_cons: NULL face field");
+        if (!pflag[b] || !fflag[b]) return ctm_fail(KHB_ERR_ARG, "khb_ctmesh_exchange_cons: NULL flag array");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    CtmBlock *bu = nullptr, *bs = nullptr, *bf = nullptr;
+    CtmZoneBlock* zb = nullptr;
+    if ((rc = state_blocks(m, U, nullptr, &bu)) || (rc = state_blocks(m, P_s, nullptr, &bs)) ||
+        (rc = state_blocks(m, P_out, Bf, &bf)) ||
+        (rc = zone_blocks(m, P_s, U, P_out, Bf, pflag, fflag, &zb)))
+        return rc;
+    long long lo = 0;
+    for (long long hi : m->cell_ends) {
+        if (hi > lo) k_ctm_cell_cons<<<blocks_for(hi - lo, 128), 128, 0, st>>>(bu, bs, m->d, m->cell, lo, hi);
+        lo = hi;
+    }
+    lo = 0;
+    for (long long hi : m->face_ends) {
+        if (hi > lo) k_ctm_face<<<blocks_for(hi - lo, 128), 128, 0, st>>>(bf, m->d, m->face, lo, hi);
+        lo = hi;
+    }
+    if (m->n_cell) {
+        constexpr int C = M_UTOP | M_FLOORS | M_PTOU | M_BCT | M_GHOSTB;
+        if (m->ctx[0]->ph.inverter == KHB_INVERTER_KASTAUN)
+            k_ctm_ghost_cell<C | M_KASTAUN><<<blocks_for(m->n_cell, 128), 128, 0, st>>>(zb, m->cell, m->n_cell);
+        else
+            k_ctm_ghost_cell<C><<<blocks_for(m->n_cell, 128), 128, 0, st>>>(zb, m->cell, m->n_cell);
     }
     KHB_MCUDA(cudaGetLastError());
     return KHB_OK;

@@ -400,6 +400,20 @@ __device__ __forceinline__ void ct_zone_b(const Dims& d, const DevGeom& g, const
                          : __ldg(Bf[2] + c) / __ldg(g.gdet[2] + gi);
 }
 
+// ct_zone_b for any zone of the block: the last layer of a direction (i = n1-1, j = n2-1, k = n3-1)
+// takes its lower face alone, as k_ghost_ptou does
+__device__ __forceinline__ void ct_zone_b_edge(const Dims& d, const DevGeom& g, const double* const Bf[3], long long c,
+                                               int j, int i, int k, double Bp[3])
+{
+    const long long gi = (long long)j*g.G1 + i;
+    Bp[0] = (i == d.n1 - 1) ? __ldg(Bf[0] + c) / __ldg(g.gdet[0] + gi)
+                            : (__ldg(Bf[0] + c) / __ldg(g.gdet[0] + gi) + __ldg(Bf[0] + c + 1) / __ldg(g.gdet[0] + gi + 1)) / 2;
+    Bp[1] = (d.ndim > 1 && j < d.n2 - 1) ? (__ldg(Bf[1] + c) / __ldg(g.gdet[1] + gi) + __ldg(Bf[1] + c + d.sj) / __ldg(g.gdet[1] + gi + g.G1)) / 2
+                                         : __ldg(Bf[1] + c) / __ldg(g.gdet[1] + gi);
+    Bp[2] = (d.ndim > 2 && k < d.n3 - 1) ? (__ldg(Bf[2] + c) / __ldg(g.gdet[2] + gi) + __ldg(Bf[2] + c + d.sk) / __ldg(g.gdet[2] + gi)) / 2
+                                         : __ldg(Bf[2] + c) / __ldg(g.gdet[2] + gi);
+}
+
 // The geometric source of one zone (flux.cpp:413-441): new_du[lam] = sum over mu, nu of
 // T^mu_nu gdet Gamma^nu_lam mu for the UU and U1-U3 components, from the zone's primitives Ps
 template <int NV>
@@ -512,6 +526,13 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
         } else {
 #pragma unroll
             for (int p = 0; p < NV; ++p) U[p] = a.Us.v[p][c];
+            if (NV > 5 && (MODE & M_GHOSTB) && (mode & M_BCT)) {
+                // B_CT::BlockUtoP over the entire block before the inversion (b_ct.cpp:160-188)
+                double Bp[3];
+                ct_zone_b_edge(d, g, a.Bf, c, j, i, k, Bp);
+#pragma unroll
+                for (int v = 0; v < 3; ++v) U[5 + v] = Bp[v] * G.gdet;
+            }
         }
 
         int pflag = 0, fflag = 0;
@@ -528,7 +549,8 @@ __device__ __forceinline__ double zone_body(const Dims& d, const DevGeom& g, con
             if (NV > 5) {
                 if (mode & M_BCT) {
                     double Bp[3];
-                    ct_zone_b(d, g, a.Bf, c, j, i, Bp);
+                    if (MODE & M_GHOSTB) ct_zone_b_edge(d, g, a.Bf, c, j, i, k, Bp);
+                    else ct_zone_b(d, g, a.Bf, c, j, i, Bp);
 #pragma unroll
                     for (int v = 0; v < 3; ++v) P[5 + v] = Bp[v];
                 } else {

@@ -100,6 +100,10 @@ enum { M_KASTAUN = 64 };
 // B_CT: the zone B comes from the face field (ZoneArgs::Bf) instead of the flux-CT divergence; run
 // through the run-time-mode kernel (MODE = 0)
 enum { M_BCT = 128 };
+// Ghost zones of a B_CT mesh block (compile-time only): without M_UPDATE, U_B is rebuilt from the
+// faces before the inversion, and the last ghost layer of a direction, whose upper face the arrays
+// do not hold, takes B from its lower face
+enum { M_GHOSTB = 256 };
 
 struct Box {
     int lo_i, lo_j, lo_k, cnt_i, cnt_j, cnt_k;

@@ -305,10 +305,14 @@ class CTMesh:
     """An SMRMesh of B_CT MHD blocks stepped with RK2: per block khb_ct_stage_fluxes, the mesh's flux
     and EMF corrections, khb_ct_stage_update, then the ghost exchange of the stage output.
     P_blocks: each block's primitives (8, n3, n2, n1) over the whole block; Bf_blocks: each block's
-    face field (3, n3, n2, n1), or None to interpolate it from the zone B."""
+    face field (3, n3, n2, n1), or None to interpolate it from the zone B.  conserved: the kharma
+    driver's exchange (default: when the blocks' driver is kharma): the update, the exchange of the
+    updated conserved state with the seed primitives and the faces, the ghost zones inverted like the
+    interior, then the interior's inversion and fixups (khb_ct_stage_update_part,
+    khb_ctmesh_exchange_cons).  The initial ghost zones come from the initial primitives."""
 
     def __init__(self, mesh: SMRMesh, P_blocks, Bf_blocks=None, emf_correction=True, flux_correction=True,
-                 streams=1):
+                 streams=1, conserved=None):
         import torch
         from .block import Block, Fields
         self.torch = torch
@@ -319,6 +323,7 @@ class CTMesh:
             b.set_prims(P_blocks[n], faces=None if Bf_blocks is None else Bf_blocks[n])
             self.blocks.append(b)
         self.lib = self.blocks[0].lib
+        self.conserved = (mesh.base.driver == "kharma") if conserved is None else bool(conserved)
         self._physical = [any(x not in ("exchange", "periodic") for x in blk.spec.bc) for blk in mesh.blocks]
         self.P1 = [torch.zeros_like(b.P) for b in self.blocks]
         self.U1 = [torch.zeros_like(b.U) for b in self.blocks]
@@ -399,6 +404,17 @@ class CTMesh:
                 _lib.check(self.lib.khb_ct_boundaries(b.ctx, Pf.ref, Uf.ref, Bff.ref, b.stream), "khb_ct_boundaries")
         self._per_block(ghosts)
 
+    def exchange_cons(self, P_s, U, P_out, Bf):
+        """The kharma driver's exchange (khb_ctmesh_exchange_cons) on per-block Fields: seeds P_s, updated
+        conserved state U, output primitives P_out, faces Bf."""
+        n = len(self.blocks)
+        arr = lambda fs: C.cast((_lib.KhbFields * n)(*[f.s for f in fs]), C.c_void_p)
+        pf = (C.c_void_p * n)(*[b.pflag.data_ptr() for b in self.blocks])
+        ff = (C.c_void_p * n)(*[b.fflag.data_ptr() for b in self.blocks])
+        _lib.check(self.lib.khb_ctmesh_exchange_cons(self.m, arr(P_s), arr(U), arr(P_out), arr(Bf),
+                                                     C.cast(pf, C.c_void_p), C.cast(ff, C.c_void_p), self.stream),
+                   "khb_ctmesh_exchange_cons")
+
     def step(self, dt):
         for stage in (1, 2):
             src = self._state(stage - 1)
@@ -408,18 +424,33 @@ class CTMesh:
             def fluxes(n, b):
                 _lib.check(self.lib.khb_ct_stage_fluxes(b.ctx, src[n][0].ref, b.stream), "khb_ct_stage_fluxes")
 
-            def update(n, b):
+            def args(n, b):
                 (Ps, Us, Bs), (_, U0, B0), (Po, Uo, Bo) = src[n], st0[n], out[n]
-                _lib.check(self.lib.khb_ct_stage_update(b.ctx, stage, float(dt), Ps.ref, Us.ref, U0.ref, Bs.ref,
-                                                        B0.ref, Po.ref, Uo.ref, Bo.ref,
-                                                        C.c_void_p(b.pflag.data_ptr()),
-                                                        C.c_void_p(b.fflag.data_ptr()), b.stream),
-                           "khb_ct_stage_update")
+                return (stage, float(dt), Ps.ref, Us.ref, U0.ref, Bs.ref, B0.ref, Po.ref, Uo.ref, Bo.ref,
+                        C.c_void_p(b.pflag.data_ptr()), C.c_void_p(b.fflag.data_ptr()), b.stream)
+
+            def update(n, b):
+                _lib.check(self.lib.khb_ct_stage_update(b.ctx, *args(n, b)), "khb_ct_stage_update")
+
+            def update1(n, b):
+                _lib.check(self.lib.khb_ct_stage_update_part(b.ctx, 1, *args(n, b)), "khb_ct_stage_update_part")
+
+            def update2(n, b):
+                _lib.check(self.lib.khb_ct_stage_update_part(b.ctx, 2, *args(n, b)), "khb_ct_stage_update_part")
+                if self._physical[n]:
+                    Po, Uo, Bo = out[n]
+                    _lib.check(self.lib.khb_ct_boundaries(b.ctx, Po.ref, Uo.ref, Bo.ref, b.stream), "khb_ct_boundaries")
 
             self._per_block(fluxes)
             _lib.check(self.lib.khb_ctmesh_correct(self.m, self.stream), "khb_ctmesh_correct")
-            self._per_block(update)
-            self.exchange(1 if stage == 1 else 0)
+            if self.conserved:
+                self._per_block(update1)
+                self.exchange_cons([x[0] for x in src], [x[1] for x in out], [x[0] for x in out],
+                                   [x[2] for x in out])
+                self._per_block(update2)
+            else:
+                self._per_block(update)
+                self.exchange(1 if stage == 1 else 0)
 
     def step_graph(self, dt):
         """One step replayed from a CUDA graph of the whole mesh step (captured on the first call for

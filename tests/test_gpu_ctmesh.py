@@ -74,11 +74,12 @@ def uniform_mesh_and_block(nd):
     return mesh, big
 
 
+@pytest.mark.parametrize("conserved", [False, True])
 @pytest.mark.parametrize("nd", [2, 3])
-def test_one_level_steps_as_one_block(nd):
+def test_one_level_steps_as_one_block(nd, conserved):
     mesh, big = uniform_mesh_and_block(nd)
     Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh)
-    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl), conserved=conserved)
     one = SMRMesh(big, (1, 1, 1), (32, 32, 32 if nd > 2 else 1))
     Pb, Fb = cut(one, Pl), cut(one, Fl)
     b = Block(big)
@@ -163,11 +164,12 @@ def ghost_divb(m, depth=2):
     return worst
 
 
+@pytest.mark.parametrize("conserved", [False, True])
 @pytest.mark.parametrize("name", ["2d_two_levels", "2d_three_levels", "3d_two_levels"])
-def test_refined_mesh_keeps_divb_and_mass(name):
+def test_refined_mesh_keeps_divb_and_mass(name, conserved):
     mesh = MESHES[name]()
     Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh)
-    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl), conserved=conserved)
     m0 = m.conserved_totals()
     d0 = ghost_divb(m)
     dt = 0.4 * min(min(b.spec.dx[:mesh.ndim]) for b in mesh.blocks)
@@ -237,13 +239,14 @@ def test_fast_mode_across_refinement():
     assert errs[128] < e_mesh < errs[64]
 
 
-def test_graph_step_equals_eager_step():
+@pytest.mark.parametrize("conserved", [False, True])
+def test_graph_step_equals_eager_step(conserved):
     """The mesh step captured in a CUDA graph with the per-block work spread over four streams, and
     replayed, gives bitwise the eagerly launched single-stream steps."""
     mesh = MESHES["2d_two_levels"]()
     Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh)
-    a = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
-    b = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl), streams=4)
+    a = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl), conserved=conserved)
+    b = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl), streams=4, conserved=conserved)
     dt = 0.4 / 128
     for _ in range(4):
         a.step(dt)
@@ -253,8 +256,9 @@ def test_graph_step_equals_eager_step():
         assert torch.equal(x.P, y.P) and torch.equal(x.U, y.U) and torch.equal(x.Bf, y.Bf)
 
 
+@pytest.mark.parametrize("conserved", [False, True])
 @pytest.mark.parametrize("bc", ["walls", "open"])
-def test_one_level_with_physical_faces_steps_as_one_block(bc):
+def test_one_level_with_physical_faces_steps_as_one_block(bc, conserved):
     """2x2 blocks of one level with physical domain faces (reflecting walls, or outflow X1 with
     reflecting X2): the blocks on the domain faces keep them, applied after the exchange over the
     ghost rows it fills; the mesh steps bitwise as the single block with those faces."""
@@ -263,7 +267,7 @@ def test_one_level_with_physical_faces_steps_as_one_block(bc):
     mesh = SMRMesh(base(2, nx=16, bc=faces), (2, 2, 1), (16, 16, 1))
     big = base(2, nx=32, bc=faces)
     Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh, walls=True)
-    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl), conserved=conserved)
     one = SMRMesh(big, (1, 1, 1), (32, 32, 1))
     b = Block(big)
     b.set_prims(cut(one, Pl)[0], faces=cut(one, Fl)[0])
@@ -317,3 +321,55 @@ def test_refined_mesh_with_walls_keeps_divb_and_mass():
     assert m.max_divb() * (1.0 / 128) < 1e-13 * scale
     assert abs(m1[0] - m0[0]) < 1e-13 * abs(m0[0])
     assert interface_mismatch(m) < 1e-13 * scale
+
+
+@pytest.mark.parametrize("name", ["2d_two_levels", "3d_two_levels"])
+def test_conserved_exchange_matches_oracle_inversion(oracle_mod, name):
+    """The kharma driver's exchange on a state whose fluid U is not U(P): every ghost zone the cell
+    entries fill holds the oracle's inversion of the restated conserved state (copy, restriction or
+    prolongation of the blocks' U) from the restated seed, with B and U_B from its exchanged faces
+    (the last layer of a direction from its lower face), no failure, and U = U(P)."""
+    mesh = MESHES[name]()
+    Pl, Fl = fluid_levels(mesh), curl_faces_levels(mesh)
+    m = ctmesh.CTMesh(mesh, cut(mesh, Pl), cut(mesh, Fl))
+    torch.cuda.synchronize()
+    rng = np.random.Generator(np.random.PCG64(12))
+    P, U = [], []
+    for b in m.blocks:
+        u = b.U.cpu().numpy()
+        u[:5] = u[:5] * (1 + 1e-3 * rng.standard_normal(u[:5].shape))
+        b.U.copy_(torch.as_tensor(u))
+        P.append(b.P.cpu().numpy())
+        U.append(u)
+    torch.cuda.synchronize()
+    st = m._state(0)
+    m.exchange_cons([x[0] for x in st], [x[1] for x in st], [x[0] for x in st], [x[2] for x in st])
+    torch.cuda.synchronize()
+    o = oracle_mod.Oracle(mesh.blocks[0].spec)
+    cell = m.tables["cell"]
+    exp_u, exp_p = smr_ref.expected_ghosts(mesh, U), smr_ref.expected_ghosts(mesh, P)
+    worst, checked = 0.0, 0
+    for n, b in enumerate(m.blocks):
+        Pg, Ug, Fg, pf = b.P.cpu().numpy(), b.U.cpu().numpy(), b.Bf.cpu().numpy(), b.pflag.cpu().numpy()
+        n3, n2, n1 = b.spec.shape
+        Eu, Ep = exp_u[n][1], exp_p[n][1]
+        zones = cell[cell[:, 0] == n, 1]
+        for c in zones[:: max(1, len(zones) // 600)]:
+            k, r = divmod(int(c), n1 * n2)
+            j, i = divmod(r, n1)
+            Bp = np.array([Fg[0, k, j, i] if i == n1 - 1 else (Fg[0, k, j, i] + Fg[0, k, j, i + 1]) / 2,
+                           Fg[1, k, j, i] if j == n2 - 1 else (Fg[1, k, j, i] + Fg[1, k, j + 1, i]) / 2,
+                           Fg[2, k, j, i] if (mesh.ndim < 3 or k == n3 - 1) else (Fg[2, k, j, i] + Fg[2, k + 1, j, i]) / 2])
+            uz = np.concatenate([Eu[:5, k, j, i], Bp])
+            pz = np.concatenate([Ep[:5, k, j, i], Bp])
+            flag = o.lib.orc_utop_cell(o.h, int(j), int(i), oracle_mod._ptr(uz), oracle_mod._ptr(pz))
+            pz[5:] = Bp
+            assert flag == 0 and pf[k, j, i] == 0
+            worst = max(worst, float(np.max(np.abs(Pg[:, k, j, i] - pz) / np.maximum(np.abs(pz), 1.0))))
+            checked += 1
+        mask = np.zeros(Pg[0].size, dtype=bool)
+        mask[zones] = True
+        mask = mask.reshape(Pg[0].shape)
+        assert np.array_equal(Ug[:, mask], o.ptou(Pg)[:, mask]), n
+    print("B_CT conserved exchange:", checked, "ghost zones, worst relative P difference", worst)
+    assert checked > 0 and worst <= 1e-12
