@@ -509,11 +509,13 @@ def smr_form(steps=20, warm=3):
 def smr_b_ct_form(steps=5, warm=2):
     """A multilevel mesh of B_CT MHD blocks (khb_ctmesh): the 4 x 4 x 4 root grid of 32^3 blocks with the
     central 2 x 2 x 2 refined (56 + 64 blocks, 3.9M zones), magnetized entropy wave (faces the curl of
-    a vector potential), linear MC, LLF, gs05_c EMFs, FP64, fixed dt; each stage runs every block's
-    khb_ct_stage_fluxes, the flux and EMF corrections, every block's khb_ct_stage_update and the
-    exchange, launched block by block from the host (eager) or replayed from a CUDA graph of the whole
-    step, the per-block work spread over 8 streams; against the same blocks stepped alone (khb_ct_step,
-    eager, one stream).  CUDA events on the current
+    a vector potential), linear MC, LLF, gs05_c EMFs, FP64, fixed dt, kharma driver; each stage runs
+    every block's khb_ct_stage_fluxes, the flux and EMF corrections, every block's update half, the
+    exchange of the updated conserved state and seeds with every ghost zone inverted, and every
+    block's inversion and fixups (khb_ct_stage_update_part, khb_ctmesh_exchange_cons), launched block
+    by block from the host (eager) or replayed from a CUDA graph of the whole step, the per-block work
+    spread over 8 streams; the simple/ImEx drivers' exchange of primitives (graph) beside it; against
+    the same blocks stepped alone (khb_ct_step, eager, one stream).  CUDA events on the current
     stream; max face divergence after the run."""
     import torch
     from kharma_b200 import ctmesh
@@ -546,13 +548,22 @@ def smr_b_ct_form(steps=5, warm=2):
     ms = timed(lambda: m.step_graph(dt))
     divb = m.max_divb() * min(mesh.blocks[0].spec.dx)
     ms_alone = timed(lambda: [b.step(dt) for b in m.blocks])
+    n_face, n_emf = int(len(m.tables["face"])), int(len(m.tables["emf"]))
+    m._graph = None
+    del m
+    torch.cuda.empty_cache()
+    mp = ctmesh.CTMesh(mesh, cut(mesh, fluid_levels(mesh)), cut(mesh, curl_faces_levels(mesh)), streams=8,
+                       conserved=False)
+    ms_prims = timed(lambda: mp.step_graph(dt))
+    mp._graph = None
+    del mp
     out = {"workload": f"B_CT MHD mesh: 4x4x4 root blocks of 32^3, central 2x2x2 refined: {len(mesh.blocks)} blocks, "
                        f"{mesh.zones:,} zones, magnetized entropy wave, linear MC, LLF, gs05_c, FP64",
            "graph_ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0), "eager_ms_per_step": ms_eager,
+           "prims_exchange_graph_ms_per_step": ms_prims,
            "blocks_alone_eager_one_stream_ms_per_step": ms_alone,
            "max_face_divb_dx_after": divb,
-           "face_entries": int(len(m.tables["face"])), "emf_entries": int(len(m.tables["emf"]))}
-    del m
+           "face_entries": n_face, "emf_entries": n_emf}
     torch.cuda.empty_cache()
     return out
 
