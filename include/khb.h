@@ -197,6 +197,12 @@ int khb_set_geometry(khb_ctx* ctx, const double* gcov, const double* gcon, const
  * cover [s, e+1] along dir and [s-1, e+1] across it. */
 int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream);
 
+/* khb_get_flux over the faces whose x3 index lies in [k_lo, k_hi] only (each face's flux is
+ * independent of the others: the union of calls over disjoint ranges equals khb_get_flux).  A slab
+ * of an x3 decomposition computes the faces that read no x3 ghost plane while its halo exchange is in
+ * flight, then the rest (the interior compute the halo exchange overlaps, kharma_driver.cpp:151). */
+int khb_get_flux_planes(khb_ctx* ctx, int dir, const khb_fields* P, int k_lo, int k_hi, void* stream);
+
 /* First-order flux correction of one stage (KHARMADriver::AddFOFC, kharma_driver.cpp:292-337;
  * Flux::MarkFOFC and Flux::FOFC, fofc.cpp:45-226), between khb_get_flux and khb_fix_flux: a guess of
  * the stage's conserved state from the raw face fluxes (interior plus the zones whose flags the

@@ -198,6 +198,7 @@ SIGNATURES = {
     "khb_batch_set_mesh": (_I, [_P, _P, C.c_int64, C.c_int64, _P, C.c_int64]),
     "khb_batch_mesh_exchange": (_I, [_P, _P]),
     "khb_batch_set_mesh_sync": (_I, [_P, C.c_int]),
+    "khb_get_flux_planes": (_I, [_P, _I, C.POINTER(KhbFields), _I, _I, _P]),
 }
 
 _lib = None

@@ -46,7 +46,8 @@ int check_fields(const khb_ctx* ctx, const khb_fields* f, const char* name)
 }
 
 // ------------------------------------------------------------------ fluxes
-int launch_flux(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
+// k_lo <= k_hi: only the faces whose x3 index lies in [k_lo, k_hi]
+int launch_flux(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st, int k_lo = 0, int k_hi = -1)
 {
     const Dims& d = ctx->d;
     int lo[3], cnt[3];
@@ -57,6 +58,11 @@ int launch_flux(khb_ctx* ctx, int dir, const khb_fields& P, cudaStream_t st)
         if (a + 1 == dir) { lo[a] = s[a]; hi = e[a] + 1; }
         else if (active) { lo[a] = s[a] - 1; hi = e[a] + 1; }
         else { lo[a] = s[a]; hi = e[a]; }
+        if (a == 2 && k_lo <= k_hi) {
+            lo[a] = lo[a] > k_lo ? lo[a] : k_lo;
+            hi = hi < k_hi ? hi : k_hi;
+            if (hi < lo[a]) return KHB_OK;
+        }
         cnt[a] = hi - lo[a] + 1;
     }
     if (ctx->fp32)
@@ -723,6 +729,17 @@ int khb_get_flux(khb_ctx* ctx, int dir, const khb_fields* P, void* stream)
     int rc;
     if ((rc = check_fields(ctx, P, "P"))) return rc;
     return launch_flux(ctx, dir, *P, S(stream));
+}
+
+int khb_get_flux_planes(khb_ctx* ctx, int dir, const khb_fields* P, int k_lo, int k_hi, void* stream)
+{
+    KHB_RANGE("khb_get_flux_planes");
+    KHB_NEED_GEOM(ctx);
+    if (dir < 1 || dir > ctx->d.ndim) return fail(KHB_ERR_ARG, "khb_get_flux_planes: dir out of range");
+    if (k_lo > k_hi) return fail(KHB_ERR_ARG, "khb_get_flux_planes: empty plane range");
+    int rc;
+    if ((rc = check_fields(ctx, P, "P"))) return rc;
+    return launch_flux(ctx, dir, *P, S(stream), k_lo, k_hi);
 }
 
 int khb_fofc(khb_ctx* ctx, int stage, double dt, const khb_fields* P_s, const khb_fields* U_s,

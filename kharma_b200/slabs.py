@@ -14,6 +14,13 @@ per-rank minimum, max divB the maximum (kharma_driver.cpp:439-460, b_flux_ct.cpp
 Two exchangers implement the same plan: LocalExchange runs all slabs in one process (one GPU, or
 CPU tensors), DistExchange uses torch.distributed point-to-point operations (NCCL between GPUs,
 gloo on CPU), one rank per slab.
+
+With overlap (step(..., overlap=True), SlabDriver(overlap=True)) the second exchange is started, not
+waited for: the next stage first computes the faces that read no x3 ghost plane (x1/x2 faces of the
+interior planes, x3 faces at least ng planes inside; khb_get_flux_planes), then completes the
+exchange (NCCL: the compute stream waits on the communication stream; gloo: the host waits while
+those kernels run) and computes the rest.  Every face is computed once either way, so the
+overlapped step equals the plain one bit for bit.
 """
 import dataclasses
 
@@ -48,13 +55,23 @@ class LocalExchange:
 
     def exchange(self, per_slab, spec, nplanes):
         """per_slab[r] = list of this slab's (..., n3, n2, n1) arrays, same order on every slab."""
+        self.finish(self.start(per_slab, spec, nplanes))
+
+    def start(self, per_slab, spec, nplanes):
+        """The sent planes are copied out now; the ghost planes are written by finish()."""
         n = len(per_slab)
         slo, shi, rlo, rhi = plane_ranges(spec, nplanes)
+        moves = []
         for r in range(n):
             left, right = per_slab[(r - 1) % n], per_slab[(r + 1) % n]
             for a, al, ar in zip(per_slab[r], left, right):
-                a[..., rlo, :, :].copy_(al[..., shi, :, :])
-                a[..., rhi, :, :].copy_(ar[..., slo, :, :])
+                moves.append((a[..., rlo, :, :], al[..., shi, :, :].clone()))
+                moves.append((a[..., rhi, :, :], ar[..., slo, :, :].clone()))
+        return moves
+
+    def finish(self, moves):
+        for dst, src in moves or ():
+            dst.copy_(src)
 
 
 class DistExchange:
@@ -75,10 +92,13 @@ class DistExchange:
 
     def exchange(self, arrays, spec, nplanes):
         """arrays: this rank's list of (n3, n2, n1) (or (nv, n3, n2, n1)) arrays."""
+        self.finish(self.start(arrays, spec, nplanes))
+
+    def start(self, arrays, spec, nplanes):
+        """Pack and post the sends and receives; the ghost planes are written by finish()."""
         slo, shi, rlo, rhi = plane_ranges(spec, nplanes)
         if self.world == 1:
-            LocalExchange().exchange([arrays], spec, nplanes)
-            return
+            return ("local", LocalExchange().start([arrays], spec, nplanes))
         dist = self.dist
         left, right = (self.rank - 1) % self.world, (self.rank + 1) % self.world
         views = []
@@ -98,11 +118,23 @@ class DistExchange:
         # two ranks (left == right) the low planes still land in the peer's high ghosts.
         ops = [dist.P2POp(dist.isend, send_lo, left), dist.P2POp(dist.isend, send_hi, right),
                dist.P2POp(dist.irecv, recv_hi, right), dist.P2POp(dist.irecv, recv_lo, left)]
-        for req in dist.batch_isend_irecv(ops):
+        reqs = dist.batch_isend_irecv(ops)
+        return ("dist", (reqs, (send_lo, send_hi), recv_hi, recv_lo, stage, views, rhi, rlo))
+
+    def finish(self, handle):
+        if handle is None:
+            return
+        kind, h = handle
+        if kind == "local":
+            LocalExchange().finish(h)
+            return
+        reqs, _sends, recv_hi, recv_lo, stage, views, rhi, rlo = h
+        for req in reqs:
             req.wait()
         if stage:
             dev = views[0].device
             recv_hi, recv_lo = recv_hi.to(dev), recv_lo.to(dev)
+        as_bytes = lambda t: t.reshape(-1).view(torch.uint8)
         off = 0
         for a in views:
             hi, lo = a[rhi], a[rlo]
@@ -125,15 +157,36 @@ class SlabBlock:
         self.U1 = torch.zeros_like(self.block.U)
 
     # The pieces of one stage (khb_stage = fluxes + fix_flux + zone pass + fixups + boundaries)
-    def stage_compute(self, stage, dt, Pin, Uin, Pout, Uout):
+    def stage_fluxes(self, Pin, part):
+        """The faces of a stage in two parts: 'inner' reads no x3 ghost plane (x1/x2 faces of planes
+        ks..ke, x3 faces ks+ng..ke+1-ng), 'outer' the rest."""
+        from .block import Fields
+        from . import _lib
+        b = self.block
+        Pi = Fields(Pin)
+        ng = self.spec.ng
+        ks, ke = ng, ng + self.spec.nx3 - 1
+        for d in range(1, self.spec.ndim + 1):
+            if d < 3:
+                inner = [(ks, ke)]
+                outer = [(ks - 1, ks - 1), (ke + 1, ke + 1)]
+            else:
+                inner = [(ks + ng, ke + 1 - ng)]
+                outer = [(ks, min(ks + ng - 1, ke + 1)), (max(ke + 2 - ng, ks + ng), ke + 1)]
+            for lo, hi in (inner if part == "inner" else outer):
+                if lo <= hi:
+                    _lib.check(b.lib.khb_get_flux_planes(b.ctx, d, Pi.ref, lo, hi, b.stream), "khb_get_flux_planes")
+
+    def stage_compute(self, stage, dt, Pin, Uin, Pout, Uout, fluxes=True):
         from .block import Fields
         import ctypes as C
         from . import _lib
         b = self.block
         lib, ctx, st = b.lib, b.ctx, b.stream
         Pi, Ui, Po, Uo, U0 = Fields(Pin), Fields(Uin), Fields(Pout), Fields(Uout), Fields(b.U)
-        for d in range(1, self.spec.ndim + 1):
-            _lib.check(lib.khb_get_flux(ctx, d, Pi.ref, st), "khb_get_flux")
+        if fluxes:
+            for d in range(1, self.spec.ndim + 1):
+                _lib.check(lib.khb_get_flux(ctx, d, Pi.ref, st), "khb_get_flux")
         _lib.check(lib.khb_fix_flux(ctx, st), "khb_fix_flux")
         pf, ff = C.c_void_p(b.pflag.data_ptr()), C.c_void_p(b.fflag.data_ptr())
         _lib.check(lib.khb_zone_pass(ctx, stage, dt, Pi.ref, Ui.ref, U0.ref, Po.ref, Uo.ref, pf, ff, st),
@@ -181,20 +234,39 @@ def _exchange_fix(slabs, exchanger, local, P):
         exchanger.exchange([P[0][0:5], slabs[0].block.pflag], spec, 1)
 
 
-def step(slabs, exchanger, dt, local=True):
+def _start_full(slabs, exchanger, local, P, U):
+    spec = slabs[0].spec
+    if local:
+        return exchanger.start([[P[i], U[i]] for i in range(len(slabs))], spec, spec.ng)
+    return exchanger.start([P[0], U[0]], spec, spec.ng)
+
+
+def step(slabs, exchanger, dt, local=True, overlap=False, pending=None):
     """One RK2 step of every slab in this process (all slabs with LocalExchange, this rank's one
-    with DistExchange)."""
+    with DistExchange).  overlap: the second exchange of each stage is left in flight and completed
+    by the next stage after the faces that do not need it; pending is the one the previous step left
+    (None: complete), and the return value the one this step leaves (None without overlap)."""
     for stage in (1, 2):
         Pin = [s.block.P if stage == 1 else s.P1 for s in slabs]
         Uin = [s.block.U if stage == 1 else s.U1 for s in slabs]
         Pout = [s.P1 if stage == 1 else s.block.P for s in slabs]
         Uout = [s.U1 if stage == 1 else s.block.U for s in slabs]
+        if overlap:
+            for i, s in enumerate(slabs):
+                s.stage_fluxes(Pin[i], "inner")
+            exchanger.finish(pending)
+            for i, s in enumerate(slabs):
+                s.stage_fluxes(Pin[i], "outer")
         for i, s in enumerate(slabs):
-            s.stage_compute(stage, dt, Pin[i], Uin[i], Pout[i], Uout[i])
+            s.stage_compute(stage, dt, Pin[i], Uin[i], Pout[i], Uout[i], fluxes=not overlap)
         _exchange_fix(slabs, exchanger, local, Pout)
         for i, s in enumerate(slabs):
             s.stage_fix(Pout[i], Uout[i])
-        _exchange_full(slabs, exchanger, local, Pout, Uout)
+        if overlap:
+            pending = _start_full(slabs, exchanger, local, Pout, Uout)
+        else:
+            _exchange_full(slabs, exchanger, local, Pout, Uout)
+    return pending
 
 
 def min_ndt(slabs, local=True):
@@ -213,17 +285,24 @@ class SlabDriver:
     """The reference's timestep schedule (Driver) over decomposed slabs: the per-rank minimum zone
     timestep is reduced over all slabs (and ranks) before the next dt is chosen."""
 
-    def __init__(self, slabs, exchanger, local=True, dt_start=None):
+    def __init__(self, slabs, exchanger, local=True, dt_start=None, overlap=False):
         self.slabs = slabs
         self.ex = exchanger
         self.local = local
+        self.overlap = overlap
+        self.pending = None
         spec = slabs[0].spec
         self.dt = spec.dt_min if dt_start is None else dt_start
         self.nstep = 0
 
+    def sync(self):
+        """Complete the exchange the last step left in flight (the state's ghost planes)."""
+        self.ex.finish(self.pending)
+        self.pending = None
+
     def step(self, dt=None):
         dt = self.dt if dt is None else dt
-        step(self.slabs, self.ex, dt, self.local)
+        self.pending = step(self.slabs, self.ex, dt, self.local, self.overlap, self.pending)
         mn = min_ndt(self.slabs, self.local)
         s = self.slabs[0].spec
         ndt = min(max(mn * s.cfl, s.dt_min), s.max_dt_increase * dt)

@@ -24,7 +24,7 @@ def _free_port():
         return sk.getsockname()[1]
 
 
-def _worker(rank, nranks, port, outdir):
+def _worker(rank, nranks, port, outdir, overlap):
     from datetime import timedelta
 
     import torch.distributed as dist
@@ -43,10 +43,11 @@ def _worker(rank, nranks, port, outdir):
         sb = slabs.SlabBlock(spec, nranks, rank, ex, geometry=geom)
         ng, n = spec.ng, spec.nx3 // nranks
         slabs.set_prims([sb], ex, [P0[:, rank * n:rank * n + n + 2 * ng]], local=False)
-        drv = slabs.SlabDriver([sb], ex, local=False)
+        drv = slabs.SlabDriver([sb], ex, local=False, overlap=overlap)
         out = {}
         for step in range(NSTEPS):
             dt, mn = drv.step()
+            drv.sync()
             torch.cuda.synchronize()
             out[f"P{step}"] = sb.block.P.cpu().numpy()
             out[f"U{step}"] = sb.block.U.cpu().numpy()
@@ -56,15 +57,18 @@ def _worker(rank, nranks, port, outdir):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("nranks", [2])
-def test_distributed_slabs_match_single_block(nranks):
+def test_distributed_slabs_match_single_block(nranks, overlap):
+    """overlap: each stage's second exchange completes only after the next stage's faces that read no
+    ghost plane have been launched."""
     from kharma_b200 import problems
     from kharma_b200.block import Block, Driver, build_geometry
     from kharma_b200.spec import torus_spec
     with tempfile.TemporaryDirectory() as outdir:
         ctx = mp.get_context("spawn")
         port = _free_port()
-        procs = [ctx.Process(target=_worker, args=(r, nranks, port, outdir)) for r in range(nranks)]
+        procs = [ctx.Process(target=_worker, args=(r, nranks, port, outdir, overlap)) for r in range(nranks)]
         for p in procs:
             p.start()
         for p in procs:

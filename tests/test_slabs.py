@@ -79,7 +79,7 @@ def _free_port():
         return sk.getsockname()[1]
 
 
-def _worker(rank, nranks, port, nplanes, out):
+def _worker(rank, nranks, port, nplanes, out, split=False):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -87,21 +87,30 @@ def _worker(rank, nranks, port, nplanes, out):
     try:
         gspec = torus_spec(16, 8, 12)
         s, P, f = slab_arrays(gspec, nranks, rank)
-        DistExchange().exchange([P, f], s, nplanes)
+        ex = DistExchange()
+        ok = True
+        if split:
+            # started, not finished: the ghost planes are untouched until finish()
+            P0, f0 = P.clone(), f.clone()
+            h = ex.start([P, f], s, nplanes)
+            ok = torch.equal(P, P0) and torch.equal(f, f0)
+            ex.finish(h)
+        else:
+            ex.exchange([P, f], s, nplanes)
         eP, ef = expected_after_exchange(gspec, nranks, rank, nplanes)
         ng = gspec.ng
         sl = slice(ng - nplanes, ng + s.nx3 + nplanes)
-        out[rank] = int(torch.equal(P[:, sl], eP[:, sl]) and torch.equal(f[sl], ef[sl]))
+        out[rank] = int(ok and torch.equal(P[:, sl], eP[:, sl]) and torch.equal(f[sl], ef[sl]))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("nranks,nplanes", [(2, 4), (3, 1)])
-def test_distributed_exchange_gloo(nranks, nplanes):
+@pytest.mark.parametrize("nranks,nplanes,split", [(2, 4, False), (3, 1, False), (2, 4, True), (3, 2, True)])
+def test_distributed_exchange_gloo(nranks, nplanes, split):
     ctx = mp.get_context("spawn")
     out = ctx.Manager().dict()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, nranks, port, nplanes, out)) for r in range(nranks)]
+    procs = [ctx.Process(target=_worker, args=(r, nranks, port, nplanes, out, split)) for r in range(nranks)]
     for p in procs:
         p.start()
     for p in procs:
