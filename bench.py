@@ -502,6 +502,27 @@ def smr_form(steps=20, warm=3):
                            "launches_per_step": launches3}
     del b
     torch.cuda.empty_cache()
+    # spherical-KS Bondi on the two-level layout: r in [3, 30] (MKS, outflow x1), reflecting x2,
+    # periodic x3, WENO5; the kharma driver's exchange (conserved variables and seeds, ghost zones
+    # inverted) and the primitive exchange
+    from kharma_b200.block import build_geometry
+    from kharma_b200.spec import bondi_spec
+    ks = bondi_spec(32, 32, 32, float(np.log(3.0)), float(np.log(30.0)), 0.0, 1.0, 0.0, 2 * np.pi,
+                    bc=("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"))
+    mesh = SMRMesh(ks, (4, 4, 4), (32, 32, 32), refine=refine)
+    ks_out = {"workload": f"Bondi (r_s = 8) in spherical KS (a = 0, MKS), r in [3, 30], 4x4x4 root blocks of 32^3 "
+                          f"with the central 2x2x2 refined: {len(mesh.blocks)} blocks, {mesh.zones:,} zones, "
+                          f"WENO5, LLF, FP64, outflow/reflecting/periodic faces"}
+    for conserved in (True, False):
+        b = smr_batch(mesh, lambda sp: problems.bondi(sp, build_geometry(sp)), conserved=conserved)
+        dt = 1e-3
+        ms_k, launches_k = timed(steps)
+        ks_out["kharma_driver_exchange" if conserved else "primitive_exchange"] = {
+            "graph_ms_per_step": ms_k, "zone_cycles_per_s": mesh.zones / (ms_k / 1000.0),
+            "launches_per_step": launches_k}
+        del b
+        torch.cuda.empty_cache()
+    out["ks_bondi"] = ks_out
     out["b_ct_mhd"] = smr_b_ct_form()
     return out
 
