@@ -82,6 +82,17 @@ def detail(name, obj):
     print(f"detail {name}: " + json.dumps(obj), flush=True)
 
 
+def compact(obj, digits=6):
+    """obj with every float rounded to `digits` significant digits (keeps the final line short)."""
+    if isinstance(obj, float):
+        return float(f"{obj:.{digits}g}")
+    if isinstance(obj, dict):
+        return {k: compact(v, digits) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return [compact(v, digits) for v in obj]
+    return obj
+
+
 def profile_traffic(kernel, size, form):
     """DRAM bytes per launch of `kernel` (dram__bytes_read.sum + dram__bytes_write.sum) from the
     committed ncu summary of this workload, which states it on a line
@@ -216,7 +227,7 @@ def cpu_baseline_block(n1, n2, n3, runs=5):
     return {"value": zones / med, "unit": UNIT, "cores": threads, "kind": "port",
             "single_thread_value": zones / one,
             "sample": f"oracle port, same {n1}x{n2}x{n3} block, {threads} threads ({_cpu_model()}): median of {runs} "
-                      f"RK2 steps after 1 warm-up ({min(per):.2f}-{max(per):.2f} s); 1 thread: {one:.2f} s/step"}
+                      f"RK2 steps after 1 warm-up; 1 thread: {one:.2f} s/step"}
 
 
 def reference_arm(args, rank, world):
@@ -985,7 +996,7 @@ def gpu_arm(args, rank, world, local_rank):
                "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
                "fp32_flux": fp32, "e2e": e2e, "cpu_baseline": cpu,
                "emhd_newton": emhd_summary(emhd) if emhd else None}
-        print(json.dumps(out), flush=True)
+        print(json.dumps(compact(out)), flush=True)
 
 
 def main():
