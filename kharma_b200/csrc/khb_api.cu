@@ -281,6 +281,82 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
     return KHB_OK;
 }
 
+// The launches launch_boundaries(ctx, P, U, st) makes (no face field, the context's nvar), appended as
+// tasks to the phase each belongs to (phases[0..BOUND_PHASES-1], run in that order): a batch runs each
+// phase of all its blocks in one k_bound_tasks launch, with the same work per zone
+void boundary_tasks_of(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, std::vector<BoundTask>* phases)
+{
+    const Dims& d = ctx->d;
+    const bool xj = d.ndim >= 2 && (d.bc[2] == KHB_BC_EXCHANGE || d.bc[3] == KHB_BC_EXCHANGE);
+    const bool xk = d.ndim >= 3 && (d.bc[4] == KHB_BC_EXCHANGE || d.bc[5] == KHB_BC_EXCHANGE);
+    const int lo_k = xk ? 0 : d.ks;
+    const int cnt_k = xk ? d.n3 : d.ke - d.ks + 1;
+    int pfaces = 0;
+    bool exch = false;
+    for (int f = 0; f < 2 * d.ndim; ++f) {
+        if (phys_face(d.bc[f])) pfaces |= 1 << f;
+        exch = exch || d.bc[f] == KHB_BC_EXCHANGE;
+    }
+    if (!exch) pfaces = 0;
+    BoundTask base;
+    std::memset((void*)&base, 0, sizeof(base));
+    base.d = d; base.g = ctx->g; base.ph = ctx->ph; base.P = P; base.U = U;
+    auto bc = [&](int phase, int face, int lo_a, int cnt_a, int lk, int ck) {
+        BoundTask t = base;
+        t.kind = BOUND_BC; t.face = face; t.lo_a = lo_a; t.cnt_a = cnt_a; t.lo_k = lk; t.cnt_k = ck;
+        const int bdir = face / 2 + 1;
+        const int ng = (bdir == 1) ? d.is : ((bdir == 2) ? d.js : d.ks);
+        t.count = (long long)ng * cnt_a * ck;
+        if (t.count > 0) phases[phase].push_back(t);
+    };
+    auto ghost = [&](int phase, int kplanes) {
+        BoundTask t = base;
+        t.kind = BOUND_GHOST_PTOU; t.kplanes = kplanes; t.pfaces = pfaces;
+        const long long plane = (long long)d.n1 * d.n2;
+        const long long per = plane - (long long)(d.ie - d.is + 1) * (d.je - d.js + 1);
+        t.count = kplanes ? plane * (((kplanes & 1) ? d.ks : 0) + ((kplanes & 2) ? d.n3 - 1 - d.ke : 0))
+                          : per * (d.ke - d.ks + 1);
+        if (t.count > 0) phases[phase].push_back(t);
+    };
+    bool physical = false;
+    for (int face = 0; face < 2; ++face) {
+        if (!phys_face(d.bc[face])) continue;
+        physical = true;
+        bc(0, face, xj ? 0 : d.js, xj ? d.n2 : d.je - d.js + 1, lo_k, cnt_k);
+    }
+    if (d.ndim >= 2) {
+        for (int face = 2; face < 4; ++face) {
+            if (!phys_face(d.bc[face])) continue;
+            physical = true;
+            bc(1, face, 0, d.n1, lo_k, cnt_k);
+        }
+        if (ctx->cfg.fix_corner_inner && phys_face(d.bc[0]) && phys_face(d.bc[3])) bc(2, 0, 0, d.n2, lo_k, cnt_k);
+    }
+    if (physical) {
+        ghost(3, 0);
+        if (xk) ghost(4, 3);
+    }
+    int kplanes = 0;
+    if (d.ndim >= 3) {
+        for (int face = 4; face < 6; ++face) {
+            if (!phys_face(d.bc[face])) continue;
+            kplanes |= 1 << (face - 4);
+            bc(5, face, 0, d.n1 * d.n2, 0, 1);
+        }
+        if (kplanes) ghost(6, kplanes);
+    }
+    int pmask = 0;
+    if (d.bc[0] == KHB_BC_PERIODIC) pmask |= 1;
+    if (d.ndim >= 2 && d.bc[2] == KHB_BC_PERIODIC) pmask |= 2;
+    if (d.ndim >= 3 && d.bc[4] == KHB_BC_PERIODIC) pmask |= 4;
+    if (pmask) {
+        BoundTask t = base;
+        t.kind = BOUND_PERIODIC; t.pmask = pmask;
+        t.count = d.N - (long long)(d.ie - d.is + 1) * (d.je - d.js + 1) * (d.ke - d.ks + 1);
+        if (t.count > 0) phases[7].push_back(t);
+    }
+}
+
 size_t ft_size(const khb_ctx* ctx) { return ctx->fp32 ? sizeof(float) : sizeof(double); }
 
 bool has_exchange_face(const Dims& d)
@@ -437,6 +513,11 @@ int do_ct_stage(khb_ctx* ctx, int stage, double dt, const khb_fields& Ps, const 
 
 int khb::set_error(int code, const std::string& msg) { return fail(code, msg); }
 int khb::ctx_fix_flux(khb_ctx* ctx, cudaStream_t st) { return launch_fix_flux(ctx, ctx->ph, st); }
+void khb::boundary_tasks(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, std::vector<BoundTask>* phases)
+{
+    boundary_tasks_of(ctx, P, U, phases);
+}
+
 int khb::ctx_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st)
 {
     return launch_boundaries(ctx, P, U, st);

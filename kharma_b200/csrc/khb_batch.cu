@@ -27,8 +27,9 @@ struct khb_batch {
     int persistent = 0;                            // 1: grid of (SMs x resident CTAs), CTAs loop over tiles
     // launch plan: 0 one launch per kernel per stage (counter reset, faces per direction, ghost-shell
     // copy, update half, cell half, fixups); 1 fused: three launches per stage (all faces with the
-    // resets and shell copies, the whole zone pass, fixups), plus the per-block launches of physical
-    // faces and the mesh kernels of SMR meshes
+    // resets and shell copies, the whole zone pass, fixups), plus the per-block flux fixes of
+    // physical faces, one launch per boundary phase for all blocks with physical or periodic faces,
+    // and the mesh kernels of SMR meshes
     int plan = 0;
     int nsm = 0;
     // device tables
@@ -44,6 +45,11 @@ struct khb_batch {
     unsigned long long* word = nullptr;            // minimum zone timestep (bit pattern)
     double dt_host = 0.;                           // source of the timestep upload
     std::vector<int> needs_fix_flux, needs_bounds; // blocks with physical (or periodic) faces
+    // the boundary work of those blocks per stage output (0: stage 1's, 1: the state), as tasks of
+    // k_bound_tasks grouped by phase: [bound_off[s][p], bound_off[s][p + 1]) in bound_dev[s]
+    BoundTask* bound_dev[2] = {nullptr, nullptr};
+    std::vector<int> bound_off[2];
+    std::vector<long long> bound_max[2];
     bool any_exchange = false;                     // some block carries its ghost shell over
     // SMR: ghost-exchange and flux-correction tables (6 ints per entry) of the mesh the blocks form
     int* mesh_ghost = nullptr;
@@ -115,6 +121,10 @@ void free_tables(khb_batch* b)
     cudaFree(b->fix); b->fix = nullptr;
     cudaFree(b->counts); b->counts = nullptr;
     for (int x = 0; x < 5; ++x) { cudaFree(b->tiles[x]); b->tiles[x] = nullptr; }
+    for (int s = 0; s < 2; ++s) {
+        cudaFree(b->bound_dev[s]); b->bound_dev[s] = nullptr;
+        b->bound_off[s].clear(); b->bound_max[s].clear();
+    }
 }
 
 void drop_graph(khb_batch* b)
@@ -138,6 +148,8 @@ void flux_range(const Dims& d, int dir, int lo[3], int cnt[3])
         cnt[a] = hi - lo[a] + 1;
     }
 }
+
+int build_bound_tasks(khb_batch* b);
 
 // Descriptors and tile tables for the current tile shapes
 template <typename FT>
@@ -226,6 +238,8 @@ int build_tables(khb_batch* b)
         KHB_BCUDA(cudaMalloc((void**)&b->tiles[q], sizeof(int) * tiles[q].size()));
         KHB_BCUDA(cudaMemcpy(b->tiles[q], tiles[q].data(), sizeof(int) * tiles[q].size(), cudaMemcpyHostToDevice));
     }
+    int rc_b = build_bound_tasks(b);
+    if (rc_b) return rc_b;
     // copies from pageable memory may return before they land, and the caller's non-blocking
     // streams do not wait for the legacy stream: the tables must be on the device before any
     // batched kernel reads them
@@ -243,25 +257,52 @@ int build_tables(khb_batch* b)
 
 int rebuild(khb_batch* b) { return b->fp32 ? build_tables<float>(b) : build_tables<double>(b); }
 
-// The boundaries of blocks with physical or periodic faces (per-block launches of the context)
+// The boundaries of blocks with physical or periodic faces: each phase of the per-block boundary
+// launches (faces by direction, ghost P->U, periodic images) for all those blocks in one launch
 int enqueue_bounds(khb_batch* b, int s, cudaStream_t st)
 {
-    for (int x : b->needs_bounds) {
-        khb_ctx* c = b->ctx[x];
-        khb_fields Po, Uo;
-        if (s == 0) {
-            std::memset(&Po, 0, sizeof(Po)); std::memset(&Uo, 0, sizeof(Uo));
-            for (int p = 0; p < c->nv; ++p) {
-                Po.v[p] = c->stageP + (size_t)p * c->d.N;
-                Uo.v[p] = c->stageU + (size_t)p * c->d.N;
+    if (!b->bound_dev[s]) return KHB_OK;
+    for (int p = 0; p < BOUND_PHASES; ++p) {
+        const int n = b->bound_off[s][p + 1] - b->bound_off[s][p];
+        if (!n) continue;
+        LaunchCommon::bound_tasks(b->nv, b->bound_dev[s] + b->bound_off[s][p], n, b->bound_max[s][p], st);
+        KHB_BLAUNCHED(b, 1);
+    }
+    return KHB_OK;
+}
+
+// The boundary tasks of each stage output, uploaded once with the other tables
+int build_bound_tasks(khb_batch* b)
+{
+    for (int s = 0; s < 2; ++s) {
+        std::vector<BoundTask> phases[BOUND_PHASES];
+        for (int x : b->needs_bounds) {
+            khb_ctx* c = b->ctx[x];
+            khb_fields Po, Uo;
+            if (s == 0) {
+                std::memset(&Po, 0, sizeof(Po)); std::memset(&Uo, 0, sizeof(Uo));
+                for (int p = 0; p < c->nv; ++p) {
+                    Po.v[p] = c->stageP + (size_t)p * c->d.N;
+                    Uo.v[p] = c->stageU + (size_t)p * c->d.N;
+                }
+            } else {
+                Po = b->P[x]; Uo = b->U[x];
             }
-        } else {
-            Po = b->P[x]; Uo = b->U[x];
+            boundary_tasks(c, Po, Uo, phases);
         }
-        const int64_t l0 = c->launches;
-        int rc = ctx_boundaries(c, Po, Uo, st);
-        if (rc) return rc;
-        b->launches += c->launches - l0;
+        std::vector<BoundTask> all;
+        b->bound_off[s].assign(1, 0);
+        b->bound_max[s].clear();
+        for (int p = 0; p < BOUND_PHASES; ++p) {
+            long long mx = 0;
+            for (const BoundTask& t : phases[p]) mx = t.count > mx ? t.count : mx;
+            all.insert(all.end(), phases[p].begin(), phases[p].end());
+            b->bound_off[s].push_back((int)all.size());
+            b->bound_max[s].push_back(mx);
+        }
+        if (all.empty()) continue;
+        KHB_BCUDA(cudaMalloc((void**)&b->bound_dev[s], sizeof(BoundTask) * all.size()));
+        KHB_BCUDA(cudaMemcpy(b->bound_dev[s], all.data(), sizeof(BoundTask) * all.size(), cudaMemcpyHostToDevice));
     }
     return KHB_OK;
 }

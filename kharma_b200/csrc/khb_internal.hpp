@@ -5,6 +5,7 @@
 #include "khb_types.cuh"
 
 #include <string>
+#include <vector>
 
 #include <nvtx3/nvToolsExt.h>
 
@@ -92,6 +93,8 @@ int set_error(int code, const std::string& msg);
 // Flux fixes and ghost zones of one block, as khb_stage issues them
 int ctx_fix_flux(khb_ctx* ctx, cudaStream_t st);
 int ctx_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cudaStream_t st);
+// ctx_boundaries as tasks of k_bound_tasks, by phase (phases: BOUND_PHASES vectors)
+void boundary_tasks(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, std::vector<BoundTask>* phases);
 // B_CT stage pieces (khb_ct.cu): edge EMFs from the stage's face fluxes and primitives, and the face
 // update Bf_out = gam0 Bf_s + gam1 Bf_0 + beta dt dBf/dt
 int ct_emf(khb_ctx* ctx, const khb_fields& Ps, cudaStream_t st);

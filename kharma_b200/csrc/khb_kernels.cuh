@@ -885,14 +885,15 @@ __device__ __forceinline__ void inflow_fix(const ZoneGeom& G, const R gcov[4][4]
 // Parthenon's outflow/reflecting functions (unvendored) as KHARMA applies them: fluid primitives
 // and the conserved field; then the inflow check (boundaries.hpp:101-136).  NV = 10: the EMHD state,
 // whose scalar primitives q~, dP~ (slots 8, 9) are copied as the density is.
+// One zone (thread t of the face's ng x cnt_a x cnt_k enumeration) of k_bc
 template <int NV>
-__global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int face,
-                     int lo_a, int cnt_a, int lo_k, int cnt_k)
+__device__ __forceinline__ void bc_zone(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                                        const khb_fields& U, int face, int lo_a, int cnt_a, int lo_k, int cnt_k,
+                                        long long t)
 {
     const int bdir = face / 2 + 1;
     const bool inner = (face % 2) == 0;
     const int ng = (bdir == 1) ? d.is : ((bdir == 2) ? d.js : d.ks);
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ng*cnt_a*cnt_k) return;
     const int gidx = (int)(t % ng);
     const long long r = t / ng;
@@ -952,6 +953,12 @@ __global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int
 #pragma unroll
     for (int p = 0; p < 5; ++p) P.v[p][c] = Pz[p];
 }
+template <int NV>
+__global__ void k_bc(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, int face,
+                     int lo_a, int cnt_a, int lo_k, int cnt_k)
+{
+    bc_zone<NV>(d, g, ph, P, U, face, lo_a, cnt_a, lo_k, cnt_k, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // Ghost zones of one (j, i) plane, enumerated without the interior: the rows below js, the zones
 // left and right of the interior in rows js..je, the rows above je.  Returns false past the end.
@@ -986,10 +993,10 @@ __host__ __device__ inline unsigned plane_ghost_count(const Dims& d)
 // pfaces (nonzero): a zone is taken only if it lies past a face whose bit is set (the boundary
 // domains inner_x1 ... outer_x3 of those faces; the exchanged ghost zones keep their values)
 template <int NV>
-__global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, khb_fields Bf, int ct_mask,
-                             int kplanes, int pfaces)
+__device__ __forceinline__ void ghost_ptou_zone(const Dims& d, const DevGeom& g, const Phys& ph, const khb_fields& P,
+                                                const khb_fields& U, const khb_fields& Bf, int ct_mask, int kplanes,
+                                                int pfaces, unsigned t)
 {
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     int j, i, k;
     if (kplanes) {
         const unsigned plane = (unsigned)(d.n1 * d.n2);
@@ -1038,17 +1045,23 @@ __global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_field
 #pragma unroll
     for (int p = 0; p < NV; ++p) U.v[p][c] = Uz[p];
 }
+template <int NV>
+__global__ void k_ghost_ptou(Dims d, DevGeom g, Phys ph, khb_fields P, khb_fields U, khb_fields Bf, int ct_mask,
+                             int kplanes, int pfaces)
+{
+    ghost_ptou_zone<NV>(d, g, ph, P, U, Bf, ct_mask, kplanes, pfaces, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // Periodic images: every zone outside the interior in a periodic direction copies all variables
 // of P and U from its image (wrapping only the periodic directions).
 // Launched over the zones outside the interior only: the k ghost planes whole, then the X1/X2
 // ghost zones of each interior plane.
 template <int NV>
-__global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
+__device__ __forceinline__ void periodic_zone(const Dims& d, const khb_fields& P, const khb_fields& U, int pmask,
+                                              unsigned u)
 {
     const unsigned plane = (unsigned)(d.n1 * d.n2);
     const unsigned kg = (unsigned)(d.n3 - (d.ke - d.ks + 1));     // k ghost planes
-    unsigned u = blockIdx.x * blockDim.x + threadIdx.x;
     int k, j, i;
     if (u < kg * plane) {
         const unsigned kp = u / plane, r = u - kp * plane;
@@ -1077,6 +1090,25 @@ __global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
         if (NV > 8 && !P.v[p]) continue;       // EMHD slots that are not evolved
         P.v[p][t] = P.v[p][s]; U.v[p][t] = U.v[p][s];
     }
+}
+template <int NV>
+__global__ void k_periodic(Dims d, khb_fields P, khb_fields U, int pmask)
+{
+    periodic_zone<NV>(d, P, U, pmask, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The boundary work of many blocks, one launch per phase of launch_boundaries: blockIdx.y picks the
+// task (one block's face, ghost P->U pass or periodic images), blockIdx.x * blockDim.x + threadIdx.x
+// the zone of its enumeration; the tasks of one phase are different blocks' or disjoint regions
+template <int NV>
+__global__ void __launch_bounds__(128) k_bound_tasks(const BoundTask* __restrict__ tasks)
+{
+    const BoundTask& T = tasks[blockIdx.y];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T.count) return;
+    if (T.kind == BOUND_BC) bc_zone<NV>(T.d, T.g, T.ph, T.P, T.U, T.face, T.lo_a, T.cnt_a, T.lo_k, T.cnt_k, t);
+    else if (T.kind == BOUND_GHOST_PTOU) ghost_ptou_zone<NV>(T.d, T.g, T.ph, T.P, T.U, T.Bf, 0, T.kplanes, T.pfaces, (unsigned)t);
+    else periodic_zone<NV>(T.d, T.P, T.U, T.pmask, (unsigned)t);
 }
 
 // The ghost shell (every zone outside the interior) of a stage's input copied to its output: the
@@ -1915,6 +1947,14 @@ void LaunchCommon::ghost_ptou(int nv, const Dims& d, const DevGeom& g, const Phy
     if (Bf) for (int x = 0; x < 3; ++x) F.v[x] = Bf->v[x];
     if (nv == 8) k_ghost_ptou<8><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes, pfaces);
     else k_ghost_ptou<5><<<blocks_for(tot, 128), 128, 0, st>>>(d, g, ph, P, U, F, ct_mask, kplanes, pfaces);
+}
+
+void LaunchCommon::bound_tasks(int nv, const BoundTask* tasks, int ntasks, long long max_count, cudaStream_t st)
+{
+    if (ntasks <= 0 || max_count <= 0) return;
+    const dim3 grid(blocks_for(max_count, 128), (unsigned)ntasks);
+    if (nv == 8) k_bound_tasks<8><<<grid, 128, 0, st>>>(tasks);
+    else k_bound_tasks<5><<<grid, 128, 0, st>>>(tasks);
 }
 
 void LaunchCommon::periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st)

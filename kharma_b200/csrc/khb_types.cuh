@@ -163,6 +163,23 @@ struct BatchBlock {
     unsigned tile0c[4];        // first tile of each kind in the fused plan's combined table (x1-x3 faces, shell)
 };
 
+// One launch of launch_boundaries (a block's physical face, its ghost P->U pass or its periodic
+// images) as a task of k_bound_tasks, which runs a phase's tasks of many blocks in one launch
+enum { BOUND_BC = 0, BOUND_GHOST_PTOU = 1, BOUND_PERIODIC = 2 };
+enum { BOUND_PHASES = 8 };         // X1 faces, X2 faces, corner fix, ghost P->U, its X3 planes, X3 faces,
+                                   // P->U of the X3 ghost planes, periodic images
+struct BoundTask {
+    Dims d;
+    DevGeom g;
+    Phys ph;
+    khb_fields P, U, Bf;           // Bf: all NULL (no face field)
+    int kind;
+    int face, lo_a, cnt_a, lo_k, cnt_k;     // BOUND_BC
+    int kplanes, pfaces;                    // BOUND_GHOST_PTOU
+    int pmask;                              // BOUND_PERIODIC
+    long long count;                        // zones (threads) of the task
+};
+
 // What the batched fixup reads of each block (independent of the flux precision)
 struct FixupBlock {
     Dims d;
@@ -227,6 +244,8 @@ struct LaunchCommon {
                            const khb_fields& U, cudaStream_t st, const khb_fields* Bf = nullptr, int ct_mask = 0,
                            int kplanes = 0, int pfaces = 0);
     static void periodic(int nv, const Dims& d, const khb_fields& P, const khb_fields& U, int pmask, cudaStream_t st);
+    // ntasks tasks of one boundary phase in one launch; max_count: the largest task's zone count
+    static void bound_tasks(int nv, const BoundTask* tasks, int ntasks, long long max_count, cudaStream_t st);
     static void ghost_copy(int nv, const Dims& d, const khb_fields& Pin, const khb_fields& Uin, const khb_fields& Pout,
                            const khb_fields& Uout, cudaStream_t st);
     static void batch_ghost_copy(int nv, const FixupBlock* blocks, int nblocks, int stage, cudaStream_t st);
