@@ -446,6 +446,62 @@ def batching(steps=20, warm=3):
         out[prec] = r
         del b
         torch.cuda.empty_cache()
+    out["smr_mesh"] = batching_mesh(steps, warm)
+    return out
+
+
+def batching_mesh(steps=20, warm=3):
+    """The batching form's problem on a conforming three-level SMR mesh with the ghost exchange and
+    flux correction between blocks (Parthenon meshes have one block size): Bondi in spherical KS
+    (a = 0, MKS), r in [3, 30], 4 x 4 x 2 root blocks of 32^3, the central 2 x 2 (x 2) roots refined
+    and the 2 x 2 (x 4) level-1 blocks away from level 0 refined again (24 + 48 + 128 = 200 blocks),
+    outflow x1, reflecting x2, periodic x3, WENO5, LLF, FP64, the kharma driver's exchange; the
+    autotuned CUDA-graph step against the blocks stepped one after another with khb_step (no
+    exchange, so a lower bound for a per-block path).  CUDA events on the batch's stream."""
+    import numpy as np
+    import torch
+    from kharma_b200 import problems
+    from kharma_b200.block import build_geometry
+    from kharma_b200.mesh import SMRMesh, smr_batch
+    from kharma_b200.spec import bondi_spec
+
+    ks = bondi_spec(32, 32, 32, float(np.log(3.0)), float(np.log(30.0)), 0.0, 1.0, 0.0, 2 * np.pi,
+                    bc=("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"))
+    refine = ([(i, j, k) for i in (1, 2) for j in (1, 2) for k in (0, 1)] +
+              [(1, (i, j, k)) for i in (3, 4) for j in (3, 4) for k in range(4)])
+    mesh = SMRMesh(ks, (4, 4, 2), (32, 32, 32), refine=refine)
+    b = smr_batch(mesh, lambda sp: problems.bondi(sp, build_geometry(sp)))
+    dt = 1e-3
+
+    def timed(fn, n):
+        with torch.cuda.stream(b.torch_stream):
+            for _ in range(warm):
+                fn()
+            torch.cuda.synchronize()
+            l0 = b.launch_count()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(b.torch_stream)
+            for _ in range(n):
+                fn()
+            e1.record(b.torch_stream)
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, (b.launch_count() - l0) / n
+
+    per_block, _ = timed(lambda: b.step_per_block(dt), max(3, steps // 4))
+    with torch.cuda.stream(b.torch_stream):
+        tune, pers = b.autotune(3)
+    ms, launches = timed(lambda: b.step_graph(dt), steps)
+    out = {"workload": f"Bondi in spherical KS (a=0, MKS), r 3-30, 3-level SMR mesh of {len(mesh.blocks)} blocks of "
+                       f"32^3 (24 + 48 + 128), {mesh.zones:,} zones, WENO5, LLF, FP64, outflow/reflecting/periodic "
+                       f"faces, kharma driver exchange",
+           "ghost_entries": int(len(mesh.tables()[0])),
+           "graph_ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0), "launches_per_step": launches,
+           "autotune": {"planes_per_cta": tune, "persistent": pers, "plan": b.plan()},
+           "per_block_no_exchange_ms_per_step": per_block,
+           "speedup_graph_vs_per_block": per_block / ms}
+    del b
+    torch.cuda.empty_cache()
     return out
 
 
