@@ -409,8 +409,8 @@ int khb_ct_ghost_from_faces(khb_ctx* ctx, const khb_fields* P, const khb_fields*
 
 /* ---------------------------------------------------------------------------------------------
  * SMR meshes of B_CT blocks (KHARMA's default field transport on multilevel meshes,
- * kharma.cpp:376-395): tables from kharma_b200/ctmesh.py.  Blocks: FP64, Cartesian Minkowski,
- * one shape, 2D or 3D; every face an exchange face or an outflow/reflecting domain face, which the
+ * kharma.cpp:376-395): tables from kharma_b200/ctmesh.py.  Blocks: FP64, any coordinates (the
+ * operators act on the native grid; faces, fluxes and EMFs carry sqrt(-g)), one shape, 2D or 3D; every face an exchange face or an outflow/reflecting domain face, which the
  * block applies with khb_ct_boundaries after the exchange (no table entry reaches past it).  Per stage: khb_ct_stage_fluxes on every
  * block, khb_ctmesh_correct (the fluid fluxes of coarse faces on a fine-coarse boundary become the
  * mean of the fine fluxes, and coarse edge EMFs that coincide with fine edges the mean of the fine

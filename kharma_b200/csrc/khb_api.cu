@@ -222,6 +222,9 @@ int launch_boundaries(khb_ctx* ctx, const khb_fields& P, const khb_fields& U, cu
         if (d.ndim >= 2 && (phys_face(d.bc[2]) || phys_face(d.bc[3]))) ct_mask |= 2;
         if (d.ndim >= 3 && (phys_face(d.bc[4]) || phys_face(d.bc[5]))) ct_mask |= 4;
         if (!ct_mask) Bf = nullptr;
+        // a block of a mesh: every zone past a physical face takes B from its faces, also where it lies
+        // in the ghost rows the exchange filled (B_CT::BlockUtoP over the face's boundary domain)
+        else if (exch) ct_mask = 7;
     }
     if (Bf) {
         const int rc = khb::ct_face_boundaries(ctx, *Bf, st);

@@ -14,8 +14,10 @@
 // updated conserved fluid variables and the seed primitives by the same entries, between the update
 // and the inversion, then inverts each ghost zone like the interior:
 //   k_ctm_cell_cons    ghost-zone U (fluid) and seed P (fluid) by the entries
-//   k_ctm_ghost_cell   B and U_B from the faces, inversion, floors, U = U(P) (the zone pass's cell half)  All blocks have one shape, FP64 fluxes and the Minkowski metric of a
-// uniform Cartesian grid (areas and lengths are products of the zone widths).
+//   k_ctm_ghost_cell   B and U_B from the faces, inversion, floors, U = U(P) (the zone pass's cell half)
+// All blocks have one shape and FP64 fluxes, in any coordinate system: the face field holds
+// sqrt(-g) B^i and the EMFs and fluxes their sqrt(-g)-weighted values, so that, as in Parthenon's
+// operators, areas and lengths are products of the native zone widths.
 #include "khb_internal.hpp"
 #include "khb_kernels.cuh"
 
@@ -414,8 +416,6 @@ int khb_ctmesh_create(khb_ctx* const* ctxs, int nblocks, const int32_t* cell, in
         if (!c->ph.ct_scheme || c->nv != 8)
             return ctm_fail(KHB_ERR_UNSUPPORTED, "khb_ctmesh_create: B_CT MHD blocks (nvar 8) only");
         if (c->fp32) return ctm_fail(KHB_ERR_UNSUPPORTED, "khb_ctmesh_create: FP64 blocks only");
-        if (!c->ph.cart_minkowski)
-            return ctm_fail(KHB_ERR_UNSUPPORTED, "khb_ctmesh_create: Cartesian Minkowski blocks only");
         if (c->d.n1 != c0->d.n1 || c->d.n2 != c0->d.n2 || c->d.n3 != c0->d.n3 || c->d.ndim != c0->d.ndim)
             return ctm_fail(KHB_ERR_ARG, "khb_ctmesh_create: blocks of one shape only");
         if (c->d.ndim < 2) return ctm_fail(KHB_ERR_UNSUPPORTED, "khb_ctmesh_create: 2D and 3D blocks only");

@@ -1,5 +1,6 @@
 """Static mesh refinement of magnetized blocks with a face-centred field (B_CT): the tables and the
-driver of an SMR mesh of Cartesian Minkowski MHD blocks stepped with B_CT.
+driver of an SMR mesh of MHD blocks stepped with B_CT (any coordinate system: the operators act on the
+native grid, the faces holding sqrt(-g) B^i).
 
 KHARMA defaults multilevel meshes to B_CT (kharma.cpp:376-395): the field lives on faces and its
 divergence stays at round-off only if every block sees the same field across a fine-coarse

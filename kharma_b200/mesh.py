@@ -18,8 +18,8 @@ the updated conserved variables with the primitives as the inversion's seeds, th
 inverted, floored and given U = U(P) like the interior (kharma_step.cpp:209-236); every block has the
 same zone count,
 as Parthenon requires, and the fine blocks cover whole coarse blocks (2:1 in each active direction,
-neighbouring blocks at most one level apart).  Scope: hydro blocks (5 variables, any coordinates:
-the operators act on the uniform native grid) through the batch,
+neighbouring blocks at most one level apart).  Scope (any coordinates: the operators act on the
+uniform native grid): hydro blocks (5 variables) through the batch,
 MHD blocks with B_CT through kharma_b200/ctmesh.py; any number of levels; each direction periodic, or
 outflow/reflecting on the domain faces (a block on such a face keeps it; ghost entries stop at it and
 the block's boundary condition fills what lies beyond, after the exchange; refined blocks keep a
@@ -56,7 +56,7 @@ class MeshBlock:
 class SMRMesh:
     """Root grid of nb = (nb1, nb2, nb3) blocks of nx = (nx1, nx2, nx3) zones over `base`'s domain
     (a BlockSpec supplying the physics options, the coordinates and the domain extent in native
-    coordinates: hydro blocks in any coordinate system, or Cartesian Minkowski MHD blocks with B_CT.
+    coordinates: hydro blocks, or MHD blocks with B_CT, in any coordinate system.
     Parthenon's operators act on the uniform grid of native coordinates, so the tables are the same
     in every coordinate system; each block carries its own metric); a block
     named in `refine` is replaced by its 2^ndim children one level up.  Entries are root locations
@@ -64,8 +64,7 @@ class SMRMesh:
     level); refinements apply recursively, coarsest first."""
 
     def __init__(self, base: BlockSpec, nb, nx, refine=()):
-        assert base.nvar == 5 or (base.cart_minkowski and base.b_ct != "none"), \
-            "SMR: hydro blocks, or Cartesian Minkowski MHD blocks with B_CT"
+        assert base.nvar == 5 or base.b_ct != "none", "SMR: hydro blocks, or MHD blocks with B_CT"
         self.base = base
         self.nb = tuple(nb)
         self.nx = tuple(nx)
