@@ -7,6 +7,8 @@ launches per stage); graph replay and any tile shape or plan chosen by the autot
 nothing; autotuning leaves the state alone; and each block matches the CPU oracle stepped with the
 same ghost inputs to 1e-12 per variable (max |gpu - oracle| <= 1e-12 max |oracle|), flags exactly.
 The mesh here has the production block counts (8 + 48 + 128) with 16^3, 8^3 and 4^3 blocks.
+Blocks with physical and periodic faces (FM torus, Bondi, a periodic box), whose boundary work the
+batch runs as one launch per boundary phase, also step bitwise as khb_step on each block.
 """
 import numpy as np
 import pytest
@@ -102,3 +104,39 @@ def test_fused_plan_three_launches_per_stage(persistent):
         b.step_graph(dt)
     assert_same(a, b)
     assert (b.launch_count() - l0) / len(DTS) == 6
+
+
+@pytest.mark.parametrize("plan", [0, 1])
+def test_physical_and_periodic_faces_equal_per_block(plan):
+    """Blocks with outflow, reflecting and periodic faces, whose boundary work (faces by direction,
+    ghost P->U, periodic images) the batch runs as one launch per phase over all of them, step
+    bitwise as khb_step on each block: two FM torus blocks of different sizes (flux-CT MHD: outflow
+    x1 with the inflow checks, reflecting x2, periodic x3), and a hydro batch of a Bondi block
+    (outflow x1, reflecting x2, periodic x3) beside a periodic Cartesian block."""
+    from kharma_b200.block import build_geometry
+    from kharma_b200.spec import BlockSpec, bondi_spec, torus_spec
+
+    def pair(specs, inits):
+        out = []
+        for _ in range(2):
+            bb = Batch(specs, init=None)
+            with torch.cuda.stream(bb.torch_stream):
+                for blk, P in zip(bb.blocks, inits):
+                    blk.set_prims(P)
+            out.append(bb)
+        return out
+
+    torus = [torus_spec(32, 24, 16), torus_spec(24, 16, 8)]
+    bondi = bondi_spec(16, 16, 8, float(np.log(3.0)), float(np.log(30.0)), recon="linear_mc",
+                       bc=("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"))
+    box = BlockSpec(nx1=16, nx2=8, nx3=8, x1min=0., x1max=1., x2min=0., x2max=1., x3min=0., x3max=1., gam=5. / 3.,
+                    nvar=5, recon="linear_mc")
+    cases = [(torus, [problems.fm_torus(s, build_geometry(s), seed=3 + n) for n, s in enumerate(torus)]),
+             ([bondi, box], [problems.bondi(bondi, build_geometry(bondi)), problems.entropy_wave(box, amp=0.1)])]
+    for specs, inits in cases:
+        a, b = pair(specs, inits)
+        a.set_plan(plan)
+        for dt in (1e-3, 2e-3):
+            a.step(dt)
+            b.step_per_block(dt)
+        assert_same(a, b)
