@@ -13,6 +13,8 @@ a periodic box, and one-level meshes with outflow or reflecting domain faces.
 * The kharma driver's exchange (conserved variables and inversion seeds, the ghost zones inverted
   like the interior): ghost zones equal the oracle's inversion of the restated conserved state from
   the restated seed; one level steps bitwise as one block; conservation and uniformity as above.
+* MKS (spherical KS) meshes: exchange bitwise as restated, one level as one block to 1e-9.
+* The FP32-flux form on a mesh stays within 1e-5 relative L1 density of the FP64 mesh.
 """
 import dataclasses
 import importlib.util
@@ -311,3 +313,24 @@ def test_mks_one_level_steps_as_one_block(conserved):
     worst = float(np.max(diff / scale))
     print("MKS one level vs one block: per-variable relative difference", diff / scale)
     assert worst <= 1e-9
+
+
+@pytest.mark.parametrize("conserved", [False, True])
+def test_fp32_flux_mesh_close_to_fp64(conserved):
+    """The FP32-flux form on a two-level mesh (the flux correction and the exchange on FP32 fluxes):
+    after 20 steps its density is within 1e-5 relative L1 of the FP64 mesh's, with either exchange."""
+    import dataclasses
+    out = {}
+    for prec in ("fp64", "fp32_flux"):
+        base_ = dataclasses.replace(base(2), precision=prec)
+        mesh = SMRMesh(base_, (2, 2, 1), (16, 16, 1), refine=[(0, 0, 0)])
+        b = smr_batch(mesh, lambda s: random_smooth(s, 5), conserved=conserved)
+        dt = 0.2 * min(blk.spec.dx[0] for blk in mesh.blocks)
+        for _ in range(20):
+            b.step(dt)
+        torch.cuda.synchronize()
+        out[prec] = [blk.P.cpu().numpy()[(0,) + mb.spec.interior] for blk, mb in zip(b.blocks, mesh.blocks)]
+    num = sum(float(np.abs(x - y).sum()) for x, y in zip(out["fp32_flux"], out["fp64"]))
+    den = sum(float(np.abs(y).sum()) for y in out["fp64"])
+    print("FP32-flux mesh vs FP64 mesh: relative L1 density difference", num / den)
+    assert 0 < num / den < 1e-5
