@@ -555,9 +555,10 @@ int khb_batch_autotune(khb_batch* batch, int reps, int32_t* kz_out, int32_t* per
  * stage for all blocks (counter reset, faces per direction, ghost-shell copy, update half, cell
  * half, fixups: 8 launches per stage for blocks with exchange faces); 1 fuses them into three (all
  * faces of all directions with the resets and ghost-shell copies, the whole zone pass, fixups).
- * Blocks with physical faces add their per-block flux fixes and one launch per boundary phase for
- * all of them (faces by direction, corner fix, ghost P->U, X3 planes, periodic images), SMR meshes
- * the flux correction and ghost exchange, in either plan.  A captured graph is captured again. */
+ * Blocks with physical faces add one launch for all their flux fixes and one launch per boundary
+ * phase for all of them (faces by direction, corner fix, ghost P->U, X3 planes, periodic images),
+ * SMR meshes the flux correction and ghost exchange, in either plan.  A captured graph is captured
+ * again. */
 int khb_batch_set_plan(khb_batch* batch, int plan);
 int khb_batch_get_plan(khb_batch* batch, int32_t* plan);
 

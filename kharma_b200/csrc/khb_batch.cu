@@ -27,9 +27,9 @@ struct khb_batch {
     int persistent = 0;                            // 1: grid of (SMs x resident CTAs), CTAs loop over tiles
     // launch plan: 0 one launch per kernel per stage (counter reset, faces per direction, ghost-shell
     // copy, update half, cell half, fixups); 1 fused: three launches per stage (all faces with the
-    // resets and shell copies, the whole zone pass, fixups), plus the per-block flux fixes of
-    // physical faces, one launch per boundary phase for all blocks with physical or periodic faces,
-    // and the mesh kernels of SMR meshes
+    // resets and shell copies, the whole zone pass, fixups), plus one launch for the flux fixes of
+    // all blocks with physical faces, one launch per boundary phase for all blocks with physical or
+    // periodic faces, and the mesh kernels of SMR meshes
     int plan = 0;
     int nsm = 0;
     // device tables
@@ -48,6 +48,9 @@ struct khb_batch {
     // the boundary work of those blocks per stage output (0: stage 1's, 1: the state), as tasks of
     // k_bound_tasks grouped by phase: [bound_off[s][p], bound_off[s][p + 1]) in bound_dev[s]
     BoundTask* bound_dev[2] = {nullptr, nullptr};
+    // the flux fixes of the blocks in needs_fix_flux, as tasks of k_fix_tasks (FixTask<FT>[n_fix])
+    void* fix_dev = nullptr;
+    int n_fix = 0, fix_max = 0;
     std::vector<int> bound_off[2];
     std::vector<long long> bound_max[2];
     bool any_exchange = false;                     // some block carries its ghost shell over
@@ -125,6 +128,8 @@ void free_tables(khb_batch* b)
         cudaFree(b->bound_dev[s]); b->bound_dev[s] = nullptr;
         b->bound_off[s].clear(); b->bound_max[s].clear();
     }
+    cudaFree(b->fix_dev); b->fix_dev = nullptr;
+    b->n_fix = 0; b->fix_max = 0;
 }
 
 void drop_graph(khb_batch* b)
@@ -150,6 +155,7 @@ void flux_range(const Dims& d, int dir, int lo[3], int cnt[3])
 }
 
 int build_bound_tasks(khb_batch* b);
+template <typename FT> int build_fix_tasks(khb_batch* b);
 
 // Descriptors and tile tables for the current tile shapes
 template <typename FT>
@@ -240,6 +246,7 @@ int build_tables(khb_batch* b)
     }
     int rc_b = build_bound_tasks(b);
     if (rc_b) return rc_b;
+    if ((rc_b = build_fix_tasks<FT>(b))) return rc_b;
     // copies from pageable memory may return before they land, and the caller's non-blocking
     // streams do not wait for the legacy stream: the tables must be on the device before any
     // batched kernel reads them
@@ -307,14 +314,46 @@ int build_bound_tasks(khb_batch* b)
     return KHB_OK;
 }
 
+// The flux fixes of all blocks with physical faces that need them, in one launch
+template <typename FT>
 int enqueue_fix_flux(khb_batch* b, cudaStream_t st)
 {
+    if (!b->n_fix) return KHB_OK;
+    Launch<FT>::fix_tasks(b->nv, (const FixTask<FT>*)b->fix_dev, b->n_fix, b->fix_max, st);
+    KHB_BLAUNCHED(b, 1);
+    return KHB_OK;
+}
+
+// The fixes the per-block path makes (launch_fix_flux: polar x2 faces, then x1 inflow checks), as tasks
+template <typename FT>
+int build_fix_tasks(khb_batch* b)
+{
+    std::vector<FixTask<FT>> tasks;
     for (int x : b->needs_fix_flux) {
-        const int64_t l0 = b->ctx[x]->launches;
-        int rc = ctx_fix_flux(b->ctx[x], st);
-        if (rc) return rc;
-        b->launches += b->ctx[x]->launches - l0;
+        khb_ctx* c = b->ctx[x];
+        const Dims& d = c->d;
+        FixTask<FT> t;
+        std::memset((void*)&t, 0, sizeof(t));
+        t.d = d; t.ph = c->ph;
+        t.F1 = (FT*)c->F[0]; t.F2 = (FT*)c->F[1]; t.F3 = (FT*)c->F[2];
+        const int nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
+        if (d.ndim >= 2 && (c->ph.zero_polar_flux || (c->nv > 5 && c->ph.fix_polar_flux))) {
+            for (int face = 2; face <= 3; ++face) {
+                if (!phys_face(d.bc[face])) continue;
+                t.x1 = 0; t.inner = face == 2; t.count = (d.ie - d.is + 3) * nk;
+                tasks.push_back(t);
+            }
+        }
+        const int nj = (d.ndim > 1) ? d.je - d.js + 3 : 1;
+        if (c->ph.check_inflow_in && phys_face(d.bc[0])) { t.x1 = 1; t.inner = 1; t.count = nj * nk; tasks.push_back(t); }
+        if (c->ph.check_inflow_out && phys_face(d.bc[1])) { t.x1 = 1; t.inner = 0; t.count = nj * nk; tasks.push_back(t); }
     }
+    b->n_fix = (int)tasks.size();
+    b->fix_max = 0;
+    for (const auto& t : tasks) b->fix_max = t.count > b->fix_max ? t.count : b->fix_max;
+    if (tasks.empty()) return KHB_OK;
+    KHB_BCUDA(cudaMalloc(&b->fix_dev, sizeof(FixTask<FT>) * tasks.size()));
+    KHB_BCUDA(cudaMemcpy(b->fix_dev, tasks.data(), sizeof(FixTask<FT>) * tasks.size(), cudaMemcpyHostToDevice));
     return KHB_OK;
 }
 
@@ -329,7 +368,7 @@ int enqueue_stage_fused(khb_batch* b, int s, cudaStream_t st)
                                s == 1 ? b->word : nullptr, st);
     KHB_BLAUNCHED(b, 1);
     int rc;
-    if ((rc = enqueue_fix_flux(b, st))) return rc;
+    if ((rc = enqueue_fix_flux<FT>(b, st))) return rc;
     if (b->n_flux) {
         Launch<FT>::mesh_flux(b->nv, desc, b->mesh_flux, b->n_flux, st);
         KHB_BLAUNCHED(b, 1);
@@ -364,7 +403,7 @@ int enqueue_stage(khb_batch* b, int s, cudaStream_t st)
         KHB_BLAUNCHED(b, 1);
     }
     int rc;
-    if ((rc = enqueue_fix_flux(b, st))) return rc;
+    if ((rc = enqueue_fix_flux<FT>(b, st))) return rc;
     if (b->n_flux) {
         Launch<FT>::mesh_flux(b->nv, desc, b->mesh_flux, b->n_flux, st);
         KHB_BLAUNCHED(b, 1);

@@ -273,11 +273,10 @@ k_flux(Dims d, DevGeom g, Phys ph, khb_fields P, FT* __restrict__ F, FT* __restr
 // (boundaries.cpp:611-690) for inflow checks on X1 faces and zero polar fluxes on X2 faces.
 // One thread per (k, i) of an X2 face or (k, j) of an X1 face; the halo is one zone.
 template <int NV, typename FT>
-__global__ void k_fix_flux_x2(Dims d, Phys ph, FT* F1, FT* F2, FT* F3, int inner)
+__device__ __forceinline__ void fix_x2_zone(const Dims& d, const Phys& ph, FT* F1, FT* F2, FT* F3, int inner, int t)
 {
     const int ni = d.ie - d.is + 3;
     const int nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ni*nk) return;
     const int i = d.is - 1 + t % ni;
     const int k = (d.ndim > 2) ? d.ks - 1 + t / ni : d.ks;
@@ -298,12 +297,16 @@ __global__ void k_fix_flux_x2(Dims d, Phys ph, FT* F1, FT* F2, FT* F3, int inner
 #pragma unroll
         for (int p = 0; p < NV; ++p) F2[p*N + c] = (FT)0;
 }
+template <int NV, typename FT>
+__global__ void k_fix_flux_x2(Dims d, Phys ph, FT* F1, FT* F2, FT* F3, int inner)
+{
+    fix_x2_zone<NV, FT>(d, ph, F1, F2, F3, inner, blockIdx.x * blockDim.x + threadIdx.x);
+}
 template <typename FT>
-__global__ void k_fix_flux_x1(Dims d, FT* F1, int inner)
+__device__ __forceinline__ void fix_x1_zone(const Dims& d, FT* F1, int inner, int t)
 {
     const int nj = (d.ndim > 1) ? d.je - d.js + 3 : 1;
     const int nk = (d.ndim > 2) ? d.ke - d.ks + 3 : 1;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nj*nk) return;
     const int j = (d.ndim > 1) ? d.js - 1 + t % nj : d.js;
     const int k = (d.ndim > 2) ? d.ks - 1 + t / nj : d.ks;
@@ -311,6 +314,21 @@ __global__ void k_fix_flux_x1(Dims d, FT* F1, int inner)
     const long long c = ((long long)k*d.n2 + j)*d.n1 + i;
     FT& f = F1[c];
     f = inner ? kmin(f, (FT)0) : kmax(f, (FT)0);
+}
+template <typename FT>
+__global__ void k_fix_flux_x1(Dims d, FT* F1, int inner)
+{
+    fix_x1_zone<FT>(d, F1, inner, blockIdx.x * blockDim.x + threadIdx.x);
+}
+// The flux fixes of every block of a batch in one launch: blockIdx.y picks a block's fix (its faces
+// and slots are disjoint from every other fix's)
+template <int NV, typename FT>
+__global__ void __launch_bounds__(128) k_fix_tasks(const FixTask<FT>* __restrict__ tasks)
+{
+    const FixTask<FT>& T = tasks[blockIdx.y];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (T.x1) fix_x1_zone<FT>(T.d, T.F1, T.inner, t);
+    else fix_x2_zone<NV, FT>(T.d, T.ph, T.F1, T.F2, T.F3, T.inner, t);
 }
 
 // ===================================================================================== zone pass
@@ -1642,6 +1660,15 @@ void Launch<FT>::fix_flux_x2(int nv, const Dims& d, const Phys& ph, FT* F1, FT* 
     if (nv == 10) k_fix_flux_x2<10, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
     else if (nv == 8) k_fix_flux_x2<8, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
     else k_fix_flux_x2<5, FT><<<nb, 128, 0, st>>>(d, ph, F1, F2, F3, inner);
+}
+
+template <typename FT>
+void Launch<FT>::fix_tasks(int nv, const FixTask<FT>* tasks, int ntasks, int max_count, cudaStream_t st)
+{
+    if (ntasks <= 0 || max_count <= 0) return;
+    const dim3 grid(blocks_for(max_count, 128), (unsigned)ntasks);
+    if (nv == 8) k_fix_tasks<8, FT><<<grid, 128, 0, st>>>(tasks);
+    else k_fix_tasks<5, FT><<<grid, 128, 0, st>>>(tasks);
 }
 
 template <typename FT>

@@ -180,6 +180,19 @@ struct BoundTask {
     long long count;                        // zones (threads) of the task
 };
 
+// One block's flux fix (a polar x2 face or an x1 inflow check) as a task of k_fix_tasks
+template <typename FT>
+struct FixTask {
+    Dims d;
+    Phys ph;
+    FT* F1;
+    FT* F2;
+    FT* F3;
+    int x1;                        // 1: the x1 inflow fix, 0: the polar x2 fix
+    int inner;
+    int count;                     // zones (threads) of the fix
+};
+
 // What the batched fixup reads of each block (independent of the flux precision)
 struct FixupBlock {
     Dims d;
@@ -201,6 +214,8 @@ struct Launch {
                      const khb_fields& P, FT* F, FT* ctop, const int lo[3], const int cnt[3], cudaStream_t st);
     static void fix_flux_x2(int nv, const Dims& d, const Phys& ph, FT* F1, FT* F2, FT* F3, int inner, cudaStream_t st);
     static void fix_flux_x1(const Dims& d, FT* F1, int inner, cudaStream_t st);
+    // the flux fixes of many blocks in one launch (max_count: the largest task's zone count)
+    static void fix_tasks(int nv, const FixTask<FT>* tasks, int ntasks, int max_count, cudaStream_t st);
     static void zone(int nv, const Dims& d, const DevGeom& g, const Phys& ph, const ZoneArgs<FT>& a, cudaStream_t st);
     static void flux_ct(const Dims& d, FT* F1, FT* F2, FT* F3, FT* emf, cudaStream_t st);
     static void copy_flux(long long N, int nv, const FT* F, const FT* ctop, const khb_fields& out, double* ctop_out,
