@@ -77,10 +77,16 @@ class SMRMesh:
         self.periodic = tuple(d >= self.ndim or base.bc[2 * d] == "periodic" for d in range(3))
         for d in range(self.ndim):
             if not self.periodic[d]:
-                assert base.bc[2 * d] in ("outflow", "reflecting") and base.bc[2 * d + 1] in ("outflow", "reflecting"), \
-                    "SMR: domain faces periodic, outflow or reflecting"
+                ok = ("outflow", "reflecting") + (("transmitting",) if d == 1 else ())
+                assert base.bc[2 * d] in ok and base.bc[2 * d + 1] in ok, \
+                    "SMR: domain faces periodic, outflow or reflecting (x2: or transmitting)"
             else:
                 assert base.bc[2 * d + 1] == "periodic", "SMR: a periodic direction is periodic on both faces"
+        if "transmitting" in base.bc[2:4]:
+            # the mirror zone lies half-way round in x3 inside the block: the blocks on the poles
+            # (never refined) span all of a periodic x3
+            assert self.ndim == 3 and self.periodic[2] and self.nb[2] == 1 and nx[2] % 2 == 0, \
+                "SMR: transmitting x2 faces need 3D root blocks spanning all of a periodic x3 (even nx3)"
         lo = (base.x1min, base.x2min, base.x3min)
         hi = (base.x1max, base.x2max, base.x3max)
         self.lo, self.size = lo, tuple(hi[d] - lo[d] for d in range(3))
@@ -116,8 +122,8 @@ class SMRMesh:
 
         def face_bc(face):
             d, upper = face // 2, face % 2
-            if d >= self.ndim:
-                return "periodic"
+            if d >= self.ndim or (self.periodic[d] and nl[d] == 1):
+                return "periodic"                   # the block spans the periodic direction itself
             at_edge = (loc[d] == nl[d] - 1) if upper else (loc[d] == 0)
             return self.base.bc[face] if (at_edge and not self.periodic[d]) else "exchange"
         spec = dataclasses.replace(self.base, nx1=self.nx[0], nx2=self.nx[1], nx3=self.nx[2],

@@ -376,11 +376,11 @@ def test_conserved_exchange_matches_oracle_inversion(oracle_mod, name):
 
 
 # ------------------------------------------------------------------ B_CT meshes in spherical KS
-def ks_ct_base(nx):
+def ks_ct_base(nx, poles="reflecting"):
     import dataclasses as dc
     from kharma_b200.spec import bondi_spec
     s = bondi_spec(nx, nx, nx, float(np.log(3.0)), float(np.log(30.0)), 0.0, 1.0, 0.0, 2 * np.pi, recon="linear_mc",
-                   bc=("outflow", "outflow", "reflecting", "reflecting", "periodic", "periodic"))
+                   bc=("outflow", "outflow", poles, poles, "periodic", "periodic"))
     return dc.replace(s, nvar=8, b_ct="gs05_c")
 
 
@@ -442,19 +442,23 @@ def test_ks_refined_mesh_keeps_divb(conserved):
     assert interface_mismatch(m) < 1e-12 * scale
 
 
+@pytest.mark.parametrize("poles", ["reflecting", "transmitting"])
 @pytest.mark.parametrize("conserved", [False, True])
-def test_ks_one_level_steps_as_one_block(conserved):
-    """2x2x2 spherical-KS B_CT blocks step as the single block of the domain to 1e-9 of each
+def test_ks_one_level_steps_as_one_block(conserved, poles):
+    """2x2x2 spherical-KS B_CT blocks (reflecting poles), or 2x2x1 blocks spanning x3 (transmitting
+    poles: the mirror rows half-way round in x3 and the averaged polar EMFs inside each block), step
+    as the single block of the domain to 1e-9 of each
     variable's (velocities and fields: their group's) largest magnitude over 3 steps, with either
     exchange.  Not bitwise: each block evaluates its metric, and the connection as a centred difference
     of it with step 1e-8, at its own zone centres, which differ from the single block's by rounding."""
     import dataclasses as dc
     from kharma_b200 import problems
     from kharma_b200.block import build_geometry
-    base_ = ks_ct_base(16)
-    mesh = SMRMesh(base_, (2, 2, 2), (16, 16, 16))
-    big = dc.replace(base_, nx1=32, nx2=32, nx3=32)
-    one = SMRMesh(big, (1, 1, 1), (32, 32, 32))
+    base_ = ks_ct_base(16, poles)
+    nb3 = 2 if poles == "reflecting" else 1
+    mesh = SMRMesh(base_, (2, 2, nb3), (16, 16, 16))
+    big = dc.replace(base_, nx1=32, nx2=32, nx3=16 * nb3)
+    one = SMRMesh(big, (1, 1, 1), (32, 32, 16 * nb3))
     ng = big.ng
     P5 = problems.bondi(dc.replace(big, nvar=5, b_ct="none"), build_geometry(big))
     Pbig = np.zeros((8,) + P5.shape[1:])

@@ -270,8 +270,10 @@ def test_mks_exchange_matches_restatement():
 
 
 @pytest.mark.parametrize("conserved", [False, True])
-def test_mks_one_level_steps_as_one_block(conserved):
-    """2x2x2 MKS blocks of the Bondi problem (outflow x1, reflecting x2, periodic x3) step as the
+@pytest.mark.parametrize("poles", ["reflecting", "transmitting"])
+def test_mks_one_level_steps_as_one_block(conserved, poles):
+    """2x2x2 MKS blocks of the Bondi problem (outflow x1, reflecting x2, periodic x3) — or 2x2x1
+    blocks spanning x3 with transmitting poles — step as the
     single block of the domain, with either exchange, to 1e-9 of each variable's (velocities: the
     velocity's) largest magnitude over 3 steps.  Not bitwise: each block evaluates its metric at its
     own zone centres, which differ from the single block's by rounding, and the connection is a
@@ -279,9 +281,11 @@ def test_mks_one_level_steps_as_one_block(conserved):
     shifts of the centres move it by up to ~1e-8 of its size; over 3 steps that leaves ~1e-11."""
     from kharma_b200.batch import Batch
     from kharma_b200.block import build_geometry
-    base_ = mks_base(16)
-    mesh = SMRMesh(base_, (2, 2, 2), (16, 16, 16))
-    big = dataclasses.replace(base_, nx1=32, nx2=32, nx3=32)
+    bc = ("outflow", "outflow", poles, poles, "periodic", "periodic")
+    base_ = mks_base(16, bc=bc)
+    nb3 = 2 if poles == "reflecting" else 1
+    mesh = SMRMesh(base_, (2, 2, nb3), (16, 16, 16))
+    big = dataclasses.replace(base_, nx1=32, nx2=32, nx3=16 * nb3)
     ng = big.ng
     Pbig = problems.bondi(big, build_geometry(big))
 

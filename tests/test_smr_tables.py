@@ -86,3 +86,21 @@ def test_unbalanced_mesh_is_rejected():
     mesh = SMRMesh(hydro_base(2), (2, 2, 1), (8, 8, 1), refine=[(0, 0, 0), (1, (0, 0, 0))])
     with pytest.raises(AssertionError, match="2:1"):
         mesh.tables()
+
+
+def test_transmitting_poles_mesh():
+    """Transmitting x2 faces: root blocks spanning all of a periodic x3 keep them (x3 periodic on
+    the block itself); refined blocks are kept off the poles; split x3 roots are rejected."""
+    import numpy as np
+    from kharma_b200.spec import bondi_spec
+    bc = ("outflow", "outflow", "transmitting", "transmitting", "periodic", "periodic")
+    base = bondi_spec(16, 16, 16, float(np.log(3.0)), float(np.log(30.0)), 0.0, 1.0, 0.0, 2 * np.pi, bc=bc)
+    mesh = SMRMesh(base, (4, 4, 1), (16, 16, 16), refine=[(1, 1, 0)])
+    polar = [b for b in mesh.blocks if b.level == 0 and b.loc[1] in (0, 3)]
+    assert polar and all(b.spec.bc[4:] == ("periodic", "periodic") for b in polar)
+    assert all(("transmitting" in b.spec.bc[2:4]) == (b.loc[1] in (0, 3)) for b in mesh.blocks if b.level == 0)
+    assert all(b.spec.bc[4:] == ("exchange", "exchange") for b in mesh.blocks if b.level == 1)
+    with pytest.raises(AssertionError):
+        SMRMesh(base, (4, 4, 1), (16, 16, 16), refine=[(1, 0, 0)])
+    with pytest.raises(AssertionError):
+        SMRMesh(base, (4, 4, 2), (16, 16, 16))
