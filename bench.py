@@ -591,6 +591,51 @@ def smr_form(steps=20, warm=3):
         torch.cuda.empty_cache()
     out["ks_bondi"] = ks_out
     out["b_ct_mhd"] = smr_b_ct_form()
+    out["b_ct_torus"] = smr_b_ct_torus_form()
+    return out
+
+
+def smr_b_ct_torus_form(steps=5, warm=2):
+    """The FM torus (FMKS, a = 0.9375, MC, LLF, drift-frame floors, outflow x1 with inflow checks,
+    reflecting x2 with the polar flux fixes, periodic x3) on a two-level B_CT mesh: 4 x 4 x 2 root
+    blocks of 32^3 with the central 2 x 2 x 2 refined (24 + 64 = 88 blocks), a weak field (the curl of
+    a vector potential in native coordinates, no normal field at the poles), gs05_c EMFs, FP64, the
+    kharma driver's exchange; the CUDA-graph step with the per-block work over 8 streams.  CUDA events
+    on the current stream; max face divergence after the run."""
+    import dataclasses
+    import torch
+    from kharma_b200 import ctmesh
+    from kharma_b200.ctmesh import cut
+    from kharma_b200.mesh import SMRMesh
+    from kharma_b200.spec import torus_spec
+
+    # the domain of the 128 x 128 x 64 torus: 5.5 level-0 zones inside the horizon
+    base = dataclasses.replace(torus_spec(128, 128, 64), b_ct="gs05_c")
+    refine = [(i, j, k) for i in (1, 2) for j in (1, 2) for k in (0, 1)]
+    mesh = SMRMesh(base, (4, 4, 2), (32, 32, 32), refine=refine)
+    m = ctmesh.CTMesh(mesh, ctmesh.torus_blocks(mesh), cut(mesh, ctmesh.potential_faces_levels(mesh, 1e-3, 5e-4)),
+                      streams=8)
+    dt = 1e-3
+    for _ in range(warm):
+        m.step_graph(dt)
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        m.step_graph(dt)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out = {"workload": f"FM torus (FMKS a=0.9375) on a two-level B_CT mesh: {len(mesh.blocks)} blocks of 32^3 "
+                       f"(24 + 64), {mesh.zones:,} zones, MC, LLF, gs05_c, drift floors, FP64, kharma driver exchange",
+           "graph_ms_per_step": ms, "zone_cycles_per_s": mesh.zones / (ms / 1000.0),
+           "max_face_divb_dx_after": m.max_divb() * min(min(b.spec.dx) for b in mesh.blocks),
+           "all_finite": bool(all(torch.isfinite(b.P).all() for b in m.blocks))}
+    m._graph = None
+    del m
+    torch.cuda.empty_cache()
     return out
 
 

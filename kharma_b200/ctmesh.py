@@ -541,6 +541,51 @@ def curl_faces_levels(mesh, B0=(1.0, 0.5, 0.25), amp=0.05, walls=False):
     return out
 
 
+def potential_faces_levels(mesh, a=0.02, b=0.01):
+    """Whole-domain face arrays (sqrt(-g) B^i) per level for any coordinates: the discrete curl in
+    native coordinates of A_3 = a sin(pi x2^) (1 + x1^) and A_2 = b sin(2 pi x3^) sin(pi x1^), with
+    x^ = corner index / zones along each direction (the same function on every level, periodic in
+    x3).  A_3 does not depend on x3 nor A_2 on x2, so a coarse face is the mean of the fine faces on
+    it to rounding; the normal field vanishes on the x2 faces (poles)."""
+    out = []
+    for L in range(mesh.levels):
+        t = mesh._zones_at(L)
+        dx = level_dx(mesh)[L]
+        u = [np.arange(t[q] + 1) / t[q] for q in range(3)]
+        I1, J2 = np.meshgrid(u[0], u[1], indexing="xy")                # (t2+1, t1+1): A3 at (i f, j f)
+        A3 = a * np.sin(np.pi * J2) * (1 + I1)
+        K3, I1b = np.meshgrid(u[2], u[0], indexing="ij")              # (t3+1, t1+1): A2 at (i f, k f)
+        A2 = b * np.sin(2 * np.pi * K3) * np.sin(np.pi * I1b)
+        F = np.zeros((3, t[2], t[1], t[0]))
+        F[0] = ((A3[1:, :-1] - A3[:-1, :-1]) / dx[1])[None] - ((A2[1:, :-1] - A2[:-1, :-1]) / dx[2])[:, None, :]
+        F[1] = -((A3[:-1, 1:] - A3[:-1, :-1]) / dx[0])[None]
+        F[2] = ((A2[:-1, 1:] - A2[:-1, :-1]) / dx[0])[:, None, :]
+        out.append(F)
+    return out
+
+
+def torus_blocks(mesh, seed=1234, u_jitter=0.08):
+    """Each block's primitives (8, n3, n2, n1) of the FM torus (problems.fm_torus at the block's own
+    zones, the density normalised by the mesh's midplane maximum, the jitter seeded per block), the
+    zone field zero (it comes from the faces)."""
+    import math
+    from . import problems
+    from .block import build_geometry
+    base = mesh.base
+    xs = base.x1min + np.arange(int((base.x1max - base.x1min) / 0.001) + 1) * 0.001
+    rho_max = float(np.max(problems._torus_rho(base.a, 6.0, 12.0, base.gam, 1e-3, np.exp(xs),
+                                               np.full_like(xs, math.pi / 2))))
+    import dataclasses
+    out = []
+    for n, blk in enumerate(mesh.blocks):
+        fluid = dataclasses.replace(blk.spec, nvar=5, b_ct="none")       # no field seeding
+        P5 = problems.fm_torus(fluid, build_geometry(blk.spec), seed=seed + n, u_jitter=u_jitter, rho_max=rho_max)
+        P = np.zeros((8,) + P5.shape[1:])
+        P[:5] = P5
+        out.append(P)
+    return out
+
+
 def fluid_levels(mesh, amp=0.1, v=(0.3, 0.2, 0.1)):
     """Whole-domain primitives (8, t3, t2, t1) per level: an entropy wave rho = 1 + amp sin(2 pi (x1 + x2
     (+ x3))) at uniform pressure and velocity; B slots zero (taken from the faces)."""

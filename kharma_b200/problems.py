@@ -170,7 +170,8 @@ def _torus_rho(a, rin, rmax, gam, kappa, r, th):
     return np.where((lnh >= 0.) & (r >= rin), rho, 0.0)
 
 
-def fm_torus(spec, geom, rin=6.0, rmax=12.0, kappa=1e-3, beta_min=100.0, u_jitter=0.08, seed=1234, faces=False):
+def fm_torus(spec, geom, rin=6.0, rmax=12.0, kappa=1e-3, beta_min=100.0, u_jitter=0.08, seed=1234, faces=False,
+             rho_max=None):
     """Fishbone-Moncrief torus + SANE field, on a spherical-KS FMKS block.
 
     geom: dict with the centre tables 'gcov', 'gcon' (arrays [7][n2+1][n1+1][4][4]) and 'gdet'
@@ -178,6 +179,8 @@ def fm_torus(spec, geom, rin=6.0, rmax=12.0, kappa=1e-3, beta_min=100.0, u_jitte
     curled with the flux-CT averaged curl and normalised so max(p_gas)/max(p_B) = beta_min.
     faces=True also returns the B_CT face field sqrt(-g) B^d (3, n3, n2, n1): the face curl of the
     same A_phi with the same normalisation (B_CT's seeding, divergence-free to rounding).
+    rho_max: the density normalisation (default: the midplane maximum over this block's x1 range,
+    as the reference takes it over the mesh's; a block of a mesh passes the mesh's).
     """
     gam, a = spec.gam, spec.a
     n3, n2, n1 = spec.shape
@@ -219,8 +222,9 @@ def fm_torus(spec, geom, rin=6.0, rmax=12.0, kappa=1e-3, beta_min=100.0, u_jitte
     alpha2 = -1.0 / gcon[..., 0, 0]
     uprim = [ucon_n[1 + v] + ucon_n[0] * alpha2 * gcon[..., 0, 1 + v] for v in range(3)]
     # rho_max along the midplane (fm_torus.cpp:145-169)
-    xs = spec.x1min + np.arange(int((spec.x1max - spec.x1min) / 0.001) + 1) * 0.001
-    rho_max = float(np.max(_torus_rho(a, rin, rmax, gam, kappa, np.exp(xs), np.full_like(xs, math.pi / 2))))
+    if rho_max is None:
+        xs = spec.x1min + np.arange(int((spec.x1max - spec.x1min) / 0.001) + 1) * 0.001
+        rho_max = float(np.max(_torus_rho(a, rin, rmax, gam, kappa, np.exp(xs), np.full_like(xs, math.pi / 2))))
     P = np.zeros((spec.nvar, n3, n2, n1))
     for plane, val in ((0, rho_l / rho_max), (1, u_l / rho_max), (2, uprim[0]), (3, uprim[1]), (4, uprim[2])):
         P[plane] = np.where(inside, val, 0.0)[None, :, :]
